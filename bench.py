@@ -1,0 +1,334 @@
+"""Benchmark of the explicit unstructured FV step on one B200 (or N replicas).
+
+Workload (default): Mach 3 forward-facing step, ~1.0M triangles from a seeded
+Delaunay of a jittered lattice, second-order Green-Gauss + smooth-switch
+limiter with Venkatakrishnan phi (K = 5), Roe flux, 5-stage RK, CFL 0.8,
+global time step.  One bench step = one RK5 time step over the whole mesh.
+
+Metric: cell-updates per second per RK stage = n_real * stages * steps / time.
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+Under torchrun every rank runs an independent replica of the workload (the
+single-GPU path has no data exchange); value = all ranks' cell updates /
+max-over-ranks device time.  Prints one JSON line on rank 0.
+"""
+import argparse
+import json
+import os
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "finite-volume-2d-cpp_b200")
+ORACLE = os.path.join(ROOT, "oracle")
+for _p in (PKG, ORACLE):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+import numpy as np  # noqa: E402
+
+import meshgen  # noqa: E402
+import physics as P  # noqa: E402
+
+METRIC = "cell-updates/s per RK stage"
+UNIT = "cell-updates/s"
+# Algorithmic (unique compulsory) bytes per cell and RK stage, FP64, V = 4,
+# E/N = 1.5 (one figure per kernel):
+#   gradients + limiters: q 32 + area 8 + centroid 16 + edges 1.5*(8 + 5*8) = 72 ... = 224
+#   flux + update + ghost fill: q, gx, gy, lim 128 + q_base 32 + area 8 + centroid 16
+#                               + edges 1.5*(8 + 5*8) = 72 + write 32 + dt 8 = 296
+ALGO_BYTES = {"grad_lim": 224.0, "stage": 296.0, "stage_o1": 160.0, "dt": 96.0}
+
+
+def build_workload(name):
+    if name == "step":
+        em = meshgen.forward_step()
+        ph = P.forward_step(order2=True, limiter="venkat", K=5.0, cfl=0.8)
+        return em, ph, P.RK5_ALPHA, lambda ccx, n: P.ic_forward_step(n), \
+            "forward step Mach 3, 2nd-order GG + Venkatakrishnan K=5, RK5, CFL 0.8"
+    if name == "sod":
+        em = meshgen.sod_strip(400, 40)
+        return em, P.sod(cfl=0.5), P.RK1_ALPHA, lambda ccx, n: P.ic_sod(ccx), \
+            "Sod shock tube 400x40x2, 1st-order Roe, RK1, CFL 0.5"
+    if name == "naca":
+        em = meshgen.naca_ogrid()
+        return em, P.naca(), P.RK5_ALPHA, lambda ccx, n: P.ic_naca(n), \
+            "NACA 0012 O-grid 1024x512x2, M 0.8, Michalak, local dt, RK5"
+    raise SystemExit(f"unknown workload {name}")
+
+
+class ClockSampler:
+    """SM clocks and clock-event (throttle) reasons sampled through NVML every
+    few milliseconds while the timed region runs."""
+
+    REASONS = {"hw_slowdown": 0x8, "hw_thermal_slowdown": 0x40, "sw_thermal_slowdown": 0x20,
+               "sw_power_cap": 0x4}
+
+    def __init__(self, index, period_s=0.005):
+        self.index = index
+        self.period = period_s
+        self.sm, self.reasons = [], set()
+        self.max_sm = None
+        self._stop = threading.Event()
+
+    def __enter__(self):
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            self.nv = pynvml
+            self.h = pynvml.nvmlDeviceGetHandleByIndex(self.index)
+            self.max_sm = pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM)
+            self.thread = threading.Thread(target=self._loop, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.nv = None
+        return self
+
+    def _sample(self):
+        nv = self.nv
+        self.sm.append(nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM))
+        try:
+            r = nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+        except AttributeError:
+            r = nv.nvmlDeviceGetCurrentClocksThrottleReasons(self.h)
+        for name, bit in self.REASONS.items():
+            if r & bit:
+                self.reasons.add(name)
+
+    def _loop(self):
+        while not self._stop.is_set():
+            try:
+                self._sample()
+            except Exception:
+                return
+            time.sleep(self.period)
+
+    def __exit__(self, *a):
+        self._stop.set()
+        if self.nv is not None:
+            self.thread.join(timeout=2)
+            try:
+                self._sample()  # at least one sample at the end of the region
+            except Exception:
+                pass
+
+    def summary(self):
+        if not self.sm:
+            return {"sm_mhz": None, "sm_max_mhz": self.max_sm, "reasons": ["unsampled"]}
+        return {"sm_mhz": float(np.median(self.sm)), "sm_max_mhz": self.max_sm,
+                "reasons": sorted(self.reasons), "samples": len(self.sm)}
+
+
+def measured_peak_hbm():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+# --------------------------------------------------------------- reference --
+def _ref_worker(args):
+    """One single-rank reference process (spawned): K RK1 steps on the mesh."""
+    variant, base, consts, aliases, n_total, warmup, steps = args
+    from oracle import RefLib
+    ref = RefLib(variant)
+    for name, src in aliases.items():
+        ref.bc_set(name, ref.bc_get(src))
+    ref.set_consts(**consts)
+    if ref.lib.ref_read_mesh(base.encode()) != 0:
+        raise RuntimeError("reference reader failed")
+    s = np.zeros(5, np.int64)
+    import ctypes
+    ref.lib.ref_mesh_sizes(s.ctypes.data_as(ctypes.c_void_p))
+    ref.n_nodes, ref.n_real, ref.n_total, ref.n_edges, ref.n_bound = (int(x) for x in s)
+    ref.nq = ref.V * ref.n_total
+    q0 = P.ic_forward_step(ref.n_total).ravel()
+    r = ref.run_loop(q0, P.RK1_ALPHA, max(warmup, 1))
+    t0 = time.perf_counter()
+    ref.run_loop(r["q"], P.RK1_ALPHA, steps)
+    return time.perf_counter() - t0, ref.n_real
+
+
+def reference_samples(em, procs, warmup, steps):
+    """Times the reference library (oracle/_ref, built from the reference's
+    own sources) on the forward-step workload in `procs` independent
+    single-rank processes.  Returns (cell-updates/s aggregate, sample text)."""
+    import multiprocessing as mp
+    from oracle import ref_available
+    if not ref_available("forwardStep_o2venk5"):
+        return None
+    tmp = tempfile.mkdtemp(prefix="fvbench_")
+    base = os.path.join(tmp, "step")
+    meshgen.write_msh41(base + ".msh", em)
+    job = ("forwardStep_o2venk5", base, dict(cfl=0.8), {"step": "wall"}, 0, warmup, steps)
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(procs) as pool:
+        res = pool.map(_ref_worker, [job] * procs)
+    t = max(r[0] for r in res)
+    n = res[0][1]
+    return procs * n * steps / t, n
+
+
+def run_reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    em, ph, alpha, ic, desc = build_workload("step")
+    procs = os.cpu_count() or 1
+    r = reference_samples(em, procs, args.warmup, args.steps)
+    if r is None:
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref not built (reference sources absent when building)"}))
+        return
+    value, n = r
+    sample = (f"{procs} independent single-rank processes of the reference library (no MPI on the box), "
+              f"each {args.steps} single-stage steps (calc_dt + complete_calc_qt + update_cells + update_bounds) "
+              f"of the {n}-cell forward step after {args.warmup} warm-up steps")
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": desc, "n_real_cells": n, "parallelism": f"{procs} host processes"},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": procs, "kind": "reference", "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+# ---------------------------------------------------------------- our arm --
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=500)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="step", choices=["step", "sod", "naca"])
+    ap.add_argument("--precision", default="fp64_exact", choices=["fp64_exact", "fp64", "fp32"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    if args.impl == "reference":
+        return run_reference_arm(args)
+
+    import torch
+    import fvgpu
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    em, ph, alpha, ic, desc = build_workload(args.workload)
+    mesh = fvgpu.Mesh.from_elements(em)
+    geo = mesh.geometry()
+    s = fvgpu.Solver(mesh, ph, args.precision, device=local)
+    stream = torch.cuda.Stream(device=local)
+    s.set_stream(stream.cuda_stream)
+    q0 = ic(geo["ccx"], mesh.n_total).ravel()
+    s.set_state(q0)
+    stages = len(alpha)
+    N = mesh.n_real
+
+    # warm-up (also builds the step graph)
+    s.run(args.warmup, alpha=alpha)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    barrier(); torch.cuda.synchronize()
+    ev0 = torch.cuda.Event(enable_timing=True); ev1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        ev0.record(stream)
+        info = s.run(args.warmup + args.steps, alpha=alpha, restart=False)
+        ev1.record(stream)
+        ev1.synchronize()
+    barrier(); torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    assert info["step"] == args.warmup + args.steps
+    launches = s.last_run_stats()[1]  # kernels launched inside the timed region
+    ms_t = torch.tensor([ms], device=f"cuda:{local}")
+    if dist is not None:
+        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
+    ms_max = float(ms_t.item())
+    value = world * N * stages * args.steps / (ms_max / 1e3)
+    healthy = s.check_state() == 0
+
+    # end to end through the C ABI with pinned host buffers, every step:
+    # H2D of the state, one time step, D2H of the state
+    nq = mesh.n_total * ph.V
+    h_in = torch.from_numpy(s.get_state()).pin_memory()
+    h_out = torch.empty(nq, dtype=torch.float64).pin_memory()
+    e2e_steps = max(3, min(args.steps, 20))
+    s.set_chunk(1)
+    s.set_state_ptr(h_in.data_ptr(), device=False)
+    s.run(1, alpha=alpha)  # builds the one-step graph outside the timed region
+    barrier(); torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for k in range(e2e_steps):
+        s.set_state_ptr(h_in.data_ptr(), device=False)
+        s.run(k + 1, alpha=alpha, restart=(k == 0))
+        s.get_state_ptr(h_out.data_ptr(), device=False)
+    torch.cuda.synchronize()
+    e2e_wall = time.perf_counter() - t0
+    s.set_chunk(16)
+    barrier()
+    e2e_t = torch.tensor([e2e_wall], device=f"cuda:{local}")
+    if dist is not None:
+        dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
+    e2e_value = world * N * stages * e2e_steps / float(e2e_t.item())
+
+    # per-kernel device timing (events around every kernel, same stream)
+    prof_steps = max(2, min(args.steps, 10))
+    ms_k = np.zeros(5); cnt_k = np.zeros(5, np.int64)
+    a = np.ascontiguousarray(alpha, np.float64)
+    import ctypes as C
+    rc = fvgpu.lib().fv_profile_kernels(s._h, a.ctypes.data_as(C.POINTER(C.c_double)), C.c_int32(a.size),
+                                        C.c_int32(prof_steps), ms_k.ctypes.data_as(C.POINTER(C.c_double)),
+                                        cnt_k.ctypes.data_as(C.POINTER(C.c_int64)))
+    fvgpu._check(rc)
+    kinds = ["step_begin", "dt", "grad_lim", "stage", "step_end"]
+    per_launch = {kinds[k]: (ms_k[k] / cnt_k[k] if cnt_k[k] else 0.0) for k in range(5)}
+    stage_key = "stage" if ph.order2 else "stage_o1"
+    stage_bytes = ALGO_BYTES[stage_key] * N
+    peak, peak_kind = measured_peak_hbm()
+    achieved = stage_bytes / (per_launch["stage"] / 1e3) / 1e9
+    share = {kinds[k]: float(ms_k[k] / ms_k.sum()) for k in range(5)}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision != "fp32" else "f32+f64",
+                "data": "synthetic",
+                "config": {"workload": desc, "n_real_cells": N, "n_edges": mesh.n_edges, "stages": stages,
+                           "precision": args.precision, "l2": "inputs larger than L2 (working set > 126 MB)",
+                           "parallelism": f"{world} independent replicas" if world > 1 else "single GPU"},
+                "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": nq * 8, "d2h_bytes_per_step": nq * 8,
+                        "steps": e2e_steps},
+                "gpu_launches": int(launches),
+                "roofline": {"bound": "hbm", "kernel": "flux+update+ghost fill (k_stage)",
+                             "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                             "peak_source": peak_kind, "traffic": None,
+                             "algorithmic_bytes_per_launch": stage_bytes},
+                "kernel_ms_per_launch": per_launch, "kernel_time_share": share,
+                "clocks": clk.summary(), "state_finite": bool(healthy)}
+        if not args.no_cpu_baseline and world == 1:
+            r = reference_samples(em, 1, 1, 25)
+            if r is not None:
+                line["cpu_baseline"] = {"value": r[0], "unit": UNIT, "cores": 1, "kind": "reference",
+                                        "sample": f"reference library, 1 process, 25 single-stage steps of the {r[1]}-cell mesh"}
+        print(json.dumps(line))
+    s.close()
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,435 @@
+// Host mesh construction: reference-equivalent geometry, MSH 4.1 reader,
+// Hilbert renumbering and per-cell face lists.
+#include "fv_mesh.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <map>
+#include <numeric>
+#include <sstream>
+
+namespace fvgpu {
+
+namespace {
+
+// Open-addressing map from an undirected node pair to an edge index.
+struct EdgeMap {
+    std::vector<uint64_t> key;
+    std::vector<int64_t> val;
+    uint64_t mask = 0;
+    explicit EdgeMap(size_t expected) {
+        size_t cap = 16;
+        while (cap < 2 * expected + 16) cap <<= 1;
+        key.assign(cap, UINT64_MAX);
+        val.assign(cap, -1);
+        mask = cap - 1;
+    }
+    static uint64_t mix(uint64_t x) {
+        x ^= x >> 33; x *= 0xff51afd7ed558ccdULL; x ^= x >> 33; x *= 0xc4ceb9fe1a85ec53ULL; x ^= x >> 33;
+        return x;
+    }
+    static uint64_t make(uint32_t a, uint32_t b) {
+        uint32_t lo = std::min(a, b), hi = std::max(a, b);
+        return (uint64_t(lo) << 32) | hi;
+    }
+    // returns slot value pointer; *found tells whether the key existed
+    int64_t* slot(uint64_t k, bool* found) {
+        uint64_t h = mix(k) & mask;
+        while (key[h] != UINT64_MAX) {
+            if (key[h] == k) { *found = true; return &val[h]; }
+            h = (h + 1) & mask;
+        }
+        *found = false;
+        key[h] = k;
+        return &val[h];
+    }
+    int64_t find(uint64_t k) const {
+        uint64_t h = mix(k) & mask;
+        while (key[h] != UINT64_MAX) {
+            if (key[h] == k) return val[h];
+            h = (h + 1) & mask;
+        }
+        return -1;
+    }
+};
+
+// Hilbert index of (x, y) on a 2^order grid (the classic rotate-and-reflect walk).
+uint64_t hilbert_d(uint32_t x, uint32_t y, int order) {
+    uint64_t d = 0;
+    for (uint32_t s = 1u << (order - 1); s > 0; s >>= 1) {
+        uint32_t rx = (x & s) > 0, ry = (y & s) > 0;
+        d += uint64_t(s) * s * ((3 * rx) ^ ry);
+        if (ry == 0) {
+            if (rx == 1) { x = s - 1 - x; y = s - 1 - y; }
+            std::swap(x, y);
+        }
+    }
+    return d;
+}
+
+}  // namespace
+
+// mesh::read_file's geometry passes: add_cell_edges (mesh.cpp:130-154),
+// convert_node_face_info (157-187), compute_mesh (190-260) and
+// add_boundary_cells (623-669).  Same arithmetic, same order, so every
+// array is bit-identical to the reference's.
+std::string build_geometry(HostMesh& m) {
+    const int64_t nc = (int64_t)m.cells4.size() / 4;
+    const int64_t nb = (int64_t)m.bnd_group.size();
+    const double* X = m.nodes_x.data();
+    const double* Y = m.nodes_y.data();
+    const int64_t nn = (int64_t)m.nodes_x.size();
+    for (int64_t c = 0; c < nc; ++c)
+        for (int k = 0; k < 4; ++k) {
+            int32_t v = m.cells4[4 * c + k];
+            if ((k < 3 && v < 0) || v >= nn) return "cell " + std::to_string(c) + " has an invalid node";
+        }
+    EdgeMap em((size_t)(2 * nc + 4));
+    m.edge_cells.clear(); m.edge_nodes.clear();
+    m.edge_cells.reserve(3 * nc); m.edge_nodes.reserve(3 * nc);
+    for (int64_t c = 0; c < nc; ++c) {
+        const int32_t* cn = &m.cells4[4 * c];
+        const int sz = cn[3] < 0 ? 3 : 4;
+        for (int i = 0; i < sz; ++i) {
+            const int j = (i < sz - 1) ? i + 1 : 0;
+            bool found;
+            int64_t* v = em.slot(EdgeMap::make(cn[i], cn[j]), &found);
+            if (!found) {
+                *v = (int64_t)m.edge_cells.size() / 2;
+                m.edge_cells.push_back((uint32_t)c); m.edge_cells.push_back(0);
+                m.edge_nodes.push_back(cn[i]); m.edge_nodes.push_back(cn[j]);
+            }
+        }
+    }
+    const int64_t E = (int64_t)m.edge_cells.size() / 2;
+    for (int64_t c = 0; c < nc; ++c) {
+        const int32_t* cn = &m.cells4[4 * c];
+        const int sz = cn[3] < 0 ? 3 : 4;
+        for (int i = 0; i < sz; ++i) {
+            const int j = (i < sz - 1) ? i + 1 : 0;
+            int64_t e = em.find(EdgeMap::make(cn[i], cn[j]));
+            if ((uint32_t)c != m.edge_cells[2 * e]) {
+                if (m.edge_cells[2 * e + 1] != 0 && m.edge_cells[2 * e + 1] != (uint32_t)c)
+                    return "edge shared by more than two cells (non-manifold mesh)";
+                m.edge_cells[2 * e + 1] = (uint32_t)c;
+            }
+        }
+    }
+    const int64_t nt = nc + nb;
+    m.n_real = nc; m.n_total = nt; m.n_edges = E; m.n_bound = nb;
+    m.enx.assign(E, 0.); m.eny.assign(E, 0.); m.elen.assign(E, 0.);
+    m.ecx.assign(E, 0.); m.ecy.assign(E, 0.);
+    m.area.assign(nt, 0.); m.ccx.assign(nt, 0.); m.ccy.assign(nt, 0.);
+    for (int64_t c = 0; c < nc; ++c) {
+        const int32_t* cn = &m.cells4[4 * c];
+        const int sz = cn[3] < 0 ? 3 : 4;
+        double cx = 0., cy = 0.;
+        for (int j = 0; j < sz; ++j) {
+            cx += X[cn[j]] / ((double)sz);
+            cy += Y[cn[j]] / ((double)sz);
+        }
+        m.ccx[c] = cx; m.ccy[c] = cy;
+    }
+    for (int64_t e = 0; e < E; ++e) {
+        const uint32_t a = m.edge_nodes[2 * e], b = m.edge_nodes[2 * e + 1];
+        m.ecx[e] = (X[b] + X[a]) * 0.5;
+        m.ecy[e] = (Y[b] + Y[a]) * 0.5;
+        double dex = X[b] - X[a], dey = Y[b] - Y[a];
+        double l = std::sqrt(dex * dex + dey * dey);
+        m.elen[e] = l;
+        m.enx[e] = -dey / l;
+        m.eny[e] = dex / l;
+        const uint32_t c0 = m.edge_cells[2 * e];
+        double dot = m.enx[e] * (m.ecx[e] - m.ccx[c0]) + m.eny[e] * (m.ecy[e] - m.ccy[c0]);
+        if (dot < 0) { m.enx[e] *= -1.; m.eny[e] *= -1.; }
+    }
+    for (int64_t c = 0; c < nc; ++c) {
+        const int32_t* cn = &m.cells4[4 * c];
+        double x1 = X[cn[0]], x2 = X[cn[1]], x3 = X[cn[2]];
+        double y1 = Y[cn[0]], y2 = Y[cn[1]], y3 = Y[cn[2]];
+        if (cn[3] < 0) {
+            m.area[c] = 0.5 * std::fabs(x1 * (y2 - y3) + x2 * (y3 - y1) + x3 * (y1 - y2));
+        } else {
+            double x4 = X[cn[3]], y4 = Y[cn[3]];
+            m.area[c] = 0.5 * std::fabs(x1 * (y2 - y3) + x2 * (y3 - y1) + x3 * (y1 - y2)) +
+                        0.5 * std::fabs(x1 * (y3 - y4) + x3 * (y4 - y1) + x4 * (y1 - y3));
+        }
+        if (!(m.area[c] >= 1e-300)) return "cell " + std::to_string(c) + " has zero area";
+    }
+    m.bound_edges.assign(nb, 0);
+    std::vector<uint8_t> is_bnd(E, 0);
+    for (int64_t b = 0; b < nb; ++b) {
+        int64_t e = em.find(EdgeMap::make(m.bnd_nodes[2 * b], m.bnd_nodes[2 * b + 1]));
+        if (e < 0)
+            return "invalid edge ref (" + std::to_string(std::min(m.bnd_nodes[2 * b], m.bnd_nodes[2 * b + 1])) +
+                   ", " + std::to_string(std::max(m.bnd_nodes[2 * b], m.bnd_nodes[2 * b + 1])) + ")";
+        if (is_bnd[e]) return "boundary segment listed twice";
+        if (m.edge_cells[2 * e + 1] != 0) return "boundary segment on an interior edge";
+        is_bnd[e] = 1;
+        const uint32_t cell = m.edge_cells[2 * e];
+        double dx = m.ecx[e] - m.ccx[cell], dy = m.ecy[e] - m.ccy[cell];
+        double dist = std::sqrt(dx * dx + dy * dy);
+        const int64_t g = nc + b;
+        m.area[g] = m.area[cell];
+        m.ccx[g] = m.ecx[e] + dist * m.enx[e];
+        m.ccy[g] = m.ecy[e] + dist * m.eny[e];
+        m.edge_cells[2 * e + 1] = (uint32_t)g;
+        m.bound_edges[b] = (uint32_t)e;
+    }
+    // Every edge must now have a second cell: an edge seen by one cell only
+    // and not declared as a boundary would point at cell 0 in the reference.
+    std::vector<uint8_t> deg(nc, 0);
+    for (int64_t e = 0; e < E; ++e) {
+        uint32_t i = m.edge_cells[2 * e], j = m.edge_cells[2 * e + 1];
+        if (i == j) return "edge " + std::to_string(e) + " has one cell and is not a boundary segment";
+        if (i < (uint32_t)nc) deg[i]++;
+        if (j < (uint32_t)nc) deg[j]++;
+    }
+    for (int64_t c = 0; c < nc; ++c) {
+        const int sz = m.cells4[4 * c + 3] < 0 ? 3 : 4;
+        if (deg[c] != sz) return "cell " + std::to_string(c) + " has an open face (undeclared boundary)";
+    }
+    return "";
+}
+
+void build_device_numbering(HostMesh& m) {
+    const int64_t nc = m.n_real, nt = m.n_total, E = m.n_edges;
+    double xmin = 1e300, xmax = -1e300, ymin = 1e300, ymax = -1e300;
+    for (int64_t c = 0; c < nc; ++c) {
+        xmin = std::min(xmin, m.ccx[c]); xmax = std::max(xmax, m.ccx[c]);
+        ymin = std::min(ymin, m.ccy[c]); ymax = std::max(ymax, m.ccy[c]);
+    }
+    const int order = 16;
+    const double span = std::max(std::max(xmax - xmin, ymax - ymin), 1e-300);
+    const double scale = ((1u << order) - 1) / span;
+    std::vector<uint64_t> key(nc);
+    for (int64_t c = 0; c < nc; ++c) {
+        uint32_t qx = (uint32_t)((m.ccx[c] - xmin) * scale);
+        uint32_t qy = (uint32_t)((m.ccy[c] - ymin) * scale);
+        key[c] = hilbert_d(qx, qy, order);
+    }
+    m.new2ref.resize(nt);
+    std::iota(m.new2ref.begin(), m.new2ref.begin() + nc, 0);
+    std::stable_sort(m.new2ref.begin(), m.new2ref.begin() + nc,
+                     [&](int32_t a, int32_t b) { return key[a] < key[b]; });
+    m.ref2new.assign(nt, -1);
+    for (int64_t n = 0; n < nc; ++n) m.ref2new[m.new2ref[n]] = (int32_t)n;
+    // ghosts follow their interior cell's new index (stable in reference order)
+    std::vector<int32_t> gorder(m.n_bound);
+    std::iota(gorder.begin(), gorder.end(), 0);
+    std::stable_sort(gorder.begin(), gorder.end(), [&](int32_t a, int32_t b) {
+        return m.ref2new[m.edge_cells[2 * m.bound_edges[a]]] < m.ref2new[m.edge_cells[2 * m.bound_edges[b]]];
+    });
+    for (int64_t k = 0; k < m.n_bound; ++k) {
+        const int32_t ref = (int32_t)(nc + gorder[k]);
+        m.new2ref[nc + k] = ref;
+        m.ref2new[ref] = (int32_t)(nc + k);
+    }
+    // faces per new cell in increasing reference edge order
+    m.face_edge.assign(nc * HostMesh::MAXF, -1);
+    m.face_side.assign(nc * HostMesh::MAXF, 0);
+    m.n_faces.assign(nc, 0);
+    for (int64_t e = 0; e < E; ++e) {
+        for (int s = 0; s < 2; ++s) {
+            const uint32_t rc = m.edge_cells[2 * e + s];
+            if (rc >= (uint32_t)nc) continue;
+            const int32_t c = m.ref2new[rc];
+            const int k = m.n_faces[c]++;
+            m.face_edge[c * HostMesh::MAXF + k] = (int32_t)e;
+            m.face_side[c * HostMesh::MAXF + k] = (uint8_t)s;
+        }
+    }
+}
+
+// The per-face quantities use the reference's arithmetic: the Green-Gauss
+// weight of calc_gradients (explicit.cpp:132-140) and the face-centre offsets
+// of calc_limiters / calc_time_derivatives (explicit.cpp:216-217, 297-301).
+void build_face_arrays(const HostMesh& m, FaceArrays& fa) {
+    const int64_t N = m.n_real, NT = m.n_total, F = HostMesh::MAXF;
+    fa.nbr.assign(F * N, 0xFFFFFFFFu);
+    for (auto* v : {&fa.nx, &fa.ny, &fa.le, &fa.g, &fa.dsx, &fa.dsy, &fa.dnx, &fa.dny}) v->assign(F * N, 0.);
+    for (int64_t c = 0; c < N; ++c) {
+        const int32_t self_ref = m.new2ref[c];
+        for (int k = 0; k < m.n_faces[c]; ++k) {
+            const int32_t e = m.face_edge[c * F + k];
+            const int side = m.face_side[c * F + k];
+            const uint32_t i = m.edge_cells[2 * e], j = m.edge_cells[2 * e + 1];
+            const uint32_t nb_ref = side == 0 ? j : i;
+            const size_t s = (size_t)k * N + c;
+            fa.nbr[s] = (uint32_t)m.ref2new[nb_ref] | ((uint32_t)side << 31);
+            fa.nx[s] = m.enx[e]; fa.ny[s] = m.eny[e]; fa.le[s] = m.elen[e];
+            const double dxif = m.ecx[e] - m.ccx[i], dyif = m.ecy[e] - m.ccy[i];
+            const double dif = std::sqrt(dxif * dxif + dyif * dyif);
+            const double dxij = m.ccx[i] - m.ccx[j], dyij = m.ccy[i] - m.ccy[j];
+            const double dij = std::sqrt(dxij * dxij + dyij * dyij);
+            fa.g[s] = dif / dij;
+            fa.dsx[s] = m.ecx[e] - m.ccx[self_ref]; fa.dsy[s] = m.ecy[e] - m.ccy[self_ref];
+            fa.dnx[s] = m.ecx[e] - m.ccx[nb_ref]; fa.dny[s] = m.ecy[e] - m.ccy[nb_ref];
+        }
+    }
+    const int64_t G = m.n_bound;
+    fa.ghost_group.assign(G, 0); fa.ghost_cell.assign(G, 0); fa.ghost_slot.assign(G, 0);
+    for (int64_t b = 0; b < G; ++b) {
+        const int32_t ref = m.new2ref[N + b];          // reference ghost index
+        const int64_t rb = ref - N;                    // its boundary segment
+        const uint32_t e = m.bound_edges[rb];
+        const int32_t c = m.ref2new[m.edge_cells[2 * e]];
+        fa.ghost_group[b] = m.bnd_group[rb];
+        fa.ghost_cell[b] = c;
+        for (int k = 0; k < m.n_faces[c]; ++k)
+            if (m.face_edge[c * F + k] == (int32_t)e) fa.ghost_slot[b] = (uint8_t)k;
+    }
+    fa.area.assign(NT, 0.);
+    for (int64_t n = 0; n < NT; ++n) fa.area[n] = m.area[m.new2ref[n]];
+    fa.cell0 = m.ref2new[0];
+}
+
+// ----------------------------------------------------------------------------
+// MSH 4.1 ASCII reader.  Accepts what fvhyper's reader accepts for a single
+// partition: $PhysicalNames, $Entities (curve -> physical tag, token 8 of a
+// curve line, mesh.cpp:308-311), $Nodes (node index = order of appearance,
+// mesh.cpp:392-401), $Elements (dim-1 two-node elements are boundary
+// segments, mesh.cpp:460-473; dim-2 three/four-node elements are cells in
+// file order, mesh.cpp:528-559).
+// ----------------------------------------------------------------------------
+std::string read_msh41(const std::string& path, HostMesh& m) {
+    FILE* f = std::fopen(path.c_str(), "rb");
+    if (!f) return "cannot open " + path;
+    std::fseek(f, 0, SEEK_END);
+    long sz = std::ftell(f);
+    std::fseek(f, 0, SEEK_SET);
+    std::string buf((size_t)sz, '\0');
+    if (sz > 0 && std::fread(&buf[0], 1, (size_t)sz, f) != (size_t)sz) { std::fclose(f); return "read error"; }
+    std::fclose(f);
+    const char* p = buf.c_str();
+    const char* end = p + buf.size();
+    auto next_line = [&](std::string& line) -> bool {
+        if (p >= end) return false;
+        const char* q = (const char*)std::memchr(p, '\n', end - p);
+        if (!q) q = end;
+        line.assign(p, q);
+        if (!line.empty() && line.back() == '\r') line.pop_back();
+        p = (q < end) ? q + 1 : end;
+        return true;
+    };
+    std::map<long, std::string> phys_names;
+    std::map<long, long> curve_phys;
+    std::map<long, long> node_index;  // MSH node tag -> index
+    std::map<long, int32_t> tag_group;
+    m.nodes_x.clear(); m.nodes_y.clear(); m.cells4.clear();
+    m.bnd_nodes.clear(); m.bnd_group.clear(); m.group_names.clear();
+    std::string line;
+    bool have_nodes = false, have_elements = false;
+    try {
+        while (next_line(line)) {
+            if (line.empty() || line[0] != '$') continue;
+            const std::string sec = line.substr(1);
+            if (sec == "PhysicalNames") {
+                next_line(line);
+                long n = std::stol(line);
+                for (long i = 0; i < n; ++i) {
+                    next_line(line);
+                    std::istringstream ss(line);
+                    long dim, tag; std::string name;
+                    ss >> dim >> tag;
+                    std::getline(ss, name);
+                    name.erase(std::remove(name.begin(), name.end(), '"'), name.end());
+                    name.erase(0, name.find_first_not_of(' '));
+                    phys_names[tag] = name;
+                }
+            } else if (sec == "Entities") {
+                next_line(line);
+                long np, ncv, ns, nv;
+                if (std::sscanf(line.c_str(), "%ld %ld %ld %ld", &np, &ncv, &ns, &nv) != 4) return "bad $Entities header";
+                for (long i = 0; i < np; ++i) next_line(line);
+                for (long i = 0; i < ncv; ++i) {
+                    next_line(line);
+                    std::istringstream ss(line);
+                    std::vector<std::string> tok; std::string t;
+                    while (ss >> t) tok.push_back(t);
+                    if (tok.size() < 9) return "bad curve entity line";
+                    curve_phys[std::stol(tok[0])] = (long)std::stod(tok[8]);
+                }
+            } else if (sec == "PartitionedEntities" || sec == "GhostElements") {
+                return "partitioned meshes are not supported on the single-GPU path";
+            } else if (sec == "Nodes") {
+                next_line(line);
+                long nblocks, nnodes, mn, mx;
+                if (std::sscanf(line.c_str(), "%ld %ld %ld %ld", &nblocks, &nnodes, &mn, &mx) != 4) return "bad $Nodes header";
+                m.nodes_x.reserve(nnodes); m.nodes_y.reserve(nnodes);
+                for (long b = 0; b < nblocks; ++b) {
+                    next_line(line);
+                    long edim, etag, param, nin;
+                    if (std::sscanf(line.c_str(), "%ld %ld %ld %ld", &edim, &etag, &param, &nin) != 4) return "bad node block";
+                    std::vector<long> tags(nin);
+                    for (long i = 0; i < nin; ++i) { next_line(line); tags[i] = std::stol(line); }
+                    for (long i = 0; i < nin; ++i) {
+                        next_line(line);
+                        char* e1; char* e2;
+                        double x = std::strtod(line.c_str(), &e1);
+                        double y = std::strtod(e1, &e2);
+                        node_index[tags[i]] = (long)m.nodes_x.size();
+                        m.nodes_x.push_back(x); m.nodes_y.push_back(y);
+                    }
+                }
+                have_nodes = true;
+            } else if (sec == "Elements") {
+                if (!have_nodes) return "$Elements before $Nodes";
+                next_line(line);
+                long nblocks, nel, mn, mx;
+                if (std::sscanf(line.c_str(), "%ld %ld %ld %ld", &nblocks, &nel, &mn, &mx) != 4) return "bad $Elements header";
+                for (long b = 0; b < nblocks; ++b) {
+                    next_line(line);
+                    long edim, etag, etype, nin;
+                    if (std::sscanf(line.c_str(), "%ld %ld %ld %ld", &edim, &etag, &etype, &nin) != 4) return "bad element block";
+                    int32_t group = -1;
+                    if (edim == 1) {
+                        auto it = curve_phys.find(etag);
+                        if (it == curve_phys.end()) return "curve entity " + std::to_string(etag) + " has no physical tag";
+                        auto g = tag_group.find(it->second);
+                        if (g == tag_group.end()) {
+                            group = (int32_t)m.group_names.size();
+                            tag_group[it->second] = group;
+                            auto nm = phys_names.find(it->second);
+                            m.group_names.push_back(nm == phys_names.end() ? std::string() : nm->second);
+                        } else {
+                            group = g->second;
+                        }
+                    }
+                    for (long i = 0; i < nin; ++i) {
+                        next_line(line);
+                        long v[16]; int nv = 0;
+                        const char* s = line.c_str();
+                        char* e;
+                        while (nv < 16) {
+                            long x = std::strtol(s, &e, 10);
+                            if (e == s) break;
+                            v[nv++] = x; s = e;
+                        }
+                        const int nnode = nv - 1;
+                        if (edim == 1 && nnode == 2) {
+                            m.bnd_nodes.push_back((int32_t)node_index.at(v[1]));
+                            m.bnd_nodes.push_back((int32_t)node_index.at(v[2]));
+                            m.bnd_group.push_back(group);
+                        } else if (edim == 2) {
+                            if (nnode != 3 && nnode != 4) return "only 3- and 4-node cells are supported";
+                            for (int k = 0; k < 4; ++k)
+                                m.cells4.push_back(k < nnode ? (int32_t)node_index.at(v[1 + k]) : -1);
+                        }
+                    }
+                }
+                have_elements = true;
+            }
+        }
+    } catch (const std::exception& ex) {
+        return std::string("malformed MSH file: ") + ex.what();
+    }
+    if (!have_nodes || !have_elements) return "missing $Nodes or $Elements";
+    return "";
+}
+
+}  // namespace fvgpu

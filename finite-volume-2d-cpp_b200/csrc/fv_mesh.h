@@ -1,0 +1,62 @@
+// Host-side finite-volume mesh: the geometry fvhyper's reader builds
+// (fvhyper/src/mesh.cpp:821-853), in the reference numbering, plus the
+// device numbering (Hilbert order of real cells) and the per-cell face
+// lists the kernels gather through.
+#pragma once
+#include <cstdint>
+#include <string>
+#include <vector>
+
+namespace fvgpu {
+
+struct HostMesh {
+    // ---- element mesh (as read) ----
+    std::vector<double> nodes_x, nodes_y;
+    std::vector<int32_t> cells4;        // [n_real][4], -1 pads triangles
+    std::vector<int32_t> bnd_nodes;     // [n_bound][2]
+    std::vector<int32_t> bnd_group;     // [n_bound]
+    std::vector<std::string> group_names;
+
+    // ---- reference-numbered FV geometry (mesh.h:151-171) ----
+    int64_t n_real = 0, n_total = 0, n_edges = 0, n_bound = 0;
+    std::vector<uint32_t> edge_cells, edge_nodes;        // [E][2]
+    std::vector<double> enx, eny, elen, ecx, ecy;        // [E]
+    std::vector<double> area, ccx, ccy;                  // [n_total]
+    std::vector<uint32_t> bound_edges;                   // [n_bound]
+
+    // ---- device numbering ----
+    // new index of reference cell r: ref2new[r]; reference index of new cell n: new2ref[n].
+    // Real cells occupy [0, n_real), ghosts [n_real, n_total) in both numberings.
+    std::vector<int32_t> ref2new, new2ref;
+    // Faces of each new-numbered real cell, in increasing reference edge order
+    // (the order the reference's edge loops accumulate into that cell).
+    static constexpr int MAXF = 4;
+    std::vector<int32_t> face_edge;  // [n_real][MAXF] reference edge index or -1
+    std::vector<uint8_t> face_side;  // [n_real][MAXF] 0: cell is edge_cells(e,0), 1: cell is edge_cells(e,1)
+    std::vector<uint8_t> n_faces;    // [n_real]
+};
+
+// Per-face arrays of the device kernels, slot-major [MAXF][n_real] in device
+// numbering, plus ghost metadata in device ghost order.
+struct FaceArrays {
+    std::vector<uint32_t> nbr;            // neighbour | side << 31, 0xFFFFFFFF if no face
+    std::vector<double> nx, ny, le, g;    // edge normal, length, Green-Gauss weight
+    std::vector<double> dsx, dsy;         // x_f - x_self
+    std::vector<double> dnx, dny;         // x_f - x_neighbour
+    std::vector<int32_t> ghost_group, ghost_cell;
+    std::vector<uint8_t> ghost_slot;
+    std::vector<double> area;             // [n_total] device numbering
+    int32_t cell0 = 0;                    // device index of reference cell 0
+};
+void build_face_arrays(const HostMesh& m, FaceArrays& fa);
+
+// Builds the reference geometry from an element mesh (mesh.cpp:130-260,
+// 623-669).  Returns "" on success, else an error message.
+std::string build_geometry(HostMesh& m);
+// Hilbert renumbering of real cells + ghost order + face lists.
+void build_device_numbering(HostMesh& m);
+// Gmsh MSH 4.1 ASCII reader (the subset fvhyper's reader accepts,
+// mesh.cpp:264-570).  Fills the element-mesh part of m.
+std::string read_msh41(const std::string& path, HostMesh& m);
+
+}  // namespace fvgpu

@@ -1,0 +1,169 @@
+// Device physics kinds in the reference's exact evaluation order.
+//
+// Compiled with -fmad=false: every expression below is evaluated with the
+// same operations, operand order, IEEE divisions and square roots as the
+// reference example code it cites, so the FP64 results are bit-identical to
+// the reference CPU solver.
+#pragma once
+#include "fv_internal.h"
+
+namespace fvgpu {
+namespace exact {
+
+__device__ __forceinline__ double dmin(double a, double b) { return (b < a) ? b : a; }  // std::min
+__device__ __forceinline__ double dmax(double a, double b) { return (a < b) ? b : a; }  // std::max
+
+// Roe flux with the "cures" eigenvalue modification.
+// FS_ASSOC: examples/forwardStep/main.cpp:72-135 (central flux as one sum);
+// otherwise examples/shockTube/main.cpp:68-135 = examples/naca/main.cpp:71-137.
+template <bool FS_ASSOC>
+__device__ __forceinline__ void roe(double gamma, double* f, const double* qi, const double* qj,
+                                    double n0, double n1) {
+    const double pi = (gamma - 1) * (qi[3] - 0.5 / qi[0] * (qi[1] * qi[1] + qi[2] * qi[2]));
+    const double pj = (gamma - 1) * (qj[3] - 0.5 / qj[0] * (qj[1] * qj[1] + qj[2] * qj[2]));
+    const double Vi = (qi[1] * n0 + qi[2] * n1) / qi[0];
+    const double Vj = (qj[1] * n0 + qj[2] * n1) / qj[0];
+    if (FS_ASSOC) {
+        f[0] = (qi[0] * Vi + qj[0] * Vj) * 0.5;
+        f[1] = (qi[1] * Vi + pi * n0 + qj[1] * Vj + pj * n0) * 0.5;
+        f[2] = (qi[2] * Vi + pi * n1 + qj[2] * Vj + pj * n1) * 0.5;
+        f[3] = ((qi[3] + pi) * Vi + (qj[3] + pj) * Vj) * 0.5;
+    } else {
+        f[0] = qi[0] * Vi;
+        f[1] = qi[1] * Vi + pi * n0;
+        f[2] = qi[2] * Vi + pi * n1;
+        f[3] = (qi[3] + pi) * Vi;
+        f[0] += qj[0] * Vj;
+        f[1] += qj[1] * Vj + pj * n0;
+        f[2] += qj[2] * Vj + pj * n1;
+        f[3] += (qj[3] + pj) * Vj;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) f[i] *= 0.5;
+    }
+    const double pL = pi, pR = pj;
+    const double uL = qi[1] / qi[0], vL = qi[2] / qi[0];
+    const double uR = qj[1] / qj[0], vR = qj[2] / qj[0];
+    const double srhoL = sqrt(qi[0]), srhoR = sqrt(qj[0]);
+    const double rho = srhoR * srhoL;
+    const double u = (uL * srhoL + uR * srhoR) / (srhoL + srhoR);
+    const double v = (vL * srhoL + vR * srhoR) / (srhoL + srhoR);
+    const double h = ((qi[3] + pL) / qi[0] * srhoL + (qj[3] + pR) / qj[0] * srhoR) / (srhoL + srhoR);
+    const double q2 = u * u + v * v;
+    const double c = sqrt((gamma - 1.) * (h - 0.5 * q2));
+    const double V = u * n0 + v * n1;
+    const double VR = uR * n0 + vR * n1;
+    const double VL = uL * n0 + vL * n1;
+    const double lambda_cm = fabs(dmin(V - c, VL - c));
+    const double lambda_c = fabs(V);
+    const double lambda_cp = fabs(dmax(V + c, VR + c));
+    const double kF1 = lambda_cm * ((pR - pL) - rho * c * (VR - VL)) / (2. * c * c);
+    const double kF234_0 = lambda_c * ((qj[0] - qi[0]) - (pR - pL) / (c * c));
+    const double kF234_1 = lambda_c * rho;
+    const double kF5 = lambda_cp * ((pR - pL) + rho * c * (VR - VL)) / (2. * c * c);
+    f[0] -= 0.5 * (kF1 + kF234_0 + kF5);
+    f[1] -= 0.5 * (kF1 * (u - c * n0) + kF234_0 * u + kF234_1 * (uR - uL - (VR - VL) * n0) + kF5 * (u + c * n0));
+    f[2] -= 0.5 * (kF1 * (v - c * n1) + kF234_0 * v + kF234_1 * (vR - vL - (VR - VL) * n1) + kF5 * (v + c * n1));
+    f[3] -= 0.5 * (kF1 * (h - c * V) + kF234_0 * q2 * 0.5 + kF234_1 * (u * (uR - uL) + v * (vR - vL) - V * (VR - VL)) + kF5 * (h + c * V));
+}
+
+// Upwind advection flux, examples/burgers/main.cpp:68-96.
+__device__ __forceinline__ void burgers(double* f, const double* qi, const double* qj, double n0, double n1) {
+    const double Vi = qi[0] * n0 + qi[1] * n1;
+    const double Vj = qj[0] * n0 + qj[1] * n1;
+    const double fi0 = Vi * qi[0], fi1 = Vi * qi[1];
+    const double fj0 = Vj * qj[0], fj1 = Vj * qj[1];
+    const double V = dmax(fabs(Vi), fabs(Vj));
+    f[0] = 0.5 * (fi0 + fj0) - 0.5 * V * (qj[0] - qi[0]);
+    f[1] = 0.5 * (fi1 + fj1) - 0.5 * V * (qj[1] - qi[1]);
+}
+
+template <int FLUX>
+__device__ __forceinline__ void flux(double gamma, double* f, const double* qi, const double* qj,
+                                     double n0, double n1) {
+    if (FLUX == 3) burgers(f, qi, qj, n0, n1);
+    else roe<FLUX == 1>(gamma, f, qi, qj, n0, n1);
+}
+
+// Limiter functions phi (limiter_func).  ZERO: shockTube/main.cpp:60-62.
+// MICHALAK (y_t = 2): forwardStep/main.cpp:57-66.  MINMOD: burgers/main.cpp:
+// 51-53.  VENKAT: (y^2 + 2y)/(y^2 + y + 2), Venkatakrishnan (1995).
+__device__ __forceinline__ double limiter_func(int kind, double y) {
+    if (kind == 1) {
+        const double yt = 2.0;
+        if (y >= yt) return 1.0;
+        const double a = 1.0 / (yt * yt) - 2.0 / (yt * yt * yt);
+        const double b = -3.0 / 2.0 * a * yt - 0.5 / yt;
+        return a * y * y * y + b * y * y + y;
+    }
+    if (kind == 2) return (y * y + 2.0 * y) / (y * y + y + 2.0);
+    if (kind == 3) return dmax(0., dmin(1., y));
+    return 0.;
+}
+
+// Boundary conditions (boundaries::bounds entries).  COPY: shockTube/main.cpp:
+// 158-163.  WALL: forwardStep/main.cpp:262-269.  INLET_OUTLET: forwardStep/
+// main.cpp:194-261.  FARFIELD: naca/main.cpp:192-259.  Subsonic outlets keep
+// the reference's b[2] = b[1]*(...).
+template <int V>
+__device__ __forceinline__ void bc(const Params& P, int group, double* b, const double* q, double n0, double n1) {
+    const int kind = P.group_bc[group];
+    if (kind == 0 || V != 4) {
+#pragma unroll
+        for (int k = 0; k < V; ++k) b[k] = q[k];
+        return;
+    }
+    if (kind == 1) {
+        b[0] = q[0];
+        b[1] = q[1] - 2.0 * n0 * (n0 * q[1] + n1 * q[2]);
+        b[2] = q[2] - 2.0 * n1 * (n0 * q[1] + n1 * q[2]);
+        b[3] = q[3];
+        return;
+    }
+    const double gamma = P.gamma;
+    const double* bv = P.group_bv + 4 * group;
+    const double U0 = q[1] / q[0], U1 = q[2] / q[0];
+    const double u_norm = sqrt(U0 * U0 + U1 * U1);
+    const double u_dot_n = U0 * n0 + U1 * n1;
+    const double p = (gamma - 1) * (q[3] - 0.5 / q[0] * (q[1] * q[1] + q[2] * q[2]));
+    const double c = sqrt(gamma * p / q[0]);
+    const double mach = u_norm / c;
+    if (mach > 1) {
+        if (u_dot_n < 0) {
+            b[0] = bv[0]; b[1] = bv[1]; b[2] = bv[2]; b[3] = bv[3];
+        } else {
+            b[0] = q[0]; b[1] = q[1]; b[2] = q[2]; b[3] = q[3];
+        }
+        return;
+    }
+    const double pa = (gamma - 1) * (bv[3] - 0.5 / bv[0] * (bv[1] * bv[1] + bv[2] * bv[2]));
+    const double rhoa = bv[0], ua = bv[1] / bv[0], va = bv[2] / bv[0];
+    const double pd = p, rhod = q[0], ud = q[1] / q[0], vd = q[2] / q[0];
+    const double rho0 = q[0], c0 = c;
+    if (u_dot_n < 0) {
+        if (kind == 2) {
+            const double pb = pd;
+            b[0] = bv[0]; b[1] = bv[1]; b[2] = bv[2];
+            b[3] = pb / (gamma - 1.) + 0.5 / b[0] * (b[1] * b[1] + b[2] * b[2]);
+        } else {
+            const double pb = 0.5 * (pa + pd - rho0 * c0 * (n0 * (ua - ud) + n1 * (va - vd)));
+            b[0] = rhoa + (pb - pa) / (c0 * c0);
+            b[1] = b[0] * (ua - n0 * (pa - pb) / (rho0 * c0));
+            b[2] = b[1] * (va - n1 * (pa - pb) / (rho0 * c0));
+            b[3] = pb / (gamma - 1) + 0.5 / b[0] * (b[1] * b[1] + b[2] * b[2]);
+        }
+    } else {
+        const double pb = pa;
+        b[0] = rhod + (pb - pd) / (c0 * c0);
+        b[1] = b[0] * (ud + n0 * (pd - pb) / (rho0 * c0));
+        b[2] = b[1] * (va + n1 * (pd - pb) / (rho0 * c0));
+        b[3] = pb / (gamma - 1.) + 0.5 / b[0] * (b[1] * b[1] + b[2] * b[2]);
+    }
+}
+
+// Pressure, forwardStep/main.cpp:37-39.
+__device__ __forceinline__ double pres(double gamma, const double* q) {
+    return (gamma - 1) * (q[3] - 0.5 / q[0] * (q[1] * q[1] + q[2] * q[2]));
+}
+
+}  // namespace exact
+}  // namespace fvgpu

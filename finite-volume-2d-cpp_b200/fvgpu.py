@@ -1,0 +1,270 @@
+"""Python binding of the C ABI in include/fvgpu.h (libfvgpu.so).
+
+This is a thin ctypes layer for tests, benchmarks and scripting; the C++
+drop-in for fvhyper's own API lives in ``shim/``.  There is no CPU fallback:
+if libfvgpu.so is missing or fails to load, every entry point raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Callable, Optional, Sequence
+
+import numpy as np
+
+import physics as _phys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libfvgpu.so")
+
+FLUX = {"roe_fs": 1, "roe_st": 2, "burgers": 3}
+LIMITER = {"zero": 0, "michalak": 1, "venkat": 2, "minmod": 3}
+DT = {"const": 0, "cfl_sum": 1, "cfl_min_signed": 2}
+BC = {"copy": 0, "wall": 1, "inlet_outlet": 2, "farfield": 3}
+PREC = {"fp64_exact": 0, "fp64": 1, "fp32": 2}
+
+_dp = C.POINTER(C.c_double)
+_i32p = C.POINTER(C.c_int32)
+_u32p = C.POINTER(C.c_uint32)
+_i64p = C.POINTER(C.c_int64)
+
+
+class FvError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"fvgpu error {code}: {msg}")
+        self.code = code
+
+
+class _Physics(C.Structure):
+    _fields_ = [("V", C.c_int32), ("flux", C.c_int32), ("order2", C.c_int32), ("limiter", C.c_int32),
+                ("dt_kind", C.c_int32), ("global_dt", C.c_int32), ("gamma", C.c_double), ("K", C.c_double),
+                ("cfl", C.c_double), ("dt_const", C.c_double), ("n_groups", C.c_int32),
+                ("group_bc", _i32p), ("group_bv", _dp)]
+
+
+_PRINT_CB = C.CFUNCTYPE(None, C.c_void_p, C.c_uint64, C.c_double, _dp, C.c_int32)
+
+
+class _RunOptions(C.Structure):
+    _fields_ = [("max_step", C.c_uint64), ("max_time", C.c_double), ("tolerance", C.c_double),
+                ("print_interval", C.c_uint64), ("n_alpha", C.c_int32), ("alpha", _dp),
+                ("restart", C.c_int32), ("on_print", _PRINT_CB), ("user", C.c_void_p)]
+
+
+class _RunInfo(C.Structure):
+    _fields_ = [("step", C.c_uint64), ("time", C.c_double), ("R", C.c_double * 8), ("R0", C.c_double * 8)]
+
+
+_lib = None
+
+
+def lib():
+    """Load libfvgpu.so (raises if it is not built: there is no fallback)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise FvError(-100, f"{LIB_PATH} is not built; run `make -C {HERE}` (or __graft_entry__.build())")
+        L = C.CDLL(LIB_PATH)
+        L.fv_last_error.restype = C.c_char_p
+        for name in ("fv_mesh_create", "fv_mesh_read_msh", "fv_solver_create"):
+            getattr(L, name).restype = C.c_int
+        L.fv_stage_update.argtypes = [C.c_void_p, _dp, _dp, _dp, _dp, _dp, _dp, C.c_double, _dp]
+        _lib = L
+    return _lib
+
+
+def _check(rc):
+    if rc != 0:
+        raise FvError(rc, lib().fv_last_error().decode(errors="replace"))
+
+
+def _p(a, t=_dp):
+    return a.ctypes.data_as(t)
+
+
+class Mesh:
+    """FV mesh built by the native library exactly as fvhyper's reader builds it."""
+
+    def __init__(self, handle, group_names):
+        self._h = C.c_void_p(handle)
+        self.group_names = list(group_names)
+        s = np.zeros(5, np.int64)
+        _check(lib().fv_mesh_sizes(self._h, _p(s, _i64p)))
+        self.n_nodes, self.n_real, self.n_total, self.n_edges, self.n_bound = (int(v) for v in s)
+
+    @classmethod
+    def from_elements(cls, em):
+        h = C.c_void_p()
+        cells = np.ascontiguousarray(em.cells, np.int32)
+        bn = np.ascontiguousarray(em.bnd_nodes, np.int32)
+        bg = np.ascontiguousarray(em.bnd_group, np.int32)
+        x = np.ascontiguousarray(em.nodes_x, np.float64); y = np.ascontiguousarray(em.nodes_y, np.float64)
+        _check(lib().fv_mesh_create(C.c_int64(x.size), _p(x), _p(y), C.c_int64(cells.shape[0]), _p(cells, _i32p),
+                                    C.c_int64(bn.shape[0]), _p(bn, _i32p), _p(bg, _i32p),
+                                    C.c_int32(len(em.group_names)), C.byref(h)))
+        return cls(h.value, em.group_names)
+
+    @classmethod
+    def read_msh(cls, path):
+        h = C.c_void_p()
+        _check(lib().fv_mesh_read_msh(os.fsencode(path), C.byref(h)))
+        n = lib().fv_mesh_group_count(h)
+        names = []
+        for i in range(n):
+            buf = C.create_string_buffer(256)
+            _check(lib().fv_mesh_group_name(h, C.c_int32(i), buf, C.c_int32(256)))
+            names.append(buf.value.decode())
+        return cls(h.value, names)
+
+    def __del__(self):
+        try:
+            if self._h and _lib is not None:
+                _lib.fv_mesh_destroy(self._h)
+        except Exception:
+            pass
+
+    def geometry(self):
+        E, NT, NB = self.n_edges, self.n_total, self.n_bound
+        out = dict(edge_cells=np.zeros(2 * E, np.uint32), edge_nodes=np.zeros(2 * E, np.uint32),
+                   enx=np.zeros(E), eny=np.zeros(E), elen=np.zeros(E), ecx=np.zeros(E), ecy=np.zeros(E),
+                   area=np.zeros(NT), ccx=np.zeros(NT), ccy=np.zeros(NT),
+                   bound_edges=np.zeros(NB, np.uint32), bound_group=np.zeros(NB, np.int32))
+        _check(lib().fv_mesh_geometry(self._h, _p(out["edge_cells"], _u32p), _p(out["edge_nodes"], _u32p),
+                                      *[_p(out[k]) for k in ("enx", "eny", "elen", "ecx", "ecy", "area", "ccx", "ccy")],
+                                      _p(out["bound_edges"], _u32p), _p(out["bound_group"], _i32p)))
+        return out
+
+    def device_order(self):
+        a = np.zeros(self.n_total, np.int32)
+        _check(lib().fv_mesh_device_order(self._h, _p(a, _i32p)))
+        return a
+
+
+def physics_struct(ph: _phys.Physics, group_names: Sequence[str]):
+    gbc = np.array([BC[ph.bcs[n][0]] for n in group_names], np.int32)
+    gbv = np.array([list(ph.bcs[n][1]) if ph.bcs[n][1] is not None else [0.0] * 4 for n in group_names],
+                   np.float64).reshape(-1)
+    s = _Physics(V=ph.V, flux=FLUX[ph.flux], order2=int(ph.order2), limiter=LIMITER[ph.limiter],
+                 dt_kind=DT[ph.dt_kind], global_dt=int(ph.global_dt), gamma=ph.gamma, K=ph.K, cfl=ph.cfl,
+                 dt_const=ph.dt_const, n_groups=len(group_names))
+    s.group_bc = _p(gbc, _i32p); s.group_bv = _p(gbv)
+    s._keep = (gbc, gbv)
+    return s
+
+
+class Solver:
+    """Device solver for one mesh + physics (one CUDA device)."""
+
+    def __init__(self, mesh: Mesh, ph: _phys.Physics, precision: str = "fp64_exact", device: int = 0):
+        self.mesh = mesh
+        self.phys = ph
+        self.V = ph.V
+        self.precision = precision
+        self._ps = physics_struct(ph, mesh.group_names)
+        h = C.c_void_p()
+        _check(lib().fv_solver_create(mesh._h, C.byref(self._ps), C.c_int32(PREC[precision]), C.c_int32(device),
+                                      C.byref(h)))
+        self._h = h
+
+    def close(self):
+        if self._h:
+            lib().fv_solver_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def nq(self):
+        return self.mesh.n_total * self.V
+
+    def set_stream(self, stream_ptr: int):
+        _check(lib().fv_solver_set_stream(self._h, C.c_void_p(stream_ptr)))
+
+    def sync(self):
+        _check(lib().fv_solver_sync(self._h))
+
+    def set_chunk(self, n):
+        _check(lib().fv_solver_set_chunk(self._h, C.c_int32(n)))
+
+    # -- state -----------------------------------------------------------
+    def set_state(self, q):
+        q = np.ascontiguousarray(q, np.float64).reshape(-1)
+        assert q.size == self.nq
+        _check(lib().fv_set_state(self._h, _p(q)))
+
+    def get_state(self):
+        q = np.zeros(self.nq)
+        _check(lib().fv_get_state(self._h, _p(q)))
+        return q
+
+    def set_state_ptr(self, ptr: int, device: bool):
+        fn = lib().fv_set_state_device if device else lib().fv_set_state
+        _check(fn(self._h, C.c_void_p(ptr)))
+
+    def get_state_ptr(self, ptr: int, device: bool):
+        fn = lib().fv_get_state_device if device else lib().fv_get_state
+        _check(fn(self._h, C.c_void_p(ptr)))
+
+    # -- time loop -------------------------------------------------------
+    def run(self, max_step, alpha=_phys.RK5_ALPHA, max_time=1e10, tolerance=1e-16, print_interval=1,
+            restart=True, on_print: Optional[Callable] = None):
+        a = np.ascontiguousarray(alpha, np.float64)
+        cb = _PRINT_CB(0)
+        if on_print is not None:
+            def _cb(user, step, time, R, V):
+                on_print(int(step), float(time), [R[k] for k in range(V)])
+            cb = _PRINT_CB(_cb)
+        o = _RunOptions(max_step=int(max_step), max_time=float(max_time), tolerance=float(tolerance),
+                        print_interval=int(print_interval), n_alpha=a.size, alpha=_p(a), restart=int(restart),
+                        on_print=cb, user=None)
+        info = _RunInfo()
+        _check(lib().fv_run(self._h, C.byref(o), C.byref(info)))
+        return dict(step=info.step, time=info.time, R=np.array(info.R[: self.V]), R0=np.array(info.R0[: self.V]))
+
+    def last_run_stats(self):
+        ms = C.c_double(); n = C.c_int64()
+        _check(lib().fv_last_run_stats(self._h, C.byref(ms), C.byref(n)))
+        return ms.value, n.value
+
+    def check_state(self):
+        rc = lib().fv_check_state(self._h)
+        return rc
+
+    def boundary_force(self, group_name):
+        g = self.mesh.group_names.index(group_name)
+        fx = C.c_double(); fy = C.c_double()
+        _check(lib().fv_boundary_force(self._h, C.c_int32(g), C.byref(fx), C.byref(fy)))
+        return fx.value, fy.value
+
+    def residuals(self):
+        R = np.zeros(self.V)
+        _check(lib().fv_residuals(self._h, _p(R)))
+        return R
+
+    # -- stage entry points (reference numbering) -------------------------
+    def stage_dt(self, q, global_min=False):
+        q = np.ascontiguousarray(q, np.float64); dt = np.zeros(self.mesh.n_total)
+        _check(lib().fv_stage_dt(self._h, _p(q), _p(dt), C.c_int32(int(global_min))))
+        return dt
+
+    def stage_gradients_limiters(self, q):
+        q = np.ascontiguousarray(q, np.float64)
+        gx = np.zeros(self.nq); gy = np.zeros(self.nq); lim = np.zeros(self.nq)
+        _check(lib().fv_stage_gradients_limiters(self._h, _p(q), _p(gx), _p(gy), _p(lim)))
+        return gx, gy, lim
+
+    def stage_update(self, q_base, q_stage, gx, gy, lim, dt, alpha):
+        arrs = [np.ascontiguousarray(a, np.float64) for a in (q_base, q_stage, gx, gy, lim, dt)]
+        out = np.zeros(self.nq)
+        _check(lib().fv_stage_update(self._h, *[_p(a) for a in arrs], C.c_double(alpha), _p(out)))
+        return out
+
+    def stage_bounds(self, q, gx, gy, lim):
+        q = np.ascontiguousarray(q, np.float64).copy()
+        arrs = [np.ascontiguousarray(a, np.float64) for a in (gx, gy, lim)]
+        _check(lib().fv_stage_bounds(self._h, _p(q), *[_p(a) for a in arrs]))
+        return q

@@ -1,0 +1,191 @@
+/*
+ * fvgpu.h — C ABI of the B200 explicit finite-volume step.
+ *
+ * Plain C types only (no CUDA or torch types): pointers are host pointers
+ * unless the name ends in _device, sizes are int64_t, every call returns an
+ * fv_status (0 = OK, negative = error; fv_last_error() gives the message).
+ * Calls on one fv_solver are not thread-safe; different solvers are
+ * independent.  State arrays use fvhyper's layout: AoS q[V*cell + k] over
+ * n_total = real cells + boundary ghost cells, reference cell numbering
+ * (fvhyper/src/explicit.cpp:665-678).
+ *
+ * Reference interfaces replaced (paths relative to the fvhyper repository):
+ *   fv_mesh_create / fv_mesh_read_msh  <- mesh::read_file          fvhyper/mesh.h:193, src/mesh.cpp:803-855
+ *   fv_solver_create (fv_physics)      <- the user's link-time physics symbols
+ *                                         (vars, solver:: flags, calc_flux, calc_dt,
+ *                                         limiter_func, boundaries::bounds)
+ *                                         fvhyper/explicit.h:31-85, fvhyper/mesh.h:36-39
+ *   fv_run                             <- run(name, q, pool, m, opt) fvhyper/explicit.h:175-181
+ *   fv_run_options                     <- solverOptions              fvhyper/explicit.h:152-160
+ *   fv_stage_dt                        <- calc_dt + min_dt           explicit.cpp:729-734, 555-564
+ *   fv_stage_gradients_limiters        <- calc_gradients + calc_limiters explicit.cpp:112-258
+ *   fv_stage_update                    <- calc_time_derivatives + update_cells + update_bounds
+ *                                                                    explicit.cpp:261-417
+ *   fv_residuals                       <- calc_residuals             explicit.cpp:481-552
+ */
+#ifndef FVGPU_H
+#define FVGPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    FV_OK = 0,
+    FV_ERR_ARG = -1,          /* invalid argument */
+    FV_ERR_CUDA = -2,         /* CUDA runtime error (message has the CUDA error string) */
+    FV_ERR_MESH = -3,         /* malformed mesh (open face, missing boundary edge, zero area, ...) */
+    FV_ERR_UNSUPPORTED = -4,  /* option outside the implemented device physics kinds */
+    FV_ERR_NONFINITE = -5,    /* state became non-finite (checked by fv_check_state) */
+    FV_ERR_NOMEM = -6,        /* device allocation failed */
+    FV_ERR_IO = -7            /* file could not be read or written */
+} fv_status;
+
+/* Physics kinds implemented on the device (see finite-volume-2d-cpp_b200/physics.py). */
+enum { FV_FLUX_ROE_FS = 1, FV_FLUX_ROE_ST = 2, FV_FLUX_BURGERS = 3 };
+enum { FV_LIM_ZERO = 0, FV_LIM_MICHALAK = 1, FV_LIM_VENKAT = 2, FV_LIM_MINMOD = 3 };
+enum { FV_DT_CONST = 0, FV_DT_CFL_SUM = 1, FV_DT_CFL_MIN_SIGNED = 2 };
+enum { FV_BC_COPY = 0, FV_BC_WALL = 1, FV_BC_INLET_OUTLET = 2, FV_BC_FARFIELD = 3 };
+
+/* Arithmetic of the step.
+ * FP64_EXACT: FP64, the reference's evaluation order, no FMA contraction:
+ *             bit-identical to the reference CPU solver.
+ * FP64:       FP64 with fused multiply-adds and reciprocal reuse
+ *             (<= 1e-12 relative per step against the reference).
+ * FP32:       FP32 bulk flux/gradient/limiter arithmetic; FP64 conserved
+ *             state, RK accumulation, residual and force sums. */
+enum { FV_PREC_FP64_EXACT = 0, FV_PREC_FP64 = 1, FV_PREC_FP32 = 2 };
+
+typedef struct {
+    int32_t V;          /* vars (explicit.h:31): 4 for Euler, 2 for the Burgers kind */
+    int32_t flux;       /* FV_FLUX_* */
+    int32_t order2;     /* do_calc_gradients && do_calc_limiters && linear_interpolate */
+    int32_t limiter;    /* FV_LIM_* (limiter_func) */
+    int32_t dt_kind;    /* FV_DT_* (calc_dt) */
+    int32_t global_dt;  /* solver::global_dt */
+    double gamma;       /* ratio of specific heats */
+    double K;           /* limiter constant (explicit.cpp:27 hard-codes 7.5) */
+    double cfl;
+    double dt_const;
+    int32_t n_groups;          /* boundary groups (physical names) */
+    const int32_t* group_bc;   /* [n_groups] FV_BC_* per group */
+    const double* group_bv;    /* [n_groups*4] far-field/inflow state for INLET_OUTLET/FARFIELD */
+} fv_physics;
+
+typedef struct {
+    uint64_t max_step;        /* solverOptions::max_step */
+    double max_time;          /* solverOptions::max_time */
+    double tolerance;         /* solverOptions::tolerance */
+    uint64_t print_interval;  /* solverOptions::print_interval */
+    int32_t n_alpha;          /* RK stages; the reference hard-codes 5 (explicit.cpp:681-687) */
+    const double* alpha;      /* [n_alpha] stage coefficients */
+    int32_t restart;          /* 1: step = 0, time = 0, fill ghosts first (as run() does);
+                                 0: continue from the solver's current step/time/R0 */
+    /* Called on the host after each chunk for every print step
+       (step % print_interval == 0, and step 0), with the time at the start of
+       that step and R normalised as run() prints it.  May be NULL. */
+    void (*on_print)(void* user, uint64_t step, double time, const double* R, int32_t V);
+    void* user;
+} fv_run_options;
+
+typedef struct {
+    uint64_t step;     /* steps taken in total */
+    double time;       /* accumulated time (time += dt[0], explicit.cpp:800) */
+    double R[8];       /* residual norms as run() leaves them */
+    double R0[8];      /* step-0 residual norms */
+} fv_run_info;
+
+typedef struct fv_mesh fv_mesh;
+typedef struct fv_solver fv_solver;
+
+const char* fv_last_error(void);
+int fv_version(void);
+
+/* ---- mesh (host) -------------------------------------------------------- */
+/* Element mesh -> FV geometry exactly as mesh::read_file builds it
+ * (mesh.cpp:821-853): edges in first-visit order, centroids, outward normals,
+ * areas, one ghost cell per boundary segment in segment order.
+ * cells4: [n_cells][4] node indices, -1 in column 3 for triangles.
+ * bnd_nodes: [n_bnd][2]; bnd_group: [n_bnd] group index < n_groups. */
+int fv_mesh_create(int64_t n_nodes, const double* nodes_x, const double* nodes_y,
+                   int64_t n_cells, const int32_t* cells4, int64_t n_bnd,
+                   const int32_t* bnd_nodes, const int32_t* bnd_group, int32_t n_groups,
+                   fv_mesh** out);
+/* Gmsh MSH 4.1 ASCII file (single partition) -> mesh; boundary groups are
+ * the physical names of the boundary curves, in order of first use. */
+int fv_mesh_read_msh(const char* path, fv_mesh** out);
+void fv_mesh_destroy(fv_mesh* m);
+/* out[5] = {n_nodes, n_real, n_total, n_edges, n_bound} */
+int fv_mesh_sizes(const fv_mesh* m, int64_t* out);
+int fv_mesh_group_count(const fv_mesh* m);
+/* copies group i's name (NUL-terminated, truncated to cap) */
+int fv_mesh_group_name(const fv_mesh* m, int32_t i, char* buf, int32_t cap);
+/* Reference-numbered geometry (mesh.h:151-171).  Any pointer may be NULL. */
+int fv_mesh_geometry(const fv_mesh* m, uint32_t* edge_cells, uint32_t* edge_nodes,
+                     double* enx, double* eny, double* elen, double* ecx, double* ecy,
+                     double* area, double* ccx, double* ccy, uint32_t* bound_edges,
+                     int32_t* bound_group);
+/* Element data for output: nodes [n_nodes], cells4 [n_real*4]. */
+int fv_mesh_elements(const fv_mesh* m, double* nodes_x, double* nodes_y, int32_t* cells4);
+/* Device cell order: new2ref[n_total] (reference index of each device cell). */
+int fv_mesh_device_order(const fv_mesh* m, int32_t* new2ref);
+
+/* ---- solver (device) ---------------------------------------------------- */
+int fv_solver_create(const fv_mesh* m, const fv_physics* ph, int32_t precision, int32_t device,
+                     fv_solver** out);
+int fv_solver_destroy(fv_solver* s);
+/* cudaStream_t as void*; NULL = the solver's own stream */
+int fv_solver_set_stream(fv_solver* s, void* stream);
+int fv_solver_sync(fv_solver* s);
+/* State in reference numbering, AoS [n_total][V]. */
+int fv_set_state(fv_solver* s, const double* q);
+int fv_get_state(fv_solver* s, double* q);
+int fv_set_state_device(fv_solver* s, const double* q_device);
+int fv_get_state_device(fv_solver* s, double* q_device);
+/* The run() time loop on the device (explicit.cpp:708-801).  Steps are
+ * captured in CUDA graphs of `chunk` steps; stopping criteria are evaluated
+ * on the device, so the host only waits once per chunk. */
+int fv_run(fv_solver* s, const fv_run_options* opt, fv_run_info* info);
+/* R after the last step (sqrt of sum qt^2 A over real cells, un-normalised). */
+int fv_residuals(fv_solver* s, double* R);
+/* Returns FV_ERR_NONFINITE if any real-cell state is NaN/Inf, or if an
+ * Euler state has rho <= 0 or p <= 0. */
+int fv_check_state(fv_solver* s);
+/* Pressure force on the faces of boundary group `group` (FP64 sum over the
+ * group's faces of p(interior state) * n * length). */
+int fv_boundary_force(fv_solver* s, int32_t group, double* fx, double* fy);
+/* Chunk length of the captured step graphs (default 16). */
+int fv_solver_set_chunk(fv_solver* s, int32_t steps);
+/* Device time of the last fv_run's chunks and per-kernel launch count. */
+int fv_last_run_stats(fv_solver* s, double* device_ms, int64_t* kernel_launches);
+
+/* Per-kernel device timing: runs n_steps more time steps without graph
+ * capture, with a CUDA event after every kernel on the solver's stream.
+ * out_ms[5] / out_count[5] per kernel kind: 0 step control, 1 time step,
+ * 2 gradients + limiters, 3 flux + update + ghost fill, 4 step end. */
+int fv_profile_kernels(fv_solver* s, const double* alpha, int32_t n_alpha, int32_t n_steps,
+                       double* out_ms, int64_t* out_count);
+
+/* ---- stage-level entry points (host arrays, reference numbering) -------- */
+/* dt per cell [n_total]; global_min applies min_dt (explicit.cpp:555-564). */
+int fv_stage_dt(fv_solver* s, const double* q, double* dt, int32_t global_min);
+/* gx, gy, lim [n_total*V] from the fused gradient + limiter kernel. */
+int fv_stage_gradients_limiters(fv_solver* s, const double* q, double* gx, double* gy,
+                                double* lim);
+/* One RK stage from the fused flux + update + ghost-fill kernel:
+ * q_out = q_base + qt(q_stage) * dt * alpha on real cells, then the ghost
+ * fill from q_out with the given gx, gy, lim (explicit.cpp:742-745).
+ * dt [n_total].  q_out [n_total*V]. */
+int fv_stage_update(fv_solver* s, const double* q_base, const double* q_stage,
+                    const double* gx, const double* gy, const double* lim, const double* dt,
+                    double alpha, double* q_out);
+/* Ghost fill alone (explicit.cpp:380-417) on q (in place). */
+int fv_stage_bounds(fv_solver* s, double* q, const double* gx, const double* gy,
+                    const double* lim);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,169 @@
+"""GPU parity: the CUDA kernels, called through the C ABI, against the CPU
+oracle on the same inputs.  The FP64_EXACT path must match bit for bit
+(tolerance 0); residual norms, whose sums are reduced in a different order,
+within 1e-12 relative."""
+import numpy as np
+import pytest
+
+import fvgpu
+import physics as P
+from cases import CASES, random_euler_state
+
+pytestmark = pytest.mark.gpu
+
+R_RTOL = 1e-12
+
+
+def bits_equal(a, b):
+    a = np.ascontiguousarray(a); b = np.ascontiguousarray(b)
+    return a.shape == b.shape and a.tobytes() == b.tobytes()
+
+
+def setup(name, oracle, precision="fp64_exact"):
+    case = CASES[name]
+    em = case["mesh"]()
+    ph = case["phys"]()
+    mesh = fvgpu.Mesh.from_elements(em)
+    s = fvgpu.Solver(mesh, ph, precision)
+    g = oracle.build_mesh(em)
+    p = oracle.physics(ph, em.group_names)
+    return case, em, ph, s, g, p
+
+
+def rand_state(g, ph, seed):
+    if ph.V == 4:
+        return random_euler_state(g.n_total, seed)
+    return np.random.default_rng(seed).uniform(-1, 1, g.n_total * ph.V)
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_stage_dt(name, oracle):
+    case, em, ph, s, g, p = setup(name, oracle)
+    q = rand_state(g, ph, 3)
+    for glob in (False, True):
+        assert bits_equal(s.stage_dt(q, glob), oracle.calc_dt(g, p, q, glob))
+
+
+@pytest.mark.parametrize("name", [n for n in sorted(CASES) if CASES[n]["phys"]().order2])
+def test_stage_gradients_limiters(name, oracle):
+    case, em, ph, s, g, p = setup(name, oracle)
+    q = rand_state(g, ph, 4)
+    gx, gy, lim = s.stage_gradients_limiters(q)
+    ogx, ogy = oracle.gradients(g, p, q)
+    olim = oracle.limiters(g, p, q, ogx, ogy)
+    assert bits_equal(gx, ogx) and bits_equal(gy, ogy) and bits_equal(lim, olim)
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_stage_update_and_ghost_fill(name, oracle):
+    case, em, ph, s, g, p = setup(name, oracle)
+    qb = rand_state(g, ph, 5)
+    qs = rand_state(g, ph, 6)
+    if ph.order2:
+        gx, gy = oracle.gradients(g, p, qs)
+        lim = oracle.limiters(g, p, qs, gx, gy)
+    else:
+        gx = np.zeros_like(qs); gy = np.zeros_like(qs); lim = np.zeros_like(qs)
+    dt = oracle.calc_dt(g, p, qs, ph.global_dt)
+    alpha = 0.2898
+    qt = oracle.time_derivatives(g, p, qs, gx, gy, lim)
+    expect = qb + qt * np.repeat(dt, ph.V) * alpha            # update_cells
+    expect = oracle.update_bounds(g, p, expect, gx, gy, lim)  # update_bounds
+    got = s.stage_update(qb, qs, gx, gy, lim, dt, alpha)
+    assert bits_equal(got, expect)
+    assert bits_equal(s.stage_bounds(qs, gx, gy, lim), oracle.update_bounds(g, p, qs, gx, gy, lim))
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_time_loop(name, oracle):
+    case, em, ph, s, g, p = setup(name, oracle)
+    q0 = case["ic"](g)
+    steps = case["steps"]
+    want = oracle.run_loop(g, p, q0, case["alpha"], steps)
+    s.set_state(q0)
+    got = s.run(steps, alpha=case["alpha"])
+    q = s.get_state()
+    assert got["step"] == want["step"] == steps
+    assert bits_equal(q, want["q"])
+    assert got["time"] == want["time"]
+    np.testing.assert_allclose(got["R"], want["R"], rtol=R_RTOL, atol=0)
+
+
+def test_stopping_criteria(oracle):
+    case, em, ph, s, g, p = setup("sod", oracle)
+    q0 = case["ic"](g)
+    want = oracle.run_loop(g, p, q0, case["alpha"], 10 ** 6, max_time=0.02)
+    s.set_state(q0)
+    got = s.run(10 ** 6, alpha=case["alpha"], max_time=0.02)
+    assert got["step"] == want["step"] and got["time"] == want["time"]
+    assert bits_equal(s.get_state(), want["q"])
+    case, em, ph, s, g, p = setup("naca", oracle)
+    q0 = case["ic"](g)
+    want = oracle.run_loop(g, p, q0, case["alpha"], 500, tolerance=0.5)
+    s.set_state(q0)
+    got = s.run(500, alpha=case["alpha"], tolerance=0.5)
+    assert got["step"] == want["step"] < 500
+    assert bits_equal(s.get_state(), want["q"])
+
+
+def test_chunking_and_continuation_invariance(oracle):
+    """Graph chunk length and splitting a run into continued runs do not
+    change a single bit (RK1 alternates state buffers between steps)."""
+    for name in ("sod", "step_o2_venk5"):
+        case, em, ph, s, g, p = setup(name, oracle)
+        q0 = case["ic"](g)
+        want = oracle.run_loop(g, p, q0, case["alpha"], 13)["q"]
+        for chunk in (1, 4, 7):
+            s.set_chunk(chunk)
+            s.set_state(q0)
+            s.run(13, alpha=case["alpha"])
+            assert bits_equal(s.get_state(), want), (name, chunk)
+        s.set_chunk(16)
+        s.set_state(q0)
+        s.run(5, alpha=case["alpha"])
+        r = s.run(13, alpha=case["alpha"], restart=False)
+        assert r["step"] == 13
+        assert bits_equal(s.get_state(), want)
+
+
+def test_print_records(oracle):
+    case, em, ph, s, g, p = setup("naca", oracle)
+    s.set_state(case["ic"](g))
+    recs = []
+    s.run(25, alpha=case["alpha"], print_interval=10, on_print=lambda st, t, R: recs.append((st, t, R)))
+    assert [r[0] for r in recs] == [0, 10, 20]
+    assert recs[0][2] == [1.0] * 4 and recs[0][1] == 0.0
+    want = oracle.run_loop(g, p, case["ic"](g), case["alpha"], 11, print_interval=10)
+    np.testing.assert_allclose(recs[1][2], want["R"], rtol=R_RTOL)
+
+
+def test_boundary_force(oracle):
+    case, em, ph, s, g, p = setup("naca", oracle)
+    q = random_euler_state(g.n_total, 9)
+    s.set_state(q)
+    fx, fy = s.boundary_force("airfoil")
+    ox, oy = oracle.boundary_force(g, p, q, em.group_names.index("airfoil"))
+    np.testing.assert_allclose([fx, fy], [ox, oy], rtol=1e-12, atol=1e-14)
+
+
+def test_nonfinite_state_is_reported(oracle):
+    case, em, ph, s, g, p = setup("sod", oracle)
+    q = case["ic"](g)
+    s.set_state(q)
+    assert s.check_state() == 0
+    q = q.copy(); q[4 * 7] = np.nan
+    s.set_state(q)
+    assert s.check_state() == -5
+    q[4 * 7] = -1.0  # negative density
+    s.set_state(q)
+    assert s.check_state() == -5
+
+
+def test_unsupported_physics_rejected():
+    em = CASES["sod"]["mesh"]()
+    mesh = fvgpu.Mesh.from_elements(em)
+    bad = P.sod()
+    bad.V = 2
+    with pytest.raises(fvgpu.FvError) as e:
+        fvgpu.Solver(mesh, bad)
+    assert e.value.code == -4
