@@ -10,6 +10,8 @@
 #include "../../include/fvgpu.h"
 #include "fv_launch.h"
 #include "fv_mesh.h"
+#include "fv_tile.cuh"
+#include <cmath>
 
 using namespace fvgpu;
 
@@ -51,20 +53,25 @@ struct GraphEntry {
 struct fv_solver {
     int device = 0;
     int precision = FV_PREC_FP64_EXACT;
+    bool f32 = false;
+    size_t ssz = 8;                 // bytes of one stored stage value
     cudaStream_t stream = nullptr;
     bool own_stream = false;
     int V = 4;
     int64_t n_real = 0, n_total = 0, n_bound = 0;
-    std::vector<int32_t> new2ref_h;
-    Params P{};
+    int n_tiles = 0;
+    TileParams TP{};
     // device buffers
     std::vector<void*> allocs;
-    double *qA = nullptr, *qB = nullptr, *qC = nullptr;
-    double *gx = nullptr, *gy = nullptr, *lim = nullptr, *dt = nullptr;
-    double *stage_buf = nullptr;  // [n_total*V] staging for host transfers / stage tests
-    double *partials = nullptr;
-    double *scratch2 = nullptr;
-    int *flag = nullptr;
+    double* qbase[2] = {nullptr, nullptr};   // FP64 step-start state (RK1 alternates)
+    void* sbase[2] = {nullptr, nullptr};     // stage-precision copy of the base (== qbase unless FP32)
+    void* tmp[2] = {nullptr, nullptr};       // intermediate stage outputs
+    void *gx = nullptr, *gy = nullptr, *lim = nullptr;
+    double* dt = nullptr;
+    double* stage_buf = nullptr;   // [n_total*V] staging for host transfers
+    double* partials = nullptr;
+    double* scratch2 = nullptr;
+    int* flag = nullptr;
     int32_t* new2ref = nullptr;
     Ctrl* ctrl = nullptr;
     RunLimits* limits = nullptr;
@@ -76,9 +83,9 @@ struct fv_solver {
     int64_t last_launches = 0;
 
     template <class T>
-    cudaError_t alloc(T** p, size_t n) {
-        cudaError_t e = cudaMalloc((void**)p, std::max<size_t>(n, 1) * sizeof(T));
-        if (e == cudaSuccess) allocs.push_back(*p);
+    cudaError_t alloc(T** p, size_t n, size_t elem = sizeof(T)) {
+        cudaError_t e = cudaMalloc((void**)p, std::max<size_t>(n, 1) * elem);
+        if (e == cudaSuccess) allocs.push_back((void*)*p);
         return e;
     }
     ~fv_solver() {
@@ -89,6 +96,30 @@ struct fv_solver {
         if (own_stream && stream) cudaStreamDestroy(stream);
     }
 };
+
+namespace {
+// host vector<double> -> device array of the stage precision
+int upload_s(fv_solver* s, const std::vector<double>& v, const void** out) {
+    void* d = nullptr;
+    CK(s->alloc(&d, v.size(), s->ssz));
+    if (s->f32) {
+        std::vector<float> f(v.begin(), v.end());
+        CK(cudaMemcpy(d, f.data(), f.size() * 4, cudaMemcpyHostToDevice));
+    } else {
+        CK(cudaMemcpy(d, v.data(), v.size() * 8, cudaMemcpyHostToDevice));
+    }
+    *out = d;
+    return FV_OK;
+}
+template <class T>
+int upload_v(fv_solver* s, const std::vector<T>& v, const T** out) {
+    T* d = nullptr;
+    CK(s->alloc(&d, v.size()));
+    if (!v.empty()) CK(cudaMemcpy(d, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+    *out = d;
+    return FV_OK;
+}
+}  // namespace
 
 extern "C" {
 
@@ -217,7 +248,7 @@ int fv_solver_create(const fv_mesh* fm, const fv_physics* ph, int32_t precision,
     const HostMesh& m = fm->m;
     int rc = validate_physics(ph, (int)m.group_names.size());
     if (rc) return rc;
-    if (precision != FV_PREC_FP64_EXACT) return fail(FV_ERR_UNSUPPORTED, "precision mode not built yet");
+    if (precision < FV_PREC_FP64_EXACT || precision > FV_PREC_FP32) return fail(FV_ERR_ARG, "unknown precision mode");
     int ndev = 0;
     CK(cudaGetDeviceCount(&ndev));
     if (device < 0 || device >= ndev) return fail(FV_ERR_ARG, "no such CUDA device");
@@ -225,62 +256,88 @@ int fv_solver_create(const fv_mesh* fm, const fv_physics* ph, int32_t precision,
     std::unique_ptr<fv_solver> s(new fv_solver());
     s->device = device;
     s->precision = precision;
+    s->f32 = precision == FV_PREC_FP32;
+    s->ssz = s->f32 ? 4 : 8;
     s->V = ph->V;
     s->n_real = m.n_real; s->n_total = m.n_total; s->n_bound = m.n_bound;
-    s->new2ref_h = m.new2ref;
     CK(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
     s->own_stream = true;
     FaceArrays fa;
     build_face_arrays(m, fa);
-    Params& P = s->P;
+    TileArrays ta;
+    build_tiles(m, fa, kBlock, ta);
+    if (ta.max_halo + kBlock > 65535 || ta.max_edges > kFaceEdgeMask)
+        return fail(FV_ERR_MESH, "tile halo too large for 16-bit local indices");
+    s->n_tiles = ta.n_tiles;
+    TileParams& TP = s->TP;
+    Params& P = TP.P;
     P.n_real = (int)m.n_real; P.n_total = (int)m.n_total; P.n_bound = (int)m.n_bound; P.V = ph->V;
     P.cell0 = fa.cell0;
-    uint32_t* d_nbr; double *d_nx, *d_ny, *d_le, *d_g, *d_dsx, *d_dsy, *d_dnx, *d_dny, *d_area;
-    int32_t *d_gg, *d_gc; uint8_t* d_gs; int32_t* d_n2r;
-    CK(upload(&d_nbr, fa.nbr)); s->allocs.push_back(d_nbr);
-    CK(upload(&d_nx, fa.nx)); s->allocs.push_back(d_nx);
-    CK(upload(&d_ny, fa.ny)); s->allocs.push_back(d_ny);
-    CK(upload(&d_le, fa.le)); s->allocs.push_back(d_le);
-    CK(upload(&d_g, fa.g)); s->allocs.push_back(d_g);
-    CK(upload(&d_dsx, fa.dsx)); s->allocs.push_back(d_dsx);
-    CK(upload(&d_dsy, fa.dsy)); s->allocs.push_back(d_dsy);
-    CK(upload(&d_dnx, fa.dnx)); s->allocs.push_back(d_dnx);
-    CK(upload(&d_dny, fa.dny)); s->allocs.push_back(d_dny);
-    CK(upload(&d_area, fa.area)); s->allocs.push_back(d_area);
-    CK(upload(&d_gg, fa.ghost_group)); s->allocs.push_back(d_gg);
-    CK(upload(&d_gc, fa.ghost_cell)); s->allocs.push_back(d_gc);
-    CK(upload(&d_gs, fa.ghost_slot)); s->allocs.push_back(d_gs);
-    CK(upload(&d_n2r, m.new2ref)); s->allocs.push_back(d_n2r);
-    s->new2ref = d_n2r;
-    P.face_nbr = d_nbr; P.f_nx = d_nx; P.f_ny = d_ny; P.f_le = d_le; P.f_g = d_g;
-    P.f_dsx = d_dsx; P.f_dsy = d_dsy; P.f_dnx = d_dnx; P.f_dny = d_dny; P.area = d_area;
-    P.ghost_group = d_gg; P.ghost_cell = d_gc; P.ghost_slot = d_gs;
+    if ((rc = upload_v(s.get(), fa.ghost_group, &P.ghost_group))) return rc;
+    if ((rc = upload_v(s.get(), fa.ghost_cell, &P.ghost_cell))) return rc;
+    if ((rc = upload_v(s.get(), fa.g_nx, &P.g_nx))) return rc;
+    if ((rc = upload_v(s.get(), fa.g_ny, &P.g_ny))) return rc;
+    if ((rc = upload_v(s.get(), fa.g_le, &P.g_le))) return rc;
+    if ((rc = upload_v(s.get(), fa.g_dx, &P.g_dx))) return rc;
+    if ((rc = upload_v(s.get(), fa.g_dy, &P.g_dy))) return rc;
     P.flux = ph->flux; P.order2 = ph->order2 ? 1 : 0; P.limiter = ph->limiter; P.dt_kind = ph->dt_kind;
     P.global_dt = ph->global_dt ? 1 : 0;
+    P.positivity_guard = ph->positivity_guard ? 1 : 0;
     P.gamma = ph->gamma; P.K = ph->K; P.cfl = ph->cfl; P.dt_const = ph->dt_const;
     P.n_groups = ph->n_groups;
     for (int g = 0; g < ph->n_groups; ++g) {
         P.group_bc[g] = ph->group_bc[g];
         for (int k = 0; k < 4; ++k) P.group_bv[4 * g + k] = ph->group_bv ? ph->group_bv[4 * g + k] : 0.0;
     }
+    TP.T = ta.tile_cells; TP.max_halo = ta.max_halo; TP.max_edges = ta.max_edges;
+    const int32_t* info; const int32_t* halo; const uint32_t* eij; const uint16_t* face;
+    if ((rc = upload_v(s.get(), ta.info, &info))) return rc;
+    TP.info = reinterpret_cast<const int4*>(info);
+    if ((rc = upload_v(s.get(), ta.halo, &halo))) return rc;
+    TP.halo = halo;
+    if ((rc = upload_v(s.get(), ta.edge_ij, &eij))) return rc;
+    TP.edge_ij = eij;
+    if ((rc = upload_v(s.get(), ta.face, &face))) return rc;
+    TP.face = face;
+    if ((rc = upload_s(s.get(), ta.enx, &TP.enx))) return rc;
+    if ((rc = upload_s(s.get(), ta.eny, &TP.eny))) return rc;
+    if ((rc = upload_s(s.get(), ta.ele, &TP.ele))) return rc;
+    if ((rc = upload_s(s.get(), ta.exf, &TP.exf))) return rc;
+    if ((rc = upload_s(s.get(), ta.eyf, &TP.eyf))) return rc;
+    if ((rc = upload_s(s.get(), ta.eg, &TP.eg))) return rc;
+    if ((rc = upload_s(s.get(), ta.ccx, &TP.ccx))) return rc;
+    if ((rc = upload_s(s.get(), ta.ccy, &TP.ccy))) return rc;
+    if ((rc = upload_s(s.get(), fa.area, &TP.area))) return rc;
+    const int32_t* n2r;
+    if ((rc = upload_v(s.get(), m.new2ref, &n2r))) return rc;
+    s->new2ref = const_cast<int32_t*>(n2r);
+    CK(tile::prepare(precision, TP));
     const size_t nq = (size_t)m.n_total * ph->V;
-    CK(s->alloc(&s->qA, nq)); CK(s->alloc(&s->qB, nq)); CK(s->alloc(&s->qC, nq));
-    CK(s->alloc(&s->gx, nq)); CK(s->alloc(&s->gy, nq)); CK(s->alloc(&s->lim, nq));
+    CK(s->alloc(&s->qbase[0], nq)); CK(s->alloc(&s->qbase[1], nq));
+    if (s->f32) {
+        CK(s->alloc(&s->sbase[0], nq, 4)); CK(s->alloc(&s->sbase[1], nq, 4));
+    } else {
+        s->sbase[0] = s->qbase[0]; s->sbase[1] = s->qbase[1];
+    }
+    CK(s->alloc(&s->tmp[0], nq, s->ssz)); CK(s->alloc(&s->tmp[1], nq, s->ssz));
+    CK(s->alloc(&s->gx, nq, s->ssz)); CK(s->alloc(&s->gy, nq, s->ssz)); CK(s->alloc(&s->lim, nq, s->ssz));
     CK(s->alloc(&s->stage_buf, nq));
     CK(s->alloc(&s->dt, (size_t)m.n_total));
-    CK(s->alloc(&s->partials, (size_t)grid_for((int)m.n_real) * ph->V));
+    CK(s->alloc(&s->partials, (size_t)ta.n_tiles * ph->V));
     CK(s->alloc(&s->scratch2, 8));
     CK(s->alloc(&s->flag, 4));
     CK(s->alloc(&s->ctrl, 1));
     CK(s->alloc(&s->limits, 1));
     s->hist_cap = 4096;
     CK(s->alloc(&s->hist, (size_t)s->hist_cap));
-    CK(cudaMemsetAsync(s->qA, 0, nq * 8, s->stream));
-    CK(cudaMemsetAsync(s->gx, 0, nq * 8, s->stream));
-    CK(cudaMemsetAsync(s->gy, 0, nq * 8, s->stream));
-    CK(cudaMemsetAsync(s->lim, 0, nq * 8, s->stream));
+    for (void* p : {(void*)s->qbase[0], (void*)s->qbase[1], s->tmp[0], s->tmp[1], s->gx, s->gy, s->lim})
+        CK(cudaMemsetAsync(p, 0, nq * (p == (void*)s->qbase[0] || p == (void*)s->qbase[1] ? 8 : s->ssz), s->stream));
+    if (s->f32) {
+        CK(cudaMemsetAsync(s->sbase[0], 0, nq * 4, s->stream));
+        CK(cudaMemsetAsync(s->sbase[1], 0, nq * 4, s->stream));
+    }
     CK(cudaMemsetAsync(s->ctrl, 0, sizeof(Ctrl), s->stream));
-    launch_fill_ghost_grad(s->gx, s->gy, s->lim, (int)m.n_real, (int)m.n_total, ph->V, s->stream);
+    launch_fill_ghost_grad(s->gx, s->gy, s->lim, (int)m.n_real, (int)m.n_total, ph->V, s->f32, s->stream);
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(s->stream));
     *out = s.release();
@@ -322,12 +379,18 @@ int fv_solver_set_chunk(fv_solver* s, int32_t steps) {
     return FV_OK;
 }
 
+// after the FP64 base changes, refresh its stage-precision copy
+static void sync_shadow(fv_solver* s, int b) {
+    if (s->f32) launch_to_float(s->qbase[b], (float*)s->sbase[b], (size_t)s->n_total * s->V, s->stream);
+}
+
 static int set_state_common(fv_solver* s, const double* q, cudaMemcpyKind kind) {
     if (!s || !q) return fail(FV_ERR_ARG, "null argument");
     CK(cudaSetDevice(s->device));
     const size_t nq = (size_t)s->n_total * s->V;
     CK(cudaMemcpyAsync(s->stage_buf, q, nq * 8, kind, s->stream));
-    launch_permute_to_device(s->stage_buf, s->qA, s->new2ref, (int)s->n_total, s->V, s->stream);
+    launch_permute_to_device(s->stage_buf, s->qbase[0], s->new2ref, (int)s->n_total, s->V, s->stream);
+    sync_shadow(s, 0);
     CK(cudaGetLastError());
     return FV_OK;
 }
@@ -335,7 +398,7 @@ static int get_state_common(fv_solver* s, double* q, cudaMemcpyKind kind) {
     if (!s || !q) return fail(FV_ERR_ARG, "null argument");
     CK(cudaSetDevice(s->device));
     const size_t nq = (size_t)s->n_total * s->V;
-    launch_permute_to_ref(s->qA, s->stage_buf, s->new2ref, (int)s->n_total, s->V, s->stream);
+    launch_permute_to_ref(s->qbase[0], s->stage_buf, s->new2ref, (int)s->n_total, s->V, s->stream);
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(q, s->stage_buf, nq * 8, kind, s->stream));
     if (kind == cudaMemcpyDeviceToHost) CK(cudaStreamSynchronize(s->stream));
@@ -368,52 +431,63 @@ struct EventLog {
     }
 };
 
-// Enqueues one time step (explicit.cpp:715-801) reading/writing the base
-// state in `base`.  Returns the number of kernels launched.
-static int enqueue_step(fv_solver* s, const std::vector<double>& alpha, double* base, double* other,
-                        EventLog* log = nullptr) {
-    const Params& P = s->P;
+// Enqueues one time step (explicit.cpp:715-801) whose base state is
+// qbase[b] (RK1 writes its result to qbase[1-b]).  Returns the number of
+// kernels launched.
+static int enqueue_step(fv_solver* s, const std::vector<double>& alpha, int b, EventLog* log = nullptr) {
+    const TileParams& TP = s->TP;
     cudaStream_t st = s->stream;
     int n = 0;
     auto mark = [&](int k) { if (log) log->mark(k); };
     launch_step_begin(s->ctrl, s->limits, s->V, st); ++n; mark(KK_BEGIN);
-    exact::launch_dt(P, base, s->dt, &s->ctrl->dtmin_key, s->ctrl, st); ++n; mark(KK_DT);
+    TileIO io{};
+    io.gx = s->gx; io.gy = s->gy; io.lim = s->lim; io.dt = s->dt; io.ctrl = s->ctrl;
+    io.dtkeys = s->ctrl->dtkeys;
+    io.q_stage = s->sbase[b];
+    tile::launch_dt(s->precision, TP, io, st); ++n; mark(KK_DT);
     const int ns = (int)alpha.size();
-    const double* in = base;
+    const void* in = s->sbase[b];
     for (int k = 0; k < ns; ++k) {
-        double* out;
-        if (ns == 1) out = other;
-        else if (k == ns - 1) out = base;
-        else out = (k % 2 == 0) ? s->qB : s->qC;
-        StageIO io{};
-        io.q_stage = in; io.q_base = base; io.q_out = out;
-        io.gx = s->gx; io.gy = s->gy; io.lim = s->lim; io.dt = s->dt; io.alpha = alpha[k];
-        io.ctrl = s->ctrl;
-        io.partials = (k == ns - 1) ? s->partials : nullptr;
-        if (P.order2) { exact::launch_grad_lim(P, io, st); ++n; mark(KK_GRADLIM); }
-        exact::launch_stage(P, io, st); ++n; mark(KK_STAGE);
-        in = out;
+        const bool last = k == ns - 1;
+        TileIO so = io;
+        so.q_stage = in;
+        so.q_base = s->qbase[b];
+        so.alpha = alpha[k];
+        so.partials = last ? s->partials : nullptr;
+        void* out_s;
+        if (ns == 1) {
+            so.q_out = s->qbase[1 - b];
+            out_s = s->sbase[1 - b];
+        } else if (last) {
+            so.q_out = s->qbase[b];
+            out_s = s->sbase[b];
+        } else {
+            out_s = s->tmp[k % 2];
+            so.q_out = s->f32 ? nullptr : (double*)out_s;
+        }
+        so.s_out = s->f32 ? out_s : nullptr;
+        so.write_f64 = last ? 1 : 0;
+        if (TP.P.order2) { tile::launch_gradlim(s->precision, TP, so, st); ++n; mark(KK_GRADLIM); }
+        tile::launch_stage(s->precision, TP, so, st); ++n; mark(KK_STAGE);
+        in = out_s;
     }
-    launch_step_end(P, s->ctrl, s->limits, s->partials, grid_for((int)s->n_real), s->dt, s->hist, s->hist_cap, st);
+    launch_step_end(TP.P, s->ctrl, s->limits, s->partials, s->n_tiles, s->dt, s->hist, s->hist_cap, st);
     ++n; mark(KK_END);
     return n;
 }
 
-static int get_graph(fv_solver* s, const std::vector<double>& alpha, GraphEntry** out) {
-    const int chunk = (alpha.size() == 1 && s->chunk % 2) ? s->chunk + 1 : s->chunk;
+// One captured graph of `len` consecutive steps starting from qbase[0]
+// (RK1 alternates qbase[0] and qbase[1] between steps).
+static int get_graph(fv_solver* s, const std::vector<double>& alpha, int len, GraphEntry** out) {
     for (auto& g : s->graphs)
-        if (g.alpha == alpha && g.chunk == chunk) { *out = &g; return FV_OK; }
+        if (g.alpha == alpha && g.chunk == len) { *out = &g; return FV_OK; }
     GraphEntry g;
     g.alpha = alpha;
-    g.chunk = chunk;
+    g.chunk = len;
     cudaGraph_t graph;
     CK(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
     int launches = 0;
-    for (int k = 0; k < chunk; ++k) {
-        double* base = (alpha.size() == 1 && (k % 2)) ? s->qB : s->qA;
-        double* other = (alpha.size() == 1 && (k % 2)) ? s->qA : s->qB;
-        launches += enqueue_step(s, alpha, base, other);
-    }
+    for (int k = 0; k < len; ++k) launches += enqueue_step(s, alpha, (alpha.size() == 1 && (k % 2)) ? 1 : 0);
     cudaError_t e = cudaStreamEndCapture(s->stream, &graph);
     if (e != cudaSuccess) return fail(FV_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
     e = cudaGraphInstantiate(&g.exec, graph, 0);
@@ -422,6 +496,18 @@ static int get_graph(fv_solver* s, const std::vector<double>& alpha, GraphEntry*
     g.launches = launches;
     s->graphs.push_back(g);
     *out = &s->graphs.back();
+    return FV_OK;
+}
+
+// RK1 leaves the state in qbase[1] after an odd number of steps
+static int settle_base(fv_solver* s, unsigned long long steps_taken) {
+    if (steps_taken % 2) {
+        CK(cudaMemcpyAsync(s->qbase[0], s->qbase[1], (size_t)s->n_total * s->V * 8, cudaMemcpyDeviceToDevice,
+                           s->stream));
+        if (s->f32)
+            CK(cudaMemcpyAsync(s->sbase[0], s->sbase[1], (size_t)s->n_total * s->V * 4, cudaMemcpyDeviceToDevice,
+                               s->stream));
+    }
     return FV_OK;
 }
 
@@ -441,21 +527,29 @@ int fv_run(fv_solver* s, const fv_run_options* o, fv_run_info* info) {
         hc.active = 1;
         CK(cudaMemcpyAsync(s->ctrl, &hc, sizeof(hc), cudaMemcpyHostToDevice, st));
         // run(): initial ghost fill with zeroed gx, gy, limiters (explicit.cpp:712)
-        exact::launch_bounds(s->P, s->qA, s->gx, s->gy, s->lim, 1, st);
+        exact::launch_bounds(s->TP.P, s->qbase[0], nullptr, nullptr, nullptr, 1, st);
+        sync_shadow(s, 0);
         CK(cudaGetLastError());
+    } else {
+        CK(cudaMemcpyAsync(&hc, s->ctrl, sizeof(hc), cudaMemcpyDeviceToHost, st));
     }
-    if (!o->restart) CK(cudaMemcpyAsync(&hc, s->ctrl, sizeof(hc), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
     const unsigned long long start_step = o->restart ? 0ull : hc.step;
-    GraphEntry* g = nullptr;
-    int rc = get_graph(s, alpha, &g);
-    if (rc) return rc;
     cudaEvent_t e0, e1;
     CK(cudaEventCreate(&e0)); CK(cudaEventCreate(&e1));
     std::vector<PrintRec> recs(s->hist_cap);
     double total_ms = 0.0;
     int64_t launches = 0;
+    unsigned long long cur = start_step;
     for (;;) {
+        // graph length: the largest power of two <= min(chunk, steps left), so
+        // runs bounded by max_step launch no idle steps
+        const unsigned long long left = o->max_step > cur ? o->max_step - cur : 1ull;
+        int len = 1;
+        while ((unsigned long long)(len * 2) <= left && len * 2 <= s->chunk) len *= 2;
+        GraphEntry* g = nullptr;
+        int rc = get_graph(s, alpha, len, &g);
+        if (rc) { cudaEventDestroy(e0); cudaEventDestroy(e1); return rc; }
         CK(cudaMemsetAsync(&s->ctrl->n_hist, 0, sizeof(int), st));
         CK(cudaEventRecord(e0, st));
         CK(cudaGraphLaunch(g->exec, st));
@@ -466,6 +560,8 @@ int fv_run(fv_solver* s, const fv_run_options* o, fv_run_info* info) {
         float ms = 0.f;
         CK(cudaEventElapsedTime(&ms, e0, e1));
         total_ms += ms;
+        if (alpha.size() == 1 && (rc = settle_base(s, hc.step - cur))) return rc;
+        cur = hc.step;
         if (o->on_print && hc.n_hist > 0) {
             CK(cudaMemcpy(recs.data(), s->hist, sizeof(PrintRec) * hc.n_hist, cudaMemcpyDeviceToHost));
             for (int k = 0; k < hc.n_hist; ++k) o->on_print(o->user, recs[k].step, recs[k].time, recs[k].R, s->V);
@@ -473,20 +569,13 @@ int fv_run(fv_solver* s, const fv_run_options* o, fv_run_info* info) {
         double Rmax = 1.0;
         if (hc.step > 0) {
             Rmax = 0.0;
-            for (int k = 0; k < s->V; ++k) Rmax = (Rmax < hc.R[k]) ? hc.R[k] : Rmax;
+            // std::max(R[k], Rmax) as in explicit.cpp:720 (a NaN residual propagates)
+            for (int k = 0; k < s->V; ++k) Rmax = (hc.R[k] < Rmax) ? Rmax : hc.R[k];
         }
         const bool done = !hc.active || hc.step >= o->max_step || hc.time >= o->max_time || Rmax < o->tolerance;
         if (done) break;
     }
     cudaEventDestroy(e0); cudaEventDestroy(e1);
-    // RK1 alternates the base buffer; an odd number of steps leaves it in qB.
-    if (alpha.size() == 1) {
-        // every graph replay starts from qA and full chunks are even, so the
-        // base ends in qB exactly when this run took an odd number of steps
-        if ((hc.step - start_step) % 2) {
-            CK(cudaMemcpyAsync(s->qA, s->qB, (size_t)s->n_total * s->V * 8, cudaMemcpyDeviceToDevice, st));
-        }
-    }
     CK(cudaStreamSynchronize(st));
     s->last_ms = total_ms;
     s->last_launches = launches;
@@ -513,15 +602,8 @@ int fv_profile_kernels(fv_solver* s, const double* alpha, int32_t n_alpha, int32
     CK(cudaMemcpyAsync(s->limits, &L, sizeof(L), cudaMemcpyHostToDevice, st));
     EventLog log;
     log.st = st;
-    cudaEvent_t e0;
-    CK(cudaEventCreate(&e0));
-    CK(cudaEventRecord(e0, st));
-    log.ev.push_back(e0);
-    log.kind.push_back(-1);
-    for (int k = 0; k < n_steps; ++k) {
-        const bool odd = a.size() == 1 && (k % 2);
-        enqueue_step(s, a, odd ? s->qB : s->qA, odd ? s->qA : s->qB, &log);
-    }
+    log.mark(-1);
+    for (int k = 0; k < n_steps; ++k) enqueue_step(s, a, (a.size() == 1 && (k % 2)) ? 1 : 0, &log);
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(st));
     for (int k = 0; k < KK_N; ++k) { out_ms[k] = 0.0; out_count[k] = 0; }
@@ -532,9 +614,16 @@ int fv_profile_kernels(fv_solver* s, const double* alpha, int32_t n_alpha, int32
         out_count[log.kind[i]] += 1;
     }
     for (auto e : log.ev) cudaEventDestroy(e);
-    if (a.size() == 1 && (n_steps % 2))
-        CK(cudaMemcpyAsync(s->qA, s->qB, (size_t)s->n_total * s->V * 8, cudaMemcpyDeviceToDevice, st));
+    int rc;
+    if (a.size() == 1 && (rc = settle_base(s, (unsigned long long)n_steps))) return rc;
     CK(cudaStreamSynchronize(st));
+    return FV_OK;
+}
+
+int fv_solver_info(fv_solver* s, int64_t* out) {
+    if (!s || !out) return fail(FV_ERR_ARG, "null argument");
+    out[0] = s->n_tiles; out[1] = s->TP.T; out[2] = s->TP.max_halo; out[3] = s->TP.max_edges;
+    out[4] = s->precision; out[5] = (int64_t)s->ssz;
     return FV_OK;
 }
 
@@ -560,7 +649,7 @@ int fv_check_state(fv_solver* s) {
     CK(cudaSetDevice(s->device));
     int h = 0;
     CK(cudaMemsetAsync(s->flag, 0, 4, s->stream));
-    launch_check_state(s->P, s->qA, s->flag, s->stream);
+    launch_check_state(s->TP.P, s->qbase[0], s->flag, s->stream);
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(&h, s->flag, 4, cudaMemcpyDeviceToHost, s->stream));
     CK(cudaStreamSynchronize(s->stream));
@@ -571,7 +660,7 @@ int fv_check_state(fv_solver* s) {
 int fv_boundary_force(fv_solver* s, int32_t group, double* fx, double* fy) {
     if (!s || !fx || !fy || s->V != 4) return fail(FV_ERR_ARG, "fv_boundary_force: invalid arguments");
     CK(cudaSetDevice(s->device));
-    launch_force(s->P, s->qA, group, s->scratch2, s->stream);
+    launch_force(s->TP.P, s->qbase[0], group, s->scratch2, s->stream);
     CK(cudaGetLastError());
     double h[2];
     CK(cudaMemcpyAsync(h, s->scratch2, 16, cudaMemcpyDeviceToHost, s->stream));
@@ -581,38 +670,71 @@ int fv_boundary_force(fv_solver* s, int32_t group, double* fx, double* fy) {
 }
 
 // ------------------------------------------------------- stage entry points --
-static int to_device(fv_solver* s, const double* h, double* d, int V) {
+// Test and debugging paths: host arrays in reference numbering, converted to
+// the device numbering and the stage precision.  Temporaries are allocated
+// per call.
+namespace {
+struct DevTmp {
+    std::vector<void*> p;
+    ~DevTmp() { for (void* x : p) cudaFree(x); }
+    cudaError_t get(void** out, size_t bytes) {
+        cudaError_t e = cudaMalloc(out, std::max<size_t>(bytes, 16));
+        if (e == cudaSuccess) p.push_back(*out);
+        return e;
+    }
+};
+}  // namespace
+
+// host (reference order, FP64) -> device (device order, FP64 in d64 and,
+// if d_s != nullptr and FP32 mode, an FP32 copy in d_s)
+static int h2d(fv_solver* s, const double* h, double* d64, void* d_s, int V) {
     CK(cudaMemcpyAsync(s->stage_buf, h, (size_t)s->n_total * V * 8, cudaMemcpyHostToDevice, s->stream));
-    launch_permute_to_device(s->stage_buf, d, s->new2ref, (int)s->n_total, V, s->stream);
+    launch_permute_to_device(s->stage_buf, d64, s->new2ref, (int)s->n_total, V, s->stream);
+    if (d_s && s->f32) launch_to_float(d64, (float*)d_s, (size_t)s->n_total * V, s->stream);
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(s->stream));
     return FV_OK;
 }
-static int to_host(fv_solver* s, const double* d, double* h, int V) {
-    launch_permute_to_ref(d, s->stage_buf, s->new2ref, (int)s->n_total, V, s->stream);
+static int d2h(fv_solver* s, const double* d64, double* h, int V) {
+    launch_permute_to_ref(d64, s->stage_buf, s->new2ref, (int)s->n_total, V, s->stream);
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(h, s->stage_buf, (size_t)s->n_total * V * 8, cudaMemcpyDeviceToHost, s->stream));
     CK(cudaStreamSynchronize(s->stream));
     return FV_OK;
 }
+// device array of the stage precision -> FP64 (in place for FP64 modes)
+static const double* as_f64(fv_solver* s, const void* a, double* tmp64, int V) {
+    if (!s->f32) return (const double*)a;
+    launch_to_double((const float*)a, tmp64, (size_t)s->n_total * V, s->stream);
+    return tmp64;
+}
 
 int fv_stage_dt(fv_solver* s, const double* q, double* dt, int32_t global_min) {
     if (!s || !q || !dt) return fail(FV_ERR_ARG, "null argument");
     CK(cudaSetDevice(s->device));
-    int rc = to_device(s, q, s->qB, s->V);
+    DevTmp T;
+    const size_t nq = (size_t)s->n_total * s->V;
+    double* q64; void* qs; unsigned long long* keys;
+    CK(T.get((void**)&q64, nq * 8));
+    CK(T.get(&qs, nq * s->ssz));
+    CK(T.get((void**)&keys, kDtSlots * 8));
+    int rc = h2d(s, q, q64, qs, s->V);
     if (rc) return rc;
-    unsigned long long init = ~0ull;
-    CK(cudaMemcpyAsync(s->scratch2, &init, 8, cudaMemcpyHostToDevice, s->stream));
-    Params P = s->P;
-    P.global_dt = global_min ? 1 : 0;
-    exact::launch_dt(P, s->qB, s->dt, (unsigned long long*)s->scratch2, nullptr, s->stream);
+    CK(cudaMemsetAsync(keys, 0xFF, kDtSlots * 8, s->stream));
+    TileParams TP = s->TP;
+    TP.P.global_dt = global_min ? 1 : 0;
+    TileIO io{};
+    io.q_stage = s->f32 ? qs : q64;
+    io.dt = s->dt;
+    io.dtkeys = keys;
+    tile::launch_dt(s->precision, TP, io, s->stream);
     CK(cudaGetLastError());
     std::vector<double> dd(s->n_total);
-    rc = to_host(s, s->dt, dd.data(), 1);
-    if (rc) return rc;
+    if ((rc = d2h(s, s->dt, dd.data(), 1))) return rc;
     if (global_min) {
-        unsigned long long key;
-        CK(cudaMemcpy(&key, s->scratch2, 8, cudaMemcpyDeviceToHost));
+        unsigned long long hk[kDtSlots], key = ~0ull;
+        CK(cudaMemcpy(hk, keys, sizeof(hk), cudaMemcpyDeviceToHost));
+        for (int i = 0; i < kDtSlots; ++i) key = hk[i] < key ? hk[i] : key;
         double mn;
         if (key == ~0ull) {
             mn = std::nan("");
@@ -630,38 +752,60 @@ int fv_stage_dt(fv_solver* s, const double* q, double* dt, int32_t global_min) {
 int fv_stage_gradients_limiters(fv_solver* s, const double* q, double* gx, double* gy, double* lim) {
     if (!s || !q || !gx || !gy || !lim) return fail(FV_ERR_ARG, "null argument");
     CK(cudaSetDevice(s->device));
-    int rc = to_device(s, q, s->qB, s->V);
+    DevTmp T;
+    const size_t nq = (size_t)s->n_total * s->V;
+    double* q64; void* qs; double* t64;
+    CK(T.get((void**)&q64, nq * 8)); CK(T.get(&qs, nq * s->ssz)); CK(T.get((void**)&t64, nq * 8));
+    int rc = h2d(s, q, q64, qs, s->V);
     if (rc) return rc;
-    StageIO io{};
-    io.q_stage = s->qB; io.gx = s->gx; io.gy = s->gy; io.lim = s->lim;
-    exact::launch_grad_lim(s->P, io, s->stream);
+    TileIO io{};
+    io.q_stage = s->f32 ? qs : q64;
+    io.gx = s->gx; io.gy = s->gy; io.lim = s->lim;
+    tile::launch_gradlim(s->precision, s->TP, io, s->stream);
     CK(cudaGetLastError());
-    if ((rc = to_host(s, s->gx, gx, s->V))) return rc;
-    if ((rc = to_host(s, s->gy, gy, s->V))) return rc;
-    return to_host(s, s->lim, lim, s->V);
+    if ((rc = d2h(s, as_f64(s, s->gx, t64, s->V), gx, s->V))) return rc;
+    if ((rc = d2h(s, as_f64(s, s->gy, t64, s->V), gy, s->V))) return rc;
+    if (s->precision != FV_PREC_FP64_EXACT) {  // limiter already folded into gx, gy
+        for (size_t i = 0; i < nq; ++i) lim[i] = 1.0;
+        return FV_OK;
+    }
+    return d2h(s, as_f64(s, s->lim, t64, s->V), lim, s->V);
 }
 
 int fv_stage_update(fv_solver* s, const double* q_base, const double* q_stage, const double* gx, const double* gy,
                     const double* lim, const double* dt, double alpha, double* q_out) {
     if (!s || !q_base || !q_stage || !gx || !gy || !lim || !dt || !q_out) return fail(FV_ERR_ARG, "null argument");
     CK(cudaSetDevice(s->device));
+    DevTmp T;
+    const size_t nq = (size_t)s->n_total * s->V;
+    double *b64, *s64, *o64, *t64;
+    void *ss, *os;
+    CK(T.get((void**)&b64, nq * 8)); CK(T.get((void**)&s64, nq * 8)); CK(T.get((void**)&o64, nq * 8));
+    CK(T.get((void**)&t64, nq * 8)); CK(T.get(&ss, nq * s->ssz)); CK(T.get(&os, nq * s->ssz));
     int rc;
-    if ((rc = to_device(s, q_base, s->qA, s->V))) return rc;
-    if ((rc = to_device(s, q_stage, s->qB, s->V))) return rc;
-    if ((rc = to_device(s, gx, s->gx, s->V))) return rc;
-    if ((rc = to_device(s, gy, s->gy, s->V))) return rc;
-    if ((rc = to_device(s, lim, s->lim, s->V))) return rc;
-    if ((rc = to_device(s, dt, s->dt, 1))) return rc;
-    // the output buffer starts as the stage state so untouched ghosts match
-    CK(cudaMemcpyAsync(s->qC, s->qB, (size_t)s->n_total * s->V * 8, cudaMemcpyDeviceToDevice, s->stream));
-    StageIO io{};
-    io.q_stage = s->qB; io.q_base = s->qA; io.q_out = s->qC;
+    if ((rc = h2d(s, q_base, b64, nullptr, s->V))) return rc;
+    if ((rc = h2d(s, q_stage, s64, ss, s->V))) return rc;
+    if ((rc = h2d(s, gx, t64, s->gx, s->V))) return rc;
+    if (!s->f32) CK(cudaMemcpy(s->gx, t64, nq * 8, cudaMemcpyDeviceToDevice));
+    if ((rc = h2d(s, gy, t64, s->gy, s->V))) return rc;
+    if (!s->f32) CK(cudaMemcpy(s->gy, t64, nq * 8, cudaMemcpyDeviceToDevice));
+    if ((rc = h2d(s, lim, t64, s->lim, s->V))) return rc;
+    if (!s->f32) CK(cudaMemcpy(s->lim, t64, nq * 8, cudaMemcpyDeviceToDevice));
+    if ((rc = h2d(s, dt, s->dt, nullptr, 1))) return rc;
+    // ghosts of the output start as the stage state (every ghost is then overwritten)
+    CK(cudaMemcpyAsync(o64, s64, nq * 8, cudaMemcpyDeviceToDevice, s->stream));
+    TileIO io{};
+    io.q_stage = s->f32 ? ss : s64;
+    io.q_base = b64;
+    io.q_out = o64;
+    io.s_out = s->f32 ? os : nullptr;
+    io.write_f64 = 1;
     io.gx = s->gx; io.gy = s->gy; io.lim = s->lim; io.dt = s->dt; io.alpha = alpha;
-    exact::launch_stage(s->P, io, s->stream);
+    tile::launch_stage(s->precision, s->TP, io, s->stream);
     CK(cudaGetLastError());
-    rc = to_host(s, s->qC, q_out, s->V);
+    rc = d2h(s, o64, q_out, s->V);
     // restore the invariant ghost gradient/limiter values
-    launch_fill_ghost_grad(s->gx, s->gy, s->lim, (int)s->n_real, (int)s->n_total, s->V, s->stream);
+    launch_fill_ghost_grad(s->gx, s->gy, s->lim, (int)s->n_real, (int)s->n_total, s->V, s->f32, s->stream);
     CK(cudaStreamSynchronize(s->stream));
     return rc;
 }
@@ -669,17 +813,19 @@ int fv_stage_update(fv_solver* s, const double* q_base, const double* q_stage, c
 int fv_stage_bounds(fv_solver* s, double* q, const double* gx, const double* gy, const double* lim) {
     if (!s || !q || !gx || !gy || !lim) return fail(FV_ERR_ARG, "null argument");
     CK(cudaSetDevice(s->device));
+    DevTmp T;
+    const size_t nq = (size_t)s->n_total * s->V;
+    double *q64, *gx64, *gy64, *l64;
+    CK(T.get((void**)&q64, nq * 8)); CK(T.get((void**)&gx64, nq * 8));
+    CK(T.get((void**)&gy64, nq * 8)); CK(T.get((void**)&l64, nq * 8));
     int rc;
-    if ((rc = to_device(s, q, s->qB, s->V))) return rc;
-    if ((rc = to_device(s, gx, s->gx, s->V))) return rc;
-    if ((rc = to_device(s, gy, s->gy, s->V))) return rc;
-    if ((rc = to_device(s, lim, s->lim, s->V))) return rc;
-    exact::launch_bounds(s->P, s->qB, s->gx, s->gy, s->lim, 0, s->stream);
+    if ((rc = h2d(s, q, q64, nullptr, s->V))) return rc;
+    if ((rc = h2d(s, gx, gx64, nullptr, s->V))) return rc;
+    if ((rc = h2d(s, gy, gy64, nullptr, s->V))) return rc;
+    if ((rc = h2d(s, lim, l64, nullptr, s->V))) return rc;
+    exact::launch_bounds(s->TP.P, q64, gx64, gy64, l64, 0, s->stream);
     CK(cudaGetLastError());
-    rc = to_host(s, s->qB, q, s->V);
-    launch_fill_ghost_grad(s->gx, s->gy, s->lim, (int)s->n_real, (int)s->n_total, s->V, s->stream);
-    CK(cudaStreamSynchronize(s->stream));
-    return rc;
+    return d2h(s, q64, q, s->V);
 }
 
 }  // extern "C"

@@ -24,7 +24,9 @@ __device__ __forceinline__ bool inactive(const Ctrl* c) {
     return c != nullptr && *(volatile const int*)&c->active == 0;
 }
 // min_dt (explicit.cpp:555-564): min over all cells; a NaN in dt[0] wins.
-__device__ __forceinline__ double global_dt_value(const Params& P, const double* dt, unsigned long long key) {
+__device__ __forceinline__ double global_dt_value(const Params& P, const double* dt, const unsigned long long* keys) {
+    unsigned long long key = ~0ull;
+    for (int i = 0; i < 64; ++i) key = keys[i] < key ? keys[i] : key;
     const double d0 = dt[P.cell0];
     return (d0 != d0) ? d0 : dkey_inv(key);
 }
@@ -54,6 +56,8 @@ __device__ __forceinline__ void store_cell(double* __restrict__ a, int c, const 
 
 // ------------------------------------------------------------ step control --
 __global__ void k_step_begin(Ctrl* c, const RunLimits* L, int V) {
+    c->dtkeys[threadIdx.x] = ~0ull;
+    c->dtkeys[threadIdx.x + 32] = ~0ull;
     if (threadIdx.x != 0) return;
     double Rmax;
     if (c->step > 0) {
@@ -65,7 +69,6 @@ __global__ void k_step_begin(Ctrl* c, const RunLimits* L, int V) {
     const int stop = (c->step >= L->max_step) | (c->time >= L->max_time) | (Rmax < L->tolerance);
     c->active = !stop;
     c->need_R = !stop && (c->step == 0 || (c->step % L->print_interval) == 0 || (L->tolerance > 1.01e-16));
-    c->dtmin_key = ~0ull;
 }
 
 // Residual norms, step/time bookkeeping and print records
@@ -103,7 +106,7 @@ __global__ void k_step_end(Params P, Ctrl* c, const RunLimits* L, const double* 
         r.time = c->time;
         for (int k = 0; k < V; ++k) r.R[k] = (c->step == 0) ? 1.0 : c->R[k];
     }
-    const double dt0 = P.global_dt ? global_dt_value(P, dt, c->dtmin_key) : dt[P.cell0];
+    const double dt0 = P.global_dt ? global_dt_value(P, dt, c->dtkeys) : dt[P.cell0];
     c->step += 1;
     c->time += dt0;
 }
@@ -118,283 +121,6 @@ void launch_step_end(const Params& P, Ctrl* c, const RunLimits* lim, const doubl
 
 namespace exact {
 
-// ---------------------------------------------------------------- time step --
-// calc_dt kinds (forwardStep/main.cpp:140-185, naca/main.cpp:142-183,
-// shockTube/main.cpp:140-147).  Each real cell also computes the dt of its
-// boundary ghosts (their only edge is the cell's boundary face).  With a
-// global dt the block minimum goes to *dtmin_key (ordered-key atomicMin,
-// exact since min is order independent).
-template <int V>
-__global__ void __launch_bounds__(kBlock) k_dt(Params P, const double* __restrict__ q, double* __restrict__ dt,
-                                               unsigned long long* dtmin_key, const Ctrl* ctrl) {
-    if (inactive(ctrl)) return;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    unsigned long long kmin = ~0ull;
-    if (i < P.n_real) {
-        const double gamma = P.gamma, gm1 = gamma - 1, cfl = P.cfl;
-        const int N = P.n_real;
-        if (P.dt_kind == 0) {
-            dt[i] = P.dt_const;
-            kmin = dkey(P.dt_const);
-            for (int f = 0; f < kMaxFaces; ++f) {
-                const uint32_t w = P.face_nbr[f * N + i];
-                if (w == kNoFace) break;
-                const int nb = (int)(w & 0x7fffffffu);
-                if (nb >= N) dt[nb] = P.dt_const;
-            }
-        } else if (V == 4) {
-            double qs[4];
-            load_cell<4>(q, i, qs);
-            const double cs = sqrt(((gm1) * (qs[3] - 0.5 / qs[0] * (qs[1] * qs[1] + qs[2] * qs[2]))) * gamma / qs[0]);
-            const bool sum = P.dt_kind == 1;
-            const double Ai = P.area[i];
-            double acc = sum ? 0. : 1.0;
-            for (int f = 0; f < kMaxFaces; ++f) {
-                const uint32_t w = P.face_nbr[f * N + i];
-                if (w == kNoFace) break;
-                const int nb = (int)(w & 0x7fffffffu);
-                const bool side1 = (w >> 31) != 0;
-                const double n0 = P.f_nx[f * N + i], n1 = P.f_ny[f * N + i], le = P.f_le[f * N + i];
-                double qn[4];
-                load_cell<4>(q, nb, qn);
-                const double cn = sqrt(((gm1) * (qn[3] - 0.5 / qn[0] * (qn[1] * qn[1] + qn[2] * qn[2]))) * gamma / qn[0]);
-                if (sum) {
-                    const double es = cs + fabs(qs[1] / qs[0] * n0 + qs[2] / qs[0] * n1);
-                    const double en = cn + fabs(qn[1] / qn[0] * n0 + qn[2] / qn[0] * n1);
-                    const double center = side1 ? dmax(en, es) : dmax(es, en);
-                    acc += center * le;
-                    if (nb >= N) {
-                        double d = 0.;
-                        d += center * le;
-                        const double dg = cfl * P.area[nb] / d;
-                        dt[nb] = dg;
-                        const unsigned long long kg = dkey(dg);
-                        kmin = kg < kmin ? kg : kmin;
-                    }
-                } else {
-                    const double es = (cs + fabs(qs[1] / qs[0])) * n0 + (cs + fabs(qs[2] / qs[0])) * n1;
-                    const double dti = cfl * (Ai / le) / fabs(es);
-                    acc = dmin(acc, dti);
-                    if (nb >= N) {
-                        const double en = (cn + fabs(qn[1] / qn[0])) * n0 + (cn + fabs(qn[2] / qn[0])) * n1;
-                        const double dg = dmin(1.0, cfl * (P.area[nb] / le) / fabs(en));
-                        dt[nb] = dg;
-                        const unsigned long long kg = dkey(dg);
-                        kmin = kg < kmin ? kg : kmin;
-                    }
-                }
-            }
-            const double di = sum ? cfl * Ai / acc : acc;
-            dt[i] = di;
-            const unsigned long long ki = dkey(di);
-            kmin = ki < kmin ? ki : kmin;
-        }
-    }
-    if (P.global_dt && dtmin_key != nullptr) {
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            const unsigned long long other = __shfl_xor_sync(0xffffffffu, kmin, o);
-            kmin = other < kmin ? other : kmin;
-        }
-        if ((threadIdx.x & 31) == 0 && kmin != ~0ull) atomicMin(dtmin_key, kmin);
-    }
-}
-
-// ------------------------------------------------ gradients + limiters (K1) --
-// Green-Gauss gradients (explicit.cpp:112-171) and the min/max smooth-switch
-// limiter (explicit.cpp:174-258) fused per cell.  Ghost cells keep gx=gy=0,
-// lim=1, as the reference leaves them.
-template <int V>
-__global__ void __launch_bounds__(kBlock) k_grad_lim(Params P, StageIO io) {
-    if (inactive(io.ctrl)) return;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const int N = P.n_real;
-    if (i >= N) return;
-    double qs[V], gx[V], gy[V], qmn[V], qmx[V];
-    load_cell<V>(io.q_stage, i, qs);
-#pragma unroll
-    for (int k = 0; k < V; ++k) { gx[k] = 0.; gy[k] = 0.; qmn[k] = qs[k]; qmx[k] = qs[k]; }
-    for (int f = 0; f < kMaxFaces; ++f) {
-        const uint32_t w = P.face_nbr[f * N + i];
-        if (w == kNoFace) break;
-        const int nb = (int)(w & 0x7fffffffu);
-        const bool side1 = (w >> 31) != 0;
-        const double nx = P.f_nx[f * N + i], ny = P.f_ny[f * N + i], le = P.f_le[f * N + i];
-        const double g = P.f_g[f * N + i];
-        double qn[V];
-        load_cell<V>(io.q_stage, nb, qn);
-#pragma unroll
-        for (int k = 0; k < V; ++k) {
-            if (!side1) {
-                const double fl = (qs[k] * (1.0 - g) + qn[k] * g) * le;
-                gx[k] += fl * nx;
-                gy[k] += fl * ny;
-            } else {
-                const double fl = (qn[k] * (1.0 - g) + qs[k] * g) * le;
-                gx[k] -= fl * nx;
-                gy[k] -= fl * ny;
-            }
-            qmn[k] = dmin(qmn[k], qn[k]);
-            qmx[k] = dmax(qmx[k], qn[k]);
-        }
-    }
-    const double A = P.area[i];
-    const double invA = 1. / A;
-#pragma unroll
-    for (int k = 0; k < V; ++k) { gx[k] *= invA; gy[k] *= invA; }
-    double lim[V];
-#pragma unroll
-    for (int k = 0; k < V; ++k) lim[k] = 1.;
-    const double sqrt_area = sqrt(A);
-    const double tol = 1e-15;
-    for (int f = 0; f < kMaxFaces; ++f) {
-        const uint32_t w = P.face_nbr[f * N + i];
-        if (w == kNoFace) break;
-        const double dx = P.f_dsx[f * N + i], dy = P.f_dsy[f * N + i];
-#pragma unroll
-        for (int k = 0; k < V; ++k) {
-            const double dqg = gx[k] * dx + gy[k] * dy;
-            const double delta_max = qmx[k] - qs[k];
-            const double delta_min = qmn[k] - qs[k];
-            const double Ka = P.K * sqrt_area;
-            const double K3a = Ka * Ka * Ka;
-            const double d2 = (delta_max - delta_min) * (delta_max - delta_min);
-            double sig;
-            if (d2 <= K3a) {
-                sig = 1.;
-            } else if (d2 <= 2 * K3a) {
-                const double y = (d2 / K3a - 1.0);
-                sig = 2.0 * y * y * y - 3.0 * y * y + 1.0;
-            } else {
-                sig = 0.;
-            }
-            double l = 1.0;
-            if (sig < 1.0) {
-                if (dqg > tol) l = limiter_func(P.limiter, delta_max / dqg);
-                else if (dqg < -tol) l = limiter_func(P.limiter, delta_min / dqg);
-                else l = 1.0;
-            }
-            l = sig + (1.0 - sig) * l;
-            lim[k] = dmin(lim[k], l);
-        }
-    }
-    store_cell<V>(io.gx, i, gx);
-    store_cell<V>(io.gy, i, gy);
-    store_cell<V>(io.lim, i, lim);
-}
-
-// --------------------------------------- flux + RK update + ghost fill (K2) --
-// calc_time_derivatives (explicit.cpp:261-364), update_cells (368-378) and
-// update_bounds (380-417) fused per cell.  The ghost fill uses the updated
-// interior state with this stage's (stale) gradients and limiters, exactly
-// as the reference does.  Optionally writes per-block sums of qt^2 * A.
-template <int V, bool ORDER2, int FLUX>
-__global__ void __launch_bounds__(kBlock) k_stage(Params P, StageIO io) {
-    if (inactive(io.ctrl)) return;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const int N = P.n_real;
-    double res[V];
-#pragma unroll
-    for (int k = 0; k < V; ++k) res[k] = 0.;
-    if (i < N) {
-        double qs[V], gxs[V], gys[V], lms[V];
-        load_cell<V>(io.q_stage, i, qs);
-        if (ORDER2) {
-            load_cell<V>(io.gx, i, gxs);
-            load_cell<V>(io.gy, i, gys);
-            load_cell<V>(io.lim, i, lms);
-        }
-        const double A = P.area[i];
-        double qt[V];
-#pragma unroll
-        for (int k = 0; k < V; ++k) qt[k] = 0.;
-        for (int f = 0; f < kMaxFaces; ++f) {
-            const uint32_t w = P.face_nbr[f * N + i];
-            if (w == kNoFace) break;
-            const int nb = (int)(w & 0x7fffffffu);
-            const bool side1 = (w >> 31) != 0;
-            const double nx = P.f_nx[f * N + i], ny = P.f_ny[f * N + i], le = P.f_le[f * N + i];
-            double qn[V], qsf[V], qnf[V];
-            load_cell<V>(io.q_stage, nb, qn);
-            if (ORDER2) {
-                double gxn[V], gyn[V], lmn[V];
-                load_cell<V>(io.gx, nb, gxn);
-                load_cell<V>(io.gy, nb, gyn);
-                load_cell<V>(io.lim, nb, lmn);
-                const double dsx = P.f_dsx[f * N + i], dsy = P.f_dsy[f * N + i];
-                const double dnx = P.f_dnx[f * N + i], dny = P.f_dny[f * N + i];
-#pragma unroll
-                for (int k = 0; k < V; ++k) {
-                    qsf[k] = qs[k] + (gxs[k] * dsx + gys[k] * dsy) * lms[k];
-                    qnf[k] = qn[k] + (gxn[k] * dnx + gyn[k] * dny) * lmn[k];
-                }
-            } else {
-#pragma unroll
-                for (int k = 0; k < V; ++k) { qsf[k] = qs[k]; qnf[k] = qn[k]; }
-            }
-            double fl[V];
-            if (!side1) {
-                flux<FLUX>(P.gamma, fl, qsf, qnf, nx, ny);
-#pragma unroll
-                for (int k = 0; k < V; ++k) qt[k] -= fl[k] * le / A;
-            } else {
-                flux<FLUX>(P.gamma, fl, qnf, qsf, nx, ny);
-#pragma unroll
-                for (int k = 0; k < V; ++k) qt[k] += fl[k] * le / A;
-            }
-        }
-        double dtc;
-        if (io.ctrl != nullptr && P.global_dt) dtc = global_dt_value(P, io.dt, io.ctrl->dtmin_key);
-        else dtc = io.dt[i];
-        double qb[V], qnew[V];
-        load_cell<V>(io.q_base, i, qb);
-#pragma unroll
-        for (int k = 0; k < V; ++k) qnew[k] = qb[k] + qt[k] * dtc * io.alpha;
-        store_cell<V>(io.q_out, i, qnew);
-        // boundary ghosts of this cell
-        for (int f = 0; f < kMaxFaces; ++f) {
-            const uint32_t w = P.face_nbr[f * N + i];
-            if (w == kNoFace) break;
-            const int nb = (int)(w & 0x7fffffffu);
-            if (nb < N) continue;
-            const double nx = P.f_nx[f * N + i], ny = P.f_ny[f * N + i];
-            double qint[V], b[V];
-            if (ORDER2) {
-                const double d0 = P.f_dsx[f * N + i], d1 = P.f_dsy[f * N + i];
-#pragma unroll
-                for (int k = 0; k < V; ++k) qint[k] = qnew[k] + (gxs[k] * d0 + gys[k] * d1) * lms[k];
-            } else {
-#pragma unroll
-                for (int k = 0; k < V; ++k) qint[k] = qnew[k];
-            }
-            bc<V>(P, P.ghost_group[nb - N], b, qint, nx, ny);
-            store_cell<V>(io.q_out, nb, b);
-        }
-        if (io.partials != nullptr) {
-#pragma unroll
-            for (int k = 0; k < V; ++k) res[k] = qt[k] * qt[k] * A;
-        }
-    }
-    if (io.partials != nullptr) {
-        __shared__ double red[kBlock / 32][V];
-#pragma unroll
-        for (int k = 0; k < V; ++k)
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) res[k] += __shfl_xor_sync(0xffffffffu, res[k], o);
-        if ((threadIdx.x & 31) == 0)
-#pragma unroll
-            for (int k = 0; k < V; ++k) red[threadIdx.x >> 5][k] = res[k];
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            for (int k = 0; k < V; ++k) {
-                double s = 0.;
-                for (int w = 0; w < kBlock / 32; ++w) s += red[w][k];
-                io.partials[(size_t)blockIdx.x * V + k] = s;
-            }
-        }
-    }
-}
-
 // Standalone ghost fill (update_bounds, explicit.cpp:380-417), one thread
 // per ghost.  zero_grad: the initial fill run() does before the loop with
 // freshly zeroed gx, gy, limiters (explicit.cpp:712).
@@ -404,12 +130,12 @@ __global__ void k_bounds(Params P, double* __restrict__ q, const double* __restr
     const int b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= P.n_bound) return;
     const int N = P.n_real;
-    const int c = P.ghost_cell[b], f = P.ghost_slot[b];
-    const double nx = P.f_nx[f * N + c], ny = P.f_ny[f * N + c];
+    const int c = P.ghost_cell[b];
+    const double nx = P.g_nx[b], ny = P.g_ny[b];
     double qc[V], qint[V], out[V];
     load_cell<V>(q, c, qc);
     if (P.order2) {
-        const double d0 = P.f_dsx[f * N + c], d1 = P.f_dsy[f * N + c];
+        const double d0 = P.g_dx[b], d1 = P.g_dy[b];
         double gxc[V], gyc[V], lc[V];
         if (zero_grad) {
 #pragma unroll
@@ -419,40 +145,17 @@ __global__ void k_bounds(Params P, double* __restrict__ q, const double* __restr
         }
 #pragma unroll
         for (int k = 0; k < V; ++k) qint[k] = qc[k] + (gxc[k] * d0 + gyc[k] * d1) * lc[k];
+        if (V == 4 && P.positivity_guard) {  // optional guard, see fv_tile.cuh
+            const double p = (P.gamma - 1) * (qint[3] - 0.5 / qint[0] * (qint[1] * qint[1] + qint[2] * qint[2]));
+            if (!(qint[0] > 0.) || !(p > 0.))
+                for (int k = 0; k < V; ++k) qint[k] = qc[k];
+        }
     } else {
 #pragma unroll
         for (int k = 0; k < V; ++k) qint[k] = qc[k];
     }
     bc<V>(P, P.ghost_group[b], out, qint, nx, ny);
     store_cell<V>(q, N + b, out);
-}
-
-// ----------------------------------------------------------------- launchers --
-void launch_dt(const Params& P, const double* q, double* dt, unsigned long long* key, const Ctrl* c,
-               cudaStream_t st) {
-    const int g = grid_for(P.n_real);
-    if (P.V == 4) k_dt<4><<<g, kBlock, 0, st>>>(P, q, dt, key, c);
-    else k_dt<2><<<g, kBlock, 0, st>>>(P, q, dt, key, c);
-}
-
-void launch_grad_lim(const Params& P, const StageIO& io, cudaStream_t st) {
-    const int g = grid_for(P.n_real);
-    if (P.V == 4) k_grad_lim<4><<<g, kBlock, 0, st>>>(P, io);
-    else k_grad_lim<2><<<g, kBlock, 0, st>>>(P, io);
-}
-
-void launch_stage(const Params& P, const StageIO& io, cudaStream_t st) {
-    const int g = grid_for(P.n_real);
-    if (P.flux == 3) {
-        if (P.order2) k_stage<2, true, 3><<<g, kBlock, 0, st>>>(P, io);
-        else k_stage<2, false, 3><<<g, kBlock, 0, st>>>(P, io);
-    } else if (P.flux == 1) {
-        if (P.order2) k_stage<4, true, 1><<<g, kBlock, 0, st>>>(P, io);
-        else k_stage<4, false, 1><<<g, kBlock, 0, st>>>(P, io);
-    } else {
-        if (P.order2) k_stage<4, true, 2><<<g, kBlock, 0, st>>>(P, io);
-        else k_stage<4, false, 2><<<g, kBlock, 0, st>>>(P, io);
-    }
 }
 
 }  // namespace exact
@@ -491,7 +194,23 @@ void launch_permute_to_ref(const double* q_dev, double* q_ref, const int32_t* ne
     k_permute_to_ref<<<grid_for(n), kBlock, 0, st>>>(q_dev, q_ref, new2ref, n, V);
 }
 
-__global__ void k_fill_ghost_grad(double* gx, double* gy, double* lim, int n_real, int n_total, int V) {
+__global__ void k_to_float(const double* __restrict__ a, float* __restrict__ b, size_t n) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) b[i] = (float)a[i];
+}
+__global__ void k_to_double(const float* __restrict__ a, double* __restrict__ b, size_t n) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) b[i] = (double)a[i];
+}
+void launch_to_float(const double* a, float* b, size_t n, cudaStream_t st) {
+    if (n) k_to_float<<<(unsigned)((n + kBlock - 1) / kBlock), kBlock, 0, st>>>(a, b, n);
+}
+void launch_to_double(const float* a, double* b, size_t n, cudaStream_t st) {
+    if (n) k_to_double<<<(unsigned)((n + kBlock - 1) / kBlock), kBlock, 0, st>>>(a, b, n);
+}
+
+template <class S>
+__global__ void k_fill_ghost_grad_t(S* gx, S* gy, S* lim, int n_real, int n_total, int V) {
     const int i = n_real + blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n_total) return;
     for (int k = 0; k < V; ++k) {
@@ -500,8 +219,13 @@ __global__ void k_fill_ghost_grad(double* gx, double* gy, double* lim, int n_rea
         lim[(size_t)V * i + k] = 1.;
     }
 }
-void launch_fill_ghost_grad(double* gx, double* gy, double* lim, int n_real, int n_total, int V, cudaStream_t st) {
-    if (n_total > n_real) k_fill_ghost_grad<<<grid_for(n_total - n_real), kBlock, 0, st>>>(gx, gy, lim, n_real, n_total, V);
+// Ghost cells keep gx = gy = 0 and lim = 1 (the reference never updates them).
+void launch_fill_ghost_grad(void* gx, void* gy, void* lim, int n_real, int n_total, int V, bool f32,
+                            cudaStream_t st) {
+    if (n_total <= n_real) return;
+    const int g = grid_for(n_total - n_real);
+    if (f32) k_fill_ghost_grad_t<float><<<g, kBlock, 0, st>>>((float*)gx, (float*)gy, (float*)lim, n_real, n_total, V);
+    else k_fill_ghost_grad_t<double><<<g, kBlock, 0, st>>>((double*)gx, (double*)gy, (double*)lim, n_real, n_total, V);
 }
 
 __global__ void k_check_state(Params P, const double* __restrict__ q, int* flag) {
@@ -528,16 +252,14 @@ void launch_check_state(const Params& P, const double* q, int* flag, cudaStream_
 __global__ void k_force(Params P, const double* __restrict__ q, int group, double* out) {
     __shared__ double sx[kBlock], sy[kBlock];
     double ax = 0., ay = 0.;
-    const int N = P.n_real;
     for (int b = threadIdx.x; b < P.n_bound; b += blockDim.x) {
         if (P.ghost_group[b] != group) continue;
-        const int c = P.ghost_cell[b], f = P.ghost_slot[b];
         double s[4];
-        load_cell<4>(q, c, s);
+        load_cell<4>(q, P.ghost_cell[b], s);
         const double p = exact::pres(P.gamma, s);
-        const double le = P.f_le[f * N + c];
-        ax += p * P.f_nx[f * N + c] * le;
-        ay += p * P.f_ny[f * N + c] * le;
+        const double le = P.g_le[b];
+        ax += p * P.g_nx[b] * le;
+        ay += p * P.g_ny[b] * le;
     }
     sx[threadIdx.x] = ax; sy[threadIdx.x] = ay;
     __syncthreads();

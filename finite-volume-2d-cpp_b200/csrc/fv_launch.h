@@ -14,12 +14,8 @@ void launch_step_begin(Ctrl* c, const RunLimits* lim, int V, cudaStream_t st);
 void launch_step_end(const Params& P, Ctrl* c, const RunLimits* lim, const double* partials,
                      int nblocks, const double* dt, PrintRec* hist, int hist_cap, cudaStream_t st);
 
-// FP64 kernels in the reference's exact evaluation order (fv_kernels_exact.cu)
+// initial / standalone ghost fill (update_bounds) in FP64 (fv_kernels_exact.cu)
 namespace exact {
-void launch_dt(const Params& P, const double* q, double* dt, unsigned long long* dtmin_key,
-               const Ctrl* c, cudaStream_t st);
-void launch_grad_lim(const Params& P, const StageIO& io, cudaStream_t st);
-void launch_stage(const Params& P, const StageIO& io, cudaStream_t st);
 void launch_bounds(const Params& P, double* q, const double* gx, const double* gy,
                    const double* lim, int zero_grad, cudaStream_t st);
 }  // namespace exact
@@ -29,8 +25,10 @@ void launch_permute_to_device(const double* q_ref, double* q_dev, const int32_t*
                               int n_total, int V, cudaStream_t st);
 void launch_permute_to_ref(const double* q_dev, double* q_ref, const int32_t* new2ref,
                            int n_total, int V, cudaStream_t st);
-void launch_fill_ghost_grad(double* gx, double* gy, double* lim, int n_real, int n_total, int V,
+void launch_fill_ghost_grad(void* gx, void* gy, void* lim, int n_real, int n_total, int V, bool f32,
                             cudaStream_t st);
+void launch_to_float(const double* a, float* b, size_t n, cudaStream_t st);
+void launch_to_double(const float* a, double* b, size_t n, cudaStream_t st);
 void launch_check_state(const Params& P, const double* q, int* flag, cudaStream_t st);
 void launch_force(const Params& P, const double* q, int group, double* out2, cudaStream_t st);
 

@@ -273,6 +273,7 @@ void build_face_arrays(const HostMesh& m, FaceArrays& fa) {
     }
     const int64_t G = m.n_bound;
     fa.ghost_group.assign(G, 0); fa.ghost_cell.assign(G, 0); fa.ghost_slot.assign(G, 0);
+    for (auto* v : {&fa.g_nx, &fa.g_ny, &fa.g_le, &fa.g_dx, &fa.g_dy}) v->assign(G, 0.);
     for (int64_t b = 0; b < G; ++b) {
         const int32_t ref = m.new2ref[N + b];          // reference ghost index
         const int64_t rb = ref - N;                    // its boundary segment
@@ -282,10 +283,71 @@ void build_face_arrays(const HostMesh& m, FaceArrays& fa) {
         fa.ghost_cell[b] = c;
         for (int k = 0; k < m.n_faces[c]; ++k)
             if (m.face_edge[c * F + k] == (int32_t)e) fa.ghost_slot[b] = (uint8_t)k;
+        const uint32_t ci = m.edge_cells[2 * e];  // reference index of the interior cell
+        fa.g_nx[b] = m.enx[e]; fa.g_ny[b] = m.eny[e]; fa.g_le[b] = m.elen[e];
+        fa.g_dx[b] = m.ecx[e] - m.ccx[ci];
+        fa.g_dy[b] = m.ecy[e] - m.ccy[ci];
     }
     fa.area.assign(NT, 0.);
     for (int64_t n = 0; n < NT; ++n) fa.area[n] = m.area[m.new2ref[n]];
     fa.cell0 = m.ref2new[0];
+}
+
+void build_tiles(const HostMesh& m, const FaceArrays& fa, int T, TileArrays& ta) {
+    const int64_t N = m.n_real, NT = m.n_total, F = HostMesh::MAXF;
+    ta.tile_cells = T;
+    ta.n_tiles = (int)((N + T - 1) / T);
+    ta.info.assign((size_t)ta.n_tiles * 4, 0);
+    ta.halo.clear(); ta.edge_ij.clear(); ta.edge_ref.clear();
+    for (auto* v : {&ta.enx, &ta.eny, &ta.ele, &ta.exf, &ta.eyf, &ta.eg}) v->clear();
+    ta.face.assign((size_t)F * N, 0xFFFF);
+    ta.max_halo = 0; ta.max_edges = 0;
+    std::vector<int32_t> local(NT, -1);          // device cell -> local index in the current tile
+    std::vector<int32_t> edge_stamp(m.n_edges, -1), edge_local(m.n_edges, 0);
+    std::vector<int32_t> touched;
+    for (int t = 0; t < ta.n_tiles; ++t) {
+        const int64_t c0 = (int64_t)t * T, c1 = std::min<int64_t>(c0 + T, N);
+        const int edge_off = (int)ta.edge_ij.size(), halo_off = (int)ta.halo.size();
+        int n_halo = 0, n_edges = 0;
+        touched.clear();
+        for (int64_t c = c0; c < c1; ++c) { local[c] = (int32_t)(c - c0); touched.push_back((int32_t)c); }
+        auto loc = [&](int32_t dev) {
+            if (local[dev] < 0) {
+                local[dev] = T + n_halo++;
+                ta.halo.push_back(dev);
+                touched.push_back(dev);
+            }
+            return local[dev];
+        };
+        for (int64_t c = c0; c < c1; ++c) {
+            for (int k = 0; k < m.n_faces[c]; ++k) {
+                const int32_t e = m.face_edge[c * F + k];
+                const int side = m.face_side[c * F + k];
+                if (edge_stamp[e] != t) {
+                    edge_stamp[e] = t;
+                    edge_local[e] = n_edges++;
+                    const int32_t di = m.ref2new[m.edge_cells[2 * e]], dj = m.ref2new[m.edge_cells[2 * e + 1]];
+                    const uint32_t li = (uint32_t)loc(di), lj = (uint32_t)loc(dj);
+                    ta.edge_ij.push_back(li | (lj << 16));
+                    ta.edge_ref.push_back(e);
+                    ta.enx.push_back(m.enx[e]); ta.eny.push_back(m.eny[e]); ta.ele.push_back(m.elen[e]);
+                    ta.exf.push_back(m.ecx[e]); ta.eyf.push_back(m.ecy[e]);
+                    const size_t s = (size_t)k * N + c;
+                    ta.eg.push_back(fa.g[s]);
+                }
+                const uint32_t other = m.edge_cells[2 * e + (side ? 0 : 1)];
+                const int ghost = other >= (uint32_t)N ? 1 : 0;
+                ta.face[(size_t)k * N + c] = (uint16_t)(edge_local[e] | (ghost << 14) | (side << 15));
+            }
+        }
+        ta.info[4 * t + 0] = edge_off; ta.info[4 * t + 1] = n_edges;
+        ta.info[4 * t + 2] = halo_off; ta.info[4 * t + 3] = n_halo;
+        ta.max_halo = std::max(ta.max_halo, n_halo);
+        ta.max_edges = std::max(ta.max_edges, n_edges);
+        for (int32_t d : touched) local[d] = -1;
+    }
+    ta.ccx.assign(NT, 0.); ta.ccy.assign(NT, 0.);
+    for (int64_t n = 0; n < NT; ++n) { ta.ccx[n] = m.ccx[m.new2ref[n]]; ta.ccy[n] = m.ccy[m.new2ref[n]]; }
 }
 
 // ----------------------------------------------------------------------------

@@ -45,10 +45,29 @@ struct FaceArrays {
     std::vector<double> dnx, dny;         // x_f - x_neighbour
     std::vector<int32_t> ghost_group, ghost_cell;
     std::vector<uint8_t> ghost_slot;
+    std::vector<double> g_nx, g_ny, g_le, g_dx, g_dy;   // per ghost: face normal, length, x_f - x_interior
     std::vector<double> area;             // [n_total] device numbering
     int32_t cell0 = 0;                    // device index of reference cell 0
 };
 void build_face_arrays(const HostMesh& m, FaceArrays& fa);
+
+// Tiles of `tile_cells` consecutive device-numbered real cells.  Each tile
+// lists the edges touching its cells (an edge cut by a tile boundary is
+// listed by both tiles) with tile-local cell indices: owned cell c ->
+// c - tile_start, halo cell h -> tile_cells + h.  Edges keep the reference
+// orientation (first index = edge_cells(e, 0)).
+struct TileArrays {
+    int tile_cells = 0, n_tiles = 0;
+    int max_halo = 0, max_edges = 0;
+    std::vector<int32_t> info;        // [n_tiles][4]: edge_off, n_edges, halo_off, n_halo
+    std::vector<int32_t> halo;        // device cell index of each halo slot
+    std::vector<uint32_t> edge_ij;    // local i | local j << 16
+    std::vector<int32_t> edge_ref;    // reference edge index of each tile edge
+    std::vector<double> enx, eny, ele, exf, eyf, eg;  // per tile edge
+    std::vector<uint16_t> face;       // [MAXF][n_real]: local edge | side << 15, 0xFFFF = none
+    std::vector<double> ccx, ccy;     // [n_total] device numbering
+};
+void build_tiles(const HostMesh& m, const FaceArrays& fa, int tile_cells, TileArrays& ta);
 
 // Builds the reference geometry from an element mesh (mesh.cpp:130-260,
 // 623-669).  Returns "" on success, else an error message.

@@ -1,0 +1,783 @@
+// Tile kernels of the explicit FV step.
+//
+// The device-numbered (Hilbert-ordered) real cells are cut into tiles of T
+// consecutive cells; one CTA of T threads owns one tile.  A CTA stages the
+// records of its cells and their halo (state, gradients, centroid) into
+// shared memory, computes every edge flux touching the tile once, and then
+// lets each thread sum its cell's faces from shared memory in increasing
+// reference edge order -- deterministic, atomic-free, and (with the Exact
+// policy) bit-identical to the reference's edge-scatter loops.
+//
+// Math policies: MExact (FP64, reference evaluation order; instantiated in a
+// -fmad=false translation unit), MF64 (FP64, fast algebra), MF32 (FP32 bulk
+// arithmetic and storage of stage states, gradients and geometry; FP64
+// conserved state, per-cell flux sums, RK accumulation and residuals).  The
+// fast policies store the limiter already multiplied into the gradients.
+//
+// Face words (uint16, [4][n_real]): bits 0-13 tile-local edge, bit 14 the
+// neighbour is a boundary ghost, bit 15 the cell is the edge's second cell;
+// 0xFFFF = no face.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <type_traits>
+
+#include "fv_internal.h"
+#include "fv_physics_exact.cuh"
+#include "fv_physics_fast.cuh"
+
+namespace fvgpu {
+
+struct MExact { using S = double; static constexpr bool exact = true; };
+struct MF64 { using S = double; static constexpr bool exact = false; };
+struct MF32 { using S = float; static constexpr bool exact = false; };
+
+constexpr int kDtSlots = 64;        // atomic slots of the global dt minimum
+constexpr int kTileMax = 256;       // threads (= cells) per tile at most
+constexpr uint16_t kFaceNone = 0xFFFF;
+constexpr int kFaceEdgeMask = 0x3FFF;
+
+struct TileParams {
+    Params P;                  // sizes, ghost metadata and physics
+    int T;                     // cells per tile (= threads per CTA)
+    int max_halo, max_edges;
+    const int4* info;          // [n_tiles]: edge_off, n_edges, halo_off, n_halo
+    const int32_t* halo;       // device cell index per halo slot
+    const uint32_t* edge_ij;   // local i | local j << 16
+    const void* enx;           // S [tile edges]: normal, length, face centre, GG weight
+    const void* eny;
+    const void* ele;
+    const void* exf;
+    const void* eyf;
+    const void* eg;
+    const uint16_t* face;      // [4][n_real] face words
+    const void* ccx;           // S [n_total] centroids
+    const void* ccy;
+    const void* area;          // S [n_total]
+};
+
+struct TileIO {
+    const void* q_stage;       // S [n_total][V] stage input
+    const double* q_base;      // [n_total][V] step-start state (FP64)
+    double* q_out;             // FP64 output (FP64 modes: every stage; FP32: last stage only)
+    void* s_out;               // FP32 mode: FP32 stage output (the next stage's input)
+    void* gx;                  // S [n_total][V]; fast modes: limited gradients; ghosts hold 0
+    void* gy;
+    void* lim;                 // exact mode only; ghosts hold 1
+    double* dt;                // [n_total]
+    double alpha;
+    Ctrl* ctrl;                // nullptr: always active, dt from dt[]
+    double* partials;          // [n_tiles][V] or nullptr
+    unsigned long long* dtkeys;  // [kDtSlots] ordered keys of the global dt minimum
+    int write_f64;             // FP32 mode: also write q_out (last stage)
+};
+
+__device__ __forceinline__ unsigned long long tkey(double x) {
+    if (x != x) return ~0ull;
+    const long long b = __double_as_longlong(x);
+    return b < 0 ? ~(unsigned long long)b : ((unsigned long long)b | 0x8000000000000000ull);
+}
+__device__ __forceinline__ double tkey_inv(unsigned long long k) {
+    if (k == ~0ull) return __longlong_as_double(0x7ff8000000000000ll);
+    const unsigned long long b = (k & 0x8000000000000000ull) ? (k & 0x7fffffffffffffffull) : ~k;
+    return __longlong_as_double((long long)b);
+}
+__device__ __forceinline__ bool t_inactive(const Ctrl* c) { return c != nullptr && *(volatile const int*)&c->active == 0; }
+__device__ __forceinline__ unsigned long long kmin_(unsigned long long a, unsigned long long b) { return b < a ? b : a; }
+
+template <class S, int V>
+__device__ __forceinline__ void ld(const S* __restrict__ a, int c, S* v) {
+    if (V == 4 && sizeof(S) == 8) {
+        const double2* p = reinterpret_cast<const double2*>(a + 4 * (size_t)c);
+        const double2 x = p[0], y = p[1];
+        v[0] = (S)x.x; v[1] = (S)x.y; v[2] = (S)y.x; v[3] = (S)y.y;
+    } else if (V == 4) {
+        const float4 x = *reinterpret_cast<const float4*>(a + 4 * (size_t)c);
+        v[0] = (S)x.x; v[1] = (S)x.y; v[2] = (S)x.z; v[3] = (S)x.w;
+    } else {
+#pragma unroll
+        for (int k = 0; k < V; ++k) v[k] = a[(size_t)V * c + k];
+    }
+}
+template <class S, int V>
+__device__ __forceinline__ void st(S* __restrict__ a, int c, const S* v) {
+    if (V == 4 && sizeof(S) == 8) {
+        double2* p = reinterpret_cast<double2*>(a + 4 * (size_t)c);
+        p[0] = make_double2((double)v[0], (double)v[1]);
+        p[1] = make_double2((double)v[2], (double)v[3]);
+    } else if (V == 4) {
+        *reinterpret_cast<float4*>(a + 4 * (size_t)c) = make_float4((float)v[0], (float)v[1], (float)v[2], (float)v[3]);
+    } else {
+#pragma unroll
+        for (int k = 0; k < V; ++k) a[(size_t)V * c + k] = v[k];
+    }
+}
+// V consecutive values at a 16-byte aligned shared-memory address
+template <class S, int V>
+__device__ __forceinline__ void lds(const S* p, S* v) {
+    if (V == 4 && sizeof(S) == 8) {
+        const double2 x = reinterpret_cast<const double2*>(p)[0], y = reinterpret_cast<const double2*>(p)[1];
+        v[0] = (S)x.x; v[1] = (S)x.y; v[2] = (S)y.x; v[3] = (S)y.y;
+    } else if (V == 4) {
+        const float4 x = reinterpret_cast<const float4*>(p)[0];
+        v[0] = (S)x.x; v[1] = (S)x.y; v[2] = (S)x.z; v[3] = (S)x.w;
+    } else {
+#pragma unroll
+        for (int k = 0; k < V; ++k) v[k] = p[k];
+    }
+}
+
+// Shared-memory record of one tile-local cell: q[V], then (second order)
+// gx[V], gy[V], (exact) lim[V], then the centroid; padded to 16 bytes.
+template <class M, int V, bool ORDER2, bool CENTROID>
+struct Rec {
+    using S = typename M::S;
+    static constexpr int NG = ORDER2 ? (M::exact ? 3 : 2) : 0;
+    static constexpr int OGX = V, OGY = 2 * V, OLM = 3 * V;
+    static constexpr int OC = V * (1 + NG);
+    static constexpr int RAW = OC + (CENTROID ? 2 : 0);
+    static constexpr int AL = 16 / (int)sizeof(S);
+    static constexpr int NR = (RAW + AL - 1) / AL * AL;
+};
+
+// Optional positivity guard (not in the reference): a reconstructed Euler
+// face state with rho <= 0 or p <= 0 is replaced by the cell value.
+template <class S, int V>
+__device__ __forceinline__ void guard_face(const Params& P, S* qf, const S* qc) {
+    if (V != 4 || !P.positivity_guard) return;
+    const S p = ((S)P.gamma - S(1)) * (qf[3] - S(0.5) / qf[0] * (qf[1] * qf[1] + qf[2] * qf[2]));
+    if (!(qf[0] > S(0)) || !(p > S(0))) {
+#pragma unroll
+        for (int k = 0; k < V; ++k) qf[k] = qc[k];
+    }
+}
+
+// Loads the records of the tile's owned cells and halo.
+template <class M, int V, bool ORDER2, bool CENTROID>
+__device__ __forceinline__ void stage_records(const TileParams& TP, const TileIO& io, const int4& inf, int c0,
+                                              int nown, typename M::S* rec) {
+    using S = typename M::S;
+    using R = Rec<M, V, ORDER2, CENTROID>;
+    const S* Q = (const S*)io.q_stage;
+    const S* CX = (const S*)TP.ccx;
+    const S* CY = (const S*)TP.ccy;
+    for (int l = threadIdx.x; l < nown + inf.w; l += blockDim.x) {
+        int slot, g;
+        if (l < nown) { slot = l; g = c0 + l; }
+        else { slot = TP.T + (l - nown); g = TP.halo[inf.z + (l - nown)]; }
+        S* r = rec + (size_t)slot * R::NR;
+        S v[V];
+        ld<S, V>(Q, g, v); st<S, V>(r, 0, v);
+        if (ORDER2) {
+            ld<S, V>((const S*)io.gx, g, v); st<S, V>(r + R::OGX, 0, v);
+            ld<S, V>((const S*)io.gy, g, v); st<S, V>(r + R::OGY, 0, v);
+            if (M::exact) { ld<S, V>((const S*)io.lim, g, v); st<S, V>(r + R::OLM, 0, v); }
+        }
+        if (CENTROID) { r[R::OC] = CX[g]; r[R::OC + 1] = CY[g]; }
+    }
+}
+
+// Loads the tile's edge geometry (contiguous per tile) into shared memory.
+template <class S, bool GG>
+__device__ __forceinline__ void stage_edges(const TileParams& TP, const int4& inf, uint32_t* sij, S* snx, S* sny,
+                                            S* sle, S* sg, S* sxf, S* syf) {
+    for (int e = threadIdx.x; e < inf.y; e += blockDim.x) {
+        const int ge = inf.x + e;
+        sij[e] = TP.edge_ij[ge];
+        snx[e] = ((const S*)TP.enx)[ge];
+        sny[e] = ((const S*)TP.eny)[ge];
+        sle[e] = ((const S*)TP.ele)[ge];
+        if (GG) {
+            sg[e] = ((const S*)TP.eg)[ge];
+            sxf[e] = ((const S*)TP.exf)[ge];
+            syf[e] = ((const S*)TP.eyf)[ge];
+        }
+    }
+}
+
+__device__ __forceinline__ void load_faces(const TileParams& TP, int c, uint16_t* w) {
+    const int N = TP.P.n_real;
+#pragma unroll
+    for (int f = 0; f < kMaxFaces; ++f) w[f] = TP.face[f * N + c];
+}
+
+// ------------------------------------------------------------------ K0: dt --
+template <class M, int V>
+__global__ void __launch_bounds__(kTileMax) k_tile_dt(TileParams TP, TileIO io) {
+    using S = typename M::S;
+    using R = Rec<M, V, false, false>;
+    if (t_inactive(io.ctrl)) return;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const Params& P = TP.P;
+    const int N = P.n_real, T = TP.T, t = blockIdx.x;
+    const int4 inf = TP.info[t];
+    const int c0 = t * T, nown = min(T, N - c0);
+    const int LT = T + TP.max_halo;
+    S* rec = reinterpret_cast<S*>(smem_raw);
+    S* snx = rec + (size_t)LT * R::NR;
+    S* sny = snx + TP.max_edges;
+    S* sle = sny + TP.max_edges;
+    uint32_t* sij = reinterpret_cast<uint32_t*>(sle + TP.max_edges);
+    __shared__ unsigned long long wmin[kTileMax / 32];
+    stage_records<M, V, false, false>(TP, io, inf, c0, nown, rec);
+    stage_edges<S, false>(TP, inf, sij, snx, sny, sle, nullptr, nullptr, nullptr);
+    __syncthreads();
+    unsigned long long kmin = ~0ull;
+    const int l = threadIdx.x;
+    if (l < nown) {
+        const int c = c0 + l;
+        const S* AR = (const S*)TP.area;
+        uint16_t w[kMaxFaces];
+        load_faces(TP, c, w);
+        if (P.dt_kind == 0) {
+            io.dt[c] = P.dt_const;
+            kmin = tkey(P.dt_const);
+#pragma unroll
+            for (int f = 0; f < kMaxFaces; ++f) {
+                if (w[f] == kFaceNone || !(w[f] & 0x4000)) continue;
+                const int el = w[f] & kFaceEdgeMask, side = w[f] >> 15;
+                const uint32_t ij = sij[el];
+                const int o = side ? (int)(ij & 0xffff) : (int)(ij >> 16);
+                io.dt[TP.halo[inf.z + o - T]] = P.dt_const;
+            }
+        } else if (V == 4) {
+            S qs[4];
+            lds<S, 4>(rec + (size_t)l * R::NR, qs);
+            const bool sum = P.dt_kind == 1;
+            if constexpr (M::exact) {
+                const double gamma = P.gamma, gm1 = gamma - 1, cfl = P.cfl;
+                const double cs = sqrt((gm1 * (qs[3] - 0.5 / qs[0] * (qs[1] * qs[1] + qs[2] * qs[2]))) * gamma / qs[0]);
+                const double Ai = AR[c];
+                double acc = sum ? 0. : 1.0;
+#pragma unroll
+                for (int f = 0; f < kMaxFaces; ++f) {
+                    if (w[f] == kFaceNone) continue;
+                    const int el = w[f] & kFaceEdgeMask, side = w[f] >> 15;
+                    const uint32_t ij = sij[el];
+                    const int o = side ? (int)(ij & 0xffff) : (int)(ij >> 16);
+                    const double n0 = snx[el], n1 = sny[el], le = sle[el];
+                    double qn[4];
+                    lds<double, 4>(rec + (size_t)o * R::NR, qn);
+                    const double cn = sqrt((gm1 * (qn[3] - 0.5 / qn[0] * (qn[1] * qn[1] + qn[2] * qn[2]))) * gamma / qn[0]);
+                    const bool ghost = (w[f] & 0x4000) != 0;
+                    if (sum) {
+                        const double es = cs + fabs(qs[1] / qs[0] * n0 + qs[2] / qs[0] * n1);
+                        const double en = cn + fabs(qn[1] / qn[0] * n0 + qn[2] / qn[0] * n1);
+                        const double center = side ? exact::dmax(en, es) : exact::dmax(es, en);
+                        acc += center * le;
+                        if (ghost) {
+                            const int g = TP.halo[inf.z + o - T];
+                            double d = 0.;
+                            d += center * le;
+                            const double dg = cfl * AR[g] / d;
+                            io.dt[g] = dg;
+                            kmin = kmin_(kmin, tkey(dg));
+                        }
+                    } else {
+                        const double es = (cs + fabs(qs[1] / qs[0])) * n0 + (cs + fabs(qs[2] / qs[0])) * n1;
+                        acc = exact::dmin(acc, cfl * (Ai / le) / fabs(es));
+                        if (ghost) {
+                            const int g = TP.halo[inf.z + o - T];
+                            const double en = (cn + fabs(qn[1] / qn[0])) * n0 + (cn + fabs(qn[2] / qn[0])) * n1;
+                            const double dg = exact::dmin(1.0, cfl * (AR[g] / le) / fabs(en));
+                            io.dt[g] = dg;
+                            kmin = kmin_(kmin, tkey(dg));
+                        }
+                    }
+                }
+                const double di = sum ? cfl * Ai / acc : acc;
+                io.dt[c] = di;
+                kmin = kmin_(kmin, tkey(di));
+            } else {
+                const S gamma = (S)P.gamma, gm1 = gamma - S(1), cfl = (S)P.cfl;
+                const S ri = fast::rcp(qs[0]);
+                const S us = qs[1] * ri, vs = qs[2] * ri;
+                const S cs = fast::sqrt_(gamma * gm1 * (qs[3] * ri - S(0.5) * (us * us + vs * vs)));
+                const S Ai = AR[c];
+                S acc = sum ? S(0) : S(1);
+#pragma unroll
+                for (int f = 0; f < kMaxFaces; ++f) {
+                    if (w[f] == kFaceNone) continue;
+                    const int el = w[f] & kFaceEdgeMask, side = w[f] >> 15;
+                    const uint32_t ij = sij[el];
+                    const int o = side ? (int)(ij & 0xffff) : (int)(ij >> 16);
+                    const S n0 = snx[el], n1 = sny[el], le = sle[el];
+                    S qn[4];
+                    lds<S, 4>(rec + (size_t)o * R::NR, qn);
+                    const S rn = fast::rcp(qn[0]);
+                    const S un = qn[1] * rn, vn = qn[2] * rn;
+                    const S cn = fast::sqrt_(gamma * gm1 * (qn[3] * rn - S(0.5) * (un * un + vn * vn)));
+                    const bool ghost = (w[f] & 0x4000) != 0;
+                    if (sum) {
+                        const S center = fast::tmax(cs + fabs(us * n0 + vs * n1), cn + fabs(un * n0 + vn * n1));
+                        acc += center * le;
+                        if (ghost) {
+                            const int g = TP.halo[inf.z + o - T];
+                            const double dg = (double)(cfl * AR[g] * fast::rcp(center * le));
+                            io.dt[g] = dg;
+                            kmin = kmin_(kmin, tkey(dg));
+                        }
+                    } else {
+                        const S es = (cs + fabs(us)) * n0 + (cs + fabs(vs)) * n1;
+                        acc = fast::tmin(acc, cfl * Ai * fast::rcp(le * fabs(es)));
+                        if (ghost) {
+                            const int g = TP.halo[inf.z + o - T];
+                            const S en = (cn + fabs(un)) * n0 + (cn + fabs(vn)) * n1;
+                            const double dg = (double)fast::tmin(S(1), cfl * (S)AR[g] * fast::rcp(le * fabs(en)));
+                            io.dt[g] = dg;
+                            kmin = kmin_(kmin, tkey(dg));
+                        }
+                    }
+                }
+                const double di = (double)(sum ? cfl * Ai * fast::rcp(acc) : acc);
+                io.dt[c] = di;
+                kmin = kmin_(kmin, tkey(di));
+            }
+        }
+    }
+    if (P.global_dt && io.dtkeys != nullptr) {
+        // block minimum, then one atomic per block spread over kDtSlots slots
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) kmin = kmin_(kmin, __shfl_xor_sync(0xffffffffu, kmin, o));
+        if ((threadIdx.x & 31) == 0) wmin[threadIdx.x >> 5] = kmin;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            unsigned long long b = ~0ull;
+            for (int i = 0; i < (int)(blockDim.x >> 5); ++i) b = kmin_(b, wmin[i]);
+            if (b != ~0ull) atomicMin(io.dtkeys + (blockIdx.x % kDtSlots), b);
+        }
+    }
+}
+
+// ------------------------------------------------ K1: gradients + limiters --
+template <class M, int V>
+__global__ void __launch_bounds__(kTileMax) k_tile_gradlim(TileParams TP, TileIO io) {
+    using S = typename M::S;
+    using R = Rec<M, V, false, true>;
+    if (t_inactive(io.ctrl)) return;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const Params& P = TP.P;
+    const int N = P.n_real, T = TP.T, t = blockIdx.x;
+    const int4 inf = TP.info[t];
+    const int c0 = t * T, nown = min(T, N - c0);
+    const int LT = T + TP.max_halo, EM = TP.max_edges;
+    S* rec = reinterpret_cast<S*>(smem_raw);
+    S* snx = rec + (size_t)LT * R::NR;
+    S* sny = snx + EM; S* sle = sny + EM; S* sg = sle + EM; S* sxf = sg + EM; S* syf = sxf + EM;
+    uint32_t* sij = reinterpret_cast<uint32_t*>(syf + EM);
+    stage_records<M, V, false, true>(TP, io, inf, c0, nown, rec);
+    stage_edges<S, true>(TP, inf, sij, snx, sny, sle, sg, sxf, syf);
+    __syncthreads();
+    const int l = threadIdx.x;
+    if (l >= nown) return;
+    const int c = c0 + l;
+    uint16_t w[kMaxFaces];
+    load_faces(TP, c, w);
+    const S A = ((const S*)TP.area)[c];
+    const S* rs = rec + (size_t)l * R::NR;
+    S qs[V], gx[V], gy[V], qmn[V], qmx[V], lim[V];
+    lds<S, V>(rs, qs);
+#pragma unroll
+    for (int k = 0; k < V; ++k) { gx[k] = 0; gy[k] = 0; qmn[k] = qs[k]; qmx[k] = qs[k]; lim[k] = 1; }
+#pragma unroll
+    for (int f = 0; f < kMaxFaces; ++f) {
+        if (w[f] == kFaceNone) continue;
+        const int el = w[f] & kFaceEdgeMask, side = w[f] >> 15;
+        const uint32_t ij = sij[el];
+        const int o = side ? (int)(ij & 0xffff) : (int)(ij >> 16);
+        const S nx = snx[el], ny = sny[el], le = sle[el], g = sg[el];
+        S qn[V];
+        lds<S, V>(rec + (size_t)o * R::NR, qn);
+#pragma unroll
+        for (int k = 0; k < V; ++k) {
+            if constexpr (M::exact) {
+                if (!side) {
+                    const double fl = (qs[k] * (1.0 - g) + qn[k] * g) * le;
+                    gx[k] += fl * nx; gy[k] += fl * ny;
+                } else {
+                    const double fl = (qn[k] * (1.0 - g) + qs[k] * g) * le;
+                    gx[k] -= fl * nx; gy[k] -= fl * ny;
+                }
+                qmn[k] = exact::dmin(qmn[k], qn[k]); qmx[k] = exact::dmax(qmx[k], qn[k]);
+            } else {
+                const S qi = side ? qn[k] : qs[k], qj = side ? qs[k] : qn[k];
+                const S fl = (qi + (qj - qi) * g) * (side ? -le : le);
+                gx[k] += fl * nx; gy[k] += fl * ny;
+                qmn[k] = fast::tmin(qmn[k], qn[k]); qmx[k] = fast::tmax(qmx[k], qn[k]);
+            }
+        }
+    }
+    const S xc = rs[R::OC], yc = rs[R::OC + 1];
+    if constexpr (M::exact) {
+        const double invA = 1. / A;
+#pragma unroll
+        for (int k = 0; k < V; ++k) { gx[k] *= invA; gy[k] *= invA; }
+        const double sqrt_area = sqrt(A);
+        const double tol = 1e-15;
+#pragma unroll
+        for (int f = 0; f < kMaxFaces; ++f) {
+            if (w[f] == kFaceNone) continue;
+            const int el = w[f] & kFaceEdgeMask;
+            const double dx = sxf[el] - xc, dy = syf[el] - yc;
+#pragma unroll
+            for (int k = 0; k < V; ++k) {
+                const double dqg = gx[k] * dx + gy[k] * dy;
+                const double delta_max = qmx[k] - qs[k];
+                const double delta_min = qmn[k] - qs[k];
+                const double Ka = P.K * sqrt_area;
+                const double K3a = Ka * Ka * Ka;
+                const double d2 = (delta_max - delta_min) * (delta_max - delta_min);
+                double sig;
+                if (d2 <= K3a) sig = 1.;
+                else if (d2 <= 2 * K3a) {
+                    const double y = (d2 / K3a - 1.0);
+                    sig = 2.0 * y * y * y - 3.0 * y * y + 1.0;
+                } else sig = 0.;
+                double lv = 1.0;
+                if (sig < 1.0) {
+                    if (dqg > tol) lv = exact::limiter_func(P.limiter, delta_max / dqg);
+                    else if (dqg < -tol) lv = exact::limiter_func(P.limiter, delta_min / dqg);
+                    else lv = 1.0;
+                }
+                lv = sig + (1.0 - sig) * lv;
+                lim[k] = exact::dmin(lim[k], lv);
+            }
+        }
+        st<S, V>((S*)io.gx, c, gx);
+        st<S, V>((S*)io.gy, c, gy);
+        st<S, V>((S*)io.lim, c, lim);
+    } else {
+        const S invA = fast::rcp(A);
+#pragma unroll
+        for (int k = 0; k < V; ++k) { gx[k] *= invA; gy[k] *= invA; }
+        const S Ka = (S)P.K * fast::sqrt_(A);
+        const S K3a = Ka * Ka * Ka, rK3a = fast::rcp(K3a);
+        const S tol = S(1e-15);
+        // the smooth switch sigma depends on the cell and variable only
+        S sig[V];
+#pragma unroll
+        for (int k = 0; k < V; ++k) {
+            const S d = qmx[k] - qmn[k];
+            const S d2 = d * d;
+            if (d2 <= K3a) sig[k] = 1;
+            else if (d2 <= 2 * K3a) {
+                const S y = d2 * rK3a - S(1);
+                sig[k] = (S(2) * y - S(3)) * y * y + S(1);
+            } else sig[k] = 0;
+        }
+#pragma unroll
+        for (int f = 0; f < kMaxFaces; ++f) {
+            if (w[f] == kFaceNone) continue;
+            const int el = w[f] & kFaceEdgeMask;
+            const S dx = sxf[el] - xc, dy = syf[el] - yc;
+#pragma unroll
+            for (int k = 0; k < V; ++k) {
+                if (sig[k] < S(1)) {
+                    const S dqg = gx[k] * dx + gy[k] * dy;
+                    S phi = 1;
+                    if (dqg > tol) phi = fast::limiter_func(P.limiter, fast::div_(qmx[k] - qs[k], dqg));
+                    else if (dqg < -tol) phi = fast::limiter_func(P.limiter, fast::div_(qmn[k] - qs[k], dqg));
+                    lim[k] = fast::tmin(lim[k], sig[k] + (S(1) - sig[k]) * phi);
+                }
+            }
+        }
+        // limited gradients
+#pragma unroll
+        for (int k = 0; k < V; ++k) { gx[k] *= lim[k]; gy[k] *= lim[k]; }
+        st<S, V>((S*)io.gx, c, gx);
+        st<S, V>((S*)io.gy, c, gy);
+    }
+}
+
+// ------------------------------------- K2: flux + RK update + ghost fill --
+template <class M, int V, bool ORDER2, int FLUX>
+__global__ void __launch_bounds__(kTileMax) k_tile_stage(TileParams TP, TileIO io) {
+    using S = typename M::S;
+    using FT = typename std::conditional<M::exact, double, S>::type;  // flux storage
+    using R = Rec<M, V, ORDER2, ORDER2>;
+    if (t_inactive(io.ctrl)) return;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ unsigned long long s_dtkey;
+    const Params& P = TP.P;
+    const int N = P.n_real, T = TP.T, t = blockIdx.x;
+    const int4 inf = TP.info[t];
+    const int c0 = t * T, nown = min(T, N - c0);
+    const int LT = T + TP.max_halo;
+    S* rec = reinterpret_cast<S*>(smem_raw);
+    FT* sF = reinterpret_cast<FT*>(rec + (size_t)LT * R::NR);
+    stage_records<M, V, ORDER2, ORDER2>(TP, io, inf, c0, nown, rec);
+    const bool global_dt = io.ctrl != nullptr && P.global_dt;
+    if (global_dt && threadIdx.x < 32) {
+        unsigned long long k = kmin_(io.dtkeys[threadIdx.x], io.dtkeys[threadIdx.x + 32]);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) k = kmin_(k, __shfl_xor_sync(0xffffffffu, k, o));
+        if (threadIdx.x == 0) s_dtkey = k;
+    }
+    __syncthreads();
+    const S* NX = (const S*)TP.enx; const S* NY = (const S*)TP.eny; const S* LE = (const S*)TP.ele;
+    const S* XF = (const S*)TP.exf; const S* YF = (const S*)TP.eyf;
+    // ---- one flux per tile edge
+    for (int el = threadIdx.x; el < inf.y; el += blockDim.x) {
+        const int e = inf.x + el;
+        const uint32_t ij = TP.edge_ij[e];
+        const int li = (int)(ij & 0xffff), lj = (int)(ij >> 16);
+        const S n0 = NX[e], n1 = NY[e];
+        const S* ri = rec + (size_t)li * R::NR;
+        const S* rj = rec + (size_t)lj * R::NR;
+        S qL[V], qR[V];
+        lds<S, V>(ri, qL);
+        lds<S, V>(rj, qR);
+        if (ORDER2) {
+            const S xf = XF[e], yf = YF[e];
+            const S di0 = xf - ri[R::OC], di1 = yf - ri[R::OC + 1];
+            const S dj0 = xf - rj[R::OC], dj1 = yf - rj[R::OC + 1];
+            S gxi[V], gyi[V], gxj[V], gyj[V];
+            lds<S, V>(ri + R::OGX, gxi); lds<S, V>(ri + R::OGY, gyi);
+            lds<S, V>(rj + R::OGX, gxj); lds<S, V>(rj + R::OGY, gyj);
+            S ci[V], cj[V];
+#pragma unroll
+            for (int k = 0; k < V; ++k) { ci[k] = qL[k]; cj[k] = qR[k]; }
+            if constexpr (M::exact) {
+                S li_[V], lj_[V];
+                lds<S, V>(ri + R::OLM, li_); lds<S, V>(rj + R::OLM, lj_);
+#pragma unroll
+                for (int k = 0; k < V; ++k) {
+                    qL[k] = ci[k] + (gxi[k] * di0 + gyi[k] * di1) * li_[k];
+                    qR[k] = cj[k] + (gxj[k] * dj0 + gyj[k] * dj1) * lj_[k];
+                }
+            } else {
+#pragma unroll
+                for (int k = 0; k < V; ++k) {
+                    qL[k] = ci[k] + gxi[k] * di0 + gyi[k] * di1;
+                    qR[k] = cj[k] + gxj[k] * dj0 + gyj[k] * dj1;
+                }
+            }
+            guard_face<S, V>(P, qL, ci);
+            guard_face<S, V>(P, qR, cj);
+        }
+        FT f[V];
+        if constexpr (M::exact) {
+            exact::flux<FLUX>(P.gamma, f, qL, qR, n0, n1);
+        } else {
+            fast::flux<FLUX, S>((S)P.gamma, f, qL, qR, n0, n1);
+            const S le = LE[e];
+#pragma unroll
+            for (int k = 0; k < V; ++k) f[k] *= le;
+        }
+#pragma unroll
+        for (int k = 0; k < V; ++k) sF[el * V + k] = f[k];
+    }
+    __syncthreads();
+    // ---- per-cell sums in reference edge order, RK update, ghost fill
+    const int l = threadIdx.x;
+    double res[V];
+#pragma unroll
+    for (int k = 0; k < V; ++k) res[k] = 0.;
+    if (l < nown) {
+        const int c = c0 + l;
+        uint16_t w[kMaxFaces];
+        load_faces(TP, c, w);
+        const double A = (double)((const S*)TP.area)[c];
+        double qt[V];
+#pragma unroll
+        for (int k = 0; k < V; ++k) qt[k] = 0.;
+        bool has_ghost = false;
+#pragma unroll
+        for (int f = 0; f < kMaxFaces; ++f) {
+            if (w[f] == kFaceNone) continue;
+            const int el = w[f] & kFaceEdgeMask, side = w[f] >> 15;
+            has_ghost |= (w[f] & 0x4000) != 0;
+            if constexpr (M::exact) {
+                const double le = LE[inf.x + el];
+#pragma unroll
+                for (int k = 0; k < V; ++k) {
+                    if (!side) qt[k] -= sF[el * V + k] * le / A;
+                    else qt[k] += sF[el * V + k] * le / A;
+                }
+            } else {
+#pragma unroll
+                for (int k = 0; k < V; ++k) qt[k] += side ? (double)sF[el * V + k] : -(double)sF[el * V + k];
+            }
+        }
+        if constexpr (!M::exact) {
+            const double rA = 1.0 / A;
+#pragma unroll
+            for (int k = 0; k < V; ++k) qt[k] *= rA;
+        }
+        double dtc;
+        if (global_dt) {
+            const double d0 = io.dt[P.cell0];
+            dtc = (d0 != d0) ? d0 : tkey_inv(s_dtkey);
+        } else {
+            dtc = io.dt[c];
+        }
+        double qb[V], qnew[V];
+        ld<double, V>(io.q_base, c, qb);
+        if constexpr (M::exact) {
+#pragma unroll
+            for (int k = 0; k < V; ++k) qnew[k] = qb[k] + qt[k] * dtc * io.alpha;
+        } else {
+            const double da = dtc * io.alpha;
+#pragma unroll
+            for (int k = 0; k < V; ++k) qnew[k] = fma(qt[k], da, qb[k]);
+        }
+        if (sizeof(S) == 8) {
+            st<double, V>(io.q_out, c, qnew);
+        } else {
+            S qs[V];
+#pragma unroll
+            for (int k = 0; k < V; ++k) qs[k] = (S)qnew[k];
+            st<S, V>((S*)io.s_out, c, qs);
+            if (io.write_f64) st<double, V>(io.q_out, c, qnew);
+        }
+        if (has_ghost) {
+            const S* rs = rec + (size_t)l * R::NR;
+#pragma unroll
+            for (int f = 0; f < kMaxFaces; ++f) {
+                if (w[f] == kFaceNone || !(w[f] & 0x4000)) continue;
+                const int el = w[f] & kFaceEdgeMask, side = w[f] >> 15;
+                const uint32_t ij = TP.edge_ij[inf.x + el];
+                const int o = side ? (int)(ij & 0xffff) : (int)(ij >> 16);
+                const int g = TP.halo[inf.z + o - T];
+                const S n0 = NX[inf.x + el], n1 = NY[inf.x + el];
+                S qint[V], qc[V], b[V];
+#pragma unroll
+                for (int k = 0; k < V; ++k) { qc[k] = (S)qnew[k]; qint[k] = qc[k]; }
+                if (ORDER2) {
+                    const S d0 = XF[inf.x + el] - rs[R::OC], d1 = YF[inf.x + el] - rs[R::OC + 1];
+                    S gxs[V], gys[V];
+                    lds<S, V>(rs + R::OGX, gxs); lds<S, V>(rs + R::OGY, gys);
+                    if constexpr (M::exact) {
+                        S lms[V];
+                        lds<S, V>(rs + R::OLM, lms);
+#pragma unroll
+                        for (int k = 0; k < V; ++k) qint[k] = qc[k] + (gxs[k] * d0 + gys[k] * d1) * lms[k];
+                    } else {
+#pragma unroll
+                        for (int k = 0; k < V; ++k) qint[k] = qc[k] + gxs[k] * d0 + gys[k] * d1;
+                    }
+                    guard_face<S, V>(P, qint, qc);
+                }
+                if constexpr (M::exact) exact::bc<V>(P, P.ghost_group[g - N], b, qint, n0, n1);
+                else fast::bc<V, S>(P, P.ghost_group[g - N], b, qint, n0, n1);
+                if (sizeof(S) == 8) {
+                    st<double, V>(io.q_out, g, (const double*)b);
+                } else {
+                    st<S, V>((S*)io.s_out, g, b);
+                    if (io.write_f64) {
+                        double bd[V];
+#pragma unroll
+                        for (int k = 0; k < V; ++k) bd[k] = (double)b[k];
+                        st<double, V>(io.q_out, g, bd);
+                    }
+                }
+            }
+        }
+        if (io.partials != nullptr) {
+#pragma unroll
+            for (int k = 0; k < V; ++k) res[k] = qt[k] * qt[k] * A;
+        }
+    }
+    if (io.partials != nullptr) {
+        __shared__ double red[kTileMax / 32][V];
+#pragma unroll
+        for (int k = 0; k < V; ++k)
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) res[k] += __shfl_xor_sync(0xffffffffu, res[k], o);
+        if ((threadIdx.x & 31) == 0)
+#pragma unroll
+            for (int k = 0; k < V; ++k) red[threadIdx.x >> 5][k] = res[k];
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            const int nw = blockDim.x >> 5;
+            for (int k = 0; k < V; ++k) {
+                double s = 0.;
+                for (int w = 0; w < nw; ++w) s += red[w][k];
+                io.partials[(size_t)blockIdx.x * V + k] = s;
+            }
+        }
+    }
+}
+
+// shared memory bytes of each kernel for a tile layout
+template <class M, int V>
+inline size_t smem_dt(const TileParams& TP) {
+    using S = typename M::S;
+    return (size_t)(TP.T + TP.max_halo) * Rec<M, V, false, false>::NR * sizeof(S) +
+           (size_t)TP.max_edges * (3 * sizeof(S) + 4);
+}
+template <class M, int V>
+inline size_t smem_gradlim(const TileParams& TP) {
+    using S = typename M::S;
+    return (size_t)(TP.T + TP.max_halo) * Rec<M, V, false, true>::NR * sizeof(S) +
+           (size_t)TP.max_edges * (6 * sizeof(S) + 4);
+}
+template <class M, int V, bool ORDER2>
+inline size_t smem_stage(const TileParams& TP) {
+    using S = typename M::S;
+    using FT = typename std::conditional<M::exact, double, S>::type;
+    return (size_t)(TP.T + TP.max_halo) * Rec<M, V, ORDER2, ORDER2>::NR * sizeof(S) +
+           (size_t)TP.max_edges * V * sizeof(FT);
+}
+
+// ------------------------------------------------------------- launchers --
+template <class M>
+struct TileLaunch {
+    static cudaError_t prepare(const TileParams& TP) {
+        cudaError_t e = cudaSuccess;
+        auto set = [&](const void* fn, size_t bytes) {
+            if (e == cudaSuccess)
+                e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+            if (e == cudaSuccess)
+                e = cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                         (int)cudaSharedmemCarveoutMaxShared);
+        };
+        if (TP.P.V == 4) {
+            set((const void*)k_tile_dt<M, 4>, smem_dt<M, 4>(TP));
+            set((const void*)k_tile_gradlim<M, 4>, smem_gradlim<M, 4>(TP));
+            set((const void*)k_tile_stage<M, 4, true, 1>, smem_stage<M, 4, true>(TP));
+            set((const void*)k_tile_stage<M, 4, false, 1>, smem_stage<M, 4, false>(TP));
+            set((const void*)k_tile_stage<M, 4, true, 2>, smem_stage<M, 4, true>(TP));
+            set((const void*)k_tile_stage<M, 4, false, 2>, smem_stage<M, 4, false>(TP));
+        } else {
+            set((const void*)k_tile_dt<M, 2>, smem_dt<M, 2>(TP));
+            set((const void*)k_tile_gradlim<M, 2>, smem_gradlim<M, 2>(TP));
+            set((const void*)k_tile_stage<M, 2, true, 3>, smem_stage<M, 2, true>(TP));
+            set((const void*)k_tile_stage<M, 2, false, 3>, smem_stage<M, 2, false>(TP));
+        }
+        return e;
+    }
+    static int grid(const TileParams& TP) { return (TP.P.n_real + TP.T - 1) / TP.T; }
+    static void dt(const TileParams& TP, const TileIO& io, cudaStream_t st) {
+        if (TP.P.V == 4) k_tile_dt<M, 4><<<grid(TP), TP.T, smem_dt<M, 4>(TP), st>>>(TP, io);
+        else k_tile_dt<M, 2><<<grid(TP), TP.T, smem_dt<M, 2>(TP), st>>>(TP, io);
+    }
+    static void gradlim(const TileParams& TP, const TileIO& io, cudaStream_t st) {
+        if (TP.P.V == 4) k_tile_gradlim<M, 4><<<grid(TP), TP.T, smem_gradlim<M, 4>(TP), st>>>(TP, io);
+        else k_tile_gradlim<M, 2><<<grid(TP), TP.T, smem_gradlim<M, 2>(TP), st>>>(TP, io);
+    }
+    static void stage(const TileParams& TP, const TileIO& io, cudaStream_t st) {
+        const int g = grid(TP);
+        const bool o2 = TP.P.order2 != 0;
+        if (TP.P.flux == 3) {
+            if (o2) k_tile_stage<M, 2, true, 3><<<g, TP.T, smem_stage<M, 2, true>(TP), st>>>(TP, io);
+            else k_tile_stage<M, 2, false, 3><<<g, TP.T, smem_stage<M, 2, false>(TP), st>>>(TP, io);
+        } else if (TP.P.flux == 1) {
+            if (o2) k_tile_stage<M, 4, true, 1><<<g, TP.T, smem_stage<M, 4, true>(TP), st>>>(TP, io);
+            else k_tile_stage<M, 4, false, 1><<<g, TP.T, smem_stage<M, 4, false>(TP), st>>>(TP, io);
+        } else {
+            if (o2) k_tile_stage<M, 4, true, 2><<<g, TP.T, smem_stage<M, 4, true>(TP), st>>>(TP, io);
+            else k_tile_stage<M, 4, false, 2><<<g, TP.T, smem_stage<M, 4, false>(TP), st>>>(TP, io);
+        }
+    }
+};
+
+// Entry points per precision mode (defined in fv_tile_exact.cu / fv_tile_fast.cu).
+namespace tile {
+cudaError_t prepare(int precision, const TileParams& TP);
+void launch_dt(int precision, const TileParams& TP, const TileIO& io, cudaStream_t st);
+void launch_gradlim(int precision, const TileParams& TP, const TileIO& io, cudaStream_t st);
+void launch_stage(int precision, const TileParams& TP, const TileIO& io, cudaStream_t st);
+}  // namespace tile
+
+}  // namespace fvgpu

@@ -1,0 +1,33 @@
+// Tile kernels with the FP64 and FP32-bulk fast policies, and the
+// per-precision dispatch.
+#include "fv_tile.cuh"
+
+namespace fvgpu {
+namespace tile {
+cudaError_t prepare_exact(const TileParams& TP);
+void launch_dt_exact(const TileParams& TP, const TileIO& io, cudaStream_t st);
+void launch_gradlim_exact(const TileParams& TP, const TileIO& io, cudaStream_t st);
+void launch_stage_exact(const TileParams& TP, const TileIO& io, cudaStream_t st);
+
+cudaError_t prepare(int precision, const TileParams& TP) {
+    if (precision == 0) return prepare_exact(TP);
+    if (precision == 1) return TileLaunch<MF64>::prepare(TP);
+    return TileLaunch<MF32>::prepare(TP);
+}
+void launch_dt(int precision, const TileParams& TP, const TileIO& io, cudaStream_t st) {
+    if (precision == 0) launch_dt_exact(TP, io, st);
+    else if (precision == 1) TileLaunch<MF64>::dt(TP, io, st);
+    else TileLaunch<MF32>::dt(TP, io, st);
+}
+void launch_gradlim(int precision, const TileParams& TP, const TileIO& io, cudaStream_t st) {
+    if (precision == 0) launch_gradlim_exact(TP, io, st);
+    else if (precision == 1) TileLaunch<MF64>::gradlim(TP, io, st);
+    else TileLaunch<MF32>::gradlim(TP, io, st);
+}
+void launch_stage(int precision, const TileParams& TP, const TileIO& io, cudaStream_t st) {
+    if (precision == 0) launch_stage_exact(TP, io, st);
+    else if (precision == 1) TileLaunch<MF64>::stage(TP, io, st);
+    else TileLaunch<MF32>::stage(TP, io, st);
+}
+}  // namespace tile
+}  // namespace fvgpu

@@ -39,7 +39,7 @@ class _Physics(C.Structure):
     _fields_ = [("V", C.c_int32), ("flux", C.c_int32), ("order2", C.c_int32), ("limiter", C.c_int32),
                 ("dt_kind", C.c_int32), ("global_dt", C.c_int32), ("gamma", C.c_double), ("K", C.c_double),
                 ("cfl", C.c_double), ("dt_const", C.c_double), ("n_groups", C.c_int32),
-                ("group_bc", _i32p), ("group_bv", _dp)]
+                ("group_bc", _i32p), ("group_bv", _dp), ("positivity_guard", C.c_int32)]
 
 
 _PRINT_CB = C.CFUNCTYPE(None, C.c_void_p, C.c_uint64, C.c_double, _dp, C.c_int32)
@@ -148,6 +148,7 @@ def physics_struct(ph: _phys.Physics, group_names: Sequence[str]):
                  dt_kind=DT[ph.dt_kind], global_dt=int(ph.global_dt), gamma=ph.gamma, K=ph.K, cfl=ph.cfl,
                  dt_const=ph.dt_const, n_groups=len(group_names))
     s.group_bc = _p(gbc, _i32p); s.group_bv = _p(gbv)
+    s.positivity_guard = int(getattr(ph, "positivity_guard", False))
     s._keep = (gbc, gbv)
     return s
 
@@ -268,3 +269,10 @@ class Solver:
         arrs = [np.ascontiguousarray(a, np.float64) for a in (gx, gy, lim)]
         _check(lib().fv_stage_bounds(self._h, _p(q), *[_p(a) for a in arrs]))
         return q
+
+
+def solver_info(s: Solver):
+    out = np.zeros(6, np.int64)
+    _check(lib().fv_solver_info(s._h, _p(out, _i64p)))
+    return dict(tiles=int(out[0]), tile_cells=int(out[1]), max_halo=int(out[2]), max_edges=int(out[3]),
+                precision=int(out[4]), stage_bytes=int(out[5]))

@@ -41,6 +41,9 @@ class Physics:
     dt_const: float = 0.0
     global_dt: bool = True
     bcs: Dict[str, Tuple[str, Optional[Sequence[float]]]] = dataclasses.field(default_factory=dict)
+    # not in the reference: fall back to the cell value on MUSCL face states
+    # with rho <= 0 or p <= 0 (off = the reference's scheme, bit for bit)
+    positivity_guard: bool = False
 
 
 def euler_state(rho, u, v, p, gamma=1.4):

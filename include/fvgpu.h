@@ -72,6 +72,9 @@ typedef struct {
     int32_t n_groups;          /* boundary groups (physical names) */
     const int32_t* group_bc;   /* [n_groups] FV_BC_* per group */
     const double* group_bv;    /* [n_groups*4] far-field/inflow state for INLET_OUTLET/FARFIELD */
+    int32_t positivity_guard;  /* not in the reference (0 = the reference's scheme): a MUSCL
+                                  face state with rho <= 0 or p <= 0 falls back to the
+                                  cell value */
 } fv_physics;
 
 typedef struct {
@@ -158,6 +161,9 @@ int fv_check_state(fv_solver* s);
 int fv_boundary_force(fv_solver* s, int32_t group, double* fx, double* fy);
 /* Chunk length of the captured step graphs (default 16). */
 int fv_solver_set_chunk(fv_solver* s, int32_t steps);
+/* out[6] = {tiles, cells per tile, max halo cells per tile, max edges per
+ * tile, precision, bytes per stored stage value}. */
+int fv_solver_info(fv_solver* s, int64_t* out);
 /* Device time of the last fv_run's chunks and per-kernel launch count. */
 int fv_last_run_stats(fv_solver* s, double* device_ms, int64_t* kernel_launches);
 
@@ -171,10 +177,14 @@ int fv_profile_kernels(fv_solver* s, const double* alpha, int32_t n_alpha, int32
 /* ---- stage-level entry points (host arrays, reference numbering) -------- */
 /* dt per cell [n_total]; global_min applies min_dt (explicit.cpp:555-564). */
 int fv_stage_dt(fv_solver* s, const double* q, double* dt, int32_t global_min);
-/* gx, gy, lim [n_total*V] from the fused gradient + limiter kernel. */
+/* gx, gy, lim [n_total*V] from the fused gradient + limiter kernel.
+ * FP64_EXACT: the reference's gx, gy and limiters.  FP64 / FP32: these modes
+ * keep the limiter multiplied into the gradients, so gx, gy receive gx*lim,
+ * gy*lim and lim is filled with 1. */
 int fv_stage_gradients_limiters(fv_solver* s, const double* q, double* gx, double* gy,
                                 double* lim);
-/* One RK stage from the fused flux + update + ghost-fill kernel:
+/* One RK stage from the fused flux + update + ghost-fill kernel (FP64 / FP32:
+ * gx, gy are the limited gradients and lim is ignored):
  * q_out = q_base + qt(q_stage) * dt * alpha on real cells, then the ghost
  * fill from q_out with the given gx, gy, lim (explicit.cpp:742-745).
  * dt [n_total].  q_out [n_total*V]. */

@@ -425,6 +425,16 @@ void fvo_calc_limiters(const fvo_mesh* m, const fvo_physics* ph, const double* q
     free(qmin); free(qmax);
 }
 
+/* Optional positivity guard (an extension, not in the reference): a
+ * reconstructed Euler face state with non-positive density or pressure is
+ * replaced by the cell value. */
+static void guard_face(const fvo_physics* ph, double* qf, const double* qc) {
+    if (!ph->positivity_guard || ph->V != 4) return;
+    const double p = (ph->gamma - 1) * (qf[3] - 0.5 / qf[0] * (qf[1] * qf[1] + qf[2] * qf[2]));
+    if (!(qf[0] > 0.) || !(p > 0.))
+        for (int k = 0; k < 4; ++k) qf[k] = qc[k];
+}
+
 /* Edge flux loop, explicit.cpp:261-364 (no viscous face gradient). */
 void fvo_calc_time_derivatives(const fvo_mesh* m, const fvo_physics* ph, const double* q,
                                const double* gx, const double* gy, const double* lim, double* qt) {
@@ -444,6 +454,8 @@ void fvo_calc_time_derivatives(const fvo_mesh* m, const fvo_physics* ph, const d
                 qi[k] = q[ki] + (gx[ki] * di0 + gy[ki] * di1) * lim[ki];
                 qj[k] = q[kj] + (gx[kj] * dj0 + gy[kj] * dj1) * lim[kj];
             }
+            guard_face(ph, qi, q + (size_t)V * i);
+            guard_face(ph, qj, q + (size_t)V * j);
         } else {
             for (int k = 0; k < V; ++k) { qi[k] = q[(size_t)V * i + k]; qj[k] = q[(size_t)V * j + k]; }
         }
@@ -472,6 +484,7 @@ void fvo_update_bounds(const fvo_mesh* m, const fvo_physics* ph, double* q, cons
                 size_t kk = (size_t)V * ii + k;
                 qint[k] = q[kk] + (gx[kk] * d0 + gy[kk] * d1) * lim[kk];
             }
+            guard_face(ph, qint, q + (size_t)V * ii);
         } else {
             for (int k = 0; k < V; ++k) qint[k] = q[(size_t)V * ii + k];
         }

@@ -48,6 +48,8 @@ typedef struct {
     int n_groups;
     const int32_t* group_bc;  /* [n_groups] */
     const double* group_bv;   /* [n_groups][4] far-field / inflow state */
+    int positivity_guard;     /* 1: a MUSCL face state with rho <= 0 or p <= 0 falls back
+                                 to the cell value (not in the reference; 0 = reference) */
 } fvo_physics;
 
 int fvo_mesh_build(int64_t n_nodes, const double* nodes_x, const double* nodes_y,

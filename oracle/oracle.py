@@ -47,7 +47,7 @@ class _FvoPhysics(C.Structure):
     _fields_ = [("V", C.c_int), ("flux", C.c_int), ("gamma", C.c_double), ("order2", C.c_int),
                 ("limiter", C.c_int), ("K", C.c_double), ("dt_kind", C.c_int),
                 ("cfl", C.c_double), ("dt_const", C.c_double), ("global_dt", C.c_int),
-                ("n_groups", C.c_int), ("group_bc", _i32p), ("group_bv", _dp)]
+                ("n_groups", C.c_int), ("group_bc", _i32p), ("group_bv", _dp), ("positivity_guard", C.c_int)]
 
 
 def build_oracle():
@@ -129,6 +129,7 @@ class Oracle:
                         for n in group_names], np.float64).reshape(-1)
         p.n_groups = len(group_names)
         p.group_bc = _ptr(gbc, _i32p); p.group_bv = _ptr(gbv)
+        p.positivity_guard = int(getattr(phys, "positivity_guard", False))
         p._keep = (gbc, gbv)
         return p
 

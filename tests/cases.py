@@ -21,6 +21,11 @@ def random_euler_state(n, seed, rho=(0.5, 1.5), vel=0.5, p=(0.5, 1.5)):
                          r.uniform(*p, n)).ravel()
 
 
+def _guarded(ph):
+    ph.positivity_guard = True
+    return ph
+
+
 CASES = {
     # name: (mesh builder, physics, ic(geom)->q, alpha, steps, ref variant, ref bc aliases, ref consts)
     "sod": dict(mesh=lambda: meshgen.sod_strip(40, 4), phys=lambda: P.sod(),
@@ -39,6 +44,10 @@ CASES = {
                           ic=lambda g: P.ic_forward_step(g.n_total).ravel(), alpha=P.RK5_ALPHA, steps=30,
                           ref="forwardStep_o2venk5", alias={"step": ("forwardStep_o2venk5", "wall")},
                           consts=dict(cfl=0.8)),
+    "step_o2_guard": dict(mesh=lambda: meshgen.forward_step(n=20),
+                          phys=lambda: _guarded(P.forward_step(order2=True, limiter="venkat", K=5.0)),
+                          ic=lambda g: P.ic_forward_step(g.n_total).ravel(), alpha=P.RK5_ALPHA, steps=30,
+                          ref=None, alias={}, consts=dict(cfl=0.8)),
     "step_o2_mich": dict(mesh=lambda: meshgen.forward_step(n=20),
                          phys=lambda: P.forward_step(order2=True, limiter="michalak", K=7.5),
                          ic=lambda g: P.ic_forward_step(g.n_total).ravel(), alpha=P.RK5_ALPHA, steps=30,

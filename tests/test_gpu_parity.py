@@ -167,3 +167,119 @@ def test_unsupported_physics_rejected():
     with pytest.raises(fvgpu.FvError) as e:
         fvgpu.Solver(mesh, bad)
     assert e.value.code == -4
+
+
+# ---------------------------------------------------------------- FP64 / FP32
+def normwise_rel(a, b, V):
+    """max over variables k of max|a_k - b_k| / s_k on AoS [n][V] arrays, with
+    s_k = max(max|b_k|, 1e-3 * max|b|) so that a variable that is zero up to
+    rounding (rho*v in a 1-D problem) is measured against the state's scale.
+    Entries that are NaN in both count as equal, NaN in one only as inf."""
+    a = a.reshape(-1, V).copy(); b = b.reshape(-1, V).copy()
+    na, nb = np.isnan(a), np.isnan(b)
+    if np.any(na != nb):
+        return float("inf")
+    a[na] = 0.0; b[nb] = 0.0
+    scale = np.maximum(np.abs(b).max(axis=0), 1e-3 * np.abs(b).max())
+    scale = np.maximum(scale, 1e-300)
+    return float((np.abs(a - b).max(axis=0) / scale).max())
+
+
+FP64_STEP_RTOL = 1e-12     # plain FP64 path: max relative error per step
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_fp64_stage_functions(name, oracle):
+    case, em, ph, s, g, p = setup(name, oracle, "fp64")
+    q = rand_state(g, ph, 21)
+    e_dt = normwise_rel(s.stage_dt(q, False), oracle.calc_dt(g, p, q, False), 1)
+    assert e_dt < FP64_STEP_RTOL, e_dt
+    if ph.order2:
+        # FP64 keeps the limiter multiplied into the gradients
+        gx, gy, lim = s.stage_gradients_limiters(q)
+        ogx, ogy = oracle.gradients(g, p, q)
+        olim = oracle.limiters(g, p, q, ogx, ogy)
+        e = (normwise_rel(gx, ogx * olim, ph.V), normwise_rel(gy, ogy * olim, ph.V))
+        assert max(e) < 1e-9, e
+        assert np.all(lim == 1.0)
+    else:
+        ogx = np.zeros_like(q); ogy = np.zeros_like(q); olim = np.zeros_like(q)
+    dt = oracle.calc_dt(g, p, q, ph.global_dt)
+    qb = rand_state(g, ph, 22)
+    qt = oracle.time_derivatives(g, p, q, ogx, ogy, olim)
+    want = oracle.update_bounds(g, p, qb + qt * np.repeat(dt, ph.V) * 0.506, ogx, ogy, olim)
+    got = s.stage_update(qb, q, ogx * olim, ogy * olim, olim, dt, 0.506)
+    e = normwise_rel(got, want, ph.V)
+    assert e < FP64_STEP_RTOL, e
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_fp64_per_step_error(name, oracle):
+    """Each time step from the oracle's state: normwise relative error of the
+    state after one step <= 1e-12; over the whole run the error stays small."""
+    case, em, ph, s, g, p = setup(name, oracle, "fp64")
+    q = case["ic"](g)
+    worst = 0.0
+    for k in range(6):
+        want = oracle.run_loop(g, p, q, case["alpha"], 1)
+        s.set_state(q)
+        s.run(1, alpha=case["alpha"])
+        got = s.get_state()
+        worst = max(worst, normwise_rel(got[: g.n_real * ph.V], want["q"][: g.n_real * ph.V], ph.V))
+        q = want["q"]
+    assert worst < FP64_STEP_RTOL
+    q0 = case["ic"](g)
+    want = oracle.run_loop(g, p, q0, case["alpha"], case["steps"])
+    s.set_state(q0)
+    s.run(case["steps"], alpha=case["alpha"])
+    assert normwise_rel(s.get_state()[: g.n_real * ph.V], want["q"][: g.n_real * ph.V], ph.V) < 1e-9
+
+
+def l2_rel(a, b):
+    return float(np.sqrt(np.sum((a - b) ** 2) / np.sum(b ** 2)))
+
+
+def rho_p(q, gamma=1.4):
+    q = q.reshape(-1, 4)
+    return q[:, 0], (gamma - 1) * (q[:, 3] - 0.5 * (q[:, 1] ** 2 + q[:, 2] ** 2) / q[:, 0])
+
+
+FP32_L2_TOL = 1e-4         # FP32-bulk path: relative L2 error of density and pressure
+
+
+@pytest.mark.parametrize("name", ["sod", "step_o1", "step_o2_venk5", "step_o2_mich", "naca"])
+def test_fp32_l2_error(name, oracle):
+    case, em, ph, s, g, p = setup(name, oracle, "fp32")
+    q0 = case["ic"](g)
+    want = oracle.run_loop(g, p, q0, case["alpha"], case["steps"])
+    s.set_state(q0)
+    got = s.run(case["steps"], alpha=case["alpha"])
+    assert got["step"] == case["steps"]
+    q = s.get_state()
+    n = g.n_real * 4
+    r1, p1 = rho_p(q[:n]); r0, p0 = rho_p(want["q"][:n])
+    assert l2_rel(r1, r0) < FP32_L2_TOL and l2_rel(p1, p0) < FP32_L2_TOL
+    assert s.check_state() == 0
+
+
+def test_fp32_burgers(oracle):
+    case, em, ph, s, g, p = setup("burgers", oracle, "fp32")
+    q0 = case["ic"](g)
+    want = oracle.run_loop(g, p, q0, case["alpha"], case["steps"])
+    s.set_state(q0)
+    s.run(case["steps"], alpha=case["alpha"])
+    n = g.n_real * 2
+    assert l2_rel(s.get_state()[:n], want["q"][:n]) < FP32_L2_TOL
+
+
+@pytest.mark.parametrize("precision", ["fp64_exact", "fp64", "fp32"])
+def test_runs_are_bitwise_reproducible(precision, oracle):
+    """No atomics in any accumulation: two runs give identical bits."""
+    case, em, ph, s, g, p = setup("step_o2_venk5", oracle, precision)
+    q0 = case["ic"](g)
+    out = []
+    for _ in range(2):
+        s.set_state(q0)
+        r = s.run(20, alpha=case["alpha"])
+        out.append((s.get_state(), r["R"]))
+    assert out[0][0].tobytes() == out[1][0].tobytes() and out[0][1].tobytes() == out[1][1].tobytes()

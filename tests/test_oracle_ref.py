@@ -27,7 +27,10 @@ def _setup(name, oracle):
     return case, em, ref, g, ph, p
 
 
-@pytest.mark.parametrize("name", sorted(CASES))
+REF_CASES = sorted(n for n in CASES if CASES[n]["ref"] is not None)
+
+
+@pytest.mark.parametrize("name", REF_CASES)
 def test_geometry_bitwise(name, oracle):
     case, em, ref, g, ph, p = _setup(name, oracle)
     gr = ref.geometry()
@@ -36,7 +39,7 @@ def test_geometry_bitwise(name, oracle):
         assert bits_equal(getattr(g, k), getattr(gr, k)), k
 
 
-@pytest.mark.parametrize("name", sorted(CASES))
+@pytest.mark.parametrize("name", REF_CASES)
 def test_stage_functions_bitwise(name, oracle):
     case, em, ref, g, ph, p = _setup(name, oracle)
     if ph.V == 4:
@@ -58,7 +61,7 @@ def test_stage_functions_bitwise(name, oracle):
     assert bits_equal(oracle.update_bounds(g, p, q, gx, gy, lim), ref.update_bounds(q, gx, gy, lim))
 
 
-@pytest.mark.parametrize("name", sorted(CASES))
+@pytest.mark.parametrize("name", REF_CASES)
 def test_time_loop_bitwise(name, oracle):
     case, em, ref, g, ph, p = _setup(name, oracle)
     q0 = case["ic"](g)
@@ -123,3 +126,15 @@ def test_missing_boundary_edge_rejected(oracle):
     em.bnd_nodes[0] = (0, em.nodes_x.size - 1)  # not an edge of the mesh
     with pytest.raises(ValueError):
         oracle.build_mesh(em)
+
+
+def test_positivity_guard_is_inert_on_physical_states(oracle):
+    """The optional guard (not in the reference) changes nothing while every
+    MUSCL face state stays physical: the guarded oracle equals the reference."""
+    case, em, ref, g, ph, p = _setup("step_o2_venk5", oracle)
+    ph.positivity_guard = True
+    pg = oracle.physics(ph, em.group_names)
+    q0 = case["ic"](g)
+    a = oracle.run_loop(g, pg, q0, case["alpha"], case["steps"])
+    b = ref.run_loop(q0, case["alpha"], case["steps"])
+    assert bits_equal(a["q"], b["q"])
