@@ -4,6 +4,7 @@
 #include <cstdio>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -746,6 +747,74 @@ int fv_stage_dt(fv_solver* s, const double* q, double* dt, int32_t global_min) {
         for (auto& v : dd) v = mn;
     }
     std::memcpy(dt, dd.data(), dd.size() * 8);
+    return FV_OK;
+}
+
+// ------------------------------------------ time step without allocation --
+// fv_stage_dt_noalloc: the time-step kernel for callers that must not
+// allocate device memory.  Its working arrays live in one statically sized
+// device array (every GPU that loads this library holds it until exit).
+namespace {
+constexpr size_t kNoAllocBytes = size_t(8) << 20;  // 8 MiB of scratch per device
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+std::mutex g_noalloc_mu;
+void* g_noalloc_base[128] = {};  // device address of g_noalloc_scratch, per device ordinal
+
+size_t align256(size_t n) { return (n + 255) & ~size_t(255); }
+
+// global minimum of the slot keys (min_dt, explicit.cpp:555-564; a NaN in
+// dt[0] wins) written to every entry of the caller's output
+__global__ void k_noalloc_dt_fill(const unsigned long long* keys, const double* dt_dev, int cell0, double* out, int n) {
+    unsigned long long key = ~0ull;
+    for (int i = 0; i < kDtSlots; ++i) key = keys[i] < key ? keys[i] : key;
+    const double d0 = dt_dev[cell0];
+    const double mn = (d0 != d0) ? d0 : tkey_inv(key);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) out[i] = mn;
+}
+}  // namespace
+
+int fv_stage_dt_noalloc(fv_solver* s, const double* q_device, double* dt_device, int32_t global_min, void* stream) {
+    if (!s || !q_device || !dt_device) return fail(FV_ERR_ARG, "fv_stage_dt_noalloc: null argument");
+    const size_t nt = (size_t)s->n_total, V = (size_t)s->V;
+    const size_t need = align256(kDtSlots * 8) + align256(nt * 8) + align256(nt * V * 8) +
+                        (s->f32 ? align256(nt * V * 4) : 0);
+    if (need > kNoAllocBytes)
+        return fail(FV_ERR_ARG, "fv_stage_dt_noalloc: mesh needs " + std::to_string(need) +
+                                    " bytes of scratch, more than the fixed " + std::to_string(kNoAllocBytes) +
+                                    " (about 200k cells in FP64, 150k in FP32); use fv_stage_dt");
+    CK(cudaSetDevice(s->device));
+    if (s->device < 0 || s->device >= 128) return fail(FV_ERR_ARG, "fv_stage_dt_noalloc: device ordinal out of range");
+    unsigned char* base = nullptr;
+    {
+        // one-time set-up per device: the host-side symbol is only a stand-in,
+        // the kernels need the scratch array's device address
+        std::lock_guard<std::mutex> lock(g_noalloc_mu);
+        if (!g_noalloc_base[s->device]) {
+            void* p = nullptr;
+            CK(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+            g_noalloc_base[s->device] = p;
+        }
+        base = (unsigned char*)g_noalloc_base[s->device];
+    }
+    cudaStream_t st = stream ? (cudaStream_t)stream : s->stream;
+    unsigned long long* keys = (unsigned long long*)base;
+    double* dt_dev = (double*)(base + align256(kDtSlots * 8));
+    double* q64 = (double*)((unsigned char*)dt_dev + align256(nt * 8));
+    void* qs = s->f32 ? (void*)((unsigned char*)q64 + align256(nt * V * 8)) : (void*)q64;
+    // the slots keep the previous call's minimum: they must start at +inf
+    CK(cudaMemsetAsync(keys, 0xFF, kDtSlots * 8, st));
+    launch_permute_to_device(q_device, q64, s->new2ref, (int)nt, (int)V, st);
+    if (s->f32) launch_to_float(q64, (float*)qs, nt * V, st);
+    TileParams TP = s->TP;
+    TP.P.global_dt = global_min ? 1 : 0;
+    TileIO io{};
+    io.q_stage = qs;
+    io.dt = dt_dev;
+    io.dtkeys = keys;
+    tile::launch_dt(s->precision, TP, io, st);
+    if (global_min) k_noalloc_dt_fill<<<grid_for((int)nt), kBlock, 0, st>>>(keys, dt_dev, TP.P.cell0, dt_device, (int)nt);
+    else launch_permute_to_ref(dt_dev, dt_device, s->new2ref, (int)nt, 1, st);
+    CK(cudaGetLastError());
     return FV_OK;
 }
 

@@ -191,6 +191,22 @@ int fv_stage_gradients_limiters(fv_solver* s, const double* q, double* gx, doubl
 int fv_stage_update(fv_solver* s, const double* q_base, const double* q_stage,
                     const double* gx, const double* gy, const double* lim, const double* dt,
                     double alpha, double* q_out);
+/* fv_stage_dt without any device allocation.  No counterpart in the
+ * reference: it exists for callers that cannot call cudaMalloc -- code that
+ * embeds this solver in a loop whose GPU memory is fully reserved up front
+ * by the host application's own pool, or that must not pay the implicit
+ * device synchronisation of an allocation between its queued kernels.
+ * q_device: [n_total][V] state, dt_device: [n_total] output, both device
+ * memory in reference numbering.  Work is queued on `stream` (NULL = the
+ * solver's stream) and is complete when that stream is; nothing is copied
+ * to the host.  Its working arrays are one fixed 8 MiB device array per GPU
+ * (held until the process exits), so meshes needing more (about 200k cells
+ * in FP64, 150k in FP32) are rejected with FV_ERR_ARG.  The first call on a
+ * device looks up that array's device address; make it before any stream
+ * capture.  All calls share the array: calls that overlap on the GPU (two
+ * streams, two threads) race and must be serialised by the caller. */
+int fv_stage_dt_noalloc(fv_solver* s, const double* q_device, double* dt_device, int32_t global_min,
+                        void* stream);
 /* Ghost fill alone (explicit.cpp:380-417) on q (in place). */
 int fv_stage_bounds(fv_solver* s, double* q, const double* gx, const double* gy,
                     const double* lim);
