@@ -210,6 +210,7 @@ def main():
     ap.add_argument("--workload", default="step", choices=["step", "sod", "naca"])
     ap.add_argument("--precision", default="fp64_exact", choices=["fp64_exact", "fp64", "fp32"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--tile-cells", type=int, default=0, help="cells per tile (0: library default)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
@@ -231,7 +232,7 @@ def main():
     em, ph, alpha, ic, desc = build_workload(args.workload)
     mesh = fvgpu.Mesh.from_elements(em)
     geo = mesh.geometry()
-    s = fvgpu.Solver(mesh, ph, args.precision, device=local)
+    s = fvgpu.Solver(mesh, ph, args.precision, device=local, tile_cells=args.tile_cells)
     stream = torch.cuda.Stream(device=local)
     s.set_stream(stream.cuda_stream)
     q0 = ic(geo["ccx"], mesh.n_total).ravel()

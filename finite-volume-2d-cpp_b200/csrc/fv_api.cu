@@ -245,6 +245,11 @@ static int validate_physics(const fv_physics* ph, int n_groups_mesh) {
 }
 
 int fv_solver_create(const fv_mesh* fm, const fv_physics* ph, int32_t precision, int32_t device, fv_solver** out) {
+    return fv_solver_create_ex(fm, ph, precision, device, nullptr, out);
+}
+
+int fv_solver_create_ex(const fv_mesh* fm, const fv_physics* ph, int32_t precision, int32_t device,
+                        const fv_solver_options* opt, fv_solver** out) {
     if (!fm || !out) return fail(FV_ERR_ARG, "fv_solver_create: null");
     const HostMesh& m = fm->m;
     int rc = validate_physics(ph, (int)m.group_names.size());
@@ -266,8 +271,11 @@ int fv_solver_create(const fv_mesh* fm, const fv_physics* ph, int32_t precision,
     FaceArrays fa;
     build_face_arrays(m, fa);
     TileArrays ta;
-    build_tiles(m, fa, kBlock, ta);
-    if (ta.max_halo + kBlock > 65535 || ta.max_edges > kFaceEdgeMask)
+    const int tile_cells = (opt && opt->tile_cells) ? opt->tile_cells : 256;
+    if (tile_cells != 64 && tile_cells != 128 && tile_cells != 256)
+        return fail(FV_ERR_ARG, "tile_cells must be 64, 128 or 256");
+    build_tiles(m, fa, tile_cells, ta);
+    if (ta.max_halo + tile_cells > 65535 || ta.max_edges > kFaceEdgeMask)
         return fail(FV_ERR_MESH, "tile halo too large for 16-bit local indices");
     s->n_tiles = ta.n_tiles;
     TileParams& TP = s->TP;
@@ -306,8 +314,11 @@ int fv_solver_create(const fv_mesh* fm, const fv_physics* ph, int32_t precision,
     if ((rc = upload_s(s.get(), ta.exf, &TP.exf))) return rc;
     if ((rc = upload_s(s.get(), ta.eyf, &TP.eyf))) return rc;
     if ((rc = upload_s(s.get(), ta.eg, &TP.eg))) return rc;
-    if ((rc = upload_s(s.get(), ta.ccx, &TP.ccx))) return rc;
-    if ((rc = upload_s(s.get(), ta.ccy, &TP.ccy))) return rc;
+    {
+        std::vector<double> cxy(2 * ta.ccx.size());
+        for (size_t i = 0; i < ta.ccx.size(); ++i) { cxy[2 * i] = ta.ccx[i]; cxy[2 * i + 1] = ta.ccy[i]; }
+        if ((rc = upload_s(s.get(), cxy, &TP.ccxy))) return rc;
+    }
     if ((rc = upload_s(s.get(), fa.area, &TP.area))) return rc;
     const int32_t* n2r;
     if ((rc = upload_v(s.get(), m.new2ref, &n2r))) return rc;

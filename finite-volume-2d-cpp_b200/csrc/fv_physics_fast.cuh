@@ -12,13 +12,22 @@ namespace fast {
 
 template <class T> __device__ __forceinline__ T rcp(T x);
 template <> __device__ __forceinline__ double rcp<double>(double x) { return 1.0 / x; }
-template <> __device__ __forceinline__ float rcp<float>(float x) { return __frcp_rn(x); }
+// FP32: single MUFU approximations (<= 1 ulp rcp, <= 2 ulp sqrt; ftz)
+template <> __device__ __forceinline__ float rcp<float>(float x) {
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
 template <class T> __device__ __forceinline__ T sqrt_(T x);
 template <> __device__ __forceinline__ double sqrt_<double>(double x) { return sqrt(x); }
-template <> __device__ __forceinline__ float sqrt_<float>(float x) { return __fsqrt_rn(x); }
+template <> __device__ __forceinline__ float sqrt_<float>(float x) {
+    float r;
+    asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
 template <class T> __device__ __forceinline__ T div_(T a, T b);
 template <> __device__ __forceinline__ double div_<double>(double a, double b) { return a / b; }
-template <> __device__ __forceinline__ float div_<float>(float a, float b) { return __fdiv_rn(a, b); }
+template <> __device__ __forceinline__ float div_<float>(float a, float b) { return a * rcp<float>(b); }
 template <class T> __device__ __forceinline__ T tmin(T a, T b) { return (b < a) ? b : a; }
 template <class T> __device__ __forceinline__ T tmax(T a, T b) { return (a < b) ? b : a; }
 

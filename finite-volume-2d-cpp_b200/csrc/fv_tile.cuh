@@ -51,8 +51,7 @@ struct TileParams {
     const void* eyf;
     const void* eg;
     const uint16_t* face;      // [4][n_real] face words
-    const void* ccx;           // S [n_total] centroids
-    const void* ccy;
+    const void* ccxy;          // S [n_total][2] centroids
     const void* area;          // S [n_total]
 };
 
@@ -137,7 +136,10 @@ struct Rec {
     static constexpr int OC = V * (1 + NG);
     static constexpr int RAW = OC + (CENTROID ? 2 : 0);
     static constexpr int AL = 16 / (int)sizeof(S);
-    static constexpr int NR = (RAW + AL - 1) / AL * AL;
+    // an odd number of 16-byte units, so that 128-bit reads of records of
+    // random cells spread over all eight shared-memory bank groups
+    static constexpr int U = (RAW + AL - 1) / AL;
+    static constexpr int NR = ((U % 2) ? U : U + 1) * AL;
 };
 
 // Optional positivity guard (not in the reference): a reconstructed Euler
@@ -152,45 +154,67 @@ __device__ __forceinline__ void guard_face(const Params& P, S* qf, const S* qc) 
     }
 }
 
-// Loads the records of the tile's owned cells and halo.
+// Asynchronous global -> shared copies (no register round trip); a thread
+// issues all of its copies and waits once, so a whole tile is in flight.
+__device__ __forceinline__ void cpa16(void* dst, const void* src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src)
+                 : "memory");
+}
+__device__ __forceinline__ void cpa8(void* dst, const void* src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src)
+                 : "memory");
+}
+__device__ __forceinline__ void cpa4(void* dst, const void* src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src)
+                 : "memory");
+}
+__device__ __forceinline__ void cpa_wait() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+template <int BYTES>
+__device__ __forceinline__ void cpa(void* dst, const void* src) {
+    if (BYTES == 32) { cpa16(dst, src); cpa16((char*)dst + 16, (const char*)src + 16); }
+    else if (BYTES == 16) cpa16(dst, src);
+    else if (BYTES == 8) cpa8(dst, src);
+    else cpa4(dst, src);
+}
+
+// Loads the records of the tile's owned cells and halo (asynchronously).
 template <class M, int V, bool ORDER2, bool CENTROID>
 __device__ __forceinline__ void stage_records(const TileParams& TP, const TileIO& io, const int4& inf, int c0,
                                               int nown, typename M::S* rec) {
     using S = typename M::S;
     using R = Rec<M, V, ORDER2, CENTROID>;
+    constexpr int QB = V * (int)sizeof(S);
     const S* Q = (const S*)io.q_stage;
-    const S* CX = (const S*)TP.ccx;
-    const S* CY = (const S*)TP.ccy;
+    const S* CXY = (const S*)TP.ccxy;
     for (int l = threadIdx.x; l < nown + inf.w; l += blockDim.x) {
         int slot, g;
         if (l < nown) { slot = l; g = c0 + l; }
         else { slot = TP.T + (l - nown); g = TP.halo[inf.z + (l - nown)]; }
         S* r = rec + (size_t)slot * R::NR;
-        S v[V];
-        ld<S, V>(Q, g, v); st<S, V>(r, 0, v);
+        cpa<QB>(r, Q + (size_t)V * g);
         if (ORDER2) {
-            ld<S, V>((const S*)io.gx, g, v); st<S, V>(r + R::OGX, 0, v);
-            ld<S, V>((const S*)io.gy, g, v); st<S, V>(r + R::OGY, 0, v);
-            if (M::exact) { ld<S, V>((const S*)io.lim, g, v); st<S, V>(r + R::OLM, 0, v); }
+            cpa<QB>(r + R::OGX, (const S*)io.gx + (size_t)V * g);
+            cpa<QB>(r + R::OGY, (const S*)io.gy + (size_t)V * g);
+            if (M::exact) cpa<QB>(r + R::OLM, (const S*)io.lim + (size_t)V * g);
         }
-        if (CENTROID) { r[R::OC] = CX[g]; r[R::OC + 1] = CY[g]; }
+        if (CENTROID) cpa<2 * (int)sizeof(S)>(r + R::OC, CXY + 2 * (size_t)g);
     }
 }
 
 // Loads the tile's edge geometry (contiguous per tile) into shared memory.
-template <class S, bool GG>
+template <class S, bool GG, bool XF>
 __device__ __forceinline__ void stage_edges(const TileParams& TP, const int4& inf, uint32_t* sij, S* snx, S* sny,
                                             S* sle, S* sg, S* sxf, S* syf) {
     for (int e = threadIdx.x; e < inf.y; e += blockDim.x) {
         const int ge = inf.x + e;
-        sij[e] = TP.edge_ij[ge];
-        snx[e] = ((const S*)TP.enx)[ge];
-        sny[e] = ((const S*)TP.eny)[ge];
-        sle[e] = ((const S*)TP.ele)[ge];
-        if (GG) {
-            sg[e] = ((const S*)TP.eg)[ge];
-            sxf[e] = ((const S*)TP.exf)[ge];
-            syf[e] = ((const S*)TP.eyf)[ge];
+        cpa4(sij + e, TP.edge_ij + ge);
+        cpa<(int)sizeof(S)>(snx + e, (const S*)TP.enx + ge);
+        cpa<(int)sizeof(S)>(sny + e, (const S*)TP.eny + ge);
+        cpa<(int)sizeof(S)>(sle + e, (const S*)TP.ele + ge);
+        if (GG) cpa<(int)sizeof(S)>(sg + e, (const S*)TP.eg + ge);
+        if (XF) {
+            cpa<(int)sizeof(S)>(sxf + e, (const S*)TP.exf + ge);
+            cpa<(int)sizeof(S)>(syf + e, (const S*)TP.eyf + ge);
         }
     }
 }
@@ -219,16 +243,17 @@ __global__ void __launch_bounds__(kTileMax) k_tile_dt(TileParams TP, TileIO io) 
     S* sle = sny + TP.max_edges;
     uint32_t* sij = reinterpret_cast<uint32_t*>(sle + TP.max_edges);
     __shared__ unsigned long long wmin[kTileMax / 32];
+    const int l = threadIdx.x;
+    uint16_t w[kMaxFaces];
+    if (l < nown) load_faces(TP, c0 + l, w);  // latency overlaps the staging
     stage_records<M, V, false, false>(TP, io, inf, c0, nown, rec);
-    stage_edges<S, false>(TP, inf, sij, snx, sny, sle, nullptr, nullptr, nullptr);
+    stage_edges<S, false, false>(TP, inf, sij, snx, sny, sle, nullptr, nullptr, nullptr);
+    cpa_wait();
     __syncthreads();
     unsigned long long kmin = ~0ull;
-    const int l = threadIdx.x;
     if (l < nown) {
         const int c = c0 + l;
         const S* AR = (const S*)TP.area;
-        uint16_t w[kMaxFaces];
-        load_faces(TP, c, w);
         if (P.dt_kind == 0) {
             io.dt[c] = P.dt_const;
             kmin = tkey(P.dt_const);
@@ -365,15 +390,19 @@ __global__ void __launch_bounds__(kTileMax) k_tile_gradlim(TileParams TP, TileIO
     S* snx = rec + (size_t)LT * R::NR;
     S* sny = snx + EM; S* sle = sny + EM; S* sg = sle + EM; S* sxf = sg + EM; S* syf = sxf + EM;
     uint32_t* sij = reinterpret_cast<uint32_t*>(syf + EM);
-    stage_records<M, V, false, true>(TP, io, inf, c0, nown, rec);
-    stage_edges<S, true>(TP, inf, sij, snx, sny, sle, sg, sxf, syf);
-    __syncthreads();
     const int l = threadIdx.x;
-    if (l >= nown) return;
     const int c = c0 + l;
     uint16_t w[kMaxFaces];
-    load_faces(TP, c, w);
-    const S A = ((const S*)TP.area)[c];
+    S A = S(1);
+    if (l < nown) {  // issued before the staging so that their latency overlaps it
+        load_faces(TP, c, w);
+        A = ((const S*)TP.area)[c];
+    }
+    stage_records<M, V, false, true>(TP, io, inf, c0, nown, rec);
+    stage_edges<S, true, true>(TP, inf, sij, snx, sny, sle, sg, sxf, syf);
+    cpa_wait();
+    __syncthreads();
+    if (l >= nown) return;
     const S* rs = rec + (size_t)l * R::NR;
     S qs[V], gx[V], gy[V], qmn[V], qmx[V], lim[V];
     lds<S, V>(rs, qs);
@@ -502,33 +531,48 @@ __global__ void __launch_bounds__(kTileMax) k_tile_stage(TileParams TP, TileIO i
     const int N = P.n_real, T = TP.T, t = blockIdx.x;
     const int4 inf = TP.info[t];
     const int c0 = t * T, nown = min(T, N - c0);
-    const int LT = T + TP.max_halo;
+    const int LT = T + TP.max_halo, EM = TP.max_edges;
     S* rec = reinterpret_cast<S*>(smem_raw);
     FT* sF = reinterpret_cast<FT*>(rec + (size_t)LT * R::NR);
-    stage_records<M, V, ORDER2, ORDER2>(TP, io, inf, c0, nown, rec);
+    S* snx = reinterpret_cast<S*>(sF + (size_t)EM * V);
+    S* sny = snx + EM; S* sle = sny + EM; S* sxf = sle + EM; S* syf = sxf + EM;
+    uint32_t* sij = reinterpret_cast<uint32_t*>(syf + EM);
     const bool global_dt = io.ctrl != nullptr && P.global_dt;
+    // ---- issue this thread's cell loads first: their latency overlaps the staging
+    const int l = threadIdx.x;
+    const int c = c0 + l;
+    uint16_t w[kMaxFaces];
+    double qb[V];
+    double A = 1.0, dtc = 0.0;
+    if (l < nown) {
+        load_faces(TP, c, w);
+        ld<double, V>(io.q_base, c, qb);
+        A = (double)((const S*)TP.area)[c];
+        if (!global_dt) dtc = io.dt[c];
+    }
+    stage_records<M, V, ORDER2, ORDER2>(TP, io, inf, c0, nown, rec);
+    if (ORDER2) stage_edges<S, false, true>(TP, inf, sij, snx, sny, sle, nullptr, sxf, syf);
+    else stage_edges<S, false, false>(TP, inf, sij, snx, sny, sle, nullptr, nullptr, nullptr);
     if (global_dt && threadIdx.x < 32) {
         unsigned long long k = kmin_(io.dtkeys[threadIdx.x], io.dtkeys[threadIdx.x + 32]);
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) k = kmin_(k, __shfl_xor_sync(0xffffffffu, k, o));
         if (threadIdx.x == 0) s_dtkey = k;
     }
+    cpa_wait();
     __syncthreads();
-    const S* NX = (const S*)TP.enx; const S* NY = (const S*)TP.eny; const S* LE = (const S*)TP.ele;
-    const S* XF = (const S*)TP.exf; const S* YF = (const S*)TP.eyf;
     // ---- one flux per tile edge
     for (int el = threadIdx.x; el < inf.y; el += blockDim.x) {
-        const int e = inf.x + el;
-        const uint32_t ij = TP.edge_ij[e];
+        const uint32_t ij = sij[el];
         const int li = (int)(ij & 0xffff), lj = (int)(ij >> 16);
-        const S n0 = NX[e], n1 = NY[e];
+        const S n0 = snx[el], n1 = sny[el];
         const S* ri = rec + (size_t)li * R::NR;
         const S* rj = rec + (size_t)lj * R::NR;
         S qL[V], qR[V];
         lds<S, V>(ri, qL);
         lds<S, V>(rj, qR);
         if (ORDER2) {
-            const S xf = XF[e], yf = YF[e];
+            const S xf = sxf[el], yf = syf[el];
             const S di0 = xf - ri[R::OC], di1 = yf - ri[R::OC + 1];
             const S dj0 = xf - rj[R::OC], dj1 = yf - rj[R::OC + 1];
             S gxi[V], gyi[V], gxj[V], gyj[V];
@@ -560,24 +604,23 @@ __global__ void __launch_bounds__(kTileMax) k_tile_stage(TileParams TP, TileIO i
             exact::flux<FLUX>(P.gamma, f, qL, qR, n0, n1);
         } else {
             fast::flux<FLUX, S>((S)P.gamma, f, qL, qR, n0, n1);
-            const S le = LE[e];
+            const S le = sle[el];
 #pragma unroll
             for (int k = 0; k < V; ++k) f[k] *= le;
         }
+        if (V == 4 && sizeof(FT) == 4) {
+            reinterpret_cast<float4*>(sF)[el] = make_float4((float)f[0], (float)f[1], (float)f[2], (float)f[3]);
+        } else {
 #pragma unroll
-        for (int k = 0; k < V; ++k) sF[el * V + k] = f[k];
+            for (int k = 0; k < V; ++k) sF[el * V + k] = f[k];
+        }
     }
     __syncthreads();
     // ---- per-cell sums in reference edge order, RK update, ghost fill
-    const int l = threadIdx.x;
     double res[V];
 #pragma unroll
     for (int k = 0; k < V; ++k) res[k] = 0.;
     if (l < nown) {
-        const int c = c0 + l;
-        uint16_t w[kMaxFaces];
-        load_faces(TP, c, w);
-        const double A = (double)((const S*)TP.area)[c];
         double qt[V];
 #pragma unroll
         for (int k = 0; k < V; ++k) qt[k] = 0.;
@@ -587,16 +630,18 @@ __global__ void __launch_bounds__(kTileMax) k_tile_stage(TileParams TP, TileIO i
             if (w[f] == kFaceNone) continue;
             const int el = w[f] & kFaceEdgeMask, side = w[f] >> 15;
             has_ghost |= (w[f] & 0x4000) != 0;
+            FT fe[V];
+            lds<FT, V>(sF + (size_t)el * V, fe);
             if constexpr (M::exact) {
-                const double le = LE[inf.x + el];
+                const double le = sle[el];
 #pragma unroll
                 for (int k = 0; k < V; ++k) {
-                    if (!side) qt[k] -= sF[el * V + k] * le / A;
-                    else qt[k] += sF[el * V + k] * le / A;
+                    if (!side) qt[k] -= fe[k] * le / A;
+                    else qt[k] += fe[k] * le / A;
                 }
             } else {
 #pragma unroll
-                for (int k = 0; k < V; ++k) qt[k] += side ? (double)sF[el * V + k] : -(double)sF[el * V + k];
+                for (int k = 0; k < V; ++k) qt[k] += side ? (double)fe[k] : -(double)fe[k];
             }
         }
         if constexpr (!M::exact) {
@@ -604,15 +649,11 @@ __global__ void __launch_bounds__(kTileMax) k_tile_stage(TileParams TP, TileIO i
 #pragma unroll
             for (int k = 0; k < V; ++k) qt[k] *= rA;
         }
-        double dtc;
         if (global_dt) {
             const double d0 = io.dt[P.cell0];
             dtc = (d0 != d0) ? d0 : tkey_inv(s_dtkey);
-        } else {
-            dtc = io.dt[c];
         }
-        double qb[V], qnew[V];
-        ld<double, V>(io.q_base, c, qb);
+        double qnew[V];
         if constexpr (M::exact) {
 #pragma unroll
             for (int k = 0; k < V; ++k) qnew[k] = qb[k] + qt[k] * dtc * io.alpha;
@@ -636,15 +677,15 @@ __global__ void __launch_bounds__(kTileMax) k_tile_stage(TileParams TP, TileIO i
             for (int f = 0; f < kMaxFaces; ++f) {
                 if (w[f] == kFaceNone || !(w[f] & 0x4000)) continue;
                 const int el = w[f] & kFaceEdgeMask, side = w[f] >> 15;
-                const uint32_t ij = TP.edge_ij[inf.x + el];
+                const uint32_t ij = sij[el];
                 const int o = side ? (int)(ij & 0xffff) : (int)(ij >> 16);
                 const int g = TP.halo[inf.z + o - T];
-                const S n0 = NX[inf.x + el], n1 = NY[inf.x + el];
+                const S n0 = snx[el], n1 = sny[el];
                 S qint[V], qc[V], b[V];
 #pragma unroll
                 for (int k = 0; k < V; ++k) { qc[k] = (S)qnew[k]; qint[k] = qc[k]; }
                 if (ORDER2) {
-                    const S d0 = XF[inf.x + el] - rs[R::OC], d1 = YF[inf.x + el] - rs[R::OC + 1];
+                    const S d0 = sxf[el] - rs[R::OC], d1 = syf[el] - rs[R::OC + 1];
                     S gxs[V], gys[V];
                     lds<S, V>(rs + R::OGX, gxs); lds<S, V>(rs + R::OGY, gys);
                     if constexpr (M::exact) {
@@ -717,7 +758,7 @@ inline size_t smem_stage(const TileParams& TP) {
     using S = typename M::S;
     using FT = typename std::conditional<M::exact, double, S>::type;
     return (size_t)(TP.T + TP.max_halo) * Rec<M, V, ORDER2, ORDER2>::NR * sizeof(S) +
-           (size_t)TP.max_edges * V * sizeof(FT);
+           (size_t)TP.max_edges * (V * sizeof(FT) + 5 * sizeof(S) + 4);
 }
 
 // ------------------------------------------------------------- launchers --

@@ -156,15 +156,17 @@ def physics_struct(ph: _phys.Physics, group_names: Sequence[str]):
 class Solver:
     """Device solver for one mesh + physics (one CUDA device)."""
 
-    def __init__(self, mesh: Mesh, ph: _phys.Physics, precision: str = "fp64_exact", device: int = 0):
+    def __init__(self, mesh: Mesh, ph: _phys.Physics, precision: str = "fp64_exact", device: int = 0,
+                 tile_cells: int = 0):
         self.mesh = mesh
         self.phys = ph
         self.V = ph.V
         self.precision = precision
         self._ps = physics_struct(ph, mesh.group_names)
         h = C.c_void_p()
-        _check(lib().fv_solver_create(mesh._h, C.byref(self._ps), C.c_int32(PREC[precision]), C.c_int32(device),
-                                      C.byref(h)))
+        opt = (C.c_int32 * 1)(int(tile_cells))
+        _check(lib().fv_solver_create_ex(mesh._h, C.byref(self._ps), C.c_int32(PREC[precision]), C.c_int32(device),
+                                         opt, C.byref(h)))
         self._h = h
 
     def close(self):

@@ -138,6 +138,11 @@ int fv_mesh_device_order(const fv_mesh* m, int32_t* new2ref);
 /* ---- solver (device) ---------------------------------------------------- */
 int fv_solver_create(const fv_mesh* m, const fv_physics* ph, int32_t precision, int32_t device,
                      fv_solver** out);
+typedef struct {
+    int32_t tile_cells;  /* cells per tile = threads per CTA: 64, 128 or 256 (0 = 256) */
+} fv_solver_options;
+int fv_solver_create_ex(const fv_mesh* m, const fv_physics* ph, int32_t precision, int32_t device,
+                        const fv_solver_options* opt, fv_solver** out);
 int fv_solver_destroy(fv_solver* s);
 /* cudaStream_t as void*; NULL = the solver's own stream */
 int fv_solver_set_stream(fv_solver* s, void* stream);
