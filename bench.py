@@ -35,12 +35,19 @@ import physics as P  # noqa: E402
 
 METRIC = "cell-updates/s per RK stage"
 UNIT = "cell-updates/s"
-# Algorithmic (unique compulsory) bytes per cell and RK stage, FP64, V = 4,
-# E/N = 1.5 (one figure per kernel):
-#   gradients + limiters: q 32 + area 8 + centroid 16 + edges 1.5*(8 + 5*8) = 72 ... = 224
-#   flux + update + ghost fill: q, gx, gy, lim 128 + q_base 32 + area 8 + centroid 16
-#                               + edges 1.5*(8 + 5*8) = 72 + write 32 + dt 8 = 296
-ALGO_BYTES = {"grad_lim": 224.0, "stage": 296.0, "stage_o1": 160.0, "dt": 96.0}
+# Algorithmic (unique compulsory) bytes per real cell and launch, V = 4,
+# E/N = 1.5 ("Kernels"): the flux + update kernel reads the
+# stage state, its (limited) gradients, centroid, area, edge data
+# (2 indices + normal, length, face centre) and the FP64 base state, and
+# writes the new state.  FP64_EXACT keeps the reference's separate limiter
+# array (SURVEY's 296 B); FP64 folds the limiter into the gradients; FP32
+# stores stage states, gradients and geometry in FP32, the base in FP64, and
+# writes the FP64 state on the last of the 5 stages only.
+ALGO_BYTES = {
+    "fp64_exact": {"stage": 296.0, "grad_lim": 224.0, "stage_o1": 160.0, "dt": 96.0},
+    "fp64": {"stage": 256.0, "grad_lim": 192.0, "stage_o1": 160.0, "dt": 96.0},
+    "fp32": {"stage": 156.4, "grad_lim": 102.0, "stage_o1": 110.0, "dt": 58.0},
+}
 
 
 def build_workload(name):
@@ -201,6 +208,112 @@ def run_reference_arm(args):
 
 
 # ---------------------------------------------------------------- our arm --
+def measure_mode(args, em, mesh, geo, ph, alpha, ic, precision, local, dist, world):
+    """Times args.steps time steps of one precision mode (device resident)."""
+    import torch
+    import fvgpu
+
+    s = fvgpu.Solver(mesh, ph, precision, device=local, tile_cells=args.tile_cells)
+    stream = torch.cuda.Stream(device=local)
+    s.set_stream(stream.cuda_stream)
+    q0 = ic(geo["ccx"], mesh.n_total).ravel()
+    s.set_state(q0)
+    stages = len(alpha)
+    N = mesh.n_real
+    s.run(args.warmup, alpha=alpha)  # warm-up, also captures the step graphs
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    barrier(); torch.cuda.synchronize()
+    ev0 = torch.cuda.Event(enable_timing=True); ev1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        ev0.record(stream)
+        info = s.run(args.warmup + args.steps, alpha=alpha, restart=False)
+        ev1.record(stream)
+        ev1.synchronize()
+    barrier(); torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    if info["step"] != args.warmup + args.steps:
+        raise SystemExit(f"{precision}: run stopped at step {info['step']} (R = {info['R']}): "
+                         f"state check {s.check_state()}")
+    launches = s.last_run_stats()[1]  # kernels launched inside the timed region
+    ms_t = torch.tensor([ms], device=f"cuda:{local}")
+    if dist is not None:
+        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
+    ms_max = float(ms_t.item())
+    out = dict(solver=s, stream=stream, value=world * N * stages * args.steps / (ms_max / 1e3),
+               ms_per_step=ms_max / args.steps, launches=int(launches), clocks=clk.summary(),
+               state_finite=s.check_state() == 0, q_final=s.get_state())
+    # per-kernel device timing (events around every kernel, same stream)
+    prof_steps = max(2, min(args.steps, 10))
+    ms_k = np.zeros(5); cnt_k = np.zeros(5, np.int64)
+    a = np.ascontiguousarray(alpha, np.float64)
+    import ctypes as C
+    fvgpu._check(fvgpu.lib().fv_profile_kernels(s._h, a.ctypes.data_as(C.POINTER(C.c_double)), C.c_int32(a.size),
+                                                C.c_int32(prof_steps), ms_k.ctypes.data_as(C.POINTER(C.c_double)),
+                                                cnt_k.ctypes.data_as(C.POINTER(C.c_int64))))
+    kinds = ["step_begin", "dt", "grad_lim", "stage", "step_end"]
+    out["per_launch_ms"] = {kinds[k]: (ms_k[k] / cnt_k[k] if cnt_k[k] else 0.0) for k in range(5)}
+    out["share"] = {kinds[k]: float(ms_k[k] / ms_k.sum()) for k in range(5)}
+    stage_key = "stage" if ph.order2 else "stage_o1"
+    peak, peak_kind = measured_peak_hbm()
+    kb = ALGO_BYTES[precision][stage_key] * N
+    achieved = kb / (out["per_launch_ms"]["stage"] / 1e3) / 1e9
+    out["roofline"] = {"bound": "hbm", "kernel": "flux + RK update + ghost fill (k_tile_stage)",
+                       "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                       "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind,
+                       "traffic": None, "algorithmic_bytes_per_launch": kb}
+    if ph.order2:
+        kg = ALGO_BYTES[precision]["grad_lim"] * N
+        out["roofline_grad_lim"] = {"achieved": kg / (out["per_launch_ms"]["grad_lim"] / 1e3) / 1e9,
+                                    "frac": kg / (out["per_launch_ms"]["grad_lim"] / 1e3) / 1e9 / peak}
+    return out
+
+
+def e2e_mode(args, mesh, ph, alpha, m, local, dist, world):
+    """Same metric through the C ABI with pinned host buffers: every step is
+    an H2D copy of the state, one time step and a D2H copy of the state."""
+    import torch
+
+    s = m["solver"]
+    nq = mesh.n_total * ph.V
+    h_in = torch.from_numpy(s.get_state()).pin_memory()
+    h_out = torch.empty(nq, dtype=torch.float64).pin_memory()
+    e2e_steps = max(3, min(args.steps, 20))
+    s.set_chunk(1)
+    s.set_state_ptr(h_in.data_ptr(), device=False)
+    s.run(1, alpha=alpha)  # builds the one-step graph outside the timed region
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for k in range(e2e_steps):
+        s.set_state_ptr(h_in.data_ptr(), device=False)
+        s.run(k + 1, alpha=alpha, restart=(k == 0))
+        s.get_state_ptr(h_out.data_ptr(), device=False)
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    s.set_chunk(16)
+    t = torch.tensor([wall], device=f"cuda:{local}")
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return {"value": world * mesh.n_real * len(alpha) * e2e_steps / float(t.item()), "unit": UNIT,
+            "h2d_bytes_per_step": nq * 8, "d2h_bytes_per_step": nq * 8, "steps": e2e_steps}
+
+
+def l2_rho_p(q, q_ref, n_real, gamma=1.4):
+    a = q.reshape(-1, 4)[:n_real]; b = q_ref.reshape(-1, 4)[:n_real]
+
+    def rp(x):
+        return x[:, 0], (gamma - 1) * (x[:, 3] - 0.5 * (x[:, 1] ** 2 + x[:, 2] ** 2) / x[:, 0])
+
+    (ra, pa), (rb, pb) = rp(a), rp(b)
+    l2 = lambda u, v: float(np.sqrt(np.sum((u - v) ** 2) / np.sum(v ** 2)))
+    return {"density": l2(ra, rb), "pressure": l2(pa, pb)}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -208,7 +321,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="step", choices=["step", "sod", "naca"])
-    ap.add_argument("--precision", default="fp64_exact", choices=["fp64_exact", "fp64", "fp32"])
+    ap.add_argument("--precision", default="all", choices=["all", "fp64_exact", "fp64", "fp32"],
+                    help="all: FP32-bulk (headline) and plain FP64 in one line")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--tile-cells", type=int, default=0, help="cells per tile (0: library default)")
     args = ap.parse_args()
@@ -232,105 +346,43 @@ def main():
     em, ph, alpha, ic, desc = build_workload(args.workload)
     mesh = fvgpu.Mesh.from_elements(em)
     geo = mesh.geometry()
-    s = fvgpu.Solver(mesh, ph, args.precision, device=local, tile_cells=args.tile_cells)
-    stream = torch.cuda.Stream(device=local)
-    s.set_stream(stream.cuda_stream)
-    q0 = ic(geo["ccx"], mesh.n_total).ravel()
-    s.set_state(q0)
-    stages = len(alpha)
-    N = mesh.n_real
-
-    # warm-up (also builds the step graph)
-    s.run(args.warmup, alpha=alpha)
-
-    def barrier():
-        if dist is not None:
-            dist.barrier()
-
-    barrier(); torch.cuda.synchronize()
-    ev0 = torch.cuda.Event(enable_timing=True); ev1 = torch.cuda.Event(enable_timing=True)
-    with ClockSampler(local) as clk:
-        ev0.record(stream)
-        info = s.run(args.warmup + args.steps, alpha=alpha, restart=False)
-        ev1.record(stream)
-        ev1.synchronize()
-    barrier(); torch.cuda.synchronize()
-    ms = ev0.elapsed_time(ev1)
-    if info["step"] != args.warmup + args.steps:
-        raise SystemExit(f"run stopped at step {info['step']} (R = {info['R']}): state check {s.check_state()}")
-    launches = s.last_run_stats()[1]  # kernels launched inside the timed region
-    ms_t = torch.tensor([ms], device=f"cuda:{local}")
-    if dist is not None:
-        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
-    ms_max = float(ms_t.item())
-    value = world * N * stages * args.steps / (ms_max / 1e3)
-    healthy = s.check_state() == 0
-
-    # end to end through the C ABI with pinned host buffers, every step:
-    # H2D of the state, one time step, D2H of the state
-    nq = mesh.n_total * ph.V
-    h_in = torch.from_numpy(s.get_state()).pin_memory()
-    h_out = torch.empty(nq, dtype=torch.float64).pin_memory()
-    e2e_steps = max(3, min(args.steps, 20))
-    s.set_chunk(1)
-    s.set_state_ptr(h_in.data_ptr(), device=False)
-    s.run(1, alpha=alpha)  # builds the one-step graph outside the timed region
-    barrier(); torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    for k in range(e2e_steps):
-        s.set_state_ptr(h_in.data_ptr(), device=False)
-        s.run(k + 1, alpha=alpha, restart=(k == 0))
-        s.get_state_ptr(h_out.data_ptr(), device=False)
-    torch.cuda.synchronize()
-    e2e_wall = time.perf_counter() - t0
-    s.set_chunk(16)
-    barrier()
-    e2e_t = torch.tensor([e2e_wall], device=f"cuda:{local}")
-    if dist is not None:
-        dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
-    e2e_value = world * N * stages * e2e_steps / float(e2e_t.item())
-
-    # per-kernel device timing (events around every kernel, same stream)
-    prof_steps = max(2, min(args.steps, 10))
-    ms_k = np.zeros(5); cnt_k = np.zeros(5, np.int64)
-    a = np.ascontiguousarray(alpha, np.float64)
-    import ctypes as C
-    rc = fvgpu.lib().fv_profile_kernels(s._h, a.ctypes.data_as(C.POINTER(C.c_double)), C.c_int32(a.size),
-                                        C.c_int32(prof_steps), ms_k.ctypes.data_as(C.POINTER(C.c_double)),
-                                        cnt_k.ctypes.data_as(C.POINTER(C.c_int64)))
-    fvgpu._check(rc)
-    kinds = ["step_begin", "dt", "grad_lim", "stage", "step_end"]
-    per_launch = {kinds[k]: (ms_k[k] / cnt_k[k] if cnt_k[k] else 0.0) for k in range(5)}
-    stage_key = "stage" if ph.order2 else "stage_o1"
-    stage_bytes = ALGO_BYTES[stage_key] * N
-    peak, peak_kind = measured_peak_hbm()
-    achieved = stage_bytes / (per_launch["stage"] / 1e3) / 1e9
-    share = {kinds[k]: float(ms_k[k] / ms_k.sum()) for k in range(5)}
-
+    modes = ["fp64", "fp32"] if args.precision == "all" else [args.precision]
+    res = {}
+    for prec in modes:
+        res[prec] = measure_mode(args, em, mesh, geo, ph, alpha, ic, prec, local, dist, world)
+    head = modes[-1]  # FP32-bulk when both run
+    m = res[head]
+    e2e = e2e_mode(args, mesh, ph, alpha, m, local, dist, world)
     if rank == 0:
-        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-                "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision != "fp32" else "f32+f64",
+        line = {"metric": METRIC, "value": m["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": m["ms_per_step"], "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64" if head == "fp32" else "f64",
                 "data": "synthetic",
-                "config": {"workload": desc, "n_real_cells": N, "n_edges": mesh.n_edges, "stages": stages,
-                           "precision": args.precision, "l2": "inputs larger than L2 (working set > 126 MB)",
+                "config": {"workload": desc, "n_real_cells": mesh.n_real, "n_edges": mesh.n_edges,
+                           "stages": len(alpha), "precision": head, "tile_cells": args.tile_cells or 128,
+                           "l2": "inputs larger than L2 (working set > 126 MB), no flush",
                            "parallelism": f"{world} independent replicas" if world > 1 else "single GPU"},
-                "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": nq * 8, "d2h_bytes_per_step": nq * 8,
-                        "steps": e2e_steps},
-                "gpu_launches": int(launches),
-                "roofline": {"bound": "hbm", "kernel": "flux+update+ghost fill (k_stage)",
-                             "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                             "peak_source": peak_kind, "traffic": None,
-                             "algorithmic_bytes_per_launch": stage_bytes},
-                "kernel_ms_per_launch": per_launch, "kernel_time_share": share,
-                "clocks": clk.summary(), "state_finite": bool(healthy)}
+                "e2e": e2e, "gpu_launches": m["launches"], "roofline": m["roofline"],
+                "kernel_ms_per_launch": m["per_launch_ms"], "kernel_time_share": m["share"],
+                "clocks": m["clocks"], "state_finite": bool(m["state_finite"])}
+        line["modes"] = {p: {"value": r["value"], "ms_per_step": r["ms_per_step"], "roofline_frac": r["roofline"]["frac"],
+                             "grad_lim_frac": r.get("roofline_grad_lim", {}).get("frac"),
+                             "kernel_ms_per_launch": r["per_launch_ms"], "clocks": r["clocks"],
+                             "state_finite": bool(r["state_finite"])} for p, r in res.items()}
+        if "fp64" in res and "fp32" in res and ph.V == 4:
+            line["fp32_vs_fp64"] = {"l2_rel_error": l2_rho_p(res["fp32"]["q_final"], res["fp64"]["q_final"],
+                                                             mesh.n_real),
+                                    "after_steps": args.warmup + args.steps,
+                                    "speedup": res["fp32"]["value"] / res["fp64"]["value"]}
         if not args.no_cpu_baseline and world == 1:
             r = reference_samples(em, 1, 1, 25)
             if r is not None:
                 line["cpu_baseline"] = {"value": r[0], "unit": UNIT, "cores": 1, "kind": "reference",
-                                        "sample": f"reference library, 1 process, 25 single-stage steps of the {r[1]}-cell mesh"}
+                                        "sample": f"reference library (built from its sources), 1 process, "
+                                                  f"25 single-stage steps of the {r[1]}-cell mesh"}
         print(json.dumps(line))
-    s.close()
+    for r in res.values():
+        r["solver"].close()
     if dist is not None:
         dist.destroy_process_group()
 

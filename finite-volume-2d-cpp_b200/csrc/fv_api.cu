@@ -271,7 +271,7 @@ int fv_solver_create_ex(const fv_mesh* fm, const fv_physics* ph, int32_t precisi
     FaceArrays fa;
     build_face_arrays(m, fa);
     TileArrays ta;
-    const int tile_cells = (opt && opt->tile_cells) ? opt->tile_cells : 256;
+    const int tile_cells = (opt && opt->tile_cells) ? opt->tile_cells : 128;
     if (tile_cells != 64 && tile_cells != 128 && tile_cells != 256)
         return fail(FV_ERR_ARG, "tile_cells must be 64, 128 or 256");
     build_tiles(m, fa, tile_cells, ta);

@@ -139,7 +139,7 @@ int fv_mesh_device_order(const fv_mesh* m, int32_t* new2ref);
 int fv_solver_create(const fv_mesh* m, const fv_physics* ph, int32_t precision, int32_t device,
                      fv_solver** out);
 typedef struct {
-    int32_t tile_cells;  /* cells per tile = threads per CTA: 64, 128 or 256 (0 = 256) */
+    int32_t tile_cells;  /* cells per tile = threads per CTA: 64, 128 or 256 (0 = 128) */
 } fv_solver_options;
 int fv_solver_create_ex(const fv_mesh* m, const fv_physics* ph, int32_t precision, int32_t device,
                         const fv_solver_options* opt, fv_solver** out);
