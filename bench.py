@@ -239,10 +239,8 @@ def measure_mode(args, em, mesh, geo, ph, alpha, ic, precision, local, dist, wor
         raise SystemExit(f"{precision}: run stopped at step {info['step']} (R = {info['R']}): "
                          f"state check {s.check_state()}")
     launches = s.last_run_stats()[1]  # kernels launched inside the timed region
-    ms_t = torch.tensor([ms], device=f"cuda:{local}")
-    if dist is not None:
-        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
-    ms_max = float(ms_t.item())
+    import replicas
+    ms_max = replicas.max_over_ranks(ms, dist, device=f"cuda:{local}")
     out = dict(solver=s, stream=stream, value=world * N * stages * args.steps / (ms_max / 1e3),
                ms_per_step=ms_max / args.steps, launches=int(launches), clocks=clk.summary(),
                state_finite=s.check_state() == 0, q_final=s.get_state())
@@ -296,10 +294,9 @@ def e2e_mode(args, mesh, ph, alpha, m, local, dist, world):
     torch.cuda.synchronize()
     wall = time.perf_counter() - t0
     s.set_chunk(16)
-    t = torch.tensor([wall], device=f"cuda:{local}")
-    if dist is not None:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return {"value": world * mesh.n_real * len(alpha) * e2e_steps / float(t.item()), "unit": UNIT,
+    import replicas
+    return {"value": replicas.job_throughput(mesh.n_real * len(alpha) * e2e_steps, wall, dist, f"cuda:{local}"),
+            "unit": UNIT,
             "h2d_bytes_per_step": nq * 8, "d2h_bytes_per_step": nq * 8, "steps": e2e_steps}
 
 
