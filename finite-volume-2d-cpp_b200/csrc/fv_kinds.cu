@@ -1,0 +1,49 @@
+// Host evaluation of the device physics kinds (fv_physics_exact.cuh, the
+// reference's exact arithmetic).  A caller that holds user physics functions
+// (the fvhyper C++ shim: calc_flux, limiter_func, boundaries::bounds) compares
+// them with these on probe states to pick the device kind, and refuses what
+// matches none.  Built with -ffp-contract=off, so the results are the
+// reference's bits.
+#include <stdint.h>
+#include <string.h>
+
+#include "fv_physics_exact.cuh"
+#include "fvgpu.h"
+
+extern "C" {
+
+int fv_kind_flux(int32_t flux, double gamma, const double* qi, const double* qj, const double* n, double* f) {
+    if (!qi || !qj || !n || !f) return FV_ERR_ARG;
+    switch (flux) {
+        case FV_FLUX_ROE_FS: fvgpu::exact::roe<true>(gamma, f, qi, qj, n[0], n[1]); return FV_OK;
+        case FV_FLUX_ROE_ST: fvgpu::exact::roe<false>(gamma, f, qi, qj, n[0], n[1]); return FV_OK;
+        case FV_FLUX_BURGERS: fvgpu::exact::burgers(f, qi, qj, n[0], n[1]); return FV_OK;
+        default: return FV_ERR_UNSUPPORTED;
+    }
+}
+
+int fv_kind_limiter(int32_t kind, double y, double* out) {
+    if (!out) return FV_ERR_ARG;
+    if (kind < FV_LIM_ZERO || kind > FV_LIM_MINMOD) return FV_ERR_UNSUPPORTED;
+    *out = fvgpu::exact::limiter_func(kind, y);
+    return FV_OK;
+}
+
+int fv_kind_bc(int32_t kind, int32_t V, double gamma, const double* bv, const double* q, const double* n,
+               double* b) {
+    if (!q || !n || !b || (V != 2 && V != 4)) return FV_ERR_ARG;
+    if (kind < FV_BC_COPY || kind > FV_BC_FARFIELD) return FV_ERR_UNSUPPORTED;
+    if ((kind == FV_BC_INLET_OUTLET || kind == FV_BC_FARFIELD) && !bv) return FV_ERR_ARG;
+    fvgpu::Params P;
+    memset(&P, 0, sizeof(P));
+    P.V = V;
+    P.gamma = gamma;
+    P.n_groups = 1;
+    P.group_bc[0] = kind;
+    if (bv) memcpy(P.group_bv, bv, 4 * sizeof(double));
+    if (V == 4) fvgpu::exact::bc<4>(P, 0, b, q, n[0], n[1]);
+    else fvgpu::exact::bc<2>(P, 0, b, q, n[0], n[1]);
+    return FV_OK;
+}
+
+}  // extern "C"

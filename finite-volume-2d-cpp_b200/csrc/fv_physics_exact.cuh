@@ -1,23 +1,30 @@
 // Device physics kinds in the reference's exact evaluation order.
 //
-// Compiled with -fmad=false: every expression below is evaluated with the
-// same operations, operand order, IEEE divisions and square roots as the
-// reference example code it cites, so the FP64 results are bit-identical to
-// the reference CPU solver.
+// Compiled with -fmad=false (device) and -ffp-contract=off (host): every
+// expression below is evaluated with the same operations, operand order,
+// IEEE divisions and square roots as the reference example code it cites, so
+// the FP64 results are bit-identical to the reference CPU solver.  The same
+// functions run on the host (fv_kinds.cu), where the fvhyper shim uses them to
+// match a user's physics functions to a device kind.
 #pragma once
+#include <math.h>
 #include "fv_internal.h"
+
+#ifndef FV_HD
+#define FV_HD __host__ __device__ __forceinline__
+#endif
 
 namespace fvgpu {
 namespace exact {
 
-__device__ __forceinline__ double dmin(double a, double b) { return (b < a) ? b : a; }  // std::min
-__device__ __forceinline__ double dmax(double a, double b) { return (a < b) ? b : a; }  // std::max
+FV_HD double dmin(double a, double b) { return (b < a) ? b : a; }  // std::min
+FV_HD double dmax(double a, double b) { return (a < b) ? b : a; }  // std::max
 
 // Roe flux with the "cures" eigenvalue modification.
 // FS_ASSOC: examples/forwardStep/main.cpp:72-135 (central flux as one sum);
 // otherwise examples/shockTube/main.cpp:68-135 = examples/naca/main.cpp:71-137.
 template <bool FS_ASSOC>
-__device__ __forceinline__ void roe(double gamma, double* f, const double* qi, const double* qj,
+FV_HD void roe(double gamma, double* f, const double* qi, const double* qj,
                                     double n0, double n1) {
     const double pi = (gamma - 1) * (qi[3] - 0.5 / qi[0] * (qi[1] * qi[1] + qi[2] * qi[2]));
     const double pj = (gamma - 1) * (qj[3] - 0.5 / qj[0] * (qj[1] * qj[1] + qj[2] * qj[2]));
@@ -67,7 +74,7 @@ __device__ __forceinline__ void roe(double gamma, double* f, const double* qi, c
 }
 
 // Upwind advection flux, examples/burgers/main.cpp:68-96.
-__device__ __forceinline__ void burgers(double* f, const double* qi, const double* qj, double n0, double n1) {
+FV_HD void burgers(double* f, const double* qi, const double* qj, double n0, double n1) {
     const double Vi = qi[0] * n0 + qi[1] * n1;
     const double Vj = qj[0] * n0 + qj[1] * n1;
     const double fi0 = Vi * qi[0], fi1 = Vi * qi[1];
@@ -78,7 +85,7 @@ __device__ __forceinline__ void burgers(double* f, const double* qi, const doubl
 }
 
 template <int FLUX>
-__device__ __forceinline__ void flux(double gamma, double* f, const double* qi, const double* qj,
+FV_HD void flux(double gamma, double* f, const double* qi, const double* qj,
                                      double n0, double n1) {
     if (FLUX == 3) burgers(f, qi, qj, n0, n1);
     else roe<FLUX == 1>(gamma, f, qi, qj, n0, n1);
@@ -87,7 +94,7 @@ __device__ __forceinline__ void flux(double gamma, double* f, const double* qi, 
 // Limiter functions phi (limiter_func).  ZERO: shockTube/main.cpp:60-62.
 // MICHALAK (y_t = 2): forwardStep/main.cpp:57-66.  MINMOD: burgers/main.cpp:
 // 51-53.  VENKAT: (y^2 + 2y)/(y^2 + y + 2), Venkatakrishnan (1995).
-__device__ __forceinline__ double limiter_func(int kind, double y) {
+FV_HD double limiter_func(int kind, double y) {
     if (kind == 1) {
         const double yt = 2.0;
         if (y >= yt) return 1.0;
@@ -105,7 +112,7 @@ __device__ __forceinline__ double limiter_func(int kind, double y) {
 // main.cpp:194-261.  FARFIELD: naca/main.cpp:192-259.  Subsonic outlets keep
 // the reference's b[2] = b[1]*(...).
 template <int V>
-__device__ __forceinline__ void bc(const Params& P, int group, double* b, const double* q, double n0, double n1) {
+FV_HD void bc(const Params& P, int group, double* b, const double* q, double n0, double n1) {
     const int kind = P.group_bc[group];
     if (kind == 0 || V != 4) {
 #pragma unroll
@@ -161,7 +168,7 @@ __device__ __forceinline__ void bc(const Params& P, int group, double* b, const 
 }
 
 // Pressure, forwardStep/main.cpp:37-39.
-__device__ __forceinline__ double pres(double gamma, const double* q) {
+FV_HD double pres(double gamma, const double* q) {
     return (gamma - 1) * (q[3] - 0.5 / q[0] * (q[1] * q[1] + q[2] * q[2]));
 }
 

@@ -216,6 +216,19 @@ int fv_stage_dt_noalloc(fv_solver* s, const double* q_device, double* dt_device,
 int fv_stage_bounds(fv_solver* s, double* q, const double* gx, const double* gy,
                     const double* lim);
 
+/* ---- host evaluation of the device physics kinds ------------------------ */
+/* The device kinds' arithmetic run on the host (bit-identical to the device's
+ * FP64_EXACT mode and to the reference example functions each kind restates).
+ * The fvhyper shim compares a user's calc_flux / limiter_func /
+ * boundaries::bounds entries with these on probe states to choose the kind
+ * (explicit.h:53,71-78; mesh.h:36-39).  n = {nx, ny}. */
+int fv_kind_flux(int32_t flux, double gamma, const double* qi, const double* qj, const double* n,
+                 double* f);
+int fv_kind_limiter(int32_t kind, double y, double* out);
+/* bv: [4] boundary state of INLET_OUTLET / FARFIELD (may be NULL otherwise). */
+int fv_kind_bc(int32_t kind, int32_t V, double gamma, const double* bv, const double* q,
+               const double* n, double* b);
+
 #ifdef __cplusplus
 }
 #endif

@@ -80,6 +80,8 @@ void put(double* dst, const std::vector<double>& v) { std::memcpy(dst, v.data(),
 size_t nq() { return (size_t)fvhyper::vars * g_mesh->cellsAreas.size(); }
 }  // namespace
 
+int fvref_example_main();  // the example main(), renamed by oracle/Makefile
+
 extern "C" {
 
 int ref_vars() { return fvhyper::vars; }
@@ -280,5 +282,10 @@ int ref_run(double* q_out, uint64_t max_step, double max_time, double tolerance,
     put(q_out, q);
     return 0;
 }
+
+/* The example program's own main() (renamed at compile time), run as is in
+ * the caller's working directory: reads its mesh file, prints its log,
+ * writes its output files. */
+int ref_example_main(void) { return fvref_example_main(); }
 
 }  // extern "C"
