@@ -424,6 +424,23 @@ int fv_set_state(fv_solver* s, const double* q) {
 }
 int fv_get_state(fv_solver* s, double* q) { return get_state_common(s, q, cudaMemcpyDeviceToHost); }
 int fv_set_state_device(fv_solver* s, const double* q) { return set_state_common(s, q, cudaMemcpyDeviceToDevice); }
+
+int fv_solver_continue_from(fv_solver* dst, fv_solver* src) {
+    if (!dst || !src || dst == src) return fail(FV_ERR_ARG, "fv_solver_continue_from: need two solvers");
+    if (dst->device != src->device) return fail(FV_ERR_ARG, "fv_solver_continue_from: solvers on different devices");
+    if (dst->n_total != src->n_total || dst->n_real != src->n_real || dst->V != src->V)
+        return fail(FV_ERR_ARG, "fv_solver_continue_from: solvers of different meshes");
+    CK(cudaSetDevice(dst->device));
+    CK(cudaStreamSynchronize(src->stream));
+    // through reference numbering, so the two device orders need not agree
+    launch_permute_to_ref(src->qbase[0], dst->stage_buf, src->new2ref, (int)src->n_total, src->V, dst->stream);
+    launch_permute_to_device(dst->stage_buf, dst->qbase[0], dst->new2ref, (int)dst->n_total, dst->V, dst->stream);
+    sync_shadow(dst, 0);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(dst->ctrl, src->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToDevice, dst->stream));
+    CK(cudaStreamSynchronize(dst->stream));
+    return FV_OK;
+}
 int fv_get_state_device(fv_solver* s, double* q) { return get_state_common(s, q, cudaMemcpyDeviceToDevice); }
 
 // ---------------------------------------------------------------- run ----

@@ -228,6 +228,11 @@ class Solver:
         _check(lib().fv_run(self._h, C.byref(o), C.byref(info)))
         return dict(step=info.step, time=info.time, R=np.array(info.R[: self.V]), R0=np.array(info.R0[: self.V]))
 
+    def continue_from(self, other: "Solver"):
+        """Take over another solver's state and run control (same mesh), so
+        run(..., restart=False) continues its run in this solver's precision."""
+        _check(lib().fv_solver_continue_from(self._h, other._h))
+
     def last_run_stats(self):
         ms = C.c_double(); n = C.c_int64()
         _check(lib().fv_last_run_stats(self._h, C.byref(ms), C.byref(n)))

@@ -156,6 +156,14 @@ int fv_get_state_device(fv_solver* s, double* q_device);
  * captured in CUDA graphs of `chunk` steps; stopping criteria are evaluated
  * on the device, so the host only waits once per chunk. */
 int fv_run(fv_solver* s, const fv_run_options* opt, fv_run_info* info);
+/* Continue a run in another solver of the same mesh, typically with another
+ * precision (FP32-bulk for the transient, FP64 for the tail of a steady
+ * solve, whose residual drop FP32 flux arithmetic cannot take below about
+ * 1e-5): copies src's state and run control (step, time, R0, R) into dst, so
+ * fv_run(dst, restart = 0) carries on with the same step count, time and
+ * residual normalisation.  Both solvers must be on one device.  No
+ * counterpart in the reference (explicit.cpp:657-817 runs in one precision). */
+int fv_solver_continue_from(fv_solver* dst, fv_solver* src);
 /* R after the last step (sqrt of sum qt^2 A over real cells, un-normalised). */
 int fv_residuals(fv_solver* s, double* R);
 /* Returns FV_ERR_NONFINITE if any real-cell state is NaN/Inf, or if an

@@ -1,0 +1,182 @@
+"""Config-level parity on the GPU: the named workloads at (or near) their own
+sizes, each compared with the FP64 oracle, and the FP32-bulk path's L1/L2
+error in density and pressure against it stated and bounded.
+
+- Sod shock tube, plain method (400 x 40 quads split in 2 = 32,000 cells,
+  first-order Roe, RK1, CFL 0.5, global dt, to t = 0.2, FP64): bit-identical
+  to the oracle over the whole run, and within first-order accuracy of the
+  exact Riemann solution.
+- NACA 0012 steady transonic (M = 0.8, alpha = 1.25 deg, Michalak limiter,
+  local time stepping) on a 64 x 16 O-grid: bit-identical to the oracle for
+  1,500 steps; run to a 1e-8 residual drop in FP64, and in FP32-bulk handing
+  over to FP64 for the tail (FP32 flux arithmetic floors the residual drop
+  near 1e-5); lift and drag (FP64 force sums) agree between the two.
+"""
+import numpy as np
+import pytest
+
+import meshgen
+import physics as P
+
+pytestmark = pytest.mark.gpu
+
+
+def bits_equal(a, b):
+    return a.shape == b.shape and a.tobytes() == b.tobytes()
+
+
+def _prim(q, gamma=1.4):
+    q = q.reshape(-1, 4)
+    rho = q[:, 0]
+    p = (gamma - 1) * (q[:, 3] - 0.5 * (q[:, 1] ** 2 + q[:, 2] ** 2) / rho)
+    return rho, p
+
+
+def l1_l2(a, b, w):
+    d = np.abs(a - b)
+    return float((d * w).sum() / w.sum()), float(np.sqrt((d * d * w).sum() / w.sum()))
+
+
+def sod_exact(x, t, left=(1.0, 0.0, 1.0), right=(0.125, 0.0, 0.1), gamma=1.4, x0=0.5):
+    """Exact solution of the 1D Riemann problem (Toro, Riemann Solvers and
+    Numerical Methods for Fluid Dynamics, ch. 4): density and pressure."""
+    rl, ul, pl = left
+    rr, ur, pr = right
+    cl, cr = np.sqrt(gamma * pl / rl), np.sqrt(gamma * pr / rr)
+    g1, g2 = (gamma - 1) / (2 * gamma), (gamma + 1) / (2 * gamma)
+
+    def f(p, rk, pk, ck):
+        if p > pk:  # shock
+            A, B = 2 / ((gamma + 1) * rk), (gamma - 1) / (gamma + 1) * pk
+            return (p - pk) * np.sqrt(A / (p + B)), np.sqrt(A / (B + p)) * (1 - (p - pk) / (2 * (B + p)))
+        return 2 * ck / (gamma - 1) * ((p / pk) ** g1 - 1), (p / pk) ** (-g2) / (rk * ck)
+
+    p = 0.5 * (pl + pr)
+    for _ in range(100):
+        fl, dl = f(p, rl, pl, cl)
+        fr, dr = f(p, rr, pr, cr)
+        dp = (fl + fr + ur - ul) / (dl + dr)
+        p = max(p - dp, 1e-12)
+        if abs(dp) < 1e-14 * p:
+            break
+    fl, _ = f(p, rl, pl, cl)
+    fr, _ = f(p, rr, pr, cr)
+    u = 0.5 * (ul + ur) + 0.5 * (fr - fl)
+    s = (x - x0) / t
+    rho = np.empty_like(x); pres = np.empty_like(x)
+    # left rarefaction (p* < pl for Sod) and right shock (p* > pr)
+    shl, stl = ul - cl, u - cl * (p / pl) ** g1
+    rstar_l = rl * (p / pl) ** (1 / gamma)
+    sr = ur + cr * np.sqrt(g2 * p / pr + g1)
+    rstar_r = rr * ((p / pr + (gamma - 1) / (gamma + 1)) / ((gamma - 1) / (gamma + 1) * p / pr + 1))
+    m = s < shl
+    rho[m], pres[m] = rl, pl
+    m = (s >= shl) & (s < stl)
+    c = 2 / (gamma + 1) * (cl + (gamma - 1) / 2 * (ul - s[m]))
+    rho[m] = rl * (c / cl) ** (2 / (gamma - 1)); pres[m] = pl * (c / cl) ** (2 * gamma / (gamma - 1))
+    m = (s >= stl) & (s < u)
+    rho[m], pres[m] = rstar_l, p
+    m = (s >= u) & (s < sr)
+    rho[m], pres[m] = rstar_r, p
+    m = s >= sr
+    rho[m], pres[m] = rr, pr
+    return rho, pres
+
+
+def test_sod_full_size(oracle):
+    import fvgpu
+
+    em = meshgen.sod_strip(400, 40)
+    ph = P.sod()
+    g = oracle.build_mesh(em)
+    assert g.n_real == 32000
+    p = oracle.physics(ph, em.group_names)
+    q0 = P.ic_sod(g.ccx).ravel()
+    want = oracle.run_loop(g, p, q0, P.RK1_ALPHA, 10 ** 6, max_time=0.2, print_interval=10 ** 9)
+    mesh = fvgpu.Mesh.from_elements(em)
+    s = fvgpu.Solver(mesh, ph, "fp64_exact")
+    s.set_state(q0)
+    got = s.run(10 ** 6, alpha=P.RK1_ALPHA, max_time=0.2, print_interval=10 ** 9)
+    q = s.get_state()
+    assert got["step"] == want["step"] and got["time"] == want["time"] >= 0.2
+    assert bits_equal(q, want["q"])
+    s.close()
+    # first-order accuracy against the exact solution (cells along the tube)
+    n = g.n_real
+    rho, pres = _prim(q[: 4 * n])
+    rex, pex = sod_exact(g.ccx[:n], got["time"])
+    A = g.area[:n]
+    l1_rho, _ = l1_l2(rho, rex, A)
+    l1_p, _ = l1_l2(pres, pex, A)
+    assert l1_rho < 0.01 and l1_p < 0.01, (l1_rho, l1_p)
+    # FP32-bulk: same steps, L1/L2 errors in density and pressure vs FP64
+    s32 = fvgpu.Solver(mesh, ph, "fp32")
+    s32.set_state(q0)
+    s32.run(got["step"], alpha=P.RK1_ALPHA, print_interval=10 ** 9)
+    r32, p32 = _prim(s32.get_state()[: 4 * n])
+    e_rho = l1_l2(r32, rho, A)
+    e_p = l1_l2(p32, pres, A)
+    print(f"sod fp32 vs fp64: rho L1 {e_rho[0]:.2e} L2 {e_rho[1]:.2e}  p L1 {e_p[0]:.2e} L2 {e_p[1]:.2e}")
+    assert e_rho[1] <= 1e-4 and e_p[1] <= 1e-4
+    s32.close()
+
+
+def test_naca_converges_with_lift_and_drag(oracle):
+    import fvgpu
+
+    em = meshgen.naca_ogrid(ni=64, nj=16, r_far=10.0)
+    ph = P.naca()
+    g = oracle.build_mesh(em)
+    p = oracle.physics(ph, em.group_names)
+    q0 = P.ic_naca(g.n_total).ravel()
+    mesh = fvgpu.Mesh.from_elements(em)
+    airfoil = em.group_names.index("airfoil")
+    # bit-identical to the oracle over 1,500 steps
+    want = oracle.run_loop(g, p, q0, P.RK5_ALPHA, 1500, print_interval=10 ** 9)
+    s = fvgpu.Solver(mesh, ph, "fp64_exact")
+    s.set_state(q0)
+    s.run(1500, print_interval=10 ** 9)
+    assert bits_equal(s.get_state(), want["q"])
+    fx_o, fy_o = oracle.boundary_force(g, p, want["q"], airfoil)
+    fx, fy = s.boundary_force("airfoil")
+    # FP64 sums over the airfoil faces, reduced in a different order
+    np.testing.assert_allclose([fx, fy], [fx_o, fy_o], rtol=1e-12, atol=0)
+    s.close()
+    # to a 1e-8 residual drop: FP64 alone, and FP32-bulk to 1e-4 then FP64
+    res = {}
+    a = np.deg2rad(1.25)
+    for prec in ("fp64", "fp32"):
+        sv = fvgpu.Solver(mesh, ph, prec)
+        sv.set_state(q0)
+        r = sv.run(60000, tolerance=1e-8 if prec == "fp64" else 1e-4, print_interval=10 ** 9)
+        steps32 = r["step"] if prec == "fp32" else 0
+        if prec == "fp32":
+            assert r["step"] < 60000, r["R"]
+            q32 = sv.get_state()
+            s64 = fvgpu.Solver(mesh, ph, "fp64")
+            s64.continue_from(sv)
+            sv.close()
+            sv = s64
+            r = sv.run(60000, tolerance=1e-8, print_interval=10 ** 9, restart=False)
+        assert r["step"] < 60000 and max(r["R"]) < 1e-8, (prec, r["step"], r["R"])
+        fx, fy = sv.boundary_force("airfoil")
+        # lift / drag in the free-stream frame (alpha = 1.25 deg)
+        res[prec] = dict(q=sv.get_state(), steps=r["step"], steps32=steps32,
+                         lift=-fx * np.sin(a) + fy * np.cos(a), drag=fx * np.cos(a) + fy * np.sin(a))
+        sv.close()
+    n = g.n_real
+    A = g.area[:n]
+    r64, p64 = _prim(res["fp64"]["q"][: 4 * n])
+    r32, p32 = _prim(res["fp32"]["q"][: 4 * n])
+    e_rho, e_p = l1_l2(r32, r64, A), l1_l2(p32, p64, A)
+    r32h, p32h = _prim(q32[: 4 * n])  # the FP32 phase's end state (drop 1e-4)
+    print(f"naca fp32 phase at drop 1e-4 vs converged fp64: rho L2 {l1_l2(r32h, r64, A)[1]:.2e}, "
+          f"p L2 {l1_l2(p32h, p64, A)[1]:.2e}")
+    print(f"naca steps fp64 {res['fp64']['steps']} fp32+fp64 {res['fp32']['steps32']}+"
+          f"{res['fp32']['steps'] - res['fp32']['steps32']}; "
+          f"lift {res['fp64']['lift']:.6f} / {res['fp32']['lift']:.6f}, "
+          f"drag {res['fp64']['drag']:.6f} / {res['fp32']['drag']:.6f}; "
+          f"fp32 vs fp64 rho L1 {e_rho[0]:.2e} L2 {e_rho[1]:.2e}, p L1 {e_p[0]:.2e} L2 {e_p[1]:.2e}")
+    assert e_rho[1] <= 1e-4 and e_p[1] <= 1e-4
+    assert abs(res["fp32"]["lift"] - res["fp64"]["lift"]) <= 1e-4 * max(1.0, abs(res["fp64"]["lift"]))
+    assert abs(res["fp32"]["drag"] - res["fp64"]["drag"]) <= 1e-4 * max(1.0, abs(res["fp64"]["drag"]))
