@@ -2,6 +2,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdio>
+#include <algorithm>
 #include <cstring>
 #include <memory>
 #include <mutex>
@@ -82,6 +83,11 @@ struct fv_solver {
     std::vector<GraphEntry> graphs;
     double last_ms = 0.0;
     int64_t last_launches = 0;
+    // dt minimum key slots: [n_cases][kDtSlots] (one case: inside ctrl)
+    unsigned long long* keys = nullptr;
+    int n_cases = 1;
+    double* case_time = nullptr;                           // batches: [n_cases]
+    std::vector<int64_t> case_real_off, case_bound_off;    // batches: host copies
 
     template <class T>
     cudaError_t alloc(T** p, size_t n, size_t elem = sizeof(T)) {
@@ -170,6 +176,65 @@ int fv_mesh_read_msh(const char* path, fv_mesh** out) {
         return fail(err.rfind("cannot open", 0) == 0 ? FV_ERR_IO : FV_ERR_MESH, err);
     }
     return finish_mesh(fm, out);
+}
+
+int fv_mesh_create_batch(int32_t n_cases, const fv_mesh* const* cases, fv_mesh** out) {
+    if (!out || !cases || n_cases < 1) return fail(FV_ERR_ARG, "fv_mesh_create_batch: invalid arguments");
+    auto* fm = new fv_mesh();
+    HostMesh& u = fm->m;
+    u.case_real_off.push_back(0);
+    u.case_bound_off.push_back(0);
+    int64_t total_cells = 0, total_bnd = 0;
+    for (int32_t k = 0; k < n_cases; ++k) {
+        if (!cases[k]) {
+            delete fm;
+            return fail(FV_ERR_ARG, "fv_mesh_create_batch: null case mesh");
+        }
+        const HostMesh& c = cases[k]->m;
+        const int32_t node0 = (int32_t)u.nodes_x.size();
+        u.nodes_x.insert(u.nodes_x.end(), c.nodes_x.begin(), c.nodes_x.end());
+        u.nodes_y.insert(u.nodes_y.end(), c.nodes_y.begin(), c.nodes_y.end());
+        for (int32_t v : c.cells4) u.cells4.push_back(v < 0 ? v : v + node0);
+        for (int32_t v : c.bnd_nodes) u.bnd_nodes.push_back(v + node0);
+        // boundary groups are merged by name, in order of first use
+        for (int32_t g : c.bnd_group) {
+            const std::string& name = c.group_names[(size_t)g];
+            auto it = std::find(u.group_names.begin(), u.group_names.end(), name);
+            if (it == u.group_names.end()) {
+                u.group_names.push_back(name);
+                it = u.group_names.end() - 1;
+            }
+            u.bnd_group.push_back((int32_t)(it - u.group_names.begin()));
+        }
+        total_cells += (int64_t)c.cells4.size() / 4;
+        total_bnd += (int64_t)c.bnd_group.size();
+        u.case_real_off.push_back(total_cells);
+        u.case_bound_off.push_back(total_bnd);
+    }
+    if (total_cells + total_bnd >= (int64_t)0x7fffffff) {
+        delete fm;
+        return fail(FV_ERR_ARG, "batch too large for 31-bit cell indices");
+    }
+    if (n_cases == 1) { u.case_real_off.clear(); u.case_bound_off.clear(); }
+    return finish_mesh(fm, out);
+}
+
+int fv_mesh_case_count(const fv_mesh* fm) {
+    if (!fm) return 0;
+    return fm->m.case_real_off.size() > 2 ? (int)fm->m.case_real_off.size() - 1 : 1;
+}
+
+int fv_mesh_case_offsets(const fv_mesh* fm, int64_t* real_off, int64_t* bound_off) {
+    if (!fm || !real_off || !bound_off) return fail(FV_ERR_ARG, "fv_mesh_case_offsets: null argument");
+    const HostMesh& m = fm->m;
+    if (m.case_real_off.size() > 2) {
+        std::copy(m.case_real_off.begin(), m.case_real_off.end(), real_off);
+        std::copy(m.case_bound_off.begin(), m.case_bound_off.end(), bound_off);
+    } else {
+        real_off[0] = 0; real_off[1] = m.n_real;
+        bound_off[0] = 0; bound_off[1] = m.n_bound;
+    }
+    return FV_OK;
 }
 
 void fv_mesh_destroy(fv_mesh* m) { delete m; }
@@ -349,6 +414,37 @@ int fv_solver_create_ex(const fv_mesh* fm, const fv_physics* ph, int32_t precisi
         CK(cudaMemsetAsync(s->sbase[1], 0, nq * 4, s->stream));
     }
     CK(cudaMemsetAsync(s->ctrl, 0, sizeof(Ctrl), s->stream));
+    s->keys = s->ctrl->dtkeys;
+    if (m.case_real_off.size() > 2) {
+        // a batch of independent cases: per-case dt keys, times and lookups
+        const int nc = (int)m.case_real_off.size() - 1;
+        s->n_cases = nc;
+        s->case_real_off = m.case_real_off;
+        s->case_bound_off = m.case_bound_off;
+        auto case_of_ref = [&](int64_t r) {
+            const std::vector<int64_t>& o = r < m.n_real ? m.case_real_off : m.case_bound_off;
+            const int64_t x = r < m.n_real ? r : r - m.n_real;
+            return (int32_t)(std::upper_bound(o.begin(), o.end(), x) - o.begin() - 1);
+        };
+        std::vector<int32_t> cell_case(m.n_total), case_cell0(nc), tile_case(ta.n_tiles);
+        for (int64_t n = 0; n < m.n_total; ++n) cell_case[n] = case_of_ref(m.new2ref[n]);
+        for (int k = 0; k < nc; ++k) case_cell0[k] = m.ref2new[m.case_real_off[k]];
+        for (int t = 0; t < ta.n_tiles; ++t) {
+            const int64_t a = (int64_t)t * tile_cells, b = std::min<int64_t>(a + tile_cells, m.n_real) - 1;
+            tile_case[t] = cell_case[a] == cell_case[b] ? cell_case[a] : -1;
+        }
+        Params& Pb = s->TP.P;
+        Pb.n_cases = nc;
+        if ((rc = upload_v(s.get(), cell_case, &Pb.cell_case))) return rc;
+        if ((rc = upload_v(s.get(), case_cell0, &Pb.case_cell0))) return rc;
+        if ((rc = upload_v(s.get(), tile_case, &Pb.tile_case))) return rc;
+        CK(s->alloc(&s->case_time, (size_t)nc));
+        CK(cudaMemsetAsync(s->case_time, 0, (size_t)nc * 8, s->stream));
+        Pb.case_time = s->case_time;
+        CK(s->alloc(&s->keys, (size_t)nc * kDtSlots));
+    } else {
+        s->TP.P.n_cases = 1;
+    }
     launch_fill_ghost_grad(s->gx, s->gy, s->lim, (int)m.n_real, (int)m.n_total, ph->V, s->f32, s->stream);
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(s->stream));
@@ -438,7 +534,26 @@ int fv_solver_continue_from(fv_solver* dst, fv_solver* src) {
     sync_shadow(dst, 0);
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(dst->ctrl, src->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToDevice, dst->stream));
+    if (dst->n_cases != src->n_cases) return fail(FV_ERR_ARG, "fv_solver_continue_from: different batches");
+    if (dst->case_time)
+        CK(cudaMemcpyAsync(dst->case_time, src->case_time, (size_t)dst->n_cases * 8, cudaMemcpyDeviceToDevice,
+                           dst->stream));
     CK(cudaStreamSynchronize(dst->stream));
+    return FV_OK;
+}
+
+int fv_batch_times(fv_solver* s, double* times) {
+    if (!s || !times) return fail(FV_ERR_ARG, "fv_batch_times: null argument");
+    CK(cudaSetDevice(s->device));
+    if (s->case_time) {
+        CK(cudaMemcpyAsync(times, s->case_time, (size_t)s->n_cases * 8, cudaMemcpyDeviceToHost, s->stream));
+    } else {
+        Ctrl hc;
+        CK(cudaMemcpyAsync(&hc, s->ctrl, sizeof(hc), cudaMemcpyDeviceToHost, s->stream));
+        CK(cudaStreamSynchronize(s->stream));
+        times[0] = hc.time;
+    }
+    CK(cudaStreamSynchronize(s->stream));
     return FV_OK;
 }
 int fv_get_state_device(fv_solver* s, double* q) { return get_state_common(s, q, cudaMemcpyDeviceToDevice); }
@@ -468,10 +583,10 @@ static int enqueue_step(fv_solver* s, const std::vector<double>& alpha, int b, E
     cudaStream_t st = s->stream;
     int n = 0;
     auto mark = [&](int k) { if (log) log->mark(k); };
-    launch_step_begin(s->ctrl, s->limits, s->V, st); ++n; mark(KK_BEGIN);
+    launch_step_begin(s->ctrl, s->limits, s->V, s->keys, s->n_cases * kDtSlots, st); ++n; mark(KK_BEGIN);
     TileIO io{};
     io.gx = s->gx; io.gy = s->gy; io.lim = s->lim; io.dt = s->dt; io.ctrl = s->ctrl;
-    io.dtkeys = s->ctrl->dtkeys;
+    io.dtkeys = s->keys;
     io.q_stage = s->sbase[b];
     tile::launch_dt(s->precision, TP, io, st); ++n; mark(KK_DT);
     const int ns = (int)alpha.size();
@@ -500,7 +615,7 @@ static int enqueue_step(fv_solver* s, const std::vector<double>& alpha, int b, E
         tile::launch_stage(s->precision, TP, so, st); ++n; mark(KK_STAGE);
         in = out_s;
     }
-    launch_step_end(TP.P, s->ctrl, s->limits, s->partials, s->n_tiles, s->dt, s->hist, s->hist_cap, st);
+    launch_step_end(TP.P, s->ctrl, s->limits, s->partials, s->n_tiles, s->dt, s->keys, s->hist, s->hist_cap, st);
     ++n; mark(KK_END);
     return n;
 }
@@ -555,6 +670,7 @@ int fv_run(fv_solver* s, const fv_run_options* o, fv_run_info* info) {
         for (int k = 0; k < kMaxV; ++k) hc.R[k] = 1.0;
         hc.active = 1;
         CK(cudaMemcpyAsync(s->ctrl, &hc, sizeof(hc), cudaMemcpyHostToDevice, st));
+        if (s->case_time) CK(cudaMemsetAsync(s->case_time, 0, (size_t)s->n_cases * 8, st));
         // run(): initial ghost fill with zeroed gx, gy, limiters (explicit.cpp:712)
         exact::launch_bounds(s->TP.P, s->qbase[0], nullptr, nullptr, nullptr, 1, st);
         sync_shadow(s, 0);
@@ -746,10 +862,11 @@ int fv_stage_dt(fv_solver* s, const double* q, double* dt, int32_t global_min) {
     double* q64; void* qs; unsigned long long* keys;
     CK(T.get((void**)&q64, nq * 8));
     CK(T.get(&qs, nq * s->ssz));
-    CK(T.get((void**)&keys, kDtSlots * 8));
+    const size_t nkeys = (size_t)s->n_cases * kDtSlots;
+    CK(T.get((void**)&keys, nkeys * 8));
     int rc = h2d(s, q, q64, qs, s->V);
     if (rc) return rc;
-    CK(cudaMemsetAsync(keys, 0xFF, kDtSlots * 8, s->stream));
+    CK(cudaMemsetAsync(keys, 0xFF, nkeys * 8, s->stream));
     TileParams TP = s->TP;
     TP.P.global_dt = global_min ? 1 : 0;
     TileIO io{};
@@ -761,18 +878,27 @@ int fv_stage_dt(fv_solver* s, const double* q, double* dt, int32_t global_min) {
     std::vector<double> dd(s->n_total);
     if ((rc = d2h(s, s->dt, dd.data(), 1))) return rc;
     if (global_min) {
-        unsigned long long hk[kDtSlots], key = ~0ull;
-        CK(cudaMemcpy(hk, keys, sizeof(hk), cudaMemcpyDeviceToHost));
-        for (int i = 0; i < kDtSlots; ++i) key = hk[i] < key ? hk[i] : key;
-        double mn;
-        if (key == ~0ull) {
-            mn = std::nan("");
-        } else {
-            unsigned long long b = (key & 0x8000000000000000ull) ? (key & 0x7fffffffffffffffull) : ~key;
-            std::memcpy(&mn, &b, 8);
+        // per case (one for a single mesh): min over its real and ghost cells;
+        // a NaN in the case's dt[0] wins (min_dt, explicit.cpp:555-564)
+        std::vector<unsigned long long> hk(nkeys);
+        CK(cudaMemcpy(hk.data(), keys, nkeys * 8, cudaMemcpyDeviceToHost));
+        std::vector<int64_t> ro = s->case_real_off, bo = s->case_bound_off;
+        if (s->n_cases == 1) { ro = {0, s->n_real}; bo = {0, s->n_bound}; }
+        for (int k = 0; k < s->n_cases; ++k) {
+            unsigned long long key = ~0ull;
+            for (int i = 0; i < kDtSlots; ++i) key = hk[(size_t)k * kDtSlots + i] < key ? hk[(size_t)k * kDtSlots + i] : key;
+            double mn;
+            if (key == ~0ull) {
+                mn = std::nan("");
+            } else {
+                unsigned long long b = (key & 0x8000000000000000ull) ? (key & 0x7fffffffffffffffull) : ~key;
+                std::memcpy(&mn, &b, 8);
+            }
+            const double d0 = dd[(size_t)ro[k]];
+            if (d0 != d0) mn = d0;
+            for (int64_t r = ro[k]; r < ro[k + 1]; ++r) dd[(size_t)r] = mn;
+            for (int64_t b = bo[k]; b < bo[k + 1]; ++b) dd[(size_t)(s->n_real + b)] = mn;
         }
-        if (dd[0] != dd[0]) mn = dd[0];
-        for (auto& v : dd) v = mn;
     }
     std::memcpy(dt, dd.data(), dd.size() * 8);
     return FV_OK;
@@ -803,6 +929,7 @@ __global__ void k_noalloc_dt_fill(const unsigned long long* keys, const double* 
 
 int fv_stage_dt_noalloc(fv_solver* s, const double* q_device, double* dt_device, int32_t global_min, void* stream) {
     if (!s || !q_device || !dt_device) return fail(FV_ERR_ARG, "fv_stage_dt_noalloc: null argument");
+    if (s->n_cases > 1) return fail(FV_ERR_UNSUPPORTED, "fv_stage_dt_noalloc: batches of cases use fv_stage_dt");
     const size_t nt = (size_t)s->n_total, V = (size_t)s->V;
     const size_t need = align256(kDtSlots * 8) + align256(nt * 8) + align256(nt * V * 8) +
                         (s->f32 ? align256(nt * V * 4) : 0);

@@ -56,6 +56,13 @@ struct Params {
     int n_groups;
     int group_bc[kMaxGroups];
     double group_bv[kMaxGroups * 4];
+    // batches of independent cases (n_cases > 1): each case has its own
+    // global dt minimum (64 key slots per case) and its own time
+    int n_cases;
+    const int32_t* cell_case;   // [n_total] case of each device cell
+    const int32_t* tile_case;   // [n_tiles] case of a tile's cells, -1 if the tile spans two cases
+    const int32_t* case_cell0;  // [n_cases] device index of each case's reference cell 0
+    double* case_time;          // [n_cases]
 };
 
 }  // namespace fvgpu

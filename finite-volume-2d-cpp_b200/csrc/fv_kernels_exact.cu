@@ -55,9 +55,8 @@ __device__ __forceinline__ void store_cell(double* __restrict__ a, int c, const 
 }
 
 // ------------------------------------------------------------ step control --
-__global__ void k_step_begin(Ctrl* c, const RunLimits* L, int V) {
-    c->dtkeys[threadIdx.x] = ~0ull;
-    c->dtkeys[threadIdx.x + 32] = ~0ull;
+__global__ void k_step_begin(Ctrl* c, const RunLimits* L, int V, unsigned long long* keys, int nkeys) {
+    for (int i = threadIdx.x; i < nkeys; i += blockDim.x) keys[i] = ~0ull;
     if (threadIdx.x != 0) return;
     double Rmax;
     if (c->step > 0) {
@@ -74,8 +73,21 @@ __global__ void k_step_begin(Ctrl* c, const RunLimits* L, int V) {
 // Residual norms, step/time bookkeeping and print records
 // (explicit.cpp:752-800).  Partial sums are reduced in a fixed order.
 __global__ void k_step_end(Params P, Ctrl* c, const RunLimits* L, const double* partials, int nblocks,
-                           const double* dt, PrintRec* hist, int hist_cap) {
+                           const double* dt, const unsigned long long* keys, PrintRec* hist, int hist_cap) {
     if (!c->active) return;
+    if (P.n_cases > 1) {
+        // each case of a batch keeps its own time: time += dt[0] of that case
+        for (int k = threadIdx.x; k < P.n_cases; k += blockDim.x) {
+            const double d0 = dt[P.case_cell0[k]];
+            double dk = d0;
+            if (P.global_dt && d0 == d0) {
+                unsigned long long key = ~0ull;
+                for (int i = 0; i < 64; ++i) key = keys[(size_t)k * 64 + i] < key ? keys[(size_t)k * 64 + i] : key;
+                dk = dkey_inv(key);
+            }
+            P.case_time[k] += dk;
+        }
+    }
     __shared__ double red[kBlock][kMaxV];
     const int V = P.V;
     if (c->need_R) {
@@ -106,17 +118,18 @@ __global__ void k_step_end(Params P, Ctrl* c, const RunLimits* L, const double* 
         r.time = c->time;
         for (int k = 0; k < V; ++k) r.R[k] = (c->step == 0) ? 1.0 : c->R[k];
     }
-    const double dt0 = P.global_dt ? global_dt_value(P, dt, c->dtkeys) : dt[P.cell0];
+    // case 0 of a batch: its reference cell 0 is P.cell0 and its keys come first
+    const double dt0 = P.global_dt ? global_dt_value(P, dt, keys) : dt[P.cell0];
     c->step += 1;
     c->time += dt0;
 }
 
-void launch_step_begin(Ctrl* c, const RunLimits* lim, int V, cudaStream_t st) {
-    k_step_begin<<<1, 32, 0, st>>>(c, lim, V);
+void launch_step_begin(Ctrl* c, const RunLimits* lim, int V, unsigned long long* keys, int nkeys, cudaStream_t st) {
+    k_step_begin<<<1, 128, 0, st>>>(c, lim, V, keys, nkeys);
 }
 void launch_step_end(const Params& P, Ctrl* c, const RunLimits* lim, const double* partials, int nblocks,
-                     const double* dt, PrintRec* hist, int hist_cap, cudaStream_t st) {
-    k_step_end<<<1, kBlock, 0, st>>>(P, c, lim, partials, nblocks, dt, hist, hist_cap);
+                     const double* dt, const unsigned long long* keys, PrintRec* hist, int hist_cap, cudaStream_t st) {
+    k_step_end<<<1, kBlock, 0, st>>>(P, c, lim, partials, nblocks, dt, keys, hist, hist_cap);
 }
 
 namespace exact {

@@ -198,19 +198,25 @@ std::string build_geometry(HostMesh& m) {
 
 void build_device_numbering(HostMesh& m) {
     const int64_t nc = m.n_real, nt = m.n_total, E = m.n_edges;
-    double xmin = 1e300, xmax = -1e300, ymin = 1e300, ymax = -1e300;
-    for (int64_t c = 0; c < nc; ++c) {
-        xmin = std::min(xmin, m.ccx[c]); xmax = std::max(xmax, m.ccx[c]);
-        ymin = std::min(ymin, m.ccy[c]); ymax = std::max(ymax, m.ccy[c]);
-    }
+    // Hilbert key within each case's bounding box; the case index above it
+    // keeps the cases of a batch contiguous (a single mesh is one case)
+    std::vector<int64_t> offs = m.case_real_off;
+    if (offs.size() < 2) offs = {0, nc};
     const int order = 16;
-    const double span = std::max(std::max(xmax - xmin, ymax - ymin), 1e-300);
-    const double scale = ((1u << order) - 1) / span;
     std::vector<uint64_t> key(nc);
-    for (int64_t c = 0; c < nc; ++c) {
-        uint32_t qx = (uint32_t)((m.ccx[c] - xmin) * scale);
-        uint32_t qy = (uint32_t)((m.ccy[c] - ymin) * scale);
-        key[c] = hilbert_d(qx, qy, order);
+    for (size_t k = 0; k + 1 < offs.size(); ++k) {
+        double xmin = 1e300, xmax = -1e300, ymin = 1e300, ymax = -1e300;
+        for (int64_t c = offs[k]; c < offs[k + 1]; ++c) {
+            xmin = std::min(xmin, m.ccx[c]); xmax = std::max(xmax, m.ccx[c]);
+            ymin = std::min(ymin, m.ccy[c]); ymax = std::max(ymax, m.ccy[c]);
+        }
+        const double span = std::max(std::max(xmax - xmin, ymax - ymin), 1e-300);
+        const double scale = ((1u << order) - 1) / span;
+        for (int64_t c = offs[k]; c < offs[k + 1]; ++c) {
+            uint32_t qx = (uint32_t)((m.ccx[c] - xmin) * scale);
+            uint32_t qy = (uint32_t)((m.ccy[c] - ymin) * scale);
+            key[c] = ((uint64_t)k << 32) | hilbert_d(qx, qy, order);
+        }
     }
     m.new2ref.resize(nt);
     std::iota(m.new2ref.begin(), m.new2ref.begin() + nc, 0);

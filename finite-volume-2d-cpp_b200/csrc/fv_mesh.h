@@ -24,6 +24,12 @@ struct HostMesh {
     std::vector<double> area, ccx, ccy;                  // [n_total]
     std::vector<uint32_t> bound_edges;                   // [n_bound]
 
+    // ---- batches of independent cases (fv_mesh_create_batch) ----
+    // Case k owns reference real cells [case_real_off[k], case_real_off[k+1])
+    // and boundary ghosts [case_bound_off[k], case_bound_off[k+1]).  Empty for
+    // a single mesh.  Device numbering keeps each case's cells contiguous.
+    std::vector<int64_t> case_real_off, case_bound_off;
+
     // ---- device numbering ----
     // new index of reference cell r: ref2new[r]; reference index of new cell n: new2ref[n].
     // Real cells occupy [0, n_real), ghosts [n_real, n_total) in both numberings.

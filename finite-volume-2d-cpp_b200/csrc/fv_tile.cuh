@@ -67,7 +67,7 @@ struct TileIO {
     double alpha;
     Ctrl* ctrl;                // nullptr: always active, dt from dt[]
     double* partials;          // [n_tiles][V] or nullptr
-    unsigned long long* dtkeys;  // [kDtSlots] ordered keys of the global dt minimum
+    unsigned long long* dtkeys;  // [n_cases][kDtSlots] ordered keys of the global dt minimum
     int write_f64;             // FP32 mode: also write q_out (last stage)
 };
 
@@ -361,15 +361,21 @@ __global__ void __launch_bounds__(kTileMax) k_tile_dt(TileParams TP, TileIO io) 
         }
     }
     if (P.global_dt && io.dtkeys != nullptr) {
-        // block minimum, then one atomic per block spread over kDtSlots slots
+        const int tc = P.n_cases > 1 ? P.tile_case[t] : 0;
+        if (tc >= 0) {
+            // block minimum, then one atomic per block spread over kDtSlots slots
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) kmin = kmin_(kmin, __shfl_xor_sync(0xffffffffu, kmin, o));
-        if ((threadIdx.x & 31) == 0) wmin[threadIdx.x >> 5] = kmin;
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            unsigned long long b = ~0ull;
-            for (int i = 0; i < (int)(blockDim.x >> 5); ++i) b = kmin_(b, wmin[i]);
-            if (b != ~0ull) atomicMin(io.dtkeys + (blockIdx.x % kDtSlots), b);
+            for (int o = 16; o > 0; o >>= 1) kmin = kmin_(kmin, __shfl_xor_sync(0xffffffffu, kmin, o));
+            if ((threadIdx.x & 31) == 0) wmin[threadIdx.x >> 5] = kmin;
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                unsigned long long b = ~0ull;
+                for (int i = 0; i < (int)(blockDim.x >> 5); ++i) b = kmin_(b, wmin[i]);
+                if (b != ~0ull) atomicMin(io.dtkeys + (size_t)tc * kDtSlots + (blockIdx.x % kDtSlots), b);
+            }
+        } else if (l < nown && kmin != ~0ull) {
+            // a tile across two cases of a batch: each cell (and its ghosts) to its own case
+            atomicMin(io.dtkeys + (size_t)P.cell_case[t * T + l] * kDtSlots + (l % kDtSlots), kmin);
         }
     }
 }
@@ -553,8 +559,11 @@ __global__ void __launch_bounds__(kTileMax) k_tile_stage(TileParams TP, TileIO i
     stage_records<M, V, ORDER2, ORDER2>(TP, io, inf, c0, nown, rec);
     if (ORDER2) stage_edges<S, false, true>(TP, inf, sij, snx, sny, sle, nullptr, sxf, syf);
     else stage_edges<S, false, false>(TP, inf, sij, snx, sny, sle, nullptr, nullptr, nullptr);
-    if (global_dt && threadIdx.x < 32) {
-        unsigned long long k = kmin_(io.dtkeys[threadIdx.x], io.dtkeys[threadIdx.x + 32]);
+    // the tile's case (batches); -1: the tile spans two cases
+    const int tc = (global_dt && P.n_cases > 1) ? P.tile_case[t] : 0;
+    if (global_dt && tc >= 0 && threadIdx.x < 32) {
+        const unsigned long long* keys = io.dtkeys + (size_t)tc * kDtSlots;
+        unsigned long long k = kmin_(keys[threadIdx.x], keys[threadIdx.x + 32]);
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) k = kmin_(k, __shfl_xor_sync(0xffffffffu, k, o));
         if (threadIdx.x == 0) s_dtkey = k;
@@ -650,8 +659,19 @@ __global__ void __launch_bounds__(kTileMax) k_tile_stage(TileParams TP, TileIO i
             for (int k = 0; k < V; ++k) qt[k] *= rA;
         }
         if (global_dt) {
-            const double d0 = io.dt[P.cell0];
-            dtc = (d0 != d0) ? d0 : tkey_inv(s_dtkey);
+            // min_dt (explicit.cpp:555-564) of this cell's case; a NaN in its dt[0] wins
+            unsigned long long key = s_dtkey;
+            int cell0 = P.cell0;
+            if (P.n_cases > 1) {
+                const int k = tc >= 0 ? tc : P.cell_case[c];
+                cell0 = P.case_cell0[k];
+                if (tc < 0) {
+                    key = ~0ull;
+                    for (int i = 0; i < kDtSlots; ++i) key = kmin_(key, io.dtkeys[(size_t)k * kDtSlots + i]);
+                }
+            }
+            const double d0 = io.dt[cell0];
+            dtc = (d0 != d0) ? d0 : tkey_inv(key);
         }
         double qnew[V];
         if constexpr (M::exact) {

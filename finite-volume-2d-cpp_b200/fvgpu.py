@@ -116,6 +116,51 @@ class Mesh:
             names.append(buf.value.decode())
         return cls(h.value, names)
 
+    @classmethod
+    def batch(cls, meshes):
+        """Independent cases as one mesh (fv_mesh_create_batch).  Every case
+        must list the same boundary group names in the same order."""
+        names = meshes[0].group_names
+        for m in meshes:
+            if m.group_names != names:
+                raise ValueError("batched cases must share their boundary group names")
+        arr = (C.c_void_p * len(meshes))(*[m._h.value for m in meshes])
+        h = C.c_void_p()
+        _check(lib().fv_mesh_create_batch(C.c_int32(len(meshes)), arr, C.byref(h)))
+        out = cls(h.value, names)
+        out._cases = list(meshes)
+        return out
+
+    @property
+    def n_cases(self):
+        return int(lib().fv_mesh_case_count(self._h))
+
+    def case_offsets(self):
+        """(real_off, bound_off), each [n_cases + 1]: case k's real cells are
+        reference cells real_off[k]:real_off[k+1], its ghosts n_real + bound_off[k]:bound_off[k+1]."""
+        n = self.n_cases
+        ro = np.zeros(n + 1, np.int64); bo = np.zeros(n + 1, np.int64)
+        _check(lib().fv_mesh_case_offsets(self._h, _p(ro, _i64p), _p(bo, _i64p)))
+        return ro, bo
+
+    def split(self, a, V):
+        """Per-case arrays ([n_total_k * V], reference order) from a batch array."""
+        ro, bo = self.case_offsets()
+        a = np.asarray(a).reshape(self.n_total, V)
+        return [np.concatenate([a[ro[k]:ro[k + 1]], a[self.n_real + bo[k]:self.n_real + bo[k + 1]]]).ravel()
+                for k in range(len(ro) - 1)]
+
+    def join(self, parts, V):
+        """Batch array from per-case arrays (the inverse of split)."""
+        ro, bo = self.case_offsets()
+        out = np.zeros((self.n_total, V))
+        for k, p in enumerate(parts):
+            p = np.asarray(p).reshape(-1, V)
+            nr = ro[k + 1] - ro[k]
+            out[ro[k]:ro[k + 1]] = p[:nr]
+            out[self.n_real + bo[k]:self.n_real + bo[k + 1]] = p[nr:]
+        return out.ravel()
+
     def __del__(self):
         try:
             if self._h and _lib is not None:
@@ -227,6 +272,12 @@ class Solver:
         info = _RunInfo()
         _check(lib().fv_run(self._h, C.byref(o), C.byref(info)))
         return dict(step=info.step, time=info.time, R=np.array(info.R[: self.V]), R0=np.array(info.R0[: self.V]))
+
+    def case_times(self):
+        """Each case's accumulated time (one entry for a single mesh)."""
+        t = np.zeros(self.mesh.n_cases)
+        _check(lib().fv_batch_times(self._h, _p(t)))
+        return t
 
     def continue_from(self, other: "Solver"):
         """Take over another solver's state and run control (same mesh), so

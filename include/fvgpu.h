@@ -119,6 +119,22 @@ int fv_mesh_create(int64_t n_nodes, const double* nodes_x, const double* nodes_y
 /* Gmsh MSH 4.1 ASCII file (single partition) -> mesh; boundary groups are
  * the physical names of the boundary curves, in order of first use. */
 int fv_mesh_read_msh(const char* path, fv_mesh** out);
+/* A batch of independent cases as one mesh (the disjoint union of the case
+ * meshes): reference numbering = the real cells of case 0, 1, ..., then the
+ * ghosts of case 0, 1, ...; boundary groups are merged by name.  A solver on
+ * a batch advances every case in the same launches, each case with its own
+ * global dt minimum (min_dt over that case's cells only) and its own time
+ * (fv_batch_times).  fv_run's step counter, residual norms (sums over all
+ * cases), max_time (checked against case 0's time) and print records are
+ * shared by the batch.  No counterpart in the reference, which runs one case
+ * per process. */
+int fv_mesh_create_batch(int32_t n_cases, const fv_mesh* const* cases, fv_mesh** out);
+/* 1 for a single mesh. */
+int fv_mesh_case_count(const fv_mesh* m);
+/* real_off[n_cases + 1], bound_off[n_cases + 1]: case k's real cells are
+ * reference cells [real_off[k], real_off[k+1]), its ghosts are reference
+ * cells n_real + [bound_off[k], bound_off[k+1]). */
+int fv_mesh_case_offsets(const fv_mesh* m, int64_t* real_off, int64_t* bound_off);
 void fv_mesh_destroy(fv_mesh* m);
 /* out[5] = {n_nodes, n_real, n_total, n_edges, n_bound} */
 int fv_mesh_sizes(const fv_mesh* m, int64_t* out);
@@ -164,6 +180,8 @@ int fv_run(fv_solver* s, const fv_run_options* opt, fv_run_info* info);
  * residual normalisation.  Both solvers must be on one device.  No
  * counterpart in the reference (explicit.cpp:657-817 runs in one precision). */
 int fv_solver_continue_from(fv_solver* dst, fv_solver* src);
+/* times[n_cases]: each case's accumulated time (time += that case's dt[0]). */
+int fv_batch_times(fv_solver* s, double* times);
 /* R after the last step (sqrt of sum qt^2 A over real cells, un-normalised). */
 int fv_residuals(fv_solver* s, double* R);
 /* Returns FV_ERR_NONFINITE if any real-cell state is NaN/Inf, or if an
