@@ -51,23 +51,42 @@ ALGO_BYTES = {
 
 
 def build_workload(name):
+    """(element mesh or list of case meshes, physics, RK stages, ic(mesh, geometry) -> q, description)"""
     if name == "step":
         em = meshgen.forward_step()
         ph = P.forward_step(order2=True, limiter="venkat", K=5.0, cfl=0.8)
         # the reference scheme goes non-finite at t ~ 0.005 on this mesh; the
         # positivity guard keeps the run physical (see DESIGN.md)
         ph.positivity_guard = True
-        return em, ph, P.RK5_ALPHA, lambda ccx, n: P.ic_forward_step(n), \
+        return em, ph, P.RK5_ALPHA, lambda mesh, geo: P.ic_forward_step(mesh.n_total).ravel(), \
             "forward step Mach 3, 2nd-order GG + Venkatakrishnan K=5 + positivity guard, RK5, CFL 0.8"
     if name == "sod":
         em = meshgen.sod_strip(400, 40)
-        return em, P.sod(cfl=0.5), P.RK1_ALPHA, lambda ccx, n: P.ic_sod(ccx), \
+        return em, P.sod(cfl=0.5), P.RK1_ALPHA, lambda mesh, geo: P.ic_sod(geo["ccx"]).ravel(), \
             "Sod shock tube 400x40x2, 1st-order Roe, RK1, CFL 0.5"
     if name == "naca":
         em = meshgen.naca_ogrid()
-        return em, P.naca(), P.RK5_ALPHA, lambda ccx, n: P.ic_naca(n), \
+        return em, P.naca(), P.RK5_ALPHA, lambda mesh, geo: P.ic_naca(mesh.n_total).ravel(), \
             "NACA 0012 O-grid 1024x512x2, M 0.8, Michalak, local dt, RK5"
+    if name == "batch":
+        nx, states = meshgen.riemann_strip_sizes()
+        ems = [meshgen.riemann_strip(n) for n in nx]
+
+        def ic(mesh, geo):
+            ccx = mesh.split(geo["ccx"], 1)
+            return mesh.join([P.ic_riemann(c, st[:3], st[3:]) for c, st in zip(ccx, states)], 4)
+
+        return ems, P.riemann_strip(), P.RK5_ALPHA, ic, \
+            (f"{len(ems)} independent Riemann strips (nx x 8 x 2 triangles, 2k-200k cells log-uniform, seed 4), "
+             f"2nd-order GG + Venkatakrishnan K=5, RK5, CFL 0.8, per-case global dt, one batched solver")
     raise SystemExit(f"unknown workload {name}")
+
+
+def make_mesh(em):
+    import fvgpu
+    if isinstance(em, list):
+        return fvgpu.Mesh.batch([fvgpu.Mesh.from_elements(e) for e in em])
+    return fvgpu.Mesh.from_elements(em)
 
 
 class ClockSampler:
@@ -213,10 +232,14 @@ def measure_mode(args, em, mesh, geo, ph, alpha, ic, precision, local, dist, wor
     import torch
     import fvgpu
 
-    s = fvgpu.Solver(mesh, ph, precision, device=local, tile_cells=args.tile_cells)
+    q0 = ic(mesh, geo)
+    if args.tile_cells < 0:  # autotuned tile size
+        s = fvgpu.Solver.create_tuned(mesh, ph, precision, q0, alpha=alpha, steps=3, device=local)
+    else:
+        s = fvgpu.Solver(mesh, ph, precision, device=local, tile_cells=args.tile_cells)
+        s.tile_cells = args.tile_cells or 128
     stream = torch.cuda.Stream(device=local)
     s.set_stream(stream.cuda_stream)
-    q0 = ic(geo["ccx"], mesh.n_total).ravel()
     s.set_state(q0)
     stages = len(alpha)
     N = mesh.n_real
@@ -243,7 +266,7 @@ def measure_mode(args, em, mesh, geo, ph, alpha, ic, precision, local, dist, wor
     ms_max = replicas.max_over_ranks(ms, dist, device=f"cuda:{local}")
     out = dict(solver=s, stream=stream, value=world * N * stages * args.steps / (ms_max / 1e3),
                ms_per_step=ms_max / args.steps, launches=int(launches), clocks=clk.summary(),
-               state_finite=s.check_state() == 0, q_final=s.get_state())
+               state_finite=s.check_state() == 0, q_final=s.get_state(), case_times=s.case_times())
     # per-kernel device timing (events around every kernel, same stream)
     prof_steps = max(2, min(args.steps, 10))
     ms_k = np.zeros(5); cnt_k = np.zeros(5, np.int64)
@@ -311,19 +334,48 @@ def l2_rho_p(q, q_ref, n_real, gamma=1.4):
     return {"density": l2(ra, rb), "pressure": l2(pa, pb)}
 
 
+def batch_error_vs_exact(mesh, geo, q, times, states, gamma=1.4):
+    """L2 density / pressure error of a batch of Riemann strips against the
+    exact Riemann solution at each case's own time, area-weighted over all
+    real cells of the batch, and the worst case."""
+    import riemann
+    qs = mesh.split(q, 4)
+    ccx = mesh.split(geo["ccx"], 1)
+    area = mesh.split(geo["area"], 1)
+    ro, _ = mesh.case_offsets()
+    num_r = num_p = den = 0.0
+    worst = 0.0
+    for k in range(len(qs)):
+        n = int(ro[k + 1] - ro[k])
+        x, A = ccx[k][:n], area[k][:n]
+        ra, _, pa = riemann.sample(x, times[k], states[k][:3], states[k][3:], gamma)
+        qq = qs[k].reshape(-1, 4)[:n]
+        r = qq[:, 0]
+        p = (gamma - 1) * (qq[:, 3] - 0.5 * (qq[:, 1] ** 2 + qq[:, 2] ** 2) / r)
+        er, ep = float(((r - ra) ** 2 * A).sum()), float(((p - pa) ** 2 * A).sum())
+        num_r += er; num_p += ep; den += float(A.sum())
+        worst = max(worst, np.sqrt(er / A.sum()))
+    return {"density": float(np.sqrt(num_r / den)), "pressure": float(np.sqrt(num_p / den)),
+            "density_worst_case": float(worst)}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=500)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="step", choices=["step", "sod", "naca"])
+    ap.add_argument("--workload", default="step", choices=["step", "sod", "naca", "batch"])
     ap.add_argument("--precision", default="all", choices=["all", "fp64_exact", "fp64", "fp32"],
                     help="all: FP32-bulk (headline) and plain FP64 in one line")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--tile-cells", type=int, default=0, help="cells per tile (0: library default)")
+    ap.add_argument("--tile-cells", type=int, default=None,
+                    help="cells per tile: 64/128/256, 0 = library default (128), -1 = autotuned "
+                         "(default: autotuned for the batch workload, else 0)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    if args.tile_cells is None:
+        args.tile_cells = -1 if args.workload == "batch" else 0
     if args.impl == "reference":
         return run_reference_arm(args)
 
@@ -341,7 +393,7 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
 
     em, ph, alpha, ic, desc = build_workload(args.workload)
-    mesh = fvgpu.Mesh.from_elements(em)
+    mesh = make_mesh(em)
     geo = mesh.geometry()
     modes = ["fp64", "fp32"] if args.precision == "all" else [args.precision]
     res = {}
@@ -356,7 +408,9 @@ def main():
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64" if head == "fp32" else "f64",
                 "data": "synthetic",
                 "config": {"workload": desc, "n_real_cells": mesh.n_real, "n_edges": mesh.n_edges,
-                           "stages": len(alpha), "precision": head, "tile_cells": args.tile_cells or 128,
+                           "stages": len(alpha), "precision": head, "n_cases": mesh.n_cases,
+                           "tile_cells": m["solver"].tile_cells,
+                           "tile_choice": "autotuned" if args.tile_cells < 0 else "fixed",
                            "l2": "inputs larger than L2 (working set > 126 MB), no flush",
                            "parallelism": f"{world} independent replicas" if world > 1 else "single GPU"},
                 "e2e": e2e, "gpu_launches": m["launches"], "roofline": m["roofline"],
@@ -371,7 +425,14 @@ def main():
                                                              mesh.n_real),
                                     "after_steps": args.warmup + args.steps,
                                     "speedup": res["fp32"]["value"] / res["fp64"]["value"]}
-        if not args.no_cpu_baseline and world == 1:
+        if args.workload == "batch":
+            _, states = meshgen.riemann_strip_sizes()
+            errs = {p: batch_error_vs_exact(mesh, geo, r["q_final"], r["case_times"], states) for p, r in res.items()}
+            line["l2_error_vs_exact_riemann"] = errs
+            if "fp64" in errs and "fp32" in errs:
+                line["l2_error_vs_exact_riemann"]["fp32_minus_fp64_density"] = \
+                    errs["fp32"]["density"] - errs["fp64"]["density"]
+        if not args.no_cpu_baseline and world == 1 and args.workload == "step":
             r = reference_samples(em, 1, 1, 25)
             if r is not None:
                 line["cpu_baseline"] = {"value": r[0], "unit": UNIT, "cores": 1, "kind": "reference",

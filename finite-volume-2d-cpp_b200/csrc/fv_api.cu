@@ -457,6 +457,47 @@ int fv_solver_destroy(fv_solver* s) {
     return FV_OK;
 }
 
+int fv_solver_create_tuned(const fv_mesh* fm, const fv_physics* ph, int32_t precision, int32_t device,
+                           const double* q, const double* alpha, int32_t n_alpha, int32_t n_steps,
+                           fv_solver** out, int32_t* tile_cells, double* ms_per_step) {
+    if (!fm || !ph || !q || !alpha || n_alpha < 1 || n_steps < 1 || !out)
+        return fail(FV_ERR_ARG, "fv_solver_create_tuned: invalid arguments");
+    fv_solver* best = nullptr;
+    double best_ms = 0.0;
+    int best_t = 0;
+    for (int t : {64, 128, 256}) {
+        fv_solver_options o{t};
+        fv_solver* s = nullptr;
+        int rc = fv_solver_create_ex(fm, ph, precision, device, &o, &s);
+        if (rc == FV_ERR_MESH) continue;  // tile halo too large for this size
+        if (rc) { fv_solver_destroy(best); return rc; }
+        // one untimed step (graph capture), then n_steps timed on the device
+        fv_run_options ro{};
+        ro.max_step = 1; ro.max_time = 1e300; ro.tolerance = -1.0; ro.print_interval = 1ull << 62;
+        ro.n_alpha = n_alpha; ro.alpha = alpha; ro.restart = 1;
+        fv_run_info info{};
+        if ((rc = fv_set_state(s, q)) || (rc = fv_run(s, &ro, &info))) { fv_solver_destroy(s); fv_solver_destroy(best); return rc; }
+        ro.max_step = 1 + (uint64_t)n_steps; ro.restart = 0;
+        if ((rc = fv_run(s, &ro, &info))) { fv_solver_destroy(s); fv_solver_destroy(best); return rc; }
+        const double ms = s->last_ms / n_steps;
+        if (!best || ms < best_ms) {
+            fv_solver_destroy(best);
+            best = s; best_ms = ms; best_t = t;
+        } else {
+            fv_solver_destroy(s);
+        }
+    }
+    if (!best) return fail(FV_ERR_MESH, "fv_solver_create_tuned: no tile size fits this mesh");
+    int rc = fv_set_state(best, q);
+    if (rc) { fv_solver_destroy(best); return rc; }
+    CK(cudaMemsetAsync(best->ctrl, 0, sizeof(Ctrl), best->stream));
+    CK(cudaStreamSynchronize(best->stream));
+    *out = best;
+    if (tile_cells) *tile_cells = best_t;
+    if (ms_per_step) *ms_per_step = best_ms;
+    return FV_OK;
+}
+
 int fv_solver_set_stream(fv_solver* s, void* stream) {
     if (!s) return fail(FV_ERR_ARG, "null solver");
     CK(cudaSetDevice(s->device));

@@ -214,6 +214,28 @@ class Solver:
                                          opt, C.byref(h)))
         self._h = h
 
+    @classmethod
+    def create_tuned(cls, mesh: Mesh, ph: _phys.Physics, precision: str, q, alpha=_phys.RK5_ALPHA,
+                     steps: int = 5, device: int = 0):
+        """The solver with the fastest tile size for this mesh and physics
+        (fv_solver_create_tuned); its state is q, step 0."""
+        self = cls.__new__(cls)
+        self.mesh = mesh
+        self.phys = ph
+        self.V = ph.V
+        self.precision = precision
+        self._ps = physics_struct(ph, mesh.group_names)
+        q = np.ascontiguousarray(q, np.float64)
+        a = np.ascontiguousarray(alpha, np.float64)
+        h = C.c_void_p(); t = C.c_int32(); ms = C.c_double()
+        _check(lib().fv_solver_create_tuned(mesh._h, C.byref(self._ps), C.c_int32(PREC[precision]),
+                                            C.c_int32(device), _p(q), _p(a), C.c_int32(a.size), C.c_int32(steps),
+                                            C.byref(h), C.byref(t), C.byref(ms)))
+        self._h = h
+        self.tile_cells = t.value
+        self.tuned_ms_per_step = ms.value
+        return self
+
     def close(self):
         if self._h:
             lib().fv_solver_destroy(self._h)

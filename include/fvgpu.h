@@ -159,6 +159,14 @@ typedef struct {
 } fv_solver_options;
 int fv_solver_create_ex(const fv_mesh* m, const fv_physics* ph, int32_t precision, int32_t device,
                         const fv_solver_options* opt, fv_solver** out);
+/* Autotuned creation: builds the solver with each tile size (64, 128, 256
+ * cells per tile = threads per CTA), times n_steps steps of the given RK
+ * stages from state q on the device (after one untimed step that captures the
+ * step graph), and keeps the fastest.  The returned solver holds state q
+ * again, step 0; tile_cells and ms_per_step (may be NULL) report the choice. */
+int fv_solver_create_tuned(const fv_mesh* m, const fv_physics* ph, int32_t precision, int32_t device,
+                           const double* q, const double* alpha, int32_t n_alpha, int32_t n_steps,
+                           fv_solver** out, int32_t* tile_cells, double* ms_per_step);
 int fv_solver_destroy(fv_solver* s);
 /* cudaStream_t as void*; NULL = the solver's own stream */
 int fv_solver_set_stream(fv_solver* s, void* stream);

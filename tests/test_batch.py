@@ -120,3 +120,38 @@ def test_batch_stage_dt_is_per_case(oracle):
         g = oracle.build_mesh(em)
         assert bits_equal(got[k], oracle.calc_dt(g, oracle.physics(ph, em.group_names), qk, True)), k
     s.close()
+
+
+@pytest.mark.gpu
+def test_batch_fp32_error_equals_fp64_error_against_exact_riemann():
+    """FP32-bulk and FP64 reach the same L2 density error against the exact
+    Riemann solution (area-weighted over the batch) within 1e-4."""
+    import fvgpu
+    import riemann
+
+    nx = [300, 520, 800, 1250, 2000, 410, 950]
+    rng = np.random.default_rng(4)
+    states = [(rng.uniform(0.1, 1.0), rng.uniform(-0.5, 0.5), rng.uniform(0.1, 1.0),
+               rng.uniform(0.1, 1.0), rng.uniform(-0.5, 0.5), rng.uniform(0.1, 1.0)) for _ in nx]
+    parts = [fvgpu.Mesh.from_elements(meshgen.riemann_strip(n, 8)) for n in nx]
+    b = fvgpu.Mesh.batch(parts)
+    geo = b.geometry()
+    ccx, area = b.split(geo["ccx"], 1), b.split(geo["area"], 1)
+    q0 = b.join([P.ic_riemann(c, st[:3], st[3:]) for c, st in zip(ccx, states)], 4)
+    errs = {}
+    for prec in ("fp64", "fp32"):
+        s = fvgpu.Solver(b, P.riemann_strip(), prec)
+        s.set_state(q0)
+        s.run(300, print_interval=10 ** 9)
+        qs, times = b.split(s.get_state(), 4), s.case_times()
+        num = den = 0.0
+        for k, m in enumerate(parts):
+            n = m.n_real
+            ra, _, _ = riemann.sample(ccx[k][:n], times[k], states[k][:3], states[k][3:])
+            num += float(((qs[k].reshape(-1, 4)[:n, 0] - ra) ** 2 * area[k][:n]).sum())
+            den += float(area[k][:n].sum())
+        errs[prec] = np.sqrt(num / den)
+        s.close()
+    print(f"batch L2 density error vs exact Riemann: fp64 {errs['fp64']:.4e} fp32 {errs['fp32']:.4e}")
+    assert errs["fp64"] < 0.02
+    assert abs(errs["fp32"] - errs["fp64"]) <= 1e-4
