@@ -13,6 +13,7 @@
 #include "fv_launch.h"
 #include "fv_mesh.h"
 #include "fv_tile.cuh"
+#include "fv_adjoint.h"
 #include <cmath>
 
 using namespace fvgpu;
@@ -87,6 +88,7 @@ struct fv_solver {
     unsigned long long* keys = nullptr;
     int n_cases = 1;
     double* case_time = nullptr;                           // batches: [n_cases]
+    double* ghost_bv = nullptr;                            // per-ghost boundary states [n_bound][4]
     std::vector<int64_t> case_real_off, case_bound_off;    // batches: host copies
 
     template <class T>
@@ -580,6 +582,32 @@ int fv_solver_continue_from(fv_solver* dst, fv_solver* src) {
         CK(cudaMemcpyAsync(dst->case_time, src->case_time, (size_t)dst->n_cases * 8, cudaMemcpyDeviceToDevice,
                            dst->stream));
     CK(cudaStreamSynchronize(dst->stream));
+    return FV_OK;
+}
+
+int fv_solver_set_ghost_states(fv_solver* s, const double* bv) {
+    if (!s) return fail(FV_ERR_ARG, "fv_solver_set_ghost_states: null solver");
+    if (s->V != 4) return fail(FV_ERR_UNSUPPORTED, "per-ghost boundary states need V = 4");
+    CK(cudaSetDevice(s->device));
+    if (!bv) {
+        s->TP.P.ghost_bv = nullptr;
+    } else {
+        if (!s->ghost_bv) CK(s->alloc(&s->ghost_bv, (size_t)s->n_bound * 4));
+        // reference ghost order -> device ghost order
+        std::vector<int32_t> n2r((size_t)s->n_total);
+        CK(cudaMemcpy(n2r.data(), s->new2ref, n2r.size() * 4, cudaMemcpyDeviceToHost));
+        std::vector<double> dev((size_t)s->n_bound * 4);
+        for (int64_t b = 0; b < s->n_bound; ++b) {
+            const int64_t r = (int64_t)n2r[(size_t)(s->n_real + b)] - s->n_real;
+            for (int k = 0; k < 4; ++k) dev[(size_t)b * 4 + k] = bv[(size_t)r * 4 + k];
+        }
+        CK(cudaMemcpy(s->ghost_bv, dev.data(), dev.size() * 8, cudaMemcpyHostToDevice));
+        s->TP.P.ghost_bv = s->ghost_bv;
+    }
+    // captured step graphs hold the old parameters
+    for (auto& g : s->graphs)
+        if (g.exec) cudaGraphExecDestroy(g.exec);
+    s->graphs.clear();
     return FV_OK;
 }
 
@@ -1091,6 +1119,349 @@ int fv_stage_bounds(fv_solver* s, double* q, const double* gx, const double* gy,
     exact::launch_bounds(s->TP.P, q64, gx64, gy64, l64, 0, s->stream);
     CK(cudaGetLastError());
     return d2h(s, q64, q, s->V);
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------- adjoint ----
+// Discrete adjoint of fv_run's FP64_EXACT step for the inflow-parameter
+// problem: theta = (M, delta_1..delta_nb) sets the free stream (initial
+// state rho_inf, u = M, v = 0, p_inf) and the inflow boundary states (density
+// rho_inf (1 + delta_b) on the inflow faces of bin b, velocity M);
+// loss = sum_n dt_n sum_{faces of loss_group} p(interior) le.  The forward
+// run stores its state every `checkpoint_every` steps; the reverse sweep
+// recomputes each segment storing every stage state, gradient and limiter,
+// then runs the adjoint kernels of fv_adjoint.cu stage by stage backwards.
+struct fv_adjoint {
+    fv_solver* s = nullptr;
+    fv_adjoint_options o{};
+    std::vector<double> alpha;
+    int S = 0;                        // RK stages
+    int nseg = 0;
+    double rho_inf = 0, p_inf = 0, gamma = 1.4;
+    std::vector<int32_t> ghost_bin;   // reference ghost order: bin, or -1
+    std::vector<int32_t> ghost_kind;  // reference ghost order: boundary kind
+    AdjFaces F{};
+    std::vector<void*> allocs;
+    std::vector<double*> ckpt;        // [nseg] states at segment starts
+    std::vector<double*> Qs;          // [(every + 1) * S] stage inputs of a segment (Qs[j*S] = q_n)
+    std::vector<double*> Gx, Gy, Lim; // [every * S]
+    std::vector<double*> dtc;         // [every] per-cell dt of each step
+    double *tmp[2] = {nullptr, nullptr}, *tgx = nullptr, *tgy = nullptr, *tlim = nullptr;
+    double *dt_fill = nullptr, *dt_n = nullptr, *loss = nullptr, *lam_dt = nullptr, *partials = nullptr;
+    double *lamA = nullptr, *lamB = nullptr, *lam_qn = nullptr, *lgx = nullptr, *lgy = nullptr, *llim = nullptr;
+    double *lam_bv = nullptr;
+    unsigned long long* keys = nullptr;
+    int* argmin = nullptr;
+    int32_t* loss_ghosts = nullptr;   // device ghost indices of the loss group
+    int n_loss = 0;
+    std::vector<double> theta_last;
+    template <class T>
+    cudaError_t alloc(T** p, size_t n) {
+        cudaError_t e = cudaMalloc((void**)p, std::max<size_t>(n, 1) * sizeof(T));
+        if (e == cudaSuccess) allocs.push_back((void*)*p);
+        return e;
+    }
+    ~fv_adjoint() {
+        if (s) cudaSetDevice(s->device);
+        for (void* p : allocs) cudaFree(p);
+        delete s;
+    }
+};
+
+namespace {
+// One forward step from q (device numbering, all cells) to q_next.  With
+// `store`, stage inputs go to qs[k] (qs[0] == q), gradients to gx/gy/lim[k]
+// and per-cell dt to dtc; otherwise the adjoint's temporaries are used.
+int adj_forward_step(fv_adjoint* a, const double* q, double* q_next, double* dt_slot, bool store, int j,
+                     bool with_loss) {
+    fv_solver* s = a->s;
+    cudaStream_t st = s->stream;
+    const TileParams& TP = s->TP;
+    const size_t nt = (size_t)s->n_total;
+    double* dtcells = store ? a->dtc[j] : a->dt_fill;
+    CK(cudaMemsetAsync(a->keys, 0xFF, kDtSlots * 8, st));
+    TileIO io{};
+    io.q_stage = q;
+    io.dt = dtcells;
+    io.dtkeys = a->keys;
+    tile::launch_dt(FV_PREC_FP64_EXACT, TP, io, st);
+    adj_launch_dt_finalize(a->keys, dtcells, TP.P.cell0, a->dt_fill, (int)nt, dt_slot, st);
+    if (with_loss && a->n_loss) adj_launch_loss(TP.P, q, dt_slot, a->loss_ghosts, a->n_loss, a->loss, st);
+    const double* in = q;
+    for (int k = 0; k < a->S; ++k) {
+        double* gx = store ? a->Gx[(size_t)j * a->S + k] : a->tgx;
+        double* gy = store ? a->Gy[(size_t)j * a->S + k] : a->tgy;
+        double* lim = store ? a->Lim[(size_t)j * a->S + k] : a->tlim;
+        double* out = (k == a->S - 1) ? q_next : (store ? a->Qs[(size_t)j * a->S + k + 1] : a->tmp[k % 2]);
+        TileIO so{};
+        so.q_stage = in;
+        so.q_base = q;
+        so.q_out = out;
+        so.gx = gx; so.gy = gy; so.lim = lim;
+        so.dt = a->dt_fill;
+        so.alpha = a->alpha[(size_t)k];
+        so.write_f64 = 1;
+        if (TP.P.order2) tile::launch_gradlim(FV_PREC_FP64_EXACT, TP, so, st);
+        tile::launch_stage(FV_PREC_FP64_EXACT, TP, so, st);
+        in = out;
+    }
+    CK(cudaGetLastError());
+    return FV_OK;
+}
+
+int adj_set_theta(fv_adjoint* a, const double* theta, double* q0_dev) {
+    fv_solver* s = a->s;
+    const double M = theta[0];
+    const int nb = a->o.n_bins;
+    const double e_inf = a->p_inf / (a->gamma - 1.0);
+    // initial state: the free stream (reference numbering, ghosts filled below)
+    std::vector<double> q((size_t)s->n_total * 4, 0.0);
+    for (int64_t c = 0; c < s->n_total; ++c) {
+        q[4 * c] = a->rho_inf; q[4 * c + 1] = a->rho_inf * M; q[4 * c + 2] = 0.0;
+        q[4 * c + 3] = e_inf + 0.5 * a->rho_inf * M * M;
+    }
+    std::vector<double> bv((size_t)s->n_bound * 4, 0.0);
+    for (int64_t r = 0; r < s->n_bound; ++r) {
+        const int kind = a->ghost_kind[(size_t)r];
+        if (kind != FV_BC_INLET_OUTLET && kind != FV_BC_FARFIELD) continue;
+        const int b = a->ghost_bin[(size_t)r];
+        const double rho = a->rho_inf * (1.0 + (b >= 0 && b < nb ? theta[1 + b] : 0.0));
+        bv[4 * r] = rho; bv[4 * r + 1] = rho * M; bv[4 * r + 2] = 0.0; bv[4 * r + 3] = e_inf + 0.5 * rho * M * M;
+    }
+    int rc = fv_solver_set_ghost_states(s, bv.data());
+    if (rc) return rc;
+    if ((rc = fv_set_state(s, q.data()))) return rc;
+    CK(cudaMemcpyAsync(q0_dev, s->qbase[0], q.size() * 8, cudaMemcpyDeviceToDevice, s->stream));
+    // run(): initial ghost fill with zeroed gradients (explicit.cpp:712)
+    exact::launch_bounds(s->TP.P, q0_dev, nullptr, nullptr, nullptr, 1, s->stream);
+    CK(cudaGetLastError());
+    return FV_OK;
+}
+
+AdjStage adj_stage(fv_adjoint* a, int j, int k, double dt) {
+    AdjStage S{};
+    const size_t i = (size_t)j * a->S + k;
+    S.qs = a->Qs[i];
+    S.qs1 = a->Qs[i + 1];
+    S.gx = a->Gx[i]; S.gy = a->Gy[i]; S.lim = a->Lim[i];
+    S.dt = dt;
+    S.alpha = a->alpha[(size_t)k];
+    S.lam_next = a->lamA; S.lam_cur = a->lamB;
+    S.lam_gx = a->s->TP.P.order2 ? a->lgx : nullptr;
+    S.lam_gy = a->lgy; S.lam_lim = a->llim;
+    S.lam_qn = a->lam_qn;
+    S.lam_bv = a->lam_bv;
+    S.dt_partials = a->partials + (size_t)k * adj_residual_blocks(a->s->TP.P);
+    return S;
+}
+}  // namespace
+
+extern "C" {
+
+int fv_adjoint_create(const fv_mesh* fm, const fv_physics* ph, int32_t device, const fv_adjoint_options* o,
+                      fv_adjoint** out) {
+    if (!fm || !ph || !o || !out) return fail(FV_ERR_ARG, "fv_adjoint_create: null argument");
+    if (ph->V != 4 || (ph->flux != FV_FLUX_ROE_FS && ph->flux != FV_FLUX_ROE_ST))
+        return fail(FV_ERR_UNSUPPORTED, "fv_adjoint: Euler with a Roe flux kind only");
+    if (!ph->global_dt || (ph->dt_kind != FV_DT_CFL_SUM && ph->dt_kind != FV_DT_CONST))
+        return fail(FV_ERR_UNSUPPORTED, "fv_adjoint: the global CFL-sum or constant time step only");
+    if (o->n_steps < 1 || o->checkpoint_every < 1 || o->n_alpha < 1 || o->n_alpha > 8 || !o->alpha || o->n_bins < 0)
+        return fail(FV_ERR_ARG, "fv_adjoint_create: invalid options");
+    const HostMesh& m = fm->m;
+    const int ng = (int)m.group_names.size();
+    if (o->param_group < 0 || o->param_group >= ng || o->loss_group < 0 || o->loss_group >= ng)
+        return fail(FV_ERR_ARG, "fv_adjoint_create: group index out of range");
+    if (ph->group_bc[o->param_group] != FV_BC_INLET_OUTLET && ph->group_bc[o->param_group] != FV_BC_FARFIELD)
+        return fail(FV_ERR_ARG, "fv_adjoint_create: the parameter group must be an inflow / far-field boundary");
+    if (m.case_real_off.size() > 2) return fail(FV_ERR_UNSUPPORTED, "fv_adjoint: not on batches");
+    std::unique_ptr<fv_adjoint> a(new fv_adjoint());
+    a->o = *o;
+    a->alpha.assign(o->alpha, o->alpha + o->n_alpha);
+    a->o.alpha = nullptr;
+    a->S = o->n_alpha;
+    a->gamma = ph->gamma;
+    const double* bv = ph->group_bv + 4 * o->param_group;
+    a->rho_inf = bv[0];
+    a->p_inf = (ph->gamma - 1) * (bv[3] - 0.5 / bv[0] * (bv[1] * bv[1] + bv[2] * bv[2]));
+    int rc = fv_solver_create(fm, ph, FV_PREC_FP64_EXACT, device, &a->s);
+    if (rc) return rc;
+    fv_solver* s = a->s;
+    // parametrisation per reference ghost
+    a->ghost_bin.assign((size_t)m.n_bound, -1);
+    a->ghost_kind.assign((size_t)m.n_bound, 0);
+    for (int64_t r = 0; r < m.n_bound; ++r) {
+        const int g = m.bnd_group[(size_t)r];
+        a->ghost_kind[(size_t)r] = ph->group_bc[g];
+        if (g == o->param_group && o->n_bins > 0) {
+            const double y = m.ecy[m.bound_edges[(size_t)r]];
+            int b = (int)std::floor((y - o->bin_lo) / (o->bin_hi - o->bin_lo) * o->n_bins);
+            a->ghost_bin[(size_t)r] = std::min(std::max(b, 0), o->n_bins - 1);
+        }
+    }
+    // cell-centric face lists for the adjoint kernels
+    FaceArrays fa;
+    build_face_arrays(m, fa);
+    {
+        uint32_t* nbr; double *nx, *ny, *le, *g, *dsx, *dsy, *dnx, *dny, *area;
+        auto up = [&](auto** d, const auto& v) -> cudaError_t {
+            cudaError_t e = a->alloc(d, v.size());
+            if (e == cudaSuccess) e = cudaMemcpy(*d, v.data(), v.size() * sizeof(v[0]), cudaMemcpyHostToDevice);
+            return e;
+        };
+        CK(up(&nbr, fa.nbr)); CK(up(&nx, fa.nx)); CK(up(&ny, fa.ny)); CK(up(&le, fa.le)); CK(up(&g, fa.g));
+        CK(up(&dsx, fa.dsx)); CK(up(&dsy, fa.dsy)); CK(up(&dnx, fa.dnx)); CK(up(&dny, fa.dny));
+        CK(up(&area, fa.area));
+        a->F = AdjFaces{nbr, nx, ny, le, g, dsx, dsy, dnx, dny, area};
+    }
+    std::vector<int32_t> lg;
+    for (int64_t b = 0; b < m.n_bound; ++b)
+        if (fa.ghost_group[(size_t)b] == o->loss_group) lg.push_back((int32_t)b);
+    a->n_loss = (int)lg.size();
+    CK(a->alloc(&a->loss_ghosts, lg.size()));
+    if (!lg.empty()) CK(cudaMemcpy(a->loss_ghosts, lg.data(), lg.size() * 4, cudaMemcpyHostToDevice));
+    // buffers
+    const size_t nq = (size_t)m.n_total * 4;
+    const int every = std::min(o->checkpoint_every, o->n_steps);
+    a->o.checkpoint_every = every;
+    a->nseg = (o->n_steps + every - 1) / every;
+    a->ckpt.resize((size_t)a->nseg);
+    for (auto& p : a->ckpt) CK(a->alloc(&p, nq));
+    a->Qs.resize((size_t)(every + 1) * a->S);
+    for (auto& p : a->Qs) CK(a->alloc(&p, nq));
+    const size_t ng_ = (size_t)every * a->S;
+    a->Gx.resize(ng_); a->Gy.resize(ng_); a->Lim.resize(ng_);
+    for (size_t i = 0; i < ng_; ++i) {
+        CK(a->alloc(&a->Gx[i], nq)); CK(a->alloc(&a->Gy[i], nq)); CK(a->alloc(&a->Lim[i], nq));
+        launch_fill_ghost_grad(a->Gx[i], a->Gy[i], a->Lim[i], (int)m.n_real, (int)m.n_total, 4, false, s->stream);
+    }
+    a->dtc.resize((size_t)every);
+    for (auto& p : a->dtc) CK(a->alloc(&p, (size_t)m.n_total));
+    CK(a->alloc(&a->tmp[0], nq)); CK(a->alloc(&a->tmp[1], nq));
+    CK(a->alloc(&a->tgx, nq)); CK(a->alloc(&a->tgy, nq)); CK(a->alloc(&a->tlim, nq));
+    launch_fill_ghost_grad(a->tgx, a->tgy, a->tlim, (int)m.n_real, (int)m.n_total, 4, false, s->stream);
+    CK(a->alloc(&a->dt_fill, (size_t)m.n_total));
+    CK(a->alloc(&a->dt_n, (size_t)o->n_steps));
+    CK(a->alloc(&a->loss, 1)); CK(a->alloc(&a->lam_dt, 1));
+    CK(a->alloc(&a->partials, (size_t)a->S * adj_residual_blocks(s->TP.P)));
+    CK(a->alloc(&a->lamA, nq)); CK(a->alloc(&a->lamB, nq)); CK(a->alloc(&a->lam_qn, nq));
+    CK(a->alloc(&a->lgx, nq)); CK(a->alloc(&a->lgy, nq)); CK(a->alloc(&a->llim, nq));
+    CK(a->alloc(&a->lam_bv, (size_t)m.n_bound * 4));
+    CK(a->alloc(&a->keys, (size_t)kDtSlots));
+    CK(a->alloc(&a->argmin, 1));
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(s->stream));
+    *out = a.release();
+    return FV_OK;
+}
+
+int fv_adjoint_destroy(fv_adjoint* a) {
+    delete a;
+    return FV_OK;
+}
+
+int fv_adjoint_run(fv_adjoint* a, const double* theta, double* loss, double* grad) {
+    if (!a || !theta) return fail(FV_ERR_ARG, "fv_adjoint_run: null argument");
+    fv_solver* s = a->s;
+    CK(cudaSetDevice(s->device));
+    cudaStream_t st = s->stream;
+    const int N = a->o.n_steps, every = a->o.checkpoint_every, S = a->S;
+    const size_t nq = (size_t)s->n_total * 4;
+    int rc = adj_set_theta(a, theta, a->ckpt[0]);
+    if (rc) return rc;
+    a->theta_last.assign(theta, theta + 1 + a->o.n_bins);
+    // ---- forward: checkpoints every `every` steps, loss
+    CK(cudaMemsetAsync(a->loss, 0, 8, st));
+    double* cur = a->ckpt[0];
+    double* nxt = a->Qs[0];  // scratch for the non-checkpoint states
+    double* alt = a->Qs[1 % a->Qs.size()];
+    for (int n = 0; n < N; ++n) {
+        double* dst = ((n + 1) % every == 0 && (n + 1) / every < a->nseg) ? a->ckpt[(size_t)(n + 1) / every]
+                                                                             : (cur == nxt ? alt : nxt);
+        if ((rc = adj_forward_step(a, cur, dst, a->dt_n + n, false, 0, true))) return rc;
+        cur = dst;
+    }
+    // final state kept in the solver (fv_adjoint_final_state)
+    CK(cudaMemcpyAsync(s->qbase[0], cur, nq * 8, cudaMemcpyDeviceToDevice, st));
+    if (loss) {
+        CK(cudaMemcpyAsync(loss, a->loss, 8, cudaMemcpyDeviceToHost, st));
+    }
+    CK(cudaStreamSynchronize(st));
+    if (!grad) return FV_OK;
+    // ---- reverse
+    const TileParams& TP = s->TP;
+    const int nblk = adj_residual_blocks(TP.P);
+    CK(cudaMemsetAsync(a->lamA, 0, nq * 8, st));   // the loss does not depend on q_N
+    CK(cudaMemsetAsync(a->lam_bv, 0, (size_t)s->n_bound * 4 * 8, st));
+    std::vector<double> dts((size_t)every);
+    for (int seg = a->nseg - 1; seg >= 0; --seg) {
+        const int n0 = seg * every, len = std::min(every, N - n0);
+        CK(cudaMemcpyAsync(a->Qs[0], a->ckpt[(size_t)seg], nq * 8, cudaMemcpyDeviceToDevice, st));
+        for (int j = 0; j < len; ++j)
+            if ((rc = adj_forward_step(a, a->Qs[(size_t)j * S], a->Qs[(size_t)(j + 1) * S], a->dt_n + n0 + j, true, j,
+                                       false)))
+                return rc;
+        CK(cudaMemcpyAsync(dts.data(), a->dt_n + n0, (size_t)len * 8, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        for (int j = len - 1; j >= 0; --j) {
+            CK(cudaMemsetAsync(a->lam_qn, 0, nq * 8, st));
+            for (int k = S - 1; k >= 0; --k) {
+                AdjStage stg = adj_stage(a, j, k, dts[(size_t)j]);
+                adj_launch_ghosts(TP.P, a->F, stg, st);
+                adj_launch_residual(TP.P, a->F, stg, st);
+                if (TP.P.order2) adj_launch_gradlim(TP.P, a->F, stg, st);
+                std::swap(a->lamA, a->lamB);
+            }
+            adj_launch_add(a->lam_qn, a->lamA, nq, st);  // q_n is stage 0's input
+            adj_launch_sum(a->partials, S * nblk, a->lam_dt, st);
+            const double* qn = a->Qs[(size_t)j * S];
+            if (a->n_loss)
+                adj_launch_loss_adjoint(TP.P, qn, a->dt_n + n0 + j, a->loss_ghosts, a->n_loss, 1.0, a->lam_qn, a->lam_dt, st);
+            if (TP.P.dt_kind == FV_DT_CFL_SUM)
+                adj_launch_dt(TP.P, a->F, qn, a->dtc[(size_t)j], a->dt_n + n0 + j, a->lam_dt, a->lam_qn, a->argmin, st);
+            std::swap(a->lamA, a->lam_qn);
+            CK(cudaGetLastError());
+        }
+    }
+    // initial ghost fill (boundary states of q_0 from its interior values)
+    {
+        AdjStage stg{};
+        stg.qs1 = a->ckpt[0];
+        stg.zero_grad = 1;
+        stg.lam_next = a->lamA;
+        stg.lam_bv = a->lam_bv;
+        adj_launch_ghosts(TP.P, a->F, stg, st);
+    }
+    CK(cudaGetLastError());
+    std::vector<double> lq(nq), lbv((size_t)s->n_bound * 4);
+    std::vector<int32_t> n2r((size_t)s->n_total);
+    CK(cudaMemcpyAsync(lq.data(), a->lamA, nq * 8, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(lbv.data(), a->lam_bv, lbv.size() * 8, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(n2r.data(), s->new2ref, n2r.size() * 4, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    // dL/dtheta in a fixed order: free stream through the initial state ...
+    const double M = theta[0];
+    const int nb = a->o.n_bins;
+    for (int b = 0; b <= nb; ++b) grad[b] = 0.0;
+    for (int64_t c = 0; c < s->n_real; ++c)
+        grad[0] += lq[4 * c + 1] * a->rho_inf + lq[4 * c + 3] * a->rho_inf * M;
+    // ... and the inflow boundary states (device ghost order -> reference)
+    for (int64_t gb = 0; gb < s->n_bound; ++gb) {
+        const int64_t r = (int64_t)n2r[(size_t)(s->n_real + gb)] - s->n_real;
+        const int kind = a->ghost_kind[(size_t)r];
+        if (kind != FV_BC_INLET_OUTLET && kind != FV_BC_FARFIELD) continue;
+        const int b = a->ghost_bin[(size_t)r];
+        const double rho = a->rho_inf * (1.0 + (b >= 0 ? theta[1 + b] : 0.0));
+        const double* l = &lbv[(size_t)gb * 4];
+        grad[0] += l[1] * rho + l[3] * rho * M;
+        if (b >= 0) grad[1 + b] += a->rho_inf * (l[0] + l[1] * M + l[3] * 0.5 * M * M);
+    }
+    return FV_OK;
+}
+
+int fv_adjoint_final_state(fv_adjoint* a, double* q) {
+    if (!a || !q) return fail(FV_ERR_ARG, "fv_adjoint_final_state: null argument");
+    return fv_get_state(a->s, q);
 }
 
 }  // extern "C"

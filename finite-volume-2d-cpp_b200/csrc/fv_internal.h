@@ -56,6 +56,7 @@ struct Params {
     int n_groups;
     int group_bc[kMaxGroups];
     double group_bv[kMaxGroups * 4];
+    const double* ghost_bv;     // [n_bound][4] per-ghost boundary state (device ghost order) or nullptr
     // batches of independent cases (n_cases > 1): each case has its own
     // global dt minimum (64 key slots per case) and its own time
     int n_cases;

@@ -167,7 +167,7 @@ __global__ void k_bounds(Params P, double* __restrict__ q, const double* __restr
 #pragma unroll
         for (int k = 0; k < V; ++k) qint[k] = qc[k];
     }
-    bc<V>(P, P.ghost_group[b], out, qint, nx, ny);
+    bc<V>(P, P.ghost_group[b], b, out, qint, nx, ny);
     store_cell<V>(q, N + b, out);
 }
 

@@ -41,8 +41,8 @@ int fv_kind_bc(int32_t kind, int32_t V, double gamma, const double* bv, const do
     P.n_groups = 1;
     P.group_bc[0] = kind;
     if (bv) memcpy(P.group_bv, bv, 4 * sizeof(double));
-    if (V == 4) fvgpu::exact::bc<4>(P, 0, b, q, n[0], n[1]);
-    else fvgpu::exact::bc<2>(P, 0, b, q, n[0], n[1]);
+    if (V == 4) fvgpu::exact::bc<4>(P, 0, 0, b, q, n[0], n[1]);
+    else fvgpu::exact::bc<2>(P, 0, 0, b, q, n[0], n[1]);
     return FV_OK;
 }
 

@@ -23,13 +23,13 @@ FV_HD double dmax(double a, double b) { return (a < b) ? b : a; }  // std::max
 // Roe flux with the "cures" eigenvalue modification.
 // FS_ASSOC: examples/forwardStep/main.cpp:72-135 (central flux as one sum);
 // otherwise examples/shockTube/main.cpp:68-135 = examples/naca/main.cpp:71-137.
-template <bool FS_ASSOC>
-FV_HD void roe(double gamma, double* f, const double* qi, const double* qj,
-                                    double n0, double n1) {
-    const double pi = (gamma - 1) * (qi[3] - 0.5 / qi[0] * (qi[1] * qi[1] + qi[2] * qi[2]));
-    const double pj = (gamma - 1) * (qj[3] - 0.5 / qj[0] * (qj[1] * qj[1] + qj[2] * qj[2]));
-    const double Vi = (qi[1] * n0 + qi[2] * n1) / qi[0];
-    const double Vj = (qj[1] * n0 + qj[2] * n1) / qj[0];
+// T: double, or a forward-mode dual number (the adjoint's element Jacobians).
+template <bool FS_ASSOC, class T>
+FV_HD void roe(double gamma, T* f, const T* qi, const T* qj, double n0, double n1) {
+    const T pi = (gamma - 1) * (qi[3] - 0.5 / qi[0] * (qi[1] * qi[1] + qi[2] * qi[2]));
+    const T pj = (gamma - 1) * (qj[3] - 0.5 / qj[0] * (qj[1] * qj[1] + qj[2] * qj[2]));
+    const T Vi = (qi[1] * n0 + qi[2] * n1) / qi[0];
+    const T Vj = (qj[1] * n0 + qj[2] * n1) / qj[0];
     if (FS_ASSOC) {
         f[0] = (qi[0] * Vi + qj[0] * Vj) * 0.5;
         f[1] = (qi[1] * Vi + pi * n0 + qj[1] * Vj + pj * n0) * 0.5;
@@ -47,26 +47,26 @@ FV_HD void roe(double gamma, double* f, const double* qi, const double* qj,
 #pragma unroll
         for (int i = 0; i < 4; ++i) f[i] *= 0.5;
     }
-    const double pL = pi, pR = pj;
-    const double uL = qi[1] / qi[0], vL = qi[2] / qi[0];
-    const double uR = qj[1] / qj[0], vR = qj[2] / qj[0];
-    const double srhoL = sqrt(qi[0]), srhoR = sqrt(qj[0]);
-    const double rho = srhoR * srhoL;
-    const double u = (uL * srhoL + uR * srhoR) / (srhoL + srhoR);
-    const double v = (vL * srhoL + vR * srhoR) / (srhoL + srhoR);
-    const double h = ((qi[3] + pL) / qi[0] * srhoL + (qj[3] + pR) / qj[0] * srhoR) / (srhoL + srhoR);
-    const double q2 = u * u + v * v;
-    const double c = sqrt((gamma - 1.) * (h - 0.5 * q2));
-    const double V = u * n0 + v * n1;
-    const double VR = uR * n0 + vR * n1;
-    const double VL = uL * n0 + vL * n1;
-    const double lambda_cm = fabs(dmin(V - c, VL - c));
-    const double lambda_c = fabs(V);
-    const double lambda_cp = fabs(dmax(V + c, VR + c));
-    const double kF1 = lambda_cm * ((pR - pL) - rho * c * (VR - VL)) / (2. * c * c);
-    const double kF234_0 = lambda_c * ((qj[0] - qi[0]) - (pR - pL) / (c * c));
-    const double kF234_1 = lambda_c * rho;
-    const double kF5 = lambda_cp * ((pR - pL) + rho * c * (VR - VL)) / (2. * c * c);
+    const T pL = pi, pR = pj;
+    const T uL = qi[1] / qi[0], vL = qi[2] / qi[0];
+    const T uR = qj[1] / qj[0], vR = qj[2] / qj[0];
+    const T srhoL = sqrt(qi[0]), srhoR = sqrt(qj[0]);
+    const T rho = srhoR * srhoL;
+    const T u = (uL * srhoL + uR * srhoR) / (srhoL + srhoR);
+    const T v = (vL * srhoL + vR * srhoR) / (srhoL + srhoR);
+    const T h = ((qi[3] + pL) / qi[0] * srhoL + (qj[3] + pR) / qj[0] * srhoR) / (srhoL + srhoR);
+    const T q2 = u * u + v * v;
+    const T c = sqrt((gamma - 1.) * (h - 0.5 * q2));
+    const T V = u * n0 + v * n1;
+    const T VR = uR * n0 + vR * n1;
+    const T VL = uL * n0 + vL * n1;
+    const T lambda_cm = fabs(dmin(V - c, VL - c));
+    const T lambda_c = fabs(V);
+    const T lambda_cp = fabs(dmax(V + c, VR + c));
+    const T kF1 = lambda_cm * ((pR - pL) - rho * c * (VR - VL)) / (2. * c * c);
+    const T kF234_0 = lambda_c * ((qj[0] - qi[0]) - (pR - pL) / (c * c));
+    const T kF234_1 = lambda_c * rho;
+    const T kF5 = lambda_cp * ((pR - pL) + rho * c * (VR - VL)) / (2. * c * c);
     f[0] -= 0.5 * (kF1 + kF234_0 + kF5);
     f[1] -= 0.5 * (kF1 * (u - c * n0) + kF234_0 * u + kF234_1 * (uR - uL - (VR - VL) * n0) + kF5 * (u + c * n0));
     f[2] -= 0.5 * (kF1 * (v - c * n1) + kF234_0 * v + kF234_1 * (vR - vL - (VR - VL) * n1) + kF5 * (v + c * n1));
@@ -111,9 +111,8 @@ FV_HD double limiter_func(int kind, double y) {
 // 158-163.  WALL: forwardStep/main.cpp:262-269.  INLET_OUTLET: forwardStep/
 // main.cpp:194-261.  FARFIELD: naca/main.cpp:192-259.  Subsonic outlets keep
 // the reference's b[2] = b[1]*(...).
-template <int V>
-FV_HD void bc(const Params& P, int group, double* b, const double* q, double n0, double n1) {
-    const int kind = P.group_bc[group];
+template <int V, class T>
+FV_HD void bc_state(int kind, double gamma, const T* bv, T* b, const T* q, double n0, double n1) {
     if (kind == 0 || V != 4) {
 #pragma unroll
         for (int k = 0; k < V; ++k) b[k] = q[k];
@@ -126,14 +125,12 @@ FV_HD void bc(const Params& P, int group, double* b, const double* q, double n0,
         b[3] = q[3];
         return;
     }
-    const double gamma = P.gamma;
-    const double* bv = P.group_bv + 4 * group;
-    const double U0 = q[1] / q[0], U1 = q[2] / q[0];
-    const double u_norm = sqrt(U0 * U0 + U1 * U1);
-    const double u_dot_n = U0 * n0 + U1 * n1;
-    const double p = (gamma - 1) * (q[3] - 0.5 / q[0] * (q[1] * q[1] + q[2] * q[2]));
-    const double c = sqrt(gamma * p / q[0]);
-    const double mach = u_norm / c;
+    const T U0 = q[1] / q[0], U1 = q[2] / q[0];
+    const T u_norm = sqrt(U0 * U0 + U1 * U1);
+    const T u_dot_n = U0 * n0 + U1 * n1;
+    const T p = (gamma - 1) * (q[3] - 0.5 / q[0] * (q[1] * q[1] + q[2] * q[2]));
+    const T c = sqrt(gamma * p / q[0]);
+    const T mach = u_norm / c;
     if (mach > 1) {
         if (u_dot_n < 0) {
             b[0] = bv[0]; b[1] = bv[1]; b[2] = bv[2]; b[3] = bv[3];
@@ -142,29 +139,37 @@ FV_HD void bc(const Params& P, int group, double* b, const double* q, double n0,
         }
         return;
     }
-    const double pa = (gamma - 1) * (bv[3] - 0.5 / bv[0] * (bv[1] * bv[1] + bv[2] * bv[2]));
-    const double rhoa = bv[0], ua = bv[1] / bv[0], va = bv[2] / bv[0];
-    const double pd = p, rhod = q[0], ud = q[1] / q[0], vd = q[2] / q[0];
-    const double rho0 = q[0], c0 = c;
+    const T pa = (gamma - 1) * (bv[3] - 0.5 / bv[0] * (bv[1] * bv[1] + bv[2] * bv[2]));
+    const T rhoa = bv[0], ua = bv[1] / bv[0], va = bv[2] / bv[0];
+    const T pd = p, rhod = q[0], ud = q[1] / q[0], vd = q[2] / q[0];
+    const T rho0 = q[0], c0 = c;
     if (u_dot_n < 0) {
         if (kind == 2) {
-            const double pb = pd;
+            const T pb = pd;
             b[0] = bv[0]; b[1] = bv[1]; b[2] = bv[2];
             b[3] = pb / (gamma - 1.) + 0.5 / b[0] * (b[1] * b[1] + b[2] * b[2]);
         } else {
-            const double pb = 0.5 * (pa + pd - rho0 * c0 * (n0 * (ua - ud) + n1 * (va - vd)));
+            const T pb = 0.5 * (pa + pd - rho0 * c0 * (n0 * (ua - ud) + n1 * (va - vd)));
             b[0] = rhoa + (pb - pa) / (c0 * c0);
             b[1] = b[0] * (ua - n0 * (pa - pb) / (rho0 * c0));
             b[2] = b[1] * (va - n1 * (pa - pb) / (rho0 * c0));
             b[3] = pb / (gamma - 1) + 0.5 / b[0] * (b[1] * b[1] + b[2] * b[2]);
         }
     } else {
-        const double pb = pa;
+        const T pb = pa;
         b[0] = rhod + (pb - pd) / (c0 * c0);
         b[1] = b[0] * (ud + n0 * (pd - pb) / (rho0 * c0));
         b[2] = b[1] * (va + n1 * (pd - pb) / (rho0 * c0));
         b[3] = pb / (gamma - 1.) + 0.5 / b[0] * (b[1] * b[1] + b[2] * b[2]);
     }
+}
+
+// Ghost gb of boundary group `group`: the group's boundary kind, with the
+// ghost's own boundary state when a per-ghost inflow is set (P.ghost_bv).
+template <int V>
+FV_HD void bc(const Params& P, int group, int gb, double* b, const double* q, double n0, double n1) {
+    const double* bv = P.ghost_bv ? P.ghost_bv + 4 * (size_t)gb : P.group_bv + 4 * group;
+    bc_state<V>(P.group_bc[group], P.gamma, bv, b, q, n0, n1);
 }
 
 // Pressure, forwardStep/main.cpp:37-39.

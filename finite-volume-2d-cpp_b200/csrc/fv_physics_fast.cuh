@@ -98,7 +98,7 @@ __device__ __forceinline__ T limiter_func(int kind, T y) {
 
 // Boundary conditions (see fv_physics_exact.cuh for the references).
 template <int V, class T>
-__device__ __forceinline__ void bc(const Params& P, int group, T* b, const T* q, T n0, T n1) {
+__device__ __forceinline__ void bc(const Params& P, int group, int gb, T* b, const T* q, T n0, T n1) {
     const int kind = P.group_bc[group];
     if (kind == 0 || V != 4) {
 #pragma unroll
@@ -111,7 +111,7 @@ __device__ __forceinline__ void bc(const Params& P, int group, T* b, const T* q,
         return;
     }
     const T gamma = (T)P.gamma, gm1 = gamma - T(1);
-    const double* bvd = P.group_bv + 4 * group;
+    const double* bvd = P.ghost_bv ? P.ghost_bv + 4 * (size_t)gb : P.group_bv + 4 * group;
     const T bv[4] = {(T)bvd[0], (T)bvd[1], (T)bvd[2], (T)bvd[3]};
     const T r = rcp(q[0]);
     const T U0 = q[1] * r, U1 = q[2] * r;

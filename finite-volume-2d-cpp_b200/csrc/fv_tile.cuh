@@ -719,8 +719,8 @@ __global__ void __launch_bounds__(kTileMax) k_tile_stage(TileParams TP, TileIO i
                     }
                     guard_face<S, V>(P, qint, qc);
                 }
-                if constexpr (M::exact) exact::bc<V>(P, P.ghost_group[g - N], b, qint, n0, n1);
-                else fast::bc<V, S>(P, P.ghost_group[g - N], b, qint, n0, n1);
+                if constexpr (M::exact) exact::bc<V>(P, P.ghost_group[g - N], g - N, b, qint, n0, n1);
+                else fast::bc<V, S>(P, P.ghost_group[g - N], g - N, b, qint, n0, n1);
                 if (sizeof(S) == 8) {
                     st<double, V>(io.q_out, g, (const double*)b);
                 } else {

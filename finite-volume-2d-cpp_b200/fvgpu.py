@@ -295,6 +295,15 @@ class Solver:
         _check(lib().fv_run(self._h, C.byref(o), C.byref(info)))
         return dict(step=info.step, time=info.time, R=np.array(info.R[: self.V]), R0=np.array(info.R0[: self.V]))
 
+    def set_ghost_states(self, bv):
+        """Per-ghost boundary states [n_bound, 4] (reference ghost order) for
+        inflow / far-field ghosts; None restores the group states."""
+        if bv is None:
+            _check(lib().fv_solver_set_ghost_states(self._h, None))
+            return
+        b = np.ascontiguousarray(bv, np.float64).reshape(-1)
+        _check(lib().fv_solver_set_ghost_states(self._h, _p(b)))
+
     def case_times(self):
         """Each case's accumulated time (one entry for a single mesh)."""
         t = np.zeros(self.mesh.n_cases)
@@ -356,3 +365,62 @@ def solver_info(s: Solver):
     _check(lib().fv_solver_info(s._h, _p(out, _i64p)))
     return dict(tiles=int(out[0]), tile_cells=int(out[1]), max_halo=int(out[2]), max_edges=int(out[3]),
                 precision=int(out[4]), stage_bytes=int(out[5]))
+
+
+class _AdjOptions(C.Structure):
+    _fields_ = [("n_steps", C.c_int32), ("checkpoint_every", C.c_int32), ("n_alpha", C.c_int32),
+                ("alpha", _dp), ("loss_group", C.c_int32), ("param_group", C.c_int32), ("n_bins", C.c_int32),
+                ("bin_lo", C.c_double), ("bin_hi", C.c_double)]
+
+
+class Adjoint:
+    """Discrete adjoint of the FP64_EXACT time loop for the inflow-parameter
+    problem (fv_adjoint_*): theta = (M, delta_1..delta_nb) sets the free
+    stream and the inflow density bins; loss = time integral of the pressure
+    force magnitude sum_f p le over `loss_group`'s faces."""
+
+    def __init__(self, mesh: Mesh, ph: _phys.Physics, n_steps: int, checkpoint_every: int = 50,
+                 alpha=_phys.RK5_ALPHA, loss_group: str = "step", param_group: str = "inlet", n_bins: int = 64,
+                 bin_lo: float = 0.0, bin_hi: float = 1.0, device: int = 0):
+        self.mesh = mesh
+        self.n_bins = n_bins
+        self._ps = physics_struct(ph, mesh.group_names)
+        self._alpha = np.ascontiguousarray(alpha, np.float64)
+        self._o = _AdjOptions(n_steps=n_steps, checkpoint_every=checkpoint_every, n_alpha=self._alpha.size,
+                              alpha=_p(self._alpha), loss_group=mesh.group_names.index(loss_group),
+                              param_group=mesh.group_names.index(param_group), n_bins=n_bins,
+                              bin_lo=bin_lo, bin_hi=bin_hi)
+        h = C.c_void_p()
+        _check(lib().fv_adjoint_create(mesh._h, C.byref(self._ps), C.c_int32(device), C.byref(self._o),
+                                       C.byref(h)))
+        self._h = h
+
+    def loss(self, theta):
+        t = np.ascontiguousarray(theta, np.float64)
+        out = C.c_double()
+        _check(lib().fv_adjoint_run(self._h, _p(t), C.byref(out), None))
+        return out.value
+
+    def gradient(self, theta):
+        """(loss, dloss/dtheta)"""
+        t = np.ascontiguousarray(theta, np.float64)
+        out = C.c_double()
+        g = np.zeros(1 + self.n_bins)
+        _check(lib().fv_adjoint_run(self._h, _p(t), C.byref(out), _p(g)))
+        return out.value, g
+
+    def final_state(self):
+        q = np.zeros(self.mesh.n_total * 4)
+        _check(lib().fv_adjoint_final_state(self._h, _p(q)))
+        return q
+
+    def close(self):
+        if self._h:
+            lib().fv_adjoint_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

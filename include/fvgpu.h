@@ -188,6 +188,12 @@ int fv_run(fv_solver* s, const fv_run_options* opt, fv_run_info* info);
  * residual normalisation.  Both solvers must be on one device.  No
  * counterpart in the reference (explicit.cpp:657-817 runs in one precision). */
 int fv_solver_continue_from(fv_solver* dst, fv_solver* src);
+/* Per-ghost boundary states: bv[n_bound][4] (reference ghost order) replaces
+ * the group state of INLET_OUTLET / FARFIELD ghosts, e.g. an inflow profile
+ * that varies along the inlet.  NULL restores the group states.  The
+ * reference binds one boundary function per physical name (mesh.cpp:662-667);
+ * a varying inflow there needs one function per inlet segment. */
+int fv_solver_set_ghost_states(fv_solver* s, const double* bv);
 /* times[n_cases]: each case's accumulated time (time += that case's dt[0]). */
 int fv_batch_times(fv_solver* s, double* times);
 /* R after the last step (sqrt of sum qt^2 A over real cells, un-normalised). */
@@ -262,6 +268,43 @@ int fv_kind_limiter(int32_t kind, double y, double* out);
 /* bv: [4] boundary state of INLET_OUTLET / FARFIELD (may be NULL otherwise). */
 int fv_kind_bc(int32_t kind, int32_t V, double gamma, const double* bv, const double* q,
                const double* n, double* b);
+
+/* ---- discrete adjoint (FP64) ------------------------------------------- */
+/* Reverse mode of fv_run's FP64_EXACT time loop for an inflow-parameter
+ * problem (no counterpart in the reference):
+ *   theta = (M, delta_1 .. delta_nb): the initial state is the free stream
+ *   (rho_inf, u = M, v = 0, p_inf), rho_inf and p_inf from param_group's
+ *   boundary state; every INLET_OUTLET / FARFIELD ghost gets the state
+ *   (rho, rho M, 0, p_inf/(gamma-1) + rho M^2/2) with rho = rho_inf (1 + delta_b)
+ *   on param_group faces whose centre y falls in bin b of [bin_lo, bin_hi),
+ *   rho = rho_inf elsewhere;
+ *   loss = sum over the n_steps steps of dt_n * sum over loss_group faces of
+ *   p(interior cell at the step's start) * face length.
+ * The forward run keeps the state every checkpoint_every steps; the reverse
+ * sweep recomputes each segment, keeping every stage's state, gradients and
+ * limiters, and runs the adjoint kernels stage by stage backwards (Roe flux,
+ * MUSCL reconstruction, gradients and limiter, ghost fills, RK update, the
+ * global CFL time step and the loss).  Needs V = 4, a Roe flux kind and a
+ * global CFL-sum or constant time step. */
+typedef struct fv_adjoint fv_adjoint;
+typedef struct {
+    int32_t n_steps;
+    int32_t checkpoint_every;
+    int32_t n_alpha;          /* RK stages (<= 8) */
+    const double* alpha;
+    int32_t loss_group;
+    int32_t param_group;
+    int32_t n_bins;
+    double bin_lo, bin_hi;
+} fv_adjoint_options;
+int fv_adjoint_create(const fv_mesh* m, const fv_physics* ph, int32_t device, const fv_adjoint_options* o,
+                      fv_adjoint** out);
+/* loss (may be NULL); grad[1 + n_bins] = dL/dtheta, or NULL for the forward
+ * run alone (the loss). */
+int fv_adjoint_run(fv_adjoint* a, const double* theta, double* loss, double* grad);
+/* State after the last forward run, reference numbering [n_total][4]. */
+int fv_adjoint_final_state(fv_adjoint* a, double* q);
+int fv_adjoint_destroy(fv_adjoint* a);
 
 #ifdef __cplusplus
 }

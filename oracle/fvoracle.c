@@ -222,9 +222,16 @@ void fvo_flux(const fvo_physics* ph, double* f, const double* qi, const double* 
  * examples/forwardStep/main.cpp:194-261.  FARFIELD: examples/naca/main.cpp:
  * 192-259.  The subsonic outlet branches keep the reference's
  * b[2] = b[1]*(...) (forwardStep/main.cpp:257, naca/main.cpp:255). */
+static void bc_state(const fvo_physics* ph, int group, const double* bv, double* b, const double* q,
+                     const double* n);
+
 void fvo_bc(const fvo_physics* ph, int group, double* b, const double* q, const double* n) {
+    bc_state(ph, group, ph->group_bv + 4 * group, b, q, n);
+}
+
+static void bc_state(const fvo_physics* ph, int group, const double* bv, double* b, const double* q,
+                     const double* n) {
     const int kind = ph->group_bc[group];
-    const double* bv = ph->group_bv + 4 * group;
     const double gamma = ph->gamma;
     const int V = ph->V;
     if (kind == FVO_BC_COPY) {
@@ -488,7 +495,8 @@ void fvo_update_bounds(const fvo_mesh* m, const fvo_physics* ph, double* q, cons
         } else {
             for (int k = 0; k < V; ++k) qint[k] = q[(size_t)V * ii + k];
         }
-        fvo_bc(ph, m->bound_group[b], q + (size_t)V * ib, qint, n);
+        bc_state(ph, m->bound_group[b], ph->ghost_bv ? ph->ghost_bv + 4 * (size_t)b : ph->group_bv + 4 * m->bound_group[b],
+                 q + (size_t)V * ib, qint, n);
     }
 }
 

@@ -50,6 +50,8 @@ typedef struct {
     const double* group_bv;   /* [n_groups][4] far-field / inflow state */
     int positivity_guard;     /* 1: a MUSCL face state with rho <= 0 or p <= 0 falls back
                                  to the cell value (not in the reference; 0 = reference) */
+    const double* ghost_bv;   /* [n_bound][4] per-ghost far-field / inflow state overriding
+                                 group_bv (a spatially varying inflow; NULL = group_bv) */
 } fvo_physics;
 
 int fvo_mesh_build(int64_t n_nodes, const double* nodes_x, const double* nodes_y,

@@ -47,7 +47,8 @@ class _FvoPhysics(C.Structure):
     _fields_ = [("V", C.c_int), ("flux", C.c_int), ("gamma", C.c_double), ("order2", C.c_int),
                 ("limiter", C.c_int), ("K", C.c_double), ("dt_kind", C.c_int),
                 ("cfl", C.c_double), ("dt_const", C.c_double), ("global_dt", C.c_int),
-                ("n_groups", C.c_int), ("group_bc", _i32p), ("group_bv", _dp), ("positivity_guard", C.c_int)]
+                ("n_groups", C.c_int), ("group_bc", _i32p), ("group_bv", _dp), ("positivity_guard", C.c_int),
+                ("ghost_bv", _dp)]
 
 
 def build_oracle():
@@ -119,7 +120,9 @@ class Oracle:
 
     # -- physics ------------------------------------------------------------
     @staticmethod
-    def physics(phys, group_names):
+    def physics(phys, group_names, ghost_bv=None):
+        """ghost_bv: optional [n_bound, 4] boundary state per ghost (reference
+        ghost order) replacing the group's state."""
         p = _FvoPhysics()
         p.V = phys.V; p.flux = FLUX[phys.flux]; p.gamma = phys.gamma; p.order2 = int(phys.order2)
         p.limiter = LIMITER[phys.limiter]; p.K = phys.K; p.dt_kind = DT[phys.dt_kind]
@@ -130,7 +133,11 @@ class Oracle:
         p.n_groups = len(group_names)
         p.group_bc = _ptr(gbc, _i32p); p.group_bv = _ptr(gbv)
         p.positivity_guard = int(getattr(phys, "positivity_guard", False))
-        p._keep = (gbc, gbv)
+        gh = None
+        if ghost_bv is not None:
+            gh = np.ascontiguousarray(ghost_bv, np.float64).reshape(-1)
+            p.ghost_bv = _ptr(gh)
+        p._keep = (gbc, gbv, gh)
         return p
 
     # -- stages -------------------------------------------------------------
