@@ -105,3 +105,43 @@ def test_face_lists_follow_reference_edge_order():
     # every real cell appears 3 times over both edge columns (triangles)
     cnt = np.bincount(ec[ec < m.n_real], minlength=m.n_real)
     assert np.all(cnt == 3)
+
+
+def _build_adjoint_api(tmp_path):
+    import subprocess
+    pkg = os.path.join(ROOT, "finite-volume-2d-cpp_b200")
+    exe = str(tmp_path / "adjoint_api")
+    subprocess.run(["g++", "-O2", "-std=c++17", "-I" + os.path.join(ROOT, "include"),
+                    os.path.join(ROOT, "tests", "cpp", "adjoint_api.cpp"), "-L" + pkg, "-lfvgpu",
+                    "-Wl,-rpath," + pkg, "-o", exe], check=True)
+    return exe
+
+
+def test_cpp_adjoint_api_compiles_and_reports_errors(tmp_path):
+    """The C++ reverse-mode header builds against the library; without a
+    usable device its constructor throws with the library's message."""
+    import subprocess
+    exe = _build_adjoint_api(tmp_path)
+    r = subprocess.run([exe, str(tmp_path / "missing.msh"), "5", "3.0"], capture_output=True, text=True)
+    assert r.returncode == 3 and r.stdout.startswith("error:") and "missing.msh" in r.stdout
+
+
+@pytest.mark.gpu
+def test_cpp_adjoint_api_matches_python_binding(tmp_path):
+    import subprocess
+    import physics as P
+    exe = _build_adjoint_api(tmp_path)
+    em = meshgen.forward_step(n=20)
+    path = str(tmp_path / "step.msh")
+    meshgen.write_msh41(path, em)
+    theta = [3.0, 0.004, -0.01, 0.002]
+    r = subprocess.run([exe, path, "40"] + [repr(t) for t in theta], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+    vals = [float(x) for x in r.stdout.split()]
+    mesh = fvgpu.Mesh.read_msh(path)
+    ph = P.forward_step(order2=True, limiter="venkat", K=5.0, cfl=0.8)
+    ph.positivity_guard = True
+    adj = fvgpu.Adjoint(mesh, ph, n_steps=40, checkpoint_every=10, n_bins=3)
+    loss, g = adj.gradient(np.array(theta))
+    assert vals[0] == loss and vals[1:] == g.tolist()
+    adj.close()
