@@ -657,7 +657,8 @@ static int enqueue_step(fv_solver* s, const std::vector<double>& alpha, int b, E
     io.gx = s->gx; io.gy = s->gy; io.lim = s->lim; io.dt = s->dt; io.ctrl = s->ctrl;
     io.dtkeys = s->keys;
     io.q_stage = s->sbase[b];
-    tile::launch_dt(s->precision, TP, io, st); ++n; mark(KK_DT);
+    // second order: the first stage's gradient kernel also computes dt
+    if (!TP.P.order2) { tile::launch_dt(s->precision, TP, io, st); ++n; mark(KK_DT); }
     const int ns = (int)alpha.size();
     const void* in = s->sbase[b];
     for (int k = 0; k < ns; ++k) {
@@ -680,7 +681,7 @@ static int enqueue_step(fv_solver* s, const std::vector<double>& alpha, int b, E
         }
         so.s_out = s->f32 ? out_s : nullptr;
         so.write_f64 = last ? 1 : 0;
-        if (TP.P.order2) { tile::launch_gradlim(s->precision, TP, so, st); ++n; mark(KK_GRADLIM); }
+        if (TP.P.order2) { tile::launch_gradlim(s->precision, TP, so, st, k == 0); ++n; mark(KK_GRADLIM); }
         tile::launch_stage(s->precision, TP, so, st); ++n; mark(KK_STAGE);
         in = out_s;
     }

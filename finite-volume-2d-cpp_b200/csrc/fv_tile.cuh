@@ -226,140 +226,137 @@ __device__ __forceinline__ void load_faces(const TileParams& TP, int c, uint16_t
 }
 
 // ------------------------------------------------------------------ K0: dt --
-template <class M, int V>
-__global__ void __launch_bounds__(kTileMax) k_tile_dt(TileParams TP, TileIO io) {
+// CFL time step of owned cell c (tile-local l) and of its boundary ghosts,
+// from staged records (stride NR) and edges (calc_dt of
+// examples/forwardStep/main.cpp:140-185 and examples/naca/main.cpp:142-183);
+// returns the ordered-key minimum of the values written.
+template <class M, int V, int NR>
+__device__ __forceinline__ unsigned long long tile_cell_dt(const TileParams& TP, const TileIO& io, const int4& inf,
+                                                           int l, int c, const uint16_t* w,
+                                                           const typename M::S* rec, const uint32_t* sij,
+                                                           const typename M::S* snx, const typename M::S* sny,
+                                                           const typename M::S* sle) {
     using S = typename M::S;
-    using R = Rec<M, V, false, false>;
-    if (t_inactive(io.ctrl)) return;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
     const Params& P = TP.P;
-    const int N = P.n_real, T = TP.T, t = blockIdx.x;
-    const int4 inf = TP.info[t];
-    const int c0 = t * T, nown = min(T, N - c0);
-    const int LT = T + TP.max_halo;
-    S* rec = reinterpret_cast<S*>(smem_raw);
-    S* snx = rec + (size_t)LT * R::NR;
-    S* sny = snx + TP.max_edges;
-    S* sle = sny + TP.max_edges;
-    uint32_t* sij = reinterpret_cast<uint32_t*>(sle + TP.max_edges);
-    __shared__ unsigned long long wmin[kTileMax / 32];
-    const int l = threadIdx.x;
-    uint16_t w[kMaxFaces];
-    if (l < nown) load_faces(TP, c0 + l, w);  // latency overlaps the staging
-    stage_records<M, V, false, false>(TP, io, inf, c0, nown, rec);
-    stage_edges<S, false, false>(TP, inf, sij, snx, sny, sle, nullptr, nullptr, nullptr);
-    cpa_wait();
-    __syncthreads();
+    const int T = TP.T;
     unsigned long long kmin = ~0ull;
-    if (l < nown) {
-        const int c = c0 + l;
-        const S* AR = (const S*)TP.area;
-        if (P.dt_kind == 0) {
-            io.dt[c] = P.dt_const;
-            kmin = tkey(P.dt_const);
+    const S* AR = (const S*)TP.area;
+    if (P.dt_kind == 0) {
+        io.dt[c] = P.dt_const;
+        kmin = tkey(P.dt_const);
+#pragma unroll
+        for (int f = 0; f < kMaxFaces; ++f) {
+            if (w[f] == kFaceNone || !(w[f] & 0x4000)) continue;
+            const int el = w[f] & kFaceEdgeMask, side = w[f] >> 15;
+            const uint32_t ij = sij[el];
+            const int o = side ? (int)(ij & 0xffff) : (int)(ij >> 16);
+            io.dt[TP.halo[inf.z + o - T]] = P.dt_const;
+        }
+    } else if (V == 4) {
+        S qs[4];
+        lds<S, 4>(rec + (size_t)l * NR, qs);
+        const bool sum = P.dt_kind == 1;
+        if constexpr (M::exact) {
+            const double gamma = P.gamma, gm1 = gamma - 1, cfl = P.cfl;
+            const double cs = sqrt((gm1 * (qs[3] - 0.5 / qs[0] * (qs[1] * qs[1] + qs[2] * qs[2]))) * gamma / qs[0]);
+            const double Ai = AR[c];
+            double acc = sum ? 0. : 1.0;
 #pragma unroll
             for (int f = 0; f < kMaxFaces; ++f) {
-                if (w[f] == kFaceNone || !(w[f] & 0x4000)) continue;
+                if (w[f] == kFaceNone) continue;
                 const int el = w[f] & kFaceEdgeMask, side = w[f] >> 15;
                 const uint32_t ij = sij[el];
                 const int o = side ? (int)(ij & 0xffff) : (int)(ij >> 16);
-                io.dt[TP.halo[inf.z + o - T]] = P.dt_const;
-            }
-        } else if (V == 4) {
-            S qs[4];
-            lds<S, 4>(rec + (size_t)l * R::NR, qs);
-            const bool sum = P.dt_kind == 1;
-            if constexpr (M::exact) {
-                const double gamma = P.gamma, gm1 = gamma - 1, cfl = P.cfl;
-                const double cs = sqrt((gm1 * (qs[3] - 0.5 / qs[0] * (qs[1] * qs[1] + qs[2] * qs[2]))) * gamma / qs[0]);
-                const double Ai = AR[c];
-                double acc = sum ? 0. : 1.0;
-#pragma unroll
-                for (int f = 0; f < kMaxFaces; ++f) {
-                    if (w[f] == kFaceNone) continue;
-                    const int el = w[f] & kFaceEdgeMask, side = w[f] >> 15;
-                    const uint32_t ij = sij[el];
-                    const int o = side ? (int)(ij & 0xffff) : (int)(ij >> 16);
-                    const double n0 = snx[el], n1 = sny[el], le = sle[el];
-                    double qn[4];
-                    lds<double, 4>(rec + (size_t)o * R::NR, qn);
-                    const double cn = sqrt((gm1 * (qn[3] - 0.5 / qn[0] * (qn[1] * qn[1] + qn[2] * qn[2]))) * gamma / qn[0]);
-                    const bool ghost = (w[f] & 0x4000) != 0;
-                    if (sum) {
-                        const double es = cs + fabs(qs[1] / qs[0] * n0 + qs[2] / qs[0] * n1);
-                        const double en = cn + fabs(qn[1] / qn[0] * n0 + qn[2] / qn[0] * n1);
-                        const double center = side ? exact::dmax(en, es) : exact::dmax(es, en);
-                        acc += center * le;
-                        if (ghost) {
-                            const int g = TP.halo[inf.z + o - T];
-                            double d = 0.;
-                            d += center * le;
-                            const double dg = cfl * AR[g] / d;
-                            io.dt[g] = dg;
-                            kmin = kmin_(kmin, tkey(dg));
-                        }
-                    } else {
-                        const double es = (cs + fabs(qs[1] / qs[0])) * n0 + (cs + fabs(qs[2] / qs[0])) * n1;
-                        acc = exact::dmin(acc, cfl * (Ai / le) / fabs(es));
-                        if (ghost) {
-                            const int g = TP.halo[inf.z + o - T];
-                            const double en = (cn + fabs(qn[1] / qn[0])) * n0 + (cn + fabs(qn[2] / qn[0])) * n1;
-                            const double dg = exact::dmin(1.0, cfl * (AR[g] / le) / fabs(en));
-                            io.dt[g] = dg;
-                            kmin = kmin_(kmin, tkey(dg));
-                        }
+                const double n0 = snx[el], n1 = sny[el], le = sle[el];
+                double qn[4];
+                lds<double, 4>(rec + (size_t)o * NR, qn);
+                const double cn = sqrt((gm1 * (qn[3] - 0.5 / qn[0] * (qn[1] * qn[1] + qn[2] * qn[2]))) * gamma / qn[0]);
+                const bool ghost = (w[f] & 0x4000) != 0;
+                if (sum) {
+                    const double es = cs + fabs(qs[1] / qs[0] * n0 + qs[2] / qs[0] * n1);
+                    const double en = cn + fabs(qn[1] / qn[0] * n0 + qn[2] / qn[0] * n1);
+                    const double center = side ? exact::dmax(en, es) : exact::dmax(es, en);
+                    acc += center * le;
+                    if (ghost) {
+                        const int g = TP.halo[inf.z + o - T];
+                        double d = 0.;
+                        d += center * le;
+                        const double dg = cfl * AR[g] / d;
+                        io.dt[g] = dg;
+                        kmin = kmin_(kmin, tkey(dg));
+                    }
+                } else {
+                    const double es = (cs + fabs(qs[1] / qs[0])) * n0 + (cs + fabs(qs[2] / qs[0])) * n1;
+                    acc = exact::dmin(acc, cfl * (Ai / le) / fabs(es));
+                    if (ghost) {
+                        const int g = TP.halo[inf.z + o - T];
+                        const double en = (cn + fabs(qn[1] / qn[0])) * n0 + (cn + fabs(qn[2] / qn[0])) * n1;
+                        const double dg = exact::dmin(1.0, cfl * (AR[g] / le) / fabs(en));
+                        io.dt[g] = dg;
+                        kmin = kmin_(kmin, tkey(dg));
                     }
                 }
-                const double di = sum ? cfl * Ai / acc : acc;
-                io.dt[c] = di;
-                kmin = kmin_(kmin, tkey(di));
-            } else {
-                const S gamma = (S)P.gamma, gm1 = gamma - S(1), cfl = (S)P.cfl;
-                const S ri = fast::rcp(qs[0]);
-                const S us = qs[1] * ri, vs = qs[2] * ri;
-                const S cs = fast::sqrt_(gamma * gm1 * (qs[3] * ri - S(0.5) * (us * us + vs * vs)));
-                const S Ai = AR[c];
-                S acc = sum ? S(0) : S(1);
+            }
+            const double di = sum ? cfl * Ai / acc : acc;
+            io.dt[c] = di;
+            kmin = kmin_(kmin, tkey(di));
+        } else {
+            const S gamma = (S)P.gamma, gm1 = gamma - S(1), cfl = (S)P.cfl;
+            const S ri = fast::rcp(qs[0]);
+            const S us = qs[1] * ri, vs = qs[2] * ri;
+            const S cs = fast::sqrt_(gamma * gm1 * (qs[3] * ri - S(0.5) * (us * us + vs * vs)));
+            const S Ai = AR[c];
+            S acc = sum ? S(0) : S(1);
 #pragma unroll
-                for (int f = 0; f < kMaxFaces; ++f) {
-                    if (w[f] == kFaceNone) continue;
-                    const int el = w[f] & kFaceEdgeMask, side = w[f] >> 15;
-                    const uint32_t ij = sij[el];
-                    const int o = side ? (int)(ij & 0xffff) : (int)(ij >> 16);
-                    const S n0 = snx[el], n1 = sny[el], le = sle[el];
-                    S qn[4];
-                    lds<S, 4>(rec + (size_t)o * R::NR, qn);
-                    const S rn = fast::rcp(qn[0]);
-                    const S un = qn[1] * rn, vn = qn[2] * rn;
-                    const S cn = fast::sqrt_(gamma * gm1 * (qn[3] * rn - S(0.5) * (un * un + vn * vn)));
-                    const bool ghost = (w[f] & 0x4000) != 0;
-                    if (sum) {
-                        const S center = fast::tmax(cs + fabs(us * n0 + vs * n1), cn + fabs(un * n0 + vn * n1));
-                        acc += center * le;
-                        if (ghost) {
-                            const int g = TP.halo[inf.z + o - T];
-                            const double dg = (double)(cfl * AR[g] * fast::rcp(center * le));
-                            io.dt[g] = dg;
-                            kmin = kmin_(kmin, tkey(dg));
-                        }
-                    } else {
-                        const S es = (cs + fabs(us)) * n0 + (cs + fabs(vs)) * n1;
-                        acc = fast::tmin(acc, cfl * Ai * fast::rcp(le * fabs(es)));
-                        if (ghost) {
-                            const int g = TP.halo[inf.z + o - T];
-                            const S en = (cn + fabs(un)) * n0 + (cn + fabs(vn)) * n1;
-                            const double dg = (double)fast::tmin(S(1), cfl * (S)AR[g] * fast::rcp(le * fabs(en)));
-                            io.dt[g] = dg;
-                            kmin = kmin_(kmin, tkey(dg));
-                        }
+            for (int f = 0; f < kMaxFaces; ++f) {
+                if (w[f] == kFaceNone) continue;
+                const int el = w[f] & kFaceEdgeMask, side = w[f] >> 15;
+                const uint32_t ij = sij[el];
+                const int o = side ? (int)(ij & 0xffff) : (int)(ij >> 16);
+                const S n0 = snx[el], n1 = sny[el], le = sle[el];
+                S qn[4];
+                lds<S, 4>(rec + (size_t)o * NR, qn);
+                const S rn = fast::rcp(qn[0]);
+                const S un = qn[1] * rn, vn = qn[2] * rn;
+                const S cn = fast::sqrt_(gamma * gm1 * (qn[3] * rn - S(0.5) * (un * un + vn * vn)));
+                const bool ghost = (w[f] & 0x4000) != 0;
+                if (sum) {
+                    const S center = fast::tmax(cs + fabs(us * n0 + vs * n1), cn + fabs(un * n0 + vn * n1));
+                    acc += center * le;
+                    if (ghost) {
+                        const int g = TP.halo[inf.z + o - T];
+                        const double dg = (double)(cfl * AR[g] * fast::rcp(center * le));
+                        io.dt[g] = dg;
+                        kmin = kmin_(kmin, tkey(dg));
+                    }
+                } else {
+                    const S es = (cs + fabs(us)) * n0 + (cs + fabs(vs)) * n1;
+                    acc = fast::tmin(acc, cfl * Ai * fast::rcp(le * fabs(es)));
+                    if (ghost) {
+                        const int g = TP.halo[inf.z + o - T];
+                        const S en = (cn + fabs(un)) * n0 + (cn + fabs(vn)) * n1;
+                        const double dg = (double)fast::tmin(S(1), cfl * (S)AR[g] * fast::rcp(le * fabs(en)));
+                        io.dt[g] = dg;
+                        kmin = kmin_(kmin, tkey(dg));
                     }
                 }
-                const double di = (double)(sum ? cfl * Ai * fast::rcp(acc) : acc);
-                io.dt[c] = di;
-                kmin = kmin_(kmin, tkey(di));
             }
+            const double di = (double)(sum ? cfl * Ai * fast::rcp(acc) : acc);
+            io.dt[c] = di;
+            kmin = kmin_(kmin, tkey(di));
         }
     }
+    return kmin;
+}
+
+// min_dt's global minimum (explicit.cpp:555-564): a block minimum, then one
+// atomic per block spread over kDtSlots slots of the tile's case.  Every
+// thread of the block calls it.
+__device__ __forceinline__ void tile_dt_reduce(const TileParams& TP, const TileIO& io, int t, int l, int nown,
+                                               unsigned long long kmin) {
+    __shared__ unsigned long long wmin[kTileMax / 32];
+    const Params& P = TP.P;
+    const int T = TP.T;
     if (P.global_dt && io.dtkeys != nullptr) {
         const int tc = P.n_cases > 1 ? P.tile_case[t] : 0;
         if (tc >= 0) {
@@ -380,8 +377,38 @@ __global__ void __launch_bounds__(kTileMax) k_tile_dt(TileParams TP, TileIO io) 
     }
 }
 
-// ------------------------------------------------ K1: gradients + limiters --
 template <class M, int V>
+__global__ void __launch_bounds__(kTileMax) k_tile_dt(TileParams TP, TileIO io) {
+    using S = typename M::S;
+    using R = Rec<M, V, false, false>;
+    if (t_inactive(io.ctrl)) return;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const Params& P = TP.P;
+    const int N = P.n_real, T = TP.T, t = blockIdx.x;
+    const int4 inf = TP.info[t];
+    const int c0 = t * T, nown = min(T, N - c0);
+    const int LT = T + TP.max_halo;
+    S* rec = reinterpret_cast<S*>(smem_raw);
+    S* snx = rec + (size_t)LT * R::NR;
+    S* sny = snx + TP.max_edges;
+    S* sle = sny + TP.max_edges;
+    uint32_t* sij = reinterpret_cast<uint32_t*>(sle + TP.max_edges);
+    const int l = threadIdx.x;
+    uint16_t w[kMaxFaces];
+    if (l < nown) load_faces(TP, c0 + l, w);  // latency overlaps the staging
+    stage_records<M, V, false, false>(TP, io, inf, c0, nown, rec);
+    stage_edges<S, false, false>(TP, inf, sij, snx, sny, sle, nullptr, nullptr, nullptr);
+    cpa_wait();
+    __syncthreads();
+    unsigned long long kmin = ~0ull;
+    if (l < nown) kmin = tile_cell_dt<M, V, R::NR>(TP, io, inf, l, c0 + l, w, rec, sij, snx, sny, sle);
+    if (P.global_dt && io.dtkeys != nullptr) tile_dt_reduce(TP, io, t, l, nown, kmin);
+}
+
+// ------------------------------------------------ K1: gradients + limiters --
+// DT: the first stage of a step also computes the step's time step here, from
+// the same staged state and edges (k_tile_dt's work without a second pass).
+template <class M, int V, bool DT>
 __global__ void __launch_bounds__(kTileMax) k_tile_gradlim(TileParams TP, TileIO io) {
     using S = typename M::S;
     using R = Rec<M, V, false, true>;
@@ -408,6 +435,11 @@ __global__ void __launch_bounds__(kTileMax) k_tile_gradlim(TileParams TP, TileIO
     stage_edges<S, true, true>(TP, inf, sij, snx, sny, sle, sg, sxf, syf);
     cpa_wait();
     __syncthreads();
+    if constexpr (DT) {
+        unsigned long long kmin = ~0ull;
+        if (l < nown) kmin = tile_cell_dt<M, V, R::NR>(TP, io, inf, l, c, w, rec, sij, snx, sny, sle);
+        if (P.global_dt && io.dtkeys != nullptr) tile_dt_reduce(TP, io, t, l, nown, kmin);
+    }
     if (l >= nown) return;
     const S* rs = rec + (size_t)l * R::NR;
     S qs[V], gx[V], gy[V], qmn[V], qmx[V], lim[V];
@@ -795,14 +827,16 @@ struct TileLaunch {
         };
         if (TP.P.V == 4) {
             set((const void*)k_tile_dt<M, 4>, smem_dt<M, 4>(TP));
-            set((const void*)k_tile_gradlim<M, 4>, smem_gradlim<M, 4>(TP));
+            set((const void*)k_tile_gradlim<M, 4, false>, smem_gradlim<M, 4>(TP));
+            set((const void*)k_tile_gradlim<M, 4, true>, smem_gradlim<M, 4>(TP));
             set((const void*)k_tile_stage<M, 4, true, 1>, smem_stage<M, 4, true>(TP));
             set((const void*)k_tile_stage<M, 4, false, 1>, smem_stage<M, 4, false>(TP));
             set((const void*)k_tile_stage<M, 4, true, 2>, smem_stage<M, 4, true>(TP));
             set((const void*)k_tile_stage<M, 4, false, 2>, smem_stage<M, 4, false>(TP));
         } else {
             set((const void*)k_tile_dt<M, 2>, smem_dt<M, 2>(TP));
-            set((const void*)k_tile_gradlim<M, 2>, smem_gradlim<M, 2>(TP));
+            set((const void*)k_tile_gradlim<M, 2, false>, smem_gradlim<M, 2>(TP));
+            set((const void*)k_tile_gradlim<M, 2, true>, smem_gradlim<M, 2>(TP));
             set((const void*)k_tile_stage<M, 2, true, 3>, smem_stage<M, 2, true>(TP));
             set((const void*)k_tile_stage<M, 2, false, 3>, smem_stage<M, 2, false>(TP));
         }
@@ -813,9 +847,15 @@ struct TileLaunch {
         if (TP.P.V == 4) k_tile_dt<M, 4><<<grid(TP), TP.T, smem_dt<M, 4>(TP), st>>>(TP, io);
         else k_tile_dt<M, 2><<<grid(TP), TP.T, smem_dt<M, 2>(TP), st>>>(TP, io);
     }
-    static void gradlim(const TileParams& TP, const TileIO& io, cudaStream_t st) {
-        if (TP.P.V == 4) k_tile_gradlim<M, 4><<<grid(TP), TP.T, smem_gradlim<M, 4>(TP), st>>>(TP, io);
-        else k_tile_gradlim<M, 2><<<grid(TP), TP.T, smem_gradlim<M, 2>(TP), st>>>(TP, io);
+    static void gradlim(const TileParams& TP, const TileIO& io, cudaStream_t st, bool with_dt) {
+        const int g = grid(TP);
+        if (TP.P.V == 4) {
+            if (with_dt) k_tile_gradlim<M, 4, true><<<g, TP.T, smem_gradlim<M, 4>(TP), st>>>(TP, io);
+            else k_tile_gradlim<M, 4, false><<<g, TP.T, smem_gradlim<M, 4>(TP), st>>>(TP, io);
+        } else {
+            if (with_dt) k_tile_gradlim<M, 2, true><<<g, TP.T, smem_gradlim<M, 2>(TP), st>>>(TP, io);
+            else k_tile_gradlim<M, 2, false><<<g, TP.T, smem_gradlim<M, 2>(TP), st>>>(TP, io);
+        }
     }
     static void stage(const TileParams& TP, const TileIO& io, cudaStream_t st) {
         const int g = grid(TP);
@@ -837,7 +877,8 @@ struct TileLaunch {
 namespace tile {
 cudaError_t prepare(int precision, const TileParams& TP);
 void launch_dt(int precision, const TileParams& TP, const TileIO& io, cudaStream_t st);
-void launch_gradlim(int precision, const TileParams& TP, const TileIO& io, cudaStream_t st);
+// with_dt: also the step's time step (io.dt, io.dtkeys), as launch_dt computes it
+void launch_gradlim(int precision, const TileParams& TP, const TileIO& io, cudaStream_t st, bool with_dt = false);
 void launch_stage(int precision, const TileParams& TP, const TileIO& io, cudaStream_t st);
 }  // namespace tile
 

@@ -6,8 +6,8 @@ namespace fvgpu {
 namespace tile {
 cudaError_t prepare_exact(const TileParams& TP) { return TileLaunch<MExact>::prepare(TP); }
 void launch_dt_exact(const TileParams& TP, const TileIO& io, cudaStream_t st) { TileLaunch<MExact>::dt(TP, io, st); }
-void launch_gradlim_exact(const TileParams& TP, const TileIO& io, cudaStream_t st) {
-    TileLaunch<MExact>::gradlim(TP, io, st);
+void launch_gradlim_exact(const TileParams& TP, const TileIO& io, cudaStream_t st, bool with_dt) {
+    TileLaunch<MExact>::gradlim(TP, io, st, with_dt);
 }
 void launch_stage_exact(const TileParams& TP, const TileIO& io, cudaStream_t st) {
     TileLaunch<MExact>::stage(TP, io, st);

@@ -6,7 +6,7 @@ namespace fvgpu {
 namespace tile {
 cudaError_t prepare_exact(const TileParams& TP);
 void launch_dt_exact(const TileParams& TP, const TileIO& io, cudaStream_t st);
-void launch_gradlim_exact(const TileParams& TP, const TileIO& io, cudaStream_t st);
+void launch_gradlim_exact(const TileParams& TP, const TileIO& io, cudaStream_t st, bool with_dt);
 void launch_stage_exact(const TileParams& TP, const TileIO& io, cudaStream_t st);
 
 cudaError_t prepare(int precision, const TileParams& TP) {
@@ -19,10 +19,10 @@ void launch_dt(int precision, const TileParams& TP, const TileIO& io, cudaStream
     else if (precision == 1) TileLaunch<MF64>::dt(TP, io, st);
     else TileLaunch<MF32>::dt(TP, io, st);
 }
-void launch_gradlim(int precision, const TileParams& TP, const TileIO& io, cudaStream_t st) {
-    if (precision == 0) launch_gradlim_exact(TP, io, st);
-    else if (precision == 1) TileLaunch<MF64>::gradlim(TP, io, st);
-    else TileLaunch<MF32>::gradlim(TP, io, st);
+void launch_gradlim(int precision, const TileParams& TP, const TileIO& io, cudaStream_t st, bool with_dt) {
+    if (precision == 0) launch_gradlim_exact(TP, io, st, with_dt);
+    else if (precision == 1) TileLaunch<MF64>::gradlim(TP, io, st, with_dt);
+    else TileLaunch<MF32>::gradlim(TP, io, st, with_dt);
 }
 void launch_stage(int precision, const TileParams& TP, const TileIO& io, cudaStream_t st) {
     if (precision == 0) launch_stage_exact(TP, io, st);
