@@ -658,7 +658,10 @@ static int enqueue_step(fv_solver* s, const std::vector<double>& alpha, int b, E
     io.dtkeys = s->keys;
     io.q_stage = s->sbase[b];
     // second order: the first stage's gradient kernel also computes dt
-    if (!TP.P.order2) { tile::launch_dt(s->precision, TP, io, st); ++n; mark(KK_DT); }
+    // every kernel after step_begin is a programmatic dependent of the one
+    // before it (its constant tile data is staged during that one's tail)
+    const bool pdl = true;
+    if (!TP.P.order2) { tile::launch_dt(s->precision, TP, io, st, pdl); ++n; mark(KK_DT); }
     const int ns = (int)alpha.size();
     const void* in = s->sbase[b];
     for (int k = 0; k < ns; ++k) {
@@ -681,11 +684,12 @@ static int enqueue_step(fv_solver* s, const std::vector<double>& alpha, int b, E
         }
         so.s_out = s->f32 ? out_s : nullptr;
         so.write_f64 = last ? 1 : 0;
-        if (TP.P.order2) { tile::launch_gradlim(s->precision, TP, so, st, k == 0); ++n; mark(KK_GRADLIM); }
-        tile::launch_stage(s->precision, TP, so, st); ++n; mark(KK_STAGE);
+        if (TP.P.order2) { tile::launch_gradlim(s->precision, TP, so, st, k == 0, pdl); ++n; mark(KK_GRADLIM); }
+        tile::launch_stage(s->precision, TP, so, st, pdl); ++n; mark(KK_STAGE);
         in = out_s;
     }
-    launch_step_end(TP.P, s->ctrl, s->limits, s->partials, s->n_tiles, s->dt, s->keys, s->hist, s->hist_cap, st);
+    launch_step_end(TP.P, s->ctrl, s->limits, s->partials, s->n_tiles, s->dt, s->keys, s->hist, s->hist_cap, st,
+                    pdl);
     ++n; mark(KK_END);
     return n;
 }

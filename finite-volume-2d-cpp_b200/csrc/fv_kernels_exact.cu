@@ -74,6 +74,9 @@ __global__ void k_step_begin(Ctrl* c, const RunLimits* L, int V, unsigned long l
 // (explicit.cpp:752-800).  Partial sums are reduced in a fixed order.
 __global__ void k_step_end(Params P, Ctrl* c, const RunLimits* L, const double* partials, int nblocks,
                            const double* dt, const unsigned long long* keys, PrintRec* hist, int hist_cap) {
+    // launched as a programmatic dependent of the last stage kernel: wait for
+    // it to complete before reading anything
+    asm volatile("griddepcontrol.wait;" ::: "memory");
     if (!c->active) return;
     if (P.n_cases > 1) {
         // each case of a batch keeps its own time: time += dt[0] of that case
@@ -128,8 +131,22 @@ void launch_step_begin(Ctrl* c, const RunLimits* lim, int V, unsigned long long*
     k_step_begin<<<1, 128, 0, st>>>(c, lim, V, keys, nkeys);
 }
 void launch_step_end(const Params& P, Ctrl* c, const RunLimits* lim, const double* partials, int nblocks,
-                     const double* dt, const unsigned long long* keys, PrintRec* hist, int hist_cap, cudaStream_t st) {
-    k_step_end<<<1, kBlock, 0, st>>>(P, c, lim, partials, nblocks, dt, keys, hist, hist_cap);
+                     const double* dt, const unsigned long long* keys, PrintRec* hist, int hist_cap, cudaStream_t st,
+                     bool pdl) {
+    if (!pdl) {
+        k_step_end<<<1, kBlock, 0, st>>>(P, c, lim, partials, nblocks, dt, keys, hist, hist_cap);
+        return;
+    }
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(1);
+    cfg.blockDim = dim3(kBlock);
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, k_step_end, P, c, lim, partials, nblocks, dt, keys, hist, hist_cap);
 }
 
 namespace exact {

@@ -82,6 +82,16 @@ __device__ __forceinline__ double tkey_inv(unsigned long long k) {
     return __longlong_as_double((long long)b);
 }
 __device__ __forceinline__ bool t_inactive(const Ctrl* c) { return c != nullptr && *(volatile const int*)&c->active == 0; }
+
+// Programmatic dependent launch.  Step kernels let the next kernel of the
+// stream start as soon as all of their CTAs run (pdl_trigger), so its CTAs
+// stage the constant tile data (geometry, face words) while this kernel's
+// last CTAs finish; pdl_wait() then blocks until the previous kernel has
+// completed and its writes are visible.  Nothing a previous kernel writes
+// is read, and nothing is written to global memory, before pdl_wait().
+// Without the launch attribute both are no-ops.
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 __device__ __forceinline__ unsigned long long kmin_(unsigned long long a, unsigned long long b) { return b < a ? b : a; }
 
 template <class S, int V>
@@ -381,7 +391,7 @@ template <class M, int V>
 __global__ void __launch_bounds__(kTileMax) k_tile_dt(TileParams TP, TileIO io) {
     using S = typename M::S;
     using R = Rec<M, V, false, false>;
-    if (t_inactive(io.ctrl)) return;
+    pdl_trigger();
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const Params& P = TP.P;
     const int N = P.n_real, T = TP.T, t = blockIdx.x;
@@ -395,9 +405,12 @@ __global__ void __launch_bounds__(kTileMax) k_tile_dt(TileParams TP, TileIO io) 
     uint32_t* sij = reinterpret_cast<uint32_t*>(sle + TP.max_edges);
     const int l = threadIdx.x;
     uint16_t w[kMaxFaces];
-    if (l < nown) load_faces(TP, c0 + l, w);  // latency overlaps the staging
-    stage_records<M, V, false, false>(TP, io, inf, c0, nown, rec);
+    // constant tile data first (may overlap the previous kernel's tail)
+    if (l < nown) load_faces(TP, c0 + l, w);
     stage_edges<S, false, false>(TP, inf, sij, snx, sny, sle, nullptr, nullptr, nullptr);
+    pdl_wait();
+    if (t_inactive(io.ctrl)) { cpa_wait(); return; }
+    stage_records<M, V, false, false>(TP, io, inf, c0, nown, rec);
     cpa_wait();
     __syncthreads();
     unsigned long long kmin = ~0ull;
@@ -412,7 +425,7 @@ template <class M, int V, bool DT>
 __global__ void __launch_bounds__(kTileMax) k_tile_gradlim(TileParams TP, TileIO io) {
     using S = typename M::S;
     using R = Rec<M, V, false, true>;
-    if (t_inactive(io.ctrl)) return;
+    pdl_trigger();
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const Params& P = TP.P;
     const int N = P.n_real, T = TP.T, t = blockIdx.x;
@@ -427,12 +440,14 @@ __global__ void __launch_bounds__(kTileMax) k_tile_gradlim(TileParams TP, TileIO
     const int c = c0 + l;
     uint16_t w[kMaxFaces];
     S A = S(1);
-    if (l < nown) {  // issued before the staging so that their latency overlaps it
+    if (l < nown) {  // constant tile data first (may overlap the previous kernel's tail)
         load_faces(TP, c, w);
         A = ((const S*)TP.area)[c];
     }
-    stage_records<M, V, false, true>(TP, io, inf, c0, nown, rec);
     stage_edges<S, true, true>(TP, inf, sij, snx, sny, sle, sg, sxf, syf);
+    pdl_wait();
+    if (t_inactive(io.ctrl)) { cpa_wait(); return; }
+    stage_records<M, V, false, true>(TP, io, inf, c0, nown, rec);
     cpa_wait();
     __syncthreads();
     if constexpr (DT) {
@@ -562,7 +577,7 @@ __global__ void __launch_bounds__(kTileMax) k_tile_stage(TileParams TP, TileIO i
     using S = typename M::S;
     using FT = typename std::conditional<M::exact, double, S>::type;  // flux storage
     using R = Rec<M, V, ORDER2, ORDER2>;
-    if (t_inactive(io.ctrl)) return;
+    pdl_trigger();
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ unsigned long long s_dtkey;
     const Params& P = TP.P;
@@ -582,15 +597,19 @@ __global__ void __launch_bounds__(kTileMax) k_tile_stage(TileParams TP, TileIO i
     uint16_t w[kMaxFaces];
     double qb[V];
     double A = 1.0, dtc = 0.0;
-    if (l < nown) {
+    if (l < nown) {  // constant tile data first (may overlap the previous kernel's tail)
         load_faces(TP, c, w);
-        ld<double, V>(io.q_base, c, qb);
         A = (double)((const S*)TP.area)[c];
+    }
+    if (ORDER2) stage_edges<S, false, true>(TP, inf, sij, snx, sny, sle, nullptr, sxf, syf);
+    else stage_edges<S, false, false>(TP, inf, sij, snx, sny, sle, nullptr, nullptr, nullptr);
+    pdl_wait();
+    if (t_inactive(io.ctrl)) { cpa_wait(); return; }
+    if (l < nown) {
+        ld<double, V>(io.q_base, c, qb);
         if (!global_dt) dtc = io.dt[c];
     }
     stage_records<M, V, ORDER2, ORDER2>(TP, io, inf, c0, nown, rec);
-    if (ORDER2) stage_edges<S, false, true>(TP, inf, sij, snx, sny, sle, nullptr, sxf, syf);
-    else stage_edges<S, false, false>(TP, inf, sij, snx, sny, sle, nullptr, nullptr, nullptr);
     // the tile's case (batches); -1: the tile spans two cases
     const int tc = (global_dt && P.n_cases > 1) ? P.tile_case[t] : 0;
     if (global_dt && tc >= 0 && threadIdx.x < 32) {
@@ -843,32 +862,52 @@ struct TileLaunch {
         return e;
     }
     static int grid(const TileParams& TP) { return (TP.P.n_real + TP.T - 1) / TP.T; }
-    static void dt(const TileParams& TP, const TileIO& io, cudaStream_t st) {
-        if (TP.P.V == 4) k_tile_dt<M, 4><<<grid(TP), TP.T, smem_dt<M, 4>(TP), st>>>(TP, io);
-        else k_tile_dt<M, 2><<<grid(TP), TP.T, smem_dt<M, 2>(TP), st>>>(TP, io);
+    // <<<>>> launch, or with programmatic stream serialisation (pdl)
+    template <class... A>
+    static void go(void (*k)(A...), int g, int b, size_t smem, cudaStream_t st, bool pdl, const TileParams& TP,
+                   const TileIO& io) {
+        if (!pdl) {
+            k<<<g, b, smem, st>>>(TP, io);
+            return;
+        }
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3((unsigned)g);
+        cfg.blockDim = dim3((unsigned)b);
+        cfg.dynamicSmemBytes = smem;
+        cfg.stream = st;
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        at[0].val.programmaticStreamSerializationAllowed = 1;
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+        cudaLaunchKernelEx(&cfg, k, TP, io);
     }
-    static void gradlim(const TileParams& TP, const TileIO& io, cudaStream_t st, bool with_dt) {
+    static void dt(const TileParams& TP, const TileIO& io, cudaStream_t st, bool pdl = false) {
+        if (TP.P.V == 4) go(k_tile_dt<M, 4>, grid(TP), TP.T, smem_dt<M, 4>(TP), st, pdl, TP, io);
+        else go(k_tile_dt<M, 2>, grid(TP), TP.T, smem_dt<M, 2>(TP), st, pdl, TP, io);
+    }
+    static void gradlim(const TileParams& TP, const TileIO& io, cudaStream_t st, bool with_dt, bool pdl = false) {
         const int g = grid(TP);
         if (TP.P.V == 4) {
-            if (with_dt) k_tile_gradlim<M, 4, true><<<g, TP.T, smem_gradlim<M, 4>(TP), st>>>(TP, io);
-            else k_tile_gradlim<M, 4, false><<<g, TP.T, smem_gradlim<M, 4>(TP), st>>>(TP, io);
+            if (with_dt) go(k_tile_gradlim<M, 4, true>, g, TP.T, smem_gradlim<M, 4>(TP), st, pdl, TP, io);
+            else go(k_tile_gradlim<M, 4, false>, g, TP.T, smem_gradlim<M, 4>(TP), st, pdl, TP, io);
         } else {
-            if (with_dt) k_tile_gradlim<M, 2, true><<<g, TP.T, smem_gradlim<M, 2>(TP), st>>>(TP, io);
-            else k_tile_gradlim<M, 2, false><<<g, TP.T, smem_gradlim<M, 2>(TP), st>>>(TP, io);
+            if (with_dt) go(k_tile_gradlim<M, 2, true>, g, TP.T, smem_gradlim<M, 2>(TP), st, pdl, TP, io);
+            else go(k_tile_gradlim<M, 2, false>, g, TP.T, smem_gradlim<M, 2>(TP), st, pdl, TP, io);
         }
     }
-    static void stage(const TileParams& TP, const TileIO& io, cudaStream_t st) {
+    static void stage(const TileParams& TP, const TileIO& io, cudaStream_t st, bool pdl = false) {
         const int g = grid(TP);
         const bool o2 = TP.P.order2 != 0;
         if (TP.P.flux == 3) {
-            if (o2) k_tile_stage<M, 2, true, 3><<<g, TP.T, smem_stage<M, 2, true>(TP), st>>>(TP, io);
-            else k_tile_stage<M, 2, false, 3><<<g, TP.T, smem_stage<M, 2, false>(TP), st>>>(TP, io);
+            if (o2) go(k_tile_stage<M, 2, true, 3>, g, TP.T, smem_stage<M, 2, true>(TP), st, pdl, TP, io);
+            else go(k_tile_stage<M, 2, false, 3>, g, TP.T, smem_stage<M, 2, false>(TP), st, pdl, TP, io);
         } else if (TP.P.flux == 1) {
-            if (o2) k_tile_stage<M, 4, true, 1><<<g, TP.T, smem_stage<M, 4, true>(TP), st>>>(TP, io);
-            else k_tile_stage<M, 4, false, 1><<<g, TP.T, smem_stage<M, 4, false>(TP), st>>>(TP, io);
+            if (o2) go(k_tile_stage<M, 4, true, 1>, g, TP.T, smem_stage<M, 4, true>(TP), st, pdl, TP, io);
+            else go(k_tile_stage<M, 4, false, 1>, g, TP.T, smem_stage<M, 4, false>(TP), st, pdl, TP, io);
         } else {
-            if (o2) k_tile_stage<M, 4, true, 2><<<g, TP.T, smem_stage<M, 4, true>(TP), st>>>(TP, io);
-            else k_tile_stage<M, 4, false, 2><<<g, TP.T, smem_stage<M, 4, false>(TP), st>>>(TP, io);
+            if (o2) go(k_tile_stage<M, 4, true, 2>, g, TP.T, smem_stage<M, 4, true>(TP), st, pdl, TP, io);
+            else go(k_tile_stage<M, 4, false, 2>, g, TP.T, smem_stage<M, 4, false>(TP), st, pdl, TP, io);
         }
     }
 };
@@ -876,10 +915,12 @@ struct TileLaunch {
 // Entry points per precision mode (defined in fv_tile_exact.cu / fv_tile_fast.cu).
 namespace tile {
 cudaError_t prepare(int precision, const TileParams& TP);
-void launch_dt(int precision, const TileParams& TP, const TileIO& io, cudaStream_t st);
+// pdl: launch with programmatic stream serialisation (the step sequence)
+void launch_dt(int precision, const TileParams& TP, const TileIO& io, cudaStream_t st, bool pdl = false);
 // with_dt: also the step's time step (io.dt, io.dtkeys), as launch_dt computes it
-void launch_gradlim(int precision, const TileParams& TP, const TileIO& io, cudaStream_t st, bool with_dt = false);
-void launch_stage(int precision, const TileParams& TP, const TileIO& io, cudaStream_t st);
+void launch_gradlim(int precision, const TileParams& TP, const TileIO& io, cudaStream_t st, bool with_dt = false,
+                    bool pdl = false);
+void launch_stage(int precision, const TileParams& TP, const TileIO& io, cudaStream_t st, bool pdl = false);
 }  // namespace tile
 
 }  // namespace fvgpu

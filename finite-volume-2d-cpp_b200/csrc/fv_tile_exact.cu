@@ -5,12 +5,14 @@
 namespace fvgpu {
 namespace tile {
 cudaError_t prepare_exact(const TileParams& TP) { return TileLaunch<MExact>::prepare(TP); }
-void launch_dt_exact(const TileParams& TP, const TileIO& io, cudaStream_t st) { TileLaunch<MExact>::dt(TP, io, st); }
-void launch_gradlim_exact(const TileParams& TP, const TileIO& io, cudaStream_t st, bool with_dt) {
-    TileLaunch<MExact>::gradlim(TP, io, st, with_dt);
+void launch_dt_exact(const TileParams& TP, const TileIO& io, cudaStream_t st, bool pdl) {
+    TileLaunch<MExact>::dt(TP, io, st, pdl);
 }
-void launch_stage_exact(const TileParams& TP, const TileIO& io, cudaStream_t st) {
-    TileLaunch<MExact>::stage(TP, io, st);
+void launch_gradlim_exact(const TileParams& TP, const TileIO& io, cudaStream_t st, bool with_dt, bool pdl) {
+    TileLaunch<MExact>::gradlim(TP, io, st, with_dt, pdl);
+}
+void launch_stage_exact(const TileParams& TP, const TileIO& io, cudaStream_t st, bool pdl) {
+    TileLaunch<MExact>::stage(TP, io, st, pdl);
 }
 }  // namespace tile
 }  // namespace fvgpu

@@ -5,29 +5,29 @@
 namespace fvgpu {
 namespace tile {
 cudaError_t prepare_exact(const TileParams& TP);
-void launch_dt_exact(const TileParams& TP, const TileIO& io, cudaStream_t st);
-void launch_gradlim_exact(const TileParams& TP, const TileIO& io, cudaStream_t st, bool with_dt);
-void launch_stage_exact(const TileParams& TP, const TileIO& io, cudaStream_t st);
+void launch_dt_exact(const TileParams& TP, const TileIO& io, cudaStream_t st, bool pdl);
+void launch_gradlim_exact(const TileParams& TP, const TileIO& io, cudaStream_t st, bool with_dt, bool pdl);
+void launch_stage_exact(const TileParams& TP, const TileIO& io, cudaStream_t st, bool pdl);
 
 cudaError_t prepare(int precision, const TileParams& TP) {
     if (precision == 0) return prepare_exact(TP);
     if (precision == 1) return TileLaunch<MF64>::prepare(TP);
     return TileLaunch<MF32>::prepare(TP);
 }
-void launch_dt(int precision, const TileParams& TP, const TileIO& io, cudaStream_t st) {
-    if (precision == 0) launch_dt_exact(TP, io, st);
-    else if (precision == 1) TileLaunch<MF64>::dt(TP, io, st);
-    else TileLaunch<MF32>::dt(TP, io, st);
+void launch_dt(int precision, const TileParams& TP, const TileIO& io, cudaStream_t st, bool pdl) {
+    if (precision == 0) launch_dt_exact(TP, io, st, pdl);
+    else if (precision == 1) TileLaunch<MF64>::dt(TP, io, st, pdl);
+    else TileLaunch<MF32>::dt(TP, io, st, pdl);
 }
-void launch_gradlim(int precision, const TileParams& TP, const TileIO& io, cudaStream_t st, bool with_dt) {
-    if (precision == 0) launch_gradlim_exact(TP, io, st, with_dt);
-    else if (precision == 1) TileLaunch<MF64>::gradlim(TP, io, st, with_dt);
-    else TileLaunch<MF32>::gradlim(TP, io, st, with_dt);
+void launch_gradlim(int precision, const TileParams& TP, const TileIO& io, cudaStream_t st, bool with_dt, bool pdl) {
+    if (precision == 0) launch_gradlim_exact(TP, io, st, with_dt, pdl);
+    else if (precision == 1) TileLaunch<MF64>::gradlim(TP, io, st, with_dt, pdl);
+    else TileLaunch<MF32>::gradlim(TP, io, st, with_dt, pdl);
 }
-void launch_stage(int precision, const TileParams& TP, const TileIO& io, cudaStream_t st) {
-    if (precision == 0) launch_stage_exact(TP, io, st);
-    else if (precision == 1) TileLaunch<MF64>::stage(TP, io, st);
-    else TileLaunch<MF32>::stage(TP, io, st);
+void launch_stage(int precision, const TileParams& TP, const TileIO& io, cudaStream_t st, bool pdl) {
+    if (precision == 0) launch_stage_exact(TP, io, st, pdl);
+    else if (precision == 1) TileLaunch<MF64>::stage(TP, io, st, pdl);
+    else TileLaunch<MF32>::stage(TP, io, st, pdl);
 }
 }  // namespace tile
 }  // namespace fvgpu
