@@ -50,6 +50,12 @@ ALGO_BYTES = {
 }
 
 
+# DRAM bytes per real cell of one k_tile_stage launch (dram__bytes_read.sum +
+# dram__bytes_write.sum of one ncu capture of the forward-step workload,
+# profiles/k_tile_stage_fp32_forward_step.md), scaled by the cells of a launch.
+TRAFFIC_B_PER_CELL = {"fp32": {"stage": 151.6}}
+
+
 def build_workload(name):
     """(element mesh or list of case meshes, physics, RK stages, ic(mesh, geometry) -> q, description)"""
     if name == "step":
@@ -285,7 +291,10 @@ def measure_mode(args, em, mesh, geo, ph, alpha, ic, precision, local, dist, wor
     out["roofline"] = {"bound": "hbm", "kernel": "flux + RK update + ghost fill (k_tile_stage)",
                        "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                        "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind,
-                       "traffic": None, "algorithmic_bytes_per_launch": kb}
+                       "traffic": (TRAFFIC_B_PER_CELL[precision]["stage"] * N
+                                   if args.workload == "step" and precision in TRAFFIC_B_PER_CELL else None),
+                       "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, forward-step capture",
+                       "algorithmic_bytes_per_launch": kb}
     if ph.order2:
         kg = ALGO_BYTES[precision]["grad_lim"] * N
         out["roofline_grad_lim"] = {"achieved": kg / (out["per_launch_ms"]["grad_lim"] / 1e3) / 1e9,
