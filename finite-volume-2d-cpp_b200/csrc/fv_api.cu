@@ -647,12 +647,15 @@ struct EventLog {
 // Enqueues one time step (explicit.cpp:715-801) whose base state is
 // qbase[b] (RK1 writes its result to qbase[1-b]).  Returns the number of
 // kernels launched.
-static int enqueue_step(fv_solver* s, const std::vector<double>& alpha, int b, EventLog* log = nullptr) {
+// first: the first step of a launch sequence, which starts with the
+// begin-of-step kernel (every step end also begins the next step).
+static int enqueue_step(fv_solver* s, const std::vector<double>& alpha, int b, EventLog* log = nullptr,
+                        bool first = true) {
     const TileParams& TP = s->TP;
     cudaStream_t st = s->stream;
     int n = 0;
     auto mark = [&](int k) { if (log) log->mark(k); };
-    launch_step_begin(s->ctrl, s->limits, s->V, s->keys, s->n_cases * kDtSlots, st); ++n; mark(KK_BEGIN);
+    if (first) { launch_step_begin(s->ctrl, s->limits, s->V, s->keys, s->n_cases * kDtSlots, st); ++n; mark(KK_BEGIN); }
     TileIO io{};
     io.gx = s->gx; io.gy = s->gy; io.lim = s->lim; io.dt = s->dt; io.ctrl = s->ctrl;
     io.dtkeys = s->keys;
@@ -688,8 +691,8 @@ static int enqueue_step(fv_solver* s, const std::vector<double>& alpha, int b, E
         tile::launch_stage(s->precision, TP, so, st, pdl); ++n; mark(KK_STAGE);
         in = out_s;
     }
-    launch_step_end(TP.P, s->ctrl, s->limits, s->partials, s->n_tiles, s->dt, s->keys, s->hist, s->hist_cap, st,
-                    pdl);
+    launch_step_end(TP.P, s->ctrl, s->limits, s->partials, s->n_tiles, s->dt, s->keys, s->n_cases * kDtSlots,
+                    s->hist, s->hist_cap, st, pdl);
     ++n; mark(KK_END);
     return n;
 }
@@ -705,7 +708,8 @@ static int get_graph(fv_solver* s, const std::vector<double>& alpha, int len, Gr
     cudaGraph_t graph;
     CK(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
     int launches = 0;
-    for (int k = 0; k < len; ++k) launches += enqueue_step(s, alpha, (alpha.size() == 1 && (k % 2)) ? 1 : 0);
+    for (int k = 0; k < len; ++k)
+        launches += enqueue_step(s, alpha, (alpha.size() == 1 && (k % 2)) ? 1 : 0, nullptr, k == 0);
     cudaError_t e = cudaStreamEndCapture(s->stream, &graph);
     if (e != cudaSuccess) return fail(FV_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
     e = cudaGraphInstantiate(&g.exec, graph, 0);
@@ -822,7 +826,7 @@ int fv_profile_kernels(fv_solver* s, const double* alpha, int32_t n_alpha, int32
     EventLog log;
     log.st = st;
     log.mark(-1);
-    for (int k = 0; k < n_steps; ++k) enqueue_step(s, a, (a.size() == 1 && (k % 2)) ? 1 : 0, &log);
+    for (int k = 0; k < n_steps; ++k) enqueue_step(s, a, (a.size() == 1 && (k % 2)) ? 1 : 0, &log, k == 0);
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(st));
     for (int k = 0; k < KK_N; ++k) { out_ms[k] = 0.0; out_count[k] = 0; }

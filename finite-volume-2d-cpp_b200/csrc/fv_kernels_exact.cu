@@ -55,9 +55,8 @@ __device__ __forceinline__ void store_cell(double* __restrict__ a, int c, const 
 }
 
 // ------------------------------------------------------------ step control --
-__global__ void k_step_begin(Ctrl* c, const RunLimits* L, int V, unsigned long long* keys, int nkeys) {
-    for (int i = threadIdx.x; i < nkeys; i += blockDim.x) keys[i] = ~0ull;
-    if (threadIdx.x != 0) return;
+// Stop criteria of the step about to start (explicit.cpp:717-726), one thread.
+__device__ void begin_step(Ctrl* c, const RunLimits* L, int V) {
     double Rmax;
     if (c->step > 0) {
         Rmax = 0.0;
@@ -70,10 +69,17 @@ __global__ void k_step_begin(Ctrl* c, const RunLimits* L, int V, unsigned long l
     c->need_R = !stop && (c->step == 0 || (c->step % L->print_interval) == 0 || (L->tolerance > 1.01e-16));
 }
 
+__global__ void k_step_begin(Ctrl* c, const RunLimits* L, int V, unsigned long long* keys, int nkeys) {
+    for (int i = threadIdx.x; i < nkeys; i += blockDim.x) keys[i] = ~0ull;
+    if (threadIdx.x == 0) begin_step(c, L, V);
+}
+
 // Residual norms, step/time bookkeeping and print records
-// (explicit.cpp:752-800).  Partial sums are reduced in a fixed order.
+// (explicit.cpp:752-800), then the next step's start: its stop criteria and
+// fresh dt key slots, so that consecutive steps need no separate begin
+// kernel.  Partial sums are reduced in a fixed order.
 __global__ void k_step_end(Params P, Ctrl* c, const RunLimits* L, const double* partials, int nblocks,
-                           const double* dt, const unsigned long long* keys, PrintRec* hist, int hist_cap) {
+                           const double* dt, unsigned long long* keys, int nkeys, PrintRec* hist, int hist_cap) {
     // launched as a programmatic dependent of the last stage kernel: wait for
     // it to complete before reading anything
     asm volatile("griddepcontrol.wait;" ::: "memory");
@@ -105,7 +111,7 @@ __global__ void k_step_end(Params P, Ctrl* c, const RunLimits* L, const double* 
             __syncthreads();
         }
     }
-    if (threadIdx.x != 0) return;
+    if (threadIdx.x == 0) {
     if (c->need_R) {
         for (int k = 0; k < V; ++k) c->Rraw[k] = sqrt(red[0][k]);
         if (c->step == 0) {
@@ -125,16 +131,20 @@ __global__ void k_step_end(Params P, Ctrl* c, const RunLimits* L, const double* 
     const double dt0 = P.global_dt ? global_dt_value(P, dt, keys) : dt[P.cell0];
     c->step += 1;
     c->time += dt0;
+    begin_step(c, L, V);
+    }
+    __syncthreads();  // the keys have been read
+    for (int i = threadIdx.x; i < nkeys; i += blockDim.x) keys[i] = ~0ull;
 }
 
 void launch_step_begin(Ctrl* c, const RunLimits* lim, int V, unsigned long long* keys, int nkeys, cudaStream_t st) {
     k_step_begin<<<1, 128, 0, st>>>(c, lim, V, keys, nkeys);
 }
 void launch_step_end(const Params& P, Ctrl* c, const RunLimits* lim, const double* partials, int nblocks,
-                     const double* dt, const unsigned long long* keys, PrintRec* hist, int hist_cap, cudaStream_t st,
-                     bool pdl) {
+                     const double* dt, unsigned long long* keys, int nkeys, PrintRec* hist, int hist_cap,
+                     cudaStream_t st, bool pdl) {
     if (!pdl) {
-        k_step_end<<<1, kBlock, 0, st>>>(P, c, lim, partials, nblocks, dt, keys, hist, hist_cap);
+        k_step_end<<<1, kBlock, 0, st>>>(P, c, lim, partials, nblocks, dt, keys, nkeys, hist, hist_cap);
         return;
     }
     cudaLaunchConfig_t cfg = {};
@@ -146,7 +156,7 @@ void launch_step_end(const Params& P, Ctrl* c, const RunLimits* lim, const doubl
     at[0].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = at;
     cfg.numAttrs = 1;
-    cudaLaunchKernelEx(&cfg, k_step_end, P, c, lim, partials, nblocks, dt, keys, hist, hist_cap);
+    cudaLaunchKernelEx(&cfg, k_step_end, P, c, lim, partials, nblocks, dt, keys, nkeys, hist, hist_cap);
 }
 
 namespace exact {

@@ -13,7 +13,7 @@ inline int grid_for(int n) { return (n + kBlock - 1) / kBlock; }
 // keys: the dt minimum's ordered-key slots ([n_cases][64]), reset every step
 void launch_step_begin(Ctrl* c, const RunLimits* lim, int V, unsigned long long* keys, int nkeys, cudaStream_t st);
 void launch_step_end(const Params& P, Ctrl* c, const RunLimits* lim, const double* partials,
-                     int nblocks, const double* dt, const unsigned long long* keys, PrintRec* hist, int hist_cap,
+                     int nblocks, const double* dt, unsigned long long* keys, int nkeys, PrintRec* hist, int hist_cap,
                      cudaStream_t st, bool pdl = false);
 
 // initial / standalone ghost fill (update_bounds) in FP64 (fv_kernels_exact.cu)
