@@ -239,6 +239,17 @@ int fv_mesh_case_offsets(const fv_mesh* fm, int64_t* real_off, int64_t* bound_of
     return FV_OK;
 }
 
+int fv_mesh_read_su2(const char* path, fv_mesh** out) {
+    if (!path || !out) return fail(FV_ERR_ARG, "fv_mesh_read_su2: invalid arguments");
+    auto* fm = new fv_mesh();
+    std::string err = read_su2(path, fm->m);
+    if (!err.empty()) {
+        delete fm;
+        return fail(err.rfind("cannot open", 0) == 0 ? FV_ERR_IO : FV_ERR_MESH, err);
+    }
+    return finish_mesh(fm, out);
+}
+
 void fv_mesh_destroy(fv_mesh* m) { delete m; }
 
 int fv_mesh_sizes(const fv_mesh* fm, int64_t* out) {

@@ -500,4 +500,95 @@ std::string read_msh41(const std::string& path, HostMesh& m) {
     return "";
 }
 
+// SU2 native mesh (ASCII, 2D): NDIME= 2; NELEM= n with one element per line
+// (VTK type 5 = triangle, 9 = quadrilateral, node indices, optional element
+// index); NPOIN= n with "x y [index]" lines; NMARK= n, each MARKER_TAG= name
+// with MARKER_ELEMS= n lines of type 3 (segment) and two node indices.
+// Nodes, cells and boundary segments keep file order; boundary groups are the
+// marker tags in file order.  The reference reads Gmsh files only: its
+// examples/naca ships SU2 meshes to be converted with gmsh first
+// (examples/naca/naca.geo:1-7).
+std::string read_su2(const std::string& path, HostMesh& m) {
+    std::ifstream in(path);
+    if (!in) return "cannot open " + path;
+    m.nodes_x.clear(); m.nodes_y.clear(); m.cells4.clear();
+    m.bnd_nodes.clear(); m.bnd_group.clear(); m.group_names.clear();
+    std::string line;
+    auto value_of = [](const std::string& l, const char* key, long* v) -> bool {
+        const size_t k = l.find(key);
+        if (k == std::string::npos) return false;
+        *v = std::strtol(l.c_str() + k + std::strlen(key), nullptr, 10);
+        return true;
+    };
+    long ndime = 0, nelem = -1, npoin = -1;
+    std::vector<int32_t> cells;
+    try {
+        while (std::getline(in, line)) {
+            if (!line.empty() && line.back() == '\r') line.pop_back();
+            const size_t c = line.find('%');
+            if (c != std::string::npos) line.erase(c);
+            long v;
+            if (value_of(line, "NDIME=", &v)) {
+                ndime = v;
+                if (ndime != 2) return "SU2 mesh is not two-dimensional (NDIME= " + std::to_string(ndime) + ")";
+            } else if (value_of(line, "NELEM=", &v)) {
+                nelem = v;
+                cells.reserve((size_t)nelem * 4);
+                for (long e = 0; e < nelem; ++e) {
+                    if (!std::getline(in, line)) return "SU2: NELEM section ends early";
+                    std::istringstream ss(line);
+                    long type;
+                    ss >> type;
+                    const int nn = type == 5 ? 3 : type == 9 ? 4 : 0;
+                    if (!nn) return "SU2: element type " + std::to_string(type) + " is not a triangle or quadrilateral";
+                    int32_t id[4] = {-1, -1, -1, -1};
+                    for (int k = 0; k < nn; ++k) {
+                        long x;
+                        if (!(ss >> x)) return "SU2: short element line";
+                        id[k] = (int32_t)x;
+                    }
+                    cells.insert(cells.end(), id, id + 4);
+                }
+            } else if (value_of(line, "NPOIN=", &v)) {
+                npoin = v;
+                m.nodes_x.reserve((size_t)npoin); m.nodes_y.reserve((size_t)npoin);
+                for (long i = 0; i < npoin; ++i) {
+                    if (!std::getline(in, line)) return "SU2: NPOIN section ends early";
+                    char* e1;
+                    char* e2;
+                    const double x = std::strtod(line.c_str(), &e1);
+                    const double y = std::strtod(e1, &e2);
+                    if (e1 == line.c_str() || e2 == e1) return "SU2: bad point line";
+                    m.nodes_x.push_back(x); m.nodes_y.push_back(y);
+                }
+            } else if (line.find("MARKER_TAG=") != std::string::npos) {
+                std::string name = line.substr(line.find("MARKER_TAG=") + 11);
+                name.erase(0, name.find_first_not_of(" \t"));
+                name.erase(name.find_last_not_of(" \t") + 1);
+                long ne = 0;
+                while (std::getline(in, line) && !value_of(line, "MARKER_ELEMS=", &ne)) {}
+                const int32_t g = (int32_t)m.group_names.size();
+                m.group_names.push_back(name);
+                for (long e = 0; e < ne; ++e) {
+                    if (!std::getline(in, line)) return "SU2: MARKER_ELEMS section ends early";
+                    std::istringstream ss(line);
+                    long type, a, b;
+                    if (!(ss >> type >> a >> b) || type != 3) return "SU2: boundary element of marker " + name + " is not a segment";
+                    m.bnd_nodes.push_back((int32_t)a); m.bnd_nodes.push_back((int32_t)b);
+                    m.bnd_group.push_back(g);
+                }
+            }
+        }
+    } catch (const std::exception& e) {
+        return std::string("SU2 parse error: ") + e.what();
+    }
+    if (ndime != 2 || nelem < 0 || npoin < 0) return "SU2 mesh without NDIME= 2, NELEM= or NPOIN=";
+    for (int32_t id : cells)
+        if (id >= npoin) return "SU2: element node index out of range";
+    for (int32_t id : m.bnd_nodes)
+        if (id < 0 || id >= npoin) return "SU2: marker node index out of range";
+    m.cells4.swap(cells);
+    return "";
+}
+
 }  // namespace fvgpu

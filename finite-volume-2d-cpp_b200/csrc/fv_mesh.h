@@ -83,5 +83,7 @@ void build_device_numbering(HostMesh& m);
 // Gmsh MSH 4.1 ASCII reader (the subset fvhyper's reader accepts,
 // mesh.cpp:264-570).  Fills the element-mesh part of m.
 std::string read_msh41(const std::string& path, HostMesh& m);
+// SU2 native ASCII mesh, 2D (triangles, quadrilaterals, segment markers).
+std::string read_su2(const std::string& path, HostMesh& m);
 
 }  // namespace fvgpu

@@ -105,9 +105,18 @@ class Mesh:
         return cls(h.value, em.group_names)
 
     @classmethod
+    def read_su2(cls, path):
+        """SU2 native ASCII mesh (2D); boundary groups are the marker tags."""
+        return cls._read(lib().fv_mesh_read_su2, path)
+
+    @classmethod
     def read_msh(cls, path):
+        return cls._read(lib().fv_mesh_read_msh, path)
+
+    @classmethod
+    def _read(cls, fn, path):
         h = C.c_void_p()
-        _check(lib().fv_mesh_read_msh(os.fsencode(path), C.byref(h)))
+        _check(fn(os.fsencode(path), C.byref(h)))
         n = lib().fv_mesh_group_count(h)
         names = []
         for i in range(n):

@@ -345,3 +345,25 @@ def write_msh41(path: str, m: ElementMesh) -> None:
             f.write("\n".join(" ".join(map(str, r)) for r in arr.tolist()) + "\n")
             tag += conn.shape[0]
         f.write("$EndElements\n")
+
+
+def write_su2(path: str, m: ElementMesh) -> None:
+    """SU2 native ASCII mesh: triangles (VTK 5) / quadrilaterals (VTK 9), one
+    marker per boundary group with its segments (VTK 3), in array order."""
+    lines = ["NDIME= 2", f"NELEM= {m.cells.shape[0]}"]
+    for e, c in enumerate(m.cells):
+        if c[3] < 0:
+            lines.append(f"5 {c[0]} {c[1]} {c[2]} {e}")
+        else:
+            lines.append(f"9 {c[0]} {c[1]} {c[2]} {c[3]} {e}")
+    lines.append(f"NPOIN= {m.nodes_x.size}")
+    for i in range(m.nodes_x.size):
+        lines.append(f"{m.nodes_x[i]:.17g} {m.nodes_y[i]:.17g} {i}")
+    lines.append(f"NMARK= {len(m.group_names)}")
+    for g, name in enumerate(m.group_names):
+        segs = m.bnd_nodes[m.bnd_group == g]
+        lines.append(f"MARKER_TAG= {name}")
+        lines.append(f"MARKER_ELEMS= {segs.shape[0]}")
+        lines += [f"3 {a} {b}" for a, b in segs]
+    with open(path, "w") as f:
+        f.write("\n".join(lines) + "\n")

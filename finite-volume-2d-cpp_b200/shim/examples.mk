@@ -10,7 +10,11 @@ PKG := $(abspath $(HERE)..)
 OUT := $(HERE)_examples
 EXAMPLES := shockTube forwardStep naca burgers flatPlate heatTransfer nacaTransient
 
-all: $(EXAMPLES:%=$(OUT)/%)
+all: $(EXAMPLES:%=$(OUT)/%) $(OUT)/naca0012_129.su2
+
+# the SU2 mesh fvhyper ships for its NACA example (read directly by the shim)
+$(OUT)/naca0012_129.su2: $(REF)/examples/naca/naca0012_129.su2 | $(OUT)
+	cp $< $@
 
 $(OUT):
 	mkdir -p $(OUT)

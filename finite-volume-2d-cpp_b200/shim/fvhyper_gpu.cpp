@@ -123,7 +123,16 @@ void mesh::attach(::fv_mesh* dm, bool bind_bounds) {
 void mesh::read_file(std::string name, mpi_wrapper& pool) {
     filename = (pool.size > 1) ? (name + "_" + std::to_string(pool.rank + 1) + ".msh") : name + ".msh";
     ::fv_mesh* dm = nullptr;
-    const int rc = fv_mesh_read_msh(filename.c_str(), &dm);
+    int rc;
+    // B200 build: without <name>.msh, an SU2 mesh <name>.su2 is read instead
+    // (marker tags are the boundary names)
+    const std::string su2 = name + ".su2";
+    if (!std::ifstream(filename).good() && std::ifstream(su2).good()) {
+        filename = su2;
+        rc = fv_mesh_read_su2(filename.c_str(), &dm);
+    } else {
+        rc = fv_mesh_read_msh(filename.c_str(), &dm);
+    }
     if (rc != FV_OK) fail_rc(rc, "mesh::read_file(" + filename + ")");
     attach(dm, true);
 }

@@ -119,6 +119,11 @@ int fv_mesh_create(int64_t n_nodes, const double* nodes_x, const double* nodes_y
 /* Gmsh MSH 4.1 ASCII file (single partition) -> mesh; boundary groups are
  * the physical names of the boundary curves, in order of first use. */
 int fv_mesh_read_msh(const char* path, fv_mesh** out);
+/* SU2 native ASCII mesh (2D: triangles, quadrilaterals, segment markers) ->
+ * mesh; boundary groups are the marker tags in file order, nodes and cells
+ * keep file order.  No counterpart in the reference, whose reader takes Gmsh
+ * files only (examples/naca/naca.geo:1-7 converts its SU2 meshes first). */
+int fv_mesh_read_su2(const char* path, fv_mesh** out);
 /* A batch of independent cases as one mesh (the disjoint union of the case
  * meshes): reference numbering = the real cells of case 0, 1, ..., then the
  * ghosts of case 0, 1, ...; boundary groups are merged by name.  A solver on

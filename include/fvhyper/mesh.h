@@ -104,8 +104,9 @@ public:
 
     uint nRealCells = 0;
 
-    // Reads "<name>.msh" (Gmsh MSH 4.1 ASCII, fvhyper/src/mesh.cpp:800-855) and
-    // binds each boundary edge to boundaries::bounds[physical name].
+    // Reads "<name>.msh" (Gmsh MSH 4.1 ASCII, fvhyper/src/mesh.cpp:800-855),
+    // or "<name>.su2" (SU2 native ASCII) when there is no .msh file, and
+    // binds each boundary edge to boundaries::bounds[physical name / marker tag].
     void read_file(std::string filename, mpi_wrapper& pool);
 
     // B200 build: the device-side mesh this object was read into (owned).

@@ -145,3 +145,48 @@ def test_cpp_adjoint_api_matches_python_binding(tmp_path):
     loss, g = adj.gradient(np.array(theta))
     assert vals[0] == loss and vals[1:] == g.tolist()
     adj.close()
+
+
+def test_su2_reader_matches_element_path(tmp_path):
+    """An SU2 file of a mesh gives the geometry of the same element mesh
+    (which the MSH reader and fv_mesh_create build as the reference does)."""
+    for em in (meshgen.forward_step(n=20), meshgen.naca_ogrid(ni=48, nj=12, r_far=10.0),
+               meshgen.rect_tri(6, 3, 1.0, 0.5)):
+        path = str(tmp_path / "m.su2")
+        meshgen.write_su2(path, em)
+        a = fvgpu.Mesh.read_su2(path)
+        b = fvgpu.Mesh.from_elements(em)
+        assert a.group_names == list(em.group_names)
+        ga, gb = a.geometry(), b.geometry()
+        for k in ga:
+            assert bits_equal(ga[k], gb[k]), k
+
+
+def test_su2_reader_reads_the_reference_naca_meshes():
+    """The SU2 meshes fvhyper ships for its NACA example (to be converted with
+    gmsh there) are read directly: quadrilateral O-grids, closed, with the
+    airfoil and farfield markers."""
+    base = "/root/reference/examples/naca"
+    if not os.path.isdir(base):
+        pytest.skip("fvhyper checkout not present")
+    for fn, ncell in (("naca0012_129.su2", 16384), ("NACA_M.su2", 4096)):
+        m = fvgpu.Mesh.read_su2(os.path.join(base, fn))
+        assert m.n_real == ncell and sorted(m.group_names) == ["airfoil", "farfield"]
+        g = m.geometry()
+        assert np.all(g["area"] > 0)
+        # every real cell's outward fluxes of a constant field cancel (closed cells)
+        s = np.zeros((m.n_total, 2))
+        ec = g["edge_cells"].reshape(-1, 2).astype(np.int64)
+        for d, n in ((0, g["enx"]), (1, g["eny"])):
+            np.add.at(s[:, d], ec[:, 0], n * g["elen"])
+            np.add.at(s[:, d], ec[:, 1], -n * g["elen"])
+        assert np.abs(s[: m.n_real]).max() < 1e-12 * max(1.0, g["elen"].max())
+
+
+def test_su2_reader_errors(tmp_path):
+    bad = tmp_path / "bad.su2"
+    bad.write_text("NDIME= 3\nNELEM= 0\nNPOIN= 0\n")
+    with pytest.raises(fvgpu.FvError, match="two-dimensional"):
+        fvgpu.Mesh.read_su2(str(bad))
+    with pytest.raises(fvgpu.FvError):
+        fvgpu.Mesh.read_su2(str(tmp_path / "missing.su2"))
