@@ -89,6 +89,8 @@ struct fv_solver {
     int n_cases = 1;
     double* case_time = nullptr;                           // batches: [n_cases]
     double* ghost_bv = nullptr;                            // per-ghost boundary states [n_bound][4]
+    Ctrl* hctrl = nullptr;      // mapped pinned host copy of the run control, written by a kernel
+    Ctrl* hctrl_dev = nullptr;  // its device address
     std::vector<int64_t> case_real_off, case_bound_off;    // batches: host copies
 
     template <class T>
@@ -102,6 +104,7 @@ struct fv_solver {
         for (auto& g : graphs)
             if (g.exec) cudaGraphExecDestroy(g.exec);
         for (void* p : allocs) cudaFree(p);
+        if (hctrl) cudaFreeHost(hctrl);  // allocated with cudaHostAlloc
         if (own_stream && stream) cudaStreamDestroy(stream);
     }
 };
@@ -417,6 +420,8 @@ int fv_solver_create_ex(const fv_mesh* fm, const fv_physics* ph, int32_t precisi
     CK(s->alloc(&s->scratch2, 8));
     CK(s->alloc(&s->flag, 4));
     CK(s->alloc(&s->ctrl, 1));
+    CK(cudaHostAlloc((void**)&s->hctrl, sizeof(Ctrl), cudaHostAllocMapped));
+    CK(cudaHostGetDevicePointer((void**)&s->hctrl_dev, s->hctrl, 0));
     CK(s->alloc(&s->limits, 1));
     s->hist_cap = 4096;
     CK(s->alloc(&s->hist, (size_t)s->hist_cap));
@@ -550,8 +555,12 @@ static int set_state_common(fv_solver* s, const double* q, cudaMemcpyKind kind) 
     if (!s || !q) return fail(FV_ERR_ARG, "null argument");
     CK(cudaSetDevice(s->device));
     const size_t nq = (size_t)s->n_total * s->V;
-    CK(cudaMemcpyAsync(s->stage_buf, q, nq * 8, kind, s->stream));
-    launch_permute_to_device(s->stage_buf, s->qbase[0], s->new2ref, (int)s->n_total, s->V, s->stream);
+    const double* src = q;
+    if (kind != cudaMemcpyDeviceToDevice) {  // device input is permuted in place, without a copy
+        CK(cudaMemcpyAsync(s->stage_buf, q, nq * 8, kind, s->stream));
+        src = s->stage_buf;
+    }
+    launch_permute_to_device(src, s->qbase[0], s->new2ref, (int)s->n_total, s->V, s->stream);
     sync_shadow(s, 0);
     CK(cudaGetLastError());
     return FV_OK;
@@ -560,6 +569,11 @@ static int get_state_common(fv_solver* s, double* q, cudaMemcpyKind kind) {
     if (!s || !q) return fail(FV_ERR_ARG, "null argument");
     CK(cudaSetDevice(s->device));
     const size_t nq = (size_t)s->n_total * s->V;
+    if (kind == cudaMemcpyDeviceToDevice) {  // straight into the caller's device array
+        launch_permute_to_ref(s->qbase[0], q, s->new2ref, (int)s->n_total, s->V, s->stream);
+        CK(cudaGetLastError());
+        return FV_OK;
+    }
     launch_permute_to_ref(s->qbase[0], s->stage_buf, s->new2ref, (int)s->n_total, s->V, s->stream);
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(q, s->stage_buf, nq * 8, kind, s->stream));
@@ -751,22 +765,24 @@ int fv_run(fv_solver* s, const fv_run_options* o, fv_run_info* info) {
     CK(cudaSetDevice(s->device));
     cudaStream_t st = s->stream;
     std::vector<double> alpha(o->alpha, o->alpha + o->n_alpha);
-    RunLimits L{o->max_step, o->max_time, o->tolerance, o->print_interval};
-    CK(cudaMemcpyAsync(s->limits, &L, sizeof(L), cudaMemcpyHostToDevice, st));
-    Ctrl hc;
+    // limits and control go through small kernels and mapped memory, never
+    // through the copy engines, which callers may keep busy with state
+    // transfers on other streams
+    const RunLimits L{o->max_step, o->max_time, o->tolerance, o->print_interval};
+    launch_set_limits(s->limits, L, st);
+    const Ctrl& hc = *s->hctrl;
     if (o->restart) {
-        std::memset(&hc, 0, sizeof(hc));
-        for (int k = 0; k < kMaxV; ++k) hc.R[k] = 1.0;
-        hc.active = 1;
-        CK(cudaMemcpyAsync(s->ctrl, &hc, sizeof(hc), cudaMemcpyHostToDevice, st));
+        launch_ctrl_reset(s->ctrl, st);
+        launch_ctrl_copy(s->ctrl, s->hctrl_dev, st);
         if (s->case_time) CK(cudaMemsetAsync(s->case_time, 0, (size_t)s->n_cases * 8, st));
         // run(): initial ghost fill with zeroed gx, gy, limiters (explicit.cpp:712)
         exact::launch_bounds(s->TP.P, s->qbase[0], nullptr, nullptr, nullptr, 1, st);
         sync_shadow(s, 0);
         CK(cudaGetLastError());
     } else {
-        CK(cudaMemcpyAsync(&hc, s->ctrl, sizeof(hc), cudaMemcpyDeviceToHost, st));
+        launch_ctrl_copy(s->ctrl, s->hctrl_dev, st);
     }
+    CK(cudaGetLastError());
     CK(cudaStreamSynchronize(st));
     const unsigned long long start_step = o->restart ? 0ull : hc.step;
     cudaEvent_t e0, e1;
@@ -784,12 +800,12 @@ int fv_run(fv_solver* s, const fv_run_options* o, fv_run_info* info) {
         GraphEntry* g = nullptr;
         int rc = get_graph(s, alpha, len, &g);
         if (rc) { cudaEventDestroy(e0); cudaEventDestroy(e1); return rc; }
-        CK(cudaMemsetAsync(&s->ctrl->n_hist, 0, sizeof(int), st));
         CK(cudaEventRecord(e0, st));
-        CK(cudaGraphLaunch(g->exec, st));
+        CK(cudaGraphLaunch(g->exec, st));  // its first kernel empties the print records
         CK(cudaEventRecord(e1, st));
         launches += g->launches;
-        CK(cudaMemcpyAsync(&hc, s->ctrl, sizeof(hc), cudaMemcpyDeviceToHost, st));
+        launch_ctrl_copy(s->ctrl, s->hctrl_dev, st);
+        CK(cudaGetLastError());
         CK(cudaStreamSynchronize(st));
         float ms = 0.f;
         CK(cudaEventElapsedTime(&ms, e0, e1));

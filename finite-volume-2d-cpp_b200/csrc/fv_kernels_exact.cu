@@ -69,10 +69,40 @@ __device__ void begin_step(Ctrl* c, const RunLimits* L, int V) {
     c->need_R = !stop && (c->step == 0 || (c->step % L->print_interval) == 0 || (L->tolerance > 1.01e-16));
 }
 
+// First kernel of every launch sequence (graph): the step's start, and an
+// empty print-record list for this sequence.
 __global__ void k_step_begin(Ctrl* c, const RunLimits* L, int V, unsigned long long* keys, int nkeys) {
     for (int i = threadIdx.x; i < nkeys; i += blockDim.x) keys[i] = ~0ull;
-    if (threadIdx.x == 0) begin_step(c, L, V);
+    if (threadIdx.x == 0) {
+        c->n_hist = 0;
+        begin_step(c, L, V);
+    }
 }
+
+// Run control set and read by small kernels, not by copies: a copy would
+// queue behind state transfers that other streams keep the copy engines busy
+// with (the host reads the control through mapped pinned memory).
+static_assert(sizeof(Ctrl) % 8 == 0, "Ctrl is copied in 8-byte words");
+__global__ void k_ctrl_reset(Ctrl* c) {
+    unsigned long long* w = reinterpret_cast<unsigned long long*>(c);
+    for (int i = threadIdx.x; i < (int)(sizeof(Ctrl) / 8); i += blockDim.x) w[i] = 0ull;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int k = 0; k < kMaxV; ++k) c->R[k] = 1.0;
+        c->active = 1;
+    }
+}
+__global__ void k_ctrl_copy(const Ctrl* src, Ctrl* dst) {
+    const unsigned long long* a = reinterpret_cast<const unsigned long long*>(src);
+    unsigned long long* b = reinterpret_cast<unsigned long long*>(dst);
+    for (int i = threadIdx.x; i < (int)(sizeof(Ctrl) / 8); i += blockDim.x) b[i] = a[i];
+}
+__global__ void k_set_limits(RunLimits* d, RunLimits v) {
+    if (threadIdx.x == 0) *d = v;
+}
+void launch_ctrl_reset(Ctrl* c, cudaStream_t st) { k_ctrl_reset<<<1, 64, 0, st>>>(c); }
+void launch_ctrl_copy(const Ctrl* src, Ctrl* dst, cudaStream_t st) { k_ctrl_copy<<<1, 64, 0, st>>>(src, dst); }
+void launch_set_limits(RunLimits* d, const RunLimits& v, cudaStream_t st) { k_set_limits<<<1, 32, 0, st>>>(d, v); }
 
 // Residual norms, step/time bookkeeping and print records
 // (explicit.cpp:752-800), then the next step's start: its stop criteria and

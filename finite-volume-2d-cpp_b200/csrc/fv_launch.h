@@ -10,6 +10,10 @@ namespace fvgpu {
 inline int grid_for(int n) { return (n + kBlock - 1) / kBlock; }
 
 // step control
+// run control without copies (dst of launch_ctrl_copy may be mapped host memory)
+void launch_ctrl_reset(Ctrl* c, cudaStream_t st);
+void launch_ctrl_copy(const Ctrl* src, Ctrl* dst, cudaStream_t st);
+void launch_set_limits(RunLimits* d, const RunLimits& v, cudaStream_t st);
 // keys: the dt minimum's ordered-key slots ([n_cases][64]), reset every step
 void launch_step_begin(Ctrl* c, const RunLimits* lim, int V, unsigned long long* keys, int nkeys, cudaStream_t st);
 void launch_step_end(const Params& P, Ctrl* c, const RunLimits* lim, const double* partials,
