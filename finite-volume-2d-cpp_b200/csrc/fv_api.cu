@@ -310,9 +310,17 @@ static int validate_physics(const fv_physics* ph, int n_groups_mesh) {
         if (ph->dt_kind != FV_DT_CONST) return fail(FV_ERR_UNSUPPORTED, "the Burgers kind supports a constant dt only");
     } else if (ph->flux == FV_FLUX_ROE_FS || ph->flux == FV_FLUX_ROE_ST) {
         if (ph->V != 4) return fail(FV_ERR_UNSUPPORTED, "the Roe flux kinds have V = 4");
+    } else if (ph->flux == FV_FLUX_DIFFUSION) {
+        if (ph->V != 1) return fail(FV_ERR_UNSUPPORTED, "the diffusion flux kind has V = 1");
+        if (!ph->diffusive) return fail(FV_ERR_UNSUPPORTED, "the diffusion flux kind needs diffusive = 1");
+        if (ph->order2)
+            return fail(FV_ERR_UNSUPPORTED, "the diffusion flux kind runs without MUSCL face states (order2 = 0)");
+        if (ph->dt_kind != FV_DT_CONST) return fail(FV_ERR_UNSUPPORTED, "the diffusion kind supports a constant dt only");
     } else {
         return fail(FV_ERR_UNSUPPORTED, "unknown flux kind " + std::to_string(ph->flux));
     }
+    if (ph->diffusive && ph->flux != FV_FLUX_DIFFUSION)
+        return fail(FV_ERR_UNSUPPORTED, "diffusive gradients are used by the diffusion flux kind only");
     if (ph->limiter < 0 || ph->limiter > 3) return fail(FV_ERR_UNSUPPORTED, "unknown limiter kind");
     if (ph->dt_kind < 0 || ph->dt_kind > 2) return fail(FV_ERR_UNSUPPORTED, "unknown dt kind");
     if (ph->n_groups < n_groups_mesh) return fail(FV_ERR_ARG, "physics has fewer boundary groups than the mesh");
@@ -320,7 +328,8 @@ static int validate_physics(const fv_physics* ph, int n_groups_mesh) {
     for (int g = 0; g < ph->n_groups; ++g) {
         const int k = ph->group_bc[g];
         if (k < 0 || k > 3) return fail(FV_ERR_UNSUPPORTED, "unknown boundary condition kind");
-        if (ph->V != 4 && k != FV_BC_COPY) return fail(FV_ERR_UNSUPPORTED, "V = 2 supports the copy boundary only");
+        if (ph->V != 4 && k != FV_BC_COPY)
+            return fail(FV_ERR_UNSUPPORTED, "V = " + std::to_string(ph->V) + " supports the copy boundary only");
     }
     return FV_OK;
 }
@@ -373,6 +382,7 @@ int fv_solver_create_ex(const fv_mesh* fm, const fv_physics* ph, int32_t precisi
     P.flux = ph->flux; P.order2 = ph->order2 ? 1 : 0; P.limiter = ph->limiter; P.dt_kind = ph->dt_kind;
     P.global_dt = ph->global_dt ? 1 : 0;
     P.positivity_guard = ph->positivity_guard ? 1 : 0;
+    P.diffusive = ph->diffusive ? 1 : 0;
     P.gamma = ph->gamma; P.K = ph->K; P.cfl = ph->cfl; P.dt_const = ph->dt_const;
     P.n_groups = ph->n_groups;
     for (int g = 0; g < ph->n_groups; ++g) {
@@ -685,11 +695,13 @@ static int enqueue_step(fv_solver* s, const std::vector<double>& alpha, int b, E
     io.gx = s->gx; io.gy = s->gy; io.lim = s->lim; io.dt = s->dt; io.ctrl = s->ctrl;
     io.dtkeys = s->keys;
     io.q_stage = s->sbase[b];
-    // second order: the first stage's gradient kernel also computes dt
+    // with gradients (second order, diffusive fluxes) the first stage's
+    // gradient kernel also computes dt
     // every kernel after step_begin is a programmatic dependent of the one
     // before it (its constant tile data is staged during that one's tail)
     const bool pdl = true;
-    if (!TP.P.order2) { tile::launch_dt(s->precision, TP, io, st, pdl); ++n; mark(KK_DT); }
+    const bool grads = TP.P.order2 || TP.P.diffusive;
+    if (!grads) { tile::launch_dt(s->precision, TP, io, st, pdl); ++n; mark(KK_DT); }
     const int ns = (int)alpha.size();
     const void* in = s->sbase[b];
     for (int k = 0; k < ns; ++k) {
@@ -712,7 +724,7 @@ static int enqueue_step(fv_solver* s, const std::vector<double>& alpha, int b, E
         }
         so.s_out = s->f32 ? out_s : nullptr;
         so.write_f64 = last ? 1 : 0;
-        if (TP.P.order2) { tile::launch_gradlim(s->precision, TP, so, st, k == 0, pdl); ++n; mark(KK_GRADLIM); }
+        if (grads) { tile::launch_gradlim(s->precision, TP, so, st, k == 0, pdl); ++n; mark(KK_GRADLIM); }
         tile::launch_stage(s->precision, TP, so, st, pdl); ++n; mark(KK_STAGE);
         in = out_s;
     }

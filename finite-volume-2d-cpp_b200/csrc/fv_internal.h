@@ -52,6 +52,7 @@ struct Params {
     const double* g_dy;
     // physics
     int flux, order2, limiter, dt_kind, global_dt, positivity_guard;
+    int diffusive;                  // cell gradients feed the face gradient of the flux
     double gamma, K, cfl, dt_const;
     int n_groups;
     int group_bc[kMaxGroups];

@@ -236,7 +236,8 @@ void launch_bounds(const Params& P, double* q, const double* gx, const double* g
     if (P.n_bound == 0) return;
     const int g = grid_for(P.n_bound);
     if (P.V == 4) k_bounds<4><<<g, kBlock, 0, st>>>(P, q, gx, gy, lim, zero_grad);
-    else k_bounds<2><<<g, kBlock, 0, st>>>(P, q, gx, gy, lim, zero_grad);
+    else if (P.V == 2) k_bounds<2><<<g, kBlock, 0, st>>>(P, q, gx, gy, lim, zero_grad);
+    else k_bounds<1><<<g, kBlock, 0, st>>>(P, q, gx, gy, lim, zero_grad);
 }
 }  // namespace exact
 

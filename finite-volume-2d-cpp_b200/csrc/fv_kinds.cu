@@ -22,6 +22,27 @@ int fv_kind_flux(int32_t flux, double gamma, const double* qi, const double* qj,
     }
 }
 
+int fv_kind_flux_grad(int32_t flux, double gamma, const double* qi, const double* qj, const double* gx,
+                      const double* gy, const double* n, double* f) {
+    if (flux != FV_FLUX_DIFFUSION) return fv_kind_flux(flux, gamma, qi, qj, n, f);
+    if (!gx || !gy || !n || !f) return FV_ERR_ARG;
+    fvgpu::exact::diffusion(f, gx, gy, n[0], n[1]);
+    return FV_OK;
+}
+
+int fv_kind_face_gradient(int32_t V, const double* gxi, const double* gyi, const double* gxj, const double* gyj,
+                          const double* qi, const double* qj, const double* ci, const double* cj, double* gxf,
+                          double* gyf) {
+    if (!gxi || !gyi || !gxj || !gyj || !qi || !qj || !ci || !cj || !gxf || !gyf) return FV_ERR_ARG;
+    switch (V) {
+        case 1: fvgpu::exact::face_gradient<1>(gxf, gyf, gxi, gyi, gxj, gyj, qi, qj, ci[0], ci[1], cj[0], cj[1]); break;
+        case 2: fvgpu::exact::face_gradient<2>(gxf, gyf, gxi, gyi, gxj, gyj, qi, qj, ci[0], ci[1], cj[0], cj[1]); break;
+        case 4: fvgpu::exact::face_gradient<4>(gxf, gyf, gxi, gyi, gxj, gyj, qi, qj, ci[0], ci[1], cj[0], cj[1]); break;
+        default: return FV_ERR_ARG;
+    }
+    return FV_OK;
+}
+
 int fv_kind_limiter(int32_t kind, double y, double* out) {
     if (!out) return FV_ERR_ARG;
     if (kind < FV_LIM_ZERO || kind > FV_LIM_MINMOD) return FV_ERR_UNSUPPORTED;
@@ -31,7 +52,7 @@ int fv_kind_limiter(int32_t kind, double y, double* out) {
 
 int fv_kind_bc(int32_t kind, int32_t V, double gamma, const double* bv, const double* q, const double* n,
                double* b) {
-    if (!q || !n || !b || (V != 2 && V != 4)) return FV_ERR_ARG;
+    if (!q || !n || !b || (V != 1 && V != 2 && V != 4)) return FV_ERR_ARG;
     if (kind < FV_BC_COPY || kind > FV_BC_FARFIELD) return FV_ERR_UNSUPPORTED;
     if ((kind == FV_BC_INLET_OUTLET || kind == FV_BC_FARFIELD) && !bv) return FV_ERR_ARG;
     fvgpu::Params P;
@@ -42,7 +63,8 @@ int fv_kind_bc(int32_t kind, int32_t V, double gamma, const double* bv, const do
     P.group_bc[0] = kind;
     if (bv) memcpy(P.group_bv, bv, 4 * sizeof(double));
     if (V == 4) fvgpu::exact::bc<4>(P, 0, 0, b, q, n[0], n[1]);
-    else fvgpu::exact::bc<2>(P, 0, 0, b, q, n[0], n[1]);
+    else if (V == 2) fvgpu::exact::bc<2>(P, 0, 0, b, q, n[0], n[1]);
+    else fvgpu::exact::bc<1>(P, 0, 0, b, q, n[0], n[1]);
     return FV_OK;
 }
 

@@ -91,6 +91,34 @@ FV_HD void flux(double gamma, double* f, const double* qi, const double* qj,
     else roe<FLUX == 1>(gamma, f, qi, qj, n0, n1);
 }
 
+// Face gradient of the diffusive fluxes (gradient_for_diffusion,
+// explicit.cpp:70-109): the mean of the two cell gradients, with its
+// component along the centroid line ci - cj replaced by the difference
+// quotient of the two cell states.
+template <int V>
+FV_HD void face_gradient(double* gxf, double* gyf, const double* gxi, const double* gyi, const double* gxj,
+                         const double* gyj, const double* qi, const double* qj, double cix, double ciy, double cjx,
+                         double cjy) {
+    double t0 = cix - cjx, t1 = ciy - cjy;
+    const double lij = sqrt(t0 * t0 + t1 * t1);
+    t0 = t0 / lij;
+    t1 = t1 / lij;
+#pragma unroll
+    for (int k = 0; k < V; ++k) {
+        const double dir = (qi[k] - qj[k]) / lij;
+        const double bx = (gxi[k] + gxj[k]) * 0.5, by = (gyi[k] + gyj[k]) * 0.5;
+        const double dot = bx * t0 + by * t1;
+        gxf[k] = bx - (dot - dir) * t0;
+        gyf[k] = by - (dot - dir) * t1;
+    }
+}
+
+// Diffusion flux F = -grad(u) . n of the face gradient
+// (examples/heatTransfer/main.cpp:63-73, V = 1).
+FV_HD void diffusion(double* f, const double* gxf, const double* gyf, double n0, double n1) {
+    f[0] = -(gxf[0] * n0 + gyf[0] * n1);
+}
+
 // Limiter functions phi (limiter_func).  ZERO: shockTube/main.cpp:60-62.
 // MICHALAK (y_t = 2): forwardStep/main.cpp:57-66.  MINMOD: burgers/main.cpp:
 // 51-53.  VENKAT: (y^2 + 2y)/(y^2 + y + 2), Venkatakrishnan (1995).

@@ -85,6 +85,24 @@ __device__ __forceinline__ void flux(T gamma, T* f, const T* qi, const T* qj, T 
     else roe(gamma, f, qi, qj, n0, n1);
 }
 
+// Diffusion flux -grad(u) . n with the corrected face gradient (see
+// fv_physics_exact.cuh): one reciprocal of |ci - cj|, and the normal
+// component of the correction taken once, (t . n).
+template <int V, class T>
+__device__ __forceinline__ void diffusion(T* f, const T* gxi, const T* gyi, const T* gxj, const T* gyj, const T* qi,
+                                          const T* qj, T t0, T t1, T n0, T n1) {
+    const T rl = rcp(sqrt_(t0 * t0 + t1 * t1));
+    t0 *= rl;
+    t1 *= rl;
+    const T tn = t0 * n0 + t1 * n1;
+#pragma unroll
+    for (int k = 0; k < V; ++k) {
+        const T bx = T(0.5) * (gxi[k] + gxj[k]), by = T(0.5) * (gyi[k] + gyj[k]);
+        const T corr = bx * t0 + by * t1 - (qi[k] - qj[k]) * rl;
+        f[k] = -(bx * n0 + by * n1 - corr * tn);
+    }
+}
+
 // limiter_func kinds (see fv_physics_exact.cuh for the references).
 template <class T>
 __device__ __forceinline__ T limiter_func(int kind, T y) {

@@ -136,14 +136,15 @@ __device__ __forceinline__ void lds(const S* p, S* v) {
     }
 }
 
-// Shared-memory record of one tile-local cell: q[V], then (second order)
-// gx[V], gy[V], (exact) lim[V], then the centroid; padded to 16 bytes.
+// Shared-memory record of one tile-local cell: q[V], then (with gradients)
+// gx[V], gy[V], (exact) lim[V], then the centroid on an even word (one
+// 2-word copy); padded to 16 bytes.
 template <class M, int V, bool ORDER2, bool CENTROID>
 struct Rec {
     using S = typename M::S;
     static constexpr int NG = ORDER2 ? (M::exact ? 3 : 2) : 0;
     static constexpr int OGX = V, OGY = 2 * V, OLM = 3 * V;
-    static constexpr int OC = V * (1 + NG);
+    static constexpr int OC = (V * (1 + NG) + 1) / 2 * 2;
     static constexpr int RAW = OC + (CENTROID ? 2 : 0);
     static constexpr int AL = 16 / (int)sizeof(S);
     // an odd number of 16-byte units, so that 128-bit reads of records of
@@ -490,6 +491,8 @@ __global__ void __launch_bounds__(kTileMax) k_tile_gradlim(TileParams TP, TileIO
         }
     }
     const S xc = rs[R::OC], yc = rs[R::OC + 1];
+    // gradients without limiters (diffusive fluxes, first order): lim = 1
+    const bool limit = P.order2 != 0;
     if constexpr (M::exact) {
         const double invA = 1. / A;
 #pragma unroll
@@ -498,7 +501,7 @@ __global__ void __launch_bounds__(kTileMax) k_tile_gradlim(TileParams TP, TileIO
         const double tol = 1e-15;
 #pragma unroll
         for (int f = 0; f < kMaxFaces; ++f) {
-            if (w[f] == kFaceNone) continue;
+            if (!limit || w[f] == kFaceNone) continue;
             const int el = w[f] & kFaceEdgeMask;
             const double dx = sxf[el] - xc, dy = syf[el] - yc;
 #pragma unroll
@@ -549,7 +552,7 @@ __global__ void __launch_bounds__(kTileMax) k_tile_gradlim(TileParams TP, TileIO
         }
 #pragma unroll
         for (int f = 0; f < kMaxFaces; ++f) {
-            if (w[f] == kFaceNone) continue;
+            if (!limit || w[f] == kFaceNone) continue;
             const int el = w[f] & kFaceEdgeMask;
             const S dx = sxf[el] - xc, dy = syf[el] - yc;
 #pragma unroll
@@ -572,11 +575,15 @@ __global__ void __launch_bounds__(kTileMax) k_tile_gradlim(TileParams TP, TileIO
 }
 
 // ------------------------------------- K2: flux + RK update + ghost fill --
+// ORDER2: the records carry gradients and centroids.  They feed the MUSCL
+// face states, or (FLUX 4, diffusion) the face gradient of the flux, whose
+// face states are the cell values (first order).
 template <class M, int V, bool ORDER2, int FLUX>
 __global__ void __launch_bounds__(kTileMax) k_tile_stage(TileParams TP, TileIO io) {
     using S = typename M::S;
     using FT = typename std::conditional<M::exact, double, S>::type;  // flux storage
     using R = Rec<M, V, ORDER2, ORDER2>;
+    constexpr bool MUSCL = ORDER2 && FLUX != 4;
     pdl_trigger();
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ unsigned long long s_dtkey;
@@ -601,7 +608,7 @@ __global__ void __launch_bounds__(kTileMax) k_tile_stage(TileParams TP, TileIO i
         load_faces(TP, c, w);
         A = (double)((const S*)TP.area)[c];
     }
-    if (ORDER2) stage_edges<S, false, true>(TP, inf, sij, snx, sny, sle, nullptr, sxf, syf);
+    if (MUSCL) stage_edges<S, false, true>(TP, inf, sij, snx, sny, sle, nullptr, sxf, syf);
     else stage_edges<S, false, false>(TP, inf, sij, snx, sny, sle, nullptr, nullptr, nullptr);
     pdl_wait();
     if (t_inactive(io.ctrl)) { cpa_wait(); return; }
@@ -631,7 +638,7 @@ __global__ void __launch_bounds__(kTileMax) k_tile_stage(TileParams TP, TileIO i
         S qL[V], qR[V];
         lds<S, V>(ri, qL);
         lds<S, V>(rj, qR);
-        if (ORDER2) {
+        if (MUSCL) {
             const S xf = sxf[el], yf = syf[el];
             const S di0 = xf - ri[R::OC], di1 = yf - ri[R::OC + 1];
             const S dj0 = xf - rj[R::OC], dj1 = yf - rj[R::OC + 1];
@@ -660,10 +667,25 @@ __global__ void __launch_bounds__(kTileMax) k_tile_stage(TileParams TP, TileIO i
             guard_face<S, V>(P, qR, cj);
         }
         FT f[V];
-        if constexpr (M::exact) {
+        if constexpr (FLUX == 4) {
+            S gxi[V], gyi[V], gxj[V], gyj[V];
+            lds<S, V>(ri + R::OGX, gxi); lds<S, V>(ri + R::OGY, gyi);
+            lds<S, V>(rj + R::OGX, gxj); lds<S, V>(rj + R::OGY, gyj);
+            if constexpr (M::exact) {
+                double gxf[V], gyf[V];
+                exact::face_gradient<V>(gxf, gyf, gxi, gyi, gxj, gyj, qL, qR, ri[R::OC], ri[R::OC + 1], rj[R::OC],
+                                        rj[R::OC + 1]);
+                exact::diffusion(f, gxf, gyf, n0, n1);
+            } else {
+                fast::diffusion<V, S>(f, gxi, gyi, gxj, gyj, qL, qR, ri[R::OC] - rj[R::OC],
+                                      ri[R::OC + 1] - rj[R::OC + 1], n0, n1);
+            }
+        } else if constexpr (M::exact) {
             exact::flux<FLUX>(P.gamma, f, qL, qR, n0, n1);
         } else {
             fast::flux<FLUX, S>((S)P.gamma, f, qL, qR, n0, n1);
+        }
+        if constexpr (!M::exact) {
             const S le = sle[el];
 #pragma unroll
             for (int k = 0; k < V; ++k) f[k] *= le;
@@ -755,7 +777,7 @@ __global__ void __launch_bounds__(kTileMax) k_tile_stage(TileParams TP, TileIO i
                 S qint[V], qc[V], b[V];
 #pragma unroll
                 for (int k = 0; k < V; ++k) { qc[k] = (S)qnew[k]; qint[k] = qc[k]; }
-                if (ORDER2) {
+                if (MUSCL) {
                     const S d0 = sxf[el] - rs[R::OC], d1 = syf[el] - rs[R::OC + 1];
                     S gxs[V], gys[V];
                     lds<S, V>(rs + R::OGX, gxs); lds<S, V>(rs + R::OGY, gys);
@@ -852,12 +874,17 @@ struct TileLaunch {
             set((const void*)k_tile_stage<M, 4, false, 1>, smem_stage<M, 4, false>(TP));
             set((const void*)k_tile_stage<M, 4, true, 2>, smem_stage<M, 4, true>(TP));
             set((const void*)k_tile_stage<M, 4, false, 2>, smem_stage<M, 4, false>(TP));
-        } else {
+        } else if (TP.P.V == 2) {
             set((const void*)k_tile_dt<M, 2>, smem_dt<M, 2>(TP));
             set((const void*)k_tile_gradlim<M, 2, false>, smem_gradlim<M, 2>(TP));
             set((const void*)k_tile_gradlim<M, 2, true>, smem_gradlim<M, 2>(TP));
             set((const void*)k_tile_stage<M, 2, true, 3>, smem_stage<M, 2, true>(TP));
             set((const void*)k_tile_stage<M, 2, false, 3>, smem_stage<M, 2, false>(TP));
+        } else {
+            set((const void*)k_tile_dt<M, 1>, smem_dt<M, 1>(TP));
+            set((const void*)k_tile_gradlim<M, 1, false>, smem_gradlim<M, 1>(TP));
+            set((const void*)k_tile_gradlim<M, 1, true>, smem_gradlim<M, 1>(TP));
+            set((const void*)k_tile_stage<M, 1, true, 4>, smem_stage<M, 1, true>(TP));
         }
         return e;
     }
@@ -884,22 +911,28 @@ struct TileLaunch {
     }
     static void dt(const TileParams& TP, const TileIO& io, cudaStream_t st, bool pdl = false) {
         if (TP.P.V == 4) go(k_tile_dt<M, 4>, grid(TP), TP.T, smem_dt<M, 4>(TP), st, pdl, TP, io);
-        else go(k_tile_dt<M, 2>, grid(TP), TP.T, smem_dt<M, 2>(TP), st, pdl, TP, io);
+        else if (TP.P.V == 2) go(k_tile_dt<M, 2>, grid(TP), TP.T, smem_dt<M, 2>(TP), st, pdl, TP, io);
+        else go(k_tile_dt<M, 1>, grid(TP), TP.T, smem_dt<M, 1>(TP), st, pdl, TP, io);
     }
     static void gradlim(const TileParams& TP, const TileIO& io, cudaStream_t st, bool with_dt, bool pdl = false) {
         const int g = grid(TP);
         if (TP.P.V == 4) {
             if (with_dt) go(k_tile_gradlim<M, 4, true>, g, TP.T, smem_gradlim<M, 4>(TP), st, pdl, TP, io);
             else go(k_tile_gradlim<M, 4, false>, g, TP.T, smem_gradlim<M, 4>(TP), st, pdl, TP, io);
-        } else {
+        } else if (TP.P.V == 2) {
             if (with_dt) go(k_tile_gradlim<M, 2, true>, g, TP.T, smem_gradlim<M, 2>(TP), st, pdl, TP, io);
             else go(k_tile_gradlim<M, 2, false>, g, TP.T, smem_gradlim<M, 2>(TP), st, pdl, TP, io);
+        } else {
+            if (with_dt) go(k_tile_gradlim<M, 1, true>, g, TP.T, smem_gradlim<M, 1>(TP), st, pdl, TP, io);
+            else go(k_tile_gradlim<M, 1, false>, g, TP.T, smem_gradlim<M, 1>(TP), st, pdl, TP, io);
         }
     }
     static void stage(const TileParams& TP, const TileIO& io, cudaStream_t st, bool pdl = false) {
         const int g = grid(TP);
         const bool o2 = TP.P.order2 != 0;
-        if (TP.P.flux == 3) {
+        if (TP.P.flux == 4) {
+            go(k_tile_stage<M, 1, true, 4>, g, TP.T, smem_stage<M, 1, true>(TP), st, pdl, TP, io);
+        } else if (TP.P.flux == 3) {
             if (o2) go(k_tile_stage<M, 2, true, 3>, g, TP.T, smem_stage<M, 2, true>(TP), st, pdl, TP, io);
             else go(k_tile_stage<M, 2, false, 3>, g, TP.T, smem_stage<M, 2, false>(TP), st, pdl, TP, io);
         } else if (TP.P.flux == 1) {

@@ -17,7 +17,7 @@ import physics as _phys
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libfvgpu.so")
 
-FLUX = {"roe_fs": 1, "roe_st": 2, "burgers": 3}
+FLUX = {"roe_fs": 1, "roe_st": 2, "burgers": 3, "diffusion": 4}
 LIMITER = {"zero": 0, "michalak": 1, "venkat": 2, "minmod": 3}
 DT = {"const": 0, "cfl_sum": 1, "cfl_min_signed": 2}
 BC = {"copy": 0, "wall": 1, "inlet_outlet": 2, "farfield": 3}
@@ -39,7 +39,8 @@ class _Physics(C.Structure):
     _fields_ = [("V", C.c_int32), ("flux", C.c_int32), ("order2", C.c_int32), ("limiter", C.c_int32),
                 ("dt_kind", C.c_int32), ("global_dt", C.c_int32), ("gamma", C.c_double), ("K", C.c_double),
                 ("cfl", C.c_double), ("dt_const", C.c_double), ("n_groups", C.c_int32),
-                ("group_bc", _i32p), ("group_bv", _dp), ("positivity_guard", C.c_int32)]
+                ("group_bc", _i32p), ("group_bv", _dp), ("positivity_guard", C.c_int32),
+                ("diffusive", C.c_int32)]
 
 
 _PRINT_CB = C.CFUNCTYPE(None, C.c_void_p, C.c_uint64, C.c_double, _dp, C.c_int32)
@@ -203,6 +204,7 @@ def physics_struct(ph: _phys.Physics, group_names: Sequence[str]):
                  dt_const=ph.dt_const, n_groups=len(group_names))
     s.group_bc = _p(gbc, _i32p); s.group_bv = _p(gbv)
     s.positivity_guard = int(getattr(ph, "positivity_guard", False))
+    s.diffusive = int(getattr(ph, "diffusive", False))
     s._keep = (gbc, gbv)
     return s
 

@@ -8,7 +8,9 @@ examples define as device kinds, selected by name:
 * flux:     ``roe_fs`` (examples/forwardStep/main.cpp:72-135),
             ``roe_st`` (examples/shockTube/main.cpp:68-135, naca/main.cpp:71-137;
             same Roe-"cures" flux, central part associated differently),
-            ``burgers`` (examples/burgers/main.cpp:68-96, V = 2)
+            ``burgers`` (examples/burgers/main.cpp:68-96, V = 2),
+            ``diffusion`` (examples/heatTransfer/main.cpp:63-73, V = 1: F = -grad T . n
+            with the face gradient of gradient_for_diffusion, explicit.cpp:70-109)
 * limiter:  ``zero`` (shockTube/main.cpp:60-62), ``michalak``
             (forwardStep/main.cpp:57-66), ``minmod`` (burgers/main.cpp:51-53),
             ``venkat`` (Venkatakrishnan 1995, not in the reference)
@@ -44,6 +46,10 @@ class Physics:
     # not in the reference: fall back to the cell value on MUSCL face states
     # with rho <= 0 or p <= 0 (off = the reference's scheme, bit for bit)
     positivity_guard: bool = False
+    # solver::diffusive_gradients: the flux receives the corrected face
+    # gradient; with order2 off the gradients are computed without limiter
+    # or interpolation (examples/heatTransfer/main.cpp:18-25)
+    diffusive: bool = False
 
 
 def euler_state(rho, u, v, p, gamma=1.4):
@@ -95,6 +101,12 @@ def riemann_strip(order2=True, limiter="venkat", K=5.0, cfl=0.8):
                    global_dt=True, bcs={"wall": ("wall", None), "ends": ("copy", None)})
 
 
+def heat(dt=1e-5):
+    """examples/heatTransfer/main.cpp: u_t = div(grad u), constant dt, zero-flux walls."""
+    return Physics(V=1, flux="diffusion", order2=False, limiter="zero", dt_kind="const", dt_const=dt,
+                   global_dt=True, diffusive=True, bcs={"wall": ("copy", None)})
+
+
 def burgers(dt=1e-4):
     return Physics(V=2, flux="burgers", order2=True, limiter="minmod", K=7.5, dt_kind="const",
                    dt_const=dt, global_dt=True, bcs={"wall": ("copy", None)})
@@ -135,6 +147,15 @@ def ic_riemann(ccx, left, right, gamma=1.4):
     m = ccx < 0.5
     q[m] = euler_state(left[0], left[1], 0.0, left[2], gamma)
     q[~m] = euler_state(right[0], right[1], 0.0, right[2], gamma)
+    return q
+
+
+def ic_heat(ccx, ccy):
+    """examples/heatTransfer/main.cpp:32-45 (radius test sqrt(r2) < 0.4*0.4 as written there)."""
+    import numpy as np
+    q = np.zeros((ccx.size, 1))
+    x = ccx - 0.5; y = ccy - 0.5
+    q[np.sqrt(x * x + y * y) < 0.4 * 0.4] = 1.0
     return q
 
 

@@ -181,15 +181,40 @@ struct Probe {
 
 const char* flux_name(int k) {
     return k == FV_FLUX_ROE_FS ? "roe (forwardStep operand order)"
-           : k == FV_FLUX_ROE_ST ? "roe (shockTube/naca operand order)" : "upwind advection";
+           : k == FV_FLUX_ROE_ST ? "roe (shockTube/naca operand order)"
+           : k == FV_FLUX_DIFFUSION ? "diffusion" : "upwind advection";
 }
 
 // calc_flux -> (kind, gamma).  gamma from a fluid at rest (f[1] = p = gamma-1
 // for q = (1, 0, 0, 1), n = (1, 0)), then 256 random state pairs must agree
 // bit for bit.
-void identify_flux(int V, int32_t* kind, double* gamma) {
+void identify_flux(int V, bool diffusive, int32_t* kind, double* gamma) {
     double zg[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     Probe pr;
+    if (diffusive) {
+        // the only diffusive device kind: F = -grad(u) . n of the face gradient
+        if (V != 1)
+            throw std::invalid_argument("fvhyper GPU: diffusive_gradients with vars = " + std::to_string(V) +
+                                        " (viscous fluxes) is not on the device path; the device's diffusive "
+                                        "kind is the vars = 1 diffusion flux of examples/heatTransfer");
+        for (int t = 0; t < 256; ++t) {
+            double qi[1] = {pr.uni(-2, 2)}, qj[1] = {pr.uni(-2, 2)}, gx[1] = {pr.uni(-5, 5)},
+                   gy[1] = {pr.uni(-5, 5)}, n[2];
+            pr.normal(n);
+            double fu[1] = {0}, fk[1] = {0};
+            calc_flux(fu, qi, qj, gx, gy, n);
+            fv_kind_flux_grad(FV_FLUX_DIFFUSION, 0.0, qi, qj, gx, gy, n, fk);
+            if (!same_bits(fu[0], fk[0]))
+                throw std::invalid_argument("fvhyper GPU: calc_flux (vars = 1, diffusive_gradients) is not the "
+                                            "diffusion flux -grad(u).n of examples/heatTransfer; no device kind "
+                                            "matches it");
+        }
+        *kind = FV_FLUX_DIFFUSION;
+        *gamma = 1.4;
+        return;
+    }
+    if (V == 1)
+        throw std::invalid_argument("fvhyper GPU: vars = 1 runs the diffusion kind only (diffusive_gradients)");
     if (V == 2) {
         for (int t = 0; t < 256; ++t) {
             double qi[2] = {pr.uni(-2, 2), pr.uni(-2, 2)}, qj[2] = {pr.uni(-2, 2), pr.uni(-2, 2)}, n[2];
@@ -205,7 +230,7 @@ void identify_flux(int V, int32_t* kind, double* gamma) {
         *gamma = 1.4;
         return;
     }
-    if (V != 4) throw std::invalid_argument("fvhyper GPU: vars must be 2 or 4");
+    if (V != 4) throw std::invalid_argument("fvhyper GPU: vars must be 1, 2 or 4");
     double q0[4] = {1.0, 0.0, 0.0, 1.0}, n0[2] = {1.0, 0.0}, f0[4] = {0, 0, 0, 0};
     calc_flux(f0, q0, q0, zg, zg, n0);
     const double g = f0[1] + 1.0;
@@ -276,7 +301,7 @@ void identify_bc(const std::string& name, void (*fn)(double*, double*, double*),
         for (int t = 0; t < 256 && ok; ++t) {
             double q[4] = {0, 0, 0, 0}, n[2];
             if (V == 4) pr.euler(q, gamma, 2.5);
-            else { q[0] = pr.uni(-2, 2); q[1] = pr.uni(-2, 2); }
+            else for (int c = 0; c < V; ++c) q[c] = pr.uni(-2, 2);
             pr.normal(n);
             double bu[4] = {0, 0, 0, 0}, bk[4] = {0, 0, 0, 0};
             double qc[4] = {q[0], q[1], q[2], q[3]}, nc[2] = {n[0], n[1]};
@@ -364,7 +389,7 @@ void identify_dt(fv_physics ph, int device, int32_t* dt_kind, double* cfl, doubl
     Probe pr;
     for (size_t i = 0; i < nt; ++i) {
         if (V == 4) pr.euler(&q[4 * i], ph.gamma);
-        else { q[2 * i] = pr.uni(-2, 2); q[2 * i + 1] = pr.uni(-2, 2); }
+        else for (int k = 0; k < V; ++k) q[V * i + k] = pr.uni(-2, 2);
     }
     calc_dt(dtu, q, pm);
     for (size_t i = 0; i < nt; ++i)
@@ -382,7 +407,9 @@ void identify_dt(fv_physics ph, int device, int32_t* dt_kind, double* cfl, doubl
         *dt_const = du[0];
         return;
     }
-    if (V != 4) throw std::invalid_argument("fvhyper GPU: calc_dt (vars = 2) must be a constant time step");
+    if (V != 4)
+        throw std::invalid_argument("fvhyper GPU: calc_dt (vars = " + std::to_string(V) +
+                                    ") must be a constant time step");
     const int32_t group_bc[1] = {FV_BC_COPY};
     const double group_bv[4] = {0, 0, 0, 0};
     ph.n_groups = 1;
@@ -457,15 +484,20 @@ void run(const std::string name, std::vector<double>& q, mpi_wrapper& pool, mesh
     q.resize((size_t)V * m.cellsAreas.size());
     generate_initial_solution(q, m);
 
-    if (solver::diffusive_gradients)
-        throw std::invalid_argument("fvhyper GPU: diffusive_gradients (viscous fluxes) is not on the device path");
     if (solver::smooth_residuals)
         throw std::invalid_argument("fvhyper GPU: smooth_residuals is not on the device path");
-    const bool o2 = solver::do_calc_gradients && solver::do_calc_limiters && solver::linear_interpolate;
-    const bool o1 = !solver::do_calc_gradients && !solver::do_calc_limiters && !solver::linear_interpolate;
-    if (!o1 && !o2)
+    const bool D = solver::diffusive_gradients;
+    const bool o2 = solver::do_calc_gradients && solver::do_calc_limiters && solver::linear_interpolate && !D;
+    const bool o1 = !solver::do_calc_gradients && !solver::do_calc_limiters && !solver::linear_interpolate && !D;
+    // diffusion: gradients for the face gradient, cell values as face states
+    const bool dg = solver::do_calc_gradients && !solver::do_calc_limiters && !solver::linear_interpolate && D;
+    if (D && V != 1)
+        throw std::invalid_argument("fvhyper GPU: diffusive_gradients with vars = " + std::to_string(V) +
+                                    " (viscous fluxes) is not on the device path");
+    if (!o1 && !o2 && !dg)
         throw std::invalid_argument("fvhyper GPU: the device runs first order (no gradients, limiters or "
-                                    "interpolation) or second order (all three); this flag mix is neither");
+                                    "interpolation), second order (all three) or diffusion (gradients and "
+                                    "diffusive_gradients only); this flag mix is none of them");
 
     const int precision = choose_precision(opt.precision);
     const int device = choose_device(opt.device);
@@ -473,8 +505,9 @@ void run(const std::string name, std::vector<double>& q, mpi_wrapper& pool, mesh
     fv_physics ph;
     std::memset(&ph, 0, sizeof(ph));
     ph.V = V;
-    identify_flux(V, &ph.flux, &ph.gamma);
+    identify_flux(V, dg, &ph.flux, &ph.gamma);
     ph.order2 = o2 ? 1 : 0;
+    ph.diffusive = dg ? 1 : 0;
     ph.limiter = o2 ? identify_limiter() : FV_LIM_ZERO;
     ph.K = solver::limiter_k_value;
     ph.global_dt = solver::global_dt ? 1 : 0;

@@ -44,7 +44,7 @@ typedef enum {
 } fv_status;
 
 /* Physics kinds implemented on the device (see finite-volume-2d-cpp_b200/physics.py). */
-enum { FV_FLUX_ROE_FS = 1, FV_FLUX_ROE_ST = 2, FV_FLUX_BURGERS = 3 };
+enum { FV_FLUX_ROE_FS = 1, FV_FLUX_ROE_ST = 2, FV_FLUX_BURGERS = 3, FV_FLUX_DIFFUSION = 4 };
 enum { FV_LIM_ZERO = 0, FV_LIM_MICHALAK = 1, FV_LIM_VENKAT = 2, FV_LIM_MINMOD = 3 };
 enum { FV_DT_CONST = 0, FV_DT_CFL_SUM = 1, FV_DT_CFL_MIN_SIGNED = 2 };
 enum { FV_BC_COPY = 0, FV_BC_WALL = 1, FV_BC_INLET_OUTLET = 2, FV_BC_FARFIELD = 3 };
@@ -59,7 +59,7 @@ enum { FV_BC_COPY = 0, FV_BC_WALL = 1, FV_BC_INLET_OUTLET = 2, FV_BC_FARFIELD = 
 enum { FV_PREC_FP64_EXACT = 0, FV_PREC_FP64 = 1, FV_PREC_FP32 = 2 };
 
 typedef struct {
-    int32_t V;          /* vars (explicit.h:31): 4 for Euler, 2 for the Burgers kind */
+    int32_t V;          /* vars (explicit.h:31): 4 for Euler, 2 for the Burgers kind, 1 for diffusion */
     int32_t flux;       /* FV_FLUX_* */
     int32_t order2;     /* do_calc_gradients && do_calc_limiters && linear_interpolate */
     int32_t limiter;    /* FV_LIM_* (limiter_func) */
@@ -75,6 +75,11 @@ typedef struct {
     int32_t positivity_guard;  /* not in the reference (0 = the reference's scheme): a MUSCL
                                   face state with rho <= 0 or p <= 0 falls back to the
                                   cell value */
+    int32_t diffusive;         /* solver::diffusive_gradients: every stage computes the cell
+                                  gradients (no limiter when order2 = 0) and the flux gets
+                                  the corrected face gradient of explicit.cpp:70-109.  Used
+                                  by FV_FLUX_DIFFUSION (V = 1, order2 = 0, constant dt,
+                                  copy boundaries: examples/heatTransfer) */
 } fv_physics;
 
 typedef struct {
@@ -269,6 +274,16 @@ int fv_stage_bounds(fv_solver* s, double* q, const double* gx, const double* gy,
  * (explicit.h:53,71-78; mesh.h:36-39).  n = {nx, ny}. */
 int fv_kind_flux(int32_t flux, double gamma, const double* qi, const double* qj, const double* n,
                  double* f);
+/* calc_flux with its face gradient arguments (explicit.h:71-78): gx, gy are
+ * the [V] face gradients the reference passes; the non-diffusive kinds
+ * ignore them.  V = 1 for FV_FLUX_DIFFUSION. */
+int fv_kind_flux_grad(int32_t flux, double gamma, const double* qi, const double* qj, const double* gx,
+                      const double* gy, const double* n, double* f);
+/* gradient_for_diffusion (explicit.cpp:70-109): the corrected face gradient
+ * [V] from the cell gradients, cell states and centroids ci, cj ([2] each). */
+int fv_kind_face_gradient(int32_t V, const double* gxi, const double* gyi, const double* gxj,
+                          const double* gyj, const double* qi, const double* qj, const double* ci,
+                          const double* cj, double* gxf, double* gyf);
 int fv_kind_limiter(int32_t kind, double y, double* out);
 /* bv: [4] boundary state of INLET_OUTLET / FARFIELD (may be NULL otherwise). */
 int fv_kind_bc(int32_t kind, int32_t V, double gamma, const double* bv, const double* q,

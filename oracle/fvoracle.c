@@ -442,12 +442,31 @@ static void guard_face(const fvo_physics* ph, double* qf, const double* qc) {
         for (int k = 0; k < 4; ++k) qf[k] = qc[k];
 }
 
-/* Edge flux loop, explicit.cpp:261-364 (no viscous face gradient). */
+/* Face gradient for the diffusive fluxes, explicit.cpp:70-109: the mean of
+ * the two cell gradients with its component along the centroid line replaced
+ * by the centroid difference quotient (cell states, not face states). */
+static void face_gradient(int V, double* gxf, double* gyf, const double* gxi, const double* gyi,
+                          const double* gxj, const double* gyj, const double* qi, const double* qj,
+                          const double* ci, const double* cj) {
+    double t0 = ci[0] - cj[0], t1 = ci[1] - cj[1];
+    const double lij = sqrt(t0 * t0 + t1 * t1);
+    t0 = t0 / lij;
+    t1 = t1 / lij;
+    for (int k = 0; k < V; ++k) {
+        const double dir = (qi[k] - qj[k]) / lij;
+        const double bx = (gxi[k] + gxj[k]) * 0.5, by = (gyi[k] + gyj[k]) * 0.5;
+        const double dot = bx * t0 + by * t1;
+        gxf[k] = bx - (dot - dir) * t0;
+        gyf[k] = by - (dot - dir) * t1;
+    }
+}
+
+/* Edge flux loop, explicit.cpp:261-364. */
 void fvo_calc_time_derivatives(const fvo_mesh* m, const fvo_physics* ph, const double* q,
                                const double* gx, const double* gy, const double* lim, double* qt) {
     const int V = ph->V;
     memset(qt, 0, sizeof(double) * V * m->n_total);
-    double qi[8], qj[8], f[8], n[2];
+    double qi[8], qj[8], f[8], n[2], gxf[8], gyf[8];
     for (int64_t e = 0; e < m->n_edges; ++e) {
         uint32_t i = m->edge_cells[2 * e], j = m->edge_cells[2 * e + 1];
         double le = m->elen[e];
@@ -466,7 +485,16 @@ void fvo_calc_time_derivatives(const fvo_mesh* m, const fvo_physics* ph, const d
         } else {
             for (int k = 0; k < V; ++k) { qi[k] = q[(size_t)V * i + k]; qj[k] = q[(size_t)V * j + k]; }
         }
-        fvo_flux(ph, f, qi, qj, n);
+        if (ph->diffusive) {
+            const double ci[2] = {m->ccx[i], m->ccy[i]}, cj[2] = {m->ccx[j], m->ccy[j]};
+            face_gradient(V, gxf, gyf, gx + (size_t)V * i, gy + (size_t)V * i, gx + (size_t)V * j,
+                          gy + (size_t)V * j, q + (size_t)V * i, q + (size_t)V * j, ci, cj);
+        }
+        if (ph->flux == FVO_FLUX_DIFFUSION) {
+            f[0] = -(gxf[0] * n[0] + gyf[0] * n[1]);  /* examples/heatTransfer/main.cpp:63-73 */
+        } else {
+            fvo_flux(ph, f, qi, qj, n);
+        }
         for (int k = 0; k < V; ++k) {
             qt[(size_t)V * i + k] -= f[k] * le / m->area[i];
             qt[(size_t)V * j + k] += f[k] * le / m->area[j];
@@ -533,10 +561,8 @@ int fvo_run_loop(const fvo_mesh* m, const fvo_physics* ph, double* q, const doub
         if (ph->global_dt) fvo_min_dt(m, dt);
         memcpy(qk, q, n * 8);
         for (int s = 0; s < n_alpha; ++s) {
-            if (ph->order2) {
-                fvo_calc_gradients(m, ph, qk, gx, gy);
-                fvo_calc_limiters(m, ph, qk, gx, gy, lim);
-            }
+            if (ph->order2 || ph->diffusive) fvo_calc_gradients(m, ph, qk, gx, gy);
+            if (ph->order2) fvo_calc_limiters(m, ph, qk, gx, gy, lim);
             fvo_calc_time_derivatives(m, ph, qk, gx, gy, lim, qt);
             for (int64_t i = 0; i < m->n_total; ++i) /* update_cells, explicit.cpp:368-378 */
                 for (int k = 0; k < V; ++k) {

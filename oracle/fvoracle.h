@@ -30,7 +30,9 @@ typedef struct {
     int32_t* bound_group;                 /* [n_bound] boundary group of ghost b */
 } fvo_mesh;
 
-enum { FVO_FLUX_ROE_FS = 1, FVO_FLUX_ROE_ST = 2, FVO_FLUX_BURGERS = 3 };
+/* DIFFUSION: the heat-equation flux F = -(grad T . n) of examples/heatTransfer
+   (V = 1), with the face gradient of gradient_for_diffusion. */
+enum { FVO_FLUX_ROE_FS = 1, FVO_FLUX_ROE_ST = 2, FVO_FLUX_BURGERS = 3, FVO_FLUX_DIFFUSION = 4 };
 enum { FVO_LIM_ZERO = 0, FVO_LIM_MICHALAK = 1, FVO_LIM_VENKAT = 2, FVO_LIM_MINMOD = 3 };
 enum { FVO_DT_CONST = 0, FVO_DT_CFL_SUM = 1, FVO_DT_CFL_MIN_SIGNED = 2 };
 enum { FVO_BC_COPY = 0, FVO_BC_WALL = 1, FVO_BC_INLET_OUTLET = 2, FVO_BC_FARFIELD = 3 };
@@ -52,6 +54,8 @@ typedef struct {
                                  to the cell value (not in the reference; 0 = reference) */
     const double* ghost_bv;   /* [n_bound][4] per-ghost far-field / inflow state overriding
                                  group_bv (a spatially varying inflow; NULL = group_bv) */
+    int diffusive;            /* solver::diffusive_gradients (with order2 = 0: gradients are
+                                 computed, no limiter, no interpolation) */
 } fvo_physics;
 
 int fvo_mesh_build(int64_t n_nodes, const double* nodes_x, const double* nodes_y,

@@ -20,7 +20,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF_DIR = os.path.join(HERE, "_ref")
 
-FLUX = {"roe_fs": 1, "roe_st": 2, "burgers": 3}
+FLUX = {"roe_fs": 1, "roe_st": 2, "burgers": 3, "diffusion": 4}
 LIMITER = {"zero": 0, "michalak": 1, "venkat": 2, "minmod": 3}
 DT = {"const": 0, "cfl_sum": 1, "cfl_min_signed": 2}
 BC = {"copy": 0, "wall": 1, "inlet_outlet": 2, "farfield": 3}
@@ -48,7 +48,7 @@ class _FvoPhysics(C.Structure):
                 ("limiter", C.c_int), ("K", C.c_double), ("dt_kind", C.c_int),
                 ("cfl", C.c_double), ("dt_const", C.c_double), ("global_dt", C.c_int),
                 ("n_groups", C.c_int), ("group_bc", _i32p), ("group_bv", _dp), ("positivity_guard", C.c_int),
-                ("ghost_bv", _dp)]
+                ("ghost_bv", _dp), ("diffusive", C.c_int)]
 
 
 def build_oracle():
@@ -133,6 +133,7 @@ class Oracle:
         p.n_groups = len(group_names)
         p.group_bc = _ptr(gbc, _i32p); p.group_bv = _ptr(gbv)
         p.positivity_guard = int(getattr(phys, "positivity_guard", False))
+        p.diffusive = int(getattr(phys, "diffusive", False))
         gh = None
         if ghost_bv is not None:
             gh = np.ascontiguousarray(ghost_bv, np.float64).reshape(-1)

@@ -44,7 +44,7 @@ extern double gamma; extern double cfl; extern double mach;
 extern double gamma; extern double cfl;
 #elif defined(FVREF_EX_SHOCKTUBE)
 extern double gamma;
-#endif
+#endif  // heatTransfer and burgers have no consts:: globals
 }
 
 #if FVREF_OVERRIDE

@@ -56,6 +56,9 @@ CASES = {
     "naca": dict(mesh=lambda: meshgen.naca_ogrid(ni=48, nj=12, r_far=10.0),
                  phys=lambda: P.naca(), ic=lambda g: P.ic_naca(g.n_total).ravel(), alpha=P.RK5_ALPHA,
                  steps=30, ref="naca", alias={}, consts=dict(cfl=1.0)),
+    "heat": dict(mesh=lambda: meshgen.rect_tri(16, 16, 1.0, 1.0, side_names=("wall", "wall")),
+                 phys=lambda: P.heat(), ic=lambda g: P.ic_heat(g.ccx, g.ccy).ravel(),
+                 alpha=P.RK5_ALPHA, steps=30, ref="heatTransfer", alias={}, consts={}),
     "burgers": dict(mesh=lambda: meshgen.rect_tri(16, 16, 1.0, 1.0, side_names=("wall", "wall")),
                     phys=lambda: P.burgers(), ic=lambda g: P.ic_burgers(g.ccx, g.ccy).ravel(),
                     alpha=P.RK5_ALPHA, steps=30, ref="burgers", alias={}, consts={}),

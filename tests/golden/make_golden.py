@@ -52,7 +52,9 @@ def make(name):
     lim = ref.limiters(q, gx, gy) if flags["lim"] else np.zeros_like(q)
     out["stage_lim"] = lim
     if not flags["linear"]:
-        gx = np.zeros_like(q); gy = np.zeros_like(q); lim = np.zeros_like(q)
+        lim = np.zeros_like(q)
+        if not flags["diffusive"]:  # the gradients feed only the diffusive face gradient
+            gx = np.zeros_like(q); gy = np.zeros_like(q)
     out["stage_qt"] = ref.time_derivatives(q, gx, gy, lim)
     out["stage_bounds"] = ref.update_bounds(q, gx, gy, lim)
     # the time loop from the example's initial condition family

@@ -36,6 +36,19 @@ def rand_state(g, ph, seed):
     return np.random.default_rng(seed).uniform(-1, 1, g.n_total * ph.V)
 
 
+def stage_inputs(oracle, g, p, ph, q):
+    """gx, gy, lim as a reference stage sees them: gradients and limiters
+    (second order), unlimited gradients (diffusive fluxes: lim is unused and
+    the device's is 1), or nothing (first order)."""
+    if ph.order2:
+        gx, gy = oracle.gradients(g, p, q)
+        return gx, gy, oracle.limiters(g, p, q, gx, gy)
+    if ph.diffusive:
+        gx, gy = oracle.gradients(g, p, q)
+        return gx, gy, np.ones_like(q)
+    return np.zeros_like(q), np.zeros_like(q), np.zeros_like(q)
+
+
 @pytest.mark.parametrize("name", sorted(CASES))
 def test_stage_dt(name, oracle):
     case, em, ph, s, g, p = setup(name, oracle)
@@ -44,13 +57,12 @@ def test_stage_dt(name, oracle):
         assert bits_equal(s.stage_dt(q, glob), oracle.calc_dt(g, p, q, glob))
 
 
-@pytest.mark.parametrize("name", [n for n in sorted(CASES) if CASES[n]["phys"]().order2])
+@pytest.mark.parametrize("name", [n for n in sorted(CASES) if CASES[n]["phys"]().order2 or CASES[n]["phys"]().diffusive])
 def test_stage_gradients_limiters(name, oracle):
     case, em, ph, s, g, p = setup(name, oracle)
     q = rand_state(g, ph, 4)
     gx, gy, lim = s.stage_gradients_limiters(q)
-    ogx, ogy = oracle.gradients(g, p, q)
-    olim = oracle.limiters(g, p, q, ogx, ogy)
+    ogx, ogy, olim = stage_inputs(oracle, g, p, ph, q)
     assert bits_equal(gx, ogx) and bits_equal(gy, ogy) and bits_equal(lim, olim)
 
 
@@ -59,11 +71,7 @@ def test_stage_update_and_ghost_fill(name, oracle):
     case, em, ph, s, g, p = setup(name, oracle)
     qb = rand_state(g, ph, 5)
     qs = rand_state(g, ph, 6)
-    if ph.order2:
-        gx, gy = oracle.gradients(g, p, qs)
-        lim = oracle.limiters(g, p, qs, gx, gy)
-    else:
-        gx = np.zeros_like(qs); gy = np.zeros_like(qs); lim = np.zeros_like(qs)
+    gx, gy, lim = stage_inputs(oracle, g, p, ph, qs)
     dt = oracle.calc_dt(g, p, qs, ph.global_dt)
     alpha = 0.2898
     qt = oracle.time_derivatives(g, p, qs, gx, gy, lim)
@@ -194,16 +202,13 @@ def test_fp64_stage_functions(name, oracle):
     q = rand_state(g, ph, 21)
     e_dt = normwise_rel(s.stage_dt(q, False), oracle.calc_dt(g, p, q, False), 1)
     assert e_dt < FP64_STEP_RTOL, e_dt
-    if ph.order2:
+    ogx, ogy, olim = stage_inputs(oracle, g, p, ph, q)
+    if ph.order2 or ph.diffusive:
         # FP64 keeps the limiter multiplied into the gradients
         gx, gy, lim = s.stage_gradients_limiters(q)
-        ogx, ogy = oracle.gradients(g, p, q)
-        olim = oracle.limiters(g, p, q, ogx, ogy)
         e = (normwise_rel(gx, ogx * olim, ph.V), normwise_rel(gy, ogy * olim, ph.V))
         assert max(e) < 1e-9, e
         assert np.all(lim == 1.0)
-    else:
-        ogx = np.zeros_like(q); ogy = np.zeros_like(q); olim = np.zeros_like(q)
     dt = oracle.calc_dt(g, p, q, ph.global_dt)
     qb = rand_state(g, ph, 22)
     qt = oracle.time_derivatives(g, p, q, ogx, ogy, olim)
@@ -262,13 +267,14 @@ def test_fp32_l2_error(name, oracle):
     assert s.check_state() == 0
 
 
-def test_fp32_burgers(oracle):
-    case, em, ph, s, g, p = setup("burgers", oracle, "fp32")
+@pytest.mark.parametrize("name", ["burgers", "heat"])
+def test_fp32_scalar_kinds(name, oracle):
+    case, em, ph, s, g, p = setup(name, oracle, "fp32")
     q0 = case["ic"](g)
     want = oracle.run_loop(g, p, q0, case["alpha"], case["steps"])
     s.set_state(q0)
     s.run(case["steps"], alpha=case["alpha"])
-    n = g.n_real * 2
+    n = g.n_real * ph.V
     assert l2_rel(s.get_state()[:n], want["q"][:n]) < FP32_L2_TOL
 
 

@@ -190,3 +190,46 @@ def test_su2_reader_errors(tmp_path):
         fvgpu.Mesh.read_su2(str(bad))
     with pytest.raises(fvgpu.FvError):
         fvgpu.Mesh.read_su2(str(tmp_path / "missing.su2"))
+
+
+def test_host_diffusion_kind_matches_its_restatement():
+    """fv_kind_face_gradient / fv_kind_flux_grad (the host copies of the
+    device's diffusion kind, which the fvhyper shim matches calc_flux to)
+    against numpy written in the order of gradient_for_diffusion
+    (explicit.cpp:70-109) and examples/heatTransfer/main.cpp:63-73: IEEE
+    float64 operations in the same order give the same bits."""
+    L = fvgpu.lib()
+    dp = ctypes.POINTER(ctypes.c_double)
+    rng = np.random.default_rng(5)
+
+    def p(a):
+        return a.ctypes.data_as(dp)
+
+    for V in (1, 2, 4):
+        for _ in range(50):
+            gxi, gyi, gxj, gyj, qi, qj = (rng.uniform(-3, 3, V) for _ in range(6))
+            ci, cj = rng.uniform(-1, 1, 2), rng.uniform(-1, 1, 2)
+            gxf, gyf = np.zeros(V), np.zeros(V)
+            assert L.fv_kind_face_gradient(V, p(gxi), p(gyi), p(gxj), p(gyj), p(qi), p(qj), p(ci), p(cj),
+                                           p(gxf), p(gyf)) == 0
+            t = ci - cj
+            lij = np.sqrt(t[0] * t[0] + t[1] * t[1])
+            t = t / lij
+            d = (qi - qj) / lij
+            bx, by = (gxi + gxj) * 0.5, (gyi + gyj) * 0.5
+            dot = bx * t[0] + by * t[1]
+            assert bits_equal(gxf, bx - (dot - d) * t[0]) and bits_equal(gyf, by - (dot - d) * t[1])
+            if V == 1:
+                n = rng.normal(size=2)
+                n /= np.hypot(*n)
+                f = np.zeros(1)
+                assert L.fv_kind_flux_grad(4, ctypes.c_double(0.0), p(qi), p(qj), p(gxf), p(gyf), p(n), p(f)) == 0
+                assert bits_equal(f, -(gxf * n[0] + gyf * n[1]))
+    # the diffusion kind needs its gradients; V = 3 is no device width
+    z = np.zeros(4)
+    assert L.fv_kind_flux(4, ctypes.c_double(0.0), p(z), p(z), p(z), p(z)) == -4
+    assert L.fv_kind_face_gradient(3, p(z), p(z), p(z), p(z), p(z), p(z), p(z), p(z), p(z), p(z)) == -1
+    # V = 1 boundaries: the copy kind
+    q, b = np.array([0.75]), np.zeros(1)
+    assert L.fv_kind_bc(0, 1, ctypes.c_double(1.4), None, p(q), p(np.array([1.0, 0.0])), p(b)) == 0
+    assert b[0] == 0.75

@@ -10,7 +10,8 @@ program built from the same source on fvhyper's own library
   ASCII layout (FVGPU_VTK_FORMAT=ascii);
 - the default binary VTU carries the same cell values.
 
-Examples whose physics the device path does not run (viscous fluxes) and
+Examples whose physics the device path does not run (the viscous Navier-Stokes
+fluxes of flatPlate and nacaTransient) and
 meshes whose boundary names the program does not define must be refused the
 way the reference refuses them: an uncaught std::invalid_argument.
 """
@@ -58,6 +59,7 @@ CASES = {
     "burgers": ("square.msh", lambda: _one_group(meshgen.rect_tri(12, 12, 1.0, 1.0), "wall"), "square.vtu"),
     "naca": ("naca.msh", lambda: meshgen.naca_ogrid(ni=40, nj=10, r_far=10.0, jitter=0.0), "naca.vtu"),
     "forwardStep": ("step.msh", _step_mesh, None),
+    "heatTransfer": ("square.msh", lambda: _one_group(meshgen.rect_tri(12, 12, 1.0, 1.0), "wall"), "square.vtu"),
 }
 
 
@@ -163,7 +165,6 @@ def test_binary_vtu_holds_the_state(tmp_path):
 
 
 @pytest.mark.parametrize("name,mesh,group_names", [
-    ("heatTransfer", "square.msh", ["wall"]),
     ("flatPlate", "square.msh", ["top", "bot0", "bot1", "left", "right"]),
     ("nacaTransient", "naca0012.msh", ["wall", "farfield"]),
 ])
