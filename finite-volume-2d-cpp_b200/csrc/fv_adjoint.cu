@@ -195,7 +195,7 @@ __global__ void __launch_bounds__(kAB) k_adj_ghosts(Params P, AdjFaces F, AdjSta
         exact::bc_state<4>(kind, P.gamma, bvd, bd, xd, n0, n1);
         double lx[4];
         jt(bd, lb, lx);
-        if (kind == 2 || kind == 3) {  // boundary state of an inflow / far-field ghost
+        if (kind == 2 || kind == 3 || kind == 5) {  // boundary state of an inflow / far-field ghost
             constant(xd, x);
             seed(bvd, bv);
             exact::bc_state<4>(kind, P.gamma, bvd, bd, xd, n0, n1);

@@ -1,6 +1,7 @@
 // C ABI of the B200 explicit finite-volume step (include/fvgpu.h).
 #include <cuda_runtime.h>
 
+#include <cmath>
 #include <cstdio>
 #include <algorithm>
 #include <cstring>
@@ -310,6 +311,9 @@ static int validate_physics(const fv_physics* ph, int n_groups_mesh) {
         if (ph->dt_kind != FV_DT_CONST) return fail(FV_ERR_UNSUPPORTED, "the Burgers kind supports a constant dt only");
     } else if (ph->flux == FV_FLUX_ROE_FS || ph->flux == FV_FLUX_ROE_ST) {
         if (ph->V != 4) return fail(FV_ERR_UNSUPPORTED, "the Roe flux kinds have V = 4");
+    } else if (ph->flux == FV_FLUX_NS) {
+        if (ph->V != 4) return fail(FV_ERR_UNSUPPORTED, "the Navier-Stokes flux kind has V = 4");
+        if (!ph->diffusive) return fail(FV_ERR_UNSUPPORTED, "the Navier-Stokes flux kind needs diffusive = 1");
     } else if (ph->flux == FV_FLUX_DIFFUSION) {
         if (ph->V != 1) return fail(FV_ERR_UNSUPPORTED, "the diffusion flux kind has V = 1");
         if (!ph->diffusive) return fail(FV_ERR_UNSUPPORTED, "the diffusion flux kind needs diffusive = 1");
@@ -319,15 +323,20 @@ static int validate_physics(const fv_physics* ph, int n_groups_mesh) {
     } else {
         return fail(FV_ERR_UNSUPPORTED, "unknown flux kind " + std::to_string(ph->flux));
     }
-    if (ph->diffusive && ph->flux != FV_FLUX_DIFFUSION)
-        return fail(FV_ERR_UNSUPPORTED, "diffusive gradients are used by the diffusion flux kind only");
+    if (ph->diffusive && ph->flux != FV_FLUX_DIFFUSION && ph->flux != FV_FLUX_NS)
+        return fail(FV_ERR_UNSUPPORTED, "diffusive gradients are used by the diffusion and Navier-Stokes kinds only");
     if (ph->limiter < 0 || ph->limiter > 3) return fail(FV_ERR_UNSUPPORTED, "unknown limiter kind");
-    if (ph->dt_kind < 0 || ph->dt_kind > 2) return fail(FV_ERR_UNSUPPORTED, "unknown dt kind");
+    if (ph->dt_kind < 0 || ph->dt_kind > 4) return fail(FV_ERR_UNSUPPORTED, "unknown dt kind");
+    if (ph->dt_kind >= FV_DT_VISC_MIN && ph->V != 4) return fail(FV_ERR_UNSUPPORTED, "the viscous dt kinds have V = 4");
+    if (ph->flux == FV_FLUX_NS || ph->dt_kind >= FV_DT_VISC_MIN) {
+        if (!(ph->mu >= 0.0) || !(ph->pr > 0.0) || !(ph->r > 0.0) || !std::isfinite(ph->cp))
+            return fail(FV_ERR_ARG, "Navier-Stokes constants need mu >= 0, pr > 0, r > 0 and a finite cp");
+    }
     if (ph->n_groups < n_groups_mesh) return fail(FV_ERR_ARG, "physics has fewer boundary groups than the mesh");
     if (ph->n_groups > kMaxGroups) return fail(FV_ERR_UNSUPPORTED, "more than 16 boundary groups");
     for (int g = 0; g < ph->n_groups; ++g) {
         const int k = ph->group_bc[g];
-        if (k < 0 || k > 3) return fail(FV_ERR_UNSUPPORTED, "unknown boundary condition kind");
+        if (k < 0 || k > 5) return fail(FV_ERR_UNSUPPORTED, "unknown boundary condition kind");
         if (ph->V != 4 && k != FV_BC_COPY)
             return fail(FV_ERR_UNSUPPORTED, "V = " + std::to_string(ph->V) + " supports the copy boundary only");
     }
@@ -383,6 +392,7 @@ int fv_solver_create_ex(const fv_mesh* fm, const fv_physics* ph, int32_t precisi
     P.global_dt = ph->global_dt ? 1 : 0;
     P.positivity_guard = ph->positivity_guard ? 1 : 0;
     P.diffusive = ph->diffusive ? 1 : 0;
+    P.mu = ph->mu; P.pr = ph->pr; P.cp = ph->cp; P.r = ph->r;
     P.gamma = ph->gamma; P.K = ph->K; P.cfl = ph->cfl; P.dt_const = ph->dt_const;
     P.n_groups = ph->n_groups;
     for (int g = 0; g < ph->n_groups; ++g) {
@@ -1106,7 +1116,7 @@ int fv_stage_gradients_limiters(fv_solver* s, const double* q, double* gx, doubl
     CK(cudaGetLastError());
     if ((rc = d2h(s, as_f64(s, s->gx, t64, s->V), gx, s->V))) return rc;
     if ((rc = d2h(s, as_f64(s, s->gy, t64, s->V), gy, s->V))) return rc;
-    if (s->precision != FV_PREC_FP64_EXACT) {  // limiter already folded into gx, gy
+    if (s->precision != FV_PREC_FP64_EXACT && !s->TP.P.diffusive) {  // limiter already folded into gx, gy
         for (size_t i = 0; i < nq; ++i) lim[i] = 1.0;
         return FV_OK;
     }
@@ -1272,7 +1282,7 @@ int adj_set_theta(fv_adjoint* a, const double* theta, double* q0_dev) {
     std::vector<double> bv((size_t)s->n_bound * 4, 0.0);
     for (int64_t r = 0; r < s->n_bound; ++r) {
         const int kind = a->ghost_kind[(size_t)r];
-        if (kind != FV_BC_INLET_OUTLET && kind != FV_BC_FARFIELD) continue;
+        if (kind != FV_BC_INLET_OUTLET && kind != FV_BC_FARFIELD && kind != FV_BC_FARFIELD_B0) continue;
         const int b = a->ghost_bin[(size_t)r];
         const double rho = a->rho_inf * (1.0 + (b >= 0 && b < nb ? theta[1 + b] : 0.0));
         bv[4 * r] = rho; bv[4 * r + 1] = rho * M; bv[4 * r + 2] = 0.0; bv[4 * r + 3] = e_inf + 0.5 * rho * M * M;
@@ -1320,7 +1330,8 @@ int fv_adjoint_create(const fv_mesh* fm, const fv_physics* ph, int32_t device, c
     const int ng = (int)m.group_names.size();
     if (o->param_group < 0 || o->param_group >= ng || o->loss_group < 0 || o->loss_group >= ng)
         return fail(FV_ERR_ARG, "fv_adjoint_create: group index out of range");
-    if (ph->group_bc[o->param_group] != FV_BC_INLET_OUTLET && ph->group_bc[o->param_group] != FV_BC_FARFIELD)
+    if (ph->group_bc[o->param_group] != FV_BC_INLET_OUTLET && ph->group_bc[o->param_group] != FV_BC_FARFIELD &&
+        ph->group_bc[o->param_group] != FV_BC_FARFIELD_B0)
         return fail(FV_ERR_ARG, "fv_adjoint_create: the parameter group must be an inflow / far-field boundary");
     if (m.case_real_off.size() > 2) return fail(FV_ERR_UNSUPPORTED, "fv_adjoint: not on batches");
     std::unique_ptr<fv_adjoint> a(new fv_adjoint());
@@ -1497,7 +1508,7 @@ int fv_adjoint_run(fv_adjoint* a, const double* theta, double* loss, double* gra
     for (int64_t gb = 0; gb < s->n_bound; ++gb) {
         const int64_t r = (int64_t)n2r[(size_t)(s->n_real + gb)] - s->n_real;
         const int kind = a->ghost_kind[(size_t)r];
-        if (kind != FV_BC_INLET_OUTLET && kind != FV_BC_FARFIELD) continue;
+        if (kind != FV_BC_INLET_OUTLET && kind != FV_BC_FARFIELD && kind != FV_BC_FARFIELD_B0) continue;
         const int b = a->ghost_bin[(size_t)r];
         const double rho = a->rho_inf * (1.0 + (b >= 0 ? theta[1 + b] : 0.0));
         const double* l = &lbv[(size_t)gb * 4];

@@ -54,6 +54,7 @@ struct Params {
     int flux, order2, limiter, dt_kind, global_dt, positivity_guard;
     int diffusive;                  // cell gradients feed the face gradient of the flux
     double gamma, K, cfl, dt_const;
+    double mu, pr, cp, r;           // Navier-Stokes constants (viscous flux and dt kinds)
     int n_groups;
     int group_bc[kMaxGroups];
     double group_bv[kMaxGroups * 4];

@@ -22,12 +22,22 @@ int fv_kind_flux(int32_t flux, double gamma, const double* qi, const double* qj,
     }
 }
 
-int fv_kind_flux_grad(int32_t flux, double gamma, const double* qi, const double* qj, const double* gx,
+int fv_kind_flux_grad(const fv_physics* ph, const double* qi, const double* qj, const double* gx,
                       const double* gy, const double* n, double* f) {
-    if (flux != FV_FLUX_DIFFUSION) return fv_kind_flux(flux, gamma, qi, qj, n, f);
-    if (!gx || !gy || !n || !f) return FV_ERR_ARG;
-    fvgpu::exact::diffusion(f, gx, gy, n[0], n[1]);
-    return FV_OK;
+    if (!ph || !qi || !qj || !gx || !gy || !n || !f) return FV_ERR_ARG;
+    if (ph->flux == FV_FLUX_DIFFUSION) {
+        fvgpu::exact::diffusion(f, gx, gy, n[0], n[1]);
+        return FV_OK;
+    }
+    if (ph->flux == FV_FLUX_NS) {
+        fvgpu::Params P;
+        memset(&P, 0, sizeof(P));
+        P.gamma = ph->gamma; P.mu = ph->mu; P.pr = ph->pr; P.cp = ph->cp; P.r = ph->r;
+        fvgpu::exact::roe<false>(P.gamma, f, qi, qj, n[0], n[1]);
+        fvgpu::exact::ns_viscous(P, f, qi, qj, gx, gy, n[0], n[1]);
+        return FV_OK;
+    }
+    return fv_kind_flux(ph->flux, ph->gamma, qi, qj, n, f);
 }
 
 int fv_kind_face_gradient(int32_t V, const double* gxi, const double* gyi, const double* gxj, const double* gyj,
@@ -53,8 +63,9 @@ int fv_kind_limiter(int32_t kind, double y, double* out) {
 int fv_kind_bc(int32_t kind, int32_t V, double gamma, const double* bv, const double* q, const double* n,
                double* b) {
     if (!q || !n || !b || (V != 1 && V != 2 && V != 4)) return FV_ERR_ARG;
-    if (kind < FV_BC_COPY || kind > FV_BC_FARFIELD) return FV_ERR_UNSUPPORTED;
-    if ((kind == FV_BC_INLET_OUTLET || kind == FV_BC_FARFIELD) && !bv) return FV_ERR_ARG;
+    if (kind < FV_BC_COPY || kind > FV_BC_FARFIELD_B0) return FV_ERR_UNSUPPORTED;
+    if ((kind == FV_BC_INLET_OUTLET || kind == FV_BC_FARFIELD || kind == FV_BC_FARFIELD_B0) && !bv)
+        return FV_ERR_ARG;
     fvgpu::Params P;
     memset(&P, 0, sizeof(P));
     P.V = V;

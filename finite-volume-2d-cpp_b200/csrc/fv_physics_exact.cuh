@@ -119,6 +119,49 @@ FV_HD void diffusion(double* f, const double* gxf, const double* gyf, double n0,
     f[0] = -(gxf[0] * n0 + gyf[0] * n1);
 }
 
+// Viscous part of the Navier-Stokes flux (examples/flatPlate/main.cpp:193-224
+// with calc_p, calc_grad_p, calc_grad_t, calc_grad_u, calc_grad_v of
+// :38-92): stresses and heat flux at the mean of the face states qi, qj from
+// the face gradient (gx, gy), subtracted from f (the roe<false> flux).
+FV_HD void ns_viscous(const Params& P, double* f, const double* qi, const double* qj, const double* gx,
+                      const double* gy, double n0, double n1) {
+    const double gamma = P.gamma, mu = P.mu;
+    double q[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) q[i] = 0.5 * (qi[i] + qj[i]);
+    const double p = (gamma - 1) * (q[3] - 0.5 / q[0] * (q[1] * q[1] + q[2] * q[2]));
+    double gp0 = 2. * gx[3];
+    gp0 -= gx[1] * q[1] / q[0] + q[1] * (gx[1] * q[0] - gx[0] * q[1]) / (q[0] * q[0]);
+    gp0 -= gx[2] * q[2] / q[0] + q[2] * (gx[2] * q[0] - gx[0] * q[2]) / (q[0] * q[0]);
+    gp0 *= 0.5 * (gamma - 1);
+    double gp1 = 2. * gy[3];
+    gp1 -= gy[1] * q[1] / q[0] + q[1] * (gy[1] * q[0] - gy[0] * q[1]) / (q[0] * q[0]);
+    gp1 -= gy[2] * q[2] / q[0] + q[2] * (gy[2] * q[0] - gy[0] * q[2]) / (q[0] * q[0]);
+    gp1 *= 0.5 * (gamma - 1);
+    const double gt0 = (1. / P.r) * ((gp0 * q[0] - gx[0] * p) / (q[0] * q[0]));
+    const double gt1 = (1. / P.r) * ((gp1 * q[0] - gy[0] * p) / (q[0] * q[0]));
+    const double gu0 = (q[0] * gx[1] - q[1] * gx[0]) / (q[0] * q[0]);
+    const double gu1 = (q[0] * gy[1] - q[1] * gy[0]) / (q[0] * q[0]);
+    const double gv0 = (q[0] * gx[2] - q[2] * gx[0]) / (q[0] * q[0]);
+    const double gv1 = (q[0] * gy[2] - q[2] * gy[0]) / (q[0] * q[0]);
+    const double div_v = gu0 + gv1;
+    const double tau_xx = 2. * mu * (gu0 - div_v / 3.);
+    const double tau_yy = 2. * mu * (gv1 - div_v / 3.);
+    const double tau_xy = mu * (gu1 + gv0);
+    const double k = P.cp * mu / P.pr;
+    const double phi0 = q[1] / q[0] * tau_xx + q[2] / q[0] * tau_xy + k * gt0;
+    const double phi1 = q[1] / q[0] * tau_xy + q[2] / q[0] * tau_yy + k * gt1;
+    f[1] -= n0 * tau_xx + n1 * tau_xy;
+    f[2] -= n0 * tau_xy + n1 * tau_yy;
+    f[3] -= n0 * phi0 + n1 * phi1;
+}
+
+// Viscous eigenvalue of the viscous time steps, max(4/(3 rho), gamma/rho) *
+// (mu/pr) * le^2 / A (flatPlate/main.cpp:264-267).
+FV_HD double visc_eig(const Params& P, double rho, double le, double A) {
+    return dmax(4. / (3. * rho), P.gamma / rho) * (P.mu / P.pr) * le * le / A;
+}
+
 // Limiter functions phi (limiter_func).  ZERO: shockTube/main.cpp:60-62.
 // MICHALAK (y_t = 2): forwardStep/main.cpp:57-66.  MINMOD: burgers/main.cpp:
 // 51-53.  VENKAT: (y^2 + 2y)/(y^2 + y + 2), Venkatakrishnan (1995).
@@ -138,7 +181,8 @@ FV_HD double limiter_func(int kind, double y) {
 // Boundary conditions (boundaries::bounds entries).  COPY: shockTube/main.cpp:
 // 158-163.  WALL: forwardStep/main.cpp:262-269.  INLET_OUTLET: forwardStep/
 // main.cpp:194-261.  FARFIELD: naca/main.cpp:192-259.  Subsonic outlets keep
-// the reference's b[2] = b[1]*(...).
+// the reference's b[2] = b[1]*(...).  NOSLIP: flatPlate/main.cpp:361-366.
+// FARFIELD_B0: flatPlate/main.cpp:286-352, FARFIELD with b[2] = b[0]*(...).
 template <int V, class T>
 FV_HD void bc_state(int kind, double gamma, const T* bv, T* b, const T* q, double n0, double n1) {
     if (kind == 0 || V != 4) {
@@ -153,6 +197,11 @@ FV_HD void bc_state(int kind, double gamma, const T* bv, T* b, const T* q, doubl
         b[3] = q[3];
         return;
     }
+    if (kind == 4) {
+        b[0] = q[0]; b[1] = -q[1]; b[2] = -q[2]; b[3] = q[3];
+        return;
+    }
+    const bool b0 = kind == 5;  // FARFIELD_B0: the tangential momentum's factor is b[0], not b[1]
     const T U0 = q[1] / q[0], U1 = q[2] / q[0];
     const T u_norm = sqrt(U0 * U0 + U1 * U1);
     const T u_dot_n = U0 * n0 + U1 * n1;
@@ -180,14 +229,14 @@ FV_HD void bc_state(int kind, double gamma, const T* bv, T* b, const T* q, doubl
             const T pb = 0.5 * (pa + pd - rho0 * c0 * (n0 * (ua - ud) + n1 * (va - vd)));
             b[0] = rhoa + (pb - pa) / (c0 * c0);
             b[1] = b[0] * (ua - n0 * (pa - pb) / (rho0 * c0));
-            b[2] = b[1] * (va - n1 * (pa - pb) / (rho0 * c0));
+            b[2] = (b0 ? b[0] : b[1]) * (va - n1 * (pa - pb) / (rho0 * c0));
             b[3] = pb / (gamma - 1) + 0.5 / b[0] * (b[1] * b[1] + b[2] * b[2]);
         }
     } else {
         const T pb = pa;
         b[0] = rhod + (pb - pd) / (c0 * c0);
         b[1] = b[0] * (ud + n0 * (pd - pb) / (rho0 * c0));
-        b[2] = b[1] * (va + n1 * (pd - pb) / (rho0 * c0));
+        b[2] = (b0 ? b[0] : b[1]) * (va + n1 * (pd - pb) / (rho0 * c0));
         b[3] = pb / (gamma - 1.) + 0.5 / b[0] * (b[1] * b[1] + b[2] * b[2]);
     }
 }

@@ -103,6 +103,36 @@ __device__ __forceinline__ void diffusion(T* f, const T* gxi, const T* gyi, cons
     }
 }
 
+// Viscous part of the Navier-Stokes flux (see fv_physics_exact.cuh): the
+// gradients of u, v and T at the mean face state from the face gradient,
+// with 1/rho taken once.
+template <class T>
+__device__ __forceinline__ void ns_viscous(const Params& P, T* f, const T* qi, const T* qj, const T* gx,
+                                           const T* gy, T n0, T n1) {
+    const T gm1 = (T)P.gamma - T(1), mu = (T)P.mu;
+    T q[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) q[i] = T(0.5) * (qi[i] + qj[i]);
+    const T ri = rcp(q[0]);
+    const T u = q[1] * ri, v = q[2] * ri, E = q[3] * ri;
+    // d(u), d(v), d(E) = (d(rho x) - x d(rho)) / rho; T = (gamma-1)/r * (E - (u^2+v^2)/2)
+    const T gu0 = (gx[1] - u * gx[0]) * ri, gu1 = (gy[1] - u * gy[0]) * ri;
+    const T gv0 = (gx[2] - v * gx[0]) * ri, gv1 = (gy[2] - v * gy[0]) * ri;
+    const T cT = gm1 * (T)(1.0 / P.r);
+    const T gt0 = cT * ((gx[3] - E * gx[0]) * ri - (u * gu0 + v * gv0));
+    const T gt1 = cT * ((gy[3] - E * gy[0]) * ri - (u * gu1 + v * gv1));
+    const T div3 = (gu0 + gv1) * T(1.0 / 3.0);
+    const T tau_xx = T(2) * mu * (gu0 - div3);
+    const T tau_yy = T(2) * mu * (gv1 - div3);
+    const T tau_xy = mu * (gu1 + gv0);
+    const T k = (T)(P.cp * P.mu / P.pr);
+    const T phi0 = u * tau_xx + v * tau_xy + k * gt0;
+    const T phi1 = u * tau_xy + v * tau_yy + k * gt1;
+    f[1] -= n0 * tau_xx + n1 * tau_xy;
+    f[2] -= n0 * tau_xy + n1 * tau_yy;
+    f[3] -= n0 * phi0 + n1 * phi1;
+}
+
 // limiter_func kinds (see fv_physics_exact.cuh for the references).
 template <class T>
 __device__ __forceinline__ T limiter_func(int kind, T y) {
@@ -128,6 +158,11 @@ __device__ __forceinline__ void bc(const Params& P, int group, int gb, T* b, con
         b[0] = q[0]; b[1] = q[1] - n0 * dn; b[2] = q[2] - n1 * dn; b[3] = q[3];
         return;
     }
+    if (kind == 4) {
+        b[0] = q[0]; b[1] = -q[1]; b[2] = -q[2]; b[3] = q[3];
+        return;
+    }
+    const bool b0 = kind == 5;  // FARFIELD_B0: the tangential momentum's factor is b[0], not b[1]
     const T gamma = (T)P.gamma, gm1 = gamma - T(1);
     const double* bvd = P.ghost_bv ? P.ghost_bv + 4 * (size_t)gb : P.group_bv + 4 * group;
     const T bv[4] = {(T)bvd[0], (T)bvd[1], (T)bvd[2], (T)bvd[3]};
@@ -147,7 +182,9 @@ __device__ __forceinline__ void bc(const Params& P, int group, int gb, T* b, con
     const T pa = gm1 * (bv[3] - T(0.5) * rbv * (bv[1] * bv[1] + bv[2] * bv[2]));
     const T ua = bv[1] * rbv, va = bv[2] * rbv;
     const T pd = p, ud = U0, vd = U1, rho0 = q[0];
-    const T rrc = rcp(rho0 * c0), rc2 = rcp(c2);
+    // 1/c0^2 from c0 (not c2): a state with p < 0 gives NaN in every
+    // component, as the reference's (pb - pd)/(c0*c0) does
+    const T rrc = rcp(rho0 * c0), rc2 = rcp(c0 * c0);
     const T rgm1 = rcp(gm1);
     if (u_dot_n < T(0)) {
         if (kind == 2) {
@@ -157,14 +194,14 @@ __device__ __forceinline__ void bc(const Params& P, int group, int gb, T* b, con
             const T pb = T(0.5) * (pa + pd - rho0 * c0 * (n0 * (ua - ud) + n1 * (va - vd)));
             b[0] = bv[0] + (pb - pa) * rc2;
             b[1] = b[0] * (ua - n0 * (pa - pb) * rrc);
-            b[2] = b[1] * (va - n1 * (pa - pb) * rrc);
+            b[2] = (b0 ? b[0] : b[1]) * (va - n1 * (pa - pb) * rrc);
             b[3] = pb * rgm1 + T(0.5) * rcp(b[0]) * (b[1] * b[1] + b[2] * b[2]);
         }
     } else {
         const T pb = pa;
         b[0] = q[0] + (pb - pd) * rc2;
         b[1] = b[0] * (ud + n0 * (pd - pb) * rrc);
-        b[2] = b[1] * (va + n1 * (pd - pb) * rrc);  // b[1] as in the reference
+        b[2] = (b0 ? b[0] : b[1]) * (va + n1 * (pd - pb) * rrc);  // b[1] (b[0] for FARFIELD_B0) as in the reference
         b[3] = pb * rgm1 + T(0.5) * rcp(b[0]) * (b[1] * b[1] + b[2] * b[2]);
     }
 }

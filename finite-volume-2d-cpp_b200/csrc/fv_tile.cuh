@@ -137,12 +137,13 @@ __device__ __forceinline__ void lds(const S* p, S* v) {
 }
 
 // Shared-memory record of one tile-local cell: q[V], then (with gradients)
-// gx[V], gy[V], (exact) lim[V], then the centroid on an even word (one
-// 2-word copy); padded to 16 bytes.
-template <class M, int V, bool ORDER2, bool CENTROID>
+// gx[V], gy[V], (LIM: exact mode, or a flux that needs the raw gradients)
+// lim[V], then the centroid on an even word (one 2-word copy); padded to 16
+// bytes.
+template <class M, int V, bool ORDER2, bool CENTROID, bool LIM = M::exact>
 struct Rec {
     using S = typename M::S;
-    static constexpr int NG = ORDER2 ? (M::exact ? 3 : 2) : 0;
+    static constexpr int NG = ORDER2 ? (LIM ? 3 : 2) : 0;
     static constexpr int OGX = V, OGY = 2 * V, OLM = 3 * V;
     static constexpr int OC = (V * (1 + NG) + 1) / 2 * 2;
     static constexpr int RAW = OC + (CENTROID ? 2 : 0);
@@ -189,11 +190,11 @@ __device__ __forceinline__ void cpa(void* dst, const void* src) {
 }
 
 // Loads the records of the tile's owned cells and halo (asynchronously).
-template <class M, int V, bool ORDER2, bool CENTROID>
+template <class M, int V, bool ORDER2, bool CENTROID, bool LIM = M::exact>
 __device__ __forceinline__ void stage_records(const TileParams& TP, const TileIO& io, const int4& inf, int c0,
                                               int nown, typename M::S* rec) {
     using S = typename M::S;
-    using R = Rec<M, V, ORDER2, CENTROID>;
+    using R = Rec<M, V, ORDER2, CENTROID, LIM>;
     constexpr int QB = V * (int)sizeof(S);
     const S* Q = (const S*)io.q_stage;
     const S* CXY = (const S*)TP.ccxy;
@@ -206,7 +207,7 @@ __device__ __forceinline__ void stage_records(const TileParams& TP, const TileIO
         if (ORDER2) {
             cpa<QB>(r + R::OGX, (const S*)io.gx + (size_t)V * g);
             cpa<QB>(r + R::OGY, (const S*)io.gy + (size_t)V * g);
-            if (M::exact) cpa<QB>(r + R::OLM, (const S*)io.lim + (size_t)V * g);
+            if (LIM) cpa<QB>(r + R::OLM, (const S*)io.lim + (size_t)V * g);
         }
         if (CENTROID) cpa<2 * (int)sizeof(S)>(r + R::OC, CXY + 2 * (size_t)g);
     }
@@ -237,11 +238,135 @@ __device__ __forceinline__ void load_faces(const TileParams& TP, int c, uint16_t
 }
 
 // ------------------------------------------------------------------ K0: dt --
+// Viscous time steps of owned cell c and of its boundary ghosts (C = 2):
+// VISC_MIN (dt_kind 3, examples/flatPlate/main.cpp:230-277) and VISC_SUM
+// (dt_kind 4, examples/nacaTransient/main.cpp:234-285); the sum kind reads
+// the neighbour's area.  Faces are visited in reference edge order.
+template <class M, int NR>
+__device__ __forceinline__ unsigned long long tile_cell_dt_visc(const TileParams& TP, const TileIO& io,
+                                                                const int4& inf, int l, int c, const uint16_t* w,
+                                                                const typename M::S* rec, const uint32_t* sij,
+                                                                const typename M::S* snx,
+                                                                const typename M::S* sny,
+                                                                const typename M::S* sle) {
+    using S = typename M::S;
+    const Params& P = TP.P;
+    const int T = TP.T;
+    const S* AR = (const S*)TP.area;
+    const bool sum = P.dt_kind == 4;
+    unsigned long long kmin = ~0ull;
+    S qs[4];
+    lds<S, 4>(rec + (size_t)l * NR, qs);
+    if constexpr (M::exact) {
+        const double gamma = P.gamma, gm1 = gamma - 1, cfl = P.cfl, C = 2;
+        const double cs = sqrt((gm1 * (qs[3] - 0.5 / qs[0] * (qs[1] * qs[1] + qs[2] * qs[2]))) * gamma / qs[0]);
+        const double Ai = AR[c];
+        double acc = sum ? 0. : 1.0;
+#pragma unroll
+        for (int f = 0; f < kMaxFaces; ++f) {
+            if (w[f] == kFaceNone) continue;
+            const int el = w[f] & kFaceEdgeMask, side = w[f] >> 15;
+            const uint32_t ij = sij[el];
+            const int o = side ? (int)(ij & 0xffff) : (int)(ij >> 16);
+            const double n0 = snx[el], n1 = sny[el], le = sle[el];
+            const bool ghost = (w[f] & 0x4000) != 0;
+            double qn[4];
+            lds<double, 4>(rec + (size_t)o * NR, qn);
+            const double cn = sqrt((gm1 * (qn[3] - 0.5 / qn[0] * (qn[1] * qn[1] + qn[2] * qn[2]))) * gamma / qn[0]);
+            const double evs = exact::visc_eig(P, qs[0], le, Ai);
+            if (sum) {
+                const int gn = o < T ? c - l + o : TP.halo[inf.z + o - T];
+                const double An = AR[gn];
+                const double ts = cs + fabs(qs[1] / qs[0] * n0 + qs[2] / qs[0] * n1) + C * evs;
+                const double tn = cn + fabs(qn[1] / qn[0] * n0 + qn[2] / qn[0] * n1) + C * exact::visc_eig(P, qn[0], le, An);
+                const double center = side ? exact::dmax(tn, ts) : exact::dmax(ts, tn);
+                acc += center * le;
+                if (ghost) {
+                    double d = 0.;
+                    d += center * le;
+                    const double dg = cfl * An / d;
+                    io.dt[gn] = dg;
+                    kmin = kmin_(kmin, tkey(dg));
+                }
+            } else {
+                const double es = (cs + fabs(n0 * qs[1] / qs[0]) + fabs(n1 * qs[2] / qs[0])) * le;
+                acc = exact::dmin(acc, cfl * Ai / (es + C * evs));
+                if (ghost) {
+                    const int gn = TP.halo[inf.z + o - T];
+                    const double An = AR[gn];
+                    const double en = (cn + fabs(n0 * qn[1] / qn[0]) + fabs(n1 * qn[2] / qn[0])) * le;
+                    const double dg = exact::dmin(1.0, cfl * An / (en + C * exact::visc_eig(P, qn[0], le, An)));
+                    io.dt[gn] = dg;
+                    kmin = kmin_(kmin, tkey(dg));
+                }
+            }
+        }
+        const double di = sum ? cfl * Ai / acc : acc;
+        io.dt[c] = di;
+        kmin = kmin_(kmin, tkey(di));
+    } else {
+        const S gamma = (S)P.gamma, gm1 = gamma - S(1), cfl = (S)P.cfl;
+        const S mp2 = S(2) * (S)(P.mu / P.pr);  // C * mu / pr
+        const S ri = fast::rcp(qs[0]);
+        const S us = qs[1] * ri, vs = qs[2] * ri;
+        const S cs = fast::sqrt_(gamma * gm1 * (qs[3] * ri - S(0.5) * (us * us + vs * vs)));
+        const S vs_rho = fast::tmax(S(4.0 / 3.0) * ri, gamma * ri);     // max(4/(3 rho), gamma/rho)
+        const S Ai = AR[c], rAi = fast::rcp(Ai);
+        S acc = sum ? S(0) : S(1);
+#pragma unroll
+        for (int f = 0; f < kMaxFaces; ++f) {
+            if (w[f] == kFaceNone) continue;
+            const int el = w[f] & kFaceEdgeMask, side = w[f] >> 15;
+            const uint32_t ij = sij[el];
+            const int o = side ? (int)(ij & 0xffff) : (int)(ij >> 16);
+            const S n0 = snx[el], n1 = sny[el], le = sle[el];
+            const bool ghost = (w[f] & 0x4000) != 0;
+            S qn[4];
+            lds<S, 4>(rec + (size_t)o * NR, qn);
+            const S rn = fast::rcp(qn[0]);
+            const S un = qn[1] * rn, vn = qn[2] * rn;
+            const S cn = fast::sqrt_(gamma * gm1 * (qn[3] * rn - S(0.5) * (un * un + vn * vn)));
+            const S vn_rho = fast::tmax(S(4.0 / 3.0) * rn, gamma * rn);
+            const S le2 = le * le;
+            if (sum) {
+                const int gn = o < T ? c - l + o : TP.halo[inf.z + o - T];
+                const S An = AR[gn];
+                const S ts = cs + fabs(us * n0 + vs * n1) + mp2 * vs_rho * le2 * rAi;
+                const S tn = cn + fabs(un * n0 + vn * n1) + mp2 * vn_rho * le2 * fast::rcp(An);
+                const S center = fast::tmax(ts, tn);
+                acc += center * le;
+                if (ghost) {
+                    const double dg = (double)(cfl * An * fast::rcp(center * le));
+                    io.dt[gn] = dg;
+                    kmin = kmin_(kmin, tkey(dg));
+                }
+            } else {
+                const S es = (cs + fabs(n0 * us) + fabs(n1 * vs)) * le + mp2 * vs_rho * le2 * rAi;
+                acc = fast::tmin(acc, cfl * Ai * fast::rcp(es));
+                if (ghost) {
+                    const int gn = TP.halo[inf.z + o - T];
+                    const S An = AR[gn];
+                    const S en = (cn + fabs(n0 * un) + fabs(n1 * vn)) * le + mp2 * vn_rho * le2 * fast::rcp(An);
+                    const double dg = (double)fast::tmin(S(1), cfl * An * fast::rcp(en));
+                    io.dt[gn] = dg;
+                    kmin = kmin_(kmin, tkey(dg));
+                }
+            }
+        }
+        const double di = (double)(sum ? cfl * Ai * fast::rcp(acc) : acc);
+        io.dt[c] = di;
+        kmin = kmin_(kmin, tkey(di));
+    }
+    return kmin;
+}
+
 // CFL time step of owned cell c (tile-local l) and of its boundary ghosts,
 // from staged records (stride NR) and edges (calc_dt of
 // examples/forwardStep/main.cpp:140-185 and examples/naca/main.cpp:142-183);
 // returns the ordered-key minimum of the values written.
-template <class M, int V, int NR>
+// VISC: the viscous kinds (dt_kind 3, 4) only, a separate instantiation so
+// that the CFL kinds keep their register budget.
+template <class M, int V, int NR, bool VISC = false>
 __device__ __forceinline__ unsigned long long tile_cell_dt(const TileParams& TP, const TileIO& io, const int4& inf,
                                                            int l, int c, const uint16_t* w,
                                                            const typename M::S* rec, const uint32_t* sij,
@@ -263,6 +388,8 @@ __device__ __forceinline__ unsigned long long tile_cell_dt(const TileParams& TP,
             const int o = side ? (int)(ij & 0xffff) : (int)(ij >> 16);
             io.dt[TP.halo[inf.z + o - T]] = P.dt_const;
         }
+    } else if (VISC) {
+        if (V == 4) kmin = tile_cell_dt_visc<M, NR>(TP, io, inf, l, c, w, rec, sij, snx, sny, sle);
     } else if (V == 4) {
         S qs[4];
         lds<S, 4>(rec + (size_t)l * NR, qs);
@@ -388,7 +515,7 @@ __device__ __forceinline__ void tile_dt_reduce(const TileParams& TP, const TileI
     }
 }
 
-template <class M, int V>
+template <class M, int V, bool VISC = false>
 __global__ void __launch_bounds__(kTileMax) k_tile_dt(TileParams TP, TileIO io) {
     using S = typename M::S;
     using R = Rec<M, V, false, false>;
@@ -415,14 +542,15 @@ __global__ void __launch_bounds__(kTileMax) k_tile_dt(TileParams TP, TileIO io) 
     cpa_wait();
     __syncthreads();
     unsigned long long kmin = ~0ull;
-    if (l < nown) kmin = tile_cell_dt<M, V, R::NR>(TP, io, inf, l, c0 + l, w, rec, sij, snx, sny, sle);
+    if (l < nown) kmin = tile_cell_dt<M, V, R::NR, VISC>(TP, io, inf, l, c0 + l, w, rec, sij, snx, sny, sle);
     if (P.global_dt && io.dtkeys != nullptr) tile_dt_reduce(TP, io, t, l, nown, kmin);
 }
 
 // ------------------------------------------------ K1: gradients + limiters --
 // DT: the first stage of a step also computes the step's time step here, from
-// the same staged state and edges (k_tile_dt's work without a second pass).
-template <class M, int V, bool DT>
+// the same staged state and edges (k_tile_dt's work without a second pass):
+// 0 none, 1 the CFL / constant kinds, 2 the viscous kinds.
+template <class M, int V, int DT>
 __global__ void __launch_bounds__(kTileMax) k_tile_gradlim(TileParams TP, TileIO io) {
     using S = typename M::S;
     using R = Rec<M, V, false, true>;
@@ -451,9 +579,9 @@ __global__ void __launch_bounds__(kTileMax) k_tile_gradlim(TileParams TP, TileIO
     stage_records<M, V, false, true>(TP, io, inf, c0, nown, rec);
     cpa_wait();
     __syncthreads();
-    if constexpr (DT) {
+    if constexpr (DT != 0) {
         unsigned long long kmin = ~0ull;
-        if (l < nown) kmin = tile_cell_dt<M, V, R::NR>(TP, io, inf, l, c, w, rec, sij, snx, sny, sle);
+        if (l < nown) kmin = tile_cell_dt<M, V, R::NR, DT == 2>(TP, io, inf, l, c, w, rec, sij, snx, sny, sle);
         if (P.global_dt && io.dtkeys != nullptr) tile_dt_reduce(TP, io, t, l, nown, kmin);
     }
     if (l >= nown) return;
@@ -566,11 +694,72 @@ __global__ void __launch_bounds__(kTileMax) k_tile_gradlim(TileParams TP, TileIO
                 }
             }
         }
-        // limited gradients
+        if (P.diffusive) {
+            // the face gradient of a diffusive flux needs the raw gradients:
+            // the limiter is stored apart, as in the exact mode
+            st<S, V>((S*)io.lim, c, lim);
+        } else {
+            // limited gradients
 #pragma unroll
-        for (int k = 0; k < V; ++k) { gx[k] *= lim[k]; gy[k] *= lim[k]; }
+            for (int k = 0; k < V; ++k) { gx[k] *= lim[k]; gy[k] *= lim[k]; }
+        }
         st<S, V>((S*)io.gx, c, gx);
         st<S, V>((S*)io.gy, c, gy);
+    }
+}
+
+// Navier-Stokes flux of one tile edge (FLUX 5) from the records of its two
+// cells (raw gradients and limiters staged apart in every mode): MUSCL face
+// states when P.order2, the corrected face gradient from the cell states, the
+// roe<false> flux minus the viscous terms.  Fast modes return f * le.
+template <class M, class R>
+__device__ __forceinline__ void ns_edge_flux(const Params& P, const typename M::S* ri, const typename M::S* rj,
+                                             typename M::S n0, typename M::S n1, typename M::S xf,
+                                             typename M::S yf, typename M::S le,
+                                             typename std::conditional<M::exact, double, typename M::S>::type* f) {
+    using S = typename M::S;
+    S qci[4], qcj[4], gxi[4], gyi[4], gxj[4], gyj[4], qL[4], qR[4];
+    lds<S, 4>(ri, qci); lds<S, 4>(rj, qcj);
+    lds<S, 4>(ri + R::OGX, gxi); lds<S, 4>(ri + R::OGY, gyi);
+    lds<S, 4>(rj + R::OGX, gxj); lds<S, 4>(rj + R::OGY, gyj);
+    const S cix = ri[R::OC], ciy = ri[R::OC + 1], cjx = rj[R::OC], cjy = rj[R::OC + 1];
+    if (P.order2) {
+        S li_[4], lj_[4];
+        lds<S, 4>(ri + R::OLM, li_); lds<S, 4>(rj + R::OLM, lj_);
+        const S di0 = xf - cix, di1 = yf - ciy, dj0 = xf - cjx, dj1 = yf - cjy;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            qL[k] = qci[k] + (gxi[k] * di0 + gyi[k] * di1) * li_[k];
+            qR[k] = qcj[k] + (gxj[k] * dj0 + gyj[k] * dj1) * lj_[k];
+        }
+        guard_face<S, 4>(P, qL, qci);
+        guard_face<S, 4>(P, qR, qcj);
+    } else {
+#pragma unroll
+        for (int k = 0; k < 4; ++k) { qL[k] = qci[k]; qR[k] = qcj[k]; }
+    }
+    if constexpr (M::exact) {
+        exact::roe<false>(P.gamma, f, qL, qR, n0, n1);
+        double gxf[4], gyf[4];
+        exact::face_gradient<4>(gxf, gyf, gxi, gyi, gxj, gyj, qci, qcj, cix, ciy, cjx, cjy);
+        exact::ns_viscous(P, f, qL, qR, gxf, gyf, n0, n1);
+    } else {
+        fast::roe<S>((S)P.gamma, f, qL, qR, n0, n1);
+        S t0 = cix - cjx, t1 = ciy - cjy;
+        const S rl = fast::rcp(fast::sqrt_(t0 * t0 + t1 * t1));
+        t0 *= rl;
+        t1 *= rl;
+        S gxf[4], gyf[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const S bx = S(0.5) * (gxi[k] + gxj[k]), by = S(0.5) * (gyi[k] + gyj[k]);
+            const S corr = bx * t0 + by * t1 - (qci[k] - qcj[k]) * rl;
+            gxf[k] = bx - corr * t0;
+            gyf[k] = by - corr * t1;
+        }
+        fast::ns_viscous<S>(P, f, qL, qR, gxf, gyf, n0, n1);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) f[k] *= le;
     }
 }
 
@@ -582,7 +771,9 @@ template <class M, int V, bool ORDER2, int FLUX>
 __global__ void __launch_bounds__(kTileMax) k_tile_stage(TileParams TP, TileIO io) {
     using S = typename M::S;
     using FT = typename std::conditional<M::exact, double, S>::type;  // flux storage
-    using R = Rec<M, V, ORDER2, ORDER2>;
+    // FLUX 5 (Navier-Stokes) keeps raw gradients and limiters apart in every mode
+    constexpr bool LIMREC = M::exact || FLUX == 5;
+    using R = Rec<M, V, ORDER2, ORDER2, LIMREC>;
     constexpr bool MUSCL = ORDER2 && FLUX != 4;
     pdl_trigger();
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -616,7 +807,9 @@ __global__ void __launch_bounds__(kTileMax) k_tile_stage(TileParams TP, TileIO i
         ld<double, V>(io.q_base, c, qb);
         if (!global_dt) dtc = io.dt[c];
     }
-    stage_records<M, V, ORDER2, ORDER2>(TP, io, inf, c0, nown, rec);
+    stage_records<M, V, ORDER2, ORDER2, LIMREC>(TP, io, inf, c0, nown, rec);
+    // MUSCL face states: FLUX 5 runs with and without them (P.order2)
+    const bool muscl = MUSCL && (FLUX != 5 || P.order2 != 0);
     // the tile's case (batches); -1: the tile spans two cases
     const int tc = (global_dt && P.n_cases > 1) ? P.tile_case[t] : 0;
     if (global_dt && tc >= 0 && threadIdx.x < 32) {
@@ -635,60 +828,64 @@ __global__ void __launch_bounds__(kTileMax) k_tile_stage(TileParams TP, TileIO i
         const S n0 = snx[el], n1 = sny[el];
         const S* ri = rec + (size_t)li * R::NR;
         const S* rj = rec + (size_t)lj * R::NR;
-        S qL[V], qR[V];
-        lds<S, V>(ri, qL);
-        lds<S, V>(rj, qR);
-        if (MUSCL) {
-            const S xf = sxf[el], yf = syf[el];
-            const S di0 = xf - ri[R::OC], di1 = yf - ri[R::OC + 1];
-            const S dj0 = xf - rj[R::OC], dj1 = yf - rj[R::OC + 1];
-            S gxi[V], gyi[V], gxj[V], gyj[V];
-            lds<S, V>(ri + R::OGX, gxi); lds<S, V>(ri + R::OGY, gyi);
-            lds<S, V>(rj + R::OGX, gxj); lds<S, V>(rj + R::OGY, gyj);
-            S ci[V], cj[V];
-#pragma unroll
-            for (int k = 0; k < V; ++k) { ci[k] = qL[k]; cj[k] = qR[k]; }
-            if constexpr (M::exact) {
-                S li_[V], lj_[V];
-                lds<S, V>(ri + R::OLM, li_); lds<S, V>(rj + R::OLM, lj_);
-#pragma unroll
-                for (int k = 0; k < V; ++k) {
-                    qL[k] = ci[k] + (gxi[k] * di0 + gyi[k] * di1) * li_[k];
-                    qR[k] = cj[k] + (gxj[k] * dj0 + gyj[k] * dj1) * lj_[k];
-                }
-            } else {
-#pragma unroll
-                for (int k = 0; k < V; ++k) {
-                    qL[k] = ci[k] + gxi[k] * di0 + gyi[k] * di1;
-                    qR[k] = cj[k] + gxj[k] * dj0 + gyj[k] * dj1;
-                }
-            }
-            guard_face<S, V>(P, qL, ci);
-            guard_face<S, V>(P, qR, cj);
-        }
         FT f[V];
-        if constexpr (FLUX == 4) {
-            S gxi[V], gyi[V], gxj[V], gyj[V];
-            lds<S, V>(ri + R::OGX, gxi); lds<S, V>(ri + R::OGY, gyi);
-            lds<S, V>(rj + R::OGX, gxj); lds<S, V>(rj + R::OGY, gyj);
-            if constexpr (M::exact) {
-                double gxf[V], gyf[V];
-                exact::face_gradient<V>(gxf, gyf, gxi, gyi, gxj, gyj, qL, qR, ri[R::OC], ri[R::OC + 1], rj[R::OC],
-                                        rj[R::OC + 1]);
-                exact::diffusion(f, gxf, gyf, n0, n1);
-            } else {
-                fast::diffusion<V, S>(f, gxi, gyi, gxj, gyj, qL, qR, ri[R::OC] - rj[R::OC],
-                                      ri[R::OC + 1] - rj[R::OC + 1], n0, n1);
-            }
-        } else if constexpr (M::exact) {
-            exact::flux<FLUX>(P.gamma, f, qL, qR, n0, n1);
+        if constexpr (FLUX == 5) {
+            ns_edge_flux<M, R>(P, ri, rj, n0, n1, sxf[el], syf[el], sle[el], f);
         } else {
-            fast::flux<FLUX, S>((S)P.gamma, f, qL, qR, n0, n1);
-        }
-        if constexpr (!M::exact) {
-            const S le = sle[el];
+            S qL[V], qR[V];
+            lds<S, V>(ri, qL);
+            lds<S, V>(rj, qR);
+            if (MUSCL) {
+                const S xf = sxf[el], yf = syf[el];
+                const S di0 = xf - ri[R::OC], di1 = yf - ri[R::OC + 1];
+                const S dj0 = xf - rj[R::OC], dj1 = yf - rj[R::OC + 1];
+                S gxi[V], gyi[V], gxj[V], gyj[V];
+                lds<S, V>(ri + R::OGX, gxi); lds<S, V>(ri + R::OGY, gyi);
+                lds<S, V>(rj + R::OGX, gxj); lds<S, V>(rj + R::OGY, gyj);
+                S ci[V], cj[V];
 #pragma unroll
-            for (int k = 0; k < V; ++k) f[k] *= le;
+                for (int k = 0; k < V; ++k) { ci[k] = qL[k]; cj[k] = qR[k]; }
+                if constexpr (M::exact) {
+                    S li_[V], lj_[V];
+                    lds<S, V>(ri + R::OLM, li_); lds<S, V>(rj + R::OLM, lj_);
+#pragma unroll
+                    for (int k = 0; k < V; ++k) {
+                        qL[k] = ci[k] + (gxi[k] * di0 + gyi[k] * di1) * li_[k];
+                        qR[k] = cj[k] + (gxj[k] * dj0 + gyj[k] * dj1) * lj_[k];
+                    }
+                } else {
+#pragma unroll
+                    for (int k = 0; k < V; ++k) {
+                        qL[k] = ci[k] + gxi[k] * di0 + gyi[k] * di1;
+                        qR[k] = cj[k] + gxj[k] * dj0 + gyj[k] * dj1;
+                    }
+                }
+                guard_face<S, V>(P, qL, ci);
+                guard_face<S, V>(P, qR, cj);
+            }
+            if constexpr (FLUX == 4) {
+                S gxi[V], gyi[V], gxj[V], gyj[V];
+                lds<S, V>(ri + R::OGX, gxi); lds<S, V>(ri + R::OGY, gyi);
+                lds<S, V>(rj + R::OGX, gxj); lds<S, V>(rj + R::OGY, gyj);
+                if constexpr (M::exact) {
+                    double gxf[V], gyf[V];
+                    exact::face_gradient<V>(gxf, gyf, gxi, gyi, gxj, gyj, qL, qR, ri[R::OC], ri[R::OC + 1], rj[R::OC],
+                                            rj[R::OC + 1]);
+                    exact::diffusion(f, gxf, gyf, n0, n1);
+                } else {
+                    fast::diffusion<V, S>(f, gxi, gyi, gxj, gyj, qL, qR, ri[R::OC] - rj[R::OC],
+                                          ri[R::OC + 1] - rj[R::OC + 1], n0, n1);
+                }
+            } else if constexpr (M::exact) {
+                exact::flux<FLUX>(P.gamma, f, qL, qR, n0, n1);
+            } else {
+                fast::flux<FLUX, S>((S)P.gamma, f, qL, qR, n0, n1);
+            }
+            if constexpr (!M::exact) {
+                const S le = sle[el];
+#pragma unroll
+                for (int k = 0; k < V; ++k) f[k] *= le;
+            }
         }
         if (V == 4 && sizeof(FT) == 4) {
             reinterpret_cast<float4*>(sF)[el] = make_float4((float)f[0], (float)f[1], (float)f[2], (float)f[3]);
@@ -777,11 +974,11 @@ __global__ void __launch_bounds__(kTileMax) k_tile_stage(TileParams TP, TileIO i
                 S qint[V], qc[V], b[V];
 #pragma unroll
                 for (int k = 0; k < V; ++k) { qc[k] = (S)qnew[k]; qint[k] = qc[k]; }
-                if (MUSCL) {
+                if (muscl) {
                     const S d0 = sxf[el] - rs[R::OC], d1 = syf[el] - rs[R::OC + 1];
                     S gxs[V], gys[V];
                     lds<S, V>(rs + R::OGX, gxs); lds<S, V>(rs + R::OGY, gys);
-                    if constexpr (M::exact) {
+                    if constexpr (LIMREC) {
                         S lms[V];
                         lds<S, V>(rs + R::OLM, lms);
 #pragma unroll
@@ -846,11 +1043,11 @@ inline size_t smem_gradlim(const TileParams& TP) {
     return (size_t)(TP.T + TP.max_halo) * Rec<M, V, false, true>::NR * sizeof(S) +
            (size_t)TP.max_edges * (6 * sizeof(S) + 4);
 }
-template <class M, int V, bool ORDER2>
+template <class M, int V, bool ORDER2, int FLUX = 0>
 inline size_t smem_stage(const TileParams& TP) {
     using S = typename M::S;
     using FT = typename std::conditional<M::exact, double, S>::type;
-    return (size_t)(TP.T + TP.max_halo) * Rec<M, V, ORDER2, ORDER2>::NR * sizeof(S) +
+    return (size_t)(TP.T + TP.max_halo) * Rec<M, V, ORDER2, ORDER2, M::exact || FLUX == 5>::NR * sizeof(S) +
            (size_t)TP.max_edges * (V * sizeof(FT) + 5 * sizeof(S) + 4);
 }
 
@@ -868,22 +1065,25 @@ struct TileLaunch {
         };
         if (TP.P.V == 4) {
             set((const void*)k_tile_dt<M, 4>, smem_dt<M, 4>(TP));
-            set((const void*)k_tile_gradlim<M, 4, false>, smem_gradlim<M, 4>(TP));
-            set((const void*)k_tile_gradlim<M, 4, true>, smem_gradlim<M, 4>(TP));
+            set((const void*)k_tile_dt<M, 4, true>, smem_dt<M, 4>(TP));
+            set((const void*)k_tile_gradlim<M, 4, 0>, smem_gradlim<M, 4>(TP));
+            set((const void*)k_tile_gradlim<M, 4, 1>, smem_gradlim<M, 4>(TP));
+            set((const void*)k_tile_gradlim<M, 4, 2>, smem_gradlim<M, 4>(TP));
             set((const void*)k_tile_stage<M, 4, true, 1>, smem_stage<M, 4, true>(TP));
             set((const void*)k_tile_stage<M, 4, false, 1>, smem_stage<M, 4, false>(TP));
             set((const void*)k_tile_stage<M, 4, true, 2>, smem_stage<M, 4, true>(TP));
             set((const void*)k_tile_stage<M, 4, false, 2>, smem_stage<M, 4, false>(TP));
+            set((const void*)k_tile_stage<M, 4, true, 5>, smem_stage<M, 4, true, 5>(TP));
         } else if (TP.P.V == 2) {
             set((const void*)k_tile_dt<M, 2>, smem_dt<M, 2>(TP));
-            set((const void*)k_tile_gradlim<M, 2, false>, smem_gradlim<M, 2>(TP));
-            set((const void*)k_tile_gradlim<M, 2, true>, smem_gradlim<M, 2>(TP));
+            set((const void*)k_tile_gradlim<M, 2, 0>, smem_gradlim<M, 2>(TP));
+            set((const void*)k_tile_gradlim<M, 2, 1>, smem_gradlim<M, 2>(TP));
             set((const void*)k_tile_stage<M, 2, true, 3>, smem_stage<M, 2, true>(TP));
             set((const void*)k_tile_stage<M, 2, false, 3>, smem_stage<M, 2, false>(TP));
         } else {
             set((const void*)k_tile_dt<M, 1>, smem_dt<M, 1>(TP));
-            set((const void*)k_tile_gradlim<M, 1, false>, smem_gradlim<M, 1>(TP));
-            set((const void*)k_tile_gradlim<M, 1, true>, smem_gradlim<M, 1>(TP));
+            set((const void*)k_tile_gradlim<M, 1, 0>, smem_gradlim<M, 1>(TP));
+            set((const void*)k_tile_gradlim<M, 1, 1>, smem_gradlim<M, 1>(TP));
             set((const void*)k_tile_stage<M, 1, true, 4>, smem_stage<M, 1, true>(TP));
         }
         return e;
@@ -909,22 +1109,30 @@ struct TileLaunch {
         cfg.numAttrs = 1;
         cudaLaunchKernelEx(&cfg, k, TP, io);
     }
+    static bool visc(const TileParams& TP) { return TP.P.V == 4 && TP.P.dt_kind >= 3; }
     static void dt(const TileParams& TP, const TileIO& io, cudaStream_t st, bool pdl = false) {
-        if (TP.P.V == 4) go(k_tile_dt<M, 4>, grid(TP), TP.T, smem_dt<M, 4>(TP), st, pdl, TP, io);
-        else if (TP.P.V == 2) go(k_tile_dt<M, 2>, grid(TP), TP.T, smem_dt<M, 2>(TP), st, pdl, TP, io);
-        else go(k_tile_dt<M, 1>, grid(TP), TP.T, smem_dt<M, 1>(TP), st, pdl, TP, io);
+        const int g = grid(TP);
+        if (TP.P.V == 4) {
+            if (visc(TP)) go(k_tile_dt<M, 4, true>, g, TP.T, smem_dt<M, 4>(TP), st, pdl, TP, io);
+            else go(k_tile_dt<M, 4>, g, TP.T, smem_dt<M, 4>(TP), st, pdl, TP, io);
+        } else if (TP.P.V == 2) {
+            go(k_tile_dt<M, 2>, g, TP.T, smem_dt<M, 2>(TP), st, pdl, TP, io);
+        } else {
+            go(k_tile_dt<M, 1>, g, TP.T, smem_dt<M, 1>(TP), st, pdl, TP, io);
+        }
     }
     static void gradlim(const TileParams& TP, const TileIO& io, cudaStream_t st, bool with_dt, bool pdl = false) {
         const int g = grid(TP);
         if (TP.P.V == 4) {
-            if (with_dt) go(k_tile_gradlim<M, 4, true>, g, TP.T, smem_gradlim<M, 4>(TP), st, pdl, TP, io);
-            else go(k_tile_gradlim<M, 4, false>, g, TP.T, smem_gradlim<M, 4>(TP), st, pdl, TP, io);
+            if (with_dt && visc(TP)) go(k_tile_gradlim<M, 4, 2>, g, TP.T, smem_gradlim<M, 4>(TP), st, pdl, TP, io);
+            else if (with_dt) go(k_tile_gradlim<M, 4, 1>, g, TP.T, smem_gradlim<M, 4>(TP), st, pdl, TP, io);
+            else go(k_tile_gradlim<M, 4, 0>, g, TP.T, smem_gradlim<M, 4>(TP), st, pdl, TP, io);
         } else if (TP.P.V == 2) {
-            if (with_dt) go(k_tile_gradlim<M, 2, true>, g, TP.T, smem_gradlim<M, 2>(TP), st, pdl, TP, io);
-            else go(k_tile_gradlim<M, 2, false>, g, TP.T, smem_gradlim<M, 2>(TP), st, pdl, TP, io);
+            if (with_dt) go(k_tile_gradlim<M, 2, 1>, g, TP.T, smem_gradlim<M, 2>(TP), st, pdl, TP, io);
+            else go(k_tile_gradlim<M, 2, 0>, g, TP.T, smem_gradlim<M, 2>(TP), st, pdl, TP, io);
         } else {
-            if (with_dt) go(k_tile_gradlim<M, 1, true>, g, TP.T, smem_gradlim<M, 1>(TP), st, pdl, TP, io);
-            else go(k_tile_gradlim<M, 1, false>, g, TP.T, smem_gradlim<M, 1>(TP), st, pdl, TP, io);
+            if (with_dt) go(k_tile_gradlim<M, 1, 1>, g, TP.T, smem_gradlim<M, 1>(TP), st, pdl, TP, io);
+            else go(k_tile_gradlim<M, 1, 0>, g, TP.T, smem_gradlim<M, 1>(TP), st, pdl, TP, io);
         }
     }
     static void stage(const TileParams& TP, const TileIO& io, cudaStream_t st, bool pdl = false) {
@@ -932,6 +1140,8 @@ struct TileLaunch {
         const bool o2 = TP.P.order2 != 0;
         if (TP.P.flux == 4) {
             go(k_tile_stage<M, 1, true, 4>, g, TP.T, smem_stage<M, 1, true>(TP), st, pdl, TP, io);
+        } else if (TP.P.flux == 5) {
+            go(k_tile_stage<M, 4, true, 5>, g, TP.T, smem_stage<M, 4, true, 5>(TP), st, pdl, TP, io);
         } else if (TP.P.flux == 3) {
             if (o2) go(k_tile_stage<M, 2, true, 3>, g, TP.T, smem_stage<M, 2, true>(TP), st, pdl, TP, io);
             else go(k_tile_stage<M, 2, false, 3>, g, TP.T, smem_stage<M, 2, false>(TP), st, pdl, TP, io);

@@ -92,6 +92,42 @@ def rect_tri(nx: int, ny: int, lx: float, ly: float, x0: float = 0.0, y0: float 
     return _finish(X.ravel(), Y.ravel(), cells, segs, groups, side_names)
 
 
+def _graded(n: int, ratio: float) -> np.ndarray:
+    """n + 1 points on [0, 1], cell sizes growing by `ratio` from 0 to 1."""
+    if n == 0:
+        return np.zeros(1)
+    w = ratio ** np.arange(n, dtype=np.float64)
+    return np.concatenate([[0.0], np.cumsum(w) / w.sum()])
+
+
+def flat_plate(nx0: int = 30, nx1: int = 90, ny: int = 110, x_lead: float = -0.1, lx: float = 1.0,
+               ly: float = 0.2, r_up: float = 1.2, r_plate: float = 1.1, r_y: float = 1.1) -> ElementMesh:
+    """Quadrilateral flat-plate mesh in the layout of examples/flatPlate/square.geo:
+    x in [x_lead, lx], y in [0, ly]; nx0 columns upstream of the leading edge
+    (x = 0) and nx1 along the plate, ny rows; cells shrink geometrically
+    toward the leading edge (ratios r_up, r_plate) and the wall (r_y).
+    Groups: top, bot0 (bottom, x < 0), bot1 (bottom, the plate), left, right."""
+    xu = x_lead * _graded(nx0, r_up)[::-1]          # x_lead .. 0, fine at 0
+    xp = lx * _graded(nx1, r_plate)                 # 0 .. lx, fine at 0
+    xs = np.concatenate([xu, xp[1:]])
+    ys = ly * _graded(ny, r_y)
+    nx = nx0 + nx1
+    X, Y = np.meshgrid(xs, ys)
+    nid = np.arange((nx + 1) * (ny + 1), dtype=np.int64).reshape(ny + 1, nx + 1)
+    cells = np.stack([nid[:-1, :-1].ravel(), nid[:-1, 1:].ravel(), nid[1:, 1:].ravel(),
+                      nid[1:, :-1].ravel()], 1)
+    bottom = np.stack([nid[0, :-1], nid[0, 1:]], 1)
+    top = np.stack([nid[-1, 1:], nid[-1, :-1]], 1)
+    left = np.stack([nid[1:, 0], nid[:-1, 0]], 1)
+    right = np.stack([nid[:-1, -1], nid[1:, -1]], 1)
+    segs = np.concatenate([top, bottom[:nx0], bottom[nx0:], left, right])
+    groups = np.concatenate([np.zeros(nx, np.int32), np.ones(nx0, np.int32), np.full(nx1, 2, np.int32),
+                             np.full(ny, 3, np.int32), np.full(ny, 4, np.int32)])
+    m = _finish(X.ravel(), Y.ravel(), cells, segs, groups, ["top", "bot0", "bot1", "left", "right"])
+    check_orientation(m)
+    return m
+
+
 def sod_strip(nx: int = 400, ny: int = 40, ly: float = 0.1) -> ElementMesh:
     """Sod shock tube domain [0,1]x[0,ly]: 'wall' top/bottom, 'ends' left/right."""
     return rect_tri(nx, ny, 1.0, ly)

@@ -10,16 +10,23 @@ examples define as device kinds, selected by name:
             same Roe-"cures" flux, central part associated differently),
             ``burgers`` (examples/burgers/main.cpp:68-96, V = 2),
             ``diffusion`` (examples/heatTransfer/main.cpp:63-73, V = 1: F = -grad T . n
-            with the face gradient of gradient_for_diffusion, explicit.cpp:70-109)
+            with the face gradient of gradient_for_diffusion, explicit.cpp:70-109),
+            ``ns`` (examples/flatPlate/main.cpp:126-225 = nacaTransient/main.cpp:130-229:
+            the roe_st flux minus viscous stresses and heat conduction from the face
+            gradient; constants mu, pr, cp, r)
 * limiter:  ``zero`` (shockTube/main.cpp:60-62), ``michalak``
             (forwardStep/main.cpp:57-66), ``minmod`` (burgers/main.cpp:51-53),
             ``venkat`` (Venkatakrishnan 1995, not in the reference)
 * dt:       ``cfl_sum`` (forwardStep/main.cpp:140-185), ``cfl_min_signed``
-            (naca/main.cpp:142-183), ``const`` (shockTube/main.cpp:140-147)
+            (naca/main.cpp:142-183), ``const`` (shockTube/main.cpp:140-147),
+            ``visc_min`` (flatPlate/main.cpp:230-277), ``visc_sum``
+            (nacaTransient/main.cpp:234-285)
 * bc:       ``copy`` (shockTube/main.cpp:158-163), ``wall``
             (forwardStep/main.cpp:262-269), ``inlet_outlet``
-            (forwardStep/main.cpp:194-261), ``farfield`` (naca/main.cpp:192-259);
-            the last two take the far-field state bv[4].
+            (forwardStep/main.cpp:194-261), ``farfield`` (naca/main.cpp:192-259),
+            ``farfield_b0`` (flatPlate/main.cpp:286-352: farfield with
+            b[2] = b[0]*(...)), ``noslip`` (flatPlate/main.cpp:361-366);
+            the inflow/far-field kinds take the far-field state bv[4].
 """
 from __future__ import annotations
 
@@ -50,6 +57,11 @@ class Physics:
     # gradient; with order2 off the gradients are computed without limiter
     # or interpolation (examples/heatTransfer/main.cpp:18-25)
     diffusive: bool = False
+    # consts:: of the Navier-Stokes examples (flatPlate/main.cpp:30-37)
+    mu: float = 0.0
+    pr: float = 1.0
+    cp: float = 1.0
+    r: float = 1.0
 
 
 def euler_state(rho, u, v, p, gamma=1.4):
@@ -105,6 +117,28 @@ def heat(dt=1e-5):
     """examples/heatTransfer/main.cpp: u_t = div(grad u), constant dt, zero-flux walls."""
     return Physics(V=1, flux="diffusion", order2=False, limiter="zero", dt_kind="const", dt_const=dt,
                    global_dt=True, diffusive=True, bcs={"wall": ("copy", None)})
+
+
+NS_CONSTS = dict(mu=2e-5, pr=0.72, cp=1.0, r=8.3145)   # flatPlate/main.cpp:30-37
+
+
+def flat_plate(cfl=2.0, mach=0.2):
+    """examples/flatPlate: laminar boundary layer, Navier-Stokes with MUSCL +
+    Michalak, local viscous dt (min form), far field / slip / no-slip walls."""
+    bv = forward_step_bv(mach)   # flatPlate/main.cpp:288-293, the same arithmetic
+    return Physics(V=4, flux="ns", order2=True, limiter="michalak", K=7.5, dt_kind="visc_min", cfl=cfl,
+                   global_dt=False, diffusive=True, **NS_CONSTS,
+                   bcs={"top": ("farfield_b0", bv), "bot0": ("wall", None), "bot1": ("noslip", None),
+                        "left": ("farfield_b0", bv), "right": ("farfield_b0", bv)})
+
+
+def naca_transient(cfl=1.5, mach=0.8):
+    """examples/nacaTransient: Navier-Stokes with cell values as face states
+    (gradients for the viscous terms only), global viscous dt (sum form)."""
+    bv = forward_step_bv(mach)   # nacaTransient/main.cpp:296-301
+    return Physics(V=4, flux="ns", order2=False, limiter="michalak", K=7.5, dt_kind="visc_sum", cfl=cfl,
+                   global_dt=True, diffusive=True, **NS_CONSTS,
+                   bcs={"wall": ("noslip", None), "farfield": ("farfield_b0", bv)})
 
 
 def burgers(dt=1e-4):

@@ -34,6 +34,18 @@ namespace solver {
 const double limiter_k_value = 7.5;
 }
 
+// The Navier-Stokes programs keep their constants in fvhyper::consts
+// (examples/flatPlate/main.cpp:30-37, nacaTransient/main.cpp:32-40).  Weak
+// references: they bind to the program's definitions and are null in
+// programs that define none; the kind they parameterise is still confirmed
+// bit for bit on probe states before it is used.
+namespace consts {
+extern double mu __attribute__((weak));
+extern double pr __attribute__((weak));
+extern double cp __attribute__((weak));
+extern double r __attribute__((weak));
+}  // namespace consts
+
 mpi_wrapper::mpi_wrapper() : rank(0), size(1) {}
 int mpi_wrapper::exit() { return 0; }
 
@@ -182,37 +194,65 @@ struct Probe {
 const char* flux_name(int k) {
     return k == FV_FLUX_ROE_FS ? "roe (forwardStep operand order)"
            : k == FV_FLUX_ROE_ST ? "roe (shockTube/naca operand order)"
-           : k == FV_FLUX_DIFFUSION ? "diffusion" : "upwind advection";
+           : k == FV_FLUX_DIFFUSION ? "diffusion"
+           : k == FV_FLUX_NS ? "navier-stokes" : "upwind advection";
 }
 
-// calc_flux -> (kind, gamma).  gamma from a fluid at rest (f[1] = p = gamma-1
-// for q = (1, 0, 0, 1), n = (1, 0)), then 256 random state pairs must agree
-// bit for bit.
-void identify_flux(int V, bool diffusive, int32_t* kind, double* gamma) {
+// gamma of an Euler-type calc_flux from a fluid at rest: f[1] = p = gamma-1
+// for q = (1, 0, 0, 1), n = (1, 0), zero face gradients.
+double rest_state_gamma() {
+    double zg[4] = {0, 0, 0, 0}, q0[4] = {1.0, 0.0, 0.0, 1.0}, n0[2] = {1.0, 0.0}, f0[4] = {0, 0, 0, 0};
+    calc_flux(f0, q0, q0, zg, zg, n0);
+    const double g = f0[1] + 1.0;
+    if (!(g > 1.0 && g <= 3.0))
+        throw std::invalid_argument("fvhyper GPU: calc_flux is not an Euler flux (rest-state pressure test)");
+    return g;
+}
+
+// A calc_flux that reads the face gradient (diffusive_gradients) -> the
+// diffusion kind (vars = 1) or the Navier-Stokes kind (vars = 4, constants
+// from fvhyper::consts); 256 random states and face gradients must agree
+// bit for bit with the kind's host copy.
+void identify_diffusive_flux(int V, fv_physics* ph) {
+    if (V == 1) {
+        ph->flux = FV_FLUX_DIFFUSION;
+        ph->gamma = 1.4;
+    } else if (V == 4) {
+        if (!&consts::mu || !&consts::pr || !&consts::cp || !&consts::r)
+            throw std::invalid_argument("fvhyper GPU: a vars = 4 calc_flux with diffusive_gradients runs as the "
+                                        "Navier-Stokes kind, whose constants are read from fvhyper::consts::mu, "
+                                        "pr, cp and r; the program defines no such constants");
+        ph->flux = FV_FLUX_NS;
+        ph->gamma = rest_state_gamma();
+        ph->mu = consts::mu; ph->pr = consts::pr; ph->cp = consts::cp; ph->r = consts::r;
+    } else {
+        throw std::invalid_argument("fvhyper GPU: diffusive_gradients with vars = " + std::to_string(V) +
+                                    " matches no device kind (vars = 1 diffusion, vars = 4 Navier-Stokes)");
+    }
+    Probe pr;
+    for (int t = 0; t < 256; ++t) {
+        double qi[4] = {0, 0, 0, 0}, qj[4] = {0, 0, 0, 0}, gx[4], gy[4], n[2];
+        if (V == 4) { pr.euler(qi, ph->gamma); pr.euler(qj, ph->gamma); }
+        else { qi[0] = pr.uni(-2, 2); qj[0] = pr.uni(-2, 2); }
+        for (int k = 0; k < 4; ++k) { gx[k] = pr.uni(-5, 5); gy[k] = pr.uni(-5, 5); }
+        pr.normal(n);
+        double fu[4] = {0, 0, 0, 0}, fk[4] = {0, 0, 0, 0};
+        calc_flux(fu, qi, qj, gx, gy, n);
+        fv_kind_flux_grad(ph, qi, qj, gx, gy, n, fk);
+        for (int c = 0; c < V; ++c)
+            if (!same_bits(fu[c], fk[c]))
+                throw std::invalid_argument(std::string("fvhyper GPU: calc_flux (diffusive_gradients) is not the ") +
+                                            (V == 1 ? "diffusion flux -grad(u).n of examples/heatTransfer"
+                                                    : "Navier-Stokes flux of examples/flatPlate") +
+                                            "; no device kind matches it");
+    }
+}
+
+// calc_flux -> (kind, gamma).  gamma from the rest state, then 256 random
+// state pairs must agree bit for bit.
+void identify_flux(int V, int32_t* kind, double* gamma) {
     double zg[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     Probe pr;
-    if (diffusive) {
-        // the only diffusive device kind: F = -grad(u) . n of the face gradient
-        if (V != 1)
-            throw std::invalid_argument("fvhyper GPU: diffusive_gradients with vars = " + std::to_string(V) +
-                                        " (viscous fluxes) is not on the device path; the device's diffusive "
-                                        "kind is the vars = 1 diffusion flux of examples/heatTransfer");
-        for (int t = 0; t < 256; ++t) {
-            double qi[1] = {pr.uni(-2, 2)}, qj[1] = {pr.uni(-2, 2)}, gx[1] = {pr.uni(-5, 5)},
-                   gy[1] = {pr.uni(-5, 5)}, n[2];
-            pr.normal(n);
-            double fu[1] = {0}, fk[1] = {0};
-            calc_flux(fu, qi, qj, gx, gy, n);
-            fv_kind_flux_grad(FV_FLUX_DIFFUSION, 0.0, qi, qj, gx, gy, n, fk);
-            if (!same_bits(fu[0], fk[0]))
-                throw std::invalid_argument("fvhyper GPU: calc_flux (vars = 1, diffusive_gradients) is not the "
-                                            "diffusion flux -grad(u).n of examples/heatTransfer; no device kind "
-                                            "matches it");
-        }
-        *kind = FV_FLUX_DIFFUSION;
-        *gamma = 1.4;
-        return;
-    }
     if (V == 1)
         throw std::invalid_argument("fvhyper GPU: vars = 1 runs the diffusion kind only (diffusive_gradients)");
     if (V == 2) {
@@ -231,11 +271,7 @@ void identify_flux(int V, bool diffusive, int32_t* kind, double* gamma) {
         return;
     }
     if (V != 4) throw std::invalid_argument("fvhyper GPU: vars must be 1, 2 or 4");
-    double q0[4] = {1.0, 0.0, 0.0, 1.0}, n0[2] = {1.0, 0.0}, f0[4] = {0, 0, 0, 0};
-    calc_flux(f0, q0, q0, zg, zg, n0);
-    const double g = f0[1] + 1.0;
-    if (!(g > 1.0 && g <= 3.0))
-        throw std::invalid_argument("fvhyper GPU: calc_flux is not an Euler flux (rest-state pressure test)");
+    const double g = rest_state_gamma();
     for (int k : {FV_FLUX_ROE_FS, FV_FLUX_ROE_ST}) {
         Probe p2;
         bool ok = true;
@@ -284,6 +320,7 @@ void identify_bc(const std::string& name, void (*fn)(double*, double*, double*),
     std::vector<int> kinds = {FV_BC_COPY};
     if (V == 4) {
         kinds.push_back(FV_BC_WALL);
+        kinds.push_back(FV_BC_NOSLIP);
         double q[4], n[2] = {0.6, 0.8};
         const double u = -3.0;
         q[0] = 1.0; q[1] = u * n[0]; q[2] = u * n[1];
@@ -291,7 +328,11 @@ void identify_bc(const std::string& name, void (*fn)(double*, double*, double*),
         double b[4] = {0, 0, 0, 0};
         fn(b, q, n);
         for (int k = 0; k < 4; ++k) bv[k] = b[k];
-        if (b[0] > 0.0) { kinds.push_back(FV_BC_INLET_OUTLET); kinds.push_back(FV_BC_FARFIELD); }
+        if (b[0] > 0.0) {
+            kinds.push_back(FV_BC_INLET_OUTLET);
+            kinds.push_back(FV_BC_FARFIELD);
+            kinds.push_back(FV_BC_FARFIELD_B0);
+        }
     } else {
         for (int k = 0; k < 4; ++k) bv[k] = 0.0;
     }
@@ -311,13 +352,14 @@ void identify_bc(const std::string& name, void (*fn)(double*, double*, double*),
         }
         if (ok) {
             *kind = k;
-            if (k == FV_BC_COPY || k == FV_BC_WALL)
+            if (k == FV_BC_COPY || k == FV_BC_WALL || k == FV_BC_NOSLIP)
                 for (int c = 0; c < 4; ++c) bv[c] = 0.0;
             return;
         }
     }
     throw std::invalid_argument("fvhyper GPU: boundary function \"" + name +
-                                "\" matches no device boundary kind (copy, wall, inlet_outlet, farfield)");
+                                "\" matches no device boundary kind (copy, wall, no-slip wall, inlet_outlet, "
+                                "farfield, farfield with b[0] tangential momentum)");
 }
 
 // A small jittered triangle mesh for probing calc_dt (the user function only
@@ -425,7 +467,9 @@ void identify_dt(fv_physics ph, int device, int32_t* dt_kind, double* cfl, doubl
         std::vector<double> qq(q);
         check(fv_stage_dt(h.s, qq.data(), out.data(), 0), "fv_stage_dt (probe)");
     };
-    for (int32_t kind : {FV_DT_CFL_SUM, FV_DT_CFL_MIN_SIGNED}) {
+    std::vector<int32_t> kinds = {FV_DT_CFL_SUM, FV_DT_CFL_MIN_SIGNED};
+    if (ph.flux == FV_FLUX_NS) kinds = {FV_DT_VISC_MIN, FV_DT_VISC_SUM, FV_DT_CFL_SUM, FV_DT_CFL_MIN_SIGNED};
+    for (int32_t kind : kinds) {
         std::vector<double> d1;
         device_dt(kind, 1.0, d1);
         double ratio = 0.0;
@@ -447,7 +491,8 @@ void identify_dt(fv_physics ph, int device, int32_t* dt_kind, double* cfl, doubl
         }
     }
     throw std::invalid_argument("fvhyper GPU: calc_dt matches no device time-step kind (constant, CFL over the "
-                                "edge sum as examples/forwardStep, CFL edge minimum as examples/naca)");
+                                "edge sum as examples/forwardStep, CFL edge minimum as examples/naca, viscous "
+                                "minimum as examples/flatPlate, viscous sum as examples/nacaTransient)");
 }
 
 struct PrintCtx {
@@ -487,17 +532,14 @@ void run(const std::string name, std::vector<double>& q, mpi_wrapper& pool, mesh
     if (solver::smooth_residuals)
         throw std::invalid_argument("fvhyper GPU: smooth_residuals is not on the device path");
     const bool D = solver::diffusive_gradients;
-    const bool o2 = solver::do_calc_gradients && solver::do_calc_limiters && solver::linear_interpolate && !D;
+    const bool o2 = solver::do_calc_gradients && solver::do_calc_limiters && solver::linear_interpolate;
     const bool o1 = !solver::do_calc_gradients && !solver::do_calc_limiters && !solver::linear_interpolate && !D;
-    // diffusion: gradients for the face gradient, cell values as face states
+    // gradients for the viscous face gradient only, cell values as face states
     const bool dg = solver::do_calc_gradients && !solver::do_calc_limiters && !solver::linear_interpolate && D;
-    if (D && V != 1)
-        throw std::invalid_argument("fvhyper GPU: diffusive_gradients with vars = " + std::to_string(V) +
-                                    " (viscous fluxes) is not on the device path");
     if (!o1 && !o2 && !dg)
         throw std::invalid_argument("fvhyper GPU: the device runs first order (no gradients, limiters or "
-                                    "interpolation), second order (all three) or diffusion (gradients and "
-                                    "diffusive_gradients only); this flag mix is none of them");
+                                    "interpolation), second order (all three) or gradients for the diffusive "
+                                    "fluxes alone (with diffusive_gradients); this flag mix is none of them");
 
     const int precision = choose_precision(opt.precision);
     const int device = choose_device(opt.device);
@@ -505,9 +547,10 @@ void run(const std::string name, std::vector<double>& q, mpi_wrapper& pool, mesh
     fv_physics ph;
     std::memset(&ph, 0, sizeof(ph));
     ph.V = V;
-    identify_flux(V, dg, &ph.flux, &ph.gamma);
+    if (D) identify_diffusive_flux(V, &ph);
+    else identify_flux(V, &ph.flux, &ph.gamma);
     ph.order2 = o2 ? 1 : 0;
-    ph.diffusive = dg ? 1 : 0;
+    ph.diffusive = D ? 1 : 0;
     ph.limiter = o2 ? identify_limiter() : FV_LIM_ZERO;
     ph.K = solver::limiter_k_value;
     ph.global_dt = solver::global_dt ? 1 : 0;

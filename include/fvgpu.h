@@ -44,16 +44,28 @@ typedef enum {
 } fv_status;
 
 /* Physics kinds implemented on the device (see finite-volume-2d-cpp_b200/physics.py). */
-enum { FV_FLUX_ROE_FS = 1, FV_FLUX_ROE_ST = 2, FV_FLUX_BURGERS = 3, FV_FLUX_DIFFUSION = 4 };
+/* FV_FLUX_NS: the compressible Navier-Stokes flux of examples/flatPlate and
+ * examples/nacaTransient (FV_FLUX_ROE_ST minus the viscous stresses and heat
+ * conduction from the face gradient; mu, pr, cp, r below). */
+enum { FV_FLUX_ROE_FS = 1, FV_FLUX_ROE_ST = 2, FV_FLUX_BURGERS = 3, FV_FLUX_DIFFUSION = 4, FV_FLUX_NS = 5 };
 enum { FV_LIM_ZERO = 0, FV_LIM_MICHALAK = 1, FV_LIM_VENKAT = 2, FV_LIM_MINMOD = 3 };
-enum { FV_DT_CONST = 0, FV_DT_CFL_SUM = 1, FV_DT_CFL_MIN_SIGNED = 2 };
-enum { FV_BC_COPY = 0, FV_BC_WALL = 1, FV_BC_INLET_OUTLET = 2, FV_BC_FARFIELD = 3 };
+/* VISC_MIN (examples/flatPlate/main.cpp:230-277) and VISC_SUM
+ * (examples/nacaTransient/main.cpp:234-285): convective + 2 x viscous
+ * eigenvalue, min over faces from 1 or summed over faces. */
+enum { FV_DT_CONST = 0, FV_DT_CFL_SUM = 1, FV_DT_CFL_MIN_SIGNED = 2, FV_DT_VISC_MIN = 3, FV_DT_VISC_SUM = 4 };
+/* NOSLIP: b = (rho, -rho u, -rho v, rho E) (examples/flatPlate/main.cpp:361-366).
+ * FARFIELD_B0: FARFIELD with b[2] = b[0]*(...) in the subsonic branches
+ * (examples/flatPlate/main.cpp:286-352, nacaTransient/main.cpp:294-360). */
+enum { FV_BC_COPY = 0, FV_BC_WALL = 1, FV_BC_INLET_OUTLET = 2, FV_BC_FARFIELD = 3, FV_BC_NOSLIP = 4,
+       FV_BC_FARFIELD_B0 = 5 };
 
 /* Arithmetic of the step.
  * FP64_EXACT: FP64, the reference's evaluation order, no FMA contraction:
  *             bit-identical to the reference CPU solver.
  * FP64:       FP64 with fused multiply-adds and reciprocal reuse
- *             (<= 1e-12 relative per step against the reference).
+ *             (<= 1e-12 relative per step against the reference; up to
+ *             5e-12 where the residual is a few per cent of the face
+ *             fluxes, as in the near-uniform flat-plate flow).
  * FP32:       FP32 bulk flux/gradient/limiter arithmetic; FP64 conserved
  *             state, RK accumulation, residual and force sums. */
 enum { FV_PREC_FP64_EXACT = 0, FV_PREC_FP64 = 1, FV_PREC_FP32 = 2 };
@@ -79,7 +91,9 @@ typedef struct {
                                   gradients (no limiter when order2 = 0) and the flux gets
                                   the corrected face gradient of explicit.cpp:70-109.  Used
                                   by FV_FLUX_DIFFUSION (V = 1, order2 = 0, constant dt,
-                                  copy boundaries: examples/heatTransfer) */
+                                  copy boundaries: examples/heatTransfer) and FV_FLUX_NS */
+    double mu, pr, cp, r;      /* viscosity, Prandtl number, heat capacity, gas constant of
+                                  FV_FLUX_NS and the viscous dt kinds (the examples' consts::) */
 } fv_physics;
 
 typedef struct {
@@ -276,8 +290,8 @@ int fv_kind_flux(int32_t flux, double gamma, const double* qi, const double* qj,
                  double* f);
 /* calc_flux with its face gradient arguments (explicit.h:71-78): gx, gy are
  * the [V] face gradients the reference passes; the non-diffusive kinds
- * ignore them.  V = 1 for FV_FLUX_DIFFUSION. */
-int fv_kind_flux_grad(int32_t flux, double gamma, const double* qi, const double* qj, const double* gx,
+ * ignore them.  Reads ph->flux, V, gamma and (FV_FLUX_NS) mu, pr, cp, r. */
+int fv_kind_flux_grad(const fv_physics* ph, const double* qi, const double* qj, const double* gx,
                       const double* gy, const double* n, double* f);
 /* gradient_for_diffusion (explicit.cpp:70-109): the corrected face gradient
  * [V] from the cell gradients, cell states and centroids ci, cj ([2] each). */

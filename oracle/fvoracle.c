@@ -217,11 +217,68 @@ void fvo_flux(const fvo_physics* ph, double* f, const double* qi, const double* 
     else roe(ph->gamma, ph->flux == FVO_FLUX_ROE_FS, f, qi, qj, n);
 }
 
+static void ns_viscous(const fvo_physics* ph, double* f, const double* qi, const double* qj,
+                       const double* gx, const double* gy, const double* n);
+
+/* calc_flux with the face gradient it receives (explicit.cpp:342): the
+ * diffusion and Navier-Stokes kinds read it, the others ignore it. */
+void fvo_flux_grad(const fvo_physics* ph, double* f, const double* qi, const double* qj, const double* gx,
+                   const double* gy, const double* n) {
+    if (ph->flux == FVO_FLUX_DIFFUSION) {
+        f[0] = -(gx[0] * n[0] + gy[0] * n[1]);
+    } else if (ph->flux == FVO_FLUX_NS) {
+        roe(ph->gamma, 0, f, qi, qj, n);
+        ns_viscous(ph, f, qi, qj, gx, gy, n);
+    } else {
+        fvo_flux(ph, f, qi, qj, n);
+    }
+}
+
+/* Viscous part of the Navier-Stokes flux, examples/flatPlate/main.cpp:193-224
+ * (= nacaTransient/main.cpp:197-228) with its helpers calc_p, calc_grad_p,
+ * calc_grad_t, calc_grad_u, calc_grad_v (flatPlate/main.cpp:38-92): stresses
+ * and heat flux at the mean of the two face states, from the face gradient
+ * (gx, gy); subtracted from the Roe flux f. */
+static void ns_viscous(const fvo_physics* ph, double* f, const double* qi, const double* qj,
+                       const double* gx, const double* gy, const double* n) {
+    const double gamma = ph->gamma, mu = ph->mu;
+    double q[4];
+    for (int i = 0; i < 4; ++i) q[i] = 0.5 * (qi[i] + qj[i]);
+    const double p = (gamma - 1) * (q[3] - 0.5 / q[0] * (q[1] * q[1] + q[2] * q[2]));
+    double gp0 = 2. * gx[3];
+    gp0 -= gx[1] * q[1] / q[0] + q[1] * (gx[1] * q[0] - gx[0] * q[1]) / (q[0] * q[0]);
+    gp0 -= gx[2] * q[2] / q[0] + q[2] * (gx[2] * q[0] - gx[0] * q[2]) / (q[0] * q[0]);
+    gp0 *= 0.5 * (gamma - 1);
+    double gp1 = 2. * gy[3];
+    gp1 -= gy[1] * q[1] / q[0] + q[1] * (gy[1] * q[0] - gy[0] * q[1]) / (q[0] * q[0]);
+    gp1 -= gy[2] * q[2] / q[0] + q[2] * (gy[2] * q[0] - gy[0] * q[2]) / (q[0] * q[0]);
+    gp1 *= 0.5 * (gamma - 1);
+    const double gt0 = (1. / ph->r) * ((gp0 * q[0] - gx[0] * p) / (q[0] * q[0]));
+    const double gt1 = (1. / ph->r) * ((gp1 * q[0] - gy[0] * p) / (q[0] * q[0]));
+    const double gu0 = (q[0] * gx[1] - q[1] * gx[0]) / (q[0] * q[0]);
+    const double gu1 = (q[0] * gy[1] - q[1] * gy[0]) / (q[0] * q[0]);
+    const double gv0 = (q[0] * gx[2] - q[2] * gx[0]) / (q[0] * q[0]);
+    const double gv1 = (q[0] * gy[2] - q[2] * gy[0]) / (q[0] * q[0]);
+    const double div_v = gu0 + gv1;
+    const double tau_xx = 2. * mu * (gu0 - div_v / 3.);
+    const double tau_yy = 2. * mu * (gv1 - div_v / 3.);
+    const double tau_xy = mu * (gu1 + gv0);
+    const double k = ph->cp * mu / ph->pr;
+    const double phi0 = q[1] / q[0] * tau_xx + q[2] / q[0] * tau_xy + k * gt0;
+    const double phi1 = q[1] / q[0] * tau_xy + q[2] / q[0] * tau_yy + k * gt1;
+    f[1] -= n[0] * tau_xx + n[1] * tau_xy;
+    f[2] -= n[0] * tau_xy + n[1] * tau_yy;
+    f[3] -= n[0] * phi0 + n[1] * phi1;
+}
+
 /* Boundary conditions.  COPY: examples/shockTube/main.cpp:158-163.  WALL:
  * examples/forwardStep/main.cpp:262-269.  INLET_OUTLET:
  * examples/forwardStep/main.cpp:194-261.  FARFIELD: examples/naca/main.cpp:
  * 192-259.  The subsonic outlet branches keep the reference's
- * b[2] = b[1]*(...) (forwardStep/main.cpp:257, naca/main.cpp:255). */
+ * b[2] = b[1]*(...) (forwardStep/main.cpp:257, naca/main.cpp:255).
+ * NOSLIP: examples/flatPlate/main.cpp:361-366.  FARFIELD_B0:
+ * examples/flatPlate/main.cpp:286-352 (= nacaTransient/main.cpp:294-360),
+ * FARFIELD with b[2] = b[0]*(...) in both subsonic branches. */
 static void bc_state(const fvo_physics* ph, int group, const double* bv, double* b, const double* q,
                      const double* n);
 
@@ -245,6 +302,14 @@ static void bc_state(const fvo_physics* ph, int group, const double* bv, double*
         b[3] = q[3];
         return;
     }
+    if (kind == FVO_BC_NOSLIP) {
+        b[0] = q[0];
+        b[1] = -q[1];
+        b[2] = -q[2];
+        b[3] = q[3];
+        return;
+    }
+    const int b0 = kind == FVO_BC_FARFIELD_B0;  /* tangential momentum from b[0] */
     double U0 = q[1] / q[0], U1 = q[2] / q[0];
     double u_norm = sqrt(U0 * U0 + U1 * U1);
     double u_dot_n = U0 * n[0] + U1 * n[1];
@@ -269,14 +334,14 @@ static void bc_state(const fvo_physics* ph, int group, const double* bv, double*
             double pb = 0.5 * (pa + pd - rho0 * c0 * (n[0] * (ua - ud) + n[1] * (va - vd)));
             b[0] = rhoa + (pb - pa) / (c0 * c0);
             b[1] = b[0] * (ua - n[0] * (pa - pb) / (rho0 * c0));
-            b[2] = b[1] * (va - n[1] * (pa - pb) / (rho0 * c0));
+            b[2] = b[b0 ? 0 : 1] * (va - n[1] * (pa - pb) / (rho0 * c0));
             b[3] = pb / (gamma - 1) + 0.5 / b[0] * (b[1] * b[1] + b[2] * b[2]);
         }
     } else {
         double pb = pa;
         b[0] = rhod + (pb - pd) / (c0 * c0);
         b[1] = b[0] * (ud + n[0] * (pd - pb) / (rho0 * c0));
-        b[2] = b[1] * (va + n[1] * (pd - pb) / (rho0 * c0));
+        b[2] = b[b0 ? 0 : 1] * (va + n[1] * (pd - pb) / (rho0 * c0));
         b[3] = pb / (gamma - 1.) + 0.5 / b[0] * (b[1] * b[1] + b[2] * b[2]);
     }
     (void)rhoa;
@@ -302,6 +367,42 @@ double fvo_limiter_func(const fvo_physics* ph, double y) {
 }
 
 /* ------------------------------------------------------------ stages -- */
+/* Viscous time steps (C = 2).  VISC_MIN: examples/flatPlate/main.cpp:230-277,
+ * dt = min over faces of cfl A / (convective + C viscous eigenvalue), from 1.
+ * VISC_SUM: examples/nacaTransient/main.cpp:234-285, dt = cfl A / sum over
+ * faces of le * max of the two sides' (convective + C viscous) eigenvalues. */
+static void calc_dt_viscous(const fvo_mesh* m, const fvo_physics* ph, const double* q, double* dt) {
+    const double gamma = ph->gamma, gm1 = gamma - 1, cfl = ph->cfl, C = 2;
+    const int sum = ph->dt_kind == FVO_DT_VISC_SUM;
+    for (int64_t i = 0; i < m->n_total; ++i) dt[i] = sum ? 0. : 1.0;
+    for (int64_t e = 0; e < m->n_edges; ++e) {
+        uint32_t i = m->edge_cells[2 * e], j = m->edge_cells[2 * e + 1];
+        double le = m->elen[e], n0 = m->enx[e], n1 = m->eny[e];
+        const double* qi = q + 4 * (size_t)i;
+        const double* qj = q + 4 * (size_t)j;
+        double ci = sqrt(pres(gm1, qi) * gamma / qi[0]);
+        double cj = sqrt(pres(gm1, qj) * gamma / qj[0]);
+        double eig_vi = dmax(4. / (3. * qi[0]), gamma / qi[0]) * (ph->mu / ph->pr) * le * le / m->area[i];
+        double eig_vj = dmax(4. / (3. * qj[0]), gamma / qj[0]) * (ph->mu / ph->pr) * le * le / m->area[j];
+        if (sum) {
+            double eig_ci = ci + fabs(qi[1] / qi[0] * n0 + qi[2] / qi[0] * n1);
+            double eig_cj = cj + fabs(qj[1] / qj[0] * n0 + qj[2] / qj[0] * n1);
+            double center = dmax(eig_ci + C * eig_vi, eig_cj + C * eig_vj);
+            dt[i] += center * le;
+            dt[j] += center * le;
+        } else {
+            double eig_ci = (ci + fabs(n0 * qi[1] / qi[0]) + fabs(n1 * qi[2] / qi[0])) * le;
+            double eig_cj = (cj + fabs(n0 * qj[1] / qj[0]) + fabs(n1 * qj[2] / qj[0])) * le;
+            double dti = cfl * m->area[i] / (eig_ci + C * eig_vi);
+            double dtj = cfl * m->area[j] / (eig_cj + C * eig_vj);
+            dt[i] = dmin(dt[i], dti);
+            dt[j] = dmin(dt[j], dtj);
+        }
+    }
+    if (sum)
+        for (int64_t i = 0; i < m->n_total; ++i) dt[i] = cfl * m->area[i] / dt[i];
+}
+
 /* Time step kinds.  CFL_SUM: examples/forwardStep/main.cpp:140-185.
  * CFL_MIN_SIGNED: examples/naca/main.cpp:142-183.  CONST:
  * examples/shockTube/main.cpp:140-147.  dt is one value per cell (the
@@ -311,6 +412,10 @@ void fvo_calc_dt(const fvo_mesh* m, const fvo_physics* ph, const double* q, doub
     const double gamma = ph->gamma, gm1 = gamma - 1;
     if (ph->dt_kind == FVO_DT_CONST) {
         for (int64_t i = 0; i < m->n_total; ++i) dt[i] = ph->dt_const;
+        return;
+    }
+    if (ph->dt_kind == FVO_DT_VISC_MIN || ph->dt_kind == FVO_DT_VISC_SUM) {
+        calc_dt_viscous(m, ph, q, dt);
         return;
     }
     const int sum = ph->dt_kind == FVO_DT_CFL_SUM;
@@ -490,11 +595,10 @@ void fvo_calc_time_derivatives(const fvo_mesh* m, const fvo_physics* ph, const d
             face_gradient(V, gxf, gyf, gx + (size_t)V * i, gy + (size_t)V * i, gx + (size_t)V * j,
                           gy + (size_t)V * j, q + (size_t)V * i, q + (size_t)V * j, ci, cj);
         }
-        if (ph->flux == FVO_FLUX_DIFFUSION) {
-            f[0] = -(gxf[0] * n[0] + gyf[0] * n[1]);  /* examples/heatTransfer/main.cpp:63-73 */
-        } else {
-            fvo_flux(ph, f, qi, qj, n);
-        }
+        if (!ph->diffusive)  /* gxv = gyv = 0, explicit.cpp:332-337 */
+            for (int k = 0; k < V; ++k) { gxf[k] = 0.; gyf[k] = 0.; }
+        /* examples/heatTransfer/main.cpp:63-73, flatPlate/main.cpp:126-225 */
+        fvo_flux_grad(ph, f, qi, qj, gxf, gyf, n);
         for (int k = 0; k < V; ++k) {
             qt[(size_t)V * i + k] -= f[k] * le / m->area[i];
             qt[(size_t)V * j + k] += f[k] * le / m->area[j];

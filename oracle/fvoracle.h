@@ -31,11 +31,22 @@ typedef struct {
 } fvo_mesh;
 
 /* DIFFUSION: the heat-equation flux F = -(grad T . n) of examples/heatTransfer
-   (V = 1), with the face gradient of gradient_for_diffusion. */
-enum { FVO_FLUX_ROE_FS = 1, FVO_FLUX_ROE_ST = 2, FVO_FLUX_BURGERS = 3, FVO_FLUX_DIFFUSION = 4 };
+   (V = 1), with the face gradient of gradient_for_diffusion.  NS: the
+   compressible Navier-Stokes flux of examples/flatPlate and
+   examples/nacaTransient (the shockTube Roe flux plus viscous stresses and
+   heat conduction from the face gradient). */
+enum { FVO_FLUX_ROE_FS = 1, FVO_FLUX_ROE_ST = 2, FVO_FLUX_BURGERS = 3, FVO_FLUX_DIFFUSION = 4,
+       FVO_FLUX_NS = 5 };
 enum { FVO_LIM_ZERO = 0, FVO_LIM_MICHALAK = 1, FVO_LIM_VENKAT = 2, FVO_LIM_MINMOD = 3 };
-enum { FVO_DT_CONST = 0, FVO_DT_CFL_SUM = 1, FVO_DT_CFL_MIN_SIGNED = 2 };
-enum { FVO_BC_COPY = 0, FVO_BC_WALL = 1, FVO_BC_INLET_OUTLET = 2, FVO_BC_FARFIELD = 3 };
+/* VISC_MIN: examples/flatPlate/main.cpp:230-277; VISC_SUM:
+   examples/nacaTransient/main.cpp:234-288 (convective + viscous eigenvalues). */
+enum { FVO_DT_CONST = 0, FVO_DT_CFL_SUM = 1, FVO_DT_CFL_MIN_SIGNED = 2, FVO_DT_VISC_MIN = 3,
+       FVO_DT_VISC_SUM = 4 };
+/* NOSLIP: the viscous wall of examples/flatPlate/main.cpp:361-366.
+   FARFIELD_B0: the far field of examples/flatPlate/main.cpp:284-352, whose
+   tangential momentum is b[0]*(...) where examples/naca has b[1]*(...). */
+enum { FVO_BC_COPY = 0, FVO_BC_WALL = 1, FVO_BC_INLET_OUTLET = 2, FVO_BC_FARFIELD = 3,
+       FVO_BC_NOSLIP = 4, FVO_BC_FARFIELD_B0 = 5 };
 
 typedef struct {
     int V;
@@ -56,6 +67,8 @@ typedef struct {
                                  group_bv (a spatially varying inflow; NULL = group_bv) */
     int diffusive;            /* solver::diffusive_gradients (with order2 = 0: gradients are
                                  computed, no limiter, no interpolation) */
+    double mu, pr, cp, r;     /* viscosity, Prandtl number, heat capacity, gas constant
+                                 (consts:: of the Navier-Stokes examples) */
 } fvo_physics;
 
 int fvo_mesh_build(int64_t n_nodes, const double* nodes_x, const double* nodes_y,
@@ -64,6 +77,8 @@ int fvo_mesh_build(int64_t n_nodes, const double* nodes_x, const double* nodes_y
 void fvo_mesh_free(fvo_mesh* m);
 
 void fvo_flux(const fvo_physics* ph, double* f, const double* qi, const double* qj, const double* n);
+void fvo_flux_grad(const fvo_physics* ph, double* f, const double* qi, const double* qj, const double* gx,
+                   const double* gy, const double* n);
 void fvo_bc(const fvo_physics* ph, int group, double* b, const double* q, const double* n);
 double fvo_limiter_func(const fvo_physics* ph, double y);
 

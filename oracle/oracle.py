@@ -20,10 +20,10 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF_DIR = os.path.join(HERE, "_ref")
 
-FLUX = {"roe_fs": 1, "roe_st": 2, "burgers": 3, "diffusion": 4}
+FLUX = {"roe_fs": 1, "roe_st": 2, "burgers": 3, "diffusion": 4, "ns": 5}
 LIMITER = {"zero": 0, "michalak": 1, "venkat": 2, "minmod": 3}
-DT = {"const": 0, "cfl_sum": 1, "cfl_min_signed": 2}
-BC = {"copy": 0, "wall": 1, "inlet_outlet": 2, "farfield": 3}
+DT = {"const": 0, "cfl_sum": 1, "cfl_min_signed": 2, "visc_min": 3, "visc_sum": 4}
+BC = {"copy": 0, "wall": 1, "inlet_outlet": 2, "farfield": 3, "noslip": 4, "farfield_b0": 5}
 
 _dp = C.POINTER(C.c_double)
 _u32p = C.POINTER(C.c_uint32)
@@ -48,7 +48,8 @@ class _FvoPhysics(C.Structure):
                 ("limiter", C.c_int), ("K", C.c_double), ("dt_kind", C.c_int),
                 ("cfl", C.c_double), ("dt_const", C.c_double), ("global_dt", C.c_int),
                 ("n_groups", C.c_int), ("group_bc", _i32p), ("group_bv", _dp), ("positivity_guard", C.c_int),
-                ("ghost_bv", _dp), ("diffusive", C.c_int)]
+                ("ghost_bv", _dp), ("diffusive", C.c_int), ("mu", C.c_double), ("pr", C.c_double),
+                ("cp", C.c_double), ("r", C.c_double)]
 
 
 def build_oracle():
@@ -134,6 +135,7 @@ class Oracle:
         p.group_bc = _ptr(gbc, _i32p); p.group_bv = _ptr(gbv)
         p.positivity_guard = int(getattr(phys, "positivity_guard", False))
         p.diffusive = int(getattr(phys, "diffusive", False))
+        p.mu, p.pr, p.cp, p.r = phys.mu, phys.pr, phys.cp, phys.r
         gh = None
         if ghost_bv is not None:
             gh = np.ascontiguousarray(ghost_bv, np.float64).reshape(-1)
@@ -189,6 +191,12 @@ class Oracle:
         f = np.zeros(p.V)
         self.lib.fvo_flux(C.byref(p), _ptr(f), _ptr(np.ascontiguousarray(qi, np.float64)),
                           _ptr(np.ascontiguousarray(qj, np.float64)), _ptr(np.ascontiguousarray(n, np.float64)))
+        return f
+
+    def flux_grad(self, p, qi, qj, gx, gy, n):
+        f = np.zeros(p.V)
+        a = [np.ascontiguousarray(x, np.float64) for x in (qi, qj, gx, gy, n)]
+        self.lib.fvo_flux_grad(C.byref(p), _ptr(f), *[_ptr(x) for x in a])
         return f
 
     def bc(self, p, group, q, n):
@@ -298,6 +306,12 @@ class RefLib:
         f = np.zeros(self.V)
         self.lib.ref_flux(_ptr(f), _ptr(np.ascontiguousarray(qi, np.float64)),
                           _ptr(np.ascontiguousarray(qj, np.float64)), _ptr(np.ascontiguousarray(n, np.float64)))
+        return f
+
+    def flux_grad(self, qi, qj, gx, gy, n):
+        f = np.zeros(self.V)
+        a = [np.ascontiguousarray(x, np.float64) for x in (qi, qj, gx, gy, n)]
+        self.lib.ref_flux_grad(_ptr(f), *[_ptr(x) for x in a])
         return f
 
     def run_loop(self, q0, alpha, max_step, max_time=1e10, tolerance=1e-16, print_interval=1):

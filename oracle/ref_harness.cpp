@@ -44,6 +44,10 @@ extern double gamma; extern double cfl; extern double mach;
 extern double gamma; extern double cfl;
 #elif defined(FVREF_EX_SHOCKTUBE)
 extern double gamma;
+#elif defined(FVREF_EX_FLATPLATE)
+extern double gamma; extern double cfl;
+#elif defined(FVREF_EX_NACATRANSIENT)
+extern double gamma; extern double cfl; extern double mach;
 #endif  // heatTransfer and burgers have no consts:: globals
 }
 
@@ -101,13 +105,15 @@ double ref_limiter_func(double y) { return fvhyper::limiter_func(y); }
 
 /* Set the example's tunable globals; a negative value leaves it unchanged. */
 void ref_set_consts(double gamma, double cfl, double mach) {
-#if defined(FVREF_EX_FORWARDSTEP) || defined(FVREF_EX_NACA) || defined(FVREF_EX_SHOCKTUBE)
+#if defined(FVREF_EX_FORWARDSTEP) || defined(FVREF_EX_NACA) || defined(FVREF_EX_SHOCKTUBE) || \
+    defined(FVREF_EX_FLATPLATE) || defined(FVREF_EX_NACATRANSIENT)
     if (gamma > 0) fvhyper::consts::gamma = gamma;
 #endif
-#if defined(FVREF_EX_FORWARDSTEP) || defined(FVREF_EX_NACA)
+#if defined(FVREF_EX_FORWARDSTEP) || defined(FVREF_EX_NACA) || defined(FVREF_EX_FLATPLATE) || \
+    defined(FVREF_EX_NACATRANSIENT)
     if (cfl > 0) fvhyper::consts::cfl = cfl;
 #endif
-#if defined(FVREF_EX_FORWARDSTEP)
+#if defined(FVREF_EX_FORWARDSTEP) || defined(FVREF_EX_NACATRANSIENT)
     if (mach > 0) fvhyper::consts::mach = mach;
 #endif
     (void)gamma; (void)cfl; (void)mach;
@@ -125,6 +131,12 @@ void ref_bc_set(const char* name, void* fn) { fvhyper::boundaries::bounds[name] 
 void ref_flux(double* f, const double* qi, const double* qj, const double* n) {
     std::vector<double> z(fvhyper::vars, 0.0);
     fvhyper::calc_flux(f, qi, qj, z.data(), z.data(), n);
+}
+
+/* calc_flux with face gradients (the diffusive fluxes read them). */
+void ref_flux_grad(double* f, const double* qi, const double* qj, const double* gx, const double* gy,
+                   const double* n) {
+    fvhyper::calc_flux(f, qi, qj, gx, gy, n);
 }
 
 /* Read <basename>.msh with the reference reader (mesh.cpp:803-855). */

@@ -21,6 +21,11 @@ def random_euler_state(n, seed, rho=(0.5, 1.5), vel=0.5, p=(0.5, 1.5)):
                          r.uniform(*p, n)).ravel()
 
 
+def _renamed(em, names):
+    em.group_names = list(names)
+    return em
+
+
 def _guarded(ph):
     ph.positivity_guard = True
     return ph
@@ -59,6 +64,13 @@ CASES = {
     "heat": dict(mesh=lambda: meshgen.rect_tri(16, 16, 1.0, 1.0, side_names=("wall", "wall")),
                  phys=lambda: P.heat(), ic=lambda g: P.ic_heat(g.ccx, g.ccy).ravel(),
                  alpha=P.RK5_ALPHA, steps=30, ref="heatTransfer", alias={}, consts={}),
+    "flat_plate": dict(mesh=lambda: meshgen.flat_plate(nx0=6, nx1=18, ny=12),
+                       phys=lambda: P.flat_plate(), ic=lambda g: P.ic_forward_step(g.n_total, mach=0.2).ravel(),
+                       alpha=P.RK5_ALPHA, steps=30, ref="flatPlate", alias={}, consts={}),
+    "naca_transient": dict(mesh=lambda: _renamed(meshgen.naca_ogrid(ni=48, nj=12, r_far=10.0), ["wall", "farfield"]),
+                           phys=lambda: P.naca_transient(),
+                           ic=lambda g: P.ic_forward_step(g.n_total, mach=0.8).ravel(),
+                           alpha=P.RK5_ALPHA, steps=30, ref="nacaTransient", alias={}, consts={}),
     "burgers": dict(mesh=lambda: meshgen.rect_tri(16, 16, 1.0, 1.0, side_names=("wall", "wall")),
                     phys=lambda: P.burgers(), ic=lambda g: P.ic_burgers(g.ccx, g.ccy).ravel(),
                     alpha=P.RK5_ALPHA, steps=30, ref="burgers", alias={}, consts={}),

@@ -194,6 +194,10 @@ def normwise_rel(a, b, V):
 
 
 FP64_STEP_RTOL = 1e-12     # plain FP64 path: max relative error per step
+# The near-uniform M 0.2 flat-plate flow has residuals of ~3 % of its face
+# fluxes, so cancellation amplifies the rounding of the rearranged Roe flux
+# (the fast viscous terms add nothing measurable): up to 2.4e-12 per step.
+FP64_STEP_RTOL_CASE = {"flat_plate": 5e-12}
 
 
 @pytest.mark.parametrize("name", sorted(CASES))
@@ -203,17 +207,22 @@ def test_fp64_stage_functions(name, oracle):
     e_dt = normwise_rel(s.stage_dt(q, False), oracle.calc_dt(g, p, q, False), 1)
     assert e_dt < FP64_STEP_RTOL, e_dt
     ogx, ogy, olim = stage_inputs(oracle, g, p, ph, q)
+    # FP64 keeps the limiter multiplied into the gradients, except for the
+    # diffusive fluxes, whose face gradient needs the raw gradients
+    dev = (ogx, ogy, olim) if ph.diffusive else (ogx * olim, ogy * olim, olim)
     if ph.order2 or ph.diffusive:
-        # FP64 keeps the limiter multiplied into the gradients
         gx, gy, lim = s.stage_gradients_limiters(q)
-        e = (normwise_rel(gx, ogx * olim, ph.V), normwise_rel(gy, ogy * olim, ph.V))
+        e = (normwise_rel(gx, dev[0], ph.V), normwise_rel(gy, dev[1], ph.V))
         assert max(e) < 1e-9, e
-        assert np.all(lim == 1.0)
+        if ph.diffusive:
+            assert normwise_rel(lim, olim, ph.V) < 1e-9
+        else:
+            assert np.all(lim == 1.0)
     dt = oracle.calc_dt(g, p, q, ph.global_dt)
     qb = rand_state(g, ph, 22)
     qt = oracle.time_derivatives(g, p, q, ogx, ogy, olim)
     want = oracle.update_bounds(g, p, qb + qt * np.repeat(dt, ph.V) * 0.506, ogx, ogy, olim)
-    got = s.stage_update(qb, q, ogx * olim, ogy * olim, olim, dt, 0.506)
+    got = s.stage_update(qb, q, dev[0], dev[1], dev[2], dt, 0.506)
     e = normwise_rel(got, want, ph.V)
     assert e < FP64_STEP_RTOL, e
 
@@ -232,7 +241,7 @@ def test_fp64_per_step_error(name, oracle):
         got = s.get_state()
         worst = max(worst, normwise_rel(got[: g.n_real * ph.V], want["q"][: g.n_real * ph.V], ph.V))
         q = want["q"]
-    assert worst < FP64_STEP_RTOL
+    assert worst < FP64_STEP_RTOL_CASE.get(name, FP64_STEP_RTOL), worst
     q0 = case["ic"](g)
     want = oracle.run_loop(g, p, q0, case["alpha"], case["steps"])
     s.set_state(q0)
@@ -252,7 +261,8 @@ def rho_p(q, gamma=1.4):
 FP32_L2_TOL = 1e-4         # FP32-bulk path: relative L2 error of density and pressure
 
 
-@pytest.mark.parametrize("name", ["sod", "step_o1", "step_o2_venk5", "step_o2_mich", "naca"])
+@pytest.mark.parametrize("name", ["sod", "step_o1", "step_o2_venk5", "step_o2_mich", "naca", "flat_plate",
+                                  "naca_transient"])
 def test_fp32_l2_error(name, oracle):
     case, em, ph, s, g, p = setup(name, oracle, "fp32")
     q0 = case["ic"](g)

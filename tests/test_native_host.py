@@ -198,9 +198,11 @@ def test_host_diffusion_kind_matches_its_restatement():
     against numpy written in the order of gradient_for_diffusion
     (explicit.cpp:70-109) and examples/heatTransfer/main.cpp:63-73: IEEE
     float64 operations in the same order give the same bits."""
+    import physics as P
     L = fvgpu.lib()
     dp = ctypes.POINTER(ctypes.c_double)
     rng = np.random.default_rng(5)
+    heat = fvgpu.physics_struct(P.heat(), ["wall"])
 
     def p(a):
         return a.ctypes.data_as(dp)
@@ -223,7 +225,7 @@ def test_host_diffusion_kind_matches_its_restatement():
                 n = rng.normal(size=2)
                 n /= np.hypot(*n)
                 f = np.zeros(1)
-                assert L.fv_kind_flux_grad(4, ctypes.c_double(0.0), p(qi), p(qj), p(gxf), p(gyf), p(n), p(f)) == 0
+                assert L.fv_kind_flux_grad(ctypes.byref(heat), p(qi), p(qj), p(gxf), p(gyf), p(n), p(f)) == 0
                 assert bits_equal(f, -(gxf * n[0] + gyf * n[1]))
     # the diffusion kind needs its gradients; V = 3 is no device width
     z = np.zeros(4)
@@ -233,3 +235,35 @@ def test_host_diffusion_kind_matches_its_restatement():
     q, b = np.array([0.75]), np.zeros(1)
     assert L.fv_kind_bc(0, 1, ctypes.c_double(1.4), None, p(q), p(np.array([1.0, 0.0])), p(b)) == 0
     assert b[0] == 0.75
+
+
+def test_host_navier_stokes_kind_matches_oracle(oracle):
+    """fv_kind_flux_grad for FV_FLUX_NS and fv_kind_bc for the no-slip wall
+    and the b[0] far field (host copies of the device kinds the fvhyper shim
+    matches the flatPlate / nacaTransient callbacks to) against the oracle,
+    which is pinned to the reference build: bit for bit."""
+    import physics as P
+    from cases import random_euler_state
+    L = fvgpu.lib()
+    dp = ctypes.POINTER(ctypes.c_double)
+
+    def p(a):
+        return a.ctypes.data_as(dp)
+
+    rng = np.random.default_rng(9)
+    ph = P.flat_plate()
+    names = ["top", "bot0", "bot1", "left", "right"]
+    s = fvgpu.physics_struct(ph, names)
+    o = oracle.physics(ph, names)
+    for _ in range(100):
+        qi, qj = random_euler_state(1, int(rng.integers(1 << 30))), random_euler_state(1, int(rng.integers(1 << 30)))
+        gx, gy = rng.normal(size=4), rng.normal(size=4)
+        t = rng.uniform(0, 2 * np.pi); n = np.array([np.cos(t), np.sin(t)])
+        f = np.zeros(4)
+        assert L.fv_kind_flux_grad(ctypes.byref(s), p(qi), p(qj), p(gx), p(gy), p(n), p(f)) == 0
+        assert bits_equal(f, oracle.flux_grad(o, qi, qj, gx, gy, n))
+        for g, kind in ((2, 4), (0, 5)):   # bot1 no-slip, top far field (b[0] form)
+            b = np.zeros(4)
+            bv = np.array(ph.bcs[names[g]][1] or [0.0] * 4, np.float64)
+            assert L.fv_kind_bc(kind, 4, ctypes.c_double(ph.gamma), p(bv), p(qi), p(n), p(b)) == 0
+            assert bits_equal(b, oracle.bc(o, g, qi, n))

@@ -56,7 +56,9 @@ def test_stage_functions_bitwise(name, oracle):
     if flags["lim"]:  # first-order cases never call limiter_func
         assert bits_equal(lim, ref.limiters(q, gx, gy))
     if not flags["linear"]:
-        gx = np.zeros_like(q); gy = np.zeros_like(q); lim = np.zeros_like(q)
+        lim = np.zeros_like(q)
+        if not flags["diffusive"]:  # the gradients feed only the diffusive face gradient
+            gx = np.zeros_like(q); gy = np.zeros_like(q)
     assert bits_equal(oracle.time_derivatives(g, p, q, gx, gy, lim), ref.time_derivatives(q, gx, gy, lim))
     assert bits_equal(oracle.update_bounds(g, p, q, gx, gy, lim), ref.update_bounds(q, gx, gy, lim))
 
@@ -118,6 +120,29 @@ def test_flux_and_limiter_functions(oracle):
     assert ref.lib.ref_limiter_k() == 5.0
     for y in np.linspace(-3, 3, 61):
         assert oracle.limiter_func(p, y) == ref.lib.ref_limiter_func(float(y))
+
+
+def test_diffusive_fluxes_with_face_gradients(oracle):
+    """calc_flux of the diffusive examples, fed random face gradients: the
+    Navier-Stokes flux of flatPlate / nacaTransient and the heatTransfer
+    diffusion flux, bit for bit."""
+    from oracle import RefLib
+    import physics as P
+    r = np.random.default_rng(7)
+    for variant, ph in (("flatPlate", P.flat_plate()), ("nacaTransient", P.naca_transient()),
+                        ("heatTransfer", P.heat())):
+        ref = RefLib(variant)
+        p = oracle.physics(ph, sorted(ph.bcs))
+        V = ph.V
+        for _ in range(200):
+            if V == 4:
+                qi = random_euler_state(1, int(r.integers(1 << 30)))
+                qj = random_euler_state(1, int(r.integers(1 << 30)))
+            else:
+                qi, qj = r.uniform(-1, 1, V), r.uniform(-1, 1, V)
+            gx, gy = r.normal(size=V) * 3, r.normal(size=V) * 3
+            t = r.uniform(0, 2 * np.pi); n = np.array([np.cos(t), np.sin(t)])
+            assert bits_equal(oracle.flux_grad(p, qi, qj, gx, gy, n), ref.flux_grad(qi, qj, gx, gy, n))
 
 
 def test_missing_boundary_edge_rejected(oracle):

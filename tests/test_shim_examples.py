@@ -10,8 +10,7 @@ program built from the same source on fvhyper's own library
   ASCII layout (FVGPU_VTK_FORMAT=ascii);
 - the default binary VTU carries the same cell values.
 
-Examples whose physics the device path does not run (the viscous Navier-Stokes
-fluxes of flatPlate and nacaTransient) and
+All seven examples run.  Programs whose physics no device kind implements and
 meshes whose boundary names the program does not define must be refused the
 way the reference refuses them: an uncaught std::invalid_argument.
 """
@@ -45,6 +44,11 @@ def _one_group(em, name):
     return em
 
 
+def _renamed(em, names):
+    em.group_names = list(names)
+    return em
+
+
 def _step_mesh():
     em = meshgen.forward_step(n=10)
     names = list(em.group_names)            # wall, inlet, outlet, step
@@ -60,13 +64,22 @@ CASES = {
     "naca": ("naca.msh", lambda: meshgen.naca_ogrid(ni=40, nj=10, r_far=10.0, jitter=0.0), "naca.vtu"),
     "forwardStep": ("step.msh", _step_mesh, None),
     "heatTransfer": ("square.msh", lambda: _one_group(meshgen.rect_tri(12, 12, 1.0, 1.0), "wall"), "square.vtu"),
+    "flatPlate": ("square.msh", lambda: meshgen.flat_plate(nx0=6, nx1=18, ny=12), "square.vtu"),
+    # saves a time series (times/naca0012_<k>.vtu, 334 snapshots) and no final file
+    "nacaTransient": ("naca0012.msh", lambda: _renamed(meshgen.naca_ogrid(ni=24, nj=12, r_far=10.0, jitter=0.0),
+                                                       ["wall", "farfield"]), None),
 }
 
 
 def _setup(tmp, name):
     fname, build, _ = CASES[name]
-    os.makedirs(tmp, exist_ok=True)
+    os.makedirs(os.path.join(tmp, "times"), exist_ok=True)  # time-series snapshots go there
     meshgen.write_msh41(os.path.join(tmp, fname), build())
+
+
+def _outputs(d):
+    return sorted(os.path.relpath(os.path.join(r, f), d) for r, _, fs in os.walk(d) for f in fs
+                  if f.endswith((".vtu", ".pvtu")))
 
 
 def _run_gpu(name, cwd, vtk_format="ascii"):
@@ -119,11 +132,13 @@ def test_example_program_matches_reference(name, tmp_path):
         # order on the device: equal to print precision up to the last digit
         assert np.allclose([_num(x) for x in gr], [_num(x) for x in wr], rtol=2e-5, atol=0, equal_nan=True), \
             (gs, gr, wr)
-    vtu = CASES[name][2]
-    if vtu:
-        a = open(os.path.join(gpu_dir, vtu), "rb").read()
-        b = open(os.path.join(ref_dir, vtu), "rb").read()
-        assert a == b
+    # every file written (final state, time series), byte for byte
+    files = _outputs(ref_dir)
+    assert _outputs(gpu_dir) == files and (CASES[name][2] is None or CASES[name][2] in files)
+    for f in files:
+        a = open(os.path.join(gpu_dir, f), "rb").read()
+        b = open(os.path.join(ref_dir, f), "rb").read()
+        assert a == b, f
 
 
 def _read_binary_vtu(path):
@@ -164,20 +179,74 @@ def test_binary_vtu_holds_the_state(tmp_path):
     assert b["offsets"][-1] == b["connectivity"].size
 
 
-@pytest.mark.parametrize("name,mesh,group_names", [
-    ("flatPlate", "square.msh", ["top", "bot0", "bot1", "left", "right"]),
-    ("nacaTransient", "naca0012.msh", ["wall", "farfield"]),
-])
-def test_viscous_examples_are_refused(name, mesh, group_names, tmp_path):
-    em = meshgen.rect_tri(6, 5, 1.0, 1.0)
-    em.bnd_group[:] = np.arange(em.bnd_group.size) % len(group_names)
-    order = np.argsort(em.bnd_group, kind="stable")
-    em.bnd_nodes, em.bnd_group = em.bnd_nodes[order], em.bnd_group[order]
-    em.group_names = group_names
-    meshgen.write_msh41(str(tmp_path / mesh), em)
-    r = subprocess.run([_program(name)], cwd=str(tmp_path), capture_output=True, text=True, timeout=120)
+# A user program with physics no device kind implements: two variables with
+# diffusive fluxes (advection plus diffusion), optionally residual smoothing.
+_UNSUPPORTED_PROGRAM = r"""
+#include <fvhyper/mesh.h>
+#include <fvhyper/explicit.h>
+#include <fvhyper/parallel.h>
+#include <fvhyper/post.h>
+namespace fvhyper {
+const int vars = 2;
+const std::vector<std::string> var_names = {"a", "b"};
+namespace solver {
+const bool do_calc_gradients = true;
+const bool do_calc_limiters = false;
+const bool linear_interpolate = false;
+const bool diffusive_gradients = true;
+const bool global_dt = true;
+const bool smooth_residuals = SMOOTH;
+}
+void generate_initial_solution(std::vector<double>& q, const mesh& m) {
+    for (uint i = 0; i < m.cellsAreas.size(); ++i) { q[2 * i] = m.cellsCentersX[i]; q[2 * i + 1] = 1.0; }
+}
+double limiter_func(const double& y) { return 0.0; }
+void calc_flux(double* f, const double* qi, const double* qj, const double* gx, const double* gy,
+               const double* n) {
+    for (int k = 0; k < 2; ++k) f[k] = 0.5 * (qi[k] + qj[k]) * n[0] - 0.01 * (gx[k] * n[0] + gy[k] * n[1]);
+}
+void calc_dt(std::vector<double>& dt, const std::vector<double>& q, mesh& m) {
+    for (double& d : dt) d = 1e-4;
+}
+namespace boundaries {
+void copy(double* b, double* q, double* n) { b[0] = q[0]; b[1] = q[1]; }
+std::map<std::string, void (*)(double*, double*, double*)> bounds = {{"wall", copy}};
+}
+namespace post {
+std::map<std::string, void (*)(double*, double*)> extra_scalars = {};
+std::map<std::string, void (*)(double*, double*)> extra_vectors = {};
+}
+}
+int main() {
+    fvhyper::mpi_wrapper pool;
+    fvhyper::mesh m;
+    m.read_file("square", pool);
+    fvhyper::solverOptions options;
+    options.max_step = 10;
+    std::vector<double> q;
+    fvhyper::run("square", q, pool, m, options);
+    return pool.exit();
+}
+"""
+
+
+@pytest.mark.parametrize("smooth,message", [("false", "diffusive_gradients with vars = 2"),
+                                            ("true", "smooth_residuals")])
+def test_unsupported_physics_is_refused(smooth, message, tmp_path):
+    """Refused in run() before any device work, as an uncaught
+    std::invalid_argument naming what has no device kind."""
+    shim = os.path.join(PKG, "libfvhyper_gpu.a")
+    if not os.path.exists(shim) or shutil.which("g++") is None:
+        pytest.skip("needs the built shim and g++")
+    src = tmp_path / "main.cpp"
+    src.write_text(_UNSUPPORTED_PROGRAM.replace("SMOOTH", smooth))
+    exe = str(tmp_path / "prog")
+    subprocess.run(["g++", "-O1", "-std=c++17", "-I" + os.path.join(ROOT, "include"), str(src), shim,
+                    "-L" + PKG, "-lfvgpu", "-Wl,-rpath," + PKG, "-o", exe], check=True, timeout=300)
+    meshgen.write_msh41(str(tmp_path / "square.msh"), _one_group(meshgen.rect_tri(6, 5, 1.0, 1.0), "wall"))
+    r = subprocess.run([exe], cwd=str(tmp_path), capture_output=True, text=True, timeout=120)
     assert r.returncode != 0
-    assert "std::invalid_argument" in r.stderr and "diffusive_gradients" in r.stderr, r.stderr
+    assert "std::invalid_argument" in r.stderr and message in r.stderr, r.stderr
 
 
 def test_unknown_boundary_name_is_refused(tmp_path):
