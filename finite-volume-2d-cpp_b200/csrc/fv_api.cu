@@ -93,6 +93,10 @@ struct fv_solver {
     Ctrl* hctrl = nullptr;      // mapped pinned host copy of the run control, written by a kernel
     Ctrl* hctrl_dev = nullptr;  // its device address
     std::vector<int64_t> case_real_off, case_bound_off;    // batches: host copies
+    // residual smoothing: time derivatives before / after each Jacobi sweep
+    // ([n_total][V], ghosts 0) and the real cells' neighbours ([4][n_real])
+    double* qts[3] = {nullptr, nullptr, nullptr};
+    uint32_t* nbr = nullptr;
 
     template <class T>
     cudaError_t alloc(T** p, size_t n, size_t elem = sizeof(T)) {
@@ -311,6 +315,11 @@ static int validate_physics(const fv_physics* ph, int n_groups_mesh) {
         if (ph->dt_kind != FV_DT_CONST) return fail(FV_ERR_UNSUPPORTED, "the Burgers kind supports a constant dt only");
     } else if (ph->flux == FV_FLUX_ROE_FS || ph->flux == FV_FLUX_ROE_ST) {
         if (ph->V != 4) return fail(FV_ERR_UNSUPPORTED, "the Roe flux kinds have V = 4");
+    } else if (ph->flux == FV_FLUX_BURGERS_DIFF) {
+        if (ph->V != 2) return fail(FV_ERR_UNSUPPORTED, "the Burgers-diffusion flux kind has V = 2");
+        if (!ph->diffusive) return fail(FV_ERR_UNSUPPORTED, "the Burgers-diffusion flux kind needs diffusive = 1");
+        if (ph->dt_kind != FV_DT_CONST)
+            return fail(FV_ERR_UNSUPPORTED, "the Burgers-diffusion kind supports a constant dt only");
     } else if (ph->flux == FV_FLUX_NS) {
         if (ph->V != 4) return fail(FV_ERR_UNSUPPORTED, "the Navier-Stokes flux kind has V = 4");
         if (!ph->diffusive) return fail(FV_ERR_UNSUPPORTED, "the Navier-Stokes flux kind needs diffusive = 1");
@@ -323,8 +332,10 @@ static int validate_physics(const fv_physics* ph, int n_groups_mesh) {
     } else {
         return fail(FV_ERR_UNSUPPORTED, "unknown flux kind " + std::to_string(ph->flux));
     }
-    if (ph->diffusive && ph->flux != FV_FLUX_DIFFUSION && ph->flux != FV_FLUX_NS)
-        return fail(FV_ERR_UNSUPPORTED, "diffusive gradients are used by the diffusion and Navier-Stokes kinds only");
+    if (ph->diffusive && ph->flux != FV_FLUX_DIFFUSION && ph->flux != FV_FLUX_NS && ph->flux != FV_FLUX_BURGERS_DIFF)
+        return fail(FV_ERR_UNSUPPORTED, "diffusive gradients are used by the diffusive flux kinds only");
+    if (ph->smooth_residuals && ph->flux != FV_FLUX_BURGERS_DIFF)
+        return fail(FV_ERR_UNSUPPORTED, "residual smoothing runs with the Burgers-diffusion kind only");
     if (ph->limiter < 0 || ph->limiter > 3) return fail(FV_ERR_UNSUPPORTED, "unknown limiter kind");
     if (ph->dt_kind < 0 || ph->dt_kind > 4) return fail(FV_ERR_UNSUPPORTED, "unknown dt kind");
     if (ph->dt_kind >= FV_DT_VISC_MIN && ph->V != 4) return fail(FV_ERR_UNSUPPORTED, "the viscous dt kinds have V = 4");
@@ -336,8 +347,9 @@ static int validate_physics(const fv_physics* ph, int n_groups_mesh) {
     if (ph->n_groups > kMaxGroups) return fail(FV_ERR_UNSUPPORTED, "more than 16 boundary groups");
     for (int g = 0; g < ph->n_groups; ++g) {
         const int k = ph->group_bc[g];
-        if (k < 0 || k > 5) return fail(FV_ERR_UNSUPPORTED, "unknown boundary condition kind");
-        if (ph->V != 4 && k != FV_BC_COPY)
+        if (k < 0 || k > 6) return fail(FV_ERR_UNSUPPORTED, "unknown boundary condition kind");
+        if (k == FV_BC_TANGENT && ph->V != 2) return fail(FV_ERR_UNSUPPORTED, "the tangent boundary has V = 2");
+        if (ph->V != 4 && k != FV_BC_COPY && k != FV_BC_TANGENT)
             return fail(FV_ERR_UNSUPPORTED, "V = " + std::to_string(ph->V) + " supports the copy boundary only");
     }
     return FV_OK;
@@ -393,6 +405,7 @@ int fv_solver_create_ex(const fv_mesh* fm, const fv_physics* ph, int32_t precisi
     P.positivity_guard = ph->positivity_guard ? 1 : 0;
     P.diffusive = ph->diffusive ? 1 : 0;
     P.mu = ph->mu; P.pr = ph->pr; P.cp = ph->cp; P.r = ph->r;
+    P.smooth = ph->smooth_residuals ? 1 : 0;
     P.gamma = ph->gamma; P.K = ph->K; P.cfl = ph->cfl; P.dt_const = ph->dt_const;
     P.n_groups = ph->n_groups;
     for (int g = 0; g < ph->n_groups; ++g) {
@@ -482,6 +495,15 @@ int fv_solver_create_ex(const fv_mesh* fm, const fv_physics* ph, int32_t precisi
         CK(s->alloc(&s->keys, (size_t)nc * kDtSlots));
     } else {
         s->TP.P.n_cases = 1;
+    }
+    if (s->TP.P.smooth) {
+        for (auto*& b : s->qts) {
+            CK(s->alloc(&b, nq));
+            CK(cudaMemsetAsync(b, 0, nq * 8, s->stream));  // ghosts keep qt = 0
+        }
+        const uint32_t* d;
+        if ((rc = upload_v(s.get(), fa.nbr, &d))) return rc;
+        s->nbr = const_cast<uint32_t*>(d);
     }
     launch_fill_ghost_grad(s->gx, s->gy, s->lim, (int)m.n_real, (int)m.n_total, ph->V, s->f32, s->stream);
     CK(cudaGetLastError());
@@ -735,7 +757,18 @@ static int enqueue_step(fv_solver* s, const std::vector<double>& alpha, int b, E
         so.s_out = s->f32 ? out_s : nullptr;
         so.write_f64 = last ? 1 : 0;
         if (grads) { tile::launch_gradlim(s->precision, TP, so, st, k == 0, pdl); ++n; mark(KK_GRADLIM); }
-        tile::launch_stage(s->precision, TP, so, st, pdl); ++n; mark(KK_STAGE);
+        if (TP.P.smooth) {
+            // time derivatives, two Jacobi sweeps of smoothing, then the update
+            // from the smoothed derivatives (explicit.cpp:742-744)
+            so.qt = s->qts[0];
+            tile::launch_stage(s->precision, TP, so, st, pdl, 1); ++n; mark(KK_STAGE);
+            launch_smooth(TP.P, s->nbr, s->qts[0], s->qts[0], s->qts[1], st); ++n; mark(KK_STAGE);
+            launch_smooth(TP.P, s->nbr, s->qts[1], s->qts[0], s->qts[2], st); ++n; mark(KK_STAGE);
+            so.qt = s->qts[2];
+            tile::launch_stage(s->precision, TP, so, st, pdl, 2); ++n; mark(KK_STAGE);
+        } else {
+            tile::launch_stage(s->precision, TP, so, st, pdl); ++n; mark(KK_STAGE);
+        }
         in = out_s;
     }
     launch_step_end(TP.P, s->ctrl, s->limits, s->partials, s->n_tiles, s->dt, s->keys, s->n_cases * kDtSlots,

@@ -53,6 +53,7 @@ struct Params {
     // physics
     int flux, order2, limiter, dt_kind, global_dt, positivity_guard;
     int diffusive;                  // cell gradients feed the face gradient of the flux
+    int smooth;                     // residual smoothing after each stage's time derivatives
     double gamma, K, cfl, dt_const;
     double mu, pr, cp, r;           // Navier-Stokes constants (viscous flux and dt kinds)
     int n_groups;

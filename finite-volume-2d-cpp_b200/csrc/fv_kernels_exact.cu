@@ -241,6 +241,46 @@ void launch_bounds(const Params& P, double* q, const double* gx, const double* g
 }
 }  // namespace exact
 
+// ------------------------------------------------------ residual smoothing --
+// One Jacobi sweep (explicit.cpp:46-64, epsilon 0.6), one thread per real
+// cell, neighbours gathered in increasing reference edge order: the same
+// operations in the same order as the reference's edge scatter.
+template <int V>
+__global__ void k_smooth(int n_real, const uint32_t* __restrict__ nbr, const double* __restrict__ qt_in,
+                         const double* __restrict__ qt0, double* __restrict__ qt_out) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= n_real) return;
+    const double epsilon = 0.6;
+    double s[V];
+#pragma unroll
+    for (int k = 0; k < V; ++k) s[k] = 0.;
+    int ne = 0;
+#pragma unroll
+    for (int f = 0; f < kMaxFaces; ++f) {
+        const uint32_t w = nbr[(size_t)f * n_real + c];
+        if (w == kNoFace) continue;
+        ++ne;
+        const int nb = (int)(w & 0x7FFFFFFFu);
+        double qn[V];
+        load_cell<V>(qt_in, nb, qn);
+#pragma unroll
+        for (int k = 0; k < V; ++k) s[k] -= qn[k] * epsilon;
+    }
+    const double nf = ne == 3 ? 3 : 4;  // cellsIsTriangle ? 3 : 4
+    double q0[V], out[V];
+    load_cell<V>(qt0, c, q0);
+#pragma unroll
+    for (int k = 0; k < V; ++k) out[k] = (q0[k] - s[k]) / (1. + nf * epsilon);
+    store_cell<V>(qt_out, c, out);
+}
+void launch_smooth(const Params& P, const uint32_t* nbr, const double* qt_in, const double* qt0, double* qt_out,
+                   cudaStream_t st) {
+    const int g = grid_for(P.n_real);
+    if (P.V == 4) k_smooth<4><<<g, kBlock, 0, st>>>(P.n_real, nbr, qt_in, qt0, qt_out);
+    else if (P.V == 2) k_smooth<2><<<g, kBlock, 0, st>>>(P.n_real, nbr, qt_in, qt0, qt_out);
+    else k_smooth<1><<<g, kBlock, 0, st>>>(P.n_real, nbr, qt_in, qt0, qt_out);
+}
+
 // ----------------------------------------------------------------- utilities --
 __global__ void k_permute_to_device(const double* __restrict__ qr, double* __restrict__ qd,
                                     const int32_t* __restrict__ new2ref, int n, int V) {

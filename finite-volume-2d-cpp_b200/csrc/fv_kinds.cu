@@ -29,6 +29,10 @@ int fv_kind_flux_grad(const fv_physics* ph, const double* qi, const double* qj, 
         fvgpu::exact::diffusion(f, gx, gy, n[0], n[1]);
         return FV_OK;
     }
+    if (ph->flux == FV_FLUX_BURGERS_DIFF) {
+        fvgpu::exact::burgers_diffusion(f, qi, qj, gx, gy, n[0], n[1]);
+        return FV_OK;
+    }
     if (ph->flux == FV_FLUX_NS) {
         fvgpu::Params P;
         memset(&P, 0, sizeof(P));
@@ -63,7 +67,7 @@ int fv_kind_limiter(int32_t kind, double y, double* out) {
 int fv_kind_bc(int32_t kind, int32_t V, double gamma, const double* bv, const double* q, const double* n,
                double* b) {
     if (!q || !n || !b || (V != 1 && V != 2 && V != 4)) return FV_ERR_ARG;
-    if (kind < FV_BC_COPY || kind > FV_BC_FARFIELD_B0) return FV_ERR_UNSUPPORTED;
+    if (kind < FV_BC_COPY || kind > FV_BC_TANGENT) return FV_ERR_UNSUPPORTED;
     if ((kind == FV_BC_INLET_OUTLET || kind == FV_BC_FARFIELD || kind == FV_BC_FARFIELD_B0) && !bv)
         return FV_ERR_ARG;
     fvgpu::Params P;

@@ -26,6 +26,13 @@ void launch_bounds(const Params& P, double* q, const double* gx, const double* g
                    const double* lim, int zero_grad, cudaStream_t st);
 }  // namespace exact
 
+// One Jacobi sweep of residual smoothing (explicit.cpp:32-66) over the real
+// cells: out = (qt0 - s) / (1 + ne eps), s = -eps * sum of the neighbours'
+// qt_in in face (reference edge) order.  nbr: [4][n_real] neighbour device
+// index | side << 31, 0xFFFFFFFF = no face; ghosts hold qt = 0.
+void launch_smooth(const Params& P, const uint32_t* nbr, const double* qt_in, const double* qt0, double* qt_out,
+                   cudaStream_t st);
+
 // utilities (fv_kernels_exact.cu)
 void launch_permute_to_device(const double* q_ref, double* q_dev, const int32_t* new2ref,
                               int n_total, int V, cudaStream_t st);

@@ -156,6 +156,15 @@ FV_HD void ns_viscous(const Params& P, double* f, const double* qi, const double
     f[3] -= n0 * phi0 + n1 * phi1;
 }
 
+// Regression-test physics (tests/tests.cpp:94-116): the upwind advection flux
+// plus -(grad q . n) of the face gradient per variable.
+FV_HD void burgers_diffusion(double* f, const double* qi, const double* qj, const double* gx, const double* gy,
+                             double n0, double n1) {
+    burgers(f, qi, qj, n0, n1);
+    f[0] += -(gx[0] * n0 + gy[0] * n1);
+    f[1] += -(gx[1] * n0 + gy[1] * n1);
+}
+
 // Viscous eigenvalue of the viscous time steps, max(4/(3 rho), gamma/rho) *
 // (mu/pr) * le^2 / A (flatPlate/main.cpp:264-267).
 FV_HD double visc_eig(const Params& P, double rho, double le, double A) {
@@ -183,8 +192,14 @@ FV_HD double limiter_func(int kind, double y) {
 // main.cpp:194-261.  FARFIELD: naca/main.cpp:192-259.  Subsonic outlets keep
 // the reference's b[2] = b[1]*(...).  NOSLIP: flatPlate/main.cpp:361-366.
 // FARFIELD_B0: flatPlate/main.cpp:286-352, FARFIELD with b[2] = b[0]*(...).
+// TANGENT (V = 2): tests/tests.cpp:132-135.
 template <int V, class T>
 FV_HD void bc_state(int kind, double gamma, const T* bv, T* b, const T* q, double n0, double n1) {
+    if (kind == 6 && V == 2) {  // TANGENT, tests/tests.cpp:132-135
+        b[0] = -n1;
+        b[1] = n0;
+        return;
+    }
     if (kind == 0 || V != 4) {
 #pragma unroll
         for (int k = 0; k < V; ++k) b[k] = q[k];

@@ -148,6 +148,11 @@ __device__ __forceinline__ T limiter_func(int kind, T y) {
 template <int V, class T>
 __device__ __forceinline__ void bc(const Params& P, int group, int gb, T* b, const T* q, T n0, T n1) {
     const int kind = P.group_bc[group];
+    if (kind == 6 && V == 2) {  // TANGENT
+        b[0] = -n1;
+        b[1] = n0;
+        return;
+    }
     if (kind == 0 || V != 4) {
 #pragma unroll
         for (int k = 0; k < V; ++k) b[k] = q[k];

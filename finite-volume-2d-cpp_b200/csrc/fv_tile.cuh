@@ -69,6 +69,7 @@ struct TileIO {
     double* partials;          // [n_tiles][V] or nullptr
     unsigned long long* dtkeys;  // [n_cases][kDtSlots] ordered keys of the global dt minimum
     int write_f64;             // FP32 mode: also write q_out (last stage)
+    double* qt;                // [n_total][V] time derivatives of the smoothing phases (FP64)
 };
 
 __device__ __forceinline__ unsigned long long tkey(double x) {
@@ -708,58 +709,70 @@ __global__ void __launch_bounds__(kTileMax) k_tile_gradlim(TileParams TP, TileIO
     }
 }
 
-// Navier-Stokes flux of one tile edge (FLUX 5) from the records of its two
-// cells (raw gradients and limiters staged apart in every mode): MUSCL face
-// states when P.order2, the corrected face gradient from the cell states, the
-// roe<false> flux minus the viscous terms.  Fast modes return f * le.
-template <class M, class R>
-__device__ __forceinline__ void ns_edge_flux(const Params& P, const typename M::S* ri, const typename M::S* rj,
-                                             typename M::S n0, typename M::S n1, typename M::S xf,
-                                             typename M::S yf, typename M::S le,
-                                             typename std::conditional<M::exact, double, typename M::S>::type* f) {
+// Flux of one tile edge for the diffusive kinds with raw gradients and
+// limiters staged apart in every mode: FLUX 5 (Navier-Stokes, V = 4) and
+// FLUX 6 (Burgers + diffusion, V = 2).  MUSCL face states when P.order2, the
+// corrected face gradient from the cell states, then the convective flux
+// (roe<false> / burgers) with the viscous or diffusive terms.  Fast modes
+// return f * le.
+template <class M, int V, int FLUX, class R>
+__device__ __forceinline__ void diffusive_edge_flux(const Params& P, const typename M::S* ri, const typename M::S* rj,
+                                                    typename M::S n0, typename M::S n1, typename M::S xf,
+                                                    typename M::S yf, typename M::S le,
+                                                    typename std::conditional<M::exact, double, typename M::S>::type* f) {
     using S = typename M::S;
-    S qci[4], qcj[4], gxi[4], gyi[4], gxj[4], gyj[4], qL[4], qR[4];
-    lds<S, 4>(ri, qci); lds<S, 4>(rj, qcj);
-    lds<S, 4>(ri + R::OGX, gxi); lds<S, 4>(ri + R::OGY, gyi);
-    lds<S, 4>(rj + R::OGX, gxj); lds<S, 4>(rj + R::OGY, gyj);
+    S qci[V], qcj[V], gxi[V], gyi[V], gxj[V], gyj[V], qL[V], qR[V];
+    lds<S, V>(ri, qci); lds<S, V>(rj, qcj);
+    lds<S, V>(ri + R::OGX, gxi); lds<S, V>(ri + R::OGY, gyi);
+    lds<S, V>(rj + R::OGX, gxj); lds<S, V>(rj + R::OGY, gyj);
     const S cix = ri[R::OC], ciy = ri[R::OC + 1], cjx = rj[R::OC], cjy = rj[R::OC + 1];
     if (P.order2) {
-        S li_[4], lj_[4];
-        lds<S, 4>(ri + R::OLM, li_); lds<S, 4>(rj + R::OLM, lj_);
+        S li_[V], lj_[V];
+        lds<S, V>(ri + R::OLM, li_); lds<S, V>(rj + R::OLM, lj_);
         const S di0 = xf - cix, di1 = yf - ciy, dj0 = xf - cjx, dj1 = yf - cjy;
 #pragma unroll
-        for (int k = 0; k < 4; ++k) {
+        for (int k = 0; k < V; ++k) {
             qL[k] = qci[k] + (gxi[k] * di0 + gyi[k] * di1) * li_[k];
             qR[k] = qcj[k] + (gxj[k] * dj0 + gyj[k] * dj1) * lj_[k];
         }
-        guard_face<S, 4>(P, qL, qci);
-        guard_face<S, 4>(P, qR, qcj);
+        guard_face<S, V>(P, qL, qci);
+        guard_face<S, V>(P, qR, qcj);
     } else {
 #pragma unroll
-        for (int k = 0; k < 4; ++k) { qL[k] = qci[k]; qR[k] = qcj[k]; }
+        for (int k = 0; k < V; ++k) { qL[k] = qci[k]; qR[k] = qcj[k]; }
     }
     if constexpr (M::exact) {
-        exact::roe<false>(P.gamma, f, qL, qR, n0, n1);
-        double gxf[4], gyf[4];
-        exact::face_gradient<4>(gxf, gyf, gxi, gyi, gxj, gyj, qci, qcj, cix, ciy, cjx, cjy);
-        exact::ns_viscous(P, f, qL, qR, gxf, gyf, n0, n1);
+        double gxf[V], gyf[V];
+        exact::face_gradient<V>(gxf, gyf, gxi, gyi, gxj, gyj, qci, qcj, cix, ciy, cjx, cjy);
+        if constexpr (FLUX == 5) {
+            exact::roe<false>(P.gamma, f, qL, qR, n0, n1);
+            exact::ns_viscous(P, f, qL, qR, gxf, gyf, n0, n1);
+        } else {
+            exact::burgers_diffusion(f, qL, qR, gxf, gyf, n0, n1);
+        }
     } else {
-        fast::roe<S>((S)P.gamma, f, qL, qR, n0, n1);
         S t0 = cix - cjx, t1 = ciy - cjy;
         const S rl = fast::rcp(fast::sqrt_(t0 * t0 + t1 * t1));
         t0 *= rl;
         t1 *= rl;
-        S gxf[4], gyf[4];
+        S gxf[V], gyf[V];
 #pragma unroll
-        for (int k = 0; k < 4; ++k) {
+        for (int k = 0; k < V; ++k) {
             const S bx = S(0.5) * (gxi[k] + gxj[k]), by = S(0.5) * (gyi[k] + gyj[k]);
             const S corr = bx * t0 + by * t1 - (qci[k] - qcj[k]) * rl;
             gxf[k] = bx - corr * t0;
             gyf[k] = by - corr * t1;
         }
-        fast::ns_viscous<S>(P, f, qL, qR, gxf, gyf, n0, n1);
+        if constexpr (FLUX == 5) {
+            fast::roe<S>((S)P.gamma, f, qL, qR, n0, n1);
+            fast::ns_viscous<S>(P, f, qL, qR, gxf, gyf, n0, n1);
+        } else {
+            fast::burgers<S>(f, qL, qR, n0, n1);
 #pragma unroll
-        for (int k = 0; k < 4; ++k) f[k] *= le;
+            for (int k = 0; k < V; ++k) f[k] -= gxf[k] * n0 + gyf[k] * n1;
+        }
+#pragma unroll
+        for (int k = 0; k < V; ++k) f[k] *= le;
     }
 }
 
@@ -767,12 +780,15 @@ __device__ __forceinline__ void ns_edge_flux(const Params& P, const typename M::
 // ORDER2: the records carry gradients and centroids.  They feed the MUSCL
 // face states, or (FLUX 4, diffusion) the face gradient of the flux, whose
 // face states are the cell values (first order).
-template <class M, int V, bool ORDER2, int FLUX>
+// PH (residual smoothing, FLUX 6 only): 0 the whole stage; 1 the time
+// derivatives only, written to io.qt; 2 the update from the smoothed io.qt
+// (RK update, ghost fill, residual partials) without fluxes.
+template <class M, int V, bool ORDER2, int FLUX, int PH = 0>
 __global__ void __launch_bounds__(kTileMax) k_tile_stage(TileParams TP, TileIO io) {
     using S = typename M::S;
     using FT = typename std::conditional<M::exact, double, S>::type;  // flux storage
-    // FLUX 5 (Navier-Stokes) keeps raw gradients and limiters apart in every mode
-    constexpr bool LIMREC = M::exact || FLUX == 5;
+    // FLUX 5 and 6 keep raw gradients and limiters apart in every mode
+    constexpr bool LIMREC = M::exact || FLUX == 5 || FLUX == 6;
     using R = Rec<M, V, ORDER2, ORDER2, LIMREC>;
     constexpr bool MUSCL = ORDER2 && FLUX != 4;
     pdl_trigger();
@@ -808,8 +824,8 @@ __global__ void __launch_bounds__(kTileMax) k_tile_stage(TileParams TP, TileIO i
         if (!global_dt) dtc = io.dt[c];
     }
     stage_records<M, V, ORDER2, ORDER2, LIMREC>(TP, io, inf, c0, nown, rec);
-    // MUSCL face states: FLUX 5 runs with and without them (P.order2)
-    const bool muscl = MUSCL && (FLUX != 5 || P.order2 != 0);
+    // MUSCL face states: FLUX 5 and 6 run with and without them (P.order2)
+    const bool muscl = MUSCL && ((FLUX != 5 && FLUX != 6) || P.order2 != 0);
     // the tile's case (batches); -1: the tile spans two cases
     const int tc = (global_dt && P.n_cases > 1) ? P.tile_case[t] : 0;
     if (global_dt && tc >= 0 && threadIdx.x < 32) {
@@ -822,15 +838,15 @@ __global__ void __launch_bounds__(kTileMax) k_tile_stage(TileParams TP, TileIO i
     cpa_wait();
     __syncthreads();
     // ---- one flux per tile edge
-    for (int el = threadIdx.x; el < inf.y; el += blockDim.x) {
+    for (int el = threadIdx.x; el < (PH == 2 ? 0 : inf.y); el += blockDim.x) {
         const uint32_t ij = sij[el];
         const int li = (int)(ij & 0xffff), lj = (int)(ij >> 16);
         const S n0 = snx[el], n1 = sny[el];
         const S* ri = rec + (size_t)li * R::NR;
         const S* rj = rec + (size_t)lj * R::NR;
         FT f[V];
-        if constexpr (FLUX == 5) {
-            ns_edge_flux<M, R>(P, ri, rj, n0, n1, sxf[el], syf[el], sle[el], f);
+        if constexpr (FLUX == 5 || FLUX == 6) {
+            diffusive_edge_flux<M, V, FLUX, R>(P, ri, rj, n0, n1, sxf[el], syf[el], sle[el], f);
         } else {
             S qL[V], qR[V];
             lds<S, V>(ri, qL);
@@ -909,6 +925,7 @@ __global__ void __launch_bounds__(kTileMax) k_tile_stage(TileParams TP, TileIO i
             if (w[f] == kFaceNone) continue;
             const int el = w[f] & kFaceEdgeMask, side = w[f] >> 15;
             has_ghost |= (w[f] & 0x4000) != 0;
+            if (PH == 2) continue;  // the smoothed time derivatives are read below
             FT fe[V];
             lds<FT, V>(sF + (size_t)el * V, fe);
             if constexpr (M::exact) {
@@ -924,10 +941,16 @@ __global__ void __launch_bounds__(kTileMax) k_tile_stage(TileParams TP, TileIO i
             }
         }
         if constexpr (!M::exact) {
-            const double rA = 1.0 / A;
+            if (PH != 2) {
+                const double rA = 1.0 / A;
 #pragma unroll
-            for (int k = 0; k < V; ++k) qt[k] *= rA;
+                for (int k = 0; k < V; ++k) qt[k] *= rA;
+            }
         }
+        if constexpr (PH == 1) {
+            st<double, V>(io.qt, c, qt);
+        } else {
+        if constexpr (PH == 2) ld<double, V>(io.qt, c, qt);
         if (global_dt) {
             // min_dt (explicit.cpp:555-564) of this cell's case; a NaN in its dt[0] wins
             unsigned long long key = s_dtkey;
@@ -1008,8 +1031,9 @@ __global__ void __launch_bounds__(kTileMax) k_tile_stage(TileParams TP, TileIO i
 #pragma unroll
             for (int k = 0; k < V; ++k) res[k] = qt[k] * qt[k] * A;
         }
+        }  // PH != 1
     }
-    if (io.partials != nullptr) {
+    if (PH != 1 && io.partials != nullptr) {
         __shared__ double red[kTileMax / 32][V];
 #pragma unroll
         for (int k = 0; k < V; ++k)
@@ -1047,7 +1071,7 @@ template <class M, int V, bool ORDER2, int FLUX = 0>
 inline size_t smem_stage(const TileParams& TP) {
     using S = typename M::S;
     using FT = typename std::conditional<M::exact, double, S>::type;
-    return (size_t)(TP.T + TP.max_halo) * Rec<M, V, ORDER2, ORDER2, M::exact || FLUX == 5>::NR * sizeof(S) +
+    return (size_t)(TP.T + TP.max_halo) * Rec<M, V, ORDER2, ORDER2, M::exact || FLUX == 5 || FLUX == 6>::NR * sizeof(S) +
            (size_t)TP.max_edges * (V * sizeof(FT) + 5 * sizeof(S) + 4);
 }
 
@@ -1080,6 +1104,9 @@ struct TileLaunch {
             set((const void*)k_tile_gradlim<M, 2, 1>, smem_gradlim<M, 2>(TP));
             set((const void*)k_tile_stage<M, 2, true, 3>, smem_stage<M, 2, true>(TP));
             set((const void*)k_tile_stage<M, 2, false, 3>, smem_stage<M, 2, false>(TP));
+            set((const void*)k_tile_stage<M, 2, true, 6>, smem_stage<M, 2, true, 6>(TP));
+            set((const void*)k_tile_stage<M, 2, true, 6, 1>, smem_stage<M, 2, true, 6>(TP));
+            set((const void*)k_tile_stage<M, 2, true, 6, 2>, smem_stage<M, 2, true, 6>(TP));
         } else {
             set((const void*)k_tile_dt<M, 1>, smem_dt<M, 1>(TP));
             set((const void*)k_tile_gradlim<M, 1, 0>, smem_gradlim<M, 1>(TP));
@@ -1135,10 +1162,16 @@ struct TileLaunch {
             else go(k_tile_gradlim<M, 1, 0>, g, TP.T, smem_gradlim<M, 1>(TP), st, pdl, TP, io);
         }
     }
-    static void stage(const TileParams& TP, const TileIO& io, cudaStream_t st, bool pdl = false) {
+    // phase: 0 the whole stage, 1 time derivatives only, 2 update only (residual smoothing, FLUX 6)
+    static void stage(const TileParams& TP, const TileIO& io, cudaStream_t st, bool pdl = false, int phase = 0) {
         const int g = grid(TP);
         const bool o2 = TP.P.order2 != 0;
-        if (TP.P.flux == 4) {
+        if (TP.P.flux == 6) {
+            const size_t sm = smem_stage<M, 2, true, 6>(TP);
+            if (phase == 1) go(k_tile_stage<M, 2, true, 6, 1>, g, TP.T, sm, st, pdl, TP, io);
+            else if (phase == 2) go(k_tile_stage<M, 2, true, 6, 2>, g, TP.T, sm, st, pdl, TP, io);
+            else go(k_tile_stage<M, 2, true, 6>, g, TP.T, sm, st, pdl, TP, io);
+        } else if (TP.P.flux == 4) {
             go(k_tile_stage<M, 1, true, 4>, g, TP.T, smem_stage<M, 1, true>(TP), st, pdl, TP, io);
         } else if (TP.P.flux == 5) {
             go(k_tile_stage<M, 4, true, 5>, g, TP.T, smem_stage<M, 4, true, 5>(TP), st, pdl, TP, io);
@@ -1163,7 +1196,8 @@ void launch_dt(int precision, const TileParams& TP, const TileIO& io, cudaStream
 // with_dt: also the step's time step (io.dt, io.dtkeys), as launch_dt computes it
 void launch_gradlim(int precision, const TileParams& TP, const TileIO& io, cudaStream_t st, bool with_dt = false,
                     bool pdl = false);
-void launch_stage(int precision, const TileParams& TP, const TileIO& io, cudaStream_t st, bool pdl = false);
+void launch_stage(int precision, const TileParams& TP, const TileIO& io, cudaStream_t st, bool pdl = false,
+                  int phase = 0);
 }  // namespace tile
 
 }  // namespace fvgpu

@@ -11,8 +11,8 @@ void launch_dt_exact(const TileParams& TP, const TileIO& io, cudaStream_t st, bo
 void launch_gradlim_exact(const TileParams& TP, const TileIO& io, cudaStream_t st, bool with_dt, bool pdl) {
     TileLaunch<MExact>::gradlim(TP, io, st, with_dt, pdl);
 }
-void launch_stage_exact(const TileParams& TP, const TileIO& io, cudaStream_t st, bool pdl) {
-    TileLaunch<MExact>::stage(TP, io, st, pdl);
+void launch_stage_exact(const TileParams& TP, const TileIO& io, cudaStream_t st, bool pdl, int phase) {
+    TileLaunch<MExact>::stage(TP, io, st, pdl, phase);
 }
 }  // namespace tile
 }  // namespace fvgpu

@@ -7,7 +7,7 @@ namespace tile {
 cudaError_t prepare_exact(const TileParams& TP);
 void launch_dt_exact(const TileParams& TP, const TileIO& io, cudaStream_t st, bool pdl);
 void launch_gradlim_exact(const TileParams& TP, const TileIO& io, cudaStream_t st, bool with_dt, bool pdl);
-void launch_stage_exact(const TileParams& TP, const TileIO& io, cudaStream_t st, bool pdl);
+void launch_stage_exact(const TileParams& TP, const TileIO& io, cudaStream_t st, bool pdl, int phase);
 
 cudaError_t prepare(int precision, const TileParams& TP) {
     if (precision == 0) return prepare_exact(TP);
@@ -24,10 +24,10 @@ void launch_gradlim(int precision, const TileParams& TP, const TileIO& io, cudaS
     else if (precision == 1) TileLaunch<MF64>::gradlim(TP, io, st, with_dt, pdl);
     else TileLaunch<MF32>::gradlim(TP, io, st, with_dt, pdl);
 }
-void launch_stage(int precision, const TileParams& TP, const TileIO& io, cudaStream_t st, bool pdl) {
-    if (precision == 0) launch_stage_exact(TP, io, st, pdl);
-    else if (precision == 1) TileLaunch<MF64>::stage(TP, io, st, pdl);
-    else TileLaunch<MF32>::stage(TP, io, st, pdl);
+void launch_stage(int precision, const TileParams& TP, const TileIO& io, cudaStream_t st, bool pdl, int phase) {
+    if (precision == 0) launch_stage_exact(TP, io, st, pdl, phase);
+    else if (precision == 1) TileLaunch<MF64>::stage(TP, io, st, pdl, phase);
+    else TileLaunch<MF32>::stage(TP, io, st, pdl, phase);
 }
 }  // namespace tile
 }  // namespace fvgpu

@@ -17,10 +17,10 @@ import physics as _phys
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libfvgpu.so")
 
-FLUX = {"roe_fs": 1, "roe_st": 2, "burgers": 3, "diffusion": 4, "ns": 5}
+FLUX = {"roe_fs": 1, "roe_st": 2, "burgers": 3, "diffusion": 4, "ns": 5, "burgers_diffusion": 6}
 LIMITER = {"zero": 0, "michalak": 1, "venkat": 2, "minmod": 3}
 DT = {"const": 0, "cfl_sum": 1, "cfl_min_signed": 2, "visc_min": 3, "visc_sum": 4}
-BC = {"copy": 0, "wall": 1, "inlet_outlet": 2, "farfield": 3, "noslip": 4, "farfield_b0": 5}
+BC = {"copy": 0, "wall": 1, "inlet_outlet": 2, "farfield": 3, "noslip": 4, "farfield_b0": 5, "tangent": 6}
 PREC = {"fp64_exact": 0, "fp64": 1, "fp32": 2}
 
 _dp = C.POINTER(C.c_double)
@@ -41,7 +41,7 @@ class _Physics(C.Structure):
                 ("cfl", C.c_double), ("dt_const", C.c_double), ("n_groups", C.c_int32),
                 ("group_bc", _i32p), ("group_bv", _dp), ("positivity_guard", C.c_int32),
                 ("diffusive", C.c_int32), ("mu", C.c_double), ("pr", C.c_double), ("cp", C.c_double),
-                ("r", C.c_double)]
+                ("r", C.c_double), ("smooth_residuals", C.c_int32)]
 
 
 _PRINT_CB = C.CFUNCTYPE(None, C.c_void_p, C.c_uint64, C.c_double, _dp, C.c_int32)
@@ -207,6 +207,7 @@ def physics_struct(ph: _phys.Physics, group_names: Sequence[str]):
     s.positivity_guard = int(getattr(ph, "positivity_guard", False))
     s.diffusive = int(getattr(ph, "diffusive", False))
     s.mu, s.pr, s.cp, s.r = ph.mu, ph.pr, ph.cp, ph.r
+    s.smooth_residuals = int(getattr(ph, "smooth", False))
     s._keep = (gbc, gbv)
     return s
 

@@ -13,7 +13,9 @@ examples define as device kinds, selected by name:
             with the face gradient of gradient_for_diffusion, explicit.cpp:70-109),
             ``ns`` (examples/flatPlate/main.cpp:126-225 = nacaTransient/main.cpp:130-229:
             the roe_st flux minus viscous stresses and heat conduction from the face
-            gradient; constants mu, pr, cp, r)
+            gradient; constants mu, pr, cp, r),
+            ``burgers_diffusion`` (tests/tests.cpp:76-117, V = 2: burgers plus
+            -grad q . n per variable from the face gradient)
 * limiter:  ``zero`` (shockTube/main.cpp:60-62), ``michalak``
             (forwardStep/main.cpp:57-66), ``minmod`` (burgers/main.cpp:51-53),
             ``venkat`` (Venkatakrishnan 1995, not in the reference)
@@ -25,7 +27,8 @@ examples define as device kinds, selected by name:
             (forwardStep/main.cpp:262-269), ``inlet_outlet``
             (forwardStep/main.cpp:194-261), ``farfield`` (naca/main.cpp:192-259),
             ``farfield_b0`` (flatPlate/main.cpp:286-352: farfield with
-            b[2] = b[0]*(...)), ``noslip`` (flatPlate/main.cpp:361-366);
+            b[2] = b[0]*(...)), ``noslip`` (flatPlate/main.cpp:361-366),
+            ``tangent`` (tests/tests.cpp:132-135, V = 2: b = (-n_y, n_x));
             the inflow/far-field kinds take the far-field state bv[4].
 """
 from __future__ import annotations
@@ -62,6 +65,9 @@ class Physics:
     pr: float = 1.0
     cp: float = 1.0
     r: float = 1.0
+    # solver::smooth_residuals: two Jacobi sweeps of implicit residual
+    # smoothing after each stage's time derivatives (explicit.cpp:32-66, 743)
+    smooth: bool = False
 
 
 def euler_state(rho, u, v, p, gamma=1.4):
@@ -139,6 +145,14 @@ def naca_transient(cfl=1.5, mach=0.8):
     return Physics(V=4, flux="ns", order2=False, limiter="michalak", K=7.5, dt_kind="visc_sum", cfl=cfl,
                    global_dt=True, diffusive=True, **NS_CONSTS,
                    bcs={"wall": ("noslip", None), "farfield": ("farfield_b0", bv)})
+
+
+def burgers_diffusion(dt=1e-3):
+    """The reference's regression-test physics (tests/tests.cpp:40-150):
+    Burgers advection plus diffusion, MUSCL with minmod, residual smoothing,
+    local constant dt, tangential boundary state."""
+    return Physics(V=2, flux="burgers_diffusion", order2=True, limiter="minmod", K=7.5, dt_kind="const",
+                   dt_const=dt, global_dt=False, diffusive=True, smooth=True, bcs={"wall": ("tangent", None)})
 
 
 def burgers(dt=1e-4):

@@ -217,6 +217,9 @@ void identify_diffusive_flux(int V, fv_physics* ph) {
     if (V == 1) {
         ph->flux = FV_FLUX_DIFFUSION;
         ph->gamma = 1.4;
+    } else if (V == 2) {
+        ph->flux = FV_FLUX_BURGERS_DIFF;
+        ph->gamma = 1.4;
     } else if (V == 4) {
         if (!&consts::mu || !&consts::pr || !&consts::cp || !&consts::r)
             throw std::invalid_argument("fvhyper GPU: a vars = 4 calc_flux with diffusive_gradients runs as the "
@@ -227,13 +230,14 @@ void identify_diffusive_flux(int V, fv_physics* ph) {
         ph->mu = consts::mu; ph->pr = consts::pr; ph->cp = consts::cp; ph->r = consts::r;
     } else {
         throw std::invalid_argument("fvhyper GPU: diffusive_gradients with vars = " + std::to_string(V) +
-                                    " matches no device kind (vars = 1 diffusion, vars = 4 Navier-Stokes)");
+                                    " matches no device kind (vars = 1 diffusion, vars = 2 Burgers-diffusion, "
+                                    "vars = 4 Navier-Stokes)");
     }
     Probe pr;
     for (int t = 0; t < 256; ++t) {
         double qi[4] = {0, 0, 0, 0}, qj[4] = {0, 0, 0, 0}, gx[4], gy[4], n[2];
         if (V == 4) { pr.euler(qi, ph->gamma); pr.euler(qj, ph->gamma); }
-        else { qi[0] = pr.uni(-2, 2); qj[0] = pr.uni(-2, 2); }
+        else for (int k = 0; k < V; ++k) { qi[k] = pr.uni(-2, 2); qj[k] = pr.uni(-2, 2); }
         for (int k = 0; k < 4; ++k) { gx[k] = pr.uni(-5, 5); gy[k] = pr.uni(-5, 5); }
         pr.normal(n);
         double fu[4] = {0, 0, 0, 0}, fk[4] = {0, 0, 0, 0};
@@ -242,8 +246,9 @@ void identify_diffusive_flux(int V, fv_physics* ph) {
         for (int c = 0; c < V; ++c)
             if (!same_bits(fu[c], fk[c]))
                 throw std::invalid_argument(std::string("fvhyper GPU: calc_flux (diffusive_gradients) is not the ") +
-                                            (V == 1 ? "diffusion flux -grad(u).n of examples/heatTransfer"
-                                                    : "Navier-Stokes flux of examples/flatPlate") +
+                                            (V == 1   ? "diffusion flux -grad(u).n of examples/heatTransfer"
+                                             : V == 2 ? "Burgers-diffusion flux of tests/tests.cpp"
+                                                      : "Navier-Stokes flux of examples/flatPlate") +
                                             "; no device kind matches it");
     }
 }
@@ -318,6 +323,7 @@ int32_t identify_limiter() {
 void identify_bc(const std::string& name, void (*fn)(double*, double*, double*), int V, double gamma,
                  int32_t* kind, double* bv) {
     std::vector<int> kinds = {FV_BC_COPY};
+    if (V == 2) kinds.push_back(FV_BC_TANGENT);
     if (V == 4) {
         kinds.push_back(FV_BC_WALL);
         kinds.push_back(FV_BC_NOSLIP);
@@ -359,7 +365,7 @@ void identify_bc(const std::string& name, void (*fn)(double*, double*, double*),
     }
     throw std::invalid_argument("fvhyper GPU: boundary function \"" + name +
                                 "\" matches no device boundary kind (copy, wall, no-slip wall, inlet_outlet, "
-                                "farfield, farfield with b[0] tangential momentum)");
+                                "farfield, farfield with b[0] tangential momentum, tangent)");
 }
 
 // A small jittered triangle mesh for probing calc_dt (the user function only
@@ -529,8 +535,6 @@ void run(const std::string name, std::vector<double>& q, mpi_wrapper& pool, mesh
     q.resize((size_t)V * m.cellsAreas.size());
     generate_initial_solution(q, m);
 
-    if (solver::smooth_residuals)
-        throw std::invalid_argument("fvhyper GPU: smooth_residuals is not on the device path");
     const bool D = solver::diffusive_gradients;
     const bool o2 = solver::do_calc_gradients && solver::do_calc_limiters && solver::linear_interpolate;
     const bool o1 = !solver::do_calc_gradients && !solver::do_calc_limiters && !solver::linear_interpolate && !D;
@@ -551,6 +555,10 @@ void run(const std::string name, std::vector<double>& q, mpi_wrapper& pool, mesh
     else identify_flux(V, &ph.flux, &ph.gamma);
     ph.order2 = o2 ? 1 : 0;
     ph.diffusive = D ? 1 : 0;
+    if (solver::smooth_residuals && ph.flux != FV_FLUX_BURGERS_DIFF)
+        throw std::invalid_argument("fvhyper GPU: smooth_residuals runs on the device with the Burgers-diffusion "
+                                    "kind only (the physics of tests/tests.cpp)");
+    ph.smooth_residuals = solver::smooth_residuals ? 1 : 0;
     ph.limiter = o2 ? identify_limiter() : FV_LIM_ZERO;
     ph.K = solver::limiter_k_value;
     ph.global_dt = solver::global_dt ? 1 : 0;

@@ -46,8 +46,12 @@ typedef enum {
 /* Physics kinds implemented on the device (see finite-volume-2d-cpp_b200/physics.py). */
 /* FV_FLUX_NS: the compressible Navier-Stokes flux of examples/flatPlate and
  * examples/nacaTransient (FV_FLUX_ROE_ST minus the viscous stresses and heat
- * conduction from the face gradient; mu, pr, cp, r below). */
-enum { FV_FLUX_ROE_FS = 1, FV_FLUX_ROE_ST = 2, FV_FLUX_BURGERS = 3, FV_FLUX_DIFFUSION = 4, FV_FLUX_NS = 5 };
+ * conduction from the face gradient; mu, pr, cp, r below).
+ * FV_FLUX_BURGERS_DIFF: FV_FLUX_BURGERS plus -(grad q . n) per variable from
+ * the face gradient, the reference's regression-test physics
+ * (tests/tests.cpp:76-117, V = 2). */
+enum { FV_FLUX_ROE_FS = 1, FV_FLUX_ROE_ST = 2, FV_FLUX_BURGERS = 3, FV_FLUX_DIFFUSION = 4, FV_FLUX_NS = 5,
+       FV_FLUX_BURGERS_DIFF = 6 };
 enum { FV_LIM_ZERO = 0, FV_LIM_MICHALAK = 1, FV_LIM_VENKAT = 2, FV_LIM_MINMOD = 3 };
 /* VISC_MIN (examples/flatPlate/main.cpp:230-277) and VISC_SUM
  * (examples/nacaTransient/main.cpp:234-285): convective + 2 x viscous
@@ -56,8 +60,9 @@ enum { FV_DT_CONST = 0, FV_DT_CFL_SUM = 1, FV_DT_CFL_MIN_SIGNED = 2, FV_DT_VISC_
 /* NOSLIP: b = (rho, -rho u, -rho v, rho E) (examples/flatPlate/main.cpp:361-366).
  * FARFIELD_B0: FARFIELD with b[2] = b[0]*(...) in the subsonic branches
  * (examples/flatPlate/main.cpp:286-352, nacaTransient/main.cpp:294-360). */
+/* TANGENT (V = 2): the fixed state b = (-n_y, n_x) of tests/tests.cpp:132-135. */
 enum { FV_BC_COPY = 0, FV_BC_WALL = 1, FV_BC_INLET_OUTLET = 2, FV_BC_FARFIELD = 3, FV_BC_NOSLIP = 4,
-       FV_BC_FARFIELD_B0 = 5 };
+       FV_BC_FARFIELD_B0 = 5, FV_BC_TANGENT = 6 };
 
 /* Arithmetic of the step.
  * FP64_EXACT: FP64, the reference's evaluation order, no FMA contraction:
@@ -94,6 +99,11 @@ typedef struct {
                                   copy boundaries: examples/heatTransfer) and FV_FLUX_NS */
     double mu, pr, cp, r;      /* viscosity, Prandtl number, heat capacity, gas constant of
                                   FV_FLUX_NS and the viscous dt kinds (the examples' consts::) */
+    int32_t smooth_residuals;  /* solver::smooth_residuals: two Jacobi sweeps of implicit
+                                  residual smoothing (explicit.cpp:32-66) after each stage's
+                                  time derivatives, in fv_run; with FV_FLUX_BURGERS_DIFF (the
+                                  only physics of the reference that uses it).  The stage-level
+                                  entry points do not smooth. */
 } fv_physics;
 
 typedef struct {

@@ -226,6 +226,10 @@ void fvo_flux_grad(const fvo_physics* ph, double* f, const double* qi, const dou
                    const double* gy, const double* n) {
     if (ph->flux == FVO_FLUX_DIFFUSION) {
         f[0] = -(gx[0] * n[0] + gy[0] * n[1]);
+    } else if (ph->flux == FVO_FLUX_BURGERS_DIFF) {  /* tests/tests.cpp:94-116 */
+        burgers(f, qi, qj, n);
+        f[0] += -(gx[0] * n[0] + gy[0] * n[1]);
+        f[1] += -(gx[1] * n[0] + gy[1] * n[1]);
     } else if (ph->flux == FVO_FLUX_NS) {
         roe(ph->gamma, 0, f, qi, qj, n);
         ns_viscous(ph, f, qi, qj, gx, gy, n);
@@ -300,6 +304,11 @@ static void bc_state(const fvo_physics* ph, int group, const double* bv, double*
         b[1] = q[1] - 2.0 * n[0] * (n[0] * q[1] + n[1] * q[2]);
         b[2] = q[2] - 2.0 * n[1] * (n[0] * q[1] + n[1] * q[2]);
         b[3] = q[3];
+        return;
+    }
+    if (kind == FVO_BC_TANGENT) {
+        b[0] = -n[1];
+        b[1] = n[0];
         return;
     }
     if (kind == FVO_BC_NOSLIP) {
@@ -632,6 +641,36 @@ void fvo_update_bounds(const fvo_mesh* m, const fvo_physics* ph, double* q, cons
     }
 }
 
+/* Implicit residual smoothing, explicit.cpp:32-66: two Jacobi sweeps of
+ * (1 + ne eps) r_i - eps sum_j r_j = qt_i (eps = 0.6, ne = 3 or 4 faces), the
+ * neighbour sums accumulated in edge order; ghosts keep qt = 0. */
+void fvo_smooth_residuals(const fvo_mesh* m, const fvo_physics* ph, double* qt) {
+    const int V = ph->V;
+    const double epsilon = 0.6;
+    const size_t n = (size_t)V * m->n_total;
+    double* qt0 = malloc(n * 8);
+    double* s = malloc(n * 8);
+    int* ne = calloc((size_t)m->n_total, sizeof(int));
+    for (int64_t e = 0; e < m->n_edges; ++e) { ne[m->edge_cells[2 * e]]++; ne[m->edge_cells[2 * e + 1]]++; }
+    memcpy(qt0, qt, n * 8);
+    for (int it = 0; it < 2; ++it) {
+        for (size_t i = 0; i < n; ++i) s[i] = 0.;
+        for (int64_t e = 0; e < m->n_edges; ++e) {
+            uint32_t i = m->edge_cells[2 * e], j = m->edge_cells[2 * e + 1];
+            for (int k = 0; k < V; ++k) {
+                s[(size_t)V * i + k] -= qt[(size_t)V * j + k] * epsilon;
+                s[(size_t)V * j + k] -= qt[(size_t)V * i + k] * epsilon;
+            }
+        }
+        for (int64_t i = 0; i < m->n_real; ++i) {
+            const double nf = ne[i] == 3 ? 3 : 4;  /* cellsIsTriangle ? 3 : 4 */
+            for (int k = 0; k < V; ++k)
+                qt[(size_t)V * i + k] = (qt0[(size_t)V * i + k] - s[(size_t)V * i + k]) / (1. + nf * epsilon);
+        }
+    }
+    free(qt0); free(s); free(ne);
+}
+
 /* Residual norms, explicit.cpp:481-496 (single rank). */
 void fvo_calc_residuals(const fvo_mesh* m, const fvo_physics* ph, const double* qt, double* R) {
     const int V = ph->V;
@@ -668,6 +707,7 @@ int fvo_run_loop(const fvo_mesh* m, const fvo_physics* ph, double* q, const doub
             if (ph->order2 || ph->diffusive) fvo_calc_gradients(m, ph, qk, gx, gy);
             if (ph->order2) fvo_calc_limiters(m, ph, qk, gx, gy, lim);
             fvo_calc_time_derivatives(m, ph, qk, gx, gy, lim, qt);
+            if (ph->smooth) fvo_smooth_residuals(m, ph, qt);  /* explicit.cpp:743 */
             for (int64_t i = 0; i < m->n_total; ++i) /* update_cells, explicit.cpp:368-378 */
                 for (int k = 0; k < V; ++k) {
                     size_t kk = (size_t)V * i + k;

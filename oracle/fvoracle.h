@@ -35,8 +35,10 @@ typedef struct {
    compressible Navier-Stokes flux of examples/flatPlate and
    examples/nacaTransient (the shockTube Roe flux plus viscous stresses and
    heat conduction from the face gradient). */
+/* BURGERS_DIFF: the upwind advection flux plus -(grad q . n) per variable
+   from the face gradient (tests/tests.cpp:76-117, V = 2). */
 enum { FVO_FLUX_ROE_FS = 1, FVO_FLUX_ROE_ST = 2, FVO_FLUX_BURGERS = 3, FVO_FLUX_DIFFUSION = 4,
-       FVO_FLUX_NS = 5 };
+       FVO_FLUX_NS = 5, FVO_FLUX_BURGERS_DIFF = 6 };
 enum { FVO_LIM_ZERO = 0, FVO_LIM_MICHALAK = 1, FVO_LIM_VENKAT = 2, FVO_LIM_MINMOD = 3 };
 /* VISC_MIN: examples/flatPlate/main.cpp:230-277; VISC_SUM:
    examples/nacaTransient/main.cpp:234-288 (convective + viscous eigenvalues). */
@@ -45,8 +47,9 @@ enum { FVO_DT_CONST = 0, FVO_DT_CFL_SUM = 1, FVO_DT_CFL_MIN_SIGNED = 2, FVO_DT_V
 /* NOSLIP: the viscous wall of examples/flatPlate/main.cpp:361-366.
    FARFIELD_B0: the far field of examples/flatPlate/main.cpp:284-352, whose
    tangential momentum is b[0]*(...) where examples/naca has b[1]*(...). */
+/* TANGENT: b = (-n_y, n_x), the fixed tangential state of tests/tests.cpp:132-135 (V = 2). */
 enum { FVO_BC_COPY = 0, FVO_BC_WALL = 1, FVO_BC_INLET_OUTLET = 2, FVO_BC_FARFIELD = 3,
-       FVO_BC_NOSLIP = 4, FVO_BC_FARFIELD_B0 = 5 };
+       FVO_BC_NOSLIP = 4, FVO_BC_FARFIELD_B0 = 5, FVO_BC_TANGENT = 6 };
 
 typedef struct {
     int V;
@@ -69,6 +72,7 @@ typedef struct {
                                  computed, no limiter, no interpolation) */
     double mu, pr, cp, r;     /* viscosity, Prandtl number, heat capacity, gas constant
                                  (consts:: of the Navier-Stokes examples) */
+    int smooth;               /* solver::smooth_residuals (explicit.cpp:32-66, 743) */
 } fvo_physics;
 
 int fvo_mesh_build(int64_t n_nodes, const double* nodes_x, const double* nodes_y,
@@ -92,6 +96,8 @@ void fvo_calc_time_derivatives(const fvo_mesh* m, const fvo_physics* ph, const d
 void fvo_update_bounds(const fvo_mesh* m, const fvo_physics* ph, double* q, const double* gx,
                        const double* gy, const double* lim);
 void fvo_calc_residuals(const fvo_mesh* m, const fvo_physics* ph, const double* qt, double* R);
+/* Implicit residual smoothing, explicit.cpp:32-66 (2 Jacobi sweeps, epsilon 0.6), in place on qt. */
+void fvo_smooth_residuals(const fvo_mesh* m, const fvo_physics* ph, double* qt);
 
 int fvo_run_loop(const fvo_mesh* m, const fvo_physics* ph, double* q_io, const double* alpha,
                  int n_alpha, uint64_t max_step, double max_time, double tolerance,

@@ -20,10 +20,10 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF_DIR = os.path.join(HERE, "_ref")
 
-FLUX = {"roe_fs": 1, "roe_st": 2, "burgers": 3, "diffusion": 4, "ns": 5}
+FLUX = {"roe_fs": 1, "roe_st": 2, "burgers": 3, "diffusion": 4, "ns": 5, "burgers_diffusion": 6}
 LIMITER = {"zero": 0, "michalak": 1, "venkat": 2, "minmod": 3}
 DT = {"const": 0, "cfl_sum": 1, "cfl_min_signed": 2, "visc_min": 3, "visc_sum": 4}
-BC = {"copy": 0, "wall": 1, "inlet_outlet": 2, "farfield": 3, "noslip": 4, "farfield_b0": 5}
+BC = {"copy": 0, "wall": 1, "inlet_outlet": 2, "farfield": 3, "noslip": 4, "farfield_b0": 5, "tangent": 6}
 
 _dp = C.POINTER(C.c_double)
 _u32p = C.POINTER(C.c_uint32)
@@ -49,7 +49,7 @@ class _FvoPhysics(C.Structure):
                 ("cfl", C.c_double), ("dt_const", C.c_double), ("global_dt", C.c_int),
                 ("n_groups", C.c_int), ("group_bc", _i32p), ("group_bv", _dp), ("positivity_guard", C.c_int),
                 ("ghost_bv", _dp), ("diffusive", C.c_int), ("mu", C.c_double), ("pr", C.c_double),
-                ("cp", C.c_double), ("r", C.c_double)]
+                ("cp", C.c_double), ("r", C.c_double), ("smooth", C.c_int)]
 
 
 def build_oracle():
@@ -136,6 +136,7 @@ class Oracle:
         p.positivity_guard = int(getattr(phys, "positivity_guard", False))
         p.diffusive = int(getattr(phys, "diffusive", False))
         p.mu, p.pr, p.cp, p.r = phys.mu, phys.pr, phys.cp, phys.r
+        p.smooth = int(getattr(phys, "smooth", False))
         gh = None
         if ghost_bv is not None:
             gh = np.ascontiguousarray(ghost_bv, np.float64).reshape(-1)
@@ -186,6 +187,11 @@ class Oracle:
                               C.c_uint64(max_step), C.c_double(max_time), C.c_double(tolerance),
                               C.c_uint64(print_interval), C.byref(step), C.byref(t), _ptr(R), _ptr(qt))
         return dict(q=q, step=step.value, time=t.value, R=R, qt=qt)
+
+    def smooth_residuals(self, g, p, qt):
+        qt = np.ascontiguousarray(qt, np.float64).copy()
+        self.lib.fvo_smooth_residuals(C.byref(g.struct()), C.byref(p), _ptr(qt))
+        return qt
 
     def flux(self, p, qi, qj, n):
         f = np.zeros(p.V)
@@ -307,6 +313,11 @@ class RefLib:
         self.lib.ref_flux(_ptr(f), _ptr(np.ascontiguousarray(qi, np.float64)),
                           _ptr(np.ascontiguousarray(qj, np.float64)), _ptr(np.ascontiguousarray(n, np.float64)))
         return f
+
+    def smooth_residuals(self, qt):
+        t = np.ascontiguousarray(qt, np.float64).copy()
+        self.lib.ref_smooth_residuals(_ptr(t))
+        return t
 
     def flux_grad(self, qi, qj, gx, gy, n):
         f = np.zeros(self.V)

@@ -48,7 +48,7 @@ extern double gamma;
 extern double gamma; extern double cfl;
 #elif defined(FVREF_EX_NACATRANSIENT)
 extern double gamma; extern double cfl; extern double mach;
-#endif  // heatTransfer and burgers have no consts:: globals
+#endif  // heatTransfer, burgers and the regression-test physics have no consts:: globals
 }
 
 #if FVREF_OVERRIDE
@@ -213,6 +213,13 @@ void ref_calc_time_derivatives(const double* q, const double* gx, const double* 
     std::vector<double> qv = vec(q, nq()), a = vec(gx, nq()), b = vec(gy, nq());
     std::vector<double> l = vec(lim, nq()), t(nq());
     fvhyper::calc_time_derivatives(t, qv, a, b, l, *g_mesh);
+    put(qt, t);
+}
+
+/* Residual smoothing (explicit.cpp:32-66) of qt, in place. */
+void ref_smooth_residuals(double* qt) {
+    std::vector<double> t = vec(qt, nq()), s0(nq()), s1(nq());
+    fvhyper::smooth_residuals(t, s0, s1, *g_mesh);
     put(qt, t);
 }
 

@@ -71,6 +71,10 @@ CASES = {
                            phys=lambda: P.naca_transient(),
                            ic=lambda g: P.ic_forward_step(g.n_total, mach=0.8).ravel(),
                            alpha=P.RK5_ALPHA, steps=30, ref="nacaTransient", alias={}, consts={}),
+    "burgers_diffusion": dict(mesh=lambda: meshgen.rect_tri(16, 16, 1.0, 1.0, side_names=("wall", "wall")),
+                              phys=lambda: P.burgers_diffusion(),
+                              ic=lambda g: np.zeros(g.n_total * 2), alpha=P.RK5_ALPHA, steps=30, ref="tests",
+                              alias={}, consts={}),
     "burgers": dict(mesh=lambda: meshgen.rect_tri(16, 16, 1.0, 1.0, side_names=("wall", "wall")),
                     phys=lambda: P.burgers(), ic=lambda g: P.ic_burgers(g.ccx, g.ccy).ravel(),
                     alpha=P.RK5_ALPHA, steps=30, ref="burgers", alias={}, consts={}),

@@ -145,6 +145,22 @@ def test_diffusive_fluxes_with_face_gradients(oracle):
             assert bits_equal(oracle.flux_grad(p, qi, qj, gx, gy, n), ref.flux_grad(qi, qj, gx, gy, n))
 
 
+def test_residual_smoothing_bitwise(oracle):
+    """smooth_residuals (explicit.cpp:32-66) on a random residual, triangle
+    and quadrilateral meshes: the restatement equals the reference."""
+    for name in ("burgers_diffusion", "flat_plate"):
+        case = CASES[name]
+        em = case["mesh"]()
+        em.bnd_group[:] = 0          # one "wall" group: the only name the test physics defines
+        em.group_names = ["wall"]
+        ref = make_ref(dict(case, ref="tests", consts={}), em)
+        g = oracle.build_mesh(em)
+        p = oracle.physics(CASES["burgers_diffusion"]["phys"](), em.group_names)
+        qt = np.random.default_rng(3).normal(size=g.n_total * 2)
+        qt[g.n_real * 2:] = 0.0   # the time derivative leaves ghosts at 0
+        assert bits_equal(oracle.smooth_residuals(g, p, qt), ref.smooth_residuals(qt))
+
+
 def test_missing_boundary_edge_rejected(oracle):
     em = meshgen.sod_strip(8, 2)
     em.bnd_nodes = em.bnd_nodes.copy()

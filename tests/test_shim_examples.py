@@ -179,38 +179,41 @@ def test_binary_vtu_holds_the_state(tmp_path):
     assert b["offsets"][-1] == b["connectivity"].size
 
 
-# A user program with physics no device kind implements: two variables with
-# diffusive fluxes (advection plus diffusion), optionally residual smoothing.
-_UNSUPPORTED_PROGRAM = r"""
+# User programs in the fvhyper API (our own code): VARS variables with
+# diffusive fluxes; FLUX is the body of calc_flux, BC of the boundary
+# function, SMOOTH the residual-smoothing flag.
+_PROGRAM = r"""
 #include <fvhyper/mesh.h>
 #include <fvhyper/explicit.h>
 #include <fvhyper/parallel.h>
 #include <fvhyper/post.h>
+#include <algorithm>
+#include <cmath>
 namespace fvhyper {
-const int vars = 2;
-const std::vector<std::string> var_names = {"a", "b"};
+const int vars = VARS;
+const std::vector<std::string> var_names = NAMES;
 namespace solver {
 const bool do_calc_gradients = true;
-const bool do_calc_limiters = false;
-const bool linear_interpolate = false;
+const bool do_calc_limiters = ORDER2;
+const bool linear_interpolate = ORDER2;
 const bool diffusive_gradients = true;
-const bool global_dt = true;
+const bool global_dt = false;
 const bool smooth_residuals = SMOOTH;
 }
 void generate_initial_solution(std::vector<double>& q, const mesh& m) {
-    for (uint i = 0; i < m.cellsAreas.size(); ++i) { q[2 * i] = m.cellsCentersX[i]; q[2 * i + 1] = 1.0; }
+    for (double& x : q) x = 0.0;
 }
-double limiter_func(const double& y) { return 0.0; }
+double limiter_func(const double& y) { return std::max(0., std::min(1., y)); }
 void calc_flux(double* f, const double* qi, const double* qj, const double* gx, const double* gy,
                const double* n) {
-    for (int k = 0; k < 2; ++k) f[k] = 0.5 * (qi[k] + qj[k]) * n[0] - 0.01 * (gx[k] * n[0] + gy[k] * n[1]);
+    FLUX
 }
 void calc_dt(std::vector<double>& dt, const std::vector<double>& q, mesh& m) {
-    for (double& d : dt) d = 1e-4;
+    for (double& d : dt) d = 1e-3;
 }
 namespace boundaries {
-void copy(double* b, double* q, double* n) { b[0] = q[0]; b[1] = q[1]; }
-std::map<std::string, void (*)(double*, double*, double*)> bounds = {{"wall", copy}};
+void side(double* b, double* q, double* n) { BC }
+std::map<std::string, void (*)(double*, double*, double*)> bounds = {{"wall", side}};
 }
 namespace post {
 std::map<std::string, void (*)(double*, double*)> extra_scalars = {};
@@ -222,31 +225,72 @@ int main() {
     fvhyper::mesh m;
     m.read_file("square", pool);
     fvhyper::solverOptions options;
-    options.max_step = 10;
+    options.max_step = STEPS;
+    options.print_interval = 10;
     std::vector<double> q;
     fvhyper::run("square", q, pool, m, options);
+    fvhyper::writeVtk("square", q, m, pool.rank, pool.size);
     return pool.exit();
 }
 """
+# upwind advection plus -(grad q . n): the Burgers-diffusion kind
+_BURGERS_DIFF = ("double a = qi[0] * n[0] + qi[1] * n[1], c = qj[0] * n[0] + qj[1] * n[1];"
+                 "double s = std::max(std::abs(a), std::abs(c));"
+                 "for (int k = 0; k < 2; ++k) {"
+                 "  f[k] = 0.5 * (a * qi[k] + c * qj[k]) - 0.5 * s * (qj[k] - qi[k]);"
+                 "  f[k] += -(gx[k] * n[0] + gy[k] * n[1]); }")
 
 
-@pytest.mark.parametrize("smooth,message", [("false", "diffusive_gradients with vars = 2"),
-                                            ("true", "smooth_residuals")])
-def test_unsupported_physics_is_refused(smooth, message, tmp_path):
-    """Refused in run() before any device work, as an uncaught
-    std::invalid_argument naming what has no device kind."""
+def _build_program(tmp_path, **kw):
     shim = os.path.join(PKG, "libfvhyper_gpu.a")
     if not os.path.exists(shim) or shutil.which("g++") is None:
         pytest.skip("needs the built shim and g++")
-    src = tmp_path / "main.cpp"
-    src.write_text(_UNSUPPORTED_PROGRAM.replace("SMOOTH", smooth))
+    src = _PROGRAM
+    for k, v in dict(dict(VARS="2", NAMES='{"u", "v"}', ORDER2="true", SMOOTH="true", STEPS="30",
+                          FLUX=_BURGERS_DIFF, BC="b[0] = -n[1]; b[1] = n[0];"), **kw).items():
+        src = src.replace(k, v)
+    (tmp_path / "main.cpp").write_text(src)
     exe = str(tmp_path / "prog")
-    subprocess.run(["g++", "-O1", "-std=c++17", "-I" + os.path.join(ROOT, "include"), str(src), shim,
-                    "-L" + PKG, "-lfvgpu", "-Wl,-rpath," + PKG, "-o", exe], check=True, timeout=300)
-    meshgen.write_msh41(str(tmp_path / "square.msh"), _one_group(meshgen.rect_tri(6, 5, 1.0, 1.0), "wall"))
+    subprocess.run(["g++", "-O1", "-std=c++17", "-ffp-contract=off", "-I" + os.path.join(ROOT, "include"),
+                    str(tmp_path / "main.cpp"), shim, "-L" + PKG, "-lfvgpu", "-Wl,-rpath," + PKG, "-o", exe],
+                   check=True, timeout=300)
+    meshgen.write_msh41(str(tmp_path / "square.msh"), _one_group(meshgen.rect_tri(8, 8, 1.0, 1.0), "wall"))
+    return exe
+
+
+@pytest.mark.parametrize("kw,message", [
+    (dict(FLUX="for (int k = 0; k < 2; ++k) f[k] = 0.5 * (qi[k] + qj[k]) * n[0] - 0.01 * gx[k];"),
+     "no device kind matches"),
+    (dict(VARS="1", NAMES='{"T"}', ORDER2="false", FLUX="f[0] = -(gx[0] * n[0] + gy[0] * n[1]);",
+          BC="b[0] = q[0];"), "smooth_residuals runs on the device with the Burgers-diffusion kind only"),
+])
+def test_unsupported_physics_is_refused(kw, message, tmp_path):
+    """Refused in run() before any device work, as an uncaught
+    std::invalid_argument naming what has no device kind."""
+    exe = _build_program(tmp_path, **kw)
     r = subprocess.run([exe], cwd=str(tmp_path), capture_output=True, text=True, timeout=120)
     assert r.returncode != 0
     assert "std::invalid_argument" in r.stderr and message in r.stderr, r.stderr
+
+
+@pytest.mark.gpu
+def test_smoothed_burgers_diffusion_program_runs(tmp_path, oracle):
+    """A program with the physics of the reference's regression test
+    (Burgers + diffusion, MUSCL with minmod, residual smoothing, tangential
+    boundary state) runs through the shim as the Burgers-diffusion kind with
+    smoothing; its VTU holds the oracle's state after 30 steps (6 decimals)."""
+    import physics as P
+    exe = _build_program(tmp_path)
+    env = dict(os.environ, FVGPU_VTK_FORMAT="ascii", FVGPU_PRECISION="fp64_exact")
+    r = subprocess.run([exe], cwd=str(tmp_path), env=env, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    em = _one_group(meshgen.rect_tri(8, 8, 1.0, 1.0), "wall")
+    g = oracle.build_mesh(em)
+    p = oracle.physics(P.burgers_diffusion(), em.group_names)
+    want = oracle.run_loop(g, p, np.zeros(g.n_total * 2), P.RK5_ALPHA, 30)["q"].reshape(-1, 2)[: g.n_real]
+    got = np.stack([_read_ascii_cell_array(str(tmp_path / "square.vtu"), nm) for nm in ("u", "v")], 1)
+    assert got.shape == want.shape and np.abs(want).max() > 1e-3
+    assert np.abs(got - want).max() <= 5e-7 * max(1.0, np.abs(want).max())
 
 
 def test_unknown_boundary_name_is_refused(tmp_path):
