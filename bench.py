@@ -48,6 +48,34 @@ ALGO_BYTES = {
     "fp64": {"stage": 256.0, "grad_lim": 192.0, "stage_o1": 160.0, "dt": 96.0},
     "fp32": {"stage": 156.4, "grad_lim": 102.0, "stage_o1": 110.0, "dt": 58.0},
 }
+# The diffusive kinds (same accounting, s = 8 or 4).
+# Navier-Stokes (V = 4, MUSCL): the stage kernel reads q, the raw gradients
+# and the limiter (kept apart in every mode), centroid, area, edges
+# (2 indices + normal, length, face centre), q_base and the local dt, and
+# writes q_new: FP64 32*4 + 16 + 8 + 1.5*44 + 32 + 8 + 32 = 290; FP32 16*4 +
+# 8 + 4 + 1.5*24 + 32 + 8 + 16 + 32/5 = 174.4.  The gradient kernel reads q,
+# centroid, area, edges (+ Green-Gauss weight) and writes gx, gy, lim:
+# FP64 32 + 16 + 8 + 1.5*52 + 96 = 230; FP32 16 + 8 + 4 + 1.5*28 + 48 = 118.
+# Diffusion (V = 1, no MUSCL): stage reads q, gx, gy (+ lim in FP64_EXACT),
+# centroid, area, edges (2 indices + normal, length), q_base and writes
+# q_new: FP64 8*3 + 16 + 8 + 1.5*28 + 8 + 8 = 106 (114 exact); FP32 4*3 + 8 +
+# 4 + 1.5*16 + 8 + 4 + 8/5 = 61.6.  Its gradient kernel needs no face centres:
+# FP64 8 + 16 + 8 + 1.5*36 + 24 = 110; FP32 4 + 8 + 4 + 1.5*20 + 12 = 58.
+ALGO_BYTES_KIND = {
+    "ns": {"fp64_exact": {"stage": 290.0, "grad_lim": 230.0}, "fp64": {"stage": 290.0, "grad_lim": 230.0},
+           "fp32": {"stage": 174.4, "grad_lim": 118.0}},
+    "diffusion": {"fp64_exact": {"stage": 114.0, "grad_lim": 110.0}, "fp64": {"stage": 106.0, "grad_lim": 110.0},
+                  "fp32": {"stage": 61.6, "grad_lim": 58.0}},
+}
+
+
+def algo_bytes(ph, precision, kernel):
+    kind = {"ns": "ns", "diffusion": "diffusion"}.get(ph.flux)
+    if kind is not None:
+        return ALGO_BYTES_KIND[kind][precision][kernel]
+    if kernel == "stage" and not ph.order2:
+        kernel = "stage_o1"
+    return ALGO_BYTES[precision][kernel]
 
 
 # DRAM bytes per real cell of one k_tile_stage launch (dram__bytes_read.sum +
@@ -85,7 +113,26 @@ def build_workload(name):
         return ems, P.riemann_strip(), P.RK5_ALPHA, ic, \
             (f"{len(ems)} independent Riemann strips (nx x 8 x 2 triangles, 2k-200k cells log-uniform, seed 4), "
              f"2nd-order GG + Venkatakrishnan K=5, RK5, CFL 0.8, per-case global dt, one batched solver")
+    if name == "flatplate":
+        # examples/flatPlate's domain and grading pattern at 1.0M quadrilaterals
+        # CFL 1: at the example's CFL 2 the scheme goes non-finite on this mesh
+        # (by step 60 in the reference's exact arithmetic)
+        em = meshgen.flat_plate(nx0=100, nx1=900, ny=1000, r_up=1.02, r_plate=1.004, r_y=1.004)
+        return em, P.flat_plate(cfl=1.0), P.RK5_ALPHA, \
+            lambda mesh, geo: P.ic_forward_step(mesh.n_total, mach=0.2).ravel(), \
+            ("flat plate M 0.2 (examples/flatPlate), 1000x1000 graded quads, Navier-Stokes, MUSCL + Michalak, "
+             "local viscous dt, RK5, CFL 1")
+    if name == "heat":
+        em = meshgen.rect_tri(708, 708, 1.0, 1.0, side_names=("wall", "wall"))
+        return em, P.heat(dt=2e-7), P.RK5_ALPHA, lambda mesh, geo: P.ic_heat(geo["ccx"], geo["ccy"]).ravel(), \
+            "heat equation (examples/heatTransfer), 708x708x2 triangles, diffusion flux with face gradients, RK5"
     raise SystemExit(f"unknown workload {name}")
+
+
+# reference build, boundary aliases and constants timed as the CPU baseline of a workload
+REF_FOR = {"step": ("forwardStep_o2venk5", {"step": "wall"}, dict(cfl=0.8)),
+           "flatplate": ("flatPlate", {}, {}),
+           "heat": ("heatTransfer", {}, {})}
 
 
 def make_mesh(em):
@@ -168,7 +215,8 @@ def measured_peak_hbm():
 
 # --------------------------------------------------------------- reference --
 def _ref_worker(args):
-    """One single-rank reference process (spawned): K RK1 steps on the mesh."""
+    """One single-rank reference process (spawned): K RK1 steps on the mesh
+    from the example's own initial state (generate_initial_solution)."""
     variant, base, consts, aliases, n_total, warmup, steps = args
     from oracle import RefLib
     ref = RefLib(variant)
@@ -182,25 +230,26 @@ def _ref_worker(args):
     ref.lib.ref_mesh_sizes(s.ctypes.data_as(ctypes.c_void_p))
     ref.n_nodes, ref.n_real, ref.n_total, ref.n_edges, ref.n_bound = (int(x) for x in s)
     ref.nq = ref.V * ref.n_total
-    q0 = P.ic_forward_step(ref.n_total).ravel()
+    q0 = ref.initial_state()
     r = ref.run_loop(q0, P.RK1_ALPHA, max(warmup, 1))
     t0 = time.perf_counter()
     ref.run_loop(r["q"], P.RK1_ALPHA, steps)
     return time.perf_counter() - t0, ref.n_real
 
 
-def reference_samples(em, procs, warmup, steps):
+def reference_samples(em, procs, warmup, steps, workload="step"):
     """Times the reference library (oracle/_ref, built from the reference's
-    own sources) on the forward-step workload in `procs` independent
-    single-rank processes.  Returns (cell-updates/s aggregate, sample text)."""
+    own sources) on a workload's mesh in `procs` independent single-rank
+    processes.  Returns (cell-updates/s aggregate, n_real) or None."""
     import multiprocessing as mp
     from oracle import ref_available
-    if not ref_available("forwardStep_o2venk5"):
+    variant, aliases, consts = REF_FOR[workload]
+    if not ref_available(variant):
         return None
     tmp = tempfile.mkdtemp(prefix="fvbench_")
-    base = os.path.join(tmp, "step")
+    base = os.path.join(tmp, "mesh")
     meshgen.write_msh41(base + ".msh", em)
-    job = ("forwardStep_o2venk5", base, dict(cfl=0.8), {"step": "wall"}, 0, warmup, steps)
+    job = (variant, base, consts, aliases, 0, warmup, steps)
     ctx = mp.get_context("spawn")
     with ctx.Pool(procs) as pool:
         res = pool.map(_ref_worker, [job] * procs)
@@ -284,9 +333,8 @@ def measure_mode(args, em, mesh, geo, ph, alpha, ic, precision, local, dist, wor
     kinds = ["step_begin", "dt", "grad_lim", "stage", "step_end"]
     out["per_launch_ms"] = {kinds[k]: (ms_k[k] / cnt_k[k] if cnt_k[k] else 0.0) for k in range(5)}
     out["share"] = {kinds[k]: float(ms_k[k] / ms_k.sum()) for k in range(5)}
-    stage_key = "stage" if ph.order2 else "stage_o1"
     peak, peak_kind = measured_peak_hbm()
-    kb = ALGO_BYTES[precision][stage_key] * N
+    kb = algo_bytes(ph, precision, "stage") * N
     achieved = kb / (out["per_launch_ms"]["stage"] / 1e3) / 1e9
     out["roofline"] = {"bound": "hbm", "kernel": "flux + RK update + ghost fill (k_tile_stage)",
                        "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
@@ -295,8 +343,8 @@ def measure_mode(args, em, mesh, geo, ph, alpha, ic, precision, local, dist, wor
                                    if args.workload == "step" and precision in TRAFFIC_B_PER_CELL else None),
                        "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, forward-step capture",
                        "algorithmic_bytes_per_launch": kb}
-    if ph.order2:
-        kg = ALGO_BYTES[precision]["grad_lim"] * N
+    if ph.order2 or ph.diffusive:
+        kg = algo_bytes(ph, precision, "grad_lim") * N
         out["roofline_grad_lim"] = {"achieved": kg / (out["per_launch_ms"]["grad_lim"] / 1e3) / 1e9,
                                     "frac": kg / (out["per_launch_ms"]["grad_lim"] / 1e3) / 1e9 / peak}
     return out
@@ -485,7 +533,8 @@ def main():
     ap.add_argument("--steps", type=int, default=500)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="step", choices=["step", "sod", "naca", "batch", "adjoint"])
+    ap.add_argument("--workload", default="step",
+                    choices=["step", "sod", "naca", "batch", "adjoint", "flatplate", "heat"])
     ap.add_argument("--precision", default="all", choices=["all", "fp64_exact", "fp64", "fp32"],
                     help="all: FP32-bulk (headline) and plain FP64 in one line")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -554,11 +603,12 @@ def main():
             if "fp64" in errs and "fp32" in errs:
                 line["l2_error_vs_exact_riemann"]["fp32_minus_fp64_density"] = \
                     errs["fp32"]["density"] - errs["fp64"]["density"]
-        if not args.no_cpu_baseline and world == 1 and args.workload == "step":
-            r = reference_samples(em, 1, 1, 25)
+        if not args.no_cpu_baseline and world == 1 and args.workload in REF_FOR:
+            r = reference_samples(em, 1, 1, 25, args.workload)
             if r is not None:
                 line["cpu_baseline"] = {"value": r[0], "unit": UNIT, "cores": 1, "kind": "reference",
-                                        "sample": f"reference library (built from its sources), 1 process, "
+                                        "sample": f"reference library (built from its sources, "
+                                                  f"{REF_FOR[args.workload][0]}), 1 process, "
                                                   f"25 single-stage steps of the {r[1]}-cell mesh"}
         print(json.dumps(line))
     for r in res.values():

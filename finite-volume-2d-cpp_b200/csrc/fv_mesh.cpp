@@ -196,32 +196,102 @@ std::string build_geometry(HostMesh& m) {
     return "";
 }
 
-void build_device_numbering(HostMesh& m) {
-    const int64_t nc = m.n_real, nt = m.n_total, E = m.n_edges;
-    // Hilbert key within each case's bounding box; the case index above it
-    // keeps the cases of a batch contiguous (a single mesh is one case)
-    std::vector<int64_t> offs = m.case_real_off;
-    if (offs.size() < 2) offs = {0, nc};
+// Rank coordinate of every cell of [c0, c1) along one axis: its position in
+// the sorted centroid coordinates (equal coordinates share their mean
+// position), scaled to [0, 1].  In rank coordinates the cells are evenly
+// spread along each axis, so a Hilbert tile is compact in cell counts even
+// where cells are strongly graded (boundary layers), not only in space.
+static void axis_ranks(const std::vector<double>& x, int64_t c0, int64_t c1, std::vector<double>& r) {
+    const int64_t n = c1 - c0;
+    std::vector<int32_t> idx(n);
+    std::iota(idx.begin(), idx.end(), 0);
+    std::stable_sort(idx.begin(), idx.end(), [&](int32_t a, int32_t b) { return x[c0 + a] < x[c0 + b]; });
+    const double scale = n > 1 ? 1.0 / (double)(n - 1) : 0.0;
+    for (int64_t i = 0; i < n;) {
+        int64_t j = i;
+        while (j + 1 < n && x[c0 + idx[j + 1]] == x[c0 + idx[i]]) ++j;
+        const double mean = 0.5 * (double)(i + j) * scale;
+        for (int64_t k = i; k <= j; ++k) r[c0 + idx[k]] = mean;
+        i = j + 1;
+    }
+}
+
+// Hilbert order of the real cells, case by case (the case index above the
+// key keeps the cases of a batch contiguous; a single mesh is one case), on
+// the centroids (rank = false: each case's bounding square) or on their rank
+// coordinates.  Returns new2ref of the real cells.
+static std::vector<int32_t> hilbert_order(const HostMesh& m, const std::vector<int64_t>& offs, bool rank) {
+    const int64_t nc = m.n_real;
     const int order = 16;
+    const double top = (double)((1u << order) - 1);
     std::vector<uint64_t> key(nc);
+    std::vector<double> rx, ry;
+    if (rank) { rx.resize(nc); ry.resize(nc); }
     for (size_t k = 0; k + 1 < offs.size(); ++k) {
-        double xmin = 1e300, xmax = -1e300, ymin = 1e300, ymax = -1e300;
-        for (int64_t c = offs[k]; c < offs[k + 1]; ++c) {
-            xmin = std::min(xmin, m.ccx[c]); xmax = std::max(xmax, m.ccx[c]);
-            ymin = std::min(ymin, m.ccy[c]); ymax = std::max(ymax, m.ccy[c]);
+        double x0 = 0, y0 = 0, scale = top;
+        if (rank) {
+            axis_ranks(m.ccx, offs[k], offs[k + 1], rx);
+            axis_ranks(m.ccy, offs[k], offs[k + 1], ry);
+        } else {
+            double xmin = 1e300, xmax = -1e300, ymin = 1e300, ymax = -1e300;
+            for (int64_t c = offs[k]; c < offs[k + 1]; ++c) {
+                xmin = std::min(xmin, m.ccx[c]); xmax = std::max(xmax, m.ccx[c]);
+                ymin = std::min(ymin, m.ccy[c]); ymax = std::max(ymax, m.ccy[c]);
+            }
+            x0 = xmin; y0 = ymin;
+            scale = top / std::max(std::max(xmax - xmin, ymax - ymin), 1e-300);
         }
-        const double span = std::max(std::max(xmax - xmin, ymax - ymin), 1e-300);
-        const double scale = ((1u << order) - 1) / span;
         for (int64_t c = offs[k]; c < offs[k + 1]; ++c) {
-            uint32_t qx = (uint32_t)((m.ccx[c] - xmin) * scale);
-            uint32_t qy = (uint32_t)((m.ccy[c] - ymin) * scale);
-            key[c] = ((uint64_t)k << 32) | hilbert_d(qx, qy, order);
+            const double fx = rank ? rx[c] * top : (m.ccx[c] - x0) * scale;
+            const double fy = rank ? ry[c] * top : (m.ccy[c] - y0) * scale;
+            key[c] = ((uint64_t)k << 32) | hilbert_d((uint32_t)fx, (uint32_t)fy, order);
         }
     }
+    std::vector<int32_t> n2r(nc);
+    std::iota(n2r.begin(), n2r.end(), 0);
+    std::stable_sort(n2r.begin(), n2r.end(), [&](int32_t a, int32_t b) { return key[a] < key[b]; });
+    return n2r;
+}
+
+// Halo cells of tiles of 128 consecutive cells in an order: mean + max / 4
+// (the mean sets the re-read traffic, the max the shared memory per tile).
+static double halo_score(const HostMesh& m, const std::vector<int32_t>& n2r) {
+    const int64_t nc = m.n_real;
+    const int T = 128;
+    std::vector<int32_t> r2n(nc);
+    for (int64_t n = 0; n < nc; ++n) r2n[n2r[n]] = (int32_t)n;
+    std::vector<uint64_t> pairs;  // tile << 32 | halo cell (ghosts keep their reference index)
+    pairs.reserve(2 * (size_t)m.n_edges);
+    for (int64_t e = 0; e < m.n_edges; ++e) {
+        const uint32_t i = m.edge_cells[2 * e], j = m.edge_cells[2 * e + 1];
+        const uint64_t ti = (uint64_t)(r2n[i] / T);
+        if (j >= (uint32_t)nc) { pairs.push_back(ti << 32 | j); continue; }
+        const uint64_t tj = (uint64_t)(r2n[j] / T);
+        if (ti != tj) { pairs.push_back(ti << 32 | j); pairs.push_back(tj << 32 | i); }
+    }
+    std::sort(pairs.begin(), pairs.end());
+    pairs.erase(std::unique(pairs.begin(), pairs.end()), pairs.end());
+    const int64_t nt = (nc + T - 1) / T;
+    std::vector<int32_t> cnt((size_t)nt, 0);
+    for (uint64_t p : pairs) cnt[(size_t)(p >> 32)]++;
+    int32_t mx = 0;
+    for (int32_t v : cnt) mx = std::max(mx, v);
+    return (double)pairs.size() / (double)std::max<int64_t>(nt, 1) + 0.25 * mx;
+}
+
+void build_device_numbering(HostMesh& m) {
+    const int64_t nc = m.n_real, nt = m.n_total, E = m.n_edges;
+    std::vector<int64_t> offs = m.case_real_off;
+    if (offs.size() < 2) offs = {0, nc};
+    // Hilbert order on the centroids keeps isotropic meshes (and O-grids,
+    // strips) compact; on rank coordinates it keeps strongly graded cells
+    // (boundary layers) compact in cell counts.  The order with the smaller
+    // tile halos is kept.
+    std::vector<int32_t> geo = hilbert_order(m, offs, false);
+    std::vector<int32_t> rnk = hilbert_order(m, offs, true);
+    const bool use_rank = halo_score(m, rnk) < halo_score(m, geo);
     m.new2ref.resize(nt);
-    std::iota(m.new2ref.begin(), m.new2ref.begin() + nc, 0);
-    std::stable_sort(m.new2ref.begin(), m.new2ref.begin() + nc,
-                     [&](int32_t a, int32_t b) { return key[a] < key[b]; });
+    std::copy(use_rank ? rnk.begin() : geo.begin(), use_rank ? rnk.end() : geo.end(), m.new2ref.begin());
     m.ref2new.assign(nt, -1);
     for (int64_t n = 0; n < nc; ++n) m.ref2new[m.new2ref[n]] = (int32_t)n;
     // ghosts follow their interior cell's new index (stable in reference order)
