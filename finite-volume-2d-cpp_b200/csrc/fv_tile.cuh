@@ -156,12 +156,22 @@ struct Rec {
 };
 
 // Optional positivity guard (not in the reference): a reconstructed Euler
-// face state with rho <= 0 or p <= 0 is replaced by the cell value.
-template <class S, int V>
+// face state with rho <= 0 or p <= 0 is replaced by the cell value.  The
+// exact mode evaluates p as the oracle does; the fast modes test the same
+// sign without a division: for rho > 0 and gamma > 1,
+// p > 0  <=>  2 rho E - (m_x^2 + m_y^2) > 0.
+template <class S, int V, bool EXACT = true>
 __device__ __forceinline__ void guard_face(const Params& P, S* qf, const S* qc) {
     if (V != 4 || !P.positivity_guard) return;
-    const S p = ((S)P.gamma - S(1)) * (qf[3] - S(0.5) / qf[0] * (qf[1] * qf[1] + qf[2] * qf[2]));
-    if (!(qf[0] > S(0)) || !(p > S(0))) {
+    bool bad;
+    if constexpr (EXACT) {
+        const S p = ((S)P.gamma - S(1)) * (qf[3] - S(0.5) / qf[0] * (qf[1] * qf[1] + qf[2] * qf[2]));
+        bad = !(qf[0] > S(0)) || !(p > S(0));
+    } else {
+        const S m2 = qf[1] * qf[1] + qf[2] * qf[2];
+        bad = !(qf[0] > S(0)) || !(S(2) * qf[0] * qf[3] - m2 > S(0));
+    }
+    if (bad) {
 #pragma unroll
         for (int k = 0; k < V; ++k) qf[k] = qc[k];
     }
@@ -182,6 +192,10 @@ __device__ __forceinline__ void cpa4(void* dst, const void* src) {
                  : "memory");
 }
 __device__ __forceinline__ void cpa_wait() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+// Groups: the constant tile data staged before the dependency wait is one
+// group; cpa_wait_prior() waits for it while the newest group stays in flight.
+__device__ __forceinline__ void cpa_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cpa_wait_prior() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
 template <int BYTES>
 __device__ __forceinline__ void cpa(void* dst, const void* src) {
     if (BYTES == 32) { cpa16(dst, src); cpa16((char*)dst + 16, (const char*)src + 16); }
@@ -190,28 +204,44 @@ __device__ __forceinline__ void cpa(void* dst, const void* src) {
     else cpa4(dst, src);
 }
 
-// Loads the records of the tile's owned cells and halo (asynchronously).
+// Loads the record of device cell g into shared-memory record r (asynchronously).
 template <class M, int V, bool ORDER2, bool CENTROID, bool LIM = M::exact>
-__device__ __forceinline__ void stage_records(const TileParams& TP, const TileIO& io, const int4& inf, int c0,
-                                              int nown, typename M::S* rec) {
+__device__ __forceinline__ void stage_record(const TileParams& TP, const TileIO& io, int g, typename M::S* r) {
     using S = typename M::S;
     using R = Rec<M, V, ORDER2, CENTROID, LIM>;
     constexpr int QB = V * (int)sizeof(S);
-    const S* Q = (const S*)io.q_stage;
-    const S* CXY = (const S*)TP.ccxy;
-    for (int l = threadIdx.x; l < nown + inf.w; l += blockDim.x) {
-        int slot, g;
-        if (l < nown) { slot = l; g = c0 + l; }
-        else { slot = TP.T + (l - nown); g = TP.halo[inf.z + (l - nown)]; }
-        S* r = rec + (size_t)slot * R::NR;
-        cpa<QB>(r, Q + (size_t)V * g);
-        if (ORDER2) {
-            cpa<QB>(r + R::OGX, (const S*)io.gx + (size_t)V * g);
-            cpa<QB>(r + R::OGY, (const S*)io.gy + (size_t)V * g);
-            if (LIM) cpa<QB>(r + R::OLM, (const S*)io.lim + (size_t)V * g);
-        }
-        if (CENTROID) cpa<2 * (int)sizeof(S)>(r + R::OC, CXY + 2 * (size_t)g);
+    cpa<QB>(r, (const S*)io.q_stage + (size_t)V * g);
+    if (ORDER2) {
+        cpa<QB>(r + R::OGX, (const S*)io.gx + (size_t)V * g);
+        cpa<QB>(r + R::OGY, (const S*)io.gy + (size_t)V * g);
+        if (LIM) cpa<QB>(r + R::OLM, (const S*)io.lim + (size_t)V * g);
     }
+    if (CENTROID) cpa<2 * (int)sizeof(S)>(r + R::OC, (const S*)TP.ccxy + 2 * (size_t)g);
+}
+
+// Loads the records of the tile's owned cells and halo (asynchronously), in
+// two groups.  The halo cell indices were staged into shalo by stage_halo
+// before the dependency wait: the owned records are issued first, then the
+// staged indices are awaited (a block barrier) and the halo records issued,
+// so no global index load sits on the chain in front of the record copies.
+template <class M, int V, bool ORDER2, bool CENTROID, bool LIM = M::exact>
+__device__ __forceinline__ void stage_records(const TileParams& TP, const TileIO& io, const int4& inf, int c0,
+                                              int nown, typename M::S* rec, const int* shalo) {
+    using R = Rec<M, V, ORDER2, CENTROID, LIM>;
+    for (int l = threadIdx.x; l < nown; l += blockDim.x)
+        stage_record<M, V, ORDER2, CENTROID, LIM>(TP, io, c0 + l, rec + (size_t)l * R::NR);
+    cpa_commit();
+    cpa_wait_prior();  // the constant group: edges and halo indices
+    __syncthreads();
+    for (int h = threadIdx.x; h < inf.w; h += blockDim.x)
+        stage_record<M, V, ORDER2, CENTROID, LIM>(TP, io, shalo[h], rec + (size_t)(TP.T + h) * R::NR);
+}
+
+// Stages the tile's halo cell indices (constant mesh data) into shared memory
+// and closes the constant group of copies issued before the dependency wait.
+__device__ __forceinline__ void stage_halo(const TileParams& TP, const int4& inf, int* shalo) {
+    for (int h = threadIdx.x; h < inf.w; h += blockDim.x) cpa4(shalo + h, TP.halo + inf.z + h);
+    cpa_commit();
 }
 
 // Loads the tile's edge geometry (contiguous per tile) into shared memory.
@@ -532,15 +562,20 @@ __global__ void __launch_bounds__(kTileMax) k_tile_dt(TileParams TP, TileIO io) 
     S* sny = snx + TP.max_edges;
     S* sle = sny + TP.max_edges;
     uint32_t* sij = reinterpret_cast<uint32_t*>(sle + TP.max_edges);
+    int* shalo = reinterpret_cast<int*>(sij + TP.max_edges);
     const int l = threadIdx.x;
     uint16_t w[kMaxFaces];
     // constant tile data first (may overlap the previous kernel's tail)
     if (l < nown) load_faces(TP, c0 + l, w);
     stage_edges<S, false, false>(TP, inf, sij, snx, sny, sle, nullptr, nullptr, nullptr);
+    stage_halo(TP, inf, shalo);
     pdl_wait();
-    if (t_inactive(io.ctrl)) { cpa_wait(); return; }
-    stage_records<M, V, false, false>(TP, io, inf, c0, nown, rec);
+    // the step-control flag is read while the records load; an inactive
+    // step's kernels write nothing
+    const bool inactive = t_inactive(io.ctrl);
+    stage_records<M, V, false, false>(TP, io, inf, c0, nown, rec, shalo);
     cpa_wait();
+    if (inactive) return;
     __syncthreads();
     unsigned long long kmin = ~0ull;
     if (l < nown) kmin = tile_cell_dt<M, V, R::NR, VISC>(TP, io, inf, l, c0 + l, w, rec, sij, snx, sny, sle);
@@ -566,6 +601,7 @@ __global__ void __launch_bounds__(kTileMax) k_tile_gradlim(TileParams TP, TileIO
     S* snx = rec + (size_t)LT * R::NR;
     S* sny = snx + EM; S* sle = sny + EM; S* sg = sle + EM; S* sxf = sg + EM; S* syf = sxf + EM;
     uint32_t* sij = reinterpret_cast<uint32_t*>(syf + EM);
+    int* shalo = reinterpret_cast<int*>(sij + EM);
     const int l = threadIdx.x;
     const int c = c0 + l;
     uint16_t w[kMaxFaces];
@@ -575,10 +611,12 @@ __global__ void __launch_bounds__(kTileMax) k_tile_gradlim(TileParams TP, TileIO
         A = ((const S*)TP.area)[c];
     }
     stage_edges<S, true, true>(TP, inf, sij, snx, sny, sle, sg, sxf, syf);
+    stage_halo(TP, inf, shalo);
     pdl_wait();
-    if (t_inactive(io.ctrl)) { cpa_wait(); return; }
-    stage_records<M, V, false, true>(TP, io, inf, c0, nown, rec);
+    const bool inactive = t_inactive(io.ctrl);
+    stage_records<M, V, false, true>(TP, io, inf, c0, nown, rec, shalo);
     cpa_wait();
+    if (inactive) return;
     __syncthreads();
     if constexpr (DT != 0) {
         unsigned long long kmin = ~0ull;
@@ -735,8 +773,8 @@ __device__ __forceinline__ void diffusive_edge_flux(const Params& P, const typen
             qL[k] = qci[k] + (gxi[k] * di0 + gyi[k] * di1) * li_[k];
             qR[k] = qcj[k] + (gxj[k] * dj0 + gyj[k] * dj1) * lj_[k];
         }
-        guard_face<S, V>(P, qL, qci);
-        guard_face<S, V>(P, qR, qcj);
+        guard_face<S, V, M::exact>(P, qL, qci);
+        guard_face<S, V, M::exact>(P, qR, qcj);
     } else {
 #pragma unroll
         for (int k = 0; k < V; ++k) { qL[k] = qci[k]; qR[k] = qcj[k]; }
@@ -804,6 +842,7 @@ __global__ void __launch_bounds__(kTileMax) k_tile_stage(TileParams TP, TileIO i
     S* snx = reinterpret_cast<S*>(sF + (size_t)EM * V);
     S* sny = snx + EM; S* sle = sny + EM; S* sxf = sle + EM; S* syf = sxf + EM;
     uint32_t* sij = reinterpret_cast<uint32_t*>(syf + EM);
+    int* shalo = reinterpret_cast<int*>(sij + EM);
     const bool global_dt = io.ctrl != nullptr && P.global_dt;
     // ---- issue this thread's cell loads first: their latency overlaps the staging
     const int l = threadIdx.x;
@@ -817,17 +856,25 @@ __global__ void __launch_bounds__(kTileMax) k_tile_stage(TileParams TP, TileIO i
     }
     if (MUSCL) stage_edges<S, false, true>(TP, inf, sij, snx, sny, sle, nullptr, sxf, syf);
     else stage_edges<S, false, false>(TP, inf, sij, snx, sny, sle, nullptr, nullptr, nullptr);
+    stage_halo(TP, inf, shalo);
+    // the tile's case (batches); -1: the tile spans two cases
+    const int tc = (global_dt && P.n_cases > 1) ? P.tile_case[t] : 0;
+    // reference cell 0 of the tile's case, whose dt carries the NaN rule of min_dt
+    const int cell0 = (P.n_cases > 1 && tc >= 0) ? P.case_cell0[tc] : P.cell0;
     pdl_wait();
-    if (t_inactive(io.ctrl)) { cpa_wait(); return; }
+    // every load of data written by earlier kernels is issued here together,
+    // ahead of the record copies: the step-control flag, the base state, the
+    // local time step or the dt of reference cell 0
+    const bool inactive = t_inactive(io.ctrl);
+    double d0 = 0.;
+    if (global_dt && tc >= 0) d0 = io.dt[cell0];
     if (l < nown) {
         ld<double, V>(io.q_base, c, qb);
         if (!global_dt) dtc = io.dt[c];
     }
-    stage_records<M, V, ORDER2, ORDER2, LIMREC>(TP, io, inf, c0, nown, rec);
+    stage_records<M, V, ORDER2, ORDER2, LIMREC>(TP, io, inf, c0, nown, rec, shalo);
     // MUSCL face states: FLUX 5 and 6 run with and without them (P.order2)
     const bool muscl = MUSCL && ((FLUX != 5 && FLUX != 6) || P.order2 != 0);
-    // the tile's case (batches); -1: the tile spans two cases
-    const int tc = (global_dt && P.n_cases > 1) ? P.tile_case[t] : 0;
     if (global_dt && tc >= 0 && threadIdx.x < 32) {
         const unsigned long long* keys = io.dtkeys + (size_t)tc * kDtSlots;
         unsigned long long k = kmin_(keys[threadIdx.x], keys[threadIdx.x + 32]);
@@ -836,6 +883,7 @@ __global__ void __launch_bounds__(kTileMax) k_tile_stage(TileParams TP, TileIO i
         if (threadIdx.x == 0) s_dtkey = k;
     }
     cpa_wait();
+    if (inactive) return;
     __syncthreads();
     // ---- one flux per tile edge
     for (int el = threadIdx.x; el < (PH == 2 ? 0 : inf.y); el += blockDim.x) {
@@ -876,8 +924,8 @@ __global__ void __launch_bounds__(kTileMax) k_tile_stage(TileParams TP, TileIO i
                         qR[k] = cj[k] + gxj[k] * dj0 + gyj[k] * dj1;
                     }
                 }
-                guard_face<S, V>(P, qL, ci);
-                guard_face<S, V>(P, qR, cj);
+                guard_face<S, V, M::exact>(P, qL, ci);
+                guard_face<S, V, M::exact>(P, qR, cj);
             }
             if constexpr (FLUX == 4) {
                 S gxi[V], gyi[V], gxj[V], gyj[V];
@@ -954,16 +1002,12 @@ __global__ void __launch_bounds__(kTileMax) k_tile_stage(TileParams TP, TileIO i
         if (global_dt) {
             // min_dt (explicit.cpp:555-564) of this cell's case; a NaN in its dt[0] wins
             unsigned long long key = s_dtkey;
-            int cell0 = P.cell0;
-            if (P.n_cases > 1) {
-                const int k = tc >= 0 ? tc : P.cell_case[c];
-                cell0 = P.case_cell0[k];
-                if (tc < 0) {
-                    key = ~0ull;
-                    for (int i = 0; i < kDtSlots; ++i) key = kmin_(key, io.dtkeys[(size_t)k * kDtSlots + i]);
-                }
+            if (tc < 0) {  // a tile across two cases of a batch: this cell's case
+                const int k = P.cell_case[c];
+                key = ~0ull;
+                for (int i = 0; i < kDtSlots; ++i) key = kmin_(key, io.dtkeys[(size_t)k * kDtSlots + i]);
+                d0 = io.dt[P.case_cell0[k]];
             }
-            const double d0 = io.dt[cell0];
             dtc = (d0 != d0) ? d0 : tkey_inv(key);
         }
         double qnew[V];
@@ -992,7 +1036,7 @@ __global__ void __launch_bounds__(kTileMax) k_tile_stage(TileParams TP, TileIO i
                 const int el = w[f] & kFaceEdgeMask, side = w[f] >> 15;
                 const uint32_t ij = sij[el];
                 const int o = side ? (int)(ij & 0xffff) : (int)(ij >> 16);
-                const int g = TP.halo[inf.z + o - T];
+                const int g = shalo[o - T];
                 const S n0 = snx[el], n1 = sny[el];
                 S qint[V], qc[V], b[V];
 #pragma unroll
@@ -1010,7 +1054,7 @@ __global__ void __launch_bounds__(kTileMax) k_tile_stage(TileParams TP, TileIO i
 #pragma unroll
                         for (int k = 0; k < V; ++k) qint[k] = qc[k] + gxs[k] * d0 + gys[k] * d1;
                     }
-                    guard_face<S, V>(P, qint, qc);
+                    guard_face<S, V, M::exact>(P, qint, qc);
                 }
                 if constexpr (M::exact) exact::bc<V>(P, P.ghost_group[g - N], g - N, b, qint, n0, n1);
                 else fast::bc<V, S>(P, P.ghost_group[g - N], g - N, b, qint, n0, n1);
@@ -1059,20 +1103,20 @@ template <class M, int V>
 inline size_t smem_dt(const TileParams& TP) {
     using S = typename M::S;
     return (size_t)(TP.T + TP.max_halo) * Rec<M, V, false, false>::NR * sizeof(S) +
-           (size_t)TP.max_edges * (3 * sizeof(S) + 4);
+           (size_t)TP.max_edges * (3 * sizeof(S) + 4) + (size_t)TP.max_halo * 4;
 }
 template <class M, int V>
 inline size_t smem_gradlim(const TileParams& TP) {
     using S = typename M::S;
     return (size_t)(TP.T + TP.max_halo) * Rec<M, V, false, true>::NR * sizeof(S) +
-           (size_t)TP.max_edges * (6 * sizeof(S) + 4);
+           (size_t)TP.max_edges * (6 * sizeof(S) + 4) + (size_t)TP.max_halo * 4;
 }
 template <class M, int V, bool ORDER2, int FLUX = 0>
 inline size_t smem_stage(const TileParams& TP) {
     using S = typename M::S;
     using FT = typename std::conditional<M::exact, double, S>::type;
     return (size_t)(TP.T + TP.max_halo) * Rec<M, V, ORDER2, ORDER2, M::exact || FLUX == 5 || FLUX == 6>::NR * sizeof(S) +
-           (size_t)TP.max_edges * (V * sizeof(FT) + 5 * sizeof(S) + 4);
+           (size_t)TP.max_edges * (V * sizeof(FT) + 5 * sizeof(S) + 4) + (size_t)TP.max_halo * 4;
 }
 
 // ------------------------------------------------------------- launchers --
