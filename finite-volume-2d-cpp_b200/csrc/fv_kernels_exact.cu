@@ -108,12 +108,17 @@ void launch_set_limits(RunLimits* d, const RunLimits& v, cudaStream_t st) { k_se
 // (explicit.cpp:752-800), then the next step's start: its stop criteria and
 // fresh dt key slots, so that consecutive steps need no separate begin
 // kernel.  Partial sums are reduced in a fixed order.
-__global__ void k_step_end(Params P, Ctrl* c, const RunLimits* L, const double* partials, int nblocks,
+constexpr int kEndBlock = 1024;  // threads of the step-end kernel (one block)
+__global__ void __launch_bounds__(kEndBlock) k_step_end(Params P, Ctrl* c, const RunLimits* L, const double* partials, int nblocks,
                            const double* dt, unsigned long long* keys, int nkeys, PrintRec* hist, int hist_cap) {
     // launched as a programmatic dependent of the last stage kernel: wait for
     // it to complete before reading anything
     asm volatile("griddepcontrol.wait;" ::: "memory");
-    if (!c->active) return;
+    // every thread reads the step's control words before thread 0 rewrites
+    // them for the next step (begin_step)
+    const bool act = c->active != 0, need_R = c->need_R != 0;
+    __syncthreads();
+    if (!act) return;
     if (P.n_cases > 1) {
         // each case of a batch keeps its own time: time += dt[0] of that case
         for (int k = threadIdx.x; k < P.n_cases; k += blockDim.x) {
@@ -127,23 +132,30 @@ __global__ void k_step_end(Params P, Ctrl* c, const RunLimits* L, const double* 
             P.case_time[k] += dk;
         }
     }
-    __shared__ double red[kBlock][kMaxV];
+    // residual sums: per-thread strided sums over the tile partials, then a
+    // fixed butterfly inside each warp and over the warps (deterministic)
+    __shared__ double red[kEndBlock / 32][kMaxV];
     const int V = P.V;
-    if (c->need_R) {
-        double s[kMaxV] = {0, 0, 0, 0};
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    double s[kMaxV] = {0, 0, 0, 0};
+    if (need_R) {
         for (int b = threadIdx.x; b < nblocks; b += blockDim.x)
             for (int k = 0; k < V; ++k) s[k] += partials[(size_t)b * V + k];
-        for (int k = 0; k < V; ++k) red[threadIdx.x][k] = s[k];
+        for (int k = 0; k < V; ++k)
+            for (int o = 16; o > 0; o >>= 1) s[k] += __shfl_xor_sync(0xffffffffu, s[k], o);
+        if (lane == 0)
+            for (int k = 0; k < V; ++k) red[warp][k] = s[k];
         __syncthreads();
-        for (int w = blockDim.x / 2; w > 0; w >>= 1) {
-            if (threadIdx.x < w)
-                for (int k = 0; k < V; ++k) red[threadIdx.x][k] += red[threadIdx.x + w][k];
-            __syncthreads();
+        if (warp == 0) {
+            for (int k = 0; k < V; ++k) {
+                s[k] = lane < (int)(blockDim.x >> 5) ? red[lane][k] : 0.;
+                for (int o = 16; o > 0; o >>= 1) s[k] += __shfl_xor_sync(0xffffffffu, s[k], o);
+            }
         }
     }
     if (threadIdx.x == 0) {
-    if (c->need_R) {
-        for (int k = 0; k < V; ++k) c->Rraw[k] = sqrt(red[0][k]);
+    if (need_R) {
+        for (int k = 0; k < V; ++k) c->Rraw[k] = sqrt(s[k]);
         if (c->step == 0) {
             for (int k = 0; k < V; ++k) { c->R0[k] = c->Rraw[k]; c->R[k] = c->Rraw[k]; }
         } else {
@@ -174,12 +186,12 @@ void launch_step_end(const Params& P, Ctrl* c, const RunLimits* lim, const doubl
                      const double* dt, unsigned long long* keys, int nkeys, PrintRec* hist, int hist_cap,
                      cudaStream_t st, bool pdl) {
     if (!pdl) {
-        k_step_end<<<1, kBlock, 0, st>>>(P, c, lim, partials, nblocks, dt, keys, nkeys, hist, hist_cap);
+        k_step_end<<<1, kEndBlock, 0, st>>>(P, c, lim, partials, nblocks, dt, keys, nkeys, hist, hist_cap);
         return;
     }
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(1);
-    cfg.blockDim = dim3(kBlock);
+    cfg.blockDim = dim3(kEndBlock);
     cfg.stream = st;
     cudaLaunchAttribute at[1];
     at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
