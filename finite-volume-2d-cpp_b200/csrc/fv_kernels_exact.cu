@@ -23,14 +23,6 @@ __device__ __forceinline__ double dkey_inv(unsigned long long k) {
 __device__ __forceinline__ bool inactive(const Ctrl* c) {
     return c != nullptr && *(volatile const int*)&c->active == 0;
 }
-// min_dt (explicit.cpp:555-564): min over all cells; a NaN in dt[0] wins.
-__device__ __forceinline__ double global_dt_value(const Params& P, const double* dt, const unsigned long long* keys) {
-    unsigned long long key = ~0ull;
-    for (int i = 0; i < 64; ++i) key = keys[i] < key ? keys[i] : key;
-    const double d0 = dt[P.cell0];
-    return (d0 != d0) ? d0 : dkey_inv(key);
-}
-
 template <int V>
 __device__ __forceinline__ void load_cell(const double* __restrict__ a, int c, double* v) {
     if (V == 4) {
@@ -56,17 +48,24 @@ __device__ __forceinline__ void store_cell(double* __restrict__ a, int c, const 
 
 // ------------------------------------------------------------ step control --
 // Stop criteria of the step about to start (explicit.cpp:717-726), one thread.
-__device__ void begin_step(Ctrl* c, const RunLimits* L, int V) {
+__device__ __forceinline__ void step_start(unsigned long long step, double time, const double* R, int V,
+                                           const RunLimits& L, int* active, int* need_R) {
     double Rmax;
-    if (c->step > 0) {
+    if (step > 0) {
         Rmax = 0.0;
-        for (int k = 0; k < V; ++k) Rmax = exact::dmax(c->R[k], Rmax);
+        for (int k = 0; k < V; ++k) Rmax = exact::dmax(R[k], Rmax);
     } else {
         Rmax = 1.0;
     }
-    const int stop = (c->step >= L->max_step) | (c->time >= L->max_time) | (Rmax < L->tolerance);
-    c->active = !stop;
-    c->need_R = !stop && (c->step == 0 || (c->step % L->print_interval) == 0 || (L->tolerance > 1.01e-16));
+    const int stop = (step >= L.max_step) | (time >= L.max_time) | (Rmax < L.tolerance);
+    *active = !stop;
+    *need_R = !stop && (step == 0 || (step % L.print_interval) == 0 || (L.tolerance > 1.01e-16));
+}
+__device__ void begin_step(Ctrl* c, const RunLimits* L, int V) {
+    int active, need_R;
+    step_start(c->step, c->time, c->R, V, *L, &active, &need_R);
+    c->active = active;
+    c->need_R = need_R;
 }
 
 // First kernel of every launch sequence (graph): the step's start, and an
@@ -115,7 +114,7 @@ __global__ void __launch_bounds__(kEndBlock) k_step_end(Params P, Ctrl* c, const
     // it to complete before reading anything
     asm volatile("griddepcontrol.wait;" ::: "memory");
     // every thread reads the step's control words before thread 0 rewrites
-    // them for the next step (begin_step)
+    // them for the next step
     const bool act = c->active != 0, need_R = c->need_R != 0;
     __syncthreads();
     if (!act) return;
@@ -153,27 +152,50 @@ __global__ void __launch_bounds__(kEndBlock) k_step_end(Params P, Ctrl* c, const
             }
         }
     }
-    if (threadIdx.x == 0) {
-    if (need_R) {
-        for (int k = 0; k < V; ++k) c->Rraw[k] = sqrt(s[k]);
-        if (c->step == 0) {
-            for (int k = 0; k < V; ++k) { c->R0[k] = c->Rraw[k]; c->R[k] = c->Rraw[k]; }
-        } else {
-            for (int k = 0; k < V; ++k) c->R[k] = c->Rraw[k] / c->R0[k];
+    // the global dt minimum of the step (case 0 of a batch: its keys come first)
+    unsigned long long kmin = ~0ull;
+    if (P.global_dt && warp == 0) {
+        kmin = keys[lane] < keys[lane + 32] ? keys[lane] : keys[lane + 32];
+        for (int o = 16; o > 0; o >>= 1) {
+            const unsigned long long x = __shfl_xor_sync(0xffffffffu, kmin, o);
+            kmin = x < kmin ? x : kmin;
         }
     }
-    const bool print = (c->step == 0) || (c->step % L->print_interval) == 0;
-    if (print && c->n_hist < hist_cap) {
-        PrintRec& r = hist[c->n_hist++];
-        r.step = c->step;
-        r.time = c->time;
-        for (int k = 0; k < V; ++k) r.R[k] = (c->step == 0) ? 1.0 : c->R[k];
-    }
-    // case 0 of a batch: its reference cell 0 is P.cell0 and its keys come first
-    const double dt0 = P.global_dt ? global_dt_value(P, dt, keys) : dt[P.cell0];
-    c->step += 1;
-    c->time += dt0;
-    begin_step(c, L, V);
+    if (threadIdx.x == 0) {
+        // every control value of the step, loaded together
+        const unsigned long long step = c->step;
+        const double time = c->time;
+        double R[kMaxV], R0[kMaxV];
+        for (int k = 0; k < V; ++k) { R[k] = c->R[k]; R0[k] = c->R0[k]; }
+        const int n_hist = c->n_hist;
+        const RunLimits lim = *L;
+        // min_dt (explicit.cpp:555-564): a NaN in dt[0] wins
+        const double d0 = dt[P.cell0];
+        if (need_R) {
+            for (int k = 0; k < V; ++k) {
+                const double r = sqrt(s[k]);
+                c->Rraw[k] = r;
+                if (step == 0) R0[k] = r;
+                R[k] = step == 0 ? r : r / R0[k];
+                c->R0[k] = R0[k];
+                c->R[k] = R[k];
+            }
+        }
+        const bool print = (step == 0) || (step % lim.print_interval) == 0;
+        if (print && n_hist < hist_cap) {
+            PrintRec& r = hist[n_hist];
+            r.step = step;
+            r.time = time;
+            for (int k = 0; k < V; ++k) r.R[k] = (step == 0) ? 1.0 : R[k];
+            c->n_hist = n_hist + 1;
+        }
+        const double dt0 = P.global_dt ? ((d0 != d0) ? d0 : dkey_inv(kmin)) : d0;
+        c->step = step + 1;
+        c->time = time + dt0;
+        int active, next_R;
+        step_start(step + 1, time + dt0, R, V, lim, &active, &next_R);
+        c->active = active;
+        c->need_R = next_R;
     }
     __syncthreads();  // the keys have been read
     for (int i = threadIdx.x; i < nkeys; i += blockDim.x) keys[i] = ~0ull;
