@@ -367,7 +367,7 @@ def e2e_mode(args, mesh, ph, alpha, m, local, dist, world):
     stream = m["stream"]
     nq = mesh.n_total * ph.V
     state = s.get_state()
-    e2e_steps = max(3, min(args.steps, 20))
+    e2e_steps = max(3, min(args.steps, 50))
     s.set_chunk(1)
     s.set_state(state)
     s.run(1, alpha=alpha)  # builds the one-step graph outside the timed region

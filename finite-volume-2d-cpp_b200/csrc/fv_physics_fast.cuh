@@ -143,6 +143,14 @@ __device__ __forceinline__ T limiter_func(int kind, T y) {
     if (kind == 3) return tmax(T(0), tmin(T(1), y));
     return T(0);
 }
+// phi(num / den) for den != 0.  Venkatakrishnan's phi is a ratio of
+// quadratics in y = num / den: multiplied through by den^2 it needs one
+// reciprocal, (num^2 + 2 num den) / (num^2 + num den + 2 den^2).
+template <class T>
+__device__ __forceinline__ T limiter_ratio(int kind, T num, T den) {
+    if (kind == 2) return num * (num + T(2) * den) * rcp(num * (num + den) + T(2) * den * den);
+    return limiter_func(kind, div_(num, den));
+}
 
 // Boundary conditions (see fv_physics_exact.cuh for the references).
 template <int V, class T>

@@ -727,8 +727,8 @@ __global__ void __launch_bounds__(kTileMax) k_tile_gradlim(TileParams TP, TileIO
                 if (sig[k] < S(1)) {
                     const S dqg = gx[k] * dx + gy[k] * dy;
                     S phi = 1;
-                    if (dqg > tol) phi = fast::limiter_func(P.limiter, fast::div_(qmx[k] - qs[k], dqg));
-                    else if (dqg < -tol) phi = fast::limiter_func(P.limiter, fast::div_(qmn[k] - qs[k], dqg));
+                    if (dqg > tol) phi = fast::limiter_ratio(P.limiter, qmx[k] - qs[k], dqg);
+                    else if (dqg < -tol) phi = fast::limiter_ratio(P.limiter, qmn[k] - qs[k], dqg);
                     lim[k] = fast::tmin(lim[k], sig[k] + (S(1) - sig[k]) * phi);
                 }
             }
