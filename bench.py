@@ -36,11 +36,11 @@ import physics as P  # noqa: E402
 METRIC = "cell-updates/s per RK stage"
 UNIT = "cell-updates/s"
 # Algorithmic (unique compulsory) bytes per real cell and launch, V = 4,
-# E/N = 1.5 ("Kernels"): the flux + update kernel reads the
+# E/N = 1.5 edges per cell: the flux + update kernel reads the
 # stage state, its (limited) gradients, centroid, area, edge data
 # (2 indices + normal, length, face centre) and the FP64 base state, and
 # writes the new state.  FP64_EXACT keeps the reference's separate limiter
-# array (SURVEY's 296 B); FP64 folds the limiter into the gradients; FP32
+# array (296 B); FP64 folds the limiter into the gradients; FP32
 # stores stage states, gradients and geometry in FP32, the base in FP64, and
 # writes the FP64 state on the last of the 5 stages only.
 ALGO_BYTES = {
@@ -90,7 +90,8 @@ def build_workload(name):
         em = meshgen.forward_step()
         ph = P.forward_step(order2=True, limiter="venkat", K=5.0, cfl=0.8)
         # the reference scheme goes non-finite at t ~ 0.005 on this mesh; the
-        # positivity guard keeps the run physical
+        # positivity guard (MUSCL face states with rho <= 0 or p <= 0 fall
+        # back to the cell value) keeps it physical to t ~ 0.025
         ph.positivity_guard = True
         return em, ph, P.RK5_ALPHA, lambda mesh, geo: P.ic_forward_step(mesh.n_total).ravel(), \
             "forward step Mach 3, 2nd-order GG + Venkatakrishnan K=5 + positivity guard, RK5, CFL 0.8"
@@ -116,7 +117,7 @@ def build_workload(name):
     if name == "flatplate":
         # examples/flatPlate's domain and grading pattern at 1.0M quadrilaterals
         # CFL 1: at the example's CFL 2 the scheme goes non-finite on this mesh
-        # (by step 60 in the reference's exact arithmetic, see DESIGN.md)
+        # (by step 60 in the reference's exact arithmetic)
         em = meshgen.flat_plate(nx0=100, nx1=900, ny=1000, r_up=1.02, r_plate=1.004, r_y=1.004)
         return em, P.flat_plate(cfl=1.0), P.RK5_ALPHA, \
             lambda mesh, geo: P.ic_forward_step(mesh.n_total, mach=0.2).ravel(), \
