@@ -20,6 +20,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <type_traits>
 
 #include "fv_internal.h"
@@ -821,8 +822,8 @@ __device__ __forceinline__ void diffusive_edge_flux(const Params& P, const typen
 // PH (residual smoothing, FLUX 6 only): 0 the whole stage; 1 the time
 // derivatives only, written to io.qt; 2 the update from the smoothed io.qt
 // (RK update, ghost fill, residual partials) without fluxes.
-template <class M, int V, bool ORDER2, int FLUX, int PH = 0>
-__global__ void __launch_bounds__(kTileMax) k_tile_stage(TileParams TP, TileIO io) {
+template <class M, int V, bool ORDER2, int FLUX, int PH>
+__device__ __forceinline__ void tile_stage(const TileParams& TP, const TileIO& io) {
     using S = typename M::S;
     using FT = typename std::conditional<M::exact, double, S>::type;  // flux storage
     // FLUX 5 and 6 keep raw gradients and limiters apart in every mode
@@ -839,10 +840,15 @@ __global__ void __launch_bounds__(kTileMax) k_tile_stage(TileParams TP, TileIO i
     const int LT = T + TP.max_halo, EM = TP.max_edges;
     S* rec = reinterpret_cast<S*>(smem_raw);
     FT* sF = reinterpret_cast<FT*>(rec + (size_t)LT * R::NR);
-    S* snx = reinterpret_cast<S*>(sF + (size_t)EM * V);
+    // the flux store's size as smem_stage lays it out
+    const size_t fbytes = max(max((size_t)EM * V * sizeof(FT), (size_t)TP.max_halo * 4),
+                              (size_t)(kTileMax / 32) * V * sizeof(double));
+    S* snx = reinterpret_cast<S*>(reinterpret_cast<unsigned char*>(sF) + (fbytes + 15) / 16 * 16);
     S* sny = snx + EM; S* sle = sny + EM; S* sxf = sle + EM; S* syf = sxf + EM;
     uint32_t* sij = reinterpret_cast<uint32_t*>(syf + EM);
-    int* shalo = reinterpret_cast<int*>(sij + EM);
+    // the halo indices are read only while the records are staged, before the
+    // first flux is stored: they share the flux store
+    int* shalo = reinterpret_cast<int*>(sF);
     const bool global_dt = io.ctrl != nullptr && P.global_dt;
     // ---- issue this thread's cell loads first: their latency overlaps the staging
     const int l = threadIdx.x;
@@ -1036,7 +1042,7 @@ __global__ void __launch_bounds__(kTileMax) k_tile_stage(TileParams TP, TileIO i
                 const int el = w[f] & kFaceEdgeMask, side = w[f] >> 15;
                 const uint32_t ij = sij[el];
                 const int o = side ? (int)(ij & 0xffff) : (int)(ij >> 16);
-                const int g = shalo[o - T];
+                const int g = TP.halo[inf.z + o - T];
                 const S n0 = snx[el], n1 = sny[el];
                 S qint[V], qc[V], b[V];
 #pragma unroll
@@ -1078,24 +1084,40 @@ __global__ void __launch_bounds__(kTileMax) k_tile_stage(TileParams TP, TileIO i
         }  // PH != 1
     }
     if (PH != 1 && io.partials != nullptr) {
-        __shared__ double red[kTileMax / 32][V];
 #pragma unroll
         for (int k = 0; k < V; ++k)
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) res[k] += __shfl_xor_sync(0xffffffffu, res[k], o);
+        // the warp sums share the flux store once every thread has read its fluxes
+        double* red = reinterpret_cast<double*>(sF);
+        __syncthreads();
         if ((threadIdx.x & 31) == 0)
 #pragma unroll
-            for (int k = 0; k < V; ++k) red[threadIdx.x >> 5][k] = res[k];
+            for (int k = 0; k < V; ++k) red[(threadIdx.x >> 5) * V + k] = res[k];
         __syncthreads();
         if (threadIdx.x == 0) {
             const int nw = blockDim.x >> 5;
             for (int k = 0; k < V; ++k) {
                 double s = 0.;
-                for (int w = 0; w < nw; ++w) s += red[w][k];
+                for (int w = 0; w < nw; ++w) s += red[w * V + k];
                 io.partials[(size_t)blockIdx.x * V + k] = s;
             }
         }
     }
+}
+
+template <class M, int V, bool ORDER2, int FLUX, int PH = 0>
+__global__ void __launch_bounds__(kTileMax) k_tile_stage(TileParams TP, TileIO io) {
+    tile_stage<M, V, ORDER2, FLUX, PH>(TP, io);
+}
+// The Roe kinds of the fast modes on tiles of at most 128 cells, with the
+// register budget that the shared memory of such tiles allows blocks for:
+// FP32 56 registers (9 blocks of 128 threads per SM), FP64 96 (5 blocks).
+template <class M>
+struct T128Regs { static constexpr int v = sizeof(typename M::S) == 4 ? 56 : 96; };
+template <class M, int V, bool ORDER2, int FLUX>
+__global__ void __launch_bounds__(128) __maxnreg__(T128Regs<M>::v) k_tile_stage_t128(TileParams TP, TileIO io) {
+    tile_stage<M, V, ORDER2, FLUX, 0>(TP, io);
 }
 
 // shared memory bytes of each kernel for a tile layout
@@ -1115,8 +1137,12 @@ template <class M, int V, bool ORDER2, int FLUX = 0>
 inline size_t smem_stage(const TileParams& TP) {
     using S = typename M::S;
     using FT = typename std::conditional<M::exact, double, S>::type;
+    // the flux store also holds the halo indices (staging) and the warp sums
+    // of the residual partials (after the per-cell sums)
+    const size_t flux = std::max({(size_t)TP.max_edges * V * sizeof(FT), (size_t)TP.max_halo * 4,
+                                  (size_t)(kTileMax / 32) * V * sizeof(double)});
     return (size_t)(TP.T + TP.max_halo) * Rec<M, V, ORDER2, ORDER2, M::exact || FLUX == 5 || FLUX == 6>::NR * sizeof(S) +
-           (size_t)TP.max_edges * (V * sizeof(FT) + 5 * sizeof(S) + 4) + (size_t)TP.max_halo * 4;
+           (flux + 15) / 16 * 16 + (size_t)TP.max_edges * (5 * sizeof(S) + 4);
 }
 
 // ------------------------------------------------------------- launchers --
@@ -1142,6 +1168,14 @@ struct TileLaunch {
             set((const void*)k_tile_stage<M, 4, true, 2>, smem_stage<M, 4, true>(TP));
             set((const void*)k_tile_stage<M, 4, false, 2>, smem_stage<M, 4, false>(TP));
             set((const void*)k_tile_stage<M, 4, true, 5>, smem_stage<M, 4, true, 5>(TP));
+            if constexpr (kT128) {
+                if (use_t128(TP)) {
+                    set((const void*)k_tile_stage_t128<M, 4, true, 1>, smem_stage<M, 4, true>(TP));
+                    set((const void*)k_tile_stage_t128<M, 4, false, 1>, smem_stage<M, 4, false>(TP));
+                    set((const void*)k_tile_stage_t128<M, 4, true, 2>, smem_stage<M, 4, true>(TP));
+                    set((const void*)k_tile_stage_t128<M, 4, false, 2>, smem_stage<M, 4, false>(TP));
+                }
+            }
         } else if (TP.P.V == 2) {
             set((const void*)k_tile_dt<M, 2>, smem_dt<M, 2>(TP));
             set((const void*)k_tile_gradlim<M, 2, 0>, smem_gradlim<M, 2>(TP));
@@ -1160,6 +1194,9 @@ struct TileLaunch {
         return e;
     }
     static int grid(const TileParams& TP) { return (TP.P.n_real + TP.T - 1) / TP.T; }
+    // the fast modes' Roe flux kernels of tiles up to 128 cells use k_tile_stage_t128
+    static constexpr bool kT128 = !M::exact;
+    static bool use_t128(const TileParams& TP) { return kT128 && TP.T <= 128; }
     // <<<>>> launch, or with programmatic stream serialisation (pdl)
     template <class... A>
     static void go(void (*k)(A...), int g, int b, size_t smem, cudaStream_t st, bool pdl, const TileParams& TP,
@@ -1223,9 +1260,23 @@ struct TileLaunch {
             if (o2) go(k_tile_stage<M, 2, true, 3>, g, TP.T, smem_stage<M, 2, true>(TP), st, pdl, TP, io);
             else go(k_tile_stage<M, 2, false, 3>, g, TP.T, smem_stage<M, 2, false>(TP), st, pdl, TP, io);
         } else if (TP.P.flux == 1) {
+            if constexpr (kT128) {
+                if (use_t128(TP)) {
+                    if (o2) go(k_tile_stage_t128<M, 4, true, 1>, g, TP.T, smem_stage<M, 4, true>(TP), st, pdl, TP, io);
+                    else go(k_tile_stage_t128<M, 4, false, 1>, g, TP.T, smem_stage<M, 4, false>(TP), st, pdl, TP, io);
+                    return;
+                }
+            }
             if (o2) go(k_tile_stage<M, 4, true, 1>, g, TP.T, smem_stage<M, 4, true>(TP), st, pdl, TP, io);
             else go(k_tile_stage<M, 4, false, 1>, g, TP.T, smem_stage<M, 4, false>(TP), st, pdl, TP, io);
         } else {
+            if constexpr (kT128) {
+                if (use_t128(TP)) {
+                    if (o2) go(k_tile_stage_t128<M, 4, true, 2>, g, TP.T, smem_stage<M, 4, true>(TP), st, pdl, TP, io);
+                    else go(k_tile_stage_t128<M, 4, false, 2>, g, TP.T, smem_stage<M, 4, false>(TP), st, pdl, TP, io);
+                    return;
+                }
+            }
             if (o2) go(k_tile_stage<M, 4, true, 2>, g, TP.T, smem_stage<M, 4, true>(TP), st, pdl, TP, io);
             else go(k_tile_stage<M, 4, false, 2>, g, TP.T, smem_stage<M, 4, false>(TP), st, pdl, TP, io);
         }
