@@ -81,7 +81,7 @@ def algo_bytes(ph, precision, kernel):
 # DRAM bytes per real cell of one k_tile_stage launch (dram__bytes_read.sum +
 # dram__bytes_write.sum of one ncu capture of the forward-step workload,
 # profiles/k_tile_stage_fp32_forward_step.md), scaled by the cells of a launch.
-TRAFFIC_B_PER_CELL = {"fp32": {"stage": 150.8}}
+TRAFFIC_B_PER_CELL = {"fp32": {"stage": 153.2}}
 
 
 def build_workload(name):
