@@ -1151,7 +1151,12 @@ struct TileLaunch {
     static cudaError_t prepare(const TileParams& TP) {
         cudaError_t e = cudaSuccess;
         auto set = [&](const void* fn, size_t bytes) {
-            if (e == cudaSuccess)
+            // the limit belongs to the kernel, shared by every solver of the
+            // process: it is only ever raised, never lowered below what a
+            // solver created earlier launches with
+            cudaFuncAttributes fa{};
+            if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, fn);
+            if (e == cudaSuccess && (size_t)fa.maxDynamicSharedSizeBytes < bytes)
                 e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
             if (e == cudaSuccess)
                 e = cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout,

@@ -299,3 +299,24 @@ def test_runs_are_bitwise_reproducible(precision, oracle):
         r = s.run(20, alpha=case["alpha"])
         out.append((s.get_state(), r["R"]))
     assert out[0][0].tobytes() == out[1][0].tobytes() and out[0][1].tobytes() == out[1][1].tobytes()
+
+
+def test_solvers_of_different_tile_sizes_coexist(oracle):
+    """Two solvers of one process whose tile kernels need different amounts of
+    shared memory (FP64_EXACT, 256- and 64-cell tiles): creating the smaller
+    one must not lower the limit the larger one launches with."""
+    case = CASES["step_o2_venk5"]
+    em, ph = case["mesh"](), case["phys"]()
+    mesh = fvgpu.Mesh.from_elements(em)
+    g = oracle.build_mesh(em)
+    p = oracle.physics(ph, em.group_names)
+    q0 = case["ic"](g)
+    want = oracle.run_loop(g, p, q0, case["alpha"], 10)
+    big = fvgpu.Solver(mesh, ph, "fp64_exact", tile_cells=256)
+    small = fvgpu.Solver(mesh, ph, "fp64_exact", tile_cells=64)
+    for s in (big, small):
+        s.set_state(q0)
+        s.run(10, alpha=case["alpha"])
+        assert s.get_state().tobytes() == want["q"].tobytes()
+    big.close()
+    small.close()
