@@ -307,6 +307,24 @@ int fv_mesh_device_order(const fv_mesh* fm, int32_t* new2ref) {
     return FV_OK;
 }
 
+int fv_mesh_tile_layout(const fv_mesh* fm, int32_t tile_cells, int64_t* sizes, int32_t* info, int32_t* halo,
+                        uint32_t* edge_ij, uint16_t* face) {
+    if (!fm || !sizes) return fail(FV_ERR_ARG, "fv_mesh_tile_layout: null");
+    if (tile_cells != 64 && tile_cells != 128 && tile_cells != 256)
+        return fail(FV_ERR_ARG, "tile_cells must be 64, 128 or 256");
+    FaceArrays fa;
+    build_face_arrays(fm->m, fa);
+    TileArrays ta;
+    build_tiles(fm->m, fa, tile_cells, ta);
+    sizes[0] = ta.n_tiles; sizes[1] = ta.max_halo; sizes[2] = ta.max_edges;
+    sizes[3] = (int64_t)ta.halo.size(); sizes[4] = (int64_t)ta.edge_ij.size();
+    if (info) std::memcpy(info, ta.info.data(), ta.info.size() * sizeof(int32_t));
+    if (halo) std::memcpy(halo, ta.halo.data(), ta.halo.size() * sizeof(int32_t));
+    if (edge_ij) std::memcpy(edge_ij, ta.edge_ij.data(), ta.edge_ij.size() * sizeof(uint32_t));
+    if (face) std::memcpy(face, ta.face.data(), ta.face.size() * sizeof(uint16_t));
+    return FV_OK;
+}
+
 // -------------------------------------------------------------- solver ----
 static int validate_physics(const fv_physics* ph, int n_groups_mesh) {
     if (!ph) return fail(FV_ERR_ARG, "physics is null");

@@ -184,6 +184,18 @@ int fv_mesh_geometry(const fv_mesh* m, uint32_t* edge_cells, uint32_t* edge_node
 int fv_mesh_elements(const fv_mesh* m, double* nodes_x, double* nodes_y, int32_t* cells4);
 /* Device cell order: new2ref[n_total] (reference index of each device cell). */
 int fv_mesh_device_order(const fv_mesh* m, int32_t* new2ref);
+/* Host-only inspection of the tile layout a solver builds for tile_cells (64,
+ * 128 or 256), in device numbering (no counterpart in the reference; it
+ * exposes the data the tile kernels index with).  sizes[5] = n_tiles,
+ * max_halo, max_edges, total halo entries, total tile edges.  Each output
+ * array may be NULL (call once for the sizes): info [n_tiles][4] = edge
+ * offset, edge count, halo offset, halo count; halo [total halo] device cell
+ * of each halo slot; edge_ij [total edges] = local i | local j << 16 (owned
+ * cell c -> c - tile start, halo slot h -> tile_cells + h); face
+ * [4][n_real] = tile-local edge | ghost neighbour << 14 | second cell << 15,
+ * 0xFFFF for no face. */
+int fv_mesh_tile_layout(const fv_mesh* m, int32_t tile_cells, int64_t* sizes, int32_t* info, int32_t* halo,
+                        uint32_t* edge_ij, uint16_t* face);
 
 /* ---- solver (device) ---------------------------------------------------- */
 int fv_solver_create(const fv_mesh* m, const fv_physics* ph, int32_t precision, int32_t device,

@@ -267,3 +267,74 @@ def test_host_navier_stokes_kind_matches_oracle(oracle):
             bv = np.array(ph.bcs[names[g]][1] or [0.0] * 4, np.float64)
             assert L.fv_kind_bc(kind, 4, ctypes.c_double(ph.gamma), p(bv), p(qi), p(n), p(b)) == 0
             assert bits_equal(b, oracle.bc(o, g, qi, n))
+
+
+def _tile_layout(m, T):
+    import ctypes as C
+    L = fvgpu.lib()
+    sizes = np.zeros(5, np.int64)
+    i64 = C.POINTER(C.c_int64)
+    rc = L.fv_mesh_tile_layout(m._h, C.c_int32(T), sizes.ctypes.data_as(i64), None, None, None, None)
+    assert rc == 0, L.fv_last_error()
+    nt, _, _, nh, ne = (int(x) for x in sizes)
+    info = np.zeros(4 * nt, np.int32)
+    halo = np.zeros(max(nh, 1), np.int32)
+    eij = np.zeros(max(ne, 1), np.uint32)
+    face = np.zeros(4 * m.n_real, np.uint16)
+    rc = L.fv_mesh_tile_layout(m._h, C.c_int32(T), sizes.ctypes.data_as(i64), info.ctypes.data_as(C.c_void_p),
+                               halo.ctypes.data_as(C.c_void_p), eij.ctypes.data_as(C.c_void_p),
+                               face.ctypes.data_as(C.c_void_p))
+    assert rc == 0, L.fv_last_error()
+    return sizes, info.reshape(nt, 4), halo[:nh], eij[:ne], face.reshape(4, m.n_real)
+
+
+@pytest.mark.parametrize("T", [64, 128, 256])
+def test_tile_layout_indices_stay_in_bounds(T):
+    """Every index the tile kernels read through is inside the buffers they
+    stage: edge endpoints inside the tile's owned + halo slots, face words
+    naming one of the tile's edges with the cell on the stated side, halo
+    lists holding exactly the neighbours outside the tile, and the sizes the
+    shared-memory layout is built from bounding every tile."""
+    meshes = [meshgen.forward_step(n=20), meshgen.naca_ogrid(ni=48, nj=12, r_far=10.0),
+              meshgen.flat_plate(nx0=6, nx1=18, ny=20), meshgen.sod_strip(40, 4)]
+    for em in meshes:
+        m = fvgpu.Mesh.from_elements(em)
+        N, NT = m.n_real, m.n_total
+        sizes, info, halo, eij, face = _tile_layout(m, T)
+        nt, max_halo, max_edges = int(sizes[0]), int(sizes[1]), int(sizes[2])
+        assert nt == (N + T - 1) // T
+        assert max_halo + T <= 65535 and max_edges <= 0x3FFF
+        assert np.all(np.diff(info[:, 0]) == info[:-1, 1]) and np.all(np.diff(info[:, 2]) == info[:-1, 3])
+        assert info[:, 1].max() == max_edges and info[:, 3].max() == max_halo
+        # neighbours of every device cell from the reference edges
+        g = m.geometry()
+        new2ref = m.device_order()
+        ref2new = np.empty_like(new2ref); ref2new[new2ref] = np.arange(NT)
+        ec = ref2new[g["edge_cells"].reshape(-1, 2).astype(np.int64)]
+        nbrs = [set() for _ in range(N)]
+        for a, b in ec:
+            if a < N: nbrs[a].add(int(b))
+            if b < N: nbrs[b].add(int(a))
+        for t in range(nt):
+            c0, nown = t * T, min(T, N - t * T)
+            e0, ne_t, h0, nh_t = (int(x) for x in info[t])
+            hl = halo[h0:h0 + nh_t]
+            outside = set().union(*(nbrs[c] for c in range(c0, c0 + nown))) - set(range(c0, c0 + nown))
+            assert set(hl.tolist()) == outside and len(hl) == len(outside)
+            li, lj = eij[e0:e0 + ne_t] & 0xFFFF, eij[e0:e0 + ne_t] >> 16
+            for x in (li, lj):
+                assert np.all((x < nown) | ((x >= T) & (x < T + nh_t)))
+            assert np.all((li < T) | (lj < T))  # every tile edge touches an owned cell
+            for c in range(c0, c0 + nown):
+                for f in range(4):
+                    w = int(face[f, c])
+                    if w == 0xFFFF:
+                        continue
+                    el, ghost, side = w & 0x3FFF, (w >> 14) & 1, w >> 15
+                    assert el < ne_t
+                    ij = int(eij[e0 + el])
+                    me, other = (ij >> 16, ij & 0xFFFF) if side else (ij & 0xFFFF, ij >> 16)
+                    assert me == c - c0
+                    dev_other = c0 + other if other < T else int(hl[other - T])
+                    assert dev_other in nbrs[c]
+                    assert ghost == (dev_other >= N)
