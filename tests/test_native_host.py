@@ -294,11 +294,14 @@ def test_tile_layout_indices_stay_in_bounds(T):
     stage: edge endpoints inside the tile's owned + halo slots, face words
     naming one of the tile's edges with the cell on the stated side, halo
     lists holding exactly the neighbours outside the tile, and the sizes the
-    shared-memory layout is built from bounding every tile."""
-    meshes = [meshgen.forward_step(n=20), meshgen.naca_ogrid(ni=48, nj=12, r_far=10.0),
-              meshgen.flat_plate(nx0=6, nx1=18, ny=20), meshgen.sod_strip(40, 4)]
-    for em in meshes:
-        m = fvgpu.Mesh.from_elements(em)
+    shared-memory layout is built from bounding every tile (four meshes and a
+    batch of three cases)."""
+    meshes = [fvgpu.Mesh.from_elements(em) for em in
+              (meshgen.forward_step(n=20), meshgen.naca_ogrid(ni=48, nj=12, r_far=10.0),
+               meshgen.flat_plate(nx0=6, nx1=18, ny=20), meshgen.sod_strip(40, 4))]
+    # a batch of strips of uneven sizes: tiles straddle case boundaries
+    meshes.append(fvgpu.Mesh.batch([fvgpu.Mesh.from_elements(meshgen.riemann_strip(n)) for n in (150, 37, 260)]))
+    for m in meshes:
         N, NT = m.n_real, m.n_total
         sizes, info, halo, eij, face = _tile_layout(m, T)
         nt, max_halo, max_edges = int(sizes[0]), int(sizes[1]), int(sizes[2])
