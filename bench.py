@@ -43,10 +43,17 @@ UNIT = "cell-updates/s"
 # array (296 B); FP64 folds the limiter into the gradients; FP32
 # stores stage states, gradients and geometry in FP32, the base in FP64, and
 # writes the FP64 state on the last of the 5 stages only.
+# The fused stage kernel (gradients, limiter, fluxes, update and ghost fill
+# of a two-ring tile in one launch) reads the stage state, centroid and area,
+# the edge data (2 indices + normal, length, face centre, Green-Gauss weight)
+# and the FP64 base state, and writes the new state: FP64 32 + 24 + 1.5*56 +
+# 32 + 32 = 204; FP32 16 + 12 + 1.5*32 + 32 + 16 + 32/5 = 130.4.  Its time
+# step comes from the dt kernel, once per step (reads the state, area and
+# edge indices + normal and length; writes dt).
 ALGO_BYTES = {
-    "fp64_exact": {"stage": 296.0, "grad_lim": 224.0, "stage_o1": 160.0, "dt": 96.0},
-    "fp64": {"stage": 256.0, "grad_lim": 192.0, "stage_o1": 160.0, "dt": 96.0},
-    "fp32": {"stage": 156.4, "grad_lim": 102.0, "stage_o1": 110.0, "dt": 58.0},
+    "fp64_exact": {"stage": 296.0, "grad_lim": 224.0, "stage_o1": 160.0, "dt": 96.0, "fused": 204.0},
+    "fp64": {"stage": 256.0, "grad_lim": 192.0, "stage_o1": 160.0, "dt": 96.0, "fused": 204.0},
+    "fp32": {"stage": 156.4, "grad_lim": 102.0, "stage_o1": 110.0, "dt": 58.0, "fused": 130.4},
 }
 # The diffusive kinds (same accounting, s = 8 or 4).
 # Navier-Stokes (V = 4, MUSCL): the stage kernel reads q, the raw gradients
@@ -78,10 +85,14 @@ def algo_bytes(ph, precision, kernel):
     return ALGO_BYTES[precision][kernel]
 
 
-# DRAM bytes per real cell of one k_tile_stage launch (dram__bytes_read.sum +
-# dram__bytes_write.sum of one ncu capture of the forward-step workload,
-# profiles/k_tile_stage_fp32_forward_step.md), scaled by the cells of a launch.
-TRAFFIC_B_PER_CELL = {"fp32": {"stage": 153.2}}
+# DRAM bytes per real cell of one stage-kernel launch on the forward-step
+# workload (dram__bytes_read.sum + dram__bytes_write.sum of one ncu capture
+# per precision mode), scaled by the cells of a launch; each entry names the
+# capture it comes from.  Modes and workloads without a capture report null.
+TRAFFIC_B_PER_CELL = {
+    ("step", "fp32"): (153.2, "ncu --set full -k regex:k_tile_stage -s 30 -c 2, "
+                              "bench.py --precision fp32 --steps 20 --warmup 3 --no-cpu-baseline"),
+}
 
 
 def build_workload(name):
@@ -292,8 +303,10 @@ def measure_mode(args, em, mesh, geo, ph, alpha, ic, precision, local, dist, wor
     if args.tile_cells < 0:  # autotuned tile size
         s = fvgpu.Solver.create_tuned(mesh, ph, precision, q0, alpha=alpha, steps=3, device=local)
     else:
-        s = fvgpu.Solver(mesh, ph, precision, device=local, tile_cells=args.tile_cells)
+        s = fvgpu.Solver(mesh, ph, precision, device=local, tile_cells=args.tile_cells,
+                         stage_kernels=args.stage_kernels)
         s.tile_cells = args.tile_cells or 128
+    fused = s.stage_kernels == "fused"
     stream = torch.cuda.Stream(device=local)
     s.set_stream(stream.cuda_stream)
     s.set_state(q0)
@@ -335,19 +348,29 @@ def measure_mode(args, em, mesh, geo, ph, alpha, ic, precision, local, dist, wor
     out["per_launch_ms"] = {kinds[k]: (ms_k[k] / cnt_k[k] if cnt_k[k] else 0.0) for k in range(5)}
     out["share"] = {kinds[k]: float(ms_k[k] / ms_k.sum()) for k in range(5)}
     peak, peak_kind = measured_peak_hbm()
-    kb = algo_bytes(ph, precision, "stage") * N
+    kb = (ALGO_BYTES[precision]["fused"] if fused else algo_bytes(ph, precision, "stage")) * N
     achieved = kb / (out["per_launch_ms"]["stage"] / 1e3) / 1e9
-    out["roofline"] = {"bound": "hbm", "kernel": "flux + RK update + ghost fill (k_tile_stage)",
+    out["stage_kernels"] = s.stage_kernels
+    kname = ("gradients + limiter + flux + RK update + ghost fill of a two-ring tile (k_tile_fused)" if fused
+             else "flux + RK update + ghost fill (k_tile_stage)")
+    out["roofline"] = {"bound": "hbm", "kernel": kname,
                        "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                        "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind,
-                       "traffic": (TRAFFIC_B_PER_CELL[precision]["stage"] * N
-                                   if args.workload == "step" and precision in TRAFFIC_B_PER_CELL else None),
-                       "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, forward-step capture",
+                       "traffic": None, "traffic_source": "no ncu capture of this mode and workload",
                        "algorithmic_bytes_per_launch": kb}
-    if ph.order2 or ph.diffusive:
+    cap = TRAFFIC_B_PER_CELL.get((args.workload, precision))
+    if cap is not None:
+        out["roofline"]["traffic"] = cap[0] * N
+        out["roofline"]["traffic_source"] = ("dram__bytes_read.sum + dram__bytes_write.sum per launch of the "
+                                             "stage kernel, from: " + cap[1])
+    if (ph.order2 or ph.diffusive) and not fused:
         kg = algo_bytes(ph, precision, "grad_lim") * N
         out["roofline_grad_lim"] = {"achieved": kg / (out["per_launch_ms"]["grad_lim"] / 1e3) / 1e9,
                                     "frac": kg / (out["per_launch_ms"]["grad_lim"] / 1e3) / 1e9 / peak}
+    if out["per_launch_ms"]["dt"] > 0 and ph.V == 4:
+        kd = ALGO_BYTES[precision]["dt"] * N
+        out["roofline_dt"] = {"achieved": kd / (out["per_launch_ms"]["dt"] / 1e3) / 1e9,
+                              "frac": kd / (out["per_launch_ms"]["dt"] / 1e3) / 1e9 / peak}
     return out
 
 
@@ -443,15 +466,56 @@ def e2e_mode(args, mesh, ph, alpha, m, local, dist, world):
             "pipelined_output_equals_serial": same}
 
 
-def l2_rho_p(q, q_ref, n_real, gamma=1.4):
+def err_rho_p(q, q_ref, n_real, gamma=1.4):
+    """Relative L1 and L2 errors of density and pressure over the real cells."""
     a = q.reshape(-1, 4)[:n_real]; b = q_ref.reshape(-1, 4)[:n_real]
 
     def rp(x):
         return x[:, 0], (gamma - 1) * (x[:, 3] - 0.5 * (x[:, 1] ** 2 + x[:, 2] ** 2) / x[:, 0])
 
     (ra, pa), (rb, pb) = rp(a), rp(b)
+    l1 = lambda u, v: float(np.sum(np.abs(u - v)) / np.sum(np.abs(v)))
     l2 = lambda u, v: float(np.sqrt(np.sum((u - v) ** 2) / np.sum(v ** 2)))
-    return {"density": l2(ra, rb), "pressure": l2(pa, pb)}
+    return {"density": {"l1": l1(ra, rb), "l2": l2(ra, rb)}, "pressure": {"l1": l1(pa, pb), "l2": l2(pa, pb)}}
+
+
+def exact_run_state(mesh, geo, ph, alpha, ic, steps, local):
+    """The FP64_EXACT path's state after `steps` time steps: the reference's
+    FP64 arithmetic, bit for bit (the oracle restates the positivity guard,
+    which the reference does not have, the same way)."""
+    import fvgpu
+    s = fvgpu.Solver(mesh, ph, "fp64_exact", device=local)
+    s.set_state(ic(mesh, geo))
+    info = s.run(steps, alpha=alpha, print_interval=10 ** 9)
+    q = s.get_state()
+    s.close()
+    return q, info["step"]
+
+
+def run_batch_modes(args, local, dist, world):
+    """The batched Riemann-strip workload (256 strips of 2k-200k cells in one
+    solver, autotuned tile size, 500 RK5 steps) in FP32-bulk and plain FP64:
+    cell-updates/s per stage and the L2 error against the exact Riemann
+    solution."""
+    import copy
+    ba = copy.copy(args)
+    ba.workload, ba.steps, ba.warmup, ba.tile_cells = "batch", args.batch_steps, 3, -1
+    em, ph, alpha, ic, desc = build_workload("batch")
+    mesh = make_mesh(em)
+    geo = mesh.geometry()
+    res = {prec: measure_mode(ba, em, mesh, geo, ph, alpha, ic, prec, local, dist, world) for prec in ("fp64", "fp32")}
+    _, states = meshgen.riemann_strip_sizes()
+    out = {"workload": desc, "n_real_cells": mesh.n_real, "n_cases": mesh.n_cases, "steps": ba.steps}
+    for prec, r in res.items():
+        out[prec] = {"value": r["value"], "ms_per_step": r["ms_per_step"], "tile_cells": r["solver"].tile_cells,
+                     "stage_roofline_frac": r["roofline"]["frac"],
+                     "l2_error_vs_exact_riemann": batch_error_vs_exact(mesh, geo, r["q_final"], r["case_times"], states),
+                     "state_finite": bool(r["state_finite"]), "clocks": r["clocks"]}
+        r["solver"].close()
+    out["fp32_speedup_over_fp64"] = out["fp32"]["value"] / out["fp64"]["value"]
+    out["fp32_minus_fp64_density_error"] = (out["fp32"]["l2_error_vs_exact_riemann"]["density"]
+                                            - out["fp64"]["l2_error_vs_exact_riemann"]["density"])
+    return out
 
 
 def batch_error_vs_exact(mesh, geo, q, times, states, gamma=1.4):
@@ -539,6 +603,12 @@ def main():
     ap.add_argument("--precision", default="all", choices=["all", "fp64_exact", "fp64", "fp32"],
                     help="all: FP32-bulk (headline) and plain FP64 in one line")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--stage-kernels", default="auto", choices=["auto", "split", "fused"],
+                    help="second-order Euler stage kernels: fused (one per stage) where the physics allow, "
+                         "or split gradient and flux kernels")
+    ap.add_argument("--batch-steps", type=int, default=500,
+                    help="steps of the batched Riemann-strip workload reported beside the forward step "
+                         "(0: not run)")
     ap.add_argument("--tile-cells", type=int, default=None,
                     help="cells per tile: 64/128/256, 0 = library default (128), -1 = autotuned "
                          "(default: autotuned for the batch workload, else 0)")
@@ -574,6 +644,10 @@ def main():
     head = modes[-1]  # FP32-bulk when both run
     m = res[head]
     e2e = e2e_mode(args, mesh, ph, alpha, m, local, dist, world)
+    batch_line = None
+    if args.workload == "step" and args.batch_steps > 0:
+        # every rank takes the same steps (replicas under torchrun)
+        batch_line = run_batch_modes(args, local, dist, world)
     if rank == 0:
         line = {"metric": METRIC, "value": m["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": m["ms_per_step"], "higher_is_better": True,
@@ -589,14 +663,22 @@ def main():
                 "kernel_ms_per_launch": m["per_launch_ms"], "kernel_time_share": m["share"],
                 "clocks": m["clocks"], "state_finite": bool(m["state_finite"])}
         line["modes"] = {p: {"value": r["value"], "ms_per_step": r["ms_per_step"], "roofline_frac": r["roofline"]["frac"],
+                             "stage_kernels": r["stage_kernels"],
                              "grad_lim_frac": r.get("roofline_grad_lim", {}).get("frac"),
+                             "dt_frac": r.get("roofline_dt", {}).get("frac"),
                              "kernel_ms_per_launch": r["per_launch_ms"], "clocks": r["clocks"],
                              "state_finite": bool(r["state_finite"])} for p, r in res.items()}
         if "fp64" in res and "fp32" in res and ph.V == 4:
-            line["fp32_vs_fp64"] = {"l2_rel_error": l2_rho_p(res["fp32"]["q_final"], res["fp64"]["q_final"],
-                                                             mesh.n_real),
-                                    "after_steps": args.warmup + args.steps,
-                                    "speedup": res["fp32"]["value"] / res["fp64"]["value"]}
+            line["fp32_vs_fp64"] = {"speedup": res["fp32"]["value"] / res["fp64"]["value"]}
+            if args.workload in ("step", "naca", "sod"):
+                # both modes against the FP64_EXACT run of the same steps
+                q_ex, n_ex = exact_run_state(mesh, geo, ph, alpha, ic, args.warmup + args.steps, local)
+                line["error_vs_fp64_exact"] = {
+                    "reference": "FP64_EXACT path (the reference's FP64 arithmetic bit for bit), same mesh, "
+                                 "same initial state, same steps",
+                    "after_steps": n_ex,
+                    "fp32": err_rho_p(res["fp32"]["q_final"], q_ex, mesh.n_real),
+                    "fp64": err_rho_p(res["fp64"]["q_final"], q_ex, mesh.n_real)}
         if args.workload == "batch":
             _, states = meshgen.riemann_strip_sizes()
             errs = {p: batch_error_vs_exact(mesh, geo, r["q_final"], r["case_times"], states) for p, r in res.items()}
@@ -604,6 +686,8 @@ def main():
             if "fp64" in errs and "fp32" in errs:
                 line["l2_error_vs_exact_riemann"]["fp32_minus_fp64_density"] = \
                     errs["fp32"]["density"] - errs["fp64"]["density"]
+        if args.workload == "step" and args.batch_steps > 0:
+            line["modes"]["batch"] = batch_line
         if not args.no_cpu_baseline and world == 1 and args.workload in REF_FOR:
             r = reference_samples(em, 1, 1, 25, args.workload)
             if r is not None:

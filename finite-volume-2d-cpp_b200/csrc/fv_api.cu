@@ -14,6 +14,7 @@
 #include "fv_launch.h"
 #include "fv_mesh.h"
 #include "fv_tile.cuh"
+#include "fv_fused.cuh"
 #include "fv_adjoint.h"
 #include <cmath>
 
@@ -65,6 +66,9 @@ struct fv_solver {
     int64_t n_real = 0, n_total = 0, n_bound = 0;
     int n_tiles = 0;
     TileParams TP{};
+    // the fused stage kernel over two-ring tiles (its Params are TP.P at launch)
+    bool fused = false;
+    FusedParams FPm{};
     // device buffers
     std::vector<void*> allocs;
     double* qbase[2] = {nullptr, nullptr};   // FP64 step-start state (RK1 alternates)
@@ -316,8 +320,32 @@ int fv_mesh_tile_layout(const fv_mesh* fm, int32_t tile_cells, int64_t* sizes, i
     build_face_arrays(fm->m, fa);
     TileArrays ta;
     build_tiles(fm->m, fa, tile_cells, ta);
+    // the layouts a solver refuses (16-bit tile-local indices) are refused here too
+    if (ta.max_halo + tile_cells > 65535 || ta.max_edges > kFaceEdgeMask)
+        return fail(FV_ERR_MESH, "tile halo too large for 16-bit local indices");
     sizes[0] = ta.n_tiles; sizes[1] = ta.max_halo; sizes[2] = ta.max_edges;
     sizes[3] = (int64_t)ta.halo.size(); sizes[4] = (int64_t)ta.edge_ij.size();
+    if (info) std::memcpy(info, ta.info.data(), ta.info.size() * sizeof(int32_t));
+    if (halo) std::memcpy(halo, ta.halo.data(), ta.halo.size() * sizeof(int32_t));
+    if (edge_ij) std::memcpy(edge_ij, ta.edge_ij.data(), ta.edge_ij.size() * sizeof(uint32_t));
+    if (face) std::memcpy(face, ta.face.data(), ta.face.size() * sizeof(uint16_t));
+    return FV_OK;
+}
+
+int fv_mesh_tile2_layout(const fv_mesh* fm, int32_t tile_cells, int64_t* sizes, int32_t* info, int32_t* halo,
+                         uint32_t* edge_ij, uint16_t* face) {
+    if (!fm || !sizes) return fail(FV_ERR_ARG, "fv_mesh_tile2_layout: null");
+    if (tile_cells != 64 && tile_cells != 128 && tile_cells != 256)
+        return fail(FV_ERR_ARG, "tile_cells must be 64, 128 or 256");
+    FaceArrays fa;
+    build_face_arrays(fm->m, fa);
+    Tile2Arrays ta;
+    build_tiles2(fm->m, fa, tile_cells, ta);
+    if (ta.max_slots > 65535 || ta.max_edges > kFaceEdgeMask)
+        return fail(FV_ERR_MESH, "two-ring tiles too large for 16-bit local indices");
+    sizes[0] = ta.n_tiles; sizes[1] = ta.max_slots; sizes[2] = ta.max_grad; sizes[3] = ta.max_edges;
+    sizes[4] = ta.max_flux; sizes[5] = (int64_t)ta.halo.size(); sizes[6] = (int64_t)ta.edge_ij.size();
+    sizes[7] = (int64_t)ta.face.size() / 4;
     if (info) std::memcpy(info, ta.info.data(), ta.info.size() * sizeof(int32_t));
     if (halo) std::memcpy(halo, ta.halo.data(), ta.halo.size() * sizeof(int32_t));
     if (edge_ij) std::memcpy(edge_ij, ta.edge_ij.data(), ta.edge_ij.size() * sizeof(uint32_t));
@@ -456,6 +484,52 @@ int fv_solver_create_ex(const fv_mesh* fm, const fv_physics* ph, int32_t precisi
     if ((rc = upload_v(s.get(), m.new2ref, &n2r))) return rc;
     s->new2ref = const_cast<int32_t*>(n2r);
     CK(tile::prepare(precision, TP));
+    {
+        // one fused kernel per stage for the second-order Roe kinds
+        const int sk = opt ? opt->stage_kernels : FV_STAGE_AUTO;
+        if (sk < FV_STAGE_AUTO || sk > FV_STAGE_FUSED) return fail(FV_ERR_ARG, "unknown stage_kernels");
+        const bool can_fuse = ph->V == 4 && ph->order2 && (ph->flux == FV_FLUX_ROE_FS || ph->flux == FV_FLUX_ROE_ST) &&
+                              !ph->diffusive && !ph->smooth_residuals;
+        if (sk == FV_STAGE_FUSED && !can_fuse)
+            return fail(FV_ERR_UNSUPPORTED, "the fused stage kernel needs a second-order Roe kind without "
+                                            "diffusive terms or residual smoothing");
+        if (can_fuse && sk != FV_STAGE_SPLIT) {
+            Tile2Arrays t2;
+            build_tiles2(m, fa, tile_cells, t2);
+            FusedParams& F = s->FPm;
+            F.T = tile_cells;
+            F.max_slots = t2.max_slots; F.max_grad = t2.max_grad;
+            F.max_edges = t2.max_edges; F.max_flux = t2.max_flux;
+            const bool fits = t2.max_slots <= 65535 && t2.max_edges <= kFaceEdgeMask &&
+                              tile::smem_fused(precision, F) <= (size_t)227 * 1024;
+            if (!fits && sk == FV_STAGE_FUSED)
+                return fail(FV_ERR_MESH, "two-ring tiles too large for the fused stage kernel at this tile size");
+            if (fits) {
+                const int32_t* i2; const int32_t* h2; const uint32_t* e2; const uint16_t* f2;
+                if ((rc = upload_v(s.get(), t2.info, &i2))) return rc;
+                F.info = reinterpret_cast<const int4*>(i2);
+                if ((rc = upload_v(s.get(), t2.halo, &h2))) return rc;
+                F.halo = h2;
+                if ((rc = upload_v(s.get(), t2.edge_ij, &e2))) return rc;
+                F.edge_ij = e2;
+                if ((rc = upload_v(s.get(), t2.face, &f2))) return rc;
+                F.face = reinterpret_cast<const uint2*>(f2);
+                if ((rc = upload_s(s.get(), t2.enx, &F.enx))) return rc;
+                if ((rc = upload_s(s.get(), t2.eny, &F.eny))) return rc;
+                if ((rc = upload_s(s.get(), t2.ele, &F.ele))) return rc;
+                if ((rc = upload_s(s.get(), t2.exf, &F.exf))) return rc;
+                if ((rc = upload_s(s.get(), t2.eyf, &F.eyf))) return rc;
+                if ((rc = upload_s(s.get(), t2.eg, &F.eg))) return rc;
+                std::vector<double> cca(4 * (size_t)m.n_total, 0.0);
+                for (size_t n = 0; n < (size_t)m.n_total; ++n) {
+                    cca[4 * n] = ta.ccx[n]; cca[4 * n + 1] = ta.ccy[n]; cca[4 * n + 2] = fa.area[n];
+                }
+                if ((rc = upload_s(s.get(), cca, &F.cca))) return rc;
+                CK(tile::prepare_fused(precision, F));
+                s->fused = true;
+            }
+        }
+    }
     const size_t nq = (size_t)m.n_total * ph->V;
     CK(s->alloc(&s->qbase[0], nq)); CK(s->alloc(&s->qbase[1], nq));
     if (s->f32) {
@@ -544,7 +618,7 @@ int fv_solver_create_tuned(const fv_mesh* fm, const fv_physics* ph, int32_t prec
     double best_ms = 0.0;
     int best_t = 0;
     for (int t : {64, 128, 256}) {
-        fv_solver_options o{t};
+        fv_solver_options o{t, FV_STAGE_AUTO};
         fv_solver* s = nullptr;
         int rc = fv_solver_create_ex(fm, ph, precision, device, &o, &s);
         if (rc == FV_ERR_MESH) continue;  // tile halo too large for this size
@@ -750,8 +824,12 @@ static int enqueue_step(fv_solver* s, const std::vector<double>& alpha, int b, E
     // every kernel after step_begin is a programmatic dependent of the one
     // before it (its constant tile data is staged during that one's tail)
     const bool pdl = true;
-    const bool grads = TP.P.order2 || TP.P.diffusive;
+    // the fused stage kernel computes its gradients itself: the step's dt
+    // comes from the dt kernel, as in first order
+    const bool grads = (TP.P.order2 || TP.P.diffusive) && !s->fused;
     if (!grads) { tile::launch_dt(s->precision, TP, io, st, pdl); ++n; mark(KK_DT); }
+    FusedParams FPl = s->FPm;
+    FPl.P = TP.P;
     const int ns = (int)alpha.size();
     const void* in = s->sbase[b];
     for (int k = 0; k < ns; ++k) {
@@ -784,6 +862,8 @@ static int enqueue_step(fv_solver* s, const std::vector<double>& alpha, int b, E
             launch_smooth(TP.P, s->nbr, s->qts[1], s->qts[0], s->qts[2], st); ++n; mark(KK_STAGE);
             so.qt = s->qts[2];
             tile::launch_stage(s->precision, TP, so, st, pdl, 2); ++n; mark(KK_STAGE);
+        } else if (s->fused) {
+            tile::launch_fused(s->precision, FPl, so, st, pdl, s->n_tiles); ++n; mark(KK_STAGE);
         } else {
             tile::launch_stage(s->precision, TP, so, st, pdl); ++n; mark(KK_STAGE);
         }
@@ -948,6 +1028,11 @@ int fv_solver_info(fv_solver* s, int64_t* out) {
     out[0] = s->n_tiles; out[1] = s->TP.T; out[2] = s->TP.max_halo; out[3] = s->TP.max_edges;
     out[4] = s->precision; out[5] = (int64_t)s->ssz;
     return FV_OK;
+}
+
+int fv_solver_stage_kernels(fv_solver* s) {
+    if (!s) return fail(FV_ERR_ARG, "null solver");
+    return s->fused ? FV_STAGE_FUSED : FV_STAGE_SPLIT;
 }
 
 int fv_last_run_stats(fv_solver* s, double* device_ms, int64_t* kernel_launches) {
@@ -1115,12 +1200,13 @@ int fv_stage_dt_noalloc(fv_solver* s, const double* q_device, double* dt_device,
         return fail(FV_ERR_ARG, "fv_stage_dt_noalloc: mesh needs " + std::to_string(need) +
                                     " bytes of scratch, more than the fixed " + std::to_string(kNoAllocBytes) +
                                     " (about 200k cells in FP64, 150k in FP32); use fv_stage_dt");
-    CK(cudaSetDevice(s->device));
     if (s->device < 0 || s->device >= 128) return fail(FV_ERR_ARG, "fv_stage_dt_noalloc: device ordinal out of range");
+    CK(cudaSetDevice(s->device));
     unsigned char* base = nullptr;
     {
         // one-time set-up per device: the host-side symbol is only a stand-in,
-        // the kernels need the scratch array's device address
+        // the kernels need the scratch array's device address (cached for the
+        // life of the device's primary context)
         std::lock_guard<std::mutex> lock(g_noalloc_mu);
         if (!g_noalloc_base[s->device]) {
             void* p = nullptr;

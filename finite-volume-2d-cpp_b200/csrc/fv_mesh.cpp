@@ -426,6 +426,79 @@ void build_tiles(const HostMesh& m, const FaceArrays& fa, int T, TileArrays& ta)
     for (int64_t n = 0; n < NT; ++n) { ta.ccx[n] = m.ccx[m.new2ref[n]]; ta.ccy[n] = m.ccy[m.new2ref[n]]; }
 }
 
+void build_tiles2(const HostMesh& m, const FaceArrays& fa, int T, Tile2Arrays& ta) {
+    const int64_t N = m.n_real, NT = m.n_total, F = HostMesh::MAXF;
+    ta = Tile2Arrays();
+    ta.tile_cells = T;
+    ta.n_tiles = (int)((N + T - 1) / T);
+    ta.info.assign((size_t)ta.n_tiles * 8, 0);
+    std::vector<int32_t> local(NT, -1);          // device cell -> local slot in the current tile
+    std::vector<int32_t> edge_stamp(m.n_edges, -1), edge_local(m.n_edges, 0);
+    std::vector<int32_t> touched, ring1;
+    for (int t = 0; t < ta.n_tiles; ++t) {
+        const int64_t c0 = (int64_t)t * T, c1 = std::min<int64_t>(c0 + T, N);
+        const int edge_off = (int)ta.edge_ij.size(), halo_off = (int)ta.halo.size();
+        const int face_off = (int)(ta.face.size() / 4);
+        int n_halo = 0, n_edges = 0;
+        touched.clear();
+        ring1.clear();
+        for (int64_t c = c0; c < c1; ++c) { local[c] = (int32_t)(c - c0); touched.push_back((int32_t)c); }
+        auto loc = [&](int32_t dev) {
+            if (local[dev] < 0) {
+                local[dev] = T + n_halo++;
+                ta.halo.push_back(dev);
+                touched.push_back(dev);
+            }
+            return local[dev];
+        };
+        // faces of one gradient cell (device index c < N); new edges get the next local index
+        auto add_faces = [&](int64_t c, uint16_t* w) {
+            for (int k = 0; k < m.n_faces[c]; ++k) {
+                const int32_t e = m.face_edge[c * F + k];
+                const int side = m.face_side[c * F + k];
+                if (edge_stamp[e] != t) {
+                    edge_stamp[e] = t;
+                    edge_local[e] = n_edges++;
+                    const int32_t di = m.ref2new[m.edge_cells[2 * e]], dj = m.ref2new[m.edge_cells[2 * e + 1]];
+                    const uint32_t li = (uint32_t)loc(di), lj = (uint32_t)loc(dj);
+                    ta.edge_ij.push_back(li | (lj << 16));
+                    ta.enx.push_back(m.enx[e]); ta.eny.push_back(m.eny[e]); ta.ele.push_back(m.elen[e]);
+                    ta.exf.push_back(m.ecx[e]); ta.eyf.push_back(m.ecy[e]);
+                    ta.eg.push_back(fa.g[(size_t)k * N + c]);
+                }
+                const uint32_t other = m.edge_cells[2 * e + (side ? 0 : 1)];
+                const int ghost = other >= (uint32_t)N ? 1 : 0;
+                w[k] = (uint16_t)(edge_local[e] | (ghost << 14) | (side << 15));
+            }
+        };
+        // owned cells: the flux edges and ring 1
+        std::vector<uint16_t> words((size_t)T * 4, 0xFFFF);
+        for (int64_t c = c0; c < c1; ++c) add_faces(c, &words[(size_t)(c - c0) * 4]);
+        const int n_flux = n_edges, n1 = n_halo;
+        for (int h = 0; h < n1; ++h) ring1.push_back(ta.halo[halo_off + h]);
+        // ring-1 real cells: their remaining edges and ring 2
+        words.resize((size_t)(T + n1) * 4, 0xFFFF);
+        for (int h = 0; h < n1; ++h)
+            if (ring1[h] < N) add_faces(ring1[h], &words[(size_t)(T + h) * 4]);
+        const int n2 = n_halo - n1;
+        ta.face.insert(ta.face.end(), words.begin(), words.end());
+        // each tile's edge run starts on a multiple of 4 entries, so that it
+        // is copied in 16-byte chunks
+        while (ta.edge_ij.size() % 4) {
+            ta.edge_ij.push_back(0);
+            for (auto* v : {&ta.enx, &ta.eny, &ta.ele, &ta.exf, &ta.eyf, &ta.eg}) v->push_back(0.);
+        }
+        int32_t* inf = &ta.info[(size_t)8 * t];
+        inf[0] = edge_off; inf[1] = n_edges; inf[2] = n_flux; inf[3] = halo_off;
+        inf[4] = n1; inf[5] = n2; inf[6] = face_off; inf[7] = 0;
+        ta.max_slots = std::max(ta.max_slots, T + n1 + n2);
+        ta.max_grad = std::max(ta.max_grad, T + n1);
+        ta.max_edges = std::max(ta.max_edges, (n_edges + 3) / 4 * 4);
+        ta.max_flux = std::max(ta.max_flux, n_flux);
+        for (int32_t d : touched) local[d] = -1;
+    }
+}
+
 // ----------------------------------------------------------------------------
 // MSH 4.1 ASCII reader.  Accepts what fvhyper's reader accepts for a single
 // partition: $PhysicalNames, $Entities (curve -> physical tag, token 8 of a

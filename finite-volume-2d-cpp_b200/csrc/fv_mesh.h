@@ -75,6 +75,30 @@ struct TileArrays {
 };
 void build_tiles(const HostMesh& m, const FaceArrays& fa, int tile_cells, TileArrays& ta);
 
+// Two-ring tiles of the fused stage kernel, which computes the gradients and
+// limiters of its own cells and of their face neighbours (ring 1) before the
+// fluxes of its edges, so it stages the states of ring 2 as well.  Local
+// slots: owned cells [0, T), ring 1 [T, T + n1) (face neighbours of owned
+// cells, real or ghost), ring 2 [T + n1, T + n1 + n2) (face neighbours of
+// ring-1 real cells not already local).  Local edges: the flux edges (those
+// touching an owned cell, in first-visit order over the owned cells' faces)
+// first, then the edges of ring-1 real cells not yet listed.  Every
+// gradient slot (owned and ring 1) has four face words (local edge | ghost
+// neighbour << 14 | side << 15, 0xFFFF = none) in increasing reference edge
+// order; ring-1 ghosts and the unused owned slots of a last, partial tile
+// have none.
+struct Tile2Arrays {
+    int tile_cells = 0, n_tiles = 0;
+    int max_slots = 0, max_grad = 0, max_edges = 0, max_flux = 0;  // max_edges: a multiple of 4
+    std::vector<int32_t> info;        // [n_tiles][8]: edge_off, n_edges, n_flux, halo_off, n1, n2, face_off, 0
+    std::vector<int32_t> halo;        // device cell index of each ring-1, then ring-2 slot
+    std::vector<uint32_t> edge_ij;    // local i | local j << 16, reference orientation; each
+                                      // tile's run padded to a multiple of 4 entries
+    std::vector<double> enx, eny, ele, exf, eyf, eg;  // per local edge
+    std::vector<uint16_t> face;       // [sum over tiles of (T + n1)][4]
+};
+void build_tiles2(const HostMesh& m, const FaceArrays& fa, int tile_cells, Tile2Arrays& ta);
+
 // Builds the reference geometry from an element mesh (mesh.cpp:130-260,
 // 623-669).  Returns "" on success, else an error message.
 std::string build_geometry(HostMesh& m);

@@ -21,6 +21,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <mutex>
 #include <type_traits>
 
 #include "fv_internal.h"
@@ -1150,6 +1151,11 @@ template <class M>
 struct TileLaunch {
     static cudaError_t prepare(const TileParams& TP) {
         cudaError_t e = cudaSuccess;
+        // solvers created on several host threads at once read and raise the
+        // same kernels' limits: one at a time, so a smaller request never
+        // overwrites a larger one
+        static std::mutex mu;
+        std::lock_guard<std::mutex> lock(mu);
         auto set = [&](const void* fn, size_t bytes) {
             // the limit belongs to the kernel, shared by every solver of the
             // process: it is only ever raised, never lowered below what a

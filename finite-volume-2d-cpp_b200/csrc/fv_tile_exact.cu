@@ -1,6 +1,7 @@
 // Tile kernels with the exact (reference evaluation order) FP64 policy.
 // Compiled with -fmad=false so that no multiply-add is contracted.
 #include "fv_tile.cuh"
+#include "fv_fused.cuh"
 
 namespace fvgpu {
 namespace tile {
@@ -13,6 +14,11 @@ void launch_gradlim_exact(const TileParams& TP, const TileIO& io, cudaStream_t s
 }
 void launch_stage_exact(const TileParams& TP, const TileIO& io, cudaStream_t st, bool pdl, int phase) {
     TileLaunch<MExact>::stage(TP, io, st, pdl, phase);
+}
+cudaError_t prepare_fused_exact(const FusedParams& FP) { return FusedLaunch<MExact>::prepare(FP); }
+size_t smem_fused_exact(const FusedParams& FP) { return FusedLaunch<MExact>::smem(FP); }
+void launch_fused_exact(const FusedParams& FP, const TileIO& io, cudaStream_t st, bool pdl, int n_tiles) {
+    FusedLaunch<MExact>::stage(FP, io, st, pdl, n_tiles);
 }
 }  // namespace tile
 }  // namespace fvgpu

@@ -1,6 +1,7 @@
 // Tile kernels with the FP64 and FP32-bulk fast policies, and the
 // per-precision dispatch.
 #include "fv_tile.cuh"
+#include "fv_fused.cuh"
 
 namespace fvgpu {
 namespace tile {
@@ -8,6 +9,9 @@ cudaError_t prepare_exact(const TileParams& TP);
 void launch_dt_exact(const TileParams& TP, const TileIO& io, cudaStream_t st, bool pdl);
 void launch_gradlim_exact(const TileParams& TP, const TileIO& io, cudaStream_t st, bool with_dt, bool pdl);
 void launch_stage_exact(const TileParams& TP, const TileIO& io, cudaStream_t st, bool pdl, int phase);
+cudaError_t prepare_fused_exact(const FusedParams& FP);
+size_t smem_fused_exact(const FusedParams& FP);
+void launch_fused_exact(const FusedParams& FP, const TileIO& io, cudaStream_t st, bool pdl, int n_tiles);
 
 cudaError_t prepare(int precision, const TileParams& TP) {
     if (precision == 0) return prepare_exact(TP);
@@ -28,6 +32,21 @@ void launch_stage(int precision, const TileParams& TP, const TileIO& io, cudaStr
     if (precision == 0) launch_stage_exact(TP, io, st, pdl, phase);
     else if (precision == 1) TileLaunch<MF64>::stage(TP, io, st, pdl, phase);
     else TileLaunch<MF32>::stage(TP, io, st, pdl, phase);
+}
+cudaError_t prepare_fused(int precision, const FusedParams& FP) {
+    if (precision == 0) return prepare_fused_exact(FP);
+    if (precision == 1) return FusedLaunch<MF64>::prepare(FP);
+    return FusedLaunch<MF32>::prepare(FP);
+}
+size_t smem_fused(int precision, const FusedParams& FP) {
+    if (precision == 0) return smem_fused_exact(FP);
+    if (precision == 1) return FusedLaunch<MF64>::smem(FP);
+    return FusedLaunch<MF32>::smem(FP);
+}
+void launch_fused(int precision, const FusedParams& FP, const TileIO& io, cudaStream_t st, bool pdl, int n_tiles) {
+    if (precision == 0) launch_fused_exact(FP, io, st, pdl, n_tiles);
+    else if (precision == 1) FusedLaunch<MF64>::stage(FP, io, st, pdl, n_tiles);
+    else FusedLaunch<MF32>::stage(FP, io, st, pdl, n_tiles);
 }
 }  // namespace tile
 }  // namespace fvgpu

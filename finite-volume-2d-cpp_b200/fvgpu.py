@@ -215,15 +215,19 @@ def physics_struct(ph: _phys.Physics, group_names: Sequence[str]):
 class Solver:
     """Device solver for one mesh + physics (one CUDA device)."""
 
+    STAGE_KERNELS = {"auto": 0, "split": 1, "fused": 2}
+
     def __init__(self, mesh: Mesh, ph: _phys.Physics, precision: str = "fp64_exact", device: int = 0,
-                 tile_cells: int = 0):
+                 tile_cells: int = 0, stage_kernels: str = "auto"):
+        """stage_kernels: "auto" (the fused stage kernel where the physics
+        allow it), "split" (gradient and flux kernels) or "fused"."""
         self.mesh = mesh
         self.phys = ph
         self.V = ph.V
         self.precision = precision
         self._ps = physics_struct(ph, mesh.group_names)
         h = C.c_void_p()
-        opt = (C.c_int32 * 1)(int(tile_cells))
+        opt = (C.c_int32 * 2)(int(tile_cells), self.STAGE_KERNELS[stage_kernels])
         _check(lib().fv_solver_create_ex(mesh._h, C.byref(self._ps), C.c_int32(PREC[precision]), C.c_int32(device),
                                          opt, C.byref(h)))
         self._h = h
@@ -249,6 +253,11 @@ class Solver:
         self.tile_cells = t.value
         self.tuned_ms_per_step = ms.value
         return self
+
+    @property
+    def stage_kernels(self):
+        """"fused" or "split": the stage kernels this solver runs."""
+        return {2: "fused", 1: "split"}[lib().fv_solver_stage_kernels(self._h)]
 
     def close(self):
         if self._h:

@@ -3,14 +3,19 @@
 # are compiled where they lie in the reference checkout (REF); the programs go
 # to shim/_examples/, which is not committed.
 #   make -C finite-volume-2d-cpp_b200/shim -f examples.mk REF=<fvhyper checkout>
-REF ?= /root/reference
+REF ?= $(FVHYPER_SRC)
 CXX ?= g++
 HERE := $(dir $(abspath $(lastword $(MAKEFILE_LIST))))
 PKG := $(abspath $(HERE)..)
 OUT := $(HERE)_examples
 EXAMPLES := shockTube forwardStep naca burgers flatPlate heatTransfer nacaTransient
 
+ifeq ($(strip $(REF)),)
+all:
+	@echo "examples: set FVHYPER_SRC (or REF=...) to the fvhyper source checkout" >&2; exit 1
+else
 all: $(EXAMPLES:%=$(OUT)/%) $(OUT)/naca0012_129.su2
+endif
 
 # the SU2 mesh fvhyper ships for its NACA example (read directly by the shim)
 $(OUT)/naca0012_129.su2: $(REF)/examples/naca/naca0012_129.su2 | $(OUT)

@@ -196,13 +196,38 @@ int fv_mesh_device_order(const fv_mesh* m, int32_t* new2ref);
  * 0xFFFF for no face. */
 int fv_mesh_tile_layout(const fv_mesh* m, int32_t tile_cells, int64_t* sizes, int32_t* info, int32_t* halo,
                         uint32_t* edge_ij, uint16_t* face);
+/* Host-only inspection of the two-ring tile layout of the fused stage
+ * kernel (no counterpart in the reference).  sizes[8] = n_tiles, max slots,
+ * max gradient slots, max edges (a multiple of 4), max flux edges, total halo
+ * entries, total edge entries (each tile's run padded to a multiple of 4),
+ * total face-word entries.  Each output array may be NULL: info [n_tiles][8]
+ * = edge offset, edge count, flux-edge count, halo offset, ring-1 count,
+ * ring-2 count, face offset, 0; halo [total] device cells of ring 1 then
+ * ring 2; edge_ij [total] = local i | local j << 16 (owned cell c -> c -
+ * tile start, halo slot h -> tile_cells + h); face [total][4] = the face
+ * words of each tile's gradient slots (owned, then ring 1), formatted as in
+ * fv_mesh_tile_layout. */
+int fv_mesh_tile2_layout(const fv_mesh* m, int32_t tile_cells, int64_t* sizes, int32_t* info, int32_t* halo,
+                         uint32_t* edge_ij, uint16_t* face);
 
 /* ---- solver (device) ---------------------------------------------------- */
 int fv_solver_create(const fv_mesh* m, const fv_physics* ph, int32_t precision, int32_t device,
                      fv_solver** out);
 typedef struct {
     int32_t tile_cells;  /* cells per tile = threads per CTA: 64, 128 or 256 (0 = 128) */
+    /* Stage kernels of the second-order Euler kinds (Roe fluxes, no
+     * diffusive terms, no residual smoothing):
+     * FV_STAGE_AUTO (0): one fused kernel per RK stage (gradients, limiter,
+     *   fluxes, update, ghost fill) over two-ring tiles, plus one time-step
+     *   kernel per step, where the physics allow; otherwise as below.
+     * FV_STAGE_SPLIT (1): a gradient + limiter kernel and a flux + update
+     *   kernel per stage (the first stage's gradient kernel also computes dt).
+     * FV_STAGE_FUSED (2): the fused kernel; FV_ERR_UNSUPPORTED when the
+     *   physics do not allow it.  All three give the same results (bit for bit
+     *   in FP64_EXACT). */
+    int32_t stage_kernels;
 } fv_solver_options;
+enum { FV_STAGE_AUTO = 0, FV_STAGE_SPLIT = 1, FV_STAGE_FUSED = 2 };
 int fv_solver_create_ex(const fv_mesh* m, const fv_physics* ph, int32_t precision, int32_t device,
                         const fv_solver_options* opt, fv_solver** out);
 /* Autotuned creation: builds the solver with each tile size (64, 128, 256
@@ -255,6 +280,8 @@ int fv_solver_set_chunk(fv_solver* s, int32_t steps);
 /* out[6] = {tiles, cells per tile, max halo cells per tile, max edges per
  * tile, precision, bytes per stored stage value}. */
 int fv_solver_info(fv_solver* s, int64_t* out);
+/* The stage kernels the solver runs: FV_STAGE_FUSED or FV_STAGE_SPLIT. */
+int fv_solver_stage_kernels(fv_solver* s);
 /* Device time of the last fv_run's chunks and per-kernel launch count. */
 int fv_last_run_stats(fv_solver* s, double* device_ms, int64_t* kernel_launches);
 
@@ -294,7 +321,10 @@ int fv_stage_update(fv_solver* s, const double* q_base, const double* q_stage,
  * (held until the process exits), so meshes needing more (about 200k cells
  * in FP64, 150k in FP32) are rejected with FV_ERR_ARG.  The first call on a
  * device looks up that array's device address; make it before any stream
- * capture.  All calls share the array: calls that overlap on the GPU (two
+ * capture.  The address is kept for the rest of the process: after a
+ * cudaDeviceReset (or anything else that tears down the device's primary
+ * context) it is stale, so do not call this entry point again in that
+ * process.  All calls share the array: calls that overlap on the GPU (two
  * streams, two threads) race and must be serialised by the caller. */
 int fv_stage_dt_noalloc(fv_solver* s, const double* q_device, double* dt_device, int32_t global_min,
                         void* stream);

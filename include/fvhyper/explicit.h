@@ -9,14 +9,21 @@
  * header and libfvhyper_gpu.a + libfvgpu.so, and run() advances it on the GPU.
  *
  * run() identifies the user's physics callbacks with a device physics kind
- * (Roe flux with the cures eigenvalues in either of the reference's two
- * operand orders, upwind advection; Michalak / Venkatakrishnan / minmod /
- * zero limiter functions; copy / reflecting wall / inlet-outlet / far-field
- * boundaries; constant, edge-sum CFL and edge-min CFL time steps) by
- * evaluating them on probe states and comparing bit for bit with the host copy
- * of each kind (fv_kind_*, include/fvgpu.h).  Callbacks that match no kind,
- * and the viscous and residual-smoothing options, are refused with
- * std::invalid_argument: there is no CPU fallback.
+ * by evaluating them on probe states and comparing bit for bit with the host
+ * copy of each kind (fv_kind_*, include/fvgpu.h):
+ *  - fluxes: Roe with the cures eigenvalues in either of the reference's two
+ *    operand orders, upwind advection, and with diffusive_gradients the heat
+ *    diffusion flux (vars = 1), the Navier-Stokes flux (vars = 4, constants
+ *    from fvhyper::consts) and the Burgers + diffusion flux (vars = 2);
+ *  - limiter functions: Michalak, Venkatakrishnan, minmod, zero;
+ *  - boundaries: copy, reflecting wall, inlet-outlet, far field (both of the
+ *    reference's forms), no-slip wall, tangential state;
+ *  - time steps: constant, edge-sum and edge-min CFL, and the two viscous
+ *    CFL forms.
+ * Residual smoothing (solverOptions::smooth_residuals) runs with the Burgers
+ * + diffusion kind.  Callbacks that match no kind, and residual smoothing
+ * with any other kind, are refused with std::invalid_argument: there is no
+ * CPU fallback.
  */
 #pragma once
 

@@ -1,0 +1,187 @@
+"""Parity at the benchmarked sizes: the CUDA path, through the C ABI, against
+the CPU oracle on the full-size meshes of the bench workloads.
+
+- Mach 3 forward step, 998,046 cells (seeded jittered Delaunay), second order,
+  Green-Gauss + smooth-switch limiter with Venkatakrishnan phi, K = 5, RK5,
+  CFL 0.8, global time step, with the positivity guard off (the reference's
+  scheme, explicit.cpp:657-817) and on (the bench workload):
+  * FP64_EXACT: bit-identical to the oracle after 3 time steps;
+  * FP64: normwise relative error <= 1e-12 per step (each step started from
+    the oracle's state);
+  * FP32-bulk: L1 and L2 density and pressure errors <= 1e-4 relative, after
+    3 steps, and after 20 steps with the guard on.
+- NACA 0012 O-grid, 1024 x 512 quads split into 1,048,576 triangles, M 0.8,
+  alpha 1.25 deg, Michalak limiter, local time stepping (examples/naca/main.cpp
+  :142-272): FP64_EXACT bit-identical over 3 steps, FP64 <= 1e-12 per step,
+  and the lift and drag (FP64 force sums) of the GPU against the oracle's on
+  the same state.
+
+The oracle needs about 1.4 s per RK5 step at this size on one core.
+"""
+import numpy as np
+import pytest
+
+import meshgen
+import physics as P
+
+pytestmark = pytest.mark.gpu
+
+FP64_STEP_RTOL = 1e-12     # plain FP64 path: max relative error per step
+FP32_TOL = 1e-4            # FP32-bulk: relative L1 and L2 error of density and pressure
+
+
+def bits_equal(a, b):
+    a = np.ascontiguousarray(a); b = np.ascontiguousarray(b)
+    return a.shape == b.shape and a.tobytes() == b.tobytes()
+
+
+def normwise_rel(a, b, V=4):
+    """max over variables of max|a_k - b_k| / max|b_k| (AoS [n][V])."""
+    a = a.reshape(-1, V); b = b.reshape(-1, V)
+    scale = np.maximum(np.abs(b).max(axis=0), 1e-3 * np.abs(b).max())
+    return float((np.abs(a - b).max(axis=0) / scale).max())
+
+
+def rho_p(q, n, gamma=1.4):
+    q = q[: 4 * n].reshape(n, 4)
+    return q[:, 0], (gamma - 1) * (q[:, 3] - 0.5 * (q[:, 1] ** 2 + q[:, 2] ** 2) / q[:, 0])
+
+
+def rel_l1_l2(a, b):
+    d = np.abs(a - b)
+    return float(d.sum() / np.abs(b).sum()), float(np.sqrt((d * d).sum() / (b * b).sum()))
+
+
+def fp32_errors(q32, q64, n):
+    r1, p1 = rho_p(q32, n)
+    r0, p0 = rho_p(q64, n)
+    return {"density": rel_l1_l2(r1, r0), "pressure": rel_l1_l2(p1, p0)}
+
+
+@pytest.fixture(scope="module")
+def step_mesh(oracle):
+    import fvgpu
+    em = meshgen.forward_step()
+    g = oracle.build_mesh(em)
+    assert g.n_real == 998046
+    return em, g, fvgpu.Mesh.from_elements(em)
+
+
+def _oracle_steps(oracle, g, p, q0, alpha, n):
+    """The oracle's state after each of n time steps (continued runs of one
+    step carry the same state as one run of n steps)."""
+    out = [q0]
+    for _ in range(n):
+        out.append(oracle.run_loop(g, p, out[-1], alpha, 1)["q"])
+    return out
+
+
+@pytest.mark.parametrize("guard", [False, True], ids=["reference_scheme", "positivity_guard"])
+def test_forward_step_full_size(guard, oracle, step_mesh):
+    import fvgpu
+
+    em, g, mesh = step_mesh
+    ph = P.forward_step(order2=True, limiter="venkat", K=5.0, cfl=0.8)
+    ph.positivity_guard = guard
+    p = oracle.physics(ph, em.group_names)
+    q0 = P.ic_forward_step(g.n_total).ravel()
+    want = _oracle_steps(oracle, g, p, q0, P.RK5_ALPHA, 3)
+    assert np.isfinite(want[-1]).all()
+    n = g.n_real
+
+    s = fvgpu.Solver(mesh, ph, "fp64_exact")
+    s.set_state(q0)
+    r = s.run(3)
+    assert r["step"] == 3
+    assert bits_equal(s.get_state(), want[3])
+    s.close()
+
+    s = fvgpu.Solver(mesh, ph, "fp64")
+    worst = 0.0
+    for k in range(3):
+        s.set_state(want[k])
+        s.run(1)
+        worst = max(worst, normwise_rel(s.get_state()[: 4 * n], want[k + 1][: 4 * n]))
+    s.close()
+    print(f"forward step (guard {guard}) FP64 worst per-step error {worst:.2e}")
+    assert worst <= FP64_STEP_RTOL, worst
+
+    s = fvgpu.Solver(mesh, ph, "fp32")
+    s.set_state(q0)
+    s.run(3)
+    e = fp32_errors(s.get_state(), want[3], n)
+    assert s.check_state() == 0
+    s.close()
+    print(f"forward step (guard {guard}) FP32 after 3 steps: {e}")
+    assert max(max(v) for v in e.values()) <= FP32_TOL, e
+
+
+def test_forward_step_full_size_20_steps_fp32(oracle, step_mesh):
+    """The bench workload (guard on) over 20 steps: FP32-bulk and FP64 against
+    the oracle's FP64 run, FP64_EXACT bit-identical."""
+    import fvgpu
+
+    em, g, mesh = step_mesh
+    ph = P.forward_step(order2=True, limiter="venkat", K=5.0, cfl=0.8)
+    ph.positivity_guard = True
+    p = oracle.physics(ph, em.group_names)
+    q0 = P.ic_forward_step(g.n_total).ravel()
+    want = oracle.run_loop(g, p, q0, P.RK5_ALPHA, 20)
+    n = g.n_real
+    got = {}
+    for prec in ("fp64_exact", "fp64", "fp32"):
+        s = fvgpu.Solver(mesh, ph, prec)
+        s.set_state(q0)
+        r = s.run(20)
+        assert r["step"] == 20
+        if prec == "fp64_exact":
+            assert r["time"] == want["time"]
+        got[prec] = s.get_state()
+        s.close()
+    assert bits_equal(got["fp64_exact"], want["q"])
+    e64 = fp32_errors(got["fp64"], want["q"], n)
+    e32 = fp32_errors(got["fp32"], want["q"], n)
+    print(f"forward step 20 steps vs oracle: FP64 {e64}, FP32 {e32}")
+    assert max(max(v) for v in e64.values()) <= 1e-10
+    assert max(max(v) for v in e32.values()) <= FP32_TOL
+
+
+def test_naca_full_size(oracle):
+    import fvgpu
+
+    em = meshgen.naca_ogrid()
+    g = oracle.build_mesh(em)
+    assert g.n_real == 1048576
+    ph = P.naca()
+    p = oracle.physics(ph, em.group_names)
+    mesh = fvgpu.Mesh.from_elements(em)
+    q0 = P.ic_naca(g.n_total).ravel()
+    want = _oracle_steps(oracle, g, p, q0, P.RK5_ALPHA, 3)
+    n = g.n_real
+    airfoil = em.group_names.index("airfoil")
+
+    s = fvgpu.Solver(mesh, ph, "fp64_exact")
+    s.set_state(q0)
+    s.run(3)
+    assert bits_equal(s.get_state(), want[3])
+    # lift and drag (FP64 sums over the airfoil faces) on the same state
+    fx, fy = s.boundary_force("airfoil")
+    ox, oy = oracle.boundary_force(g, p, want[3], airfoil)
+    np.testing.assert_allclose([fx, fy], [ox, oy], rtol=1e-12, atol=0)
+    s.close()
+
+    for prec in ("fp64", "fp32"):
+        s = fvgpu.Solver(mesh, ph, prec)
+        worst = 0.0
+        for k in range(3):
+            s.set_state(want[k])
+            s.run(1)
+            q = s.get_state()
+            if prec == "fp64":
+                worst = max(worst, normwise_rel(q[: 4 * n], want[k + 1][: 4 * n]))
+            else:
+                e = fp32_errors(q, want[k + 1], n)
+                worst = max(worst, max(max(v) for v in e.values()))
+        s.close()
+        print(f"naca full size {prec}: worst per-step error {worst:.2e}")
+        assert worst <= (FP64_STEP_RTOL if prec == "fp64" else FP32_TOL), (prec, worst)

@@ -320,3 +320,53 @@ def test_solvers_of_different_tile_sizes_coexist(oracle):
         assert s.get_state().tobytes() == want["q"].tobytes()
     big.close()
     small.close()
+
+
+FUSED_CASES = [n for n in sorted(CASES) if CASES[n]["phys"]().order2 and CASES[n]["phys"]().flux in ("roe_fs", "roe_st")
+               and not CASES[n]["phys"]().diffusive]
+
+
+@pytest.mark.parametrize("precision", ["fp64_exact", "fp64", "fp32"])
+@pytest.mark.parametrize("name", FUSED_CASES)
+def test_fused_and_split_stage_kernels_agree(name, precision, oracle):
+    """The fused stage kernel (gradients, limiter and fluxes of a two-ring
+    tile in one launch) and the split gradient + flux kernels give the same
+    bits in every precision mode, and in FP64_EXACT both equal the oracle, at
+    every tile size."""
+    case = CASES[name]
+    em, ph = case["mesh"](), case["phys"]()
+    mesh = fvgpu.Mesh.from_elements(em)
+    g = oracle.build_mesh(em)
+    p = oracle.physics(ph, em.group_names)
+    q0 = case["ic"](g)
+    want = oracle.run_loop(g, p, q0, case["alpha"], case["steps"]) if precision == "fp64_exact" else None
+    out = {}
+    for T in (64, 128, 256):
+        for sk in ("split", "fused"):
+            s = fvgpu.Solver(mesh, ph, precision, tile_cells=T, stage_kernels=sk)
+            assert s.stage_kernels == sk
+            s.set_state(q0)
+            r = s.run(case["steps"], alpha=case["alpha"])
+            out[(T, sk)] = (s.get_state(), np.asarray(r["R"]), r["time"])
+            s.close()
+    ref = out[(128, "split")]
+    for k, v in out.items():
+        assert bits_equal(v[0], ref[0]), k
+        assert v[2] == ref[2], k
+        np.testing.assert_allclose(v[1], ref[1], rtol=R_RTOL, atol=0)
+    if want is not None:
+        assert bits_equal(ref[0], want["q"])
+
+
+def test_fused_stage_kernel_is_chosen_where_the_physics_allow():
+    for name in sorted(CASES):
+        case = CASES[name]
+        ph = case["phys"]()
+        s = fvgpu.Solver(fvgpu.Mesh.from_elements(case["mesh"]()), ph, "fp64")
+        fusable = ph.V == 4 and ph.order2 and ph.flux in ("roe_fs", "roe_st") and not ph.diffusive
+        assert s.stage_kernels == ("fused" if fusable else "split"), name
+        s.close()
+    case = CASES["heat"]
+    with pytest.raises(fvgpu.FvError) as e:
+        fvgpu.Solver(fvgpu.Mesh.from_elements(case["mesh"]()), case["phys"](), "fp64", stage_kernels="fused")
+    assert e.value.code == -4

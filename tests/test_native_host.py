@@ -166,7 +166,8 @@ def test_su2_reader_reads_the_reference_naca_meshes():
     """The SU2 meshes fvhyper ships for its NACA example (to be converted with
     gmsh there) are read directly: quadrilateral O-grids, closed, with the
     airfoil and farfield markers."""
-    base = "/root/reference/examples/naca"
+    from __graft_entry__ import REFERENCE
+    base = os.path.join(REFERENCE, "examples", "naca")
     if not os.path.isdir(base):
         pytest.skip("fvhyper checkout not present")
     for fn, ncell in (("naca0012_129.su2", 16384), ("NACA_M.su2", 4096)):
@@ -341,3 +342,113 @@ def test_tile_layout_indices_stay_in_bounds(T):
                     dev_other = c0 + other if other < T else int(hl[other - T])
                     assert dev_other in nbrs[c]
                     assert ghost == (dev_other >= N)
+
+
+def _tile2_layout(m, T):
+    import ctypes as C
+    L = fvgpu.lib()
+    sizes = np.zeros(8, np.int64)
+    i64 = C.POINTER(C.c_int64)
+    rc = L.fv_mesh_tile2_layout(m._h, C.c_int32(T), sizes.ctypes.data_as(i64), None, None, None, None)
+    assert rc == 0, L.fv_last_error()
+    nt, nh, ne, nf = int(sizes[0]), int(sizes[5]), int(sizes[6]), int(sizes[7])
+    info = np.zeros(8 * nt, np.int32)
+    halo = np.zeros(max(nh, 1), np.int32)
+    eij = np.zeros(max(ne, 1), np.uint32)
+    face = np.zeros(4 * max(nf, 1), np.uint16)
+    rc = L.fv_mesh_tile2_layout(m._h, C.c_int32(T), sizes.ctypes.data_as(i64), info.ctypes.data_as(C.c_void_p),
+                                halo.ctypes.data_as(C.c_void_p), eij.ctypes.data_as(C.c_void_p),
+                                face.ctypes.data_as(C.c_void_p))
+    assert rc == 0, L.fv_last_error()
+    return sizes, info.reshape(nt, 8), halo[:nh], eij[:ne], face[: 4 * nf].reshape(-1, 4)
+
+
+@pytest.mark.parametrize("T", [64, 128, 256])
+def test_two_ring_tile_layout_indices_stay_in_bounds(T):
+    """Every index the fused stage kernel reads through is inside what it
+    stages: ring 1 is exactly the outside face neighbours of the owned cells,
+    ring 2 exactly the further neighbours of the ring-1 real cells; flux edges
+    (the first n_flux) join an owned cell to an owned or ring-1 slot; the other
+    edges join a ring-1 real cell to a ring-1 or ring-2 slot; owned cells'
+    face words name flux edges only; every gradient slot's face words name one
+    of the tile's edges with the cell on the stated side, in increasing
+    reference edge order; edge runs start on multiples of 4 and the sizes the
+    shared-memory layout is built from bound every tile (four meshes and a
+    batch of three cases)."""
+    meshes = [fvgpu.Mesh.from_elements(em) for em in
+              (meshgen.forward_step(n=20), meshgen.naca_ogrid(ni=48, nj=12, r_far=10.0),
+               meshgen.flat_plate(nx0=6, nx1=18, ny=20), meshgen.sod_strip(40, 4))]
+    meshes.append(fvgpu.Mesh.batch([fvgpu.Mesh.from_elements(meshgen.riemann_strip(n)) for n in (150, 37, 260)]))
+    for m in meshes:
+        N, NT = m.n_real, m.n_total
+        sizes, info, halo, eij, face = _tile2_layout(m, T)
+        nt, max_slots, max_grad, max_edges, max_flux = (int(x) for x in sizes[:5])
+        assert nt == (N + T - 1) // T
+        assert max_slots <= 65535 and max_edges <= 0x3FFF and max_edges % 4 == 0
+        g = m.geometry()
+        new2ref = m.device_order()
+        ref2new = np.empty_like(new2ref); ref2new[new2ref] = np.arange(NT)
+        ec_ref = g["edge_cells"].reshape(-1, 2).astype(np.int64)
+        ec = ref2new[ec_ref]
+        nbrs = [set() for _ in range(N)]
+        edge_of = {}
+        for e, (a, b) in enumerate(ec):
+            if a < N: nbrs[a].add(int(b))
+            if b < N: nbrs[b].add(int(a))
+            edge_of[(int(a), int(b))] = e
+        face_end = 0
+        for t in range(nt):
+            c0, nown = t * T, min(T, N - t * T)
+            e0, ne_t, nfl, h0, n1, n2, f0, _ = (int(x) for x in info[t])
+            assert e0 % 4 == 0 and nfl <= ne_t and (ne_t + 3) // 4 * 4 <= max_edges and nfl <= max_flux
+            assert T + n1 + n2 <= max_slots and T + n1 <= max_grad
+            assert f0 == face_end
+            face_end += T + n1
+            owned = set(range(c0, c0 + nown))
+            r1, r2 = halo[h0:h0 + n1].tolist(), halo[h0 + n1:h0 + n1 + n2].tolist()
+            ring1 = set().union(*(nbrs[c] for c in owned)) - owned
+            assert set(r1) == ring1 and len(r1) == len(ring1)
+            ring2 = set().union(*[nbrs[c] for c in r1 if c < N]) - owned - ring1 if r1 else set()
+            assert set(r2) == ring2 and len(r2) == len(ring2)
+            slots = list(range(c0, c0 + T)) + r1 + r2  # device cell of each local slot
+            li, lj = (eij[e0:e0 + ne_t] & 0xFFFF).astype(np.int64), (eij[e0:e0 + ne_t] >> 16).astype(np.int64)
+            for x in (li, lj):
+                assert np.all((x < nown) | ((x >= T) & (x < T + n1 + n2)))
+            # flux edges: an owned cell and an owned or ring-1 slot
+            assert np.all((li[:nfl] < T) | (lj[:nfl] < T))
+            assert np.all((li[:nfl] < T + n1) & (lj[:nfl] < T + n1))
+            # the other edges: a ring-1 real cell and no owned cell
+            assert np.all((li[nfl:] >= T) & (lj[nfl:] >= T))
+            for e in range(ne_t):
+                a, b = slots[li[e]], slots[lj[e]]
+                assert (a, b) in edge_of  # reference orientation
+            tf = face[f0:f0 + T + n1]
+            for r in range(T + n1):
+                if r < T and r >= nown:
+                    assert np.all(tf[r] == 0xFFFF)
+                    continue
+                cell = slots[r]
+                if cell >= N:  # ring-1 ghost: no faces
+                    assert np.all(tf[r] == 0xFFFF)
+                    continue
+                prev_e = -1
+                nf = 0
+                for f in range(4):
+                    w = int(tf[r, f])
+                    if w == 0xFFFF:
+                        continue
+                    nf += 1
+                    el, ghost, side = w & 0x3FFF, (w >> 14) & 1, w >> 15
+                    assert el < ne_t
+                    if r < T:
+                        assert el < nfl
+                    me, other = (lj[el], li[el]) if side else (li[el], lj[el])
+                    assert me == r
+                    dev_other = slots[other]
+                    assert dev_other in nbrs[cell]
+                    assert ghost == (dev_other >= N)
+                    e_ref = edge_of[(slots[li[el]], slots[lj[el]])]
+                    assert e_ref > prev_e  # reference edge order
+                    prev_e = e_ref
+                assert nf == len(nbrs[cell])
+        assert face_end == len(face)

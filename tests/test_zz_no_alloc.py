@@ -17,14 +17,16 @@ from cases import CASES, random_euler_state
 pytestmark = pytest.mark.gpu
 
 
-def noalloc_dt(solver, q_dev, out_dev, global_min):
+def noalloc_dt(solver, q_dev, out_dev, global_min, stream=None):
     return fvgpu.lib().fv_stage_dt_noalloc(solver._h, ctypes.c_void_p(q_dev.data_ptr()),
                                           ctypes.c_void_p(out_dev.data_ptr()),
-                                          ctypes.c_int32(int(global_min)), ctypes.c_void_p(None))
+                                          ctypes.c_int32(int(global_min)), ctypes.c_void_p(stream))
 
 
+# the Euler time steps (edge-sum CFL, signed-normal CFL) and the viscous one
+# of the flat plate (a separate kernel instantiation)
 @pytest.mark.parametrize("precision", ["fp64_exact", "fp64", "fp32"])
-@pytest.mark.parametrize("name", ["step_o2_venk5", "naca"])
+@pytest.mark.parametrize("name", ["step_o2_venk5", "naca", "flat_plate"])
 def test_noalloc_dt_matches_allocating_entry(name, precision):
     import torch
 
@@ -43,6 +45,26 @@ def test_noalloc_dt_matches_allocating_entry(name, precision):
             s.sync()
             got = out.cpu().numpy()
             assert got.tobytes() == want.tobytes(), (call, glob, np.abs(got - want).max())
+    s.close()
+
+
+def test_noalloc_dt_on_a_caller_stream():
+    """The work is queued on the caller's stream and complete when it is."""
+    import torch
+
+    case = CASES["step_o2_venk5"]
+    mesh = fvgpu.Mesh.from_elements(case["mesh"]())
+    s = fvgpu.Solver(mesh, case["phys"](), "fp64")
+    st = torch.cuda.Stream()
+    for call in range(2):
+        q = random_euler_state(mesh.n_total, seed=200 + call)
+        want = s.stage_dt(q, True)
+        with torch.cuda.stream(st):
+            q_dev = torch.from_numpy(q).cuda(non_blocking=False)
+            out = torch.full((mesh.n_total,), -1.0, dtype=torch.float64, device="cuda")
+            assert noalloc_dt(s, q_dev, out, True, st.cuda_stream) == 0, fvgpu.lib().fv_last_error()
+        st.synchronize()
+        assert out.cpu().numpy().tobytes() == want.tobytes(), call
     s.close()
 
 
