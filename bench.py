@@ -558,7 +558,12 @@ def run_adjoint_workload(args):
     ph.positivity_guard = True
     mesh = fvgpu.Mesh.from_elements(em)
     nb = 64
+    import torch
+    torch.cuda.init()
+    free0 = torch.cuda.mem_get_info(0)[0]
     adj = fvgpu.Adjoint(mesh, ph, n_steps=args.steps, checkpoint_every=50, n_bins=nb)
+    # the adjoint allocates everything it uses at creation
+    adj_bytes = free0 - torch.cuda.mem_get_info(0)[0]
     theta = np.concatenate([[3.0], np.random.default_rng(5).normal(0.0, 0.01, nb)])
     for _ in range(max(1, args.warmup - 2)):
         adj.loss(theta)
@@ -573,7 +578,19 @@ def run_adjoint_workload(args):
     # adjoint is the derivative of the code path taken, central differences
     # converge to it as h shrinks past the nearest kink
     checks = {"mach": {f"h={h:g}": {"adjoint": float(g[0]), "fd": fd(0, h),
-                                    "rel_error": abs(float(g[0]) - fd(0, h)) / abs(fd(0, h))} for h in (1e-6, 1e-7)}}
+                                    "rel_error": abs(float(g[0]) - fd(0, h)) / abs(fd(0, h))}
+                       for h in (1e-5, 1e-6, 1e-7, 1e-8)}}
+    # kink scan: one-sided slopes of the loss over M in steps of 2e-7 around
+    # theta; an interval whose slope departs from the adjoint holds a kink
+    step, K = 2e-7, 8
+    Ls = [adj.loss(np.concatenate([[theta[0] + k * step], theta[1:]])) for k in range(-K, K + 1)]
+    slopes = np.diff(Ls) / step
+    rel = np.abs(slopes - float(g[0])) / abs(float(g[0]))
+    checks["mach_kink_scan"] = {
+        "step": step, "intervals": [[(k - K) * step, (k - K + 1) * step] for k in range(2 * K)],
+        "slope_rel_error_vs_adjoint": rel.tolist(),
+        "kink_intervals": [[(k - K) * step, (k - K + 1) * step] for k in range(2 * K) if rel[k] > 1e-6],
+        "intervals_adjacent_to_theta_match_1e-6": bool(min(rel[K - 1], rel[K]) <= 1e-6)}
     top = [1 + int(i) for i in np.argsort(-np.abs(g[1:]))[:3]]
     checks["density_bins"] = {str(i - 1): {"adjoint": float(g[i]), "fd_h=1e-6": fd(i, 1e-6)} for i in top}
     cell_stages = mesh.n_real * 5 * args.steps
@@ -586,6 +603,7 @@ def run_adjoint_workload(args):
                                    "theta = inflow Mach + 64 inflow density bins; checkpoints every 50 steps",
                        "n_real_cells": mesh.n_real, "n_params": 1 + nb},
             "forward_seconds": t_fwd, "gradient_seconds": t_grad, "loss": L, "loss_repeat_equal": L == L2,
+            "device_memory_bytes": int(adj_bytes),
             "gradient_norm": float(np.linalg.norm(g)), "max_abs_density_bin_gradient": float(np.abs(g[1:]).max()),
             "fd_check": checks}
     print(json.dumps(line))

@@ -1324,9 +1324,12 @@ int fv_stage_bounds(fv_solver* s, double* q, const double* gx, const double* gy,
 // state rho_inf, u = M, v = 0, p_inf) and the inflow boundary states (density
 // rho_inf (1 + delta_b) on the inflow faces of bin b, velocity M);
 // loss = sum_n dt_n sum_{faces of loss_group} p(interior) le.  The forward
-// run stores its state every `checkpoint_every` steps; the reverse sweep
-// recomputes each segment storing every stage state, gradient and limiter,
-// then runs the adjoint kernels of fv_adjoint.cu stage by stage backwards.
+// run stores its state every `checkpoint_every` steps.  The reverse sweep
+// takes the segments backwards: it recomputes a segment's step states from
+// its checkpoint, then, for each step backwards, recomputes that step's
+// stage states, gradients and limiters and runs the adjoint kernels of
+// fv_adjoint.cu stage by stage backwards.  Device memory therefore holds the
+// checkpoints, one segment's step states and one step's stage data.
 struct fv_adjoint {
     fv_solver* s = nullptr;
     fv_adjoint_options o{};
@@ -1339,9 +1342,10 @@ struct fv_adjoint {
     AdjFaces F{};
     std::vector<void*> allocs;
     std::vector<double*> ckpt;        // [nseg] states at segment starts
-    std::vector<double*> Qs;          // [(every + 1) * S] stage inputs of a segment (Qs[j*S] = q_n)
-    std::vector<double*> Gx, Gy, Lim; // [every * S]
-    std::vector<double*> dtc;         // [every] per-cell dt of each step
+    std::vector<double*> Qn;          // [every + 1] step states of the segment being reversed
+    std::vector<double*> Qs;          // [S] inputs of stages 1..S-1 of the step being reversed (Qs[0] unused)
+    std::vector<double*> Gx, Gy, Lim; // [S] gradients and limiters of its stages
+    double* dtc = nullptr;            // its per-cell dt
     double *tmp[2] = {nullptr, nullptr}, *tgx = nullptr, *tgy = nullptr, *tlim = nullptr;
     double *dt_fill = nullptr, *dt_n = nullptr, *loss = nullptr, *lam_dt = nullptr, *partials = nullptr;
     double *lamA = nullptr, *lamB = nullptr, *lam_qn = nullptr, *lgx = nullptr, *lgy = nullptr, *llim = nullptr;
@@ -1366,15 +1370,16 @@ struct fv_adjoint {
 
 namespace {
 // One forward step from q (device numbering, all cells) to q_next.  With
-// `store`, stage inputs go to qs[k] (qs[0] == q), gradients to gx/gy/lim[k]
-// and per-cell dt to dtc; otherwise the adjoint's temporaries are used.
-int adj_forward_step(fv_adjoint* a, const double* q, double* q_next, double* dt_slot, bool store, int j,
+// `store`, the inputs of stages 1..S-1 go to Qs[k], gradients to
+// Gx/Gy/Lim[k] and per-cell dt to dtc; otherwise the adjoint's temporaries
+// are used.
+int adj_forward_step(fv_adjoint* a, const double* q, double* q_next, double* dt_slot, bool store,
                      bool with_loss) {
     fv_solver* s = a->s;
     cudaStream_t st = s->stream;
     const TileParams& TP = s->TP;
     const size_t nt = (size_t)s->n_total;
-    double* dtcells = store ? a->dtc[j] : a->dt_fill;
+    double* dtcells = store ? a->dtc : a->dt_fill;
     CK(cudaMemsetAsync(a->keys, 0xFF, kDtSlots * 8, st));
     TileIO io{};
     io.q_stage = q;
@@ -1385,10 +1390,10 @@ int adj_forward_step(fv_adjoint* a, const double* q, double* q_next, double* dt_
     if (with_loss && a->n_loss) adj_launch_loss(TP.P, q, dt_slot, a->loss_ghosts, a->n_loss, a->loss, st);
     const double* in = q;
     for (int k = 0; k < a->S; ++k) {
-        double* gx = store ? a->Gx[(size_t)j * a->S + k] : a->tgx;
-        double* gy = store ? a->Gy[(size_t)j * a->S + k] : a->tgy;
-        double* lim = store ? a->Lim[(size_t)j * a->S + k] : a->tlim;
-        double* out = (k == a->S - 1) ? q_next : (store ? a->Qs[(size_t)j * a->S + k + 1] : a->tmp[k % 2]);
+        double* gx = store ? a->Gx[(size_t)k] : a->tgx;
+        double* gy = store ? a->Gy[(size_t)k] : a->tgy;
+        double* lim = store ? a->Lim[(size_t)k] : a->tlim;
+        double* out = (k == a->S - 1) ? q_next : (store ? a->Qs[(size_t)k + 1] : a->tmp[k % 2]);
         TileIO so{};
         so.q_stage = in;
         so.q_base = q;
@@ -1434,11 +1439,12 @@ int adj_set_theta(fv_adjoint* a, const double* theta, double* q0_dev) {
     return FV_OK;
 }
 
-AdjStage adj_stage(fv_adjoint* a, int j, int k, double dt) {
+// stage k of the step whose input is qn and output qn1 (stages 1..S-1 in Qs)
+AdjStage adj_stage(fv_adjoint* a, const double* qn, const double* qn1, int k, double dt) {
     AdjStage S{};
-    const size_t i = (size_t)j * a->S + k;
-    S.qs = a->Qs[i];
-    S.qs1 = a->Qs[i + 1];
+    const size_t i = (size_t)k;
+    S.qs = k == 0 ? qn : a->Qs[i];
+    S.qs1 = k == a->S - 1 ? qn1 : a->Qs[i + 1];
     S.gx = a->Gx[i]; S.gy = a->Gy[i]; S.lim = a->Lim[i];
     S.dt = dt;
     S.alpha = a->alpha[(size_t)k];
@@ -1523,16 +1529,17 @@ int fv_adjoint_create(const fv_mesh* fm, const fv_physics* ph, int32_t device, c
     a->nseg = (o->n_steps + every - 1) / every;
     a->ckpt.resize((size_t)a->nseg);
     for (auto& p : a->ckpt) CK(a->alloc(&p, nq));
-    a->Qs.resize((size_t)(every + 1) * a->S);
-    for (auto& p : a->Qs) CK(a->alloc(&p, nq));
-    const size_t ng_ = (size_t)every * a->S;
-    a->Gx.resize(ng_); a->Gy.resize(ng_); a->Lim.resize(ng_);
-    for (size_t i = 0; i < ng_; ++i) {
-        CK(a->alloc(&a->Gx[i], nq)); CK(a->alloc(&a->Gy[i], nq)); CK(a->alloc(&a->Lim[i], nq));
-        launch_fill_ghost_grad(a->Gx[i], a->Gy[i], a->Lim[i], (int)m.n_real, (int)m.n_total, 4, false, s->stream);
+    a->Qn.resize((size_t)every + 1);
+    for (auto& p : a->Qn) CK(a->alloc(&p, nq));
+    a->Qs.assign((size_t)a->S, nullptr);
+    for (int k = 1; k < a->S; ++k) CK(a->alloc(&a->Qs[(size_t)k], nq));
+    a->Gx.resize((size_t)a->S); a->Gy.resize((size_t)a->S); a->Lim.resize((size_t)a->S);
+    for (int k = 0; k < a->S; ++k) {
+        CK(a->alloc(&a->Gx[(size_t)k], nq)); CK(a->alloc(&a->Gy[(size_t)k], nq)); CK(a->alloc(&a->Lim[(size_t)k], nq));
+        launch_fill_ghost_grad(a->Gx[(size_t)k], a->Gy[(size_t)k], a->Lim[(size_t)k], (int)m.n_real, (int)m.n_total, 4,
+                               false, s->stream);
     }
-    a->dtc.resize((size_t)every);
-    for (auto& p : a->dtc) CK(a->alloc(&p, (size_t)m.n_total));
+    CK(a->alloc(&a->dtc, (size_t)m.n_total));
     CK(a->alloc(&a->tmp[0], nq)); CK(a->alloc(&a->tmp[1], nq));
     CK(a->alloc(&a->tgx, nq)); CK(a->alloc(&a->tgy, nq)); CK(a->alloc(&a->tlim, nq));
     launch_fill_ghost_grad(a->tgx, a->tgy, a->tlim, (int)m.n_real, (int)m.n_total, 4, false, s->stream);
@@ -1569,12 +1576,12 @@ int fv_adjoint_run(fv_adjoint* a, const double* theta, double* loss, double* gra
     // ---- forward: checkpoints every `every` steps, loss
     CK(cudaMemsetAsync(a->loss, 0, 8, st));
     double* cur = a->ckpt[0];
-    double* nxt = a->Qs[0];  // scratch for the non-checkpoint states
-    double* alt = a->Qs[1 % a->Qs.size()];
+    double* nxt = a->Qn[0];  // scratch for the non-checkpoint states
+    double* alt = a->Qn[1];
     for (int n = 0; n < N; ++n) {
         double* dst = ((n + 1) % every == 0 && (n + 1) / every < a->nseg) ? a->ckpt[(size_t)(n + 1) / every]
                                                                              : (cur == nxt ? alt : nxt);
-        if ((rc = adj_forward_step(a, cur, dst, a->dt_n + n, false, 0, true))) return rc;
+        if ((rc = adj_forward_step(a, cur, dst, a->dt_n + n, false, true))) return rc;
         cur = dst;
     }
     // final state kept in the solver (fv_adjoint_final_state)
@@ -1592,17 +1599,19 @@ int fv_adjoint_run(fv_adjoint* a, const double* theta, double* loss, double* gra
     std::vector<double> dts((size_t)every);
     for (int seg = a->nseg - 1; seg >= 0; --seg) {
         const int n0 = seg * every, len = std::min(every, N - n0);
-        CK(cudaMemcpyAsync(a->Qs[0], a->ckpt[(size_t)seg], nq * 8, cudaMemcpyDeviceToDevice, st));
+        // the segment's step states (the same bits as the forward run's)
+        CK(cudaMemcpyAsync(a->Qn[0], a->ckpt[(size_t)seg], nq * 8, cudaMemcpyDeviceToDevice, st));
         for (int j = 0; j < len; ++j)
-            if ((rc = adj_forward_step(a, a->Qs[(size_t)j * S], a->Qs[(size_t)(j + 1) * S], a->dt_n + n0 + j, true, j,
-                                       false)))
+            if ((rc = adj_forward_step(a, a->Qn[(size_t)j], a->Qn[(size_t)j + 1], a->dt_n + n0 + j, false, false)))
                 return rc;
         CK(cudaMemcpyAsync(dts.data(), a->dt_n + n0, (size_t)len * 8, cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
         for (int j = len - 1; j >= 0; --j) {
+            // step j's stage states, gradients, limiters and per-cell dt
+            if ((rc = adj_forward_step(a, a->Qn[(size_t)j], a->tmp[0], a->dt_n + n0 + j, true, false))) return rc;
             CK(cudaMemsetAsync(a->lam_qn, 0, nq * 8, st));
             for (int k = S - 1; k >= 0; --k) {
-                AdjStage stg = adj_stage(a, j, k, dts[(size_t)j]);
+                AdjStage stg = adj_stage(a, a->Qn[(size_t)j], a->Qn[(size_t)j + 1], k, dts[(size_t)j]);
                 adj_launch_ghosts(TP.P, a->F, stg, st);
                 adj_launch_residual(TP.P, a->F, stg, st);
                 if (TP.P.order2) adj_launch_gradlim(TP.P, a->F, stg, st);
@@ -1610,11 +1619,11 @@ int fv_adjoint_run(fv_adjoint* a, const double* theta, double* loss, double* gra
             }
             adj_launch_add(a->lam_qn, a->lamA, nq, st);  // q_n is stage 0's input
             adj_launch_sum(a->partials, S * nblk, a->lam_dt, st);
-            const double* qn = a->Qs[(size_t)j * S];
+            const double* qn = a->Qn[(size_t)j];
             if (a->n_loss)
                 adj_launch_loss_adjoint(TP.P, qn, a->dt_n + n0 + j, a->loss_ghosts, a->n_loss, 1.0, a->lam_qn, a->lam_dt, st);
             if (TP.P.dt_kind == FV_DT_CFL_SUM)
-                adj_launch_dt(TP.P, a->F, qn, a->dtc[(size_t)j], a->dt_n + n0 + j, a->lam_dt, a->lam_qn, a->argmin, st);
+                adj_launch_dt(TP.P, a->F, qn, a->dtc, a->dt_n + n0 + j, a->lam_dt, a->lam_qn, a->argmin, st);
             std::swap(a->lamA, a->lam_qn);
             CK(cudaGetLastError());
         }

@@ -3,6 +3,9 @@
 #include "fv_mesh.h"
 
 #include <algorithm>
+#include <charconv>
+#include <thread>
+#include <unordered_map>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -287,9 +290,14 @@ void build_device_numbering(HostMesh& m) {
     // strips) compact; on rank coordinates it keeps strongly graded cells
     // (boundary layers) compact in cell counts.  The order with the smaller
     // tile halos is kept.
-    std::vector<int32_t> geo = hilbert_order(m, offs, false);
-    std::vector<int32_t> rnk = hilbert_order(m, offs, true);
-    const bool use_rank = halo_score(m, rnk) < halo_score(m, geo);
+    // the two candidate orders are built and scored on two threads
+    std::vector<int32_t> geo, rnk;
+    double s_geo = 0., s_rnk = 0.;
+    std::thread tr([&] { rnk = hilbert_order(m, offs, true); s_rnk = halo_score(m, rnk); });
+    geo = hilbert_order(m, offs, false);
+    s_geo = halo_score(m, geo);
+    tr.join();
+    const bool use_rank = s_rnk < s_geo;
     m.new2ref.resize(nt);
     std::copy(use_rank ? rnk.begin() : geo.begin(), use_rank ? rnk.end() : geo.end(), m.new2ref.begin());
     m.ref2new.assign(nt, -1);
@@ -527,9 +535,43 @@ std::string read_msh41(const std::string& path, HostMesh& m) {
         p = (q < end) ? q + 1 : end;
         return true;
     };
+    // the node and element lines are parsed in place: integers and doubles
+    // with std::from_chars (correctly rounded, as strtod), no line copies
+    auto skip_ws = [&]() { while (p < end && (*p == ' ' || *p == '\t')) ++p; };
+    auto eol = [&]() {
+        const char* q = (const char*)std::memchr(p, '\n', end - p);
+        p = q ? q + 1 : end;
+    };
+    auto read_long = [&](long& v) -> bool {
+        skip_ws();
+        auto r = std::from_chars(p, end, v);
+        if (r.ec != std::errc()) return false;
+        p = r.ptr;
+        return true;
+    };
+    auto read_double = [&](double& v) -> bool {
+        skip_ws();
+        auto r = std::from_chars(p, end, v);
+        if (r.ec != std::errc()) return false;
+        p = r.ptr;
+        return true;
+    };
     std::map<long, std::string> phys_names;
     std::map<long, long> curve_phys;
-    std::map<long, long> node_index;  // MSH node tag -> index
+    // MSH node tag -> index: dense over [tag_min, tag_max] when the tags are
+    // (nearly) contiguous, as gmsh writes them; a hash map otherwise
+    long tag_min = 0;
+    std::vector<int64_t> node_dense;
+    std::unordered_map<long, int64_t> node_sparse;
+    bool dense = true;
+    auto node_of = [&](long tag) -> int64_t {
+        if (dense) {
+            const long i = tag - tag_min;
+            return (i >= 0 && i < (long)node_dense.size()) ? node_dense[(size_t)i] : -1;
+        }
+        auto it = node_sparse.find(tag);
+        return it == node_sparse.end() ? -1 : it->second;
+    };
     std::map<long, int32_t> tag_group;
     m.nodes_x.clear(); m.nodes_y.clear(); m.cells4.clear();
     m.bnd_nodes.clear(); m.bnd_group.clear(); m.group_names.clear();
@@ -572,18 +614,29 @@ std::string read_msh41(const std::string& path, HostMesh& m) {
                 long nblocks, nnodes, mn, mx;
                 if (std::sscanf(line.c_str(), "%ld %ld %ld %ld", &nblocks, &nnodes, &mn, &mx) != 4) return "bad $Nodes header";
                 m.nodes_x.reserve(nnodes); m.nodes_y.reserve(nnodes);
+                tag_min = mn;
+                dense = mx >= mn && mx - mn < 4 * std::max(nnodes, 1L) + 16;
+                if (dense) node_dense.assign((size_t)(mx - mn + 1), -1);
                 for (long b = 0; b < nblocks; ++b) {
                     next_line(line);
                     long edim, etag, param, nin;
                     if (std::sscanf(line.c_str(), "%ld %ld %ld %ld", &edim, &etag, &param, &nin) != 4) return "bad node block";
                     std::vector<long> tags(nin);
-                    for (long i = 0; i < nin; ++i) { next_line(line); tags[i] = std::stol(line); }
                     for (long i = 0; i < nin; ++i) {
-                        next_line(line);
-                        char* e1; char* e2;
-                        double x = std::strtod(line.c_str(), &e1);
-                        double y = std::strtod(e1, &e2);
-                        node_index[tags[i]] = (long)m.nodes_x.size();
+                        if (!read_long(tags[i])) return "bad node tag";
+                        eol();
+                    }
+                    for (long i = 0; i < nin; ++i) {
+                        double x, y;
+                        if (!read_double(x) || !read_double(y)) return "bad node coordinates";
+                        eol();
+                        const long t = tags[i];
+                        if (dense) {
+                            if (t < mn || t > mx) return "node tag outside the $Nodes range";
+                            node_dense[(size_t)(t - mn)] = (int64_t)m.nodes_x.size();
+                        } else {
+                            node_sparse[t] = (int64_t)m.nodes_x.size();
+                        }
                         m.nodes_x.push_back(x); m.nodes_y.push_back(y);
                     }
                 }
@@ -611,25 +664,32 @@ std::string read_msh41(const std::string& path, HostMesh& m) {
                             group = g->second;
                         }
                     }
+                    if (edim == 2) m.cells4.reserve(m.cells4.size() + 4 * (size_t)nin);
                     for (long i = 0; i < nin; ++i) {
-                        next_line(line);
                         long v[16]; int nv = 0;
-                        const char* s = line.c_str();
-                        char* e;
+                        const char* le = (const char*)std::memchr(p, '\n', end - p);
+                        if (!le) le = end;
                         while (nv < 16) {
-                            long x = std::strtol(s, &e, 10);
-                            if (e == s) break;
-                            v[nv++] = x; s = e;
+                            while (p < le && (*p == ' ' || *p == '\t' || *p == '\r')) ++p;
+                            auto r = std::from_chars(p, le, v[nv]);
+                            if (r.ec != std::errc()) break;
+                            p = r.ptr;
+                            ++nv;
                         }
+                        p = le < end ? le + 1 : end;
                         const int nnode = nv - 1;
+                        int64_t idx[4] = {-1, -1, -1, -1};
+                        for (int k = 0; k < nnode && k < 4; ++k) {
+                            idx[k] = node_of(v[1 + k]);
+                            if (idx[k] < 0) return "element " + std::to_string(v[0]) + " names an unknown node";
+                        }
                         if (edim == 1 && nnode == 2) {
-                            m.bnd_nodes.push_back((int32_t)node_index.at(v[1]));
-                            m.bnd_nodes.push_back((int32_t)node_index.at(v[2]));
+                            m.bnd_nodes.push_back((int32_t)idx[0]);
+                            m.bnd_nodes.push_back((int32_t)idx[1]);
                             m.bnd_group.push_back(group);
                         } else if (edim == 2) {
                             if (nnode != 3 && nnode != 4) return "only 3- and 4-node cells are supported";
-                            for (int k = 0; k < 4; ++k)
-                                m.cells4.push_back(k < nnode ? (int32_t)node_index.at(v[1 + k]) : -1);
+                            for (int k = 0; k < 4; ++k) m.cells4.push_back(k < nnode ? (int32_t)idx[k] : -1);
                         }
                     }
                 }
