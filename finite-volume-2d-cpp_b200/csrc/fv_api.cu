@@ -1093,6 +1093,40 @@ struct DevTmp {
 };
 }  // namespace
 
+int fv_output_fields(fv_solver* s, const double* q, int64_t n, int32_t n_fields, const int32_t* kinds,
+                     double* out) {
+    if (!s || !kinds || !out || n_fields < 0 || n_fields > 8) return fail(FV_ERR_ARG, "fv_output_fields: invalid arguments");
+    if (q && n != s->n_real && n != s->n_total) return fail(FV_ERR_ARG, "fv_output_fields: n must be n_real or n_total");
+    OutputPlan plan{};
+    plan.n = n_fields;
+    int64_t total = 0;
+    for (int f = 0; f < n_fields; ++f) {
+        const int k = kinds[f];
+        const int nc = (k == FV_OUT_PRESSURE || k == FV_OUT_MACH) ? 1 : (k == FV_OUT_VELOCITY || k == FV_OUT_STATE01) ? 2 : 0;
+        if (nc == 0) return fail(FV_ERR_UNSUPPORTED, "fv_output_fields: unknown output kind");
+        if (s->V < (k == FV_OUT_STATE01 ? 2 : 4)) return fail(FV_ERR_UNSUPPORTED, "fv_output_fields: kind needs more variables");
+        plan.kind[f] = k;
+        plan.off[f] = total;
+        total += nc * s->n_real;
+    }
+    CK(cudaSetDevice(s->device));
+    DevTmp T;
+    double* d_out;
+    CK(T.get((void**)&d_out, (size_t)std::max<int64_t>(total, 1) * 8));
+    if (q) {
+        double* d_q;
+        CK(T.get((void**)&d_q, (size_t)s->n_real * s->V * 8));
+        CK(cudaMemcpyAsync(d_q, q, (size_t)s->n_real * s->V * 8, cudaMemcpyHostToDevice, s->stream));
+        launch_output_fields(d_q, s->V, nullptr, (int)s->n_real, s->TP.P.gamma, plan, d_out, s->stream);
+    } else {
+        launch_output_fields(s->qbase[0], s->V, s->new2ref, (int)s->n_real, s->TP.P.gamma, plan, d_out, s->stream);
+    }
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(out, d_out, (size_t)total * 8, cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    return FV_OK;
+}
+
 // host (reference order, FP64) -> device (device order, FP64 in d64 and,
 // if d_s != nullptr and FP32 mode, an FP32 copy in d_s)
 static int h2d(fv_solver* s, const double* h, double* d64, void* d_s, int V) {

@@ -339,6 +339,27 @@ void launch_permute_to_ref(const double* q_dev, double* q_ref, const int32_t* ne
     k_permute_to_ref<<<grid_for(n), kBlock, 0, st>>>(q_dev, q_ref, new2ref, n, V);
 }
 
+// Extra output fields of real cells (exact::output_field) into reference
+// order: field f of cell r at out[off[f] + nc[f] * r + j].  q is in device
+// numbering (new2ref given) or in reference numbering (new2ref null).
+__global__ void k_output_fields(const double* __restrict__ q, int V, const int32_t* __restrict__ new2ref, int n_real,
+                                double gamma, OutputPlan plan, double* __restrict__ out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n_real) return;
+    const int r = new2ref ? new2ref[i] : i;
+    double qc[kMaxV] = {0., 0., 0., 0.};
+    for (int k = 0; k < V; ++k) qc[k] = q[(size_t)V * i + k];
+    for (int f = 0; f < plan.n; ++f) {
+        double v[2];
+        const int nc = exact::output_field(plan.kind[f], gamma, qc, v);
+        for (int j = 0; j < nc; ++j) out[plan.off[f] + (size_t)nc * r + j] = v[j];
+    }
+}
+void launch_output_fields(const double* q, int V, const int32_t* new2ref, int n_real, double gamma,
+                          const OutputPlan& plan, double* out, cudaStream_t st) {
+    k_output_fields<<<grid_for(n_real), kBlock, 0, st>>>(q, V, new2ref, n_real, gamma, plan, out);
+}
+
 __global__ void k_to_float(const double* __restrict__ a, float* __restrict__ b, size_t n) {
     const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) b[i] = (float)a[i];

@@ -57,6 +57,12 @@ int fv_kind_face_gradient(int32_t V, const double* gxi, const double* gyi, const
     return FV_OK;
 }
 
+int fv_kind_output(int32_t kind, double gamma, const double* q, double* out) {
+    if (!q || !out) return FV_ERR_ARG;
+    const int nc = fvgpu::exact::output_field(kind, gamma, q, out);
+    return nc > 0 ? nc : FV_ERR_UNSUPPORTED;
+}
+
 int fv_kind_limiter(int32_t kind, double y, double* out) {
     if (!out) return FV_ERR_ARG;
     if (kind < FV_LIM_ZERO || kind > FV_LIM_MINMOD) return FV_ERR_UNSUPPORTED;

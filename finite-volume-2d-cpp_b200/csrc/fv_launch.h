@@ -36,6 +36,14 @@ void launch_smooth(const Params& P, const uint32_t* nbr, const double* qt_in, co
 // utilities (fv_kernels_exact.cu)
 void launch_permute_to_device(const double* q_ref, double* q_dev, const int32_t* new2ref,
                               int n_total, int V, cudaStream_t st);
+// extra output fields (exact::output_field) of the real cells, reference order
+struct OutputPlan {
+    int n;
+    int kind[8];
+    int64_t off[8];
+};
+void launch_output_fields(const double* q, int V, const int32_t* new2ref, int n_real, double gamma,
+                          const OutputPlan& plan, double* out, cudaStream_t st);
 void launch_permute_to_ref(const double* q_dev, double* q_ref, const int32_t* new2ref,
                            int n_total, int V, cudaStream_t st);
 void launch_fill_ghost_grad(void* gx, void* gy, void* lim, int n_real, int n_total, int V, bool f32,

@@ -171,6 +171,36 @@ FV_HD double visc_eig(const Params& P, double rho, double le, double A) {
     return dmax(4. / (3. * rho), P.gamma / rho) * (P.mu / P.pr) * le * le / A;
 }
 
+// Extra output fields of the examples' post:: callbacks (post.h:24-30), in
+// their evaluation order: 1 pressure (examples/forwardStep/main.cpp:37-39,
+// 289-292; shockTube/main.cpp:181-184), 2 Mach number (forwardStep/main.cpp:
+// 293-299), 3 velocity (forwardStep/main.cpp:283-287), 4 the first two state
+// components (burgers/main.cpp:133-137).  Returns the number of components.
+FV_HD int output_field(int kind, double gamma, const double* q, double* out) {
+    if (kind == 1) {
+        out[0] = (gamma - 1) * (q[3] - 0.5 / q[0] * (q[1] * q[1] + q[2] * q[2]));
+        return 1;
+    }
+    if (kind == 2) {
+        const double p = (gamma - 1) * (q[3] - 0.5 / q[0] * (q[1] * q[1] + q[2] * q[2]));
+        const double c = sqrt(gamma * p / q[0]);
+        const double unorm = sqrt(q[1] * q[1] + q[2] * q[2]) / q[0];
+        out[0] = unorm / c;
+        return 1;
+    }
+    if (kind == 3) {
+        out[0] = q[1] / q[0];
+        out[1] = q[2] / q[0];
+        return 2;
+    }
+    if (kind == 4) {
+        out[0] = q[0];
+        out[1] = q[1];
+        return 2;
+    }
+    return 0;
+}
+
 // Limiter functions phi (limiter_func).  ZERO: shockTube/main.cpp:60-62.
 // MICHALAK (y_t = 2): forwardStep/main.cpp:57-66.  MINMOD: burgers/main.cpp:
 // 51-53.  VENKAT: (y^2 + 2y)/(y^2 + y + 2), Venkatakrishnan (1995).

@@ -254,6 +254,29 @@ class Solver:
         self.tuned_ms_per_step = ms.value
         return self
 
+    OUTPUT_KINDS = {"pressure": 1, "mach": 2, "velocity": 3, "state01": 4}
+
+    def output_fields(self, kinds, q=None):
+        """Extra output fields (fv_output_fields) of the real cells in
+        reference order: a list of arrays, [n_real] for pressure / mach,
+        [n_real, 2] for velocity / state01.  q: a host state (reference
+        numbering), or None for the solver's current state."""
+        ks = (C.c_int32 * len(kinds))(*[self.OUTPUT_KINDS[k] for k in kinds])
+        ncs = [2 if k in ("velocity", "state01") else 1 for k in kinds]
+        n_real = self.mesh.n_real
+        out = np.zeros(sum(ncs) * n_real)
+        qp, n = None, 0
+        if q is not None:
+            q = np.ascontiguousarray(q, np.float64)
+            qp, n = _p(q), q.size // self.V
+        _check(lib().fv_output_fields(self._h, qp, C.c_int64(n), C.c_int32(len(kinds)), ks, _p(out)))
+        res, o = [], 0
+        for nc in ncs:
+            a = out[o:o + nc * n_real]
+            res.append(a.reshape(n_real, 2) if nc == 2 else a)
+            o += nc * n_real
+        return res
+
     @property
     def stage_kernels(self):
         """"fused" or "split": the stage kernels this solver runs."""

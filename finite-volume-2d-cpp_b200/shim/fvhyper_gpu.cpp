@@ -424,6 +424,43 @@ struct SolverHandle {
     ~SolverHandle() { if (s) fv_solver_destroy(s); }
 };
 
+// The last run()'s solver and the device output kinds of the post::
+// callbacks.  writeVtk evaluates a callback whose results match a device
+// output kind bit for bit on probe states with fv_output_fields, on the
+// device; a callback that matches none runs on the host.  The solver is kept
+// until the next run() (and, deliberately, not destroyed at process exit,
+// when the CUDA runtime may already be gone).
+struct OutputState {
+    ::fv_solver* solver = nullptr;
+    int V = 0;
+    int64_t n_real = 0, n_total = 0;
+    std::map<std::string, int> kinds;  // "s:" / "v:" + callback name -> FV_OUT_* or 0
+};
+OutputState& out_state() {
+    static OutputState* o = new OutputState();
+    return *o;
+}
+
+int identify_output(void (*fn)(double*, double*), bool vector, int V, double gamma) {
+    const int cands[2] = {vector ? FV_OUT_VELOCITY : FV_OUT_PRESSURE, vector ? FV_OUT_STATE01 : FV_OUT_MACH};
+    for (int k : cands) {
+        if ((k == FV_OUT_STATE01 && V < 2) || (k != FV_OUT_STATE01 && V != 4)) continue;
+        Probe pr;
+        bool ok = true;
+        for (int t = 0; t < 64 && ok; ++t) {
+            double q[4] = {0., 0., 0., 0.};
+            if (V == 4) pr.euler(q, gamma);
+            else for (int i = 0; i < V && i < 4; ++i) q[i] = pr.uni(-2.0, 2.0);
+            double a[2] = {0., 0.}, b[2] = {0., 0.};
+            fn(a, q);
+            const int nc = fv_kind_output(k, gamma, q, b);
+            ok = nc > 0 && std::memcmp(a, b, sizeof(double) * (size_t)nc) == 0;
+        }
+        if (ok) return k;
+    }
+    return 0;
+}
+
 // calc_dt -> (dt_kind, cfl, dt_const) on the probe mesh: the user's dt over
 // random states against the device's fv_stage_dt (FP64_EXACT), bit for bit.
 // cfl is recovered from the ratio to a cfl = 1 run, rounded to 12 significant
@@ -579,9 +616,17 @@ void run(const std::string name, std::vector<double>& q, mpi_wrapper& pool, mesh
     ph.group_bv = group_bv.data();
     ph.positivity_guard = 0;
 
-    SolverHandle h;
-    check(fv_solver_create(m.device_mesh(), &ph, precision, device, &h.s), "fv_solver_create");
-    check(fv_set_state(h.s, q.data()), "fv_set_state");
+    OutputState& os = out_state();
+    if (os.solver) { fv_solver_destroy(os.solver); os.solver = nullptr; }
+    os.V = V;
+    os.n_real = m.nRealCells;
+    os.n_total = (int64_t)m.cellsAreas.size();
+    os.kinds.clear();
+    for (auto& kv : post::extra_scalars) os.kinds["s:" + kv.first] = identify_output(kv.second, false, V, ph.gamma);
+    for (auto& kv : post::extra_vectors) os.kinds["v:" + kv.first] = identify_output(kv.second, true, V, ph.gamma);
+    check(fv_solver_create(m.device_mesh(), &ph, precision, device, &os.solver), "fv_solver_create");
+    ::fv_solver* const hs = os.solver;
+    check(fv_set_state(hs, q.data()), "fv_set_state");
 
     // RK5 stage coefficients (explicit.cpp:681-687)
     const double alpha[5] = {0.0695, 0.1602, 0.2898, 0.506, 1.};
@@ -618,21 +663,21 @@ void run(const std::string name, std::vector<double>& q, mpi_wrapper& pool, mesh
         ro.max_step = opt.max_step;
         ro.max_time = opt.max_time;
         if (opt.save_time_series) ro.max_time = std::min(opt.max_time, std::nextafter(save_time, INFINITY));
-        check(fv_run(h.s, &ro, &info), "fv_run");
+        check(fv_run(hs, &ro, &info), "fv_run");
         ro.restart = 0;
         if (!opt.save_time_series) break;
         ro.max_time = opt.max_time;
         ro.max_step = std::min<uint64_t>(opt.max_step, info.step + 1);
         if (ro.max_step <= info.step) break;
         const uint64_t before = info.step;
-        check(fv_run(h.s, &ro, &info), "fv_run");
+        check(fv_run(hs, &ro, &info), "fv_run");
         if (info.step == before) break;
-        check(fv_get_state(h.s, q.data()), "fv_get_state");
+        check(fv_get_state(hs, q.data()), "fv_get_state");
         writeVtk(name, q, m, pool.rank, pool.size, std::to_string(time_step));
         save_time += opt.time_series_interval;
         time_step += 1;
     }
-    check(fv_get_state(h.s, q.data()), "fv_get_state");
+    check(fv_get_state(hs, q.data()), "fv_get_state");
 
     if (verbose) {
         std::cout << (uint)info.step << ", " << info.time << ", " << seconds_since(pc.begin) << ", ";
@@ -647,8 +692,72 @@ void run(const std::string name, std::vector<double>& q, mpi_wrapper& pool, mesh
 // -------------------------------------------------------------- writeVtk --
 namespace {
 
+// The post:: extra fields of the real cells, in the callbacks' map order:
+// scalars (N values), then vectors (N pairs).  Callbacks identified with a
+// device output kind are evaluated on the device by the last run's solver
+// (FVGPU_POST=host evaluates every callback on the host instead).
+struct Extras {
+    std::vector<std::vector<double>> scalars, vectors;
+};
+Extras extra_fields(std::vector<double>& q, mesh& m) {
+    const size_t nv = var_names.size();
+    const uint N = m.nRealCells;
+    Extras ex;
+    const OutputState& os = out_state();
+    const char* pe = std::getenv("FVGPU_POST");
+    const bool host_only = pe && std::string(pe) == "host";
+    const int64_t nq = nv ? (int64_t)(q.size() / nv) : 0;
+    const bool device = !host_only && os.solver && os.V == (int)nv && os.n_real == (int64_t)N &&
+                        (nq == os.n_real || nq == os.n_total);
+    auto kind_of = [&](const std::string& key) {
+        auto it = os.kinds.find(key);
+        return (device && it != os.kinds.end()) ? it->second : 0;
+    };
+    std::vector<int32_t> kinds;
+    for (auto& kv : post::extra_scalars) if (int k = kind_of("s:" + kv.first)) kinds.push_back(k);
+    for (auto& kv : post::extra_vectors) if (int k = kind_of("v:" + kv.first)) kinds.push_back(k);
+    std::vector<double> dev;
+    if (!kinds.empty()) {
+        size_t total = 0;
+        for (int k : kinds) total += (k == FV_OUT_VELOCITY || k == FV_OUT_STATE01 ? 2 : 1) * (size_t)N;
+        dev.resize(total);
+        check(fv_output_fields(os.solver, q.data(), nq, (int32_t)kinds.size(), kinds.data(), dev.data()),
+              "fv_output_fields");
+    }
+    size_t off = 0;
+    for (auto& kv : post::extra_scalars) {
+        std::vector<double> col(N);
+        if (kind_of("s:" + kv.first)) {
+            std::copy(dev.begin() + (long)off, dev.begin() + (long)(off + N), col.begin());
+            off += N;
+        } else {
+            for (uint c = 0; c < N; ++c) {
+                double v[1];
+                kv.second(v, &q[nv * c]);
+                col[c] = v[0];
+            }
+        }
+        ex.scalars.push_back(std::move(col));
+    }
+    for (auto& kv : post::extra_vectors) {
+        std::vector<double> vec(2 * (size_t)N);
+        if (kind_of("v:" + kv.first)) {
+            std::copy(dev.begin() + (long)off, dev.begin() + (long)(off + 2 * (size_t)N), vec.begin());
+            off += 2 * (size_t)N;
+        } else {
+            for (uint c = 0; c < N; ++c) {
+                double v[2];
+                kv.second(v, &q[nv * c]);
+                vec[2 * c] = v[0]; vec[2 * c + 1] = v[1];
+            }
+        }
+        ex.vectors.push_back(std::move(vec));
+    }
+    return ex;
+}
+
 // the reference's ASCII layout, byte for byte (fvhyper/src/post.cpp:21-200)
-std::string vtu_ascii(std::vector<double>& q, mesh& m, int rank) {
+std::string vtu_ascii(std::vector<double>& q, mesh& m, int rank, const Extras& ex) {
     const size_t nv = var_names.size();
     const uint N = m.nRealCells;
     std::string s;
@@ -697,23 +806,21 @@ std::string vtu_ascii(std::vector<double>& q, mesh& m, int rank) {
         for (uint c = 0; c < N; ++c) s += "          " + std::to_string(q[nv * c + i]) + "\n";
         s += "        </DataArray>\n";
     }
+    size_t f = 0;
     for (auto& kv : post::extra_scalars) {
         s += "        <DataArray type=\"Float32\" Name=\"" + kv.first + "\" Format=\"ascii\">\n";
-        for (uint c = 0; c < N; ++c) {
-            double v[1];
-            kv.second(v, &q[nv * c]);
-            s += "          " + std::to_string(v[0]) + "\n";
-        }
+        const std::vector<double>& col = ex.scalars[f++];
+        for (uint c = 0; c < N; ++c) s += "          " + std::to_string(col[c]) + "\n";
         s += "        </DataArray>\n";
     }
+    f = 0;
     for (auto& kv : post::extra_vectors) {
         s += "        <DataArray type=\"Float32\" Name=\"" + kv.first +
              "\" NumberOfComponents=\"3\" Format=\"ascii\">\n";
+        const std::vector<double>& vec = ex.vectors[f++];
         for (uint c = 0; c < N; ++c) {
-            double v[2];
-            kv.second(v, &q[nv * c]);
-            s += "          " + std::to_string(v[0]) + " ";
-            s += std::to_string(v[1]) + " 0.0\n";
+            s += "          " + std::to_string(vec[2 * c]) + " ";
+            s += std::to_string(vec[2 * c + 1]) + " 0.0\n";
         }
         s += "        </DataArray>\n";
     }
@@ -737,7 +844,7 @@ struct Appended {
     }
 };
 
-std::string vtu_binary(std::vector<double>& q, mesh& m, int rank) {
+std::string vtu_binary(std::vector<double>& q, mesh& m, int rank, const Extras& ex) {
     const size_t nv = var_names.size();
     const uint N = m.nRealCells;
     Appended a;
@@ -778,21 +885,14 @@ std::string vtu_binary(std::vector<double>& q, mesh& m, int rank) {
         for (uint c = 0; c < N; ++c) col[c] = q[nv * c + i];
         a.array("type=\"Float64\" Name=\"" + var_names[i] + "\"", col, "        ");
     }
-    for (auto& kv : post::extra_scalars) {
-        for (uint c = 0; c < N; ++c) {
-            double v[1];
-            kv.second(v, &q[nv * c]);
-            col[c] = v[0];
-        }
-        a.array("type=\"Float64\" Name=\"" + kv.first + "\"", col, "        ");
-    }
+    size_t f = 0;
+    for (auto& kv : post::extra_scalars)
+        a.array("type=\"Float64\" Name=\"" + kv.first + "\"", ex.scalars[f++], "        ");
+    f = 0;
     for (auto& kv : post::extra_vectors) {
+        const std::vector<double>& v2 = ex.vectors[f++];
         std::vector<double> vec(3 * (size_t)N);
-        for (uint c = 0; c < N; ++c) {
-            double v[2];
-            kv.second(v, &q[nv * c]);
-            vec[3 * c] = v[0]; vec[3 * c + 1] = v[1]; vec[3 * c + 2] = 0.0;
-        }
+        for (uint c = 0; c < N; ++c) { vec[3 * c] = v2[2 * c]; vec[3 * c + 1] = v2[2 * c + 1]; vec[3 * c + 2] = 0.0; }
         a.array("type=\"Float64\" Name=\"" + kv.first + "\" NumberOfComponents=\"3\"", vec, "        ");
     }
     a.xml += "      </CellData>\n";
@@ -851,7 +951,8 @@ void writeVtk(const std::string name, std::vector<double>& q, mesh& m, int rank,
     }
     // as the reference: a missing times/ folder means no file, not an error
     std::ofstream out(filename, std::ios::binary);
-    const std::string body = ascii ? vtu_ascii(q, m, rank) : vtu_binary(q, m, rank);
+    const Extras ex = extra_fields(q, m);
+    const std::string body = ascii ? vtu_ascii(q, m, rank, ex) : vtu_binary(q, m, rank, ex);
     out.write(body.data(), (std::streamsize)body.size());
 }
 

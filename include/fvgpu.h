@@ -280,6 +280,15 @@ int fv_solver_set_chunk(fv_solver* s, int32_t steps);
 /* out[6] = {tiles, cells per tile, max halo cells per tile, max edges per
  * tile, precision, bytes per stored stage value}. */
 int fv_solver_info(fv_solver* s, int64_t* out);
+/* Extra output fields evaluated on the device (the writeVtk callbacks of
+ * post.cpp:165-188): for each of n_fields (at most 8) kinds FV_OUT_*, the
+ * values of the real cells in reference order, one after the other in `out`
+ * (n_real values for a one-component kind, n_real pairs for a two-component
+ * one).  q: a host state [n][V] in reference numbering, n = n_real or
+ * n_total; NULL evaluates the solver's current state.  gamma is the
+ * solver's.  Bit-identical to fv_kind_output cell by cell. */
+int fv_output_fields(fv_solver* s, const double* q, int64_t n, int32_t n_fields, const int32_t* kinds,
+                     double* out);
 /* The stage kernels the solver runs: FV_STAGE_FUSED or FV_STAGE_SPLIT. */
 int fv_solver_stage_kernels(fv_solver* s);
 /* Device time of the last fv_run's chunks and per-kernel launch count. */
@@ -351,6 +360,14 @@ int fv_kind_face_gradient(int32_t V, const double* gxi, const double* gyi, const
                           const double* gyj, const double* qi, const double* qj, const double* ci,
                           const double* cj, double* gxf, double* gyf);
 int fv_kind_limiter(int32_t kind, double y, double* out);
+/* Extra output fields of the examples' post::extra_scalars / extra_vectors
+ * callbacks (post.h:24-30): FV_OUT_PRESSURE and FV_OUT_MACH (one component,
+ * examples/forwardStep/main.cpp:289-299), FV_OUT_VELOCITY (u, v;
+ * forwardStep/main.cpp:283-287) and FV_OUT_STATE01 (q[0], q[1];
+ * examples/burgers/main.cpp:133-137), in the examples' arithmetic.  Host copy
+ * for identification: returns the number of components written to out. */
+enum { FV_OUT_PRESSURE = 1, FV_OUT_MACH = 2, FV_OUT_VELOCITY = 3, FV_OUT_STATE01 = 4 };
+int fv_kind_output(int32_t kind, double gamma, const double* q, double* out);
 /* bv: [4] boundary state of INLET_OUTLET / FARFIELD (may be NULL otherwise). */
 int fv_kind_bc(int32_t kind, int32_t V, double gamma, const double* bv, const double* q,
                const double* n, double* b);

@@ -370,3 +370,35 @@ def test_fused_stage_kernel_is_chosen_where_the_physics_allow():
     with pytest.raises(fvgpu.FvError) as e:
         fvgpu.Solver(fvgpu.Mesh.from_elements(case["mesh"]()), case["phys"](), "fp64", stage_kernels="fused")
     assert e.value.code == -4
+
+
+@pytest.mark.parametrize("precision", ["fp64_exact", "fp32"])
+def test_output_fields_on_the_device_equal_the_host_kinds(precision):
+    """fv_output_fields (the writeVtk extra fields, evaluated on the device)
+    gives the host kinds' bits for every real cell, from a host state and from
+    the solver's own state."""
+    import ctypes as C
+    case = CASES["step_o2_venk5"]
+    em = case["mesh"]()
+    mesh = fvgpu.Mesh.from_elements(em)
+    s = fvgpu.Solver(mesh, case["phys"](), precision)
+    q = random_euler_state(mesh.n_total, 31)
+    kinds = ["pressure", "mach", "velocity", "state01"]
+    L = fvgpu.lib()
+    p = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))
+    want = []
+    for k in kinds:
+        nc = 2 if k in ("velocity", "state01") else 1
+        w = np.zeros((mesh.n_real, nc))
+        for c in range(mesh.n_real):
+            o = np.zeros(2)
+            L.fv_kind_output(fvgpu.Solver.OUTPUT_KINDS[k], C.c_double(1.4), p(q[4 * c:4 * c + 4].copy()), p(o))
+            w[c] = o[:nc]
+        want.append(w if nc == 2 else w[:, 0])
+    for got in (s.output_fields(kinds, q), None):
+        if got is None:  # the solver's state (FP64 base state, device numbering)
+            s.set_state(q)
+            got = s.output_fields(kinds)
+        for g, w, k in zip(got, want, kinds):
+            assert g.tobytes() == w.tobytes(), k
+    s.close()

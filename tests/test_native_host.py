@@ -10,7 +10,7 @@ import pytest
 
 import fvgpu
 import meshgen
-from cases import CASES
+from cases import CASES, random_euler_state
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
@@ -452,3 +452,23 @@ def test_two_ring_tile_layout_indices_stay_in_bounds(T):
                     prev_e = e_ref
                 assert nf == len(nbrs[cell])
         assert face_end == len(face)
+
+
+def test_output_kinds_follow_the_examples_arithmetic():
+    """The host copies of the device output kinds are the examples' post::
+    callbacks operation for operation (examples/forwardStep/main.cpp:37-39,
+    283-299; burgers/main.cpp:133-137): pressure, Mach, velocity, q[0:2]."""
+    import ctypes as C
+    L = fvgpu.lib()
+    p = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))
+    g = 1.4
+    for seed in range(200):
+        q = random_euler_state(1, seed)
+        pres = (g - 1) * (q[3] - 0.5 / q[0] * (q[1] * q[1] + q[2] * q[2]))
+        want = {1: [pres], 2: [(np.sqrt(q[1] * q[1] + q[2] * q[2]) / q[0]) / np.sqrt(g * pres / q[0])],
+                3: [q[1] / q[0], q[2] / q[0]], 4: [q[0], q[1]]}
+        for k, w in want.items():
+            out = np.zeros(2)
+            assert L.fv_kind_output(k, C.c_double(g), p(q), p(out)) == len(w)
+            assert out[: len(w)].tobytes() == np.array(w).tobytes(), (k, seed)
+    assert L.fv_kind_output(9, C.c_double(g), p(q), p(out)) == -4

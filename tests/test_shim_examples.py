@@ -318,3 +318,26 @@ def test_naca_example_runs_from_the_reference_su2_mesh(tmp_path):
     assert max(_num(x) for x in last[2]) < 0.1 * max(_num(x) for x in first[2]), (first, last)
     q = _read_binary_vtu(str(tmp_path / "naca.vtu"))
     assert q["rho"].size == 16384 and np.all(np.isfinite(q["rho"])) and np.all(q["rho"] > 0)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["shockTube", "burgers", "naca", "nacaTransient"])
+def test_extra_fields_evaluated_on_the_device_equal_the_host_callbacks(name, tmp_path):
+    """The examples' post::extra_scalars / extra_vectors (pressure, Mach,
+    velocity; Burgers' state vector) are identified with device output kinds
+    and evaluated on the device by writeVtk: the binary VTU files (Float64
+    values) are byte-identical to those written with every callback run on
+    the host (FVGPU_POST=host)."""
+    d_dev, d_host = str(tmp_path / "dev"), str(tmp_path / "host")
+    _setup(d_dev, name)
+    _setup(d_host, name)
+    _run_gpu(name, d_dev, "binary")
+    env = dict(os.environ, FVGPU_VTK_FORMAT="binary", FVGPU_PRECISION="fp64_exact", FVGPU_POST="host")
+    r = subprocess.run([_program(name)], cwd=d_host, env=env, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    files = _outputs(d_host)
+    assert files and _outputs(d_dev) == files
+    for f in files:
+        a = open(os.path.join(d_dev, f), "rb").read()
+        b = open(os.path.join(d_host, f), "rb").read()
+        assert a == b, f
