@@ -508,6 +508,7 @@ def run_batch_modes(args, local, dist, world):
     out = {"workload": desc, "n_real_cells": mesh.n_real, "n_cases": mesh.n_cases, "steps": ba.steps}
     for prec, r in res.items():
         out[prec] = {"value": r["value"], "ms_per_step": r["ms_per_step"], "tile_cells": r["solver"].tile_cells,
+                     "stage_kernels": r["stage_kernels"],
                      "stage_roofline_frac": r["roofline"]["frac"],
                      "l2_error_vs_exact_riemann": batch_error_vs_exact(mesh, geo, r["q_final"], r["case_times"], states),
                      "state_finite": bool(r["state_finite"]), "clocks": r["clocks"]}

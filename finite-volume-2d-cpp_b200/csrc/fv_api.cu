@@ -118,6 +118,13 @@ struct fv_solver {
     }
 };
 
+// Drops the captured step graphs (their kernels change with s->fused).
+static void clear_graphs(fv_solver* s) {
+    for (auto& g : s->graphs)
+        if (g.exec) cudaGraphExecDestroy(g.exec);
+    s->graphs.clear();
+}
+
 namespace {
 // host vector<double> -> device array of the stage precision
 int upload_s(fv_solver* s, const std::vector<double>& v, const void** out) {
@@ -617,28 +624,44 @@ int fv_solver_create_tuned(const fv_mesh* fm, const fv_physics* ph, int32_t prec
     fv_solver* best = nullptr;
     double best_ms = 0.0;
     int best_t = 0;
+    bool best_fused = false;
+    // candidates: tile size x edge-tile layout (the split gradient and flux
+    // kernels over one-ring tiles, or the fused stage kernel over two-ring
+    // tiles where the physics allow it); a solver built for the fused kernel
+    // holds both layouts, so each tile size is built once
     for (int t : {64, 128, 256}) {
         fv_solver_options o{t, FV_STAGE_AUTO};
         fv_solver* s = nullptr;
         int rc = fv_solver_create_ex(fm, ph, precision, device, &o, &s);
         if (rc == FV_ERR_MESH) continue;  // tile halo too large for this size
         if (rc) { fv_solver_destroy(best); return rc; }
-        // one untimed step (graph capture), then n_steps timed on the device
-        fv_run_options ro{};
-        ro.max_step = 1; ro.max_time = 1e300; ro.tolerance = -1.0; ro.print_interval = 1ull << 62;
-        ro.n_alpha = n_alpha; ro.alpha = alpha; ro.restart = 1;
-        fv_run_info info{};
-        if ((rc = fv_set_state(s, q)) || (rc = fv_run(s, &ro, &info))) { fv_solver_destroy(s); fv_solver_destroy(best); return rc; }
-        ro.max_step = 1 + (uint64_t)n_steps; ro.restart = 0;
-        if ((rc = fv_run(s, &ro, &info))) { fv_solver_destroy(s); fv_solver_destroy(best); return rc; }
-        const double ms = s->last_ms / n_steps;
+        const bool can_fuse = s->fused;
+        double ms_of[2] = {1e300, 1e300};  // split, fused
+        for (int variant = can_fuse ? 1 : 0; variant >= 0; --variant) {
+            clear_graphs(s);
+            s->fused = variant == 1;
+            // one untimed step (graph capture), then n_steps timed on the device
+            fv_run_options ro{};
+            ro.max_step = 1; ro.max_time = 1e300; ro.tolerance = -1.0; ro.print_interval = 1ull << 62;
+            ro.n_alpha = n_alpha; ro.alpha = alpha; ro.restart = 1;
+            fv_run_info info{};
+            if ((rc = fv_set_state(s, q)) || (rc = fv_run(s, &ro, &info))) { fv_solver_destroy(s); fv_solver_destroy(best); return rc; }
+            ro.max_step = 1 + (uint64_t)n_steps; ro.restart = 0;
+            if ((rc = fv_run(s, &ro, &info))) { fv_solver_destroy(s); fv_solver_destroy(best); return rc; }
+            ms_of[variant] = s->last_ms / n_steps;
+        }
+        const bool fused = ms_of[1] < ms_of[0];
+        const double ms = fused ? ms_of[1] : ms_of[0];
+        clear_graphs(s);
+        s->fused = fused;
         if (!best || ms < best_ms) {
             fv_solver_destroy(best);
-            best = s; best_ms = ms; best_t = t;
+            best = s; best_ms = ms; best_t = t; best_fused = fused;
         } else {
             fv_solver_destroy(s);
         }
     }
+    (void)best_fused;
     if (!best) return fail(FV_ERR_MESH, "fv_solver_create_tuned: no tile size fits this mesh");
     int rc = fv_set_state(best, q);
     if (rc) { fv_solver_destroy(best); return rc; }

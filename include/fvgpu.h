@@ -231,10 +231,14 @@ enum { FV_STAGE_AUTO = 0, FV_STAGE_SPLIT = 1, FV_STAGE_FUSED = 2 };
 int fv_solver_create_ex(const fv_mesh* m, const fv_physics* ph, int32_t precision, int32_t device,
                         const fv_solver_options* opt, fv_solver** out);
 /* Autotuned creation: builds the solver with each tile size (64, 128, 256
- * cells per tile = threads per CTA), times n_steps steps of the given RK
- * stages from state q on the device (after one untimed step that captures the
- * step graph), and keeps the fastest.  The returned solver holds state q
- * again, step 0; tile_cells and ms_per_step (may be NULL) report the choice. */
+ * cells per tile = threads per CTA) and, where the physics allow the fused
+ * stage kernel, with each edge-tile layout (split gradient and flux kernels
+ * over one-ring tiles, or the fused kernel over two-ring tiles); times
+ * n_steps steps of the given RK stages from state q on the device for each
+ * candidate (after one untimed step that captures the step graph), and keeps
+ * the fastest.  The returned solver holds state q again, step 0; tile_cells
+ * and ms_per_step (may be NULL) report the choice, fv_solver_stage_kernels
+ * the layout. */
 int fv_solver_create_tuned(const fv_mesh* m, const fv_physics* ph, int32_t precision, int32_t device,
                            const double* q, const double* alpha, int32_t n_alpha, int32_t n_steps,
                            fv_solver** out, int32_t* tile_cells, double* ms_per_step);
