@@ -304,7 +304,7 @@ def measure_mode(args, em, mesh, geo, ph, alpha, ic, precision, local, dist, wor
         s = fvgpu.Solver.create_tuned(mesh, ph, precision, q0, alpha=alpha, steps=3, device=local)
     else:
         s = fvgpu.Solver(mesh, ph, precision, device=local, tile_cells=args.tile_cells,
-                         stage_kernels=args.stage_kernels)
+                         stage_kernels=args.stage_kernels, schedule=args.schedule)
         s.tile_cells = args.tile_cells or 128
     fused = s.stage_kernels == "fused"
     stream = torch.cuda.Stream(device=local)
@@ -351,6 +351,7 @@ def measure_mode(args, em, mesh, geo, ph, alpha, ic, precision, local, dist, wor
     kb = (ALGO_BYTES[precision]["fused"] if fused else algo_bytes(ph, precision, "stage")) * N
     achieved = kb / (out["per_launch_ms"]["stage"] / 1e3) / 1e9
     out["stage_kernels"] = s.stage_kernels
+    out["schedule"] = s.schedule
     kname = ("gradients + limiter + flux + RK update + ghost fill of a two-ring tile (k_tile_fused)" if fused
              else "flux + RK update + ghost fill (k_tile_stage)")
     out["roofline"] = {"bound": "hbm", "kernel": kname,
@@ -508,7 +509,7 @@ def run_batch_modes(args, local, dist, world):
     out = {"workload": desc, "n_real_cells": mesh.n_real, "n_cases": mesh.n_cases, "steps": ba.steps}
     for prec, r in res.items():
         out[prec] = {"value": r["value"], "ms_per_step": r["ms_per_step"], "tile_cells": r["solver"].tile_cells,
-                     "stage_kernels": r["stage_kernels"],
+                     "stage_kernels": r["stage_kernels"], "schedule": r["schedule"],
                      "stage_roofline_frac": r["roofline"]["frac"],
                      "l2_error_vs_exact_riemann": batch_error_vs_exact(mesh, geo, r["q_final"], r["case_times"], states),
                      "state_finite": bool(r["state_finite"]), "clocks": r["clocks"]}
@@ -625,6 +626,8 @@ def main():
     ap.add_argument("--stage-kernels", default="auto", choices=["auto", "split", "fused"],
                     help="second-order Euler stage kernels: fused (one per stage) where the physics allow, "
                          "or split gradient and flux kernels")
+    ap.add_argument("--schedule", default="tile", choices=["tile", "worklist"],
+                    help="fused stage kernel: one CTA per tile, or resident CTAs taking tiles from a work list")
     ap.add_argument("--batch-steps", type=int, default=500,
                     help="steps of the batched Riemann-strip workload reported beside the forward step "
                          "(0: not run)")
@@ -682,7 +685,7 @@ def main():
                 "kernel_ms_per_launch": m["per_launch_ms"], "kernel_time_share": m["share"],
                 "clocks": m["clocks"], "state_finite": bool(m["state_finite"])}
         line["modes"] = {p: {"value": r["value"], "ms_per_step": r["ms_per_step"], "roofline_frac": r["roofline"]["frac"],
-                             "stage_kernels": r["stage_kernels"],
+                             "stage_kernels": r["stage_kernels"], "schedule": r["schedule"], "schedule": r["schedule"],
                              "grad_lim_frac": r.get("roofline_grad_lim", {}).get("frac"),
                              "dt_frac": r.get("roofline_dt", {}).get("frac"),
                              "kernel_ms_per_launch": r["per_launch_ms"], "clocks": r["clocks"],

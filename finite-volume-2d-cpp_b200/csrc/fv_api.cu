@@ -69,6 +69,10 @@ struct fv_solver {
     // the fused stage kernel over two-ring tiles (its Params are TP.P at launch)
     bool fused = false;
     FusedParams FPm{};
+    // its work-list schedule: per-stage tile counters, CTAs per launch
+    bool worklist = false;
+    int* work = nullptr;
+    int work_grid = 0;
     // device buffers
     std::vector<void*> allocs;
     double* qbase[2] = {nullptr, nullptr};   // FP64 step-start state (RK1 alternates)
@@ -534,6 +538,12 @@ int fv_solver_create_ex(const fv_mesh* fm, const fv_physics* ph, int32_t precisi
                 if ((rc = upload_s(s.get(), cca, &F.cca))) return rc;
                 CK(tile::prepare_fused(precision, F));
                 s->fused = true;
+                CK(s->alloc(&s->work, kWorkSlots));
+                CK(cudaMemset(s->work, 0, kWorkSlots * sizeof(int)));
+                s->work_grid = tile::work_grid_fused(precision, F, ta.n_tiles);
+                const int sched = opt ? opt->schedule : FV_SCHED_TILE;
+                if (sched != FV_SCHED_TILE && sched != FV_SCHED_WORKLIST) return fail(FV_ERR_ARG, "unknown schedule");
+                s->worklist = sched == FV_SCHED_WORKLIST;
             }
         }
     }
@@ -624,22 +634,22 @@ int fv_solver_create_tuned(const fv_mesh* fm, const fv_physics* ph, int32_t prec
     fv_solver* best = nullptr;
     double best_ms = 0.0;
     int best_t = 0;
-    bool best_fused = false;
     // candidates: tile size x edge-tile layout (the split gradient and flux
     // kernels over one-ring tiles, or the fused stage kernel over two-ring
     // tiles where the physics allow it); a solver built for the fused kernel
     // holds both layouts, so each tile size is built once
     for (int t : {64, 128, 256}) {
-        fv_solver_options o{t, FV_STAGE_AUTO};
+        fv_solver_options o{t, FV_STAGE_AUTO, FV_SCHED_TILE};
         fv_solver* s = nullptr;
         int rc = fv_solver_create_ex(fm, ph, precision, device, &o, &s);
         if (rc == FV_ERR_MESH) continue;  // tile halo too large for this size
         if (rc) { fv_solver_destroy(best); return rc; }
         const bool can_fuse = s->fused;
-        double ms_of[2] = {1e300, 1e300};  // split, fused
-        for (int variant = can_fuse ? 1 : 0; variant >= 0; --variant) {
+        double ms_of[3] = {1e300, 1e300, 1e300};  // split, fused one CTA per tile, fused work list
+        for (int variant = can_fuse ? 2 : 0; variant >= 0; --variant) {
             clear_graphs(s);
-            s->fused = variant == 1;
+            s->fused = variant >= 1;
+            s->worklist = variant == 2;
             // one untimed step (graph capture), then n_steps timed on the device
             fv_run_options ro{};
             ro.max_step = 1; ro.max_time = 1e300; ro.tolerance = -1.0; ro.print_interval = 1ull << 62;
@@ -650,18 +660,18 @@ int fv_solver_create_tuned(const fv_mesh* fm, const fv_physics* ph, int32_t prec
             if ((rc = fv_run(s, &ro, &info))) { fv_solver_destroy(s); fv_solver_destroy(best); return rc; }
             ms_of[variant] = s->last_ms / n_steps;
         }
-        const bool fused = ms_of[1] < ms_of[0];
-        const double ms = fused ? ms_of[1] : ms_of[0];
+        const int v = (int)(std::min_element(ms_of, ms_of + 3) - ms_of);
+        const double ms = ms_of[v];
         clear_graphs(s);
-        s->fused = fused;
+        s->fused = v >= 1;
+        s->worklist = v == 2;
         if (!best || ms < best_ms) {
             fv_solver_destroy(best);
-            best = s; best_ms = ms; best_t = t; best_fused = fused;
+            best = s; best_ms = ms; best_t = t;
         } else {
             fv_solver_destroy(s);
         }
     }
-    (void)best_fused;
     if (!best) return fail(FV_ERR_MESH, "fv_solver_create_tuned: no tile size fits this mesh");
     int rc = fv_set_state(best, q);
     if (rc) { fv_solver_destroy(best); return rc; }
@@ -850,7 +860,13 @@ static int enqueue_step(fv_solver* s, const std::vector<double>& alpha, int b, E
     // the fused stage kernel computes its gradients itself: the step's dt
     // comes from the dt kernel, as in first order
     const bool grads = (TP.P.order2 || TP.P.diffusive) && !s->fused;
-    if (!grads) { tile::launch_dt(s->precision, TP, io, st, pdl); ++n; mark(KK_DT); }
+    // the work-list schedule: one tile counter per stage, zeroed by the dt kernel
+    const bool worklist = s->fused && s->worklist && alpha.size() <= (size_t)kWorkSlots;
+    if (!grads) {
+        TileIO dio = io;
+        dio.work_reset = worklist ? s->work : nullptr;
+        tile::launch_dt(s->precision, TP, dio, st, pdl); ++n; mark(KK_DT);
+    }
     FusedParams FPl = s->FPm;
     FPl.P = TP.P;
     const int ns = (int)alpha.size();
@@ -886,7 +902,8 @@ static int enqueue_step(fv_solver* s, const std::vector<double>& alpha, int b, E
             so.qt = s->qts[2];
             tile::launch_stage(s->precision, TP, so, st, pdl, 2); ++n; mark(KK_STAGE);
         } else if (s->fused) {
-            tile::launch_fused(s->precision, FPl, so, st, pdl, s->n_tiles); ++n; mark(KK_STAGE);
+            so.work = worklist ? s->work + k : nullptr;
+            tile::launch_fused(s->precision, FPl, so, st, pdl, s->n_tiles, s->work_grid); ++n; mark(KK_STAGE);
         } else {
             tile::launch_stage(s->precision, TP, so, st, pdl); ++n; mark(KK_STAGE);
         }
@@ -1056,6 +1073,11 @@ int fv_solver_info(fv_solver* s, int64_t* out) {
 int fv_solver_stage_kernels(fv_solver* s) {
     if (!s) return fail(FV_ERR_ARG, "null solver");
     return s->fused ? FV_STAGE_FUSED : FV_STAGE_SPLIT;
+}
+
+int fv_solver_schedule(fv_solver* s) {
+    if (!s) return fail(FV_ERR_ARG, "null solver");
+    return (s->fused && s->worklist) ? FV_SCHED_WORKLIST : FV_SCHED_TILE;
 }
 
 int fv_last_run_stats(fv_solver* s, double* device_ms, int64_t* kernel_launches) {

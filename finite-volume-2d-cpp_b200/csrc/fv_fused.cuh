@@ -110,17 +110,17 @@ __host__ __device__ inline FusedSmem fused_smem(int max_slots, int max_grad, int
     return L;
 }
 
+// One tile t.  Returns false when the step is inactive (nothing written).
 template <class M, int FLUX>
-__device__ __forceinline__ void fused_stage(const FusedParams& FP, const TileIO& io) {
+__device__ __forceinline__ bool fused_tile(const FusedParams& FP, const TileIO& io, const int t) {
     using S = typename M::S;
     using FT = typename std::conditional<M::exact, double, S>::type;  // flux storage
     using PL = Planes<S>;
     constexpr int V = 4;
-    pdl_trigger();
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ unsigned long long s_dtkey;
     const Params& P = FP.P;
-    const int N = P.n_real, T = FP.T, t = blockIdx.x;
+    const int N = P.n_real, T = FP.T;
     const int4 ia = FP.info[2 * t], ib = FP.info[2 * t + 1];
     const int edge_off = ia.x, n_edges = ia.y, n_flux = ia.z, halo_off = ia.w;
     const int n1 = ib.x, n2 = ib.y, face_off = ib.z;
@@ -196,7 +196,7 @@ __device__ __forceinline__ void fused_stage(const FusedParams& FP, const TileIO&
         if (threadIdx.x == 0) s_dtkey = k;
     }
     cpa_wait();
-    if (inactive) return;
+    if (inactive) return false;
     __syncthreads();
 
     // ---- gradients and limiters of the owned cells and ring 1
@@ -503,15 +503,37 @@ __device__ __forceinline__ void fused_stage(const FusedParams& FP, const TileIO&
             for (int k = 0; k < V; ++k) {
                 double s = 0.;
                 for (int w = 0; w < nw; ++w) s += red[w * V + k];
-                io.partials[(size_t)blockIdx.x * V + k] = s;
+                io.partials[(size_t)t * V + k] = s;
             }
         }
     }
+    return true;
 }
 
+// One CTA per tile.
 template <class M, int FLUX>
 __global__ void __launch_bounds__(kTileMax) k_tile_fused(FusedParams FP, TileIO io) {
-    fused_stage<M, FLUX>(FP, io);
+    pdl_trigger();
+    fused_tile<M, FLUX>(FP, io, blockIdx.x);
+}
+
+// Work-list schedule: as many CTAs as fit on the device at once, each taking
+// the next tile from the launch's counter (reset by the step's dt kernel)
+// until none is left, so no CTA waits at a tail of unevenly sized tiles.
+// The counter is read only after the dependency wait.
+template <class M, int FLUX>
+__global__ void __launch_bounds__(kTileMax) k_tile_fused_work(FusedParams FP, TileIO io, int n_tiles) {
+    pdl_trigger();
+    pdl_wait();
+    __shared__ int s_t;
+    for (;;) {
+        if (threadIdx.x == 0) s_t = atomicAdd(io.work, 1);
+        __syncthreads();
+        const int t = s_t;
+        if (t >= n_tiles) return;
+        if (!fused_tile<M, FLUX>(FP, io, t)) return;
+        __syncthreads();  // every thread is done with this tile's shared memory (and s_t)
+    }
 }
 
 template <class M>
@@ -524,7 +546,8 @@ struct FusedLaunch {
         std::lock_guard<std::mutex> lock(mu);
         cudaError_t e = cudaSuccess;
         const size_t bytes = smem(FP);
-        for (const void* fn : {(const void*)k_tile_fused<M, 1>, (const void*)k_tile_fused<M, 2>}) {
+        for (const void* fn : {(const void*)k_tile_fused<M, 1>, (const void*)k_tile_fused<M, 2>,
+                               (const void*)k_tile_fused_work<M, 1>, (const void*)k_tile_fused_work<M, 2>}) {
             // only ever raised: a solver created earlier may launch with more
             cudaFuncAttributes fa{};
             if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, fn);
@@ -536,10 +559,19 @@ struct FusedLaunch {
         }
         return e;
     }
-    static void stage(const FusedParams& FP, const TileIO& io, cudaStream_t st, bool pdl, int n_tiles) {
+    // CTAs of the work-list schedule: the device's resident capacity
+    static int work_grid(const FusedParams& FP, int n_tiles) {
+        int dev = 0, sms = 0, nb = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_tile_fused_work<M, 1>, FP.T, smem(FP));
+        return std::max(1, std::min(n_tiles, sms * std::max(nb, 1)));
+    }
+    // io.work != nullptr: the work-list schedule on `grid` CTAs
+    static void stage(const FusedParams& FP, const TileIO& io, cudaStream_t st, bool pdl, int n_tiles, int grid) {
         const size_t sm = smem(FP);
         cudaLaunchConfig_t cfg = {};
-        cfg.gridDim = dim3((unsigned)n_tiles);
+        cfg.gridDim = dim3((unsigned)(io.work ? grid : n_tiles));
         cfg.blockDim = dim3((unsigned)FP.T);
         cfg.dynamicSmemBytes = sm;
         cfg.stream = st;
@@ -548,15 +580,22 @@ struct FusedLaunch {
         at[0].val.programmaticStreamSerializationAllowed = 1;
         cfg.attrs = at;
         cfg.numAttrs = pdl ? 1 : 0;
-        if (FP.P.flux == 1) cudaLaunchKernelEx(&cfg, k_tile_fused<M, 1>, FP, io);
-        else cudaLaunchKernelEx(&cfg, k_tile_fused<M, 2>, FP, io);
+        if (io.work) {
+            if (FP.P.flux == 1) cudaLaunchKernelEx(&cfg, k_tile_fused_work<M, 1>, FP, io, n_tiles);
+            else cudaLaunchKernelEx(&cfg, k_tile_fused_work<M, 2>, FP, io, n_tiles);
+        } else {
+            if (FP.P.flux == 1) cudaLaunchKernelEx(&cfg, k_tile_fused<M, 1>, FP, io);
+            else cudaLaunchKernelEx(&cfg, k_tile_fused<M, 2>, FP, io);
+        }
     }
 };
 
 namespace tile {
 cudaError_t prepare_fused(int precision, const FusedParams& FP);
 size_t smem_fused(int precision, const FusedParams& FP);
-void launch_fused(int precision, const FusedParams& FP, const TileIO& io, cudaStream_t st, bool pdl, int n_tiles);
+int work_grid_fused(int precision, const FusedParams& FP, int n_tiles);
+void launch_fused(int precision, const FusedParams& FP, const TileIO& io, cudaStream_t st, bool pdl, int n_tiles,
+                  int grid);
 }  // namespace tile
 
 }  // namespace fvgpu

@@ -72,7 +72,10 @@ struct TileIO {
     unsigned long long* dtkeys;  // [n_cases][kDtSlots] ordered keys of the global dt minimum
     int write_f64;             // FP32 mode: also write q_out (last stage)
     double* qt;                // [n_total][V] time derivatives of the smoothing phases (FP64)
+    int* work;                 // fused stage kernel, work-list schedule: this launch's tile counter
+    int* work_reset;           // dt kernel: tile counters zeroed after the dependency wait, or nullptr
 };
+constexpr int kWorkSlots = 8;  // tile counters of the work-list schedule (one per RK stage)
 
 __device__ __forceinline__ unsigned long long tkey(double x) {
     if (x != x) return ~0ull;
@@ -572,6 +575,9 @@ __global__ void __launch_bounds__(kTileMax) k_tile_dt(TileParams TP, TileIO io) 
     stage_edges<S, false, false>(TP, inf, sij, snx, sny, sle, nullptr, nullptr, nullptr);
     stage_halo(TP, inf, shalo);
     pdl_wait();
+    // the step's first kernel: the work-list tile counters of its stage
+    // kernels start at zero (every kernel that used them has completed)
+    if (io.work_reset != nullptr && blockIdx.x == 0 && threadIdx.x < kWorkSlots) io.work_reset[threadIdx.x] = 0;
     // the step-control flag is read while the records load; an inactive
     // step's kernels write nothing
     const bool inactive = t_inactive(io.ctrl);

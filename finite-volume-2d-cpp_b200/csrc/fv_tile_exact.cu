@@ -17,8 +17,9 @@ void launch_stage_exact(const TileParams& TP, const TileIO& io, cudaStream_t st,
 }
 cudaError_t prepare_fused_exact(const FusedParams& FP) { return FusedLaunch<MExact>::prepare(FP); }
 size_t smem_fused_exact(const FusedParams& FP) { return FusedLaunch<MExact>::smem(FP); }
-void launch_fused_exact(const FusedParams& FP, const TileIO& io, cudaStream_t st, bool pdl, int n_tiles) {
-    FusedLaunch<MExact>::stage(FP, io, st, pdl, n_tiles);
+int work_grid_fused_exact(const FusedParams& FP, int n_tiles) { return FusedLaunch<MExact>::work_grid(FP, n_tiles); }
+void launch_fused_exact(const FusedParams& FP, const TileIO& io, cudaStream_t st, bool pdl, int n_tiles, int grid) {
+    FusedLaunch<MExact>::stage(FP, io, st, pdl, n_tiles, grid);
 }
 }  // namespace tile
 }  // namespace fvgpu

@@ -11,7 +11,8 @@ void launch_gradlim_exact(const TileParams& TP, const TileIO& io, cudaStream_t s
 void launch_stage_exact(const TileParams& TP, const TileIO& io, cudaStream_t st, bool pdl, int phase);
 cudaError_t prepare_fused_exact(const FusedParams& FP);
 size_t smem_fused_exact(const FusedParams& FP);
-void launch_fused_exact(const FusedParams& FP, const TileIO& io, cudaStream_t st, bool pdl, int n_tiles);
+int work_grid_fused_exact(const FusedParams& FP, int n_tiles);
+void launch_fused_exact(const FusedParams& FP, const TileIO& io, cudaStream_t st, bool pdl, int n_tiles, int grid);
 
 cudaError_t prepare(int precision, const TileParams& TP) {
     if (precision == 0) return prepare_exact(TP);
@@ -43,10 +44,16 @@ size_t smem_fused(int precision, const FusedParams& FP) {
     if (precision == 1) return FusedLaunch<MF64>::smem(FP);
     return FusedLaunch<MF32>::smem(FP);
 }
-void launch_fused(int precision, const FusedParams& FP, const TileIO& io, cudaStream_t st, bool pdl, int n_tiles) {
-    if (precision == 0) launch_fused_exact(FP, io, st, pdl, n_tiles);
-    else if (precision == 1) FusedLaunch<MF64>::stage(FP, io, st, pdl, n_tiles);
-    else FusedLaunch<MF32>::stage(FP, io, st, pdl, n_tiles);
+int work_grid_fused(int precision, const FusedParams& FP, int n_tiles) {
+    if (precision == 0) return work_grid_fused_exact(FP, n_tiles);
+    if (precision == 1) return FusedLaunch<MF64>::work_grid(FP, n_tiles);
+    return FusedLaunch<MF32>::work_grid(FP, n_tiles);
+}
+void launch_fused(int precision, const FusedParams& FP, const TileIO& io, cudaStream_t st, bool pdl, int n_tiles,
+                  int grid) {
+    if (precision == 0) launch_fused_exact(FP, io, st, pdl, n_tiles, grid);
+    else if (precision == 1) FusedLaunch<MF64>::stage(FP, io, st, pdl, n_tiles, grid);
+    else FusedLaunch<MF32>::stage(FP, io, st, pdl, n_tiles, grid);
 }
 }  // namespace tile
 }  // namespace fvgpu

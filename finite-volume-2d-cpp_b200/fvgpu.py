@@ -217,17 +217,20 @@ class Solver:
 
     STAGE_KERNELS = {"auto": 0, "split": 1, "fused": 2}
 
+    SCHEDULES = {"tile": 0, "worklist": 1}
+
     def __init__(self, mesh: Mesh, ph: _phys.Physics, precision: str = "fp64_exact", device: int = 0,
-                 tile_cells: int = 0, stage_kernels: str = "auto"):
+                 tile_cells: int = 0, stage_kernels: str = "auto", schedule: str = "tile"):
         """stage_kernels: "auto" (the fused stage kernel where the physics
-        allow it), "split" (gradient and flux kernels) or "fused"."""
+        allow it), "split" (gradient and flux kernels) or "fused"; schedule of
+        the fused kernel: "tile" (one CTA per tile) or "worklist"."""
         self.mesh = mesh
         self.phys = ph
         self.V = ph.V
         self.precision = precision
         self._ps = physics_struct(ph, mesh.group_names)
         h = C.c_void_p()
-        opt = (C.c_int32 * 2)(int(tile_cells), self.STAGE_KERNELS[stage_kernels])
+        opt = (C.c_int32 * 3)(int(tile_cells), self.STAGE_KERNELS[stage_kernels], self.SCHEDULES[schedule])
         _check(lib().fv_solver_create_ex(mesh._h, C.byref(self._ps), C.c_int32(PREC[precision]), C.c_int32(device),
                                          opt, C.byref(h)))
         self._h = h
@@ -281,6 +284,11 @@ class Solver:
     def stage_kernels(self):
         """"fused" or "split": the stage kernels this solver runs."""
         return {2: "fused", 1: "split"}[lib().fv_solver_stage_kernels(self._h)]
+
+    @property
+    def schedule(self):
+        """"tile" or "worklist": the fused stage kernel's schedule."""
+        return {0: "tile", 1: "worklist"}[lib().fv_solver_schedule(self._h)]
 
     def close(self):
         if self._h:

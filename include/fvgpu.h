@@ -226,8 +226,14 @@ typedef struct {
      *   physics do not allow it.  All three give the same results (bit for bit
      *   in FP64_EXACT). */
     int32_t stage_kernels;
+    /* Schedule of the fused stage kernel: FV_SCHED_TILE (0) one CTA per
+     * tile; FV_SCHED_WORKLIST (1) as many CTAs as the device holds at once,
+     * each taking the next tile from a per-stage work list.  Ignored for the
+     * split kernels. */
+    int32_t schedule;
 } fv_solver_options;
 enum { FV_STAGE_AUTO = 0, FV_STAGE_SPLIT = 1, FV_STAGE_FUSED = 2 };
+enum { FV_SCHED_TILE = 0, FV_SCHED_WORKLIST = 1 };
 int fv_solver_create_ex(const fv_mesh* m, const fv_physics* ph, int32_t precision, int32_t device,
                         const fv_solver_options* opt, fv_solver** out);
 /* Autotuned creation: builds the solver with each tile size (64, 128, 256
@@ -235,10 +241,11 @@ int fv_solver_create_ex(const fv_mesh* m, const fv_physics* ph, int32_t precisio
  * stage kernel, with each edge-tile layout (split gradient and flux kernels
  * over one-ring tiles, or the fused kernel over two-ring tiles); times
  * n_steps steps of the given RK stages from state q on the device for each
- * candidate (after one untimed step that captures the step graph), and keeps
- * the fastest.  The returned solver holds state q again, step 0; tile_cells
- * and ms_per_step (may be NULL) report the choice, fv_solver_stage_kernels
- * the layout. */
+ * candidate (after one untimed step that captures the step graph), the
+ * fused kernel with both schedules, and keeps the fastest.  The returned
+ * solver holds state q again, step 0; tile_cells and ms_per_step (may be
+ * NULL) report the choice, fv_solver_stage_kernels and fv_solver_schedule
+ * the layout and schedule. */
 int fv_solver_create_tuned(const fv_mesh* m, const fv_physics* ph, int32_t precision, int32_t device,
                            const double* q, const double* alpha, int32_t n_alpha, int32_t n_steps,
                            fv_solver** out, int32_t* tile_cells, double* ms_per_step);
@@ -295,6 +302,8 @@ int fv_output_fields(fv_solver* s, const double* q, int64_t n, int32_t n_fields,
                      double* out);
 /* The stage kernels the solver runs: FV_STAGE_FUSED or FV_STAGE_SPLIT. */
 int fv_solver_stage_kernels(fv_solver* s);
+/* The fused kernel's schedule: FV_SCHED_TILE or FV_SCHED_WORKLIST. */
+int fv_solver_schedule(fv_solver* s);
 /* Device time of the last fv_run's chunks and per-kernel launch count. */
 int fv_last_run_stats(fv_solver* s, double* device_ms, int64_t* kernel_launches);
 

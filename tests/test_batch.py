@@ -79,17 +79,21 @@ def test_batch_equals_each_case_alone(tile_cells, oracle):
         g = m.geometry()
         q0s.append(P.ic_riemann(g["ccx"], st[:3], st[3:]).ravel())
     steps = 25
-    sb = fvgpu.Solver(b, ph, "fp64_exact", tile_cells=tile_cells)
-    sb.set_state(b.join(q0s, 4))
-    sb.run(steps, print_interval=10 ** 9)
-    got = b.split(sb.get_state(), 4)
-    times = sb.case_times()
-    for k, (em, q0) in enumerate(zip(ems, q0s)):
+    wants = []
+    for em, q0 in zip(ems, q0s):
         g = oracle.build_mesh(em)
-        want = oracle.run_loop(g, oracle.physics(ph, em.group_names), q0, P.RK5_ALPHA, steps)
-        assert bits_equal(got[k], want["q"]), k
-        assert times[k] == want["time"], k
-    sb.close()
+        wants.append(oracle.run_loop(g, oracle.physics(ph, em.group_names), q0, P.RK5_ALPHA, steps))
+    # the split kernels, and the fused kernel with both schedules
+    for sk, sched in (("split", "tile"), ("fused", "tile"), ("fused", "worklist")):
+        sb = fvgpu.Solver(b, ph, "fp64_exact", tile_cells=tile_cells, stage_kernels=sk, schedule=sched)
+        sb.set_state(b.join(q0s, 4))
+        sb.run(steps, print_interval=10 ** 9)
+        got = b.split(sb.get_state(), 4)
+        times = sb.case_times()
+        for k, want in enumerate(wants):
+            assert bits_equal(got[k], want["q"]), (sk, sched, k)
+            assert times[k] == want["time"], (sk, sched, k)
+        sb.close()
     # FP32-bulk: the batch equals the cases run alone in FP32
     s32 = fvgpu.Solver(b, ph, "fp32", tile_cells=tile_cells)
     s32.set_state(b.join(q0s, 4))

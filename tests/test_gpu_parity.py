@@ -330,9 +330,10 @@ FUSED_CASES = [n for n in sorted(CASES) if CASES[n]["phys"]().order2 and CASES[n
 @pytest.mark.parametrize("name", FUSED_CASES)
 def test_fused_and_split_stage_kernels_agree(name, precision, oracle):
     """The fused stage kernel (gradients, limiter and fluxes of a two-ring
-    tile in one launch) and the split gradient + flux kernels give the same
-    bits in every precision mode, and in FP64_EXACT both equal the oracle, at
-    every tile size."""
+    tile in one launch), with one CTA per tile and with the work-list
+    schedule, and the split gradient + flux kernels give the same bits in
+    every precision mode, and in FP64_EXACT all equal the oracle, at every
+    tile size."""
     case = CASES[name]
     em, ph = case["mesh"](), case["phys"]()
     mesh = fvgpu.Mesh.from_elements(em)
@@ -342,14 +343,14 @@ def test_fused_and_split_stage_kernels_agree(name, precision, oracle):
     want = oracle.run_loop(g, p, q0, case["alpha"], case["steps"]) if precision == "fp64_exact" else None
     out = {}
     for T in (64, 128, 256):
-        for sk in ("split", "fused"):
-            s = fvgpu.Solver(mesh, ph, precision, tile_cells=T, stage_kernels=sk)
-            assert s.stage_kernels == sk
+        for sk, sched in (("split", "tile"), ("fused", "tile"), ("fused", "worklist")):
+            s = fvgpu.Solver(mesh, ph, precision, tile_cells=T, stage_kernels=sk, schedule=sched)
+            assert s.stage_kernels == sk and s.schedule == sched
             s.set_state(q0)
             r = s.run(case["steps"], alpha=case["alpha"])
-            out[(T, sk)] = (s.get_state(), np.asarray(r["R"]), r["time"])
+            out[(T, sk, sched)] = (s.get_state(), np.asarray(r["R"]), r["time"])
             s.close()
-    ref = out[(128, "split")]
+    ref = out[(128, "split", "tile")]
     for k, v in out.items():
         assert bits_equal(v[0], ref[0]), k
         assert v[2] == ref[2], k
