@@ -90,8 +90,12 @@ def algo_bytes(ph, precision, kernel):
 # per precision mode), scaled by the cells of a launch; each entry names the
 # capture it comes from.  Modes and workloads without a capture report null.
 TRAFFIC_B_PER_CELL = {
-    ("step", "fp32"): (153.2, "ncu --set full -k regex:k_tile_stage -s 30 -c 2, "
-                              "bench.py --precision fp32 --steps 20 --warmup 3 --no-cpu-baseline"),
+    ("step", "fp32", "split"): (153.2, "ncu --set full -k regex:k_tile_stage -s 30 -c 2, "
+                                       "bench.py --precision fp32 --steps 20 --warmup 3 --no-cpu-baseline"),
+    ("step", "fp32", "fused"): (149.1, "ncu --set full -k regex:k_tile_fused -s 10 -c 2, bench.py --precision "
+                                       "fp32 --steps 20 --warmup 3 --no-cpu-baseline --batch-steps 0"),
+    ("step", "fp64", "fused"): (231.8, "ncu --set full -k regex:k_tile_fused -s 10 -c 2, bench.py --precision "
+                                       "fp64 --steps 20 --warmup 3 --no-cpu-baseline --batch-steps 0"),
 }
 
 
@@ -359,7 +363,7 @@ def measure_mode(args, em, mesh, geo, ph, alpha, ic, precision, local, dist, wor
                        "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind,
                        "traffic": None, "traffic_source": "no ncu capture of this mode and workload",
                        "algorithmic_bytes_per_launch": kb}
-    cap = TRAFFIC_B_PER_CELL.get((args.workload, precision))
+    cap = TRAFFIC_B_PER_CELL.get((args.workload, precision, "fused" if fused else "split"))
     if cap is not None:
         out["roofline"]["traffic"] = cap[0] * N
         out["roofline"]["traffic_source"] = ("dram__bytes_read.sum + dram__bytes_write.sum per launch of the "
