@@ -630,8 +630,9 @@ def main():
     ap.add_argument("--stage-kernels", default="auto", choices=["auto", "split", "fused"],
                     help="second-order Euler stage kernels: fused (one per stage) where the physics allow, "
                          "or split gradient and flux kernels")
-    ap.add_argument("--schedule", default="tile", choices=["tile", "worklist"],
-                    help="fused stage kernel: one CTA per tile, or resident CTAs taking tiles from a work list")
+    ap.add_argument("--schedule", default="tile", choices=["tile", "worklist", "tile2"],
+                    help="fused stage kernel: one CTA per tile, resident CTAs taking tiles from a work list, "
+                         "or one CTA of two threads per cell per tile")
     ap.add_argument("--batch-steps", type=int, default=500,
                     help="steps of the batched Riemann-strip workload reported beside the forward step "
                          "(0: not run)")

@@ -69,8 +69,9 @@ struct fv_solver {
     // the fused stage kernel over two-ring tiles (its Params are TP.P at launch)
     bool fused = false;
     FusedParams FPm{};
-    // its work-list schedule: per-stage tile counters, CTAs per launch
-    bool worklist = false;
+    // its schedule (FV_SCHED_*); the work list's per-stage tile counters and
+    // CTAs per launch
+    int sched = 0;
     int* work = nullptr;
     int work_grid = 0;
     // device buffers
@@ -536,14 +537,17 @@ int fv_solver_create_ex(const fv_mesh* fm, const fv_physics* ph, int32_t precisi
                     cca[4 * n] = ta.ccx[n]; cca[4 * n + 1] = ta.ccy[n]; cca[4 * n + 2] = fa.area[n];
                 }
                 if ((rc = upload_s(s.get(), cca, &F.cca))) return rc;
+                F.threads = tile_cells;
                 CK(tile::prepare_fused(precision, F));
                 s->fused = true;
                 CK(s->alloc(&s->work, kWorkSlots));
                 CK(cudaMemset(s->work, 0, kWorkSlots * sizeof(int)));
                 s->work_grid = tile::work_grid_fused(precision, F, ta.n_tiles);
                 const int sched = opt ? opt->schedule : FV_SCHED_TILE;
-                if (sched != FV_SCHED_TILE && sched != FV_SCHED_WORKLIST) return fail(FV_ERR_ARG, "unknown schedule");
-                s->worklist = sched == FV_SCHED_WORKLIST;
+                if (sched < FV_SCHED_TILE || sched > FV_SCHED_TILE2) return fail(FV_ERR_ARG, "unknown schedule");
+                if (sched == FV_SCHED_TILE2 && tile_cells > kTileMax / 2)
+                    return fail(FV_ERR_ARG, "two threads per cell need tiles of at most 128 cells");
+                s->sched = sched;
             }
         }
     }
@@ -645,11 +649,13 @@ int fv_solver_create_tuned(const fv_mesh* fm, const fv_physics* ph, int32_t prec
         if (rc == FV_ERR_MESH) continue;  // tile halo too large for this size
         if (rc) { fv_solver_destroy(best); return rc; }
         const bool can_fuse = s->fused;
-        double ms_of[3] = {1e300, 1e300, 1e300};  // split, fused one CTA per tile, fused work list
-        for (int variant = can_fuse ? 2 : 0; variant >= 0; --variant) {
+        // split; fused with FV_SCHED_TILE, FV_SCHED_WORKLIST, FV_SCHED_TILE2
+        double ms_of[4] = {1e300, 1e300, 1e300, 1e300};
+        const int top = can_fuse ? (t <= kTileMax / 2 ? 3 : 2) : 0;
+        for (int variant = top; variant >= 0; --variant) {
             clear_graphs(s);
             s->fused = variant >= 1;
-            s->worklist = variant == 2;
+            s->sched = variant >= 1 ? variant - 1 : FV_SCHED_TILE;
             // one untimed step (graph capture), then n_steps timed on the device
             fv_run_options ro{};
             ro.max_step = 1; ro.max_time = 1e300; ro.tolerance = -1.0; ro.print_interval = 1ull << 62;
@@ -660,11 +666,11 @@ int fv_solver_create_tuned(const fv_mesh* fm, const fv_physics* ph, int32_t prec
             if ((rc = fv_run(s, &ro, &info))) { fv_solver_destroy(s); fv_solver_destroy(best); return rc; }
             ms_of[variant] = s->last_ms / n_steps;
         }
-        const int v = (int)(std::min_element(ms_of, ms_of + 3) - ms_of);
+        const int v = (int)(std::min_element(ms_of, ms_of + 4) - ms_of);
         const double ms = ms_of[v];
         clear_graphs(s);
         s->fused = v >= 1;
-        s->worklist = v == 2;
+        s->sched = v >= 1 ? v - 1 : FV_SCHED_TILE;
         if (!best || ms < best_ms) {
             fv_solver_destroy(best);
             best = s; best_ms = ms; best_t = t;
@@ -861,7 +867,7 @@ static int enqueue_step(fv_solver* s, const std::vector<double>& alpha, int b, E
     // comes from the dt kernel, as in first order
     const bool grads = (TP.P.order2 || TP.P.diffusive) && !s->fused;
     // the work-list schedule: one tile counter per stage, zeroed by the dt kernel
-    const bool worklist = s->fused && s->worklist && alpha.size() <= (size_t)kWorkSlots;
+    const bool worklist = s->fused && s->sched == FV_SCHED_WORKLIST && alpha.size() <= (size_t)kWorkSlots;
     if (!grads) {
         TileIO dio = io;
         dio.work_reset = worklist ? s->work : nullptr;
@@ -869,6 +875,7 @@ static int enqueue_step(fv_solver* s, const std::vector<double>& alpha, int b, E
     }
     FusedParams FPl = s->FPm;
     FPl.P = TP.P;
+    FPl.threads = (s->sched == FV_SCHED_TILE2) ? 2 * FPl.T : FPl.T;
     const int ns = (int)alpha.size();
     const void* in = s->sbase[b];
     for (int k = 0; k < ns; ++k) {
@@ -1077,7 +1084,7 @@ int fv_solver_stage_kernels(fv_solver* s) {
 
 int fv_solver_schedule(fv_solver* s) {
     if (!s) return fail(FV_ERR_ARG, "null solver");
-    return (s->fused && s->worklist) ? FV_SCHED_WORKLIST : FV_SCHED_TILE;
+    return s->fused ? s->sched : FV_SCHED_TILE;
 }
 
 int fv_last_run_stats(fv_solver* s, double* device_ms, int64_t* kernel_launches) {

@@ -27,6 +27,7 @@ namespace fvgpu {
 struct FusedParams {
     Params P;
     int T;
+    int threads;               // threads per CTA: T, or 2T (at most kTileMax)
     int max_slots, max_grad, max_edges, max_flux;  // max_edges rounded up to a multiple of 4
     const int4* info;          // [n_tiles][2]: {edge_off, n_edges, n_flux, halo_off}, {n1, n2, face_off, 0}
     const int32_t* halo;       // device cell of each ring-1, then ring-2 slot
@@ -77,12 +78,21 @@ struct Planes<double> {
 };
 
 // Shared-memory layout of one fused tile, in bytes from the start.
+//  - state planes [max_slots];
+//  - centroids [max_grad]: FP32 one float4 plane (x, y, area, 0); FP64 one
+//    double2 plane (x, y) and the ring-1 areas [max_grad - T] (an owned
+//    cell's area is held by its thread);
+//  - gradient planes [max_grad] (and the limiter in the exact policy);
+//  - edge indices and normal, length, face centre [max_edges];
+//  - the flux store, which before the flux phase holds the Green-Gauss
+//    weights [max_edges] (gradient phase) and the halo indices (staging), and
+//    after the per-cell sums the residual warp sums.
 struct FusedSmem {
-    size_t q, c, gx, gy, lm, ij, geo, flux, total;
+    size_t q, c, ar, gx, gy, lm, ij, geo, flux, halo, total;
     int ls, lg, em;  // plane strides (units) and edge-array length
 };
 template <class M>
-__host__ __device__ inline FusedSmem fused_smem(int max_slots, int max_grad, int max_edges, int max_flux) {
+__host__ __device__ inline FusedSmem fused_smem(int max_slots, int max_grad, int max_edges, int max_flux, int T) {
     using S = typename M::S;
     using FT = typename std::conditional<M::exact, double, S>::type;
     constexpr int NU = (int)(4 * sizeof(S) / 16);
@@ -92,22 +102,35 @@ __host__ __device__ inline FusedSmem fused_smem(int max_slots, int max_grad, int
     L.em = max_edges;
     size_t o = 0;
     L.q = o; o += (size_t)16 * NU * max_slots;
-    L.c = o; o += (size_t)16 * NU * max_grad;
+    L.c = o; o += (size_t)16 * max_grad;
+    L.ar = o; if (sizeof(S) == 8) o += ((size_t)8 * (max_grad - T) + 15) / 16 * 16;
     L.gx = o; o += (size_t)16 * NU * max_grad;
     L.gy = o; o += (size_t)16 * NU * max_grad;
     L.lm = o; if (M::exact) o += (size_t)16 * NU * max_grad;
     L.ij = o; o += (size_t)4 * max_edges;
-    L.geo = o; o += (size_t)6 * sizeof(S) * max_edges;
+    L.geo = o; o += (size_t)5 * sizeof(S) * max_edges;
     o = (o + 15) / 16 * 16;
     L.flux = o;
-    // the flux store also holds the halo indices (staging) and the warp sums
-    // of the residual partials (after the per-cell sums)
+    L.halo = L.flux + ((size_t)sizeof(S) * max_edges + 15) / 16 * 16;
     size_t fb = (size_t)max_flux * 4 * sizeof(FT);
-    fb = fb > (size_t)(max_slots) * 4 ? fb : (size_t)max_slots * 4;
+    const size_t before = (L.halo - L.flux) + (size_t)max_slots * 4;
+    fb = fb > before ? fb : before;
     fb = fb > (size_t)(kTileMax / 32) * 4 * sizeof(double) ? fb : (size_t)(kTileMax / 32) * 4 * sizeof(double);
     o += (fb + 15) / 16 * 16;
     L.total = o;
     return L;
+}
+
+// centroid (x, y) of slot r
+template <class S>
+__device__ __forceinline__ void cent(const uint4* C, int r, S& x, S& y) {
+    if constexpr (sizeof(S) == 4) {
+        const float4 v = reinterpret_cast<const float4*>(C)[r];
+        x = v.x; y = v.y;
+    } else {
+        const double2 v = reinterpret_cast<const double2*>(C)[r];
+        x = v.x; y = v.y;
+    }
 }
 
 // One tile t.  Returns false when the step is inactive (nothing written).
@@ -125,19 +148,21 @@ __device__ __forceinline__ bool fused_tile(const FusedParams& FP, const TileIO& 
     const int edge_off = ia.x, n_edges = ia.y, n_flux = ia.z, halo_off = ia.w;
     const int n1 = ib.x, n2 = ib.y, face_off = ib.z;
     const int c0 = t * T, nown = min(T, N - c0);
-    const FusedSmem L = fused_smem<M>(FP.max_slots, FP.max_grad, FP.max_edges, FP.max_flux);
+    const FusedSmem L = fused_smem<M>(FP.max_slots, FP.max_grad, FP.max_edges, FP.max_flux, FP.T);
     uint4* Q = reinterpret_cast<uint4*>(smem_raw + L.q);
     uint4* C = reinterpret_cast<uint4*>(smem_raw + L.c);
+    S* AR = reinterpret_cast<S*>(smem_raw + L.ar);  // FP64: ring-1 areas
     uint4* GX = reinterpret_cast<uint4*>(smem_raw + L.gx);
     uint4* GY = reinterpret_cast<uint4*>(smem_raw + L.gy);
     uint4* LM = reinterpret_cast<uint4*>(smem_raw + L.lm);
     uint32_t* sij = reinterpret_cast<uint32_t*>(smem_raw + L.ij);
     S* snx = reinterpret_cast<S*>(smem_raw + L.geo);
-    S* sny = snx + L.em; S* sle = sny + L.em; S* sxf = sle + L.em; S* syf = sxf + L.em; S* sg = syf + L.em;
+    S* sny = snx + L.em; S* sle = sny + L.em; S* sxf = sle + L.em; S* syf = sxf + L.em;
     FT* sF = reinterpret_cast<FT*>(smem_raw + L.flux);
-    // the halo indices are read only while the records are staged, before the
-    // first flux is stored: they share the flux store
-    int* shalo = reinterpret_cast<int*>(sF);
+    // the Green-Gauss weights (gradient phase) and the halo indices (staging)
+    // are dead before the first flux is stored: they share the flux store
+    S* sg = reinterpret_cast<S*>(smem_raw + L.flux);
+    int* shalo = reinterpret_cast<int*>(smem_raw + L.halo);
     const bool global_dt = io.ctrl != nullptr && P.global_dt;
     const int l = threadIdx.x;
     const int c = c0 + l;
@@ -159,12 +184,20 @@ __device__ __forceinline__ bool fused_tile(const FusedParams& FP, const TileIO& 
             cpa16(sg + d, (const S*)FP.eg + g);
         }
         for (int h = l; h < n1 + n2; h += blockDim.x) cpa4(shalo + h, FP.halo + halo_off + h);
-        for (int r = l; r < nown; r += blockDim.x) PL::stage(C, L.lg, r, (const S*)FP.cca + 4 * (size_t)(c0 + r));
+        for (int r = l; r < nown; r += blockDim.x) cpa16(C + r, (const S*)FP.cca + 4 * (size_t)(c0 + r));
         cpa_commit();
     }
-    uint2 fw0 = make_uint2(0xFFFFFFFFu, 0xFFFFFFFFu), fw1 = fw0;
-    if (l < nown) fw0 = FP.face[face_off + l];
-    if (l < n1) fw1 = FP.face[face_off + T + l];
+    // the owned cell's area (this thread's gradient slot and update)
+    const S A_own = l < nown ? ((const S*)FP.cca)[4 * (size_t)c + 2] : S(1);
+    // face words of this thread's gradient slots: slot l (pass 0) and slot
+    // l + blockDim.x (pass 1); slots [0, nown) are owned, [T, T + n1) ring 1
+    const uint2 kNoWords = make_uint2(0xFFFFFFFFu, 0xFFFFFFFFu);
+    auto slot_words = [&](int r) {
+        const bool has = r < T ? r < nown : r - T < n1;
+        return has ? FP.face[face_off + r] : kNoWords;
+    };
+    const uint2 fw0 = slot_words(l);
+    const uint2 fw1 = slot_words(l + blockDim.x);
     // the tile's case (batches); -1: the tile spans two cases
     const int tc = (global_dt && P.n_cases > 1) ? P.tile_case[t] : 0;
     // reference cell 0 of the tile's case, whose dt carries the NaN rule of min_dt
@@ -186,7 +219,10 @@ __device__ __forceinline__ bool fused_tile(const FusedParams& FP, const TileIO& 
     for (int h = l; h < n1 + n2; h += blockDim.x) {
         const int g = shalo[h];
         PL::stage(Q, L.ls, T + h, (const S*)io.q_stage + 4 * (size_t)g);
-        if (h < n1) PL::stage(C, L.lg, T + h, (const S*)FP.cca + 4 * (size_t)g);
+        if (h < n1) {
+            cpa16(C + T + h, (const S*)FP.cca + 4 * (size_t)g);
+            if constexpr (sizeof(S) == 8) cpa8(AR + h, (const S*)FP.cca + 4 * (size_t)g + 2);
+        }
     }
     if (global_dt && tc >= 0 && threadIdx.x < 32) {
         const unsigned long long* keys = io.dtkeys + (size_t)tc * kDtSlots;
@@ -203,15 +239,20 @@ __device__ __forceinline__ bool fused_tile(const FusedParams& FP, const TileIO& 
     // (calc_gradients + calc_limiters, explicit.cpp:112-258)
     for (int r = l, pass = 0; r < T + n1; r += blockDim.x, ++pass) {
         if (r < T && r >= nown) continue;
-        // blocks have T threads: pass 0 is the owned cell l, pass 1 ring-1 slot l
         const uint2 fwv = pass == 0 ? fw0 : (pass == 1 ? fw1 : FP.face[face_off + r]);
         uint16_t w[kMaxFaces];
         w[0] = (uint16_t)(fwv.x & 0xFFFF); w[1] = (uint16_t)(fwv.x >> 16);
         w[2] = (uint16_t)(fwv.y & 0xFFFF); w[3] = (uint16_t)(fwv.y >> 16);
-        S qs[V], cr[4], gx[V], gy[V], qmn[V], qmx[V], lim[V];
+        S qs[V], gx[V], gy[V], qmn[V], qmx[V], lim[V];
         PL::get(Q, L.ls, r, qs);
-        PL::get(C, L.lg, r, cr);
-        const S xc = cr[0], yc = cr[1], A = cr[2];
+        S xc, yc, A;
+        if constexpr (sizeof(S) == 4) {
+            const float4 cv = reinterpret_cast<const float4*>(C)[r];
+            xc = cv.x; yc = cv.y; A = cv.z;
+        } else {
+            cent<S>(C, r, xc, yc);
+            A = r < T ? A_own : AR[r - T];
+        }
 #pragma unroll
         for (int k = 0; k < V; ++k) { gx[k] = 0; gy[k] = 0; qmn[k] = qs[k]; qmx[k] = qs[k]; lim[k] = 1; }
 #pragma unroll
@@ -327,11 +368,11 @@ __device__ __forceinline__ bool fused_tile(const FusedParams& FP, const TileIO& 
         const int li = (int)(ij & 0xffff), lj = (int)(ij >> 16);
         const S n0 = snx[el], n1v = sny[el];
         FT f[V];
-        S qL[V], qR[V], ci[V], cj[V], gxi[V], gyi[V], gxj[V], gyj[V], pi[4], pj[4];
+        S qL[V], qR[V], ci[V], cj[V], gxi[V], gyi[V], gxj[V], gyj[V], pi[2], pj[2];
         PL::get(Q, L.ls, li, ci);
         PL::get(Q, L.ls, lj, cj);
-        PL::get(C, L.lg, li, pi);
-        PL::get(C, L.lg, lj, pj);
+        cent<S>(C, li, pi[0], pi[1]);
+        cent<S>(C, lj, pj[0], pj[1]);
         PL::get(GX, L.lg, li, gxi); PL::get(GY, L.lg, li, gyi);
         PL::get(GX, L.lg, lj, gxj); PL::get(GY, L.lg, lj, gyj);
         const S xf = sxf[el], yf = syf[el];
@@ -376,13 +417,13 @@ __device__ __forceinline__ bool fused_tile(const FusedParams& FP, const TileIO& 
     double res[V];
 #pragma unroll
     for (int k = 0; k < V; ++k) res[k] = 0.;
-    if (l < nown) {
+    if (l < nown) {  // fw0 holds the owned cell's faces (slot l < T)
         uint16_t w[kMaxFaces];
         w[0] = (uint16_t)(fw0.x & 0xFFFF); w[1] = (uint16_t)(fw0.x >> 16);
         w[2] = (uint16_t)(fw0.y & 0xFFFF); w[3] = (uint16_t)(fw0.y >> 16);
-        S cr[4];
-        PL::get(C, L.lg, l, cr);
-        const double A = (double)cr[2];
+        S cr[2];
+        cent<S>(C, l, cr[0], cr[1]);
+        const double A = (double)A_own;
         double qt[V];
 #pragma unroll
         for (int k = 0; k < V; ++k) qt[k] = 0.;
@@ -539,7 +580,7 @@ __global__ void __launch_bounds__(kTileMax) k_tile_fused_work(FusedParams FP, Ti
 template <class M>
 struct FusedLaunch {
     static size_t smem(const FusedParams& FP) {
-        return fused_smem<M>(FP.max_slots, FP.max_grad, FP.max_edges, FP.max_flux).total;
+        return fused_smem<M>(FP.max_slots, FP.max_grad, FP.max_edges, FP.max_flux, FP.T).total;
     }
     static cudaError_t prepare(const FusedParams& FP) {
         static std::mutex mu;
@@ -564,7 +605,7 @@ struct FusedLaunch {
         int dev = 0, sms = 0, nb = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_tile_fused_work<M, 1>, FP.T, smem(FP));
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_tile_fused_work<M, 1>, FP.threads, smem(FP));
         return std::max(1, std::min(n_tiles, sms * std::max(nb, 1)));
     }
     // io.work != nullptr: the work-list schedule on `grid` CTAs
@@ -572,7 +613,7 @@ struct FusedLaunch {
         const size_t sm = smem(FP);
         cudaLaunchConfig_t cfg = {};
         cfg.gridDim = dim3((unsigned)(io.work ? grid : n_tiles));
-        cfg.blockDim = dim3((unsigned)FP.T);
+        cfg.blockDim = dim3((unsigned)FP.threads);
         cfg.dynamicSmemBytes = sm;
         cfg.stream = st;
         cudaLaunchAttribute at[1];

@@ -217,13 +217,14 @@ class Solver:
 
     STAGE_KERNELS = {"auto": 0, "split": 1, "fused": 2}
 
-    SCHEDULES = {"tile": 0, "worklist": 1}
+    SCHEDULES = {"tile": 0, "worklist": 1, "tile2": 2}
 
     def __init__(self, mesh: Mesh, ph: _phys.Physics, precision: str = "fp64_exact", device: int = 0,
                  tile_cells: int = 0, stage_kernels: str = "auto", schedule: str = "tile"):
         """stage_kernels: "auto" (the fused stage kernel where the physics
         allow it), "split" (gradient and flux kernels) or "fused"; schedule of
-        the fused kernel: "tile" (one CTA per tile) or "worklist"."""
+        the fused kernel: "tile" (one CTA per tile), "worklist" or "tile2"
+        (one CTA of two threads per cell per tile)."""
         self.mesh = mesh
         self.phys = ph
         self.V = ph.V
@@ -287,8 +288,8 @@ class Solver:
 
     @property
     def schedule(self):
-        """"tile" or "worklist": the fused stage kernel's schedule."""
-        return {0: "tile", 1: "worklist"}[lib().fv_solver_schedule(self._h)]
+        """"tile", "worklist" or "tile2": the fused stage kernel's schedule."""
+        return {0: "tile", 1: "worklist", 2: "tile2"}[lib().fv_solver_schedule(self._h)]
 
     def close(self):
         if self._h:

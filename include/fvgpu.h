@@ -226,14 +226,16 @@ typedef struct {
      *   physics do not allow it.  All three give the same results (bit for bit
      *   in FP64_EXACT). */
     int32_t stage_kernels;
-    /* Schedule of the fused stage kernel: FV_SCHED_TILE (0) one CTA per
-     * tile; FV_SCHED_WORKLIST (1) as many CTAs as the device holds at once,
-     * each taking the next tile from a per-stage work list.  Ignored for the
-     * split kernels. */
+    /* Schedule of the fused stage kernel: FV_SCHED_TILE (0) one CTA of one
+     * thread per cell per tile; FV_SCHED_WORKLIST (1) as many CTAs as the
+     * device holds at once, each taking the next tile from a per-stage work
+     * list; FV_SCHED_TILE2 (2) one CTA of two threads per cell per tile
+     * (tiles of at most 128 cells), so the gradient and flux phases of a
+     * tile run in one pass.  Ignored for the split kernels. */
     int32_t schedule;
 } fv_solver_options;
 enum { FV_STAGE_AUTO = 0, FV_STAGE_SPLIT = 1, FV_STAGE_FUSED = 2 };
-enum { FV_SCHED_TILE = 0, FV_SCHED_WORKLIST = 1 };
+enum { FV_SCHED_TILE = 0, FV_SCHED_WORKLIST = 1, FV_SCHED_TILE2 = 2 };
 int fv_solver_create_ex(const fv_mesh* m, const fv_physics* ph, int32_t precision, int32_t device,
                         const fv_solver_options* opt, fv_solver** out);
 /* Autotuned creation: builds the solver with each tile size (64, 128, 256
@@ -302,7 +304,7 @@ int fv_output_fields(fv_solver* s, const double* q, int64_t n, int32_t n_fields,
                      double* out);
 /* The stage kernels the solver runs: FV_STAGE_FUSED or FV_STAGE_SPLIT. */
 int fv_solver_stage_kernels(fv_solver* s);
-/* The fused kernel's schedule: FV_SCHED_TILE or FV_SCHED_WORKLIST. */
+/* The fused kernel's schedule: FV_SCHED_TILE, FV_SCHED_WORKLIST or FV_SCHED_TILE2. */
 int fv_solver_schedule(fv_solver* s);
 /* Device time of the last fv_run's chunks and per-kernel launch count. */
 int fv_last_run_stats(fv_solver* s, double* device_ms, int64_t* kernel_launches);
