@@ -1,10 +1,13 @@
 // Discrete adjoint kernels of the explicit step (FP64, Euler, V = 4).
 //
 // Each kernel owns the cells it writes (one thread per real cell, which also
-// owns its boundary ghosts) and gathers what flows into them, so results do
-// not depend on scheduling.  Element Jacobians come from the primal element
-// functions of fv_physics_exact.cuh evaluated on Dual<4> numbers seeded on
-// one stencil cell's 4 conserved variables (fv_dual.cuh); the linear parts
+// owns its boundary ghosts; the gradient kernel one thread per real cell and
+// variable) and gathers what flows into them, so results do not depend on
+// scheduling.  Element Jacobians come from the primal element functions of
+// fv_physics_exact.cuh evaluated on dual numbers (fv_dual.cuh): Dual<4>
+// seeded on one stencil cell's 4 conserved variables for the flux, boundary
+// and time-step functions, a scalar dual seeded on one variable for the
+// gradient + limiter, which is block-diagonal over the variables; the linear parts
 // (MUSCL reconstruction, RK update, Green-Gauss sums) are differentiated by
 // hand.  Reference arithmetic followed: gradients explicit.cpp:112-171,
 // limiters 174-258, MUSCL + flux 261-364, update 368-378, ghost fill
@@ -20,6 +23,7 @@ namespace fvgpu {
 namespace {
 
 using D4 = Dual<4>;
+using D1 = Dual<1>;
 constexpr int kAB = 128;  // threads per block
 constexpr int kFaces = 4;
 constexpr uint32_t kNone = 0xFFFFFFFFu;
@@ -94,43 +98,39 @@ __device__ __forceinline__ T limiter_t(int kind, const T& y) {
     return T(0.);
 }
 
-// Gradients + limiter of real cell c (calc_gradients + calc_limiters), with
-// the state of one stencil cell seeded: seed_slot = -1 seeds cell c itself,
-// else the neighbour in face slot seed_slot.
-__device__ void gradlim_d(const Params& P, const AdjFaces& F, const double* __restrict__ qs, int c, int seed_slot,
-                          D4* gx, D4* gy, D4* lim) {
+// Gradient + limiter of variable k of real cell c: the operator is
+// block-diagonal over the conserved variables (variable k's Green-Gauss
+// gradient, min/max and limiter read only variable k of the stencil), so one
+// scalar dual seeded on variable k of one stencil cell gives the nonzero
+// entries of the cell's Jacobian block (calc_gradients + calc_limiters,
+// explicit.cpp:112-258).
+__device__ void gradlim_d1(const Params& P, const AdjFaces& F, const double* __restrict__ qs, int c, int seed_slot,
+                           int k, D1& gx, D1& gy, D1& lim) {
     const int N = P.n_real;
-    double v[4];
-    D4 q[4], qmn[4], qmx[4];
-    ld4(qs, c, v);
-    if (seed_slot < 0) seed(q, v); else constant(q, v);
-#pragma unroll
-    for (int k = 0; k < 4; ++k) { gx[k] = D4(0.0); gy[k] = D4(0.0); qmn[k] = q[k]; qmx[k] = q[k]; }
+    D1 q(qs[4 * (size_t)c + k]);
+    if (seed_slot < 0) q.d[0] = 1.0;
+    gx = D1(0.0); gy = D1(0.0);
+    D1 qmn = q, qmx = q;
     for (int f = 0; f < kFaces; ++f) {
         const size_t s = (size_t)f * N + c;
         const uint32_t w = F.nbr[s];
         if (w == kNone) continue;
         const int j = (int)(w & 0x7FFFFFFFu), side = (int)(w >> 31);
         const double nx = F.nx[s], ny = F.ny[s], le = F.le[s], g = F.g[s];
-        D4 qn[4];
-        ld4(qs, j, v);
-        if (f == seed_slot) seed(qn, v); else constant(qn, v);
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            if (!side) {
-                const D4 fl = (q[k] * (1.0 - g) + qn[k] * g) * le;
-                gx[k] += fl * nx; gy[k] += fl * ny;
-            } else {
-                const D4 fl = (qn[k] * (1.0 - g) + q[k] * g) * le;
-                gx[k] -= fl * nx; gy[k] -= fl * ny;
-            }
-            qmn[k] = dmin(qmn[k], qn[k]); qmx[k] = dmax(qmx[k], qn[k]);
+        D1 qn(qs[4 * (size_t)j + k]);
+        if (f == seed_slot) qn.d[0] = 1.0;
+        if (!side) {
+            const D1 fl = (q * (1.0 - g) + qn * g) * le;
+            gx += fl * nx; gy += fl * ny;
+        } else {
+            const D1 fl = (qn * (1.0 - g) + q * g) * le;
+            gx -= fl * nx; gy -= fl * ny;
         }
+        qmn = dmin(qmn, qn); qmx = dmax(qmx, qn);
     }
     const double A = F.area[c];
     const double invA = 1. / A;
-#pragma unroll
-    for (int k = 0; k < 4; ++k) { gx[k] *= invA; gy[k] *= invA; lim[k] = D4(1.0); }
+    gx *= invA; gy *= invA; lim = D1(1.0);
     const double Ka = P.K * sqrt(A);
     const double K3a = Ka * Ka * Ka;
     const double tol = 1e-15;
@@ -138,26 +138,23 @@ __device__ void gradlim_d(const Params& P, const AdjFaces& F, const double* __re
         const size_t s = (size_t)f * N + c;
         if (F.nbr[s] == kNone) continue;
         const double dx = F.dsx[s], dy = F.dsy[s];
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            const D4 dqg = gx[k] * dx + gy[k] * dy;
-            const D4 delta_max = qmx[k] - q[k];
-            const D4 delta_min = qmn[k] - q[k];
-            const D4 d2 = (delta_max - delta_min) * (delta_max - delta_min);
-            D4 sig;
-            if (d2 <= K3a) sig = D4(1.);
-            else if (d2 <= 2 * K3a) {
-                const D4 y = (d2 / K3a - 1.0);
-                sig = 2.0 * y * y * y - 3.0 * y * y + 1.0;
-            } else sig = D4(0.);
-            D4 lv(1.0);
-            if (sig < 1.0) {
-                if (dqg > tol) lv = limiter_t(P.limiter, delta_max / dqg);
-                else if (dqg < -tol) lv = limiter_t(P.limiter, delta_min / dqg);
-            }
-            lv = sig + (1.0 - sig) * lv;
-            lim[k] = dmin(lim[k], lv);
+        const D1 dqg = gx * dx + gy * dy;
+        const D1 delta_max = qmx - q;
+        const D1 delta_min = qmn - q;
+        const D1 d2 = (delta_max - delta_min) * (delta_max - delta_min);
+        D1 sig;
+        if (d2 <= K3a) sig = D1(1.);
+        else if (d2 <= 2 * K3a) {
+            const D1 y = (d2 / K3a - 1.0);
+            sig = 2.0 * y * y * y - 3.0 * y * y + 1.0;
+        } else sig = D1(0.);
+        D1 lv(1.0);
+        if (sig < 1.0) {
+            if (dqg > tol) lv = limiter_t(P.limiter, delta_max / dqg);
+            else if (dqg < -tol) lv = limiter_t(P.limiter, delta_min / dqg);
         }
+        lv = sig + (1.0 - sig) * lv;
+        lim = dmin(lim, lv);
     }
 }
 
@@ -310,25 +307,21 @@ __global__ void __launch_bounds__(kAB) k_adj_residual(Params P, AdjFaces F, AdjS
     }
 }
 
-__global__ void __launch_bounds__(kAB) k_adj_gradlim(Params P, AdjFaces F, AdjStage S) {
-    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+// lam_cur += (d g_k / d qs_k)^T lam_g, one thread per (real cell, variable):
+// variable k of cell m gathers from its own gradient and limiter and from
+// those of its face neighbours (scalar duals, gradlim_d1).
+__global__ void __launch_bounds__(kAB) k_adj_gradlim1(Params P, AdjFaces F, AdjStage S) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
     const int N = P.n_real;
+    const int m = t >> 2, k = t & 3;
     if (m >= N) return;
-    double acc[4] = {0, 0, 0, 0};
-    D4 gx[4], gy[4], lim[4];
-    auto contribute = [&](int c, int seed_slot, double* out) {
-        gradlim_d(P, F, S.qs, c, seed_slot, gx, gy, lim);
-        double lgx[4], lgy[4], llim[4];
-        ld4(S.lam_gx, c, lgx); ld4(S.lam_gy, c, lgy); ld4(S.lam_lim, c, llim);
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            double s = 0.0;
-#pragma unroll
-            for (int k = 0; k < 4; ++k) s += lgx[k] * gx[k].d[q] + lgy[k] * gy[k].d[q] + llim[k] * lim[k].d[q];
-            out[q] += s;
-        }
+    D1 gx, gy, lim;
+    auto contribute = [&](int c, int seed_slot) {
+        gradlim_d1(P, F, S.qs, c, seed_slot, k, gx, gy, lim);
+        const size_t i = 4 * (size_t)c + k;
+        return S.lam_gx[i] * gx.d[0] + S.lam_gy[i] * gy.d[0] + S.lam_lim[i] * lim.d[0];
     };
-    contribute(m, -1, acc);
+    double acc = contribute(m, -1);
     for (int f = 0; f < kFaces; ++f) {
         const uint32_t w = F.nbr[(size_t)f * N + m];
         if (w == kNone) continue;
@@ -337,16 +330,14 @@ __global__ void __launch_bounds__(kAB) k_adj_gradlim(Params P, AdjFaces F, AdjSt
             // m in the stencil of its neighbour c: find m's slot among c's faces
             for (int h = 0; h < kFaces; ++h) {
                 const uint32_t wc = F.nbr[(size_t)h * N + c];
-                if (wc != kNone && (int)(wc & 0x7FFFFFFFu) == m) { contribute(c, h, acc); break; }
+                if (wc != kNone && (int)(wc & 0x7FFFFFFFu) == m) { acc += contribute(c, h); break; }
             }
         } else {
             // ghost neighbour: only this cell's gradients and limiter use it
-            double lg[4] = {0, 0, 0, 0};
-            contribute(m, f, lg);
-            add4(S.lam_cur, c, lg);
+            S.lam_cur[4 * (size_t)c + k] += contribute(m, f);
         }
     }
-    add4(S.lam_cur, m, acc);
+    S.lam_cur[4 * (size_t)m + k] += acc;
 }
 
 __global__ void k_add(double* y, const double* x, size_t n) {
@@ -354,10 +345,22 @@ __global__ void k_add(double* y, const double* x, size_t n) {
         y[i] += x[i];
 }
 
-__global__ void k_sum(const double* p, int n, double* out) {
+// out = sum of p[0..n) in a fixed order: each of the block's threads sums a
+// contiguous run, then a fixed tree over the threads.
+constexpr int kSumThreads = 256;
+__global__ void __launch_bounds__(kSumThreads) k_sum(const double* p, int n, double* out) {
+    __shared__ double red[kSumThreads];
+    const int per = (n + kSumThreads - 1) / kSumThreads;
+    const int a = threadIdx.x * per, b = min(n, a + per);
     double s = 0.0;
-    for (int i = 0; i < n; ++i) s += p[i];
-    *out = s;
+    for (int i = a; i < b; ++i) s += p[i];
+    red[threadIdx.x] = s;
+    __syncthreads();
+    for (int w = kSumThreads / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *out = red[0];
 }
 
 __device__ __forceinline__ double key_inv(unsigned long long k) {
@@ -498,14 +501,14 @@ void adj_launch_residual(const Params& P, const AdjFaces& F, const AdjStage& S, 
     k_adj_residual<<<blocks_for(P.n_real), kAB, 0, st>>>(P, F, S);
 }
 void adj_launch_gradlim(const Params& P, const AdjFaces& F, const AdjStage& S, cudaStream_t st) {
-    k_adj_gradlim<<<blocks_for(P.n_real), kAB, 0, st>>>(P, F, S);
+    k_adj_gradlim1<<<blocks_for(4 * P.n_real), kAB, 0, st>>>(P, F, S);
 }
 void adj_launch_add(double* y, const double* x, size_t n, cudaStream_t st) {
     const int b = (int)std::min<size_t>((n + 255) / 256, 148 * 16);
     k_add<<<b > 0 ? b : 1, 256, 0, st>>>(y, x, n);
 }
 void adj_launch_sum(const double* partials, int n, double* out, cudaStream_t st) {
-    k_sum<<<1, 1, 0, st>>>(partials, n, out);
+    k_sum<<<1, kSumThreads, 0, st>>>(partials, n, out);
 }
 void adj_launch_dt_finalize(const unsigned long long* keys, const double* dt_cells, int cell0, double* dt_fill, int n,
                             double* dt_out, cudaStream_t st) {
