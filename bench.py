@@ -293,7 +293,13 @@ def run_reference_arm(args):
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": desc, "n_real_cells": n, "parallelism": f"{procs} host processes"},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": procs, "kind": "reference", "sample": sample},
-            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "same_config": False,
+            "comparability": ("the same mesh, physics and metric as the GPU arm (cell-updates per RK stage), but "
+                              "each timed step is one single-stage step of the reference's stage functions, so "
+                              "calc_dt runs once per stage instead of once per 5-stage step (1-2 % of its time); "
+                              "the reference scheme has no positivity guard; the processes are independent "
+                              "replicas (an upper bound of MPI scaling on these cores)")}
     print(json.dumps(line))
 
 
@@ -671,6 +677,8 @@ def main():
     head = modes[-1]  # FP32-bulk when both run
     m = res[head]
     e2e = e2e_mode(args, mesh, ph, alpha, m, local, dist, world)
+    # the plain FP64 mode end to end as well (the same host transfers)
+    e2e_other = {p: e2e_mode(args, mesh, ph, alpha, r, local, dist, world) for p, r in res.items() if p != head}
     batch_line = None
     if args.workload == "step" and args.batch_steps > 0:
         # every rank takes the same steps (replicas under torchrun)
@@ -690,6 +698,7 @@ def main():
                 "kernel_ms_per_launch": m["per_launch_ms"], "kernel_time_share": m["share"],
                 "clocks": m["clocks"], "state_finite": bool(m["state_finite"])}
         line["modes"] = {p: {"value": r["value"], "ms_per_step": r["ms_per_step"], "roofline_frac": r["roofline"]["frac"],
+                             "e2e": e2e if p == head else e2e_other.get(p),
                              "stage_kernels": r["stage_kernels"], "schedule": r["schedule"], "schedule": r["schedule"],
                              "grad_lim_frac": r.get("roofline_grad_lim", {}).get("frac"),
                              "dt_frac": r.get("roofline_dt", {}).get("frac"),
