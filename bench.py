@@ -92,9 +92,9 @@ def algo_bytes(ph, precision, kernel):
 TRAFFIC_B_PER_CELL = {
     ("step", "fp32", "split"): (153.2, "ncu --set full -k regex:k_tile_stage -s 30 -c 2, "
                                        "bench.py --precision fp32 --steps 20 --warmup 3 --no-cpu-baseline"),
-    ("step", "fp32", "fused"): (149.1, "ncu --set full -k regex:k_tile_fused -s 10 -c 2, bench.py --precision "
+    ("step", "fp32", "fused"): (150.6, "ncu --set full -k regex:k_tile_fused -s 10 -c 2, bench.py --precision "
                                        "fp32 --steps 20 --warmup 3 --no-cpu-baseline --batch-steps 0"),
-    ("step", "fp64", "fused"): (231.8, "ncu --set full -k regex:k_tile_fused -s 10 -c 2, bench.py --precision "
+    ("step", "fp64", "fused"): (231.3, "ncu --set full -k regex:k_tile_fused -s 10 -c 2, bench.py --precision "
                                        "fp64 --steps 20 --warmup 3 --no-cpu-baseline --batch-steps 0"),
 }
 
