@@ -16,6 +16,7 @@
 #include "fv_tile.cuh"
 #include "fv_fused.cuh"
 #include "fv_adjoint.h"
+#include "fv_solver.h"
 #include <cmath>
 
 using namespace fvgpu;
@@ -43,85 +44,6 @@ cudaError_t upload(T** dst, const std::vector<T>& v) {
     return e;
 }
 }  // namespace
-
-struct fv_mesh {
-    HostMesh m;
-};
-
-struct GraphEntry {
-    std::vector<double> alpha;
-    int chunk = 0;
-    cudaGraphExec_t exec = nullptr;
-    int launches = 0;
-};
-
-struct fv_solver {
-    int device = 0;
-    int precision = FV_PREC_FP64_EXACT;
-    bool f32 = false;
-    size_t ssz = 8;                 // bytes of one stored stage value
-    cudaStream_t stream = nullptr;
-    bool own_stream = false;
-    int V = 4;
-    int64_t n_real = 0, n_total = 0, n_bound = 0;
-    int n_tiles = 0;
-    TileParams TP{};
-    // the fused stage kernel over two-ring tiles (its Params are TP.P at launch)
-    bool fused = false;
-    FusedParams FPm{};
-    // its schedule (FV_SCHED_*); the work list's per-stage tile counters and
-    // CTAs per launch
-    int sched = 0;
-    int* work = nullptr;
-    int work_grid = 0;
-    // device buffers
-    std::vector<void*> allocs;
-    double* qbase[2] = {nullptr, nullptr};   // FP64 step-start state (RK1 alternates)
-    void* sbase[2] = {nullptr, nullptr};     // stage-precision copy of the base (== qbase unless FP32)
-    void* tmp[2] = {nullptr, nullptr};       // intermediate stage outputs
-    void *gx = nullptr, *gy = nullptr, *lim = nullptr;
-    double* dt = nullptr;
-    double* stage_buf = nullptr;   // [n_total*V] staging for host transfers
-    double* partials = nullptr;
-    double* scratch2 = nullptr;
-    int* flag = nullptr;
-    int32_t* new2ref = nullptr;
-    Ctrl* ctrl = nullptr;
-    RunLimits* limits = nullptr;
-    PrintRec* hist = nullptr;
-    int hist_cap = 0;
-    int chunk = 16;
-    std::vector<GraphEntry> graphs;
-    double last_ms = 0.0;
-    int64_t last_launches = 0;
-    // dt minimum key slots: [n_cases][kDtSlots] (one case: inside ctrl)
-    unsigned long long* keys = nullptr;
-    int n_cases = 1;
-    double* case_time = nullptr;                           // batches: [n_cases]
-    double* ghost_bv = nullptr;                            // per-ghost boundary states [n_bound][4]
-    Ctrl* hctrl = nullptr;      // mapped pinned host copy of the run control, written by a kernel
-    Ctrl* hctrl_dev = nullptr;  // its device address
-    std::vector<int64_t> case_real_off, case_bound_off;    // batches: host copies
-    // residual smoothing: time derivatives before / after each Jacobi sweep
-    // ([n_total][V], ghosts 0) and the real cells' neighbours ([4][n_real])
-    double* qts[3] = {nullptr, nullptr, nullptr};
-    uint32_t* nbr = nullptr;
-
-    template <class T>
-    cudaError_t alloc(T** p, size_t n, size_t elem = sizeof(T)) {
-        cudaError_t e = cudaMalloc((void**)p, std::max<size_t>(n, 1) * elem);
-        if (e == cudaSuccess) allocs.push_back((void*)*p);
-        return e;
-    }
-    ~fv_solver() {
-        cudaSetDevice(device);
-        for (auto& g : graphs)
-            if (g.exec) cudaGraphExecDestroy(g.exec);
-        for (void* p : allocs) cudaFree(p);
-        if (hctrl) cudaFreeHost(hctrl);  // allocated with cudaHostAlloc
-        if (own_stream && stream) cudaStreamDestroy(stream);
-    }
-};
 
 // Drops the captured step graphs (their kernels change with s->fused).
 static void clear_graphs(fv_solver* s) {
@@ -450,6 +372,7 @@ int fv_solver_create_ex(const fv_mesh* fm, const fv_physics* ph, int32_t precisi
     TileParams& TP = s->TP;
     Params& P = TP.P;
     P.n_real = (int)m.n_real; P.n_total = (int)m.n_total; P.n_bound = (int)m.n_bound; P.V = ph->V;
+    P.n_own = (int)m.owned_real();
     P.cell0 = fa.cell0;
     if ((rc = upload_v(s.get(), fa.ghost_group, &P.ghost_group))) return rc;
     if ((rc = upload_v(s.get(), fa.ghost_cell, &P.ghost_cell))) return rc;
@@ -561,7 +484,8 @@ int fv_solver_create_ex(const fv_mesh* fm, const fv_physics* ph, int32_t precisi
     CK(s->alloc(&s->tmp[0], nq, s->ssz)); CK(s->alloc(&s->tmp[1], nq, s->ssz));
     CK(s->alloc(&s->gx, nq, s->ssz)); CK(s->alloc(&s->gy, nq, s->ssz)); CK(s->alloc(&s->lim, nq, s->ssz));
     CK(s->alloc(&s->stage_buf, nq));
-    CK(s->alloc(&s->dt, (size_t)m.n_total));
+    // one more slot: a decomposition's copy of reference cell 0's dt
+    CK(s->alloc(&s->dt, (size_t)m.n_total + 1));
     CK(s->alloc(&s->partials, (size_t)ta.n_tiles * ph->V));
     CK(s->alloc(&s->scratch2, 8));
     CK(s->alloc(&s->flag, 4));
@@ -826,21 +750,101 @@ int fv_batch_times(fv_solver* s, double* times) {
 int fv_get_state_device(fv_solver* s, double* q) { return get_state_common(s, q, cudaMemcpyDeviceToDevice); }
 
 // ---------------------------------------------------------------- run ----
-// Kernel kinds for per-kernel timing.
-enum { KK_BEGIN = 0, KK_DT = 1, KK_GRADLIM = 2, KK_STAGE = 3, KK_END = 4, KK_N = 5 };
+}  // extern "C"
 
-struct EventLog {
-    std::vector<cudaEvent_t> ev;  // ev[0] before the first kernel, ev[k+1] after kernel k
-    std::vector<int> kind;
-    cudaStream_t st;
-    void mark(int k) {
-        cudaEvent_t e;
-        cudaEventCreate(&e);
-        cudaEventRecord(e, st);
-        ev.push_back(e);
-        kind.push_back(k);
+namespace fvgpu {
+
+int set_error(int code, const std::string& msg) { return fail(code, msg); }
+
+int step_open(fv_solver* s, const std::vector<double>& alpha, int b, bool first, StepCursor& c, EventLog* log) {
+    const TileParams& TP = s->TP;
+    cudaStream_t st = s->stream;
+    int n = 0;
+    auto mark = [&](int k) { if (log) log->mark(k); };
+    if (first) { launch_step_begin(s->ctrl, s->limits, s->V, s->keys, s->n_cases * kDtSlots, st); ++n; mark(KK_BEGIN); }
+    TileIO& io = c.io;
+    io = TileIO{};
+    io.gx = s->gx; io.gy = s->gy; io.lim = s->lim; io.dt = s->dt; io.ctrl = s->ctrl;
+    io.dtkeys = s->keys;
+    io.q_stage = s->sbase[b];
+    c.b = b;
+    // the fused stage kernel computes its gradients itself: the step's dt
+    // comes from the dt kernel, as in first order
+    c.grads = (TP.P.order2 || TP.P.diffusive) && !s->fused;
+    // the work-list schedule: one tile counter per stage, zeroed by the dt kernel
+    c.worklist = s->fused && s->sched == FV_SCHED_WORKLIST && alpha.size() <= (size_t)kWorkSlots;
+    // every kernel after step_begin is a programmatic dependent of the one
+    // before it (its constant tile data is staged during that one's tail)
+    if (!c.grads) {
+        TileIO dio = io;
+        dio.work_reset = c.worklist ? s->work : nullptr;
+        tile::launch_dt(s->precision, TP, dio, st, true); ++n; mark(KK_DT);
     }
-};
+    c.FPl = s->FPm;
+    c.FPl.P = TP.P;
+    c.FPl.threads = (s->sched == FV_SCHED_TILE2) ? 2 * c.FPl.T : c.FPl.T;
+    c.in = s->sbase[b];
+    c.out = nullptr;
+    return n;
+}
+
+int step_stage(fv_solver* s, const std::vector<double>& alpha, int k, StepCursor& c, EventLog* log) {
+    const TileParams& TP = s->TP;
+    cudaStream_t st = s->stream;
+    const bool pdl = true;
+    int n = 0;
+    auto mark = [&](int kk) { if (log) log->mark(kk); };
+    const int ns = (int)alpha.size(), b = c.b;
+    const bool last = k == ns - 1;
+    TileIO so = c.io;
+    so.q_stage = c.in;
+    so.q_base = s->qbase[b];
+    so.alpha = alpha[k];
+    so.partials = last ? s->partials : nullptr;
+    void* out_s;
+    if (ns == 1) {
+        so.q_out = s->qbase[1 - b];
+        out_s = s->sbase[1 - b];
+    } else if (last) {
+        so.q_out = s->qbase[b];
+        out_s = s->sbase[b];
+    } else {
+        out_s = s->tmp[k % 2];
+        so.q_out = s->f32 ? nullptr : (double*)out_s;
+    }
+    so.s_out = s->f32 ? out_s : nullptr;
+    so.write_f64 = last ? 1 : 0;
+    if (c.grads) { tile::launch_gradlim(s->precision, TP, so, st, k == 0, pdl); ++n; mark(KK_GRADLIM); }
+    if (TP.P.smooth) {
+        // time derivatives, two Jacobi sweeps of smoothing, then the update
+        // from the smoothed derivatives (explicit.cpp:742-744)
+        so.qt = s->qts[0];
+        tile::launch_stage(s->precision, TP, so, st, pdl, 1); ++n; mark(KK_STAGE);
+        launch_smooth(TP.P, s->nbr, s->qts[0], s->qts[0], s->qts[1], st); ++n; mark(KK_STAGE);
+        launch_smooth(TP.P, s->nbr, s->qts[1], s->qts[0], s->qts[2], st); ++n; mark(KK_STAGE);
+        so.qt = s->qts[2];
+        tile::launch_stage(s->precision, TP, so, st, pdl, 2); ++n; mark(KK_STAGE);
+    } else if (s->fused) {
+        so.work = c.worklist ? s->work + k : nullptr;
+        tile::launch_fused(s->precision, c.FPl, so, st, pdl, s->n_tiles, s->work_grid); ++n; mark(KK_STAGE);
+    } else {
+        tile::launch_stage(s->precision, TP, so, st, pdl); ++n; mark(KK_STAGE);
+    }
+    c.in = out_s;
+    c.out = out_s;
+    return n;
+}
+
+int step_close(fv_solver* s, const double* partials, int nblocks, EventLog* log) {
+    launch_step_end(s->TP.P, s->ctrl, s->limits, partials, nblocks, s->dt, s->keys, s->n_cases * kDtSlots,
+                    s->hist, s->hist_cap, s->stream, true);
+    if (log) log->mark(KK_END);
+    return 1;
+}
+
+}  // namespace fvgpu
+
+extern "C" {
 
 // Enqueues one time step (explicit.cpp:715-801) whose base state is
 // qbase[b] (RK1 writes its result to qbase[1-b]).  Returns the number of
@@ -849,76 +853,10 @@ struct EventLog {
 // begin-of-step kernel (every step end also begins the next step).
 static int enqueue_step(fv_solver* s, const std::vector<double>& alpha, int b, EventLog* log = nullptr,
                         bool first = true) {
-    const TileParams& TP = s->TP;
-    cudaStream_t st = s->stream;
-    int n = 0;
-    auto mark = [&](int k) { if (log) log->mark(k); };
-    if (first) { launch_step_begin(s->ctrl, s->limits, s->V, s->keys, s->n_cases * kDtSlots, st); ++n; mark(KK_BEGIN); }
-    TileIO io{};
-    io.gx = s->gx; io.gy = s->gy; io.lim = s->lim; io.dt = s->dt; io.ctrl = s->ctrl;
-    io.dtkeys = s->keys;
-    io.q_stage = s->sbase[b];
-    // with gradients (second order, diffusive fluxes) the first stage's
-    // gradient kernel also computes dt
-    // every kernel after step_begin is a programmatic dependent of the one
-    // before it (its constant tile data is staged during that one's tail)
-    const bool pdl = true;
-    // the fused stage kernel computes its gradients itself: the step's dt
-    // comes from the dt kernel, as in first order
-    const bool grads = (TP.P.order2 || TP.P.diffusive) && !s->fused;
-    // the work-list schedule: one tile counter per stage, zeroed by the dt kernel
-    const bool worklist = s->fused && s->sched == FV_SCHED_WORKLIST && alpha.size() <= (size_t)kWorkSlots;
-    if (!grads) {
-        TileIO dio = io;
-        dio.work_reset = worklist ? s->work : nullptr;
-        tile::launch_dt(s->precision, TP, dio, st, pdl); ++n; mark(KK_DT);
-    }
-    FusedParams FPl = s->FPm;
-    FPl.P = TP.P;
-    FPl.threads = (s->sched == FV_SCHED_TILE2) ? 2 * FPl.T : FPl.T;
-    const int ns = (int)alpha.size();
-    const void* in = s->sbase[b];
-    for (int k = 0; k < ns; ++k) {
-        const bool last = k == ns - 1;
-        TileIO so = io;
-        so.q_stage = in;
-        so.q_base = s->qbase[b];
-        so.alpha = alpha[k];
-        so.partials = last ? s->partials : nullptr;
-        void* out_s;
-        if (ns == 1) {
-            so.q_out = s->qbase[1 - b];
-            out_s = s->sbase[1 - b];
-        } else if (last) {
-            so.q_out = s->qbase[b];
-            out_s = s->sbase[b];
-        } else {
-            out_s = s->tmp[k % 2];
-            so.q_out = s->f32 ? nullptr : (double*)out_s;
-        }
-        so.s_out = s->f32 ? out_s : nullptr;
-        so.write_f64 = last ? 1 : 0;
-        if (grads) { tile::launch_gradlim(s->precision, TP, so, st, k == 0, pdl); ++n; mark(KK_GRADLIM); }
-        if (TP.P.smooth) {
-            // time derivatives, two Jacobi sweeps of smoothing, then the update
-            // from the smoothed derivatives (explicit.cpp:742-744)
-            so.qt = s->qts[0];
-            tile::launch_stage(s->precision, TP, so, st, pdl, 1); ++n; mark(KK_STAGE);
-            launch_smooth(TP.P, s->nbr, s->qts[0], s->qts[0], s->qts[1], st); ++n; mark(KK_STAGE);
-            launch_smooth(TP.P, s->nbr, s->qts[1], s->qts[0], s->qts[2], st); ++n; mark(KK_STAGE);
-            so.qt = s->qts[2];
-            tile::launch_stage(s->precision, TP, so, st, pdl, 2); ++n; mark(KK_STAGE);
-        } else if (s->fused) {
-            so.work = worklist ? s->work + k : nullptr;
-            tile::launch_fused(s->precision, FPl, so, st, pdl, s->n_tiles, s->work_grid); ++n; mark(KK_STAGE);
-        } else {
-            tile::launch_stage(s->precision, TP, so, st, pdl); ++n; mark(KK_STAGE);
-        }
-        in = out_s;
-    }
-    launch_step_end(TP.P, s->ctrl, s->limits, s->partials, s->n_tiles, s->dt, s->keys, s->n_cases * kDtSlots,
-                    s->hist, s->hist_cap, st, pdl);
-    ++n; mark(KK_END);
+    StepCursor c;
+    int n = step_open(s, alpha, b, first, c, log);
+    for (int k = 0; k < (int)alpha.size(); ++k) n += step_stage(s, alpha, k, c, log);
+    n += step_close(s, s->partials, s->n_tiles, log);
     return n;
 }
 

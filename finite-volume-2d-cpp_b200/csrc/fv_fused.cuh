@@ -147,7 +147,7 @@ __device__ __forceinline__ bool fused_tile(const FusedParams& FP, const TileIO& 
     const int4 ia = FP.info[2 * t], ib = FP.info[2 * t + 1];
     const int edge_off = ia.x, n_edges = ia.y, n_flux = ia.z, halo_off = ia.w;
     const int n1 = ib.x, n2 = ib.y, face_off = ib.z;
-    const int c0 = t * T, nown = min(T, N - c0);
+    const int c0 = t * T, nown = min(T, P.n_own - c0);
     const FusedSmem L = fused_smem<M>(FP.max_slots, FP.max_grad, FP.max_edges, FP.max_flux, FP.T);
     uint4* Q = reinterpret_cast<uint4*>(smem_raw + L.q);
     uint4* C = reinterpret_cast<uint4*>(smem_raw + L.c);

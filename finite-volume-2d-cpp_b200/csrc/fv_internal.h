@@ -40,6 +40,7 @@ struct RunLimits {
 // Sizes, boundary-ghost metadata and physics, passed to kernels by value.
 struct Params {
     int n_real, n_total, n_bound, V;
+    int n_own;                      // tiles cover real cells [0, n_own): n_real, or a part's own cells
     int cell0;                      // device index of reference cell 0 (time += dt[0])
     // boundary ghost b (device cell n_real + b): its interior cell, the face
     // normal/length, and x_f - x_interior (reference arithmetic, FP64)

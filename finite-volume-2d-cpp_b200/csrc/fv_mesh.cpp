@@ -282,8 +282,26 @@ static double halo_score(const HostMesh& m, const std::vector<int32_t>& n2r) {
     return (double)pairs.size() / (double)std::max<int64_t>(nt, 1) + 0.25 * mx;
 }
 
+// Faces of each device-numbered real cell in increasing reference edge order.
+static void build_face_lists(HostMesh& m) {
+    const int64_t nc = m.n_real, E = m.n_edges;
+    m.face_edge.assign(nc * HostMesh::MAXF, -1);
+    m.face_side.assign(nc * HostMesh::MAXF, 0);
+    m.n_faces.assign(nc, 0);
+    for (int64_t e = 0; e < E; ++e) {
+        for (int s = 0; s < 2; ++s) {
+            const uint32_t rc = m.edge_cells[2 * e + s];
+            if (rc >= (uint32_t)nc) continue;
+            const int32_t c = m.ref2new[rc];
+            const int k = m.n_faces[c]++;
+            m.face_edge[c * HostMesh::MAXF + k] = (int32_t)e;
+            m.face_side[c * HostMesh::MAXF + k] = (uint8_t)s;
+        }
+    }
+}
+
 void build_device_numbering(HostMesh& m) {
-    const int64_t nc = m.n_real, nt = m.n_total, E = m.n_edges;
+    const int64_t nc = m.n_real, nt = m.n_total;
     std::vector<int64_t> offs = m.case_real_off;
     if (offs.size() < 2) offs = {0, nc};
     // Hilbert order on the centroids keeps isotropic meshes (and O-grids,
@@ -313,20 +331,7 @@ void build_device_numbering(HostMesh& m) {
         m.new2ref[nc + k] = ref;
         m.ref2new[ref] = (int32_t)(nc + k);
     }
-    // faces per new cell in increasing reference edge order
-    m.face_edge.assign(nc * HostMesh::MAXF, -1);
-    m.face_side.assign(nc * HostMesh::MAXF, 0);
-    m.n_faces.assign(nc, 0);
-    for (int64_t e = 0; e < E; ++e) {
-        for (int s = 0; s < 2; ++s) {
-            const uint32_t rc = m.edge_cells[2 * e + s];
-            if (rc >= (uint32_t)nc) continue;
-            const int32_t c = m.ref2new[rc];
-            const int k = m.n_faces[c]++;
-            m.face_edge[c * HostMesh::MAXF + k] = (int32_t)e;
-            m.face_side[c * HostMesh::MAXF + k] = (uint8_t)s;
-        }
-    }
+    build_face_lists(m);
 }
 
 // The per-face quantities use the reference's arithmetic: the Green-Gauss
@@ -379,8 +384,9 @@ void build_face_arrays(const HostMesh& m, FaceArrays& fa) {
 
 void build_tiles(const HostMesh& m, const FaceArrays& fa, int T, TileArrays& ta) {
     const int64_t N = m.n_real, NT = m.n_total, F = HostMesh::MAXF;
+    const int64_t NO = m.owned_real();
     ta.tile_cells = T;
-    ta.n_tiles = (int)((N + T - 1) / T);
+    ta.n_tiles = (int)((NO + T - 1) / T);
     ta.info.assign((size_t)ta.n_tiles * 4, 0);
     ta.halo.clear(); ta.edge_ij.clear(); ta.edge_ref.clear();
     for (auto* v : {&ta.enx, &ta.eny, &ta.ele, &ta.exf, &ta.eyf, &ta.eg}) v->clear();
@@ -390,7 +396,7 @@ void build_tiles(const HostMesh& m, const FaceArrays& fa, int T, TileArrays& ta)
     std::vector<int32_t> edge_stamp(m.n_edges, -1), edge_local(m.n_edges, 0);
     std::vector<int32_t> touched;
     for (int t = 0; t < ta.n_tiles; ++t) {
-        const int64_t c0 = (int64_t)t * T, c1 = std::min<int64_t>(c0 + T, N);
+        const int64_t c0 = (int64_t)t * T, c1 = std::min<int64_t>(c0 + T, NO);
         const int edge_off = (int)ta.edge_ij.size(), halo_off = (int)ta.halo.size();
         int n_halo = 0, n_edges = 0;
         touched.clear();
@@ -436,15 +442,16 @@ void build_tiles(const HostMesh& m, const FaceArrays& fa, int T, TileArrays& ta)
 
 void build_tiles2(const HostMesh& m, const FaceArrays& fa, int T, Tile2Arrays& ta) {
     const int64_t N = m.n_real, NT = m.n_total, F = HostMesh::MAXF;
+    const int64_t NO = m.owned_real();
     ta = Tile2Arrays();
     ta.tile_cells = T;
-    ta.n_tiles = (int)((N + T - 1) / T);
+    ta.n_tiles = (int)((NO + T - 1) / T);
     ta.info.assign((size_t)ta.n_tiles * 8, 0);
     std::vector<int32_t> local(NT, -1);          // device cell -> local slot in the current tile
     std::vector<int32_t> edge_stamp(m.n_edges, -1), edge_local(m.n_edges, 0);
     std::vector<int32_t> touched, ring1;
     for (int t = 0; t < ta.n_tiles; ++t) {
-        const int64_t c0 = (int64_t)t * T, c1 = std::min<int64_t>(c0 + T, N);
+        const int64_t c0 = (int64_t)t * T, c1 = std::min<int64_t>(c0 + T, NO);
         const int edge_off = (int)ta.edge_ij.size(), halo_off = (int)ta.halo.size();
         const int face_off = (int)(ta.face.size() / 4);
         int n_halo = 0, n_edges = 0;
@@ -505,6 +512,173 @@ void build_tiles2(const HostMesh& m, const FaceArrays& fa, int T, Tile2Arrays& t
         ta.max_flux = std::max(ta.max_flux, n_flux);
         for (int32_t d : touched) local[d] = -1;
     }
+}
+
+// ----------------------------------------------------------------------------
+// Domain decomposition.  The reference decomposes with gmsh partitions and
+// exchanges q, gx, gy, limiters and dt of one ring of ghost elements per
+// stage (mesh.cpp:673-799, explicit.cpp:420-477, 636-648, 729-746).  Here a
+// part owns a contiguous range of the device numbering (Hilbert order, so
+// parts are compact) and holds two rings of halo cells plus the boundary
+// ghosts of ring 1, so that the fused stage kernel recomputes the ring-1
+// gradients and limiters it needs and only the stage state crosses between
+// parts, once per stage.
+// ----------------------------------------------------------------------------
+namespace {
+struct Halo {
+    std::vector<int32_t> real;   // device indices of ring-1 and ring-2 real cells, ascending
+    std::vector<int32_t> ghost;  // device ghost offsets (from n_real) of ring-1 ghosts, ascending
+    std::vector<int32_t> ring1;  // device indices of ring-1 real cells
+};
+}  // namespace
+
+std::string build_part(const HostMesh& g, int n_parts, int part, HostMesh& L, PartPlan& plan) {
+    const int64_t N = g.n_real, NB = g.n_bound, F = HostMesh::MAXF;
+    if (g.case_real_off.size() > 2) return "a batch of cases cannot be decomposed";
+    if (n_parts < 1 || part < 0 || part >= n_parts) return "part index out of range";
+    if (n_parts > N) return "more parts than cells";
+    plan = PartPlan();
+    plan.n_parts = n_parts;
+    plan.part = part;
+    plan.own_off.resize(n_parts + 1);
+    for (int p = 0; p <= n_parts; ++p) plan.own_off[p] = N * p / n_parts;
+    auto owner = [&](int64_t d) {
+        return (int)(std::upper_bound(plan.own_off.begin(), plan.own_off.end(), d) - plan.own_off.begin() - 1);
+    };
+    // device interior cell of each device ghost; ghosts are ordered by it, so
+    // each part's ghosts form a contiguous range
+    std::vector<int32_t> ghost_in(NB);
+    for (int64_t k = 0; k < NB; ++k)
+        ghost_in[k] = g.ref2new[g.edge_cells[2 * g.bound_edges[g.new2ref[N + k] - N]]];
+    plan.ghost_off.assign(n_parts + 1, NB);
+    for (int64_t k = NB - 1; k >= 0; --k) plan.ghost_off[owner(ghost_in[k])] = k;
+    for (int p = n_parts - 1; p >= 0; --p) plan.ghost_off[p] = std::min(plan.ghost_off[p], plan.ghost_off[p + 1]);
+    auto nbr = [&](int64_t c, int k) {  // device index of the other cell of face k of device cell c
+        const int32_t e = g.face_edge[c * F + k];
+        return g.ref2new[g.edge_cells[2 * e + (g.face_side[c * F + k] ? 0 : 1)]];
+    };
+    std::vector<int32_t> mark(N + NB, -1);
+    auto halo_of = [&](int p, Halo& h) {
+        const int64_t a = plan.own_off[p], b = plan.own_off[p + 1];
+        h = Halo();
+        for (int64_t c = a; c < b; ++c)
+            for (int k = 0; k < g.n_faces[c]; ++k) {
+                const int32_t d = nbr(c, k);
+                if (d < N && (d < a || d >= b) && mark[d] != p) { mark[d] = p; h.ring1.push_back(d); }
+            }
+        h.real = h.ring1;
+        for (int32_t c : h.ring1)
+            for (int k = 0; k < g.n_faces[c]; ++k) {
+                const int32_t d = nbr(c, k);
+                if (mark[d] == p) continue;
+                if (d < N && d >= a && d < b) continue;
+                mark[d] = p;
+                if (d < N) h.real.push_back(d);
+                else h.ghost.push_back(d - (int32_t)N);
+            }
+        std::sort(h.real.begin(), h.real.end());
+        std::sort(h.ghost.begin(), h.ghost.end());
+    };
+    std::vector<Halo> halos(n_parts);
+    for (int p = 0; p < n_parts; ++p) halo_of(p, halos[p]);
+    const Halo& H = halos[part];
+    const int64_t a = plan.own_off[part], b = plan.own_off[part + 1];
+    const int64_t ga = plan.ghost_off[part], gb = plan.ghost_off[part + 1];
+    plan.n_own = b - a;
+    plan.n_own_ghost = gb - ga;
+    const int64_t nr = plan.n_own + (int64_t)H.real.size();
+    const int64_t nbl = plan.n_own_ghost + (int64_t)H.ghost.size();
+    // local numbering: owned cells, halo cells (grouped by owner), owned
+    // ghosts, halo ghosts (grouped by owner); each group in device order
+    std::vector<int32_t> dev_of(nr + nbl);   // device index (ghosts: N + offset) of each local cell
+    for (int64_t i = 0; i < plan.n_own; ++i) dev_of[i] = (int32_t)(a + i);
+    for (size_t i = 0; i < H.real.size(); ++i) dev_of[plan.n_own + i] = H.real[i];
+    for (int64_t i = 0; i < plan.n_own_ghost; ++i) dev_of[nr + i] = (int32_t)(N + ga + i);
+    for (size_t i = 0; i < H.ghost.size(); ++i) dev_of[nr + plan.n_own_ghost + i] = (int32_t)(N + H.ghost[i]);
+    std::vector<int32_t> loc(N + NB, -1);    // device index -> local index
+    for (size_t i = 0; i < dev_of.size(); ++i) loc[dev_of[i]] = (int32_t)i;
+    plan.local2ref.resize(dev_of.size());
+    for (size_t i = 0; i < dev_of.size(); ++i) plan.local2ref[i] = g.new2ref[dev_of[i]];
+    // receive lists: from each owner, its real halo cells, then its ghosts
+    plan.recv_off.assign(n_parts + 1, 0);
+    plan.recv_idx.clear();
+    for (int r = 0; r < n_parts; ++r) {
+        plan.recv_off[r] = (int64_t)plan.recv_idx.size();
+        if (r == part) continue;
+        for (size_t i = 0; i < H.real.size(); ++i)
+            if (owner(H.real[i]) == r) plan.recv_idx.push_back((int32_t)(plan.n_own + i));
+        for (size_t i = 0; i < H.ghost.size(); ++i)
+            if (owner(ghost_in[H.ghost[i]]) == r) plan.recv_idx.push_back((int32_t)(nr + plan.n_own_ghost + i));
+    }
+    plan.recv_off[n_parts] = (int64_t)plan.recv_idx.size();
+    // send lists: to each part, the cells and ghosts of this part in its halo, in its receive order
+    plan.send_off.assign(n_parts + 1, 0);
+    plan.send_idx.clear();
+    for (int r = 0; r < n_parts; ++r) {
+        plan.send_off[r] = (int64_t)plan.send_idx.size();
+        if (r == part) continue;
+        for (int32_t d : halos[r].real)
+            if (d >= a && d < b) plan.send_idx.push_back((int32_t)(d - a));
+        for (int32_t o : halos[r].ghost)
+            if (o >= ga && o < gb) plan.send_idx.push_back((int32_t)(nr + (o - ga)));
+    }
+    plan.send_off[n_parts] = (int64_t)plan.send_idx.size();
+    const int32_t d0 = g.ref2new[0];
+    plan.owner0 = owner(d0);
+    plan.cell0 = plan.owner0 == part ? (int32_t)(d0 - a) : -1;
+
+    // local edges: every edge of an owned or ring-1 cell, in reference edge order
+    std::vector<int32_t> edges;
+    std::vector<uint8_t> seen(g.n_edges, 0);
+    auto take = [&](int64_t c) {
+        for (int k = 0; k < g.n_faces[c]; ++k) {
+            const int32_t e = g.face_edge[c * F + k];
+            if (!seen[e]) { seen[e] = 1; edges.push_back(e); }
+        }
+    };
+    for (int64_t c = a; c < b; ++c) take(c);
+    for (int32_t c : H.ring1) take(c);
+    std::sort(edges.begin(), edges.end());
+    plan.local_edges = edges;
+    std::vector<int32_t> eloc(g.n_edges, -1);
+    for (size_t i = 0; i < edges.size(); ++i) eloc[edges[i]] = (int32_t)i;
+
+    L = HostMesh();
+    L.group_names = g.group_names;
+    L.n_real = nr; L.n_total = nr + nbl; L.n_bound = nbl; L.n_edges = (int64_t)edges.size();
+    L.n_own = plan.n_own;
+    L.edge_cells.resize(2 * edges.size()); L.edge_nodes.resize(2 * edges.size());
+    for (auto* v : {&L.enx, &L.eny, &L.elen, &L.ecx, &L.ecy}) v->resize(edges.size());
+    for (size_t i = 0; i < edges.size(); ++i) {
+        const int32_t e = edges[i];
+        for (int s = 0; s < 2; ++s) {
+            const int32_t l = loc[g.ref2new[g.edge_cells[2 * e + s]]];
+            if (l < 0) return "internal error: an edge of the part reaches outside its halo";
+            L.edge_cells[2 * i + s] = (uint32_t)l;
+            L.edge_nodes[2 * i + s] = g.edge_nodes[2 * e + s];
+        }
+        L.enx[i] = g.enx[e]; L.eny[i] = g.eny[e]; L.elen[i] = g.elen[e];
+        L.ecx[i] = g.ecx[e]; L.ecy[i] = g.ecy[e];
+    }
+    L.area.resize(L.n_total); L.ccx.resize(L.n_total); L.ccy.resize(L.n_total);
+    for (int64_t i = 0; i < L.n_total; ++i) {
+        const int32_t r = plan.local2ref[i];
+        L.area[i] = g.area[r]; L.ccx[i] = g.ccx[r]; L.ccy[i] = g.ccy[r];
+    }
+    L.bound_edges.resize(nbl); L.bnd_group.resize(nbl);
+    for (int64_t k = 0; k < nbl; ++k) {
+        const int64_t rb = plan.local2ref[nr + k] - N;
+        const int32_t le = eloc[g.bound_edges[rb]];
+        if (le < 0) return "internal error: a ghost's boundary edge is not in the part";
+        L.bound_edges[k] = (uint32_t)le;
+        L.bnd_group[k] = g.bnd_group[rb];
+    }
+    // the local numbering is the device numbering
+    L.ref2new.resize(L.n_total);
+    std::iota(L.ref2new.begin(), L.ref2new.end(), 0);
+    L.new2ref = L.ref2new;
+    build_face_lists(L);
+    return "";
 }
 
 // ----------------------------------------------------------------------------

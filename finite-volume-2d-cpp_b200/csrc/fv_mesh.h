@@ -40,6 +40,12 @@ struct HostMesh {
     std::vector<int32_t> face_edge;  // [n_real][MAXF] reference edge index or -1
     std::vector<uint8_t> face_side;  // [n_real][MAXF] 0: cell is edge_cells(e,0), 1: cell is edge_cells(e,1)
     std::vector<uint8_t> n_faces;    // [n_real]
+
+    // ---- one part of a domain decomposition (build_part) ----
+    // The tiles cover device cells [0, n_own); real cells [n_own, n_real) are
+    // halo cells whose states other parts compute.  -1: every real cell.
+    int64_t n_own = -1;
+    int64_t owned_real() const { return n_own >= 0 ? n_own : n_real; }
 };
 
 // Per-face arrays of the device kernels, slot-major [MAXF][n_real] in device
@@ -98,6 +104,36 @@ struct Tile2Arrays {
     std::vector<uint16_t> face;       // [sum over tiles of (T + n1)][4]
 };
 void build_tiles2(const HostMesh& m, const FaceArrays& fa, int tile_cells, Tile2Arrays& ta);
+
+// One part of a decomposition of a single mesh into n_parts parts.  Part p
+// owns device real cells [own_off[p], own_off[p+1]) (contiguous ranges of the
+// Hilbert order) and the boundary ghosts of those cells; its local mesh adds
+// ring 1 (face neighbours of owned cells), ring 2 (face neighbours of ring-1
+// cells) and the boundary ghosts of ring 1, with every edge of an owned or
+// ring-1 cell in reference edge order, so that each owned and ring-1 cell
+// keeps all its faces in the order of the whole mesh.  Local numbering (also
+// the part's device numbering): owned cells, halo real cells, owned ghosts,
+// halo ghosts; the halo groups are sorted by device index and so grouped by
+// owner.
+struct PartPlan {
+    int n_parts = 1, part = 0;
+    std::vector<int64_t> own_off;     // [n_parts + 1] device real cells of each part
+    std::vector<int64_t> ghost_off;   // [n_parts + 1] device ghosts (offsets from n_real) of each part
+    std::vector<int32_t> local2ref;   // reference index of each local cell
+    std::vector<int32_t> local_edges; // reference index of each local edge, ascending
+    int64_t n_own = 0, n_own_ghost = 0;
+    int32_t cell0 = -1;               // local index of reference cell 0, -1 if another part owns it
+    int32_t owner0 = 0;               // the part that owns reference cell 0
+    // halo states from part r land in local cells recv_idx[recv_off[r] .. recv_off[r+1])
+    std::vector<int64_t> recv_off;
+    std::vector<int32_t> recv_idx;
+    // states for part r: local cells send_idx[send_off[r] .. send_off[r+1]), in r's receive order
+    std::vector<int64_t> send_off;
+    std::vector<int32_t> send_idx;
+};
+// Returns "" on success, else an error message.  g: a single mesh with its
+// device numbering.
+std::string build_part(const HostMesh& g, int n_parts, int part, HostMesh& local, PartPlan& plan);
 
 // Builds the reference geometry from an element mesh (mesh.cpp:130-260,
 // 623-669).  Returns "" on success, else an error message.

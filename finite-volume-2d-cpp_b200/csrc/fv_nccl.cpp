@@ -1,0 +1,51 @@
+#include "fv_nccl.h"
+
+#include <dlfcn.h>
+
+#include <mutex>
+#include <type_traits>
+
+namespace fvgpu {
+
+const NcclApi* nccl_api(std::string* err) {
+    static std::once_flag once;
+    static NcclApi api;
+    static bool ok = false;
+    static std::string why;
+    std::call_once(once, [] {
+        void* h = dlopen("libnccl.so.2", RTLD_NOW | RTLD_GLOBAL);
+        if (!h) {
+            const char* e = dlerror();
+            why = std::string("cannot load libnccl.so.2: ") + (e ? e : "unknown error");
+            return;
+        }
+        bool all = true;
+        auto sym = [&](auto& fn, const char* name) {
+            fn = reinterpret_cast<std::remove_reference_t<decltype(fn)>>(dlsym(h, name));
+            if (!fn) {
+                all = false;
+                why = std::string("libnccl.so.2 lacks ") + name;
+            }
+        };
+        sym(api.GetVersion, "ncclGetVersion");
+        sym(api.GetUniqueId, "ncclGetUniqueId");
+        sym(api.CommInitRank, "ncclCommInitRank");
+        sym(api.CommDestroy, "ncclCommDestroy");
+        sym(api.CommAbort, "ncclCommAbort");
+        sym(api.CommGetAsyncError, "ncclCommGetAsyncError");
+        sym(api.GetErrorString, "ncclGetErrorString");
+        sym(api.Send, "ncclSend");
+        sym(api.Recv, "ncclRecv");
+        sym(api.AllGather, "ncclAllGather");
+        sym(api.GroupStart, "ncclGroupStart");
+        sym(api.GroupEnd, "ncclGroupEnd");
+        ok = all;
+    });
+    if (!ok) {
+        if (err) *err = why;
+        return nullptr;
+    }
+    return &api;
+}
+
+}  // namespace fvgpu

@@ -558,9 +558,9 @@ __global__ void __launch_bounds__(kTileMax) k_tile_dt(TileParams TP, TileIO io) 
     pdl_trigger();
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const Params& P = TP.P;
-    const int N = P.n_real, T = TP.T, t = blockIdx.x;
+    const int T = TP.T, t = blockIdx.x;
     const int4 inf = TP.info[t];
-    const int c0 = t * T, nown = min(T, N - c0);
+    const int c0 = t * T, nown = min(T, P.n_own - c0);
     const int LT = T + TP.max_halo;
     S* rec = reinterpret_cast<S*>(smem_raw);
     S* snx = rec + (size_t)LT * R::NR;
@@ -601,9 +601,9 @@ __global__ void __launch_bounds__(kTileMax) k_tile_gradlim(TileParams TP, TileIO
     pdl_trigger();
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const Params& P = TP.P;
-    const int N = P.n_real, T = TP.T, t = blockIdx.x;
+    const int T = TP.T, t = blockIdx.x;
     const int4 inf = TP.info[t];
-    const int c0 = t * T, nown = min(T, N - c0);
+    const int c0 = t * T, nown = min(T, P.n_own - c0);
     const int LT = T + TP.max_halo, EM = TP.max_edges;
     S* rec = reinterpret_cast<S*>(smem_raw);
     S* snx = rec + (size_t)LT * R::NR;
@@ -843,7 +843,7 @@ __device__ __forceinline__ void tile_stage(const TileParams& TP, const TileIO& i
     const Params& P = TP.P;
     const int N = P.n_real, T = TP.T, t = blockIdx.x;
     const int4 inf = TP.info[t];
-    const int c0 = t * T, nown = min(T, N - c0);
+    const int c0 = t * T, nown = min(T, P.n_own - c0);
     const int LT = T + TP.max_halo, EM = TP.max_edges;
     S* rec = reinterpret_cast<S*>(smem_raw);
     FT* sF = reinterpret_cast<FT*>(rec + (size_t)LT * R::NR);
@@ -1210,7 +1210,7 @@ struct TileLaunch {
         }
         return e;
     }
-    static int grid(const TileParams& TP) { return (TP.P.n_real + TP.T - 1) / TP.T; }
+    static int grid(const TileParams& TP) { return (TP.P.n_own + TP.T - 1) / TP.T; }
     // the fast modes' Roe flux kernels of tiles up to 128 cells use k_tile_stage_t128
     static constexpr bool kT128 = !M::exact;
     static bool use_t128(const TileParams& TP) { return kT128 && TP.T <= 128; }

@@ -195,6 +195,23 @@ class Mesh:
         _check(lib().fv_mesh_device_order(self._h, _p(a, _i32p)))
         return a
 
+    def partition(self, n_parts, part):
+        """Host-only plan of one part of a decomposition (fv_mesh_partition):
+        a dict of its sizes and index lists."""
+        sz = np.zeros(10, np.int64)
+        _check(lib().fv_mesh_partition_sizes(self._h, C.c_int32(n_parts), C.c_int32(part), _p(sz, _i64p)))
+        n_real, n_total, n_edges, n_own, n_own_ghost, cell0, owner0, n_recv, n_send, n_bound = (int(v) for v in sz)
+        out = dict(n_real=n_real, n_total=n_total, n_edges=n_edges, n_own=n_own, n_own_ghost=n_own_ghost,
+                   cell0=cell0, owner0=owner0, n_bound=n_bound,
+                   local2ref=np.zeros(n_total, np.int32), local_edges=np.zeros(n_edges, np.int32),
+                   recv_off=np.zeros(n_parts + 1, np.int64), recv_idx=np.zeros(n_recv, np.int32),
+                   send_off=np.zeros(n_parts + 1, np.int64), send_idx=np.zeros(n_send, np.int32))
+        _check(lib().fv_mesh_partition(self._h, C.c_int32(n_parts), C.c_int32(part),
+                                       _p(out["local2ref"], _i32p), _p(out["local_edges"], _i32p),
+                                       _p(out["recv_off"], _i64p), _p(out["recv_idx"], _i32p),
+                                       _p(out["send_off"], _i64p), _p(out["send_idx"], _i32p)))
+        return out
+
 
 def physics_struct(ph: _phys.Physics, group_names: Sequence[str]):
     gbc = np.array([BC[ph.bcs[n][0]] for n in group_names], np.int32)
@@ -413,6 +430,89 @@ class Solver:
         arrs = [np.ascontiguousarray(a, np.float64) for a in (gx, gy, lim)]
         _check(lib().fv_stage_bounds(self._h, _p(q), *[_p(a) for a in arrs]))
         return q
+
+
+def nccl_id() -> bytes:
+    """A fresh 128-byte NCCL id for Group (create on one process, pass to all)."""
+    b = C.create_string_buffer(128)
+    _check(lib().fv_group_nccl_id(b))
+    return b.raw
+
+
+class Group:
+    """A domain decomposition of one mesh (fv_group_*): this process's parts
+    on one CUDA device, NCCL between processes.  Create it on every process
+    with the same mesh, n_parts and id; set_state takes the whole mesh's
+    state, get_state returns it with this process's cells filled in."""
+
+    def __init__(self, mesh: Mesh, ph: _phys.Physics, precision: str = "fp64_exact", n_parts: int = 2,
+                 rank: int = 0, n_ranks: int = 1, nccl_id_bytes: Optional[bytes] = None, device: int = 0,
+                 nccl_local: bool = False, tile_cells: int = 0, schedule: str = "tile"):
+        self.mesh = mesh
+        self.V = ph.V
+        self._ps = physics_struct(ph, mesh.group_names)
+        self._id = C.create_string_buffer(nccl_id_bytes, 128) if nccl_id_bytes is not None else None
+        o = _GroupOptions(n_parts=n_parts, rank=rank, n_ranks=n_ranks,
+                          nccl_id=C.cast(self._id, C.c_void_p) if self._id is not None else None,
+                          nccl_local=int(nccl_local), tile_cells=int(tile_cells), stage_kernels=0,
+                          schedule=Solver.SCHEDULES[schedule])
+        h = C.c_void_p()
+        _check(lib().fv_group_create(mesh._h, C.byref(self._ps), C.c_int32(PREC[precision]), C.c_int32(device),
+                                     C.byref(o), C.byref(h)))
+        self._h = h
+
+    def set_state(self, q):
+        q = np.ascontiguousarray(q, np.float64).reshape(-1)
+        assert q.size == self.mesh.n_total * self.V
+        _check(lib().fv_group_set_state(self._h, _p(q)))
+
+    def get_state(self, q=None):
+        q = np.zeros(self.mesh.n_total * self.V) if q is None else np.ascontiguousarray(q, np.float64)
+        _check(lib().fv_group_get_state(self._h, _p(q)))
+        return q
+
+    def run(self, max_step, alpha=_phys.RK5_ALPHA, max_time=1e10, tolerance=1e-16, print_interval=1,
+            restart=True, on_print: Optional[Callable] = None):
+        a = np.ascontiguousarray(alpha, np.float64)
+        cb = _PRINT_CB(0)
+        if on_print is not None:
+            def _cb(user, step, time, R, V):
+                on_print(int(step), float(time), [R[k] for k in range(V)])
+            cb = _PRINT_CB(_cb)
+        o = _RunOptions(max_step=int(max_step), max_time=float(max_time), tolerance=float(tolerance),
+                        print_interval=int(print_interval), n_alpha=a.size, alpha=_p(a), restart=int(restart),
+                        on_print=cb, user=None)
+        info = _RunInfo()
+        _check(lib().fv_group_run(self._h, C.byref(o), C.byref(info)))
+        return dict(step=info.step, time=info.time, R=np.array(info.R[: self.V]), R0=np.array(info.R0[: self.V]))
+
+    def info(self):
+        out = np.zeros(6, np.int64)
+        _check(lib().fv_group_info(self._h, _p(out, _i64p)))
+        return dict(local_parts=int(out[0]), owned_cells=int(out[1]), halo_cells=int(out[2]),
+                    sent_cells=int(out[3]), tiles=int(out[4]), nccl=bool(out[5]))
+
+    def last_run_stats(self):
+        ms = C.c_double(); n = C.c_int64()
+        _check(lib().fv_group_last_run_stats(self._h, C.byref(ms), C.byref(n)))
+        return ms.value, n.value
+
+    def close(self):
+        if self._h:
+            lib().fv_group_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class _GroupOptions(C.Structure):
+    _fields_ = [("n_parts", C.c_int32), ("rank", C.c_int32), ("n_ranks", C.c_int32), ("nccl_id", C.c_void_p),
+                ("nccl_local", C.c_int32), ("tile_cells", C.c_int32), ("stage_kernels", C.c_int32),
+                ("schedule", C.c_int32)]
 
 
 def solver_info(s: Solver):

@@ -22,6 +22,12 @@
  *   fv_stage_update                    <- calc_time_derivatives + update_cells + update_bounds
  *                                                                    explicit.cpp:261-417
  *   fv_residuals                       <- calc_residuals             explicit.cpp:481-552
+ *   fv_group_create / fv_group_run     <- the MPI run: mesh::read_file of a gmsh partition with
+ *                                         make_comms, run() with update_comms, validate_dt and
+ *                                         the rank sums of calc_residuals
+ *                                         mesh.cpp:574-617, 673-799; explicit.cpp:420-477, 498-550,
+ *                                         567-621, 636-648, 729-746
+ *   fv_mesh_partition                  <- make_comms' send/receive index lists mesh.cpp:673-799
  */
 #ifndef FVGPU_H
 #define FVGPU_H
@@ -40,7 +46,8 @@ typedef enum {
     FV_ERR_UNSUPPORTED = -4,  /* option outside the implemented device physics kinds */
     FV_ERR_NONFINITE = -5,    /* state became non-finite (checked by fv_check_state) */
     FV_ERR_NOMEM = -6,        /* device allocation failed */
-    FV_ERR_IO = -7            /* file could not be read or written */
+    FV_ERR_IO = -7,           /* file could not be read or written */
+    FV_ERR_COMM = -8          /* NCCL unavailable or a collective failed (decompositions) */
 } fv_status;
 
 /* Physics kinds implemented on the device (see finite-volume-2d-cpp_b200/physics.py). */
@@ -252,6 +259,66 @@ int fv_solver_create_tuned(const fv_mesh* m, const fv_physics* ph, int32_t preci
                            const double* q, const double* alpha, int32_t n_alpha, int32_t n_steps,
                            fv_solver** out, int32_t* tile_cells, double* ms_per_step);
 int fv_solver_destroy(fv_solver* s);
+
+/* ---- domain decomposition (one process per GPU, NCCL between processes) ----
+ * The mesh's real cells are split into n_parts contiguous ranges of the
+ * solver's cell order (a Hilbert order, so parts are compact).  Each part
+ * holds its cells, two rings of halo cells and the boundary ghosts of the
+ * first ring, and after every RK stage receives the stage states of its halo
+ * cells from their owners (the reference exchanges q, gx, gy, limiters and dt
+ * of one ring per stage; with two rings each part recomputes the ring-1
+ * gradients and limiters itself, so only the stage state moves).  The time
+ * step is the minimum over all parts (min_dt over the whole mesh; the
+ * reference's validate_dt, explicit.cpp:567-621, keeps the minimum of rank 0
+ * and the last rank only) and the residual norms sum every part's partial
+ * sums in one order on every process, so all parts and processes take the
+ * same steps.  The state of every cell equals the single-solver state bit
+ * for bit; R differs in summation order only.
+ * Physics: first order, or second order with the fused stage kernel (the
+ * Roe kinds); not the diffusive kinds or residual smoothing
+ * (FV_ERR_UNSUPPORTED), not batches of cases. */
+typedef struct fv_group fv_group;
+typedef struct {
+    int32_t n_parts;        /* parts of the decomposition, >= 1, a multiple of n_ranks */
+    int32_t rank, n_ranks;  /* this process and the number of processes; process r holds
+                               parts [r * n_parts / n_ranks, (r + 1) * n_parts / n_ranks) */
+    const void* nccl_id;    /* 128-byte id from fv_group_nccl_id on one process, passed to
+                               all (NULL when n_ranks == 1) */
+    int32_t nccl_local;     /* 1: parts of this process also exchange through NCCL (to
+                               itself) instead of device copies */
+    fv_solver_options solver;  /* every part's tile size, stage kernels and schedule */
+} fv_group_options;
+int fv_group_nccl_id(void* id128);
+/* Collective over the n_ranks processes (each passes the whole mesh, its rank
+ * and the same n_parts and id). */
+int fv_group_create(const fv_mesh* m, const fv_physics* ph, int32_t precision, int32_t device,
+                    const fv_group_options* o, fv_group** out);
+int fv_group_destroy(fv_group* g);
+/* q: the whole mesh's state in reference numbering, AoS [n_total][V].  get
+ * writes the cells and boundary ghosts this process's parts own and leaves
+ * the rest of q as it was. */
+int fv_group_set_state(fv_group* g, const double* q);
+int fv_group_get_state(fv_group* g, double* q);
+/* fv_run for the decomposition (collective): same options and results. */
+int fv_group_run(fv_group* g, const fv_run_options* opt, fv_run_info* info);
+/* out[6]: local parts, owned real cells, halo cells received per stage,
+ * cells sent per stage, tiles, 1 if an NCCL communicator exists */
+int fv_group_info(fv_group* g, int64_t* out);
+int fv_group_last_run_stats(fv_group* g, double* device_ms, int64_t* kernel_launches);
+/* Host-only: the plan of part `part` of n_parts.  sizes[10]: local real cells,
+ * local cells (with ghosts), local edges, owned real cells, owned ghosts,
+ * local index of reference cell 0 (-1 if another part owns it), the part
+ * that owns it, cells received and cells sent per stage, local ghosts.
+ * fv_mesh_partition fills (each may be NULL): local2ref [local cells]
+ * reference index of each local cell (owned cells, halo cells, owned ghosts,
+ * halo ghosts); local_edges [local edges] reference index of each local edge;
+ * recv_off [n_parts + 1] / recv_idx: local cells whose states come from part
+ * r; send_off [n_parts + 1] / send_idx: local cells sent to part r, in r's
+ * receive order. */
+int fv_mesh_partition_sizes(const fv_mesh* m, int32_t n_parts, int32_t part, int64_t* sizes);
+int fv_mesh_partition(const fv_mesh* m, int32_t n_parts, int32_t part, int32_t* local2ref, int32_t* local_edges,
+                      int64_t* recv_off, int32_t* recv_idx, int64_t* send_off, int32_t* send_idx);
+
 /* cudaStream_t as void*; NULL = the solver's own stream */
 int fv_solver_set_stream(fv_solver* s, void* stream);
 int fv_solver_sync(fv_solver* s);
