@@ -622,6 +622,93 @@ def run_adjoint_workload(args):
     adj.close()
 
 
+def run_decomposed_workload(args):
+    """The forward-step workload as a domain decomposition (fv_group_*):
+    n_parts = processes x --parts-per-gpu parts, each a contiguous Hilbert
+    range of the mesh with a two-ring halo, one halo exchange of the stage
+    state per RK stage (NCCL between processes, device copies between the
+    parts of one process), dt minimum and residual sums by all-gather.
+    Strong scaling: the whole job is one mesh.  On one GPU it measures what
+    the decomposition costs beside the single solver (extra launches, halo
+    packing and copies, halo cells computed twice) and checks that both give
+    the same state bit for bit."""
+    import torch
+    import fvgpu
+    import replicas
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    em, ph, alpha, ic, desc = build_workload("step")
+    mesh = make_mesh(em)
+    geo = mesh.geometry()
+    q0 = ic(mesh, geo)
+    prec = "fp32" if args.precision == "all" else args.precision
+    n_parts = world * args.parts_per_gpu
+    nid = None
+    if world > 1:
+        box = [fvgpu.nccl_id() if rank == 0 else None]
+        dist.broadcast_object_list(box, src=0)
+        nid = box[0]
+    grp = fvgpu.Group(mesh, ph, prec, n_parts=n_parts, rank=rank, n_ranks=world, nccl_id_bytes=nid, device=local,
+                      serial_exchange=args.serial_exchange)
+    grp.set_state(q0)
+    grp.run(args.warmup, alpha=alpha)
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        info = grp.run(args.warmup + args.steps, alpha=alpha, restart=False)
+    ms, launches = grp.last_run_stats()
+    if info["step"] != args.warmup + args.steps:
+        raise SystemExit(f"decomposed run stopped at step {info['step']}")
+    ms_max = replicas.max_over_ranks(ms, dist, device=f"cuda:{local}")
+    stages = len(alpha)
+    gi = grp.info()
+    line = None
+    if rank == 0:
+        cell_bytes = 4 * (4 if prec == "fp32" else 8)
+        line = {"metric": METRIC, "value": mesh.n_real * stages * args.steps / (ms_max / 1e3), "unit": UNIT,
+                "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
+                "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+                "dtype": "f32+f64" if prec == "fp32" else "f64", "data": "synthetic",
+                "config": {"workload": desc + ", domain decomposition", "n_real_cells": mesh.n_real,
+                           "n_parts": n_parts, "precision": prec,
+                           "exchange": "after all tiles" if args.serial_exchange else
+                                       "band tiles + exchange on a second stream beside the interior tiles",
+                           "parallelism": (f"{n_parts} parts over {world} processes (NCCL)" if world > 1
+                                           else f"{n_parts} parts on one GPU (device copies)"),
+                           "l2": "inputs larger than L2 (working set > 126 MB), no flush"},
+                "gpu_launches": int(launches), "clocks": clk.summary(),
+                "rank0_parts": gi, "halo_bytes_per_stage_rank0": gi["halo_cells"] * cell_bytes}
+    if world == 1:
+        # the single solver on the same steps: time and state
+        s = fvgpu.Solver(mesh, ph, prec, device=local)
+        s.set_state(q0)
+        s.run(args.warmup, alpha=alpha)
+        torch.cuda.synchronize()
+        s.run(args.warmup + args.steps, alpha=alpha, restart=False)
+        ms1, _ = s.last_run_stats()
+        q1 = s.get_state()
+        s.close()
+        q = grp.get_state()
+        line["single_solver"] = {"value": mesh.n_real * stages * args.steps / (ms1 / 1e3),
+                                 "ms_per_step": ms1 / args.steps,
+                                 "decomposition_time_ratio": ms / ms1,
+                                 "states_bit_identical": q.tobytes() == q1.tobytes()}
+    grp.close()
+    if rank == 0:
+        print(json.dumps(line))
+    if dist is not None:
+        dist.destroy_process_group()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -629,7 +716,12 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="step",
-                    choices=["step", "sod", "naca", "batch", "adjoint", "flatplate", "heat"])
+                    choices=["step", "sod", "naca", "batch", "adjoint", "flatplate", "heat", "decomposed"])
+    ap.add_argument("--parts-per-gpu", type=int, default=None,
+                    help="decomposed workload: parts per process (default 4 on one GPU, else 1)")
+    ap.add_argument("--serial-exchange", action="store_true",
+                    help="decomposed workload: halo exchange after all tiles of a stage (default: beside "
+                         "the interior tiles)")
     ap.add_argument("--precision", default="all", choices=["all", "fp64_exact", "fp64", "fp32"],
                     help="all: FP32-bulk (headline) and plain FP64 in one line")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -657,6 +749,10 @@ def main():
 
     if args.workload == "adjoint":
         return run_adjoint_workload(args)
+    if args.workload == "decomposed":
+        if args.parts_per_gpu is None:
+            args.parts_per_gpu = 4 if int(os.environ.get("WORLD_SIZE", "1")) == 1 else 1
+        return run_decomposed_workload(args)
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))

@@ -788,7 +788,8 @@ int step_open(fv_solver* s, const std::vector<double>& alpha, int b, bool first,
     return n;
 }
 
-int step_stage(fv_solver* s, const std::vector<double>& alpha, int k, StepCursor& c, EventLog* log) {
+int step_stage(fv_solver* s, const std::vector<double>& alpha, int k, StepCursor& c, EventLog* log,
+               const TileRange* r) {
     const TileParams& TP = s->TP;
     cudaStream_t st = s->stream;
     const bool pdl = true;
@@ -814,6 +815,17 @@ int step_stage(fv_solver* s, const std::vector<double>& alpha, int k, StepCursor
     }
     so.s_out = s->f32 ? out_s : nullptr;
     so.write_f64 = last ? 1 : 0;
+    if (r) {
+        if (!s->fused || c.worklist) return -1;
+        so.t0 = r->t0;
+        if (r->n > 0) {
+            tile::launch_fused(s->precision, c.FPl, so, r->stream ? r->stream : st, r->pdl, r->n, r->n);
+            ++n; mark(KK_STAGE);
+        }
+        c.out = out_s;
+        if (r->last) c.in = out_s;
+        return n;
+    }
     if (c.grads) { tile::launch_gradlim(s->precision, TP, so, st, k == 0, pdl); ++n; mark(KK_GRADLIM); }
     if (TP.P.smooth) {
         // time derivatives, two Jacobi sweeps of smoothing, then the update

@@ -555,7 +555,7 @@ __device__ __forceinline__ bool fused_tile(const FusedParams& FP, const TileIO& 
 template <class M, int FLUX>
 __global__ void __launch_bounds__(kTileMax) k_tile_fused(FusedParams FP, TileIO io) {
     pdl_trigger();
-    fused_tile<M, FLUX>(FP, io, blockIdx.x);
+    fused_tile<M, FLUX>(FP, io, io.t0 + (int)blockIdx.x);
 }
 
 // Work-list schedule: as many CTAs as fit on the device at once, each taking

@@ -33,35 +33,81 @@
 namespace fvgpu {
 namespace {
 
-// parts' minimum dt key and reference cell 0's dt (bits), one record per part
-__global__ void k_part_dtrec(const unsigned long long* __restrict__ keys, const double* __restrict__ dt, int cell0,
-                             unsigned long long* __restrict__ rec) {
-    unsigned long long k = keys[threadIdx.x] < keys[threadIdx.x + 32] ? keys[threadIdx.x] : keys[threadIdx.x + 32];
+// Per-part pointers of the local parts, passed by value to the merged
+// small kernels (block j serves local part j).
+constexpr int kMaxLocal = 16;
+struct PartPtrs {
+    unsigned long long* keys[kMaxLocal];   // the part's dt key slots
+    double* dt[kMaxLocal];                 // its dt array (extra slot at n_total)
+    const double* partials[kMaxLocal];     // its residual partial sums [n_tiles][V]
+    uint32_t* out[kMaxLocal];              // this stage's output state
+    int n_total[kMaxLocal];
+    int cell0[kMaxLocal];                  // local index of reference cell 0, -1: not here
+    int n_tiles[kMaxLocal];
+};
+
+__device__ __forceinline__ unsigned long long warp_kmin(unsigned long long k) {
     for (int o = 16; o > 0; o >>= 1) {
         const unsigned long long x = __shfl_xor_sync(0xffffffffu, k, o);
         k = x < k ? x : k;
     }
+    return k;
+}
+
+// each local part's minimum dt key and reference cell 0's dt (bits): one
+// record per part, block j = local part j (32 threads)
+__global__ void k_group_dtrec(PartPtrs pp, unsigned long long* __restrict__ recs) {
+    const int j = blockIdx.x;
+    const unsigned long long* keys = pp.keys[j];
+    unsigned long long k = keys[threadIdx.x] < keys[threadIdx.x + 32] ? keys[threadIdx.x] : keys[threadIdx.x + 32];
+    k = warp_kmin(k);
     if (threadIdx.x == 0) {
-        rec[0] = k;
-        rec[1] = cell0 >= 0 ? (unsigned long long)__double_as_longlong(dt[cell0]) : 0ull;
+        recs[2 * j] = k;
+        recs[2 * j + 1] = pp.cell0[j] >= 0 ? (unsigned long long)__double_as_longlong(pp.dt[j][pp.cell0[j]]) : 0ull;
     }
 }
 
-// the global minimum into every key slot of a part; reference cell 0's dt
-// into the part's extra dt slot when another part owns that cell
-__global__ void k_part_dtcombine(const unsigned long long* __restrict__ recs, int n_parts, int owner0, int is_owner,
-                                 unsigned long long* __restrict__ keys, double* __restrict__ dt_extra) {
+// the minimum over every part's record into every key slot of local part j,
+// and reference cell 0's dt into its extra dt slot when another part owns
+// that cell (block j, kDtSlots threads)
+__global__ void k_group_dtcombine(PartPtrs pp, const unsigned long long* __restrict__ recs, int n_parts, int owner0) {
+    const int j = blockIdx.x;
     unsigned long long k = ~0ull;
     for (int p = 0; p < n_parts; ++p) k = recs[2 * p] < k ? recs[2 * p] : k;
-    keys[threadIdx.x] = k;
-    if (threadIdx.x == 0 && !is_owner) *dt_extra = __longlong_as_double((long long)recs[2 * owner0 + 1]);
+    pp.keys[j][threadIdx.x] = k;
+    if (threadIdx.x == 0 && pp.cell0[j] < 0)
+        pp.dt[j][pp.n_total[j]] = __longlong_as_double((long long)recs[2 * owner0 + 1]);
 }
 
-// a part's residual partial sums, reduced in a fixed order
+// without a communicator: records and combine in one block over all local
+// parts (kDtSlots threads, thread t reads key slot t of every part)
+__global__ void k_group_dt_local(PartPtrs pp, int nl) {
+    __shared__ unsigned long long wmin[kDtSlots / 32];
+    __shared__ unsigned long long d0;
+    unsigned long long k = ~0ull;
+    for (int j = 0; j < nl; ++j) {
+        const unsigned long long x = pp.keys[j][threadIdx.x];
+        k = x < k ? x : k;
+        if (threadIdx.x == 0 && pp.cell0[j] >= 0) d0 = (unsigned long long)__double_as_longlong(pp.dt[j][pp.cell0[j]]);
+    }
+    k = warp_kmin(k);
+    if ((threadIdx.x & 31) == 0) wmin[threadIdx.x >> 5] = k;
+    __syncthreads();
+    k = wmin[0];
+    for (int w = 1; w < kDtSlots / 32; ++w) k = wmin[w] < k ? wmin[w] : k;
+    for (int j = 0; j < nl; ++j) {
+        pp.keys[j][threadIdx.x] = k;
+        if (threadIdx.x == 0 && pp.cell0[j] < 0) pp.dt[j][pp.n_total[j]] = __longlong_as_double((long long)d0);
+    }
+}
+
+// each local part's residual partial sums, reduced in a fixed order (block j)
 constexpr int kSumBlock = 256;
-__global__ void __launch_bounds__(kSumBlock) k_part_sum(const double* __restrict__ partials, int n, int V,
-                                                        double* __restrict__ out) {
+__global__ void __launch_bounds__(kSumBlock) k_group_psum(PartPtrs pp, int V, double* __restrict__ out) {
     __shared__ double red[kSumBlock / 32][kMaxV];
+    const int j = blockIdx.x;
+    const double* partials = pp.partials[j];
+    const int n = pp.n_tiles[j];
     double s[kMaxV] = {0, 0, 0, 0};
     for (int b = threadIdx.x; b < n; b += blockDim.x)
         for (int k = 0; k < V; ++k) s[k] += partials[(size_t)b * V + k];
@@ -77,27 +123,33 @@ __global__ void __launch_bounds__(kSumBlock) k_part_sum(const double* __restrict
             for (int o = 16; o > 0; o >>= 1) s[k] += __shfl_xor_sync(0xffffffffu, s[k], o);
         }
         if (lane == 0)
-            for (int k = 0; k < V; ++k) out[k] = s[k];
+            for (int k = 0; k < V; ++k) out[(size_t)j * V + k] = s[k];
     }
 }
 
-// halo states of `words` 32-bit words per cell: dst[i] = src[idx[i]] (pack)
-// or dst[idx[i]] = src[i] (unpack), one thread per word
-__global__ void k_pack(const uint32_t* __restrict__ src, const int32_t* __restrict__ idx, uint32_t* __restrict__ dst,
-                       int64_t n, int words) {
+// halo states of `words` 32-bit words per cell.  Pack: send[i] = the state
+// of local cell src[i] of local part part[i].  Unpack: the state of local
+// cell dst[i] of local part part[i] = recv[from[i]] (from >= 0) or
+// send[~from[i]] (a part of this process, read straight from its pack).
+// One thread per word.
+__global__ void k_group_pack(PartPtrs pp, const int32_t* __restrict__ part, const int32_t* __restrict__ src,
+                             uint32_t* __restrict__ send, int64_t n, int words) {
     const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= n * words) return;
     const int64_t i = t / words;
     const int w = (int)(t - i * words);
-    dst[t] = src[(int64_t)idx[i] * words + w];
+    send[t] = pp.out[part[i]][(int64_t)src[i] * words + w];
 }
-__global__ void k_unpack(const uint32_t* __restrict__ src, const int32_t* __restrict__ idx, uint32_t* __restrict__ dst,
-                         int64_t n, int words) {
+__global__ void k_group_unpack(PartPtrs pp, const int32_t* __restrict__ part, const int32_t* __restrict__ dst,
+                               const int64_t* __restrict__ from, const uint32_t* __restrict__ send,
+                               const uint32_t* __restrict__ recv, int64_t n, int words) {
     const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= n * words) return;
     const int64_t i = t / words;
     const int w = (int)(t - i * words);
-    dst[(int64_t)idx[i] * words + w] = src[t];
+    const int64_t f = from[i];
+    const uint32_t v = f >= 0 ? recv[f * words + w] : send[(~f) * words + w];
+    pp.out[part[i]][(int64_t)dst[i] * words + w] = v;
 }
 int blocks_of(int64_t n) { return (int)((n + kBlock - 1) / kBlock); }
 
@@ -111,14 +163,31 @@ struct fv_group {
     int owner0 = 0;
     int64_t g_real = 0, g_total = 0;
     cudaStream_t stream = nullptr;
+    // overlap: each stage computes the band tiles (every state another part
+    // reads) and then the exchange on cstream (high priority) while the
+    // interior tiles compute on stream
+    bool overlap = false;
+    cudaStream_t cstream = nullptr;
+    cudaEvent_t ev_start = nullptr, ev_halo = nullptr;
+    std::vector<int> band_tiles;         // per local part
     const NcclApi* nccl = nullptr;
     ncclComm_t comm = nullptr;
     // local parts [lo, hi): meshes, solvers, plans and exchange buffers
     std::vector<fv_mesh*> meshes;
     std::vector<fv_solver*> parts;
     std::vector<PartPlan> plans;
-    std::vector<int32_t*> send_idx, recv_idx;
-    std::vector<void*> send_buf, recv_buf;
+    // the flat pack / unpack lists over the local parts and their buffers
+    int64_t n_pack = 0, n_unpack = 0, n_recv = 0;
+    int32_t *pack_part = nullptr, *pack_src = nullptr, *unpack_part = nullptr, *unpack_dst = nullptr;
+    int64_t* unpack_from = nullptr;
+    void *send_all = nullptr, *recv_all = nullptr;
+    std::vector<int64_t> pack_off;       // [local parts + 1] each part's run of the pack list
+    // NCCL messages in the order every process issues them: (peer rank,
+    // send (1) or receive (0), offset in cells into send_all / recv_all, cells)
+    struct Msg { int peer, send; int64_t off, n; };
+    std::vector<Msg> msgs;
+    fvgpu::PartPtrs pp{};
+    std::vector<GraphEntry> graphs;
     unsigned long long* recs = nullptr;  // [n_parts][2]
     double* sums = nullptr;              // [n_parts][V]
     std::vector<void*> allocs;
@@ -137,10 +206,16 @@ struct fv_group {
     ~fv_group() {
         cudaSetDevice(device);
         if (stream) cudaStreamSynchronize(stream);
+        // graphs that hold NCCL calls go before their communicator
+        for (auto& e : graphs)
+            if (e.exec) cudaGraphExecDestroy(e.exec);
         if (comm && nccl) nccl->CommDestroy(comm);
         for (fv_solver* s : parts) fv_solver_destroy(s);
         for (fv_mesh* m : meshes) delete m;
         for (void* p : allocs) cudaFree(p);
+        if (ev_start) cudaEventDestroy(ev_start);
+        if (ev_halo) cudaEventDestroy(ev_halo);
+        if (cstream) cudaStreamDestroy(cstream);
         if (stream) cudaStreamDestroy(stream);
     }
 };
@@ -162,63 +237,28 @@ using fvgpu::set_error;
                                               (g)->nccl->GetErrorString(r_));                 \
     } while (0)
 
-// pack, move and unpack the halo states of the stage outputs out[j]
-int halo_exchange(fv_group* g, const std::vector<void*>& out) {
-    cudaStream_t st = g->stream;
-    const int P = g->n_parts, words = (int)(g->V * g->parts[0]->ssz / 4);
+// pack, move and unpack the halo states of this stage's outputs (pp.out) on st
+int halo_exchange(fv_group* g, cudaStream_t st) {
+    const int words = (int)(g->V * g->parts[0]->ssz / 4);
     const size_t cell_bytes = (size_t)words * 4;
-    for (size_t j = 0; j < g->parts.size(); ++j) {
-        const int64_t n = g->plans[j].send_off[P];
-        if (n > 0)
-            fvgpu::k_pack<<<fvgpu::blocks_of(n * words), fvgpu::kBlock, 0, st>>>(
-                (const uint32_t*)out[j], g->send_idx[j], (uint32_t*)g->send_buf[j], n, words);
-    }
+    if (g->n_pack > 0)
+        fvgpu::k_group_pack<<<fvgpu::blocks_of(g->n_pack * words), fvgpu::kBlock, 0, st>>>(
+            g->pp, g->pack_part, g->pack_src, (uint32_t*)g->send_all, g->n_pack, words);
     GK(cudaGetLastError());
-    // parts of this process: device copies (unless routed through NCCL)
-    if (!g->nccl_local) {
-        for (int s = g->lo; s < g->hi; ++s)
-            for (int r = g->lo; r < g->hi; ++r) {
-                if (s == r) continue;
-                const PartPlan &ps = g->plans[s - g->lo], &pr = g->plans[r - g->lo];
-                const int64_t n = ps.send_off[r + 1] - ps.send_off[r];
-                if (n == 0) continue;
-                GK(cudaMemcpyAsync((char*)g->recv_buf[r - g->lo] + pr.recv_off[s] * cell_bytes,
-                                   (const char*)g->send_buf[s - g->lo] + ps.send_off[r] * cell_bytes, n * cell_bytes,
-                                   cudaMemcpyDeviceToDevice, st));
-            }
-    }
-    if (g->comm) {
-        // every pair (s, r) in the same order on every process, so that the
-        // k-th send to a peer meets the k-th receive from it
+    if (!g->msgs.empty()) {
         NK(g, GroupStart());
-        for (int s = 0; s < P; ++s)
-            for (int r = 0; r < P; ++r) {
-                if (s == r) continue;
-                const int ls = g->local(s), lr = g->local(r);
-                if (ls >= 0 && lr >= 0 && !g->nccl_local) continue;
-                if (ls >= 0) {
-                    const PartPlan& ps = g->plans[ls];
-                    const int64_t n = ps.send_off[r + 1] - ps.send_off[r];
-                    if (n > 0)
-                        NK(g, Send((const char*)g->send_buf[ls] + ps.send_off[r] * cell_bytes, n * cell_bytes, ncclUint8,
-                                   g->rank_of(r), g->comm, st));
-                }
-                if (lr >= 0) {
-                    const PartPlan& pr = g->plans[lr];
-                    const int64_t n = pr.recv_off[s + 1] - pr.recv_off[s];
-                    if (n > 0)
-                        NK(g, Recv((char*)g->recv_buf[lr] + pr.recv_off[s] * cell_bytes, n * cell_bytes, ncclUint8,
-                                   g->rank_of(s), g->comm, st));
-                }
-            }
+        for (const auto& m : g->msgs) {
+            if (m.send)
+                NK(g, Send((const char*)g->send_all + m.off * cell_bytes, m.n * cell_bytes, ncclUint8, m.peer, g->comm, st));
+            else
+                NK(g, Recv((char*)g->recv_all + m.off * cell_bytes, m.n * cell_bytes, ncclUint8, m.peer, g->comm, st));
+        }
         NK(g, GroupEnd());
     }
-    for (size_t j = 0; j < g->parts.size(); ++j) {
-        const int64_t n = g->plans[j].recv_off[P];
-        if (n > 0)
-            fvgpu::k_unpack<<<fvgpu::blocks_of(n * words), fvgpu::kBlock, 0, st>>>(
-                (const uint32_t*)g->recv_buf[j], g->recv_idx[j], (uint32_t*)out[j], n, words);
-    }
+    if (g->n_unpack > 0)
+        fvgpu::k_group_unpack<<<fvgpu::blocks_of(g->n_unpack * words), fvgpu::kBlock, 0, st>>>(
+            g->pp, g->unpack_part, g->unpack_dst, g->unpack_from, (const uint32_t*)g->send_all,
+            (const uint32_t*)g->recv_all, g->n_unpack, words);
     GK(cudaGetLastError());
     return FV_OK;
 }
@@ -231,39 +271,91 @@ int64_t group_step(fv_group* g, const std::vector<double>& alpha, int b, bool fi
     std::vector<StepCursor> cur(nl);
     int64_t n = 0;
     for (int j = 0; j < nl; ++j) n += step_open(g->parts[j], alpha, b, first, cur[j], nullptr);
-    for (int j = 0; j < nl; ++j) {
-        fv_solver* s = g->parts[j];
-        fvgpu::k_part_dtrec<<<1, 32, 0, st>>>(s->keys, s->dt, g->plans[j].cell0, g->recs + 2 * (g->lo + j));
-        ++n;
-    }
-    if (g->comm) NK(g, AllGather(g->recs + 2 * g->lo, g->recs, (size_t)2 * nl, ncclUint64, g->comm, st));
-    for (int j = 0; j < nl; ++j) {
-        fv_solver* s = g->parts[j];
-        fvgpu::k_part_dtcombine<<<1, fvgpu::kDtSlots, 0, st>>>(g->recs, P, g->owner0, g->plans[j].cell0 >= 0 ? 1 : 0,
-                                                              s->keys, s->dt + s->n_total);
-        ++n;
+    if (g->comm) {
+        fvgpu::k_group_dtrec<<<nl, 32, 0, st>>>(g->pp, g->recs + 2 * g->lo);
+        NK(g, AllGather(g->recs + 2 * g->lo, g->recs, (size_t)2 * nl, ncclUint64, g->comm, st));
+        fvgpu::k_group_dtcombine<<<nl, fvgpu::kDtSlots, 0, st>>>(g->pp, g->recs, P, g->owner0);
+        n += 2;
+    } else {
+        fvgpu::k_group_dt_local<<<1, fvgpu::kDtSlots, 0, st>>>(g->pp, nl);
+        n += 1;
     }
     GK(cudaGetLastError());
-    std::vector<void*> out(nl);
     for (int k = 0; k < (int)alpha.size(); ++k) {
-        for (int j = 0; j < nl; ++j) {
-            n += step_stage(g->parts[j], alpha, k, cur[j], nullptr);
-            out[j] = cur[j].out;
+        if (g->overlap) {
+            // band tiles, pack, exchange and unpack on cstream, beside the
+            // interior tiles on st; both start once the previous stage and
+            // its exchange are complete (the first launch on each stream
+            // follows a join, so it waits without PDL).  The two write
+            // disjoint cells and read only the stage's input.
+            GK(cudaEventRecord(g->ev_start, st));
+            GK(cudaStreamWaitEvent(g->cstream, g->ev_start, 0));
+            for (int j = 0; j < nl; ++j) {
+                const TileRange r{0, g->band_tiles[j], j > 0, false, g->cstream};
+                const int m = step_stage(g->parts[j], alpha, k, cur[j], nullptr, &r);
+                if (m < 0) return set_error(FV_ERR_ARG, "internal error: ranged stage launch");
+                n += m;
+                g->pp.out[j] = (uint32_t*)cur[j].out;
+            }
+            int rc = halo_exchange(g, g->cstream);
+            if (rc) return rc;
+            GK(cudaEventRecord(g->ev_halo, g->cstream));
+            for (int j = 0; j < nl; ++j) {
+                const TileRange r{g->band_tiles[j], g->parts[j]->n_tiles - g->band_tiles[j], j > 0, true, st};
+                const int m = step_stage(g->parts[j], alpha, k, cur[j], nullptr, &r);
+                if (m < 0) return set_error(FV_ERR_ARG, "internal error: ranged stage launch");
+                n += m;
+            }
+            GK(cudaStreamWaitEvent(st, g->ev_halo, 0));
+        } else {
+            for (int j = 0; j < nl; ++j) {
+                n += step_stage(g->parts[j], alpha, k, cur[j], nullptr);
+                g->pp.out[j] = (uint32_t*)cur[j].out;
+            }
+            int rc = halo_exchange(g, st);
+            if (rc) return rc;
         }
-        int rc = halo_exchange(g, out);
-        if (rc) return rc;
-        n += 2 * nl;
+        n += (g->n_pack > 0) + (g->n_unpack > 0);
     }
-    for (int j = 0; j < nl; ++j) {
-        fv_solver* s = g->parts[j];
-        fvgpu::k_part_sum<<<1, fvgpu::kSumBlock, 0, st>>>(s->partials, s->n_tiles, g->V, g->sums + (size_t)g->V * (g->lo + j));
-        ++n;
-    }
+    fvgpu::k_group_psum<<<nl, fvgpu::kSumBlock, 0, st>>>(g->pp, g->V, g->sums + (size_t)g->V * g->lo);
+    ++n;
     if (g->comm)
         NK(g, AllGather(g->sums + (size_t)g->V * g->lo, g->sums, (size_t)g->V * nl, ncclFloat64, g->comm, st));
     for (int j = 0; j < nl; ++j) n += step_close(g->parts[j], g->sums, P, nullptr);
     GK(cudaGetLastError());
     return n;
+}
+
+// One captured graph of `len` consecutive steps (the first begins with the
+// begin-of-step kernel; RK1 alternates the base state between steps).
+int group_graph(fv_group* g, const std::vector<double>& alpha, int len, GraphEntry** out) {
+    for (auto& e : g->graphs)
+        if (e.alpha == alpha && e.chunk == len) { *out = &e; return FV_OK; }
+    GraphEntry e;
+    e.alpha = alpha;
+    e.chunk = len;
+    cudaGraph_t graph;
+    GK(cudaStreamBeginCapture(g->stream, cudaStreamCaptureModeThreadLocal));
+    int64_t launches = 0;
+    int rc = FV_OK;
+    for (int k = 0; k < len && rc == FV_OK; ++k) {
+        const int64_t n = group_step(g, alpha, (alpha.size() == 1 && (k % 2)) ? 1 : 0, k == 0);
+        if (n < 0) rc = (int)n;
+        else launches += n;
+    }
+    cudaError_t ce = cudaStreamEndCapture(g->stream, &graph);
+    if (rc) {
+        if (ce == cudaSuccess) cudaGraphDestroy(graph);
+        return rc;
+    }
+    if (ce != cudaSuccess) return set_error(FV_ERR_CUDA, std::string("group graph capture: ") + cudaGetErrorString(ce));
+    ce = cudaGraphInstantiate(&e.exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ce != cudaSuccess) return set_error(FV_ERR_CUDA, std::string("group graph instantiate: ") + cudaGetErrorString(ce));
+    e.launches = (int)launches;
+    g->graphs.push_back(e);
+    *out = &g->graphs.back();
+    return FV_OK;
 }
 
 // RK1 leaves the state in qbase[1] after an odd number of steps
@@ -304,6 +396,7 @@ int fv_mesh_partition_sizes(const fv_mesh* m, int32_t n_parts, int32_t part, int
     sizes[5] = plan.cell0; sizes[6] = plan.owner0;
     sizes[7] = plan.recv_off[n_parts]; sizes[8] = plan.send_off[n_parts];
     sizes[9] = L.n_bound;
+    sizes[10] = plan.n_band;
     return FV_OK;
 }
 
@@ -353,38 +446,109 @@ int fv_group_create(const fv_mesh* fm, const fv_physics* ph, int32_t precision, 
         std::string err = build_part(fm->m, P, p, lm->m, plan);
         if (!err.empty()) return set_error(FV_ERR_ARG, err);
         fv_solver* s = nullptr;
-        int rc = fv_solver_create_ex(lm.get(), ph, precision, device, &so, &s);
-        if (rc) return rc;
+        int rc0 = fv_solver_create_ex(lm.get(), ph, precision, device, &so, &s);
+        if (rc0) return rc0;
         g->meshes.push_back(lm.release());
         g->parts.push_back(s);
         // reference cell 0: its own dt where this part owns it, else the
         // extra dt slot past the ghosts that the combine kernel fills
         s->TP.P.cell0 = plan.cell0 >= 0 ? plan.cell0 : (int)s->n_total;
         g->owner0 = plan.owner0;
-        if ((rc = fv_solver_set_stream(s, g->stream))) return rc;
-        int32_t *si = nullptr, *ri = nullptr;
-        void *sb = nullptr, *rb = nullptr;
-        const size_t cell_bytes = (size_t)ph->V * s->ssz;
-        GK(g->alloc(&si, plan.send_idx.size()));
-        GK(g->alloc(&ri, plan.recv_idx.size()));
-        GK(g->alloc((char**)&sb, plan.send_idx.size() * cell_bytes));
-        GK(g->alloc((char**)&rb, plan.recv_idx.size() * cell_bytes));
-        if (!plan.send_idx.empty())
-            GK(cudaMemcpy(si, plan.send_idx.data(), plan.send_idx.size() * 4, cudaMemcpyHostToDevice));
-        if (!plan.recv_idx.empty())
-            GK(cudaMemcpy(ri, plan.recv_idx.data(), plan.recv_idx.size() * 4, cudaMemcpyHostToDevice));
-        g->send_idx.push_back(si); g->recv_idx.push_back(ri);
-        g->send_buf.push_back(sb); g->recv_buf.push_back(rb);
+        if ((rc0 = fv_solver_set_stream(s, g->stream))) return rc0;
         g->halo_cells += (int64_t)plan.recv_idx.size();
         g->plans.push_back(std::move(plan));
     }
-    for (fv_solver* s : g->parts)
+    const int nl = (int)g->parts.size();
+    if (nl > fvgpu::kMaxLocal) return set_error(FV_ERR_ARG, "at most 16 parts per process");
+    for (int j = 0; j < nl; ++j) {
+        fv_solver* s = g->parts[j];
         if (ph->order2 && !s->fused)
             return set_error(FV_ERR_MESH, "a part's two-ring tiles do not fit the fused stage kernel");
+        g->pp.keys[j] = s->keys;
+        g->pp.dt[j] = s->dt;
+        g->pp.partials[j] = s->partials;
+        g->pp.n_total[j] = (int)s->n_total;
+        g->pp.cell0[j] = g->plans[j].cell0;
+        g->pp.n_tiles[j] = s->n_tiles;
+    }
+    // the pack list: each local part's send list (by destination), in turn
+    std::vector<int32_t> pk_part, pk_src, up_part, up_dst;
+    std::vector<int64_t> up_from;
+    g->pack_off.assign(nl + 1, 0);
+    for (int j = 0; j < nl; ++j) {
+        g->pack_off[j] = (int64_t)pk_src.size();
+        for (int32_t c : g->plans[j].send_idx) { pk_part.push_back(j); pk_src.push_back(c); }
+    }
+    g->pack_off[nl] = (int64_t)pk_src.size();
+    // messages and receive slots, pair (s, r) in the same order on every
+    // process; pairs within this process read the sender's pack directly
+    const bool use_comm = R > 1 || g->nccl_local;
+    int64_t n_recv = 0;
+    for (int sp = 0; sp < P; ++sp)
+        for (int rp = 0; rp < P; ++rp) {
+            if (sp == rp) continue;
+            const int ls = g->local(sp), lr = g->local(rp);
+            const bool wire = use_comm && !(ls >= 0 && lr >= 0 && !g->nccl_local);
+            if (ls >= 0 && wire) {
+                const PartPlan& ps = g->plans[ls];
+                const int64_t n = ps.send_off[rp + 1] - ps.send_off[rp];
+                if (n > 0) g->msgs.push_back({g->rank_of(rp), 1, g->pack_off[ls] + ps.send_off[rp], n});
+            }
+            if (lr >= 0) {
+                const PartPlan& pr = g->plans[lr];
+                const int64_t n = pr.recv_off[sp + 1] - pr.recv_off[sp];
+                if (n == 0) continue;
+                for (int64_t i = 0; i < n; ++i) {
+                    up_part.push_back(lr);
+                    up_dst.push_back(pr.recv_idx[pr.recv_off[sp] + i]);
+                }
+                if (wire) {
+                    g->msgs.push_back({g->rank_of(sp), 0, n_recv, n});
+                    for (int64_t i = 0; i < n; ++i) up_from.push_back(n_recv + i);
+                    n_recv += n;
+                } else {
+                    const PartPlan& ps = g->plans[ls];
+                    if (ps.send_off[rp + 1] - ps.send_off[rp] != n)
+                        return set_error(FV_ERR_ARG, "internal error: send and receive lists differ");
+                    for (int64_t i = 0; i < n; ++i) up_from.push_back(~(g->pack_off[ls] + ps.send_off[rp] + i));
+                }
+            }
+        }
+    g->n_pack = (int64_t)pk_src.size();
+    g->n_unpack = (int64_t)up_dst.size();
+    g->n_recv = n_recv;
+    const size_t cell_bytes = (size_t)ph->V * g->parts[0]->ssz;
+    auto up = [&](auto** d, const auto& v) -> int {
+        GK(g->alloc(d, v.size()));
+        if (!v.empty()) GK(cudaMemcpy(*d, v.data(), v.size() * sizeof(v[0]), cudaMemcpyHostToDevice));
+        return FV_OK;
+    };
+    int rc;
+    if ((rc = up(&g->pack_part, pk_part)) || (rc = up(&g->pack_src, pk_src)) || (rc = up(&g->unpack_part, up_part)) ||
+        (rc = up(&g->unpack_dst, up_dst)) || (rc = up(&g->unpack_from, up_from)))
+        return rc;
+    GK(g->alloc((char**)&g->send_all, (size_t)g->n_pack * cell_bytes));
+    GK(g->alloc((char**)&g->recv_all, (size_t)n_recv * cell_bytes));
+    // the band-first stage: fused parts with one CTA per tile, and
+    // something to exchange
+    g->overlap = o->serial_exchange == 0 && (g->n_pack > 0 || g->n_unpack > 0);
+    for (int j = 0; j < nl; ++j) {
+        fv_solver* s = g->parts[j];
+        if (!s->fused || s->sched == FV_SCHED_WORKLIST) g->overlap = false;
+        const int T = s->fused ? s->FPm.T : 1;
+        g->band_tiles.push_back((int)std::min<int64_t>((g->plans[j].n_band + T - 1) / T, s->n_tiles));
+    }
+    if (g->overlap) {
+        int lo_pri = 0, hi_pri = 0;
+        GK(cudaDeviceGetStreamPriorityRange(&lo_pri, &hi_pri));
+        GK(cudaStreamCreateWithPriority(&g->cstream, cudaStreamNonBlocking, hi_pri));
+        GK(cudaEventCreateWithFlags(&g->ev_start, cudaEventDisableTiming));
+        GK(cudaEventCreateWithFlags(&g->ev_halo, cudaEventDisableTiming));
+    }
     GK(g->alloc(&g->recs, (size_t)2 * P));
     GK(g->alloc(&g->sums, (size_t)ph->V * P));
     GK(cudaMemset(g->sums, 0, sizeof(double) * ph->V * P));
-    if (R > 1 || g->nccl_local) {
+    if (use_comm) {
         std::string why;
         g->nccl = nccl_api(&why);
         if (!g->nccl) return set_error(FV_ERR_COMM, why);
@@ -478,15 +642,18 @@ int fv_group_run(fv_group* g, const fv_run_options* o, fv_run_info* info) {
     unsigned long long cur = start;
     int rc = FV_OK;
     for (;;) {
+        // graph length: the largest power of two <= min(chunk, steps left)
         const unsigned long long left = o->max_step > cur ? o->max_step - cur : 1ull;
-        const int len = (int)std::min<unsigned long long>(left, (unsigned long long)s0->chunk);
+        int len = 1;
+        while ((unsigned long long)(len * 2) <= left && len * 2 <= s0->chunk) len *= 2;
+        GraphEntry* ge = nullptr;
+        if ((rc = group_graph(g, alpha, len, &ge))) break;
         cudaEventRecord(e0, st);
-        for (int k = 0; k < len && rc == FV_OK; ++k) {
-            const int64_t n = group_step(g, alpha, (alpha.size() == 1 && (k % 2)) ? 1 : 0, k == 0);
-            if (n < 0) rc = (int)n;
-            else launches += n;
+        if (cudaGraphLaunch(ge->exec, st) != cudaSuccess) {
+            rc = set_error(FV_ERR_CUDA, "fv_group_run: graph launch");
+            break;
         }
-        if (rc) break;
+        launches += ge->launches;
         cudaEventRecord(e1, st);
         launch_ctrl_copy(s0->ctrl, s0->hctrl_dev, st);
         if (cudaGetLastError() != cudaSuccess || cudaStreamSynchronize(st) != cudaSuccess) {
@@ -543,6 +710,9 @@ int fv_group_info(fv_group* g, int64_t* out) {
     out[3] = sent;
     out[4] = tiles;
     out[5] = g->comm != nullptr ? 1 : 0;
+    int64_t band = 0;
+    for (int b : g->band_tiles) band += b;
+    out[6] = g->overlap ? band : -1;
     return FV_OK;
 }
 

@@ -585,13 +585,26 @@ std::string build_part(const HostMesh& g, int n_parts, int part, HostMesh& L, Pa
     const int64_t a = plan.own_off[part], b = plan.own_off[part + 1];
     const int64_t ga = plan.ghost_off[part], gb = plan.ghost_off[part + 1];
     plan.n_own = b - a;
+    // owned cells in other parts' halos (the band) first, so that the first
+    // tiles compute every state this part sends; each group in device order
+    std::vector<uint8_t> band(b - a, 0);
+    for (int r = 0; r < n_parts; ++r)
+        if (r != part)
+            for (int32_t d : halos[r].real)
+                if (d >= a && d < b) band[d - a] = 1;
+    std::vector<int32_t> own_order;
+    own_order.reserve(b - a);
+    for (int pass = 1; pass >= 0; --pass)
+        for (int64_t i = 0; i < b - a; ++i)
+            if (band[i] == pass) own_order.push_back((int32_t)(a + i));
+    plan.n_band = (int64_t)std::count(band.begin(), band.end(), (uint8_t)1);
     plan.n_own_ghost = gb - ga;
     const int64_t nr = plan.n_own + (int64_t)H.real.size();
     const int64_t nbl = plan.n_own_ghost + (int64_t)H.ghost.size();
     // local numbering: owned cells, halo cells (grouped by owner), owned
     // ghosts, halo ghosts (grouped by owner); each group in device order
     std::vector<int32_t> dev_of(nr + nbl);   // device index (ghosts: N + offset) of each local cell
-    for (int64_t i = 0; i < plan.n_own; ++i) dev_of[i] = (int32_t)(a + i);
+    for (int64_t i = 0; i < plan.n_own; ++i) dev_of[i] = own_order[i];
     for (size_t i = 0; i < H.real.size(); ++i) dev_of[plan.n_own + i] = H.real[i];
     for (int64_t i = 0; i < plan.n_own_ghost; ++i) dev_of[nr + i] = (int32_t)(N + ga + i);
     for (size_t i = 0; i < H.ghost.size(); ++i) dev_of[nr + plan.n_own_ghost + i] = (int32_t)(N + H.ghost[i]);
@@ -618,14 +631,14 @@ std::string build_part(const HostMesh& g, int n_parts, int part, HostMesh& L, Pa
         plan.send_off[r] = (int64_t)plan.send_idx.size();
         if (r == part) continue;
         for (int32_t d : halos[r].real)
-            if (d >= a && d < b) plan.send_idx.push_back((int32_t)(d - a));
+            if (d >= a && d < b) plan.send_idx.push_back(loc[d]);
         for (int32_t o : halos[r].ghost)
             if (o >= ga && o < gb) plan.send_idx.push_back((int32_t)(nr + (o - ga)));
     }
     plan.send_off[n_parts] = (int64_t)plan.send_idx.size();
     const int32_t d0 = g.ref2new[0];
     plan.owner0 = owner(d0);
-    plan.cell0 = plan.owner0 == part ? (int32_t)(d0 - a) : -1;
+    plan.cell0 = plan.owner0 == part ? loc[d0] : -1;
 
     // local edges: every edge of an owned or ring-1 cell, in reference edge order
     std::vector<int32_t> edges;

@@ -112,9 +112,9 @@ void build_tiles2(const HostMesh& m, const FaceArrays& fa, int tile_cells, Tile2
 // cells) and the boundary ghosts of ring 1, with every edge of an owned or
 // ring-1 cell in reference edge order, so that each owned and ring-1 cell
 // keeps all its faces in the order of the whole mesh.  Local numbering (also
-// the part's device numbering): owned cells, halo real cells, owned ghosts,
-// halo ghosts; the halo groups are sorted by device index and so grouped by
-// owner.
+// the part's device numbering): owned cells (those in other parts' halos, the
+// band, first), halo real cells, owned ghosts, halo ghosts; each group in
+// device order, so the halo groups are grouped by owner.
 struct PartPlan {
     int n_parts = 1, part = 0;
     std::vector<int64_t> own_off;     // [n_parts + 1] device real cells of each part
@@ -122,6 +122,7 @@ struct PartPlan {
     std::vector<int32_t> local2ref;   // reference index of each local cell
     std::vector<int32_t> local_edges; // reference index of each local edge, ascending
     int64_t n_own = 0, n_own_ghost = 0;
+    int64_t n_band = 0;               // owned cells [0, n_band) are in other parts' halos
     int32_t cell0 = -1;               // local index of reference cell 0, -1 if another part owns it
     int32_t owner0 = 0;               // the part that owns reference cell 0
     // halo states from part r land in local cells recv_idx[recv_off[r] .. recv_off[r+1])

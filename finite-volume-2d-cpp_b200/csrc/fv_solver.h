@@ -127,7 +127,17 @@ struct StepCursor {
     void* out = nullptr;
 };
 int step_open(fv_solver* s, const std::vector<double>& alpha, int b, bool first, StepCursor& c, EventLog* log);
-int step_stage(fv_solver* s, const std::vector<double>& alpha, int k, StepCursor& c, EventLog* log);
+// r: only tiles [r->t0, r->t0 + r->n) of the fused stage kernel (one CTA
+// per tile) on r->stream (nullptr: the solver's stream), with programmatic
+// dependent launch when r->pdl; the stage's output becomes the next stage's
+// input after the range with r->last set.
+struct TileRange {
+    int t0, n;
+    bool pdl, last;
+    cudaStream_t stream;
+};
+int step_stage(fv_solver* s, const std::vector<double>& alpha, int k, StepCursor& c, EventLog* log,
+               const TileRange* r = nullptr);
 int step_close(fv_solver* s, const double* partials, int nblocks, EventLog* log);
 
 // The library's last-error slot (fv_last_error) and its codes.

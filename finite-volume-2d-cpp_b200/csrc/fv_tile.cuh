@@ -74,6 +74,7 @@ struct TileIO {
     double* qt;                // [n_total][V] time derivatives of the smoothing phases (FP64)
     int* work;                 // fused stage kernel, work-list schedule: this launch's tile counter
     int* work_reset;           // dt kernel: tile counters zeroed after the dependency wait, or nullptr
+    int t0;                    // fused stage kernel, one CTA per tile: the first tile of this launch
 };
 constexpr int kWorkSlots = 8;  // tile counters of the work-list schedule (one per RK stage)
 

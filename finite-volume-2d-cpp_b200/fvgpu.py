@@ -198,11 +198,12 @@ class Mesh:
     def partition(self, n_parts, part):
         """Host-only plan of one part of a decomposition (fv_mesh_partition):
         a dict of its sizes and index lists."""
-        sz = np.zeros(10, np.int64)
+        sz = np.zeros(11, np.int64)
         _check(lib().fv_mesh_partition_sizes(self._h, C.c_int32(n_parts), C.c_int32(part), _p(sz, _i64p)))
-        n_real, n_total, n_edges, n_own, n_own_ghost, cell0, owner0, n_recv, n_send, n_bound = (int(v) for v in sz)
+        n_real, n_total, n_edges, n_own, n_own_ghost, cell0, owner0, n_recv, n_send, n_bound, n_band = \
+            (int(v) for v in sz)
         out = dict(n_real=n_real, n_total=n_total, n_edges=n_edges, n_own=n_own, n_own_ghost=n_own_ghost,
-                   cell0=cell0, owner0=owner0, n_bound=n_bound,
+                   cell0=cell0, owner0=owner0, n_bound=n_bound, n_band=n_band,
                    local2ref=np.zeros(n_total, np.int32), local_edges=np.zeros(n_edges, np.int32),
                    recv_off=np.zeros(n_parts + 1, np.int64), recv_idx=np.zeros(n_recv, np.int32),
                    send_off=np.zeros(n_parts + 1, np.int64), send_idx=np.zeros(n_send, np.int32))
@@ -447,7 +448,8 @@ class Group:
 
     def __init__(self, mesh: Mesh, ph: _phys.Physics, precision: str = "fp64_exact", n_parts: int = 2,
                  rank: int = 0, n_ranks: int = 1, nccl_id_bytes: Optional[bytes] = None, device: int = 0,
-                 nccl_local: bool = False, tile_cells: int = 0, schedule: str = "tile"):
+                 nccl_local: bool = False, tile_cells: int = 0, schedule: str = "tile",
+                 serial_exchange: bool = False):
         self.mesh = mesh
         self.V = ph.V
         self._ps = physics_struct(ph, mesh.group_names)
@@ -455,7 +457,7 @@ class Group:
         o = _GroupOptions(n_parts=n_parts, rank=rank, n_ranks=n_ranks,
                           nccl_id=C.cast(self._id, C.c_void_p) if self._id is not None else None,
                           nccl_local=int(nccl_local), tile_cells=int(tile_cells), stage_kernels=0,
-                          schedule=Solver.SCHEDULES[schedule])
+                          schedule=Solver.SCHEDULES[schedule], serial_exchange=int(serial_exchange))
         h = C.c_void_p()
         _check(lib().fv_group_create(mesh._h, C.byref(self._ps), C.c_int32(PREC[precision]), C.c_int32(device),
                                      C.byref(o), C.byref(h)))
@@ -487,10 +489,10 @@ class Group:
         return dict(step=info.step, time=info.time, R=np.array(info.R[: self.V]), R0=np.array(info.R0[: self.V]))
 
     def info(self):
-        out = np.zeros(6, np.int64)
+        out = np.zeros(7, np.int64)
         _check(lib().fv_group_info(self._h, _p(out, _i64p)))
         return dict(local_parts=int(out[0]), owned_cells=int(out[1]), halo_cells=int(out[2]),
-                    sent_cells=int(out[3]), tiles=int(out[4]), nccl=bool(out[5]))
+                    sent_cells=int(out[3]), tiles=int(out[4]), nccl=bool(out[5]), band_tiles=int(out[6]))
 
     def last_run_stats(self):
         ms = C.c_double(); n = C.c_int64()
@@ -512,7 +514,7 @@ class Group:
 class _GroupOptions(C.Structure):
     _fields_ = [("n_parts", C.c_int32), ("rank", C.c_int32), ("n_ranks", C.c_int32), ("nccl_id", C.c_void_p),
                 ("nccl_local", C.c_int32), ("tile_cells", C.c_int32), ("stage_kernels", C.c_int32),
-                ("schedule", C.c_int32)]
+                ("schedule", C.c_int32), ("serial_exchange", C.c_int32)]
 
 
 def solver_info(s: Solver):

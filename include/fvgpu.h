@@ -287,6 +287,11 @@ typedef struct {
     int32_t nccl_local;     /* 1: parts of this process also exchange through NCCL (to
                                itself) instead of device copies */
     fv_solver_options solver;  /* every part's tile size, stage kernels and schedule */
+    int32_t serial_exchange;   /* 0 (default): with the fused stage kernel and one CTA per
+                                  tile, each part's cells that other parts read come first;
+                                  their tiles and then the halo exchange run on a second,
+                                  high-priority stream while the remaining tiles compute.
+                                  1: the exchange follows all tiles of the stage. */
 } fv_group_options;
 int fv_group_nccl_id(void* id128);
 /* Collective over the n_ranks processes (each passes the whole mesh, its rank
@@ -301,14 +306,16 @@ int fv_group_set_state(fv_group* g, const double* q);
 int fv_group_get_state(fv_group* g, double* q);
 /* fv_run for the decomposition (collective): same options and results. */
 int fv_group_run(fv_group* g, const fv_run_options* opt, fv_run_info* info);
-/* out[6]: local parts, owned real cells, halo cells received per stage,
- * cells sent per stage, tiles, 1 if an NCCL communicator exists */
+/* out[7]: local parts, owned real cells, halo cells received per stage,
+ * cells sent per stage, tiles, 1 if an NCCL communicator exists, band tiles
+ * (computed before the exchange; -1 when the exchange follows all tiles) */
 int fv_group_info(fv_group* g, int64_t* out);
 int fv_group_last_run_stats(fv_group* g, double* device_ms, int64_t* kernel_launches);
-/* Host-only: the plan of part `part` of n_parts.  sizes[10]: local real cells,
+/* Host-only: the plan of part `part` of n_parts.  sizes[11]: local real cells,
  * local cells (with ghosts), local edges, owned real cells, owned ghosts,
  * local index of reference cell 0 (-1 if another part owns it), the part
- * that owns it, cells received and cells sent per stage, local ghosts.
+ * that owns it, cells received and cells sent per stage, local ghosts, owned
+ * cells in other parts' halos (the band: local cells [0, band)).
  * fv_mesh_partition fills (each may be NULL): local2ref [local cells]
  * reference index of each local cell (owned cells, halo cells, owned ghosts,
  * halo ghosts); local_edges [local edges] reference index of each local edge;

@@ -47,10 +47,11 @@ def test_group_equals_single_solver(case, prec, oracle):
     if prec == "fp64_exact":
         want = oracle.run_loop(g, oracle.physics(ph, em.group_names), q0, alpha, steps)
         assert q1.tobytes() == want["q"].tobytes()
-    for n_parts in (1, 2, 3, 4):
-        grp = fvgpu.Group(mesh, ph, prec, n_parts=n_parts)
+    for n_parts, serial in ((1, False), (2, False), (3, False), (4, False), (3, True)):
+        grp = fvgpu.Group(mesh, ph, prec, n_parts=n_parts, serial_exchange=serial)
         inf = grp.info()
         assert inf["local_parts"] == n_parts and inf["owned_cells"] == mesh.n_real
+        assert (inf["band_tiles"] >= 0) == (ph.order2 and not serial)
         grp.set_state(q0)
         r = grp.run(steps, alpha=alpha)
         q = grp.get_state()
@@ -61,11 +62,13 @@ def test_group_equals_single_solver(case, prec, oracle):
         np.testing.assert_allclose(r["R"], r1["R"], rtol=1e-12)
 
 
+@pytest.mark.parametrize("serial", [False, True], ids=["overlapped", "serial"])
 @pytest.mark.parametrize("prec", ["fp64_exact", "fp32"])
-def test_group_exchange_through_nccl(prec):
+def test_group_exchange_through_nccl(prec, serial):
     """The same decomposition with every exchange, dt record and residual sum
     going through NCCL (send/recv to this process, all-gathers) instead of
-    device copies."""
+    device copies, with the exchange on its own stream beside the interior
+    tiles or after all tiles."""
     import fvgpu
     mk_em, mk_ph, ic, alpha, steps = _cases()["forward_step"]
     em, ph = mk_em(), mk_ph()
@@ -73,8 +76,9 @@ def test_group_exchange_through_nccl(prec):
     q0 = P.ic_forward_step(mesh.n_total).ravel()
     r1, q1 = _single(mesh, ph, prec, q0, alpha, steps)
     for n_parts in (2, 3):
-        grp = fvgpu.Group(mesh, ph, prec, n_parts=n_parts, nccl_local=True)
-        assert grp.info()["nccl"]
+        grp = fvgpu.Group(mesh, ph, prec, n_parts=n_parts, nccl_local=True, serial_exchange=serial)
+        inf = grp.info()
+        assert inf["nccl"] and (inf["band_tiles"] < 0) == serial
         grp.set_state(q0)
         r = grp.run(steps, alpha=alpha)
         q = grp.get_state()

@@ -94,6 +94,9 @@ def test_part_plans_cover_the_mesh(case, n_parts, oracle):
             sent = l2r[pl["send_idx"][pl["send_off"][r]: pl["send_off"][r + 1]]]
             want = plans[r]["local2ref"][plans[r]["recv_idx"][plans[r]["recv_off"][p]: plans[r]["recv_off"][p + 1]]]
             assert np.array_equal(sent, want)
+        # the band (owned cells other parts read) comes first
+        sent_real = np.unique(pl["send_idx"][pl["send_idx"] < pl["n_real"]])
+        assert np.array_equal(sent_real, np.arange(pl["n_band"]))
         # every halo cell and halo ghost arrives from its owner
         recv = np.sort(l2r[pl["recv_idx"]])
         halo = np.sort(np.concatenate([l2r[pl["n_own"]: pl["n_real"]], l2r[pl["n_real"] + pl["n_own_ghost"]:]]))
