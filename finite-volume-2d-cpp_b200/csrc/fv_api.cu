@@ -1425,6 +1425,27 @@ int adj_forward_step(fv_adjoint* a, const double* q, double* q_next, double* dt_
     adj_launch_dt_finalize(a->keys, dtcells, TP.P.cell0, a->dt_fill, (int)nt, dt_slot, st);
     if (with_loss && a->n_loss) adj_launch_loss(TP.P, q, dt_slot, a->loss_ghosts, a->n_loss, a->loss, st);
     const double* in = q;
+    if (!store && s->fused) {
+        // states only: the fused stage kernel (the same bits as the
+        // gradient + stage kernels, without writing the gradients out)
+        FusedParams FPl = s->FPm;
+        FPl.P = TP.P;
+        FPl.threads = (s->sched == FV_SCHED_TILE2) ? 2 * FPl.T : FPl.T;
+        for (int k = 0; k < a->S; ++k) {
+            double* out = (k == a->S - 1) ? q_next : a->tmp[k % 2];
+            TileIO so{};
+            so.q_stage = in;
+            so.q_base = q;
+            so.q_out = out;
+            so.dt = a->dt_fill;
+            so.alpha = a->alpha[(size_t)k];
+            so.write_f64 = 1;
+            tile::launch_fused(FV_PREC_FP64_EXACT, FPl, so, st, false, s->n_tiles, s->work_grid);
+            in = out;
+        }
+        CK(cudaGetLastError());
+        return FV_OK;
+    }
     for (int k = 0; k < a->S; ++k) {
         double* gx = store ? a->Gx[(size_t)k] : a->tgx;
         double* gy = store ? a->Gy[(size_t)k] : a->tgy;
