@@ -422,10 +422,10 @@ int fv_solver_create_ex(const fv_mesh* fm, const fv_physics* ph, int32_t precisi
     {
         // one fused kernel per stage for the second-order Roe kinds
         const int sk = opt ? opt->stage_kernels : FV_STAGE_AUTO;
-        if (sk < FV_STAGE_AUTO || sk > FV_STAGE_FUSED) return fail(FV_ERR_ARG, "unknown stage_kernels");
+        if (sk < FV_STAGE_AUTO || sk > FV_STAGE_HYBRID) return fail(FV_ERR_ARG, "unknown stage_kernels");
         const bool can_fuse = ph->V == 4 && ph->order2 && (ph->flux == FV_FLUX_ROE_FS || ph->flux == FV_FLUX_ROE_ST) &&
                               !ph->diffusive && !ph->smooth_residuals;
-        if (sk == FV_STAGE_FUSED && !can_fuse)
+        if ((sk == FV_STAGE_FUSED || sk == FV_STAGE_HYBRID) && !can_fuse)
             return fail(FV_ERR_UNSUPPORTED, "the fused stage kernel needs a second-order Roe kind without "
                                             "diffusive terms or residual smoothing");
         if (can_fuse && sk != FV_STAGE_SPLIT) {
@@ -437,7 +437,7 @@ int fv_solver_create_ex(const fv_mesh* fm, const fv_physics* ph, int32_t precisi
             F.max_edges = t2.max_edges; F.max_flux = t2.max_flux;
             const bool fits = t2.max_slots <= 65535 && t2.max_edges <= kFaceEdgeMask &&
                               tile::smem_fused(precision, F) <= (size_t)227 * 1024;
-            if (!fits && sk == FV_STAGE_FUSED)
+            if (!fits && (sk == FV_STAGE_FUSED || sk == FV_STAGE_HYBRID))
                 return fail(FV_ERR_MESH, "two-ring tiles too large for the fused stage kernel at this tile size");
             if (fits) {
                 const int32_t* i2; const int32_t* h2; const uint32_t* e2; const uint16_t* f2;
@@ -470,7 +470,12 @@ int fv_solver_create_ex(const fv_mesh* fm, const fv_physics* ph, int32_t precisi
                 if (sched < FV_SCHED_TILE || sched > FV_SCHED_TILE2) return fail(FV_ERR_ARG, "unknown schedule");
                 if (sched == FV_SCHED_TILE2 && tile_cells > kTileMax / 2)
                     return fail(FV_ERR_ARG, "two threads per cell need tiles of at most 128 cells");
+                if (sk == FV_STAGE_HYBRID && sched == FV_SCHED_WORKLIST)
+                    return fail(FV_ERR_ARG, "the work-list schedule needs the dt kernel of the fused layout");
                 s->sched = sched;
+                // automatic choice: the split first stage (its gradient kernel
+                // computes dt) saves the separate dt kernel of the fused layout
+                s->split_first = sk == FV_STAGE_HYBRID || (sk == FV_STAGE_AUTO && sched != FV_SCHED_WORKLIST);
             }
         }
     }
@@ -573,13 +578,18 @@ int fv_solver_create_tuned(const fv_mesh* fm, const fv_physics* ph, int32_t prec
         if (rc == FV_ERR_MESH) continue;  // tile halo too large for this size
         if (rc) { fv_solver_destroy(best); return rc; }
         const bool can_fuse = s->fused;
-        // split; fused with FV_SCHED_TILE, FV_SCHED_WORKLIST, FV_SCHED_TILE2
-        double ms_of[4] = {1e300, 1e300, 1e300, 1e300};
-        const int top = can_fuse ? (t <= kTileMax / 2 ? 3 : 2) : 0;
-        for (int variant = top; variant >= 0; --variant) {
+        // split; fused with FV_SCHED_TILE, FV_SCHED_WORKLIST, FV_SCHED_TILE2;
+        // fused with the split first stage (FV_SCHED_TILE)
+        double ms_of[5] = {1e300, 1e300, 1e300, 1e300, 1e300};
+        auto set_variant = [&](int v) {
+            s->fused = v >= 1;
+            s->sched = (v >= 1 && v <= 3) ? v - 1 : FV_SCHED_TILE;
+            s->split_first = v == 4;
+        };
+        for (int variant = can_fuse ? 4 : 0; variant >= 0; --variant) {
+            if (variant == 3 && t > kTileMax / 2) continue;
             clear_graphs(s);
-            s->fused = variant >= 1;
-            s->sched = variant >= 1 ? variant - 1 : FV_SCHED_TILE;
+            set_variant(variant);
             // one untimed step (graph capture), then n_steps timed on the device
             fv_run_options ro{};
             ro.max_step = 1; ro.max_time = 1e300; ro.tolerance = -1.0; ro.print_interval = 1ull << 62;
@@ -590,11 +600,10 @@ int fv_solver_create_tuned(const fv_mesh* fm, const fv_physics* ph, int32_t prec
             if ((rc = fv_run(s, &ro, &info))) { fv_solver_destroy(s); fv_solver_destroy(best); return rc; }
             ms_of[variant] = s->last_ms / n_steps;
         }
-        const int v = (int)(std::min_element(ms_of, ms_of + 4) - ms_of);
+        const int v = (int)(std::min_element(ms_of, ms_of + 5) - ms_of);
         const double ms = ms_of[v];
         clear_graphs(s);
-        s->fused = v >= 1;
-        s->sched = v >= 1 ? v - 1 : FV_SCHED_TILE;
+        set_variant(v);
         if (!best || ms < best_ms) {
             fv_solver_destroy(best);
             best = s; best_ms = ms; best_t = t;
@@ -771,11 +780,13 @@ int step_open(fv_solver* s, const std::vector<double>& alpha, int b, bool first,
     // the fused stage kernel computes its gradients itself: the step's dt
     // comes from the dt kernel, as in first order
     c.grads = (TP.P.order2 || TP.P.diffusive) && !s->fused;
+    // the split first stage's gradient kernel computes dt
+    c.split_first = s->fused && s->split_first;
     // the work-list schedule: one tile counter per stage, zeroed by the dt kernel
     c.worklist = s->fused && s->sched == FV_SCHED_WORKLIST && alpha.size() <= (size_t)kWorkSlots;
     // every kernel after step_begin is a programmatic dependent of the one
     // before it (its constant tile data is staged during that one's tail)
-    if (!c.grads) {
+    if (!c.grads && !c.split_first) {
         TileIO dio = io;
         dio.work_reset = c.worklist ? s->work : nullptr;
         tile::launch_dt(s->precision, TP, dio, st, true); ++n; mark(KK_DT);
@@ -816,11 +827,11 @@ int step_stage(fv_solver* s, const std::vector<double>& alpha, int k, StepCursor
     so.s_out = s->f32 ? out_s : nullptr;
     so.write_f64 = last ? 1 : 0;
     if (r) {
-        if (!s->fused || c.worklist) return -1;
+        if (!s->fused || c.worklist || c.split_first) return -1;
         so.t0 = r->t0;
         if (r->n > 0) {
             tile::launch_fused(s->precision, c.FPl, so, r->stream ? r->stream : st, r->pdl, r->n, r->n);
-            ++n; mark(KK_STAGE);
+            ++n; mark(KK_FUSED);
         }
         c.out = out_s;
         if (r->last) c.in = out_s;
@@ -836,9 +847,12 @@ int step_stage(fv_solver* s, const std::vector<double>& alpha, int k, StepCursor
         launch_smooth(TP.P, s->nbr, s->qts[1], s->qts[0], s->qts[2], st); ++n; mark(KK_STAGE);
         so.qt = s->qts[2];
         tile::launch_stage(s->precision, TP, so, st, pdl, 2); ++n; mark(KK_STAGE);
+    } else if (s->fused && c.split_first && k == 0) {
+        tile::launch_gradlim(s->precision, TP, so, st, true, pdl); ++n; mark(KK_GRADLIM);
+        tile::launch_stage(s->precision, TP, so, st, pdl); ++n; mark(KK_STAGE);
     } else if (s->fused) {
         so.work = c.worklist ? s->work + k : nullptr;
-        tile::launch_fused(s->precision, c.FPl, so, st, pdl, s->n_tiles, s->work_grid); ++n; mark(KK_STAGE);
+        tile::launch_fused(s->precision, c.FPl, so, st, pdl, s->n_tiles, s->work_grid); ++n; mark(KK_FUSED);
     } else {
         tile::launch_stage(s->precision, TP, so, st, pdl); ++n; mark(KK_STAGE);
     }
@@ -1029,7 +1043,7 @@ int fv_solver_info(fv_solver* s, int64_t* out) {
 
 int fv_solver_stage_kernels(fv_solver* s) {
     if (!s) return fail(FV_ERR_ARG, "null solver");
-    return s->fused ? FV_STAGE_FUSED : FV_STAGE_SPLIT;
+    return s->fused ? (s->split_first ? FV_STAGE_HYBRID : FV_STAGE_FUSED) : FV_STAGE_SPLIT;
 }
 
 int fv_solver_schedule(fv_solver* s) {

@@ -39,6 +39,9 @@ struct fv_solver {
     TileParams TP{};
     // the fused stage kernel over two-ring tiles (its Params are TP.P at launch)
     bool fused = false;
+    // with fused: the first stage of each step runs the split kernels, whose
+    // gradient kernel also computes dt (no separate dt kernel)
+    bool split_first = false;
     FusedParams FPm{};
     // its schedule (FV_SCHED_*); the work list's per-stage tile counters and
     // CTAs per launch
@@ -97,7 +100,7 @@ struct fv_solver {
 namespace fvgpu {
 
 // Kernel kinds for per-kernel timing.
-enum { KK_BEGIN = 0, KK_DT = 1, KK_GRADLIM = 2, KK_STAGE = 3, KK_END = 4, KK_N = 5 };
+enum { KK_BEGIN = 0, KK_DT = 1, KK_GRADLIM = 2, KK_STAGE = 3, KK_END = 4, KK_FUSED = 5, KK_N = 6 };
 
 struct EventLog {
     std::vector<cudaEvent_t> ev;  // ev[0] before the first kernel, ev[k+1] after kernel k
@@ -121,7 +124,7 @@ struct EventLog {
 struct StepCursor {
     TileIO io{};
     FusedParams FPl{};
-    bool grads = false, worklist = false;
+    bool grads = false, worklist = false, split_first = false;
     int b = 0;
     const void* in = nullptr;
     void* out = nullptr;

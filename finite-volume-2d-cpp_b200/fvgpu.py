@@ -233,14 +233,16 @@ def physics_struct(ph: _phys.Physics, group_names: Sequence[str]):
 class Solver:
     """Device solver for one mesh + physics (one CUDA device)."""
 
-    STAGE_KERNELS = {"auto": 0, "split": 1, "fused": 2}
+    STAGE_KERNELS = {"auto": 0, "split": 1, "fused": 2, "hybrid": 3}
 
     SCHEDULES = {"tile": 0, "worklist": 1, "tile2": 2}
 
     def __init__(self, mesh: Mesh, ph: _phys.Physics, precision: str = "fp64_exact", device: int = 0,
                  tile_cells: int = 0, stage_kernels: str = "auto", schedule: str = "tile"):
-        """stage_kernels: "auto" (the fused stage kernel where the physics
-        allow it), "split" (gradient and flux kernels) or "fused"; schedule of
+        """stage_kernels: "auto" ("hybrid" where the physics allow the fused
+        stage kernel, else "split"), "split" (gradient and flux kernels),
+        "fused", or "hybrid" (split first stage with the time step folded into
+        its gradient kernel, fused others); schedule of
         the fused kernel: "tile" (one CTA per tile), "worklist" or "tile2"
         (one CTA of two threads per cell per tile)."""
         self.mesh = mesh
@@ -301,8 +303,9 @@ class Solver:
 
     @property
     def stage_kernels(self):
-        """"fused" or "split": the stage kernels this solver runs."""
-        return {2: "fused", 1: "split"}[lib().fv_solver_stage_kernels(self._h)]
+        """"fused", "split" or "hybrid" (split first stage, fused others): the
+        stage kernels this solver runs."""
+        return {3: "hybrid", 2: "fused", 1: "split"}[lib().fv_solver_stage_kernels(self._h)]
 
     @property
     def schedule(self):

@@ -224,14 +224,19 @@ typedef struct {
     int32_t tile_cells;  /* cells per tile = threads per CTA: 64, 128 or 256 (0 = 128) */
     /* Stage kernels of the second-order Euler kinds (Roe fluxes, no
      * diffusive terms, no residual smoothing):
-     * FV_STAGE_AUTO (0): one fused kernel per RK stage (gradients, limiter,
-     *   fluxes, update, ghost fill) over two-ring tiles, plus one time-step
-     *   kernel per step, where the physics allow; otherwise as below.
+     * FV_STAGE_AUTO (0): FV_STAGE_HYBRID where the physics allow the fused
+     *   kernel (FV_STAGE_FUSED with the work-list schedule), otherwise
+     *   FV_STAGE_SPLIT.
      * FV_STAGE_SPLIT (1): a gradient + limiter kernel and a flux + update
      *   kernel per stage (the first stage's gradient kernel also computes dt).
-     * FV_STAGE_FUSED (2): the fused kernel; FV_ERR_UNSUPPORTED when the
-     *   physics do not allow it.  All three give the same results (bit for bit
-     *   in FP64_EXACT). */
+     * FV_STAGE_FUSED (2): one fused kernel per RK stage (gradients, limiter,
+     *   fluxes, update, ghost fill) over two-ring tiles, plus one time-step
+     *   kernel per step; FV_ERR_UNSUPPORTED when the physics do not allow it.
+     * FV_STAGE_HYBRID (3): the split kernels for the first stage of each step
+     *   (whose gradient kernel also computes dt, so the step has no separate
+     *   time-step kernel) and the fused kernel for the others; not with the
+     *   work-list schedule.  All four give the same results (bit for bit in
+     *   FP64_EXACT). */
     int32_t stage_kernels;
     /* Schedule of the fused stage kernel: FV_SCHED_TILE (0) one CTA of one
      * thread per cell per tile; FV_SCHED_WORKLIST (1) as many CTAs as the
@@ -241,7 +246,7 @@ typedef struct {
      * tile run in one pass.  Ignored for the split kernels. */
     int32_t schedule;
 } fv_solver_options;
-enum { FV_STAGE_AUTO = 0, FV_STAGE_SPLIT = 1, FV_STAGE_FUSED = 2 };
+enum { FV_STAGE_AUTO = 0, FV_STAGE_SPLIT = 1, FV_STAGE_FUSED = 2, FV_STAGE_HYBRID = 3 };
 enum { FV_SCHED_TILE = 0, FV_SCHED_WORKLIST = 1, FV_SCHED_TILE2 = 2 };
 int fv_solver_create_ex(const fv_mesh* m, const fv_physics* ph, int32_t precision, int32_t device,
                         const fv_solver_options* opt, fv_solver** out);
@@ -385,8 +390,9 @@ int fv_last_run_stats(fv_solver* s, double* device_ms, int64_t* kernel_launches)
 
 /* Per-kernel device timing: runs n_steps more time steps without graph
  * capture, with a CUDA event after every kernel on the solver's stream.
- * out_ms[5] / out_count[5] per kernel kind: 0 step control, 1 time step,
- * 2 gradients + limiters, 3 flux + update + ghost fill, 4 step end. */
+ * out_ms[6] / out_count[6] per kernel kind: 0 step control, 1 time step,
+ * 2 gradients + limiters, 3 flux + update + ghost fill, 4 step end, 5 the
+ * fused stage kernel (gradients through ghost fill in one launch). */
 int fv_profile_kernels(fv_solver* s, const double* alpha, int32_t n_alpha, int32_t n_steps,
                        double* out_ms, int64_t* out_count);
 

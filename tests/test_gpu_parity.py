@@ -331,10 +331,10 @@ FUSED_CASES = [n for n in sorted(CASES) if CASES[n]["phys"]().order2 and CASES[n
 def test_fused_and_split_stage_kernels_agree(name, precision, oracle):
     """The fused stage kernel (gradients, limiter and fluxes of a two-ring
     tile in one launch), with one CTA per tile (one or two threads per cell)
-    and with the work-list schedule, and the split gradient + flux kernels
-    give the same bits in
-    every precision mode, and in FP64_EXACT all equal the oracle, at every
-    tile size."""
+    and with the work-list schedule, the split gradient + flux kernels, and
+    the hybrid (split first stage with the time step folded into its
+    gradient kernel, fused others) give the same bits in every precision
+    mode, and in FP64_EXACT all equal the oracle, at every tile size."""
     case = CASES[name]
     em, ph = case["mesh"](), case["phys"]()
     mesh = fvgpu.Mesh.from_elements(em)
@@ -344,7 +344,8 @@ def test_fused_and_split_stage_kernels_agree(name, precision, oracle):
     want = oracle.run_loop(g, p, q0, case["alpha"], case["steps"]) if precision == "fp64_exact" else None
     out = {}
     for T in (64, 128, 256):
-        for sk, sched in (("split", "tile"), ("fused", "tile"), ("fused", "worklist"), ("fused", "tile2")):
+        for sk, sched in (("split", "tile"), ("fused", "tile"), ("fused", "worklist"), ("fused", "tile2"),
+                          ("hybrid", "tile"), ("hybrid", "tile2")):
             if sched == "tile2" and T > 128:
                 continue
             s = fvgpu.Solver(mesh, ph, precision, tile_cells=T, stage_kernels=sk, schedule=sched)
@@ -368,7 +369,7 @@ def test_fused_stage_kernel_is_chosen_where_the_physics_allow():
         ph = case["phys"]()
         s = fvgpu.Solver(fvgpu.Mesh.from_elements(case["mesh"]()), ph, "fp64")
         fusable = ph.V == 4 and ph.order2 and ph.flux in ("roe_fs", "roe_st") and not ph.diffusive
-        assert s.stage_kernels == ("fused" if fusable else "split"), name
+        assert s.stage_kernels == ("hybrid" if fusable else "split"), name
         s.close()
     case = CASES["heat"]
     with pytest.raises(fvgpu.FvError) as e:
