@@ -22,7 +22,9 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cstring>
+#include <thread>
 #include <memory>
 #include <string>
 #include <vector>
@@ -172,6 +174,8 @@ struct fv_group {
     std::vector<int> band_tiles;         // per local part
     const NcclApi* nccl = nullptr;
     ncclComm_t comm = nullptr;
+    double timeout_ms = 300000.0;        // a chunk's wait limit with a communicator
+    bool aborted = false;                // the communicator was aborted: the group is unusable
     // local parts [lo, hi): meshes, solvers, plans and exchange buffers
     std::vector<fv_mesh*> meshes;
     std::vector<fv_solver*> parts;
@@ -205,7 +209,7 @@ struct fv_group {
     }
     ~fv_group() {
         cudaSetDevice(device);
-        if (stream) cudaStreamSynchronize(stream);
+        if (stream && !aborted) cudaStreamSynchronize(stream);
         // graphs that hold NCCL calls go before their communicator
         for (auto& e : graphs)
             if (e.exec) cudaGraphExecDestroy(e.exec);
@@ -358,6 +362,36 @@ int group_graph(fv_group* g, const std::vector<double>& alpha, int len, GraphEnt
     return FV_OK;
 }
 
+// Waits for the launched chunk.  With a communicator, the wait has a limit
+// (fv_group_options.timeout_ms) and watches NCCL's asynchronous error: a
+// process that died or never launched its part of a collective ends the
+// wait with FV_ERR_COMM after aborting the communicator (NCCL's kernels then
+// return), instead of a wait without end.
+int wait_chunk(fv_group* g) {
+    if (!g->comm) {
+        GK(cudaStreamSynchronize(g->stream));
+        return FV_OK;
+    }
+    const auto t0 = std::chrono::steady_clock::now();
+    for (;;) {
+        const cudaError_t q = cudaStreamQuery(g->stream);
+        if (q == cudaSuccess) return FV_OK;
+        if (q != cudaErrorNotReady) return set_error(FV_ERR_CUDA, std::string("fv_group_run: ") + cudaGetErrorString(q));
+        ncclResult_t ae = ncclSuccess;
+        g->nccl->CommGetAsyncError(g->comm, &ae);
+        const double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        if (ae != ncclSuccess || ms > g->timeout_ms) {
+            std::string why = ae != ncclSuccess ? std::string("NCCL error: ") + g->nccl->GetErrorString(ae)
+                                                : "no progress within " + std::to_string((long long)g->timeout_ms) + " ms";
+            g->nccl->CommAbort(g->comm);
+            g->comm = nullptr;
+            g->aborted = true;
+            return set_error(FV_ERR_COMM, "fv_group_run: " + why + "; the communicator was aborted");
+        }
+        std::this_thread::sleep_for(std::chrono::microseconds(50));
+    }
+}
+
 // RK1 leaves the state in qbase[1] after an odd number of steps
 int settle(fv_solver* s, unsigned long long steps) {
     if (steps % 2) {
@@ -436,8 +470,29 @@ int fv_group_create(const fv_mesh* fm, const fv_physics* ph, int32_t precision, 
     g->n_parts = P; g->rank = o->rank; g->n_ranks = R;
     g->lo = o->rank * (P / R); g->hi = g->lo + P / R;
     g->nccl_local = o->nccl_local != 0;
+    if (o->timeout_ms > 0) g->timeout_ms = o->timeout_ms;
     g->g_real = fm->m.n_real; g->g_total = fm->m.n_total;
     GK(cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking));
+    // the communicator first: every later failure of one process then ends
+    // in the others' bounded waits, not in an unbounded initialisation
+    const bool use_comm = R > 1 || g->nccl_local;
+    if (use_comm) {
+        std::string why;
+        g->nccl = nccl_api(&why);
+        if (!g->nccl) return set_error(FV_ERR_COMM, why);
+        ncclUniqueId id;
+        if (o->nccl_id) {
+            std::memcpy(&id, o->nccl_id, sizeof(id));
+        } else {
+            ncclResult_t r = g->nccl->GetUniqueId(&id);
+            if (r != ncclSuccess) return set_error(FV_ERR_COMM, std::string("ncclGetUniqueId: ") + g->nccl->GetErrorString(r));
+        }
+        ncclResult_t r = g->nccl->CommInitRank(&g->comm, R, id, o->rank);
+        if (r != ncclSuccess) {
+            g->comm = nullptr;
+            return set_error(FV_ERR_COMM, std::string("ncclCommInitRank: ") + g->nccl->GetErrorString(r));
+        }
+    }
     fv_solver_options so = o->solver;
     if (ph->order2) so.stage_kernels = FV_STAGE_FUSED;
     for (int p = g->lo; p < g->hi; ++p) {
@@ -482,7 +537,6 @@ int fv_group_create(const fv_mesh* fm, const fv_physics* ph, int32_t precision, 
     g->pack_off[nl] = (int64_t)pk_src.size();
     // messages and receive slots, pair (s, r) in the same order on every
     // process; pairs within this process read the sender's pack directly
-    const bool use_comm = R > 1 || g->nccl_local;
     int64_t n_recv = 0;
     for (int sp = 0; sp < P; ++sp)
         for (int rp = 0; rp < P; ++rp) {
@@ -548,23 +602,6 @@ int fv_group_create(const fv_mesh* fm, const fv_physics* ph, int32_t precision, 
     GK(g->alloc(&g->recs, (size_t)2 * P));
     GK(g->alloc(&g->sums, (size_t)ph->V * P));
     GK(cudaMemset(g->sums, 0, sizeof(double) * ph->V * P));
-    if (use_comm) {
-        std::string why;
-        g->nccl = nccl_api(&why);
-        if (!g->nccl) return set_error(FV_ERR_COMM, why);
-        ncclUniqueId id;
-        if (o->nccl_id) {
-            std::memcpy(&id, o->nccl_id, sizeof(id));
-        } else {
-            ncclResult_t r = g->nccl->GetUniqueId(&id);
-            if (r != ncclSuccess) return set_error(FV_ERR_COMM, std::string("ncclGetUniqueId: ") + g->nccl->GetErrorString(r));
-        }
-        ncclResult_t r = g->nccl->CommInitRank(&g->comm, R, id, o->rank);
-        if (r != ncclSuccess) {
-            g->comm = nullptr;
-            return set_error(FV_ERR_COMM, std::string("ncclCommInitRank: ") + g->nccl->GetErrorString(r));
-        }
-    }
     GK(cudaStreamSynchronize(g->stream));
     *out = g.release();
     return FV_OK;
@@ -613,6 +650,7 @@ int fv_group_run(fv_group* g, const fv_run_options* o, fv_run_info* info) {
     if (!g || !o) return set_error(FV_ERR_ARG, "fv_group_run: null argument");
     if (o->n_alpha < 1 || o->n_alpha > 16 || !o->alpha) return set_error(FV_ERR_ARG, "fv_group_run: need 1..16 RK stages");
     if (o->print_interval == 0) return set_error(FV_ERR_ARG, "fv_group_run: print_interval must be > 0");
+    if (g->aborted) return set_error(FV_ERR_COMM, "fv_group_run: the communicator was aborted by an earlier run");
     GK(cudaSetDevice(g->device));
     cudaStream_t st = g->stream;
     std::vector<double> alpha(o->alpha, o->alpha + o->n_alpha);
@@ -656,10 +694,11 @@ int fv_group_run(fv_group* g, const fv_run_options* o, fv_run_info* info) {
         launches += ge->launches;
         cudaEventRecord(e1, st);
         launch_ctrl_copy(s0->ctrl, s0->hctrl_dev, st);
-        if (cudaGetLastError() != cudaSuccess || cudaStreamSynchronize(st) != cudaSuccess) {
-            rc = set_error(FV_ERR_CUDA, "fv_group_run: a step failed on the device");
+        if (cudaGetLastError() != cudaSuccess) {
+            rc = set_error(FV_ERR_CUDA, "fv_group_run: a launch failed");
             break;
         }
+        if ((rc = wait_chunk(g))) break;
         float ms = 0.f;
         cudaEventElapsedTime(&ms, e0, e1);
         total_ms += ms;

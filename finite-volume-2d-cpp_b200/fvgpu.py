@@ -452,7 +452,7 @@ class Group:
     def __init__(self, mesh: Mesh, ph: _phys.Physics, precision: str = "fp64_exact", n_parts: int = 2,
                  rank: int = 0, n_ranks: int = 1, nccl_id_bytes: Optional[bytes] = None, device: int = 0,
                  nccl_local: bool = False, tile_cells: int = 0, schedule: str = "tile",
-                 serial_exchange: bool = False):
+                 serial_exchange: bool = False, timeout_ms: float = 0.0):
         self.mesh = mesh
         self.V = ph.V
         self._ps = physics_struct(ph, mesh.group_names)
@@ -460,7 +460,8 @@ class Group:
         o = _GroupOptions(n_parts=n_parts, rank=rank, n_ranks=n_ranks,
                           nccl_id=C.cast(self._id, C.c_void_p) if self._id is not None else None,
                           nccl_local=int(nccl_local), tile_cells=int(tile_cells), stage_kernels=0,
-                          schedule=Solver.SCHEDULES[schedule], serial_exchange=int(serial_exchange))
+                          schedule=Solver.SCHEDULES[schedule], serial_exchange=int(serial_exchange),
+                          timeout_ms=float(timeout_ms))
         h = C.c_void_p()
         _check(lib().fv_group_create(mesh._h, C.byref(self._ps), C.c_int32(PREC[precision]), C.c_int32(device),
                                      C.byref(o), C.byref(h)))
@@ -517,7 +518,7 @@ class Group:
 class _GroupOptions(C.Structure):
     _fields_ = [("n_parts", C.c_int32), ("rank", C.c_int32), ("n_ranks", C.c_int32), ("nccl_id", C.c_void_p),
                 ("nccl_local", C.c_int32), ("tile_cells", C.c_int32), ("stage_kernels", C.c_int32),
-                ("schedule", C.c_int32), ("serial_exchange", C.c_int32)]
+                ("schedule", C.c_int32), ("serial_exchange", C.c_int32), ("timeout_ms", C.c_double)]
 
 
 def solver_info(s: Solver):

@@ -297,6 +297,10 @@ typedef struct {
                                   their tiles and then the halo exchange run on a second,
                                   high-priority stream while the remaining tiles compute.
                                   1: the exchange follows all tiles of the stage. */
+    double timeout_ms;         /* with NCCL: the longest wait for one chunk of steps (0 = 300 s).
+                                  A chunk that makes no progress within it, or an NCCL error,
+                                  aborts the communicator and fv_group_run returns FV_ERR_COMM
+                                  (the group cannot run again). */
 } fv_group_options;
 int fv_group_nccl_id(void* id128);
 /* Collective over the n_ranks processes (each passes the whole mesh, its rank
