@@ -104,7 +104,7 @@ __global__ void k_group_dt_local(PartPtrs pp, int nl) {
 }
 
 // each local part's residual partial sums, reduced in a fixed order (block j)
-constexpr int kSumBlock = 256;
+constexpr int kSumBlock = 1024;
 __global__ void __launch_bounds__(kSumBlock) k_group_psum(PartPtrs pp, int V, double* __restrict__ out) {
     __shared__ double red[kSumBlock / 32][kMaxV];
     const int j = blockIdx.x;
