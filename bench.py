@@ -647,7 +647,7 @@ def measure_decomposed(args, mesh, geo, ph, alpha, ic, prec, parts_per_gpu, loca
         nid = box[0]
         dist.barrier()
     grp = fvgpu.Group(mesh, ph, prec, n_parts=n_parts, rank=rank, n_ranks=world, nccl_id_bytes=nid, device=local,
-                      serial_exchange=args.serial_exchange, timeout_ms=timeout_ms)
+                      serial_exchange=args.serial_exchange, timeout_ms=timeout_ms, transport=args.transport)
     try:
         grp.set_state(q0)
         grp.run(args.warmup, alpha=alpha)
@@ -667,6 +667,7 @@ def measure_decomposed(args, mesh, geo, ph, alpha, ic, prec, parts_per_gpu, loca
                "clocks": clk.summary(), "rank_parts": gi, "halo_bytes_per_stage": gi["halo_cells"] * cell_bytes,
                "exchange": ("after all tiles" if args.serial_exchange else
                             "band tiles + exchange on a second stream beside the interior tiles"),
+               "transport": gi["transport"],
                "parallelism": (f"{n_parts} parts over {world} processes (NCCL)" if world > 1
                                else f"{n_parts} parts on one GPU (device reads)")}
         if compare_single:
@@ -716,6 +717,7 @@ def run_decomposed_workload(args):
                            "n_parts": d["n_parts"], "precision": prec, "exchange": d["exchange"],
                            "parallelism": d["parallelism"],
                            "l2": "inputs larger than L2 (working set > 126 MB), no flush"},
+                "transport": d["transport"],
                 "gpu_launches": d["gpu_launches"], "clocks": d["clocks"], "rank0_parts": d["rank_parts"],
                 "halo_bytes_per_stage_rank0": d["halo_bytes_per_stage"]}
         if "single_solver" in d:
@@ -735,6 +737,9 @@ def main():
                     choices=["step", "sod", "naca", "batch", "adjoint", "flatplate", "heat", "decomposed"])
     ap.add_argument("--parts-per-gpu", type=int, default=None,
                     help="decomposed workload: parts per process (default 4 on one GPU, else 1)")
+    ap.add_argument("--transport", default="copy", choices=["copy", "p2p"],
+                    help="decomposed workload: halo states by NCCL between processes and device reads within "
+                         "one (copy), or stored straight into the reading part's memory with epoch flags (p2p)")
     ap.add_argument("--serial-exchange", action="store_true",
                     help="decomposed workload: halo exchange after all tiles of a stage (default: beside "
                          "the interior tiles)")

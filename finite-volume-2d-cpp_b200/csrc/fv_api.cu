@@ -765,7 +765,8 @@ namespace fvgpu {
 
 int set_error(int code, const std::string& msg) { return fail(code, msg); }
 
-int step_open(fv_solver* s, const std::vector<double>& alpha, int b, bool first, StepCursor& c, EventLog* log) {
+int step_open(fv_solver* s, const std::vector<double>& alpha, int b, bool first, StepCursor& c, EventLog* log,
+              bool with_dt) {
     const TileParams& TP = s->TP;
     cudaStream_t st = s->stream;
     int n = 0;
@@ -784,19 +785,24 @@ int step_open(fv_solver* s, const std::vector<double>& alpha, int b, bool first,
     c.split_first = s->fused && s->split_first;
     // the work-list schedule: one tile counter per stage, zeroed by the dt kernel
     c.worklist = s->fused && s->sched == FV_SCHED_WORKLIST && alpha.size() <= (size_t)kWorkSlots;
-    // every kernel after step_begin is a programmatic dependent of the one
-    // before it (its constant tile data is staged during that one's tail)
-    if (!c.grads && !c.split_first) {
-        TileIO dio = io;
-        dio.work_reset = c.worklist ? s->work : nullptr;
-        tile::launch_dt(s->precision, TP, dio, st, true); ++n; mark(KK_DT);
-    }
     c.FPl = s->FPm;
     c.FPl.P = TP.P;
     c.FPl.threads = (s->sched == FV_SCHED_TILE2) ? 2 * c.FPl.T : c.FPl.T;
     c.in = s->sbase[b];
     c.out = nullptr;
+    if (with_dt) n += step_dt(s, c, log);
     return n;
+}
+
+int step_dt(fv_solver* s, StepCursor& c, EventLog* log) {
+    // every kernel after step_begin is a programmatic dependent of the one
+    // before it (its constant tile data is staged during that one's tail)
+    if (c.grads || c.split_first) return 0;
+    TileIO dio = c.io;
+    dio.work_reset = c.worklist ? s->work : nullptr;
+    tile::launch_dt(s->precision, s->TP, dio, s->stream, true);
+    if (log) log->mark(KK_DT);
+    return 1;
 }
 
 int step_stage(fv_solver* s, const std::vector<double>& alpha, int k, StepCursor& c, EventLog* log,

@@ -24,6 +24,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cstring>
+#include <map>
 #include <thread>
 #include <memory>
 #include <string>
@@ -155,6 +156,90 @@ __global__ void k_group_unpack(PartPtrs pp, const int32_t* __restrict__ part, co
 }
 int blocks_of(int64_t n) { return (int)((n + kBlock - 1) / kBlock); }
 
+// ---- the P2P transport: stores into the reading parts' memory, epoch flags
+// A part's flag word for source part s holds the last epoch s published:
+// s's outputs of stage k of step n are complete in this part's buffers once
+// it reads n * stages + k + 1.  Epochs come from the step counter in device
+// memory, so captured graphs replay them.
+constexpr int kMaxPeers = 16;  // parts a local part sends to
+__device__ __forceinline__ unsigned long long ld_acquire_sys(const unsigned long long* p) {
+    unsigned long long v;
+    asm volatile("ld.acquire.sys.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release_sys(unsigned long long* p, unsigned long long v) {
+    asm volatile("st.release.sys.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+__device__ __forceinline__ bool ctrl_inactive(const Ctrl* c) { return *(volatile const int*)&c->active == 0; }
+
+struct PushParams {
+    const uint32_t* src;                   // the local part's output of this stage
+    uint32_t* dst[kMaxPeers];              // the same stage buffer of each reading part
+    unsigned long long* flag[kMaxPeers];   // this part's flag word in each reading part
+    int n_dst;
+    const int32_t* slot;                   // [n] reading part (slot) of entry i
+    const int32_t* from;                   // [n] local cell (real or ghost)
+    const int32_t* to;                     // [n] that cell's index in the reading part
+    int64_t n;
+    int words;                             // 32-bit words per cell state
+    unsigned long long* ctr;               // CTAs of this part's pushes that have completed
+    const Ctrl* ctrl;
+    int stages, stage;
+};
+// The states other parts read, stored straight into their buffers; the last
+// CTA of the launch then releases the stage's epoch into each reader's flag
+// word, after every CTA's stores are visible at system scope (the barrier
+// orders a CTA's stores before its thread 0, whose system-scope fence and
+// count make them visible before any later release).
+__global__ void k_p2p_push(PushParams pp) {
+    if (ctrl_inactive(pp.ctrl)) return;
+    const unsigned long long epoch = pp.ctrl->step * (unsigned long long)pp.stages + pp.stage + 1;
+    const int64_t total = pp.n * pp.words;
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = t / pp.words;
+        const int w = (int)(t - i * pp.words);
+        pp.dst[pp.slot[i]][(int64_t)pp.to[i] * pp.words + w] = pp.src[(int64_t)pp.from[i] * pp.words + w];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence_system();
+        const unsigned long long done = atomicAdd(pp.ctr, 1ull) + 1ull;
+        if (done == epoch * gridDim.x) {
+            __threadfence_system();
+            for (int d = 0; d < pp.n_dst; ++d) st_release_sys(pp.flag[d], epoch);
+        }
+    }
+}
+
+// Waits until every part that sends to local part j (block j) has released
+// the epoch this stage needs.  Each wait gives up after `limit` polls: it
+// then records the failure in err[j] and returns, and the host reports it.
+struct WaitParams {
+    const unsigned long long* flags[kMaxLocal];  // part j's flag words [n_parts]
+    const int32_t* src[kMaxLocal];               // parts that send to part j
+    int n_src[kMaxLocal];
+    int* err;                                    // [local parts]
+    const Ctrl* ctrl;
+    int stages, stage;                           // needed epoch: step * stages + stage
+    long long limit;
+};
+__global__ void k_p2p_wait(WaitParams wp) {
+    const int j = blockIdx.x;
+    if (ctrl_inactive(wp.ctrl)) return;
+    const unsigned long long need = wp.ctrl->step * (unsigned long long)wp.stages + wp.stage;
+    for (int i = threadIdx.x; i < wp.n_src[j]; i += blockDim.x) {
+        const unsigned long long* f = wp.flags[j] + wp.src[j][i];
+        long long polls = 0;
+        while (ld_acquire_sys(f) < need) {
+            if (++polls > wp.limit) {
+                atomicExch(wp.err + j, 1);
+                break;
+            }
+            __nanosleep(256);
+        }
+    }
+}
+
 }  // namespace
 }  // namespace fvgpu
 
@@ -191,6 +276,24 @@ struct fv_group {
     struct Msg { int peer, send; int64_t off, n; };
     std::vector<Msg> msgs;
     fvgpu::PartPtrs pp{};
+    // the P2P transport: per local part, what it pushes where (entries of
+    // reading-part slot, local cell, cell in the reader), the reader's stage
+    // buffers by role (tmp[0], tmp[1], sbase[0], sbase[1]) and flag word per
+    // slot, and the count of its completed push CTAs
+    bool p2p = false;
+    struct Push {
+        int32_t *slot = nullptr, *from = nullptr, *to = nullptr;
+        int64_t n = 0;
+        int n_dst = 0;
+        uint32_t* buf[4][fvgpu::kMaxPeers] = {};
+        unsigned long long* flag[fvgpu::kMaxPeers] = {};
+        unsigned long long* ctr = nullptr;
+    };
+    std::vector<Push> push;
+    unsigned long long* flags = nullptr;  // [local parts][n_parts] flag words the senders write
+    int* err = nullptr;                   // [local parts] a wait that ran out
+    fvgpu::WaitParams wp{};
+    std::vector<void*> ipc_opened;        // other processes' allocations mapped here
     std::vector<GraphEntry> graphs;
     unsigned long long* recs = nullptr;  // [n_parts][2]
     double* sums = nullptr;              // [n_parts][V]
@@ -214,6 +317,7 @@ struct fv_group {
         for (auto& e : graphs)
             if (e.exec) cudaGraphExecDestroy(e.exec);
         if (comm && nccl) nccl->CommDestroy(comm);
+        for (void* q : ipc_opened) cudaIpcCloseMemHandle(q);
         for (fv_solver* s : parts) fv_solver_destroy(s);
         for (fv_mesh* m : meshes) delete m;
         for (void* p : allocs) cudaFree(p);
@@ -240,6 +344,9 @@ using fvgpu::set_error;
             return set_error(FV_ERR_COMM, std::string("NCCL ") + #call + ": " +               \
                                               (g)->nccl->GetErrorString(r_));                 \
     } while (0)
+
+int p2p_push(fv_group* g, int j, const void* out, int role, int stages, int k, cudaStream_t st);
+int p2p_wait(fv_group* g, int stages, int k, cudaStream_t st);
 
 // pack, move and unpack the halo states of this stage's outputs (pp.out) on st
 int halo_exchange(fv_group* g, cudaStream_t st) {
@@ -273,8 +380,19 @@ int64_t group_step(fv_group* g, const std::vector<double>& alpha, int b, bool fi
     cudaStream_t st = g->stream;
     const int P = g->n_parts, nl = (int)g->parts.size();
     std::vector<StepCursor> cur(nl);
+    const int S = (int)alpha.size();
+    // the buffer role of stage k's output (tmp[0], tmp[1], sbase[0], sbase[1])
+    auto role_of = [&](int k) { return S == 1 ? 2 + (1 - b) : (k == S - 1 ? 2 + b : k % 2); };
     int64_t n = 0;
-    for (int j = 0; j < nl; ++j) n += step_open(g->parts[j], alpha, b, first, cur[j], nullptr);
+    for (int j = 0; j < nl; ++j) n += step_open(g->parts[j], alpha, b, first, cur[j], nullptr, !g->p2p);
+    if (g->p2p) {
+        // the previous step's last stage must have reached the halo before
+        // the dt kernel reads it
+        int rc = p2p_wait(g, S, 0, st);
+        if (rc) return rc;
+        ++n;
+        for (int j = 0; j < nl; ++j) n += step_dt(g->parts[j], cur[j], nullptr);
+    }
     if (g->comm) {
         fvgpu::k_group_dtrec<<<nl, 32, 0, st>>>(g->pp, g->recs + 2 * g->lo);
         NK(g, AllGather(g->recs + 2 * g->lo, g->recs, (size_t)2 * nl, ncclUint64, g->comm, st));
@@ -285,7 +403,12 @@ int64_t group_step(fv_group* g, const std::vector<double>& alpha, int b, bool fi
         n += 1;
     }
     GK(cudaGetLastError());
-    for (int k = 0; k < (int)alpha.size(); ++k) {
+    for (int k = 0; k < S; ++k) {
+        if (g->p2p && k > 0) {
+            int rc = p2p_wait(g, S, k, st);
+            if (rc) return rc;
+            ++n;
+        }
         if (g->overlap) {
             // band tiles, pack, exchange and unpack on cstream, beside the
             // interior tiles on st; both start once the previous stage and
@@ -301,7 +424,13 @@ int64_t group_step(fv_group* g, const std::vector<double>& alpha, int b, bool fi
                 n += m;
                 g->pp.out[j] = (uint32_t*)cur[j].out;
             }
-            int rc = halo_exchange(g, g->cstream);
+            int rc = FV_OK;
+            if (g->p2p) {
+                for (int j = 0; j < nl && rc == FV_OK; ++j)
+                    rc = p2p_push(g, j, cur[j].out, role_of(k), S, k, g->cstream);
+            } else {
+                rc = halo_exchange(g, g->cstream);
+            }
             if (rc) return rc;
             GK(cudaEventRecord(g->ev_halo, g->cstream));
             for (int j = 0; j < nl; ++j) {
@@ -316,10 +445,19 @@ int64_t group_step(fv_group* g, const std::vector<double>& alpha, int b, bool fi
                 n += step_stage(g->parts[j], alpha, k, cur[j], nullptr);
                 g->pp.out[j] = (uint32_t*)cur[j].out;
             }
-            int rc = halo_exchange(g, st);
+            int rc = FV_OK;
+            if (g->p2p) {
+                for (int j = 0; j < nl && rc == FV_OK; ++j) rc = p2p_push(g, j, cur[j].out, role_of(k), S, k, st);
+            } else {
+                rc = halo_exchange(g, st);
+            }
             if (rc) return rc;
         }
-        n += (g->n_pack > 0) + (g->n_unpack > 0);
+        if (g->p2p) {
+            for (int j = 0; j < nl; ++j) n += g->push[j].n > 0;
+        } else {
+            n += (g->n_pack > 0) + (g->n_unpack > 0);
+        }
     }
     fvgpu::k_group_psum<<<nl, fvgpu::kSumBlock, 0, st>>>(g->pp, g->V, g->sums + (size_t)g->V * g->lo);
     ++n;
@@ -390,6 +528,150 @@ int wait_chunk(fv_group* g) {
         }
         std::this_thread::sleep_for(std::chrono::microseconds(50));
     }
+}
+
+// A local part's stage buffer by role: tmp[0], tmp[1], sbase[0], sbase[1].
+void* role_buffer(fv_solver* s, int role) { return role < 2 ? s->tmp[role] : s->sbase[role - 2]; }
+
+// The P2P transport's plan: every push entry of the local parts, the
+// readers' buffers (this process's parts directly; other processes' parts
+// through CUDA IPC handles all-gathered over NCCL) and the wait lists.
+int setup_p2p(fv_group* g, const HostMesh& gm, long long wait_limit) {
+    const int P = g->n_parts, nl = (int)g->parts.size();
+    GK(g->alloc(&g->flags, (size_t)nl * P));
+    GK(cudaMemset(g->flags, 0, sizeof(unsigned long long) * nl * P));
+    GK(g->alloc(&g->err, (size_t)nl));
+    GK(cudaMemset(g->err, 0, sizeof(int) * nl));
+    // IPC handles of every part's stage buffers and of its process's flag words
+    struct Handles { cudaIpcMemHandle_t h[5]; };
+    std::vector<Handles> all(P);
+    if (g->n_ranks > 1) {
+        for (int j = 0; j < nl; ++j) {
+            Handles& hj = all[g->lo + j];
+            for (int role = 0; role < 4; ++role) GK(cudaIpcGetMemHandle(&hj.h[role], role_buffer(g->parts[j], role)));
+            GK(cudaIpcGetMemHandle(&hj.h[4], g->flags));
+        }
+        char* dev = nullptr;
+        GK(g->alloc(&dev, sizeof(Handles) * P));
+        GK(cudaMemcpy(dev + sizeof(Handles) * g->lo, &all[g->lo], sizeof(Handles) * nl, cudaMemcpyHostToDevice));
+        NK(g, AllGather(dev + sizeof(Handles) * g->lo, dev, sizeof(Handles) * nl, ncclUint8, g->comm, g->stream));
+        GK(cudaStreamSynchronize(g->stream));
+        GK(cudaMemcpy(all.data(), dev, sizeof(Handles) * P, cudaMemcpyDeviceToHost));
+    }
+    std::map<std::string, void*> opened;  // one mapping per handle
+    auto open = [&](const cudaIpcMemHandle_t& h, void** ptr) -> int {
+        const std::string key(reinterpret_cast<const char*>(&h), sizeof(h));
+        auto it = opened.find(key);
+        if (it == opened.end()) {
+            void* q = nullptr;
+            GK(cudaIpcOpenMemHandle(&q, h, cudaIpcMemLazyEnablePeerAccess));
+            g->ipc_opened.push_back(q);
+            it = opened.emplace(key, q).first;
+        }
+        *ptr = it->second;
+        return FV_OK;
+    };
+    std::map<int, PartPlan> other;  // plans of other processes' parts
+    auto plan_of = [&](int r) -> const PartPlan* {
+        if (g->local(r) >= 0) return &g->plans[g->local(r)];
+        auto it = other.find(r);
+        if (it == other.end()) {
+            HostMesh L;
+            PartPlan pl;
+            if (!build_part(gm, P, r, L, pl).empty()) return nullptr;
+            it = other.emplace(r, std::move(pl)).first;
+        }
+        return &it->second;
+    };
+    g->push.resize(nl);
+    for (int j = 0; j < nl; ++j) {
+        const int p = g->lo + j;
+        const PartPlan& pp = g->plans[j];
+        fv_group::Push& ps = g->push[j];
+        std::vector<int32_t> slot, from, to;
+        for (int r = 0; r < P; ++r) {
+            if (r == p) continue;
+            const int64_t n = pp.send_off[r + 1] - pp.send_off[r];
+            if (n == 0) continue;
+            const PartPlan* pr = plan_of(r);
+            if (!pr || pr->recv_off[p + 1] - pr->recv_off[p] != n)
+                return set_error(FV_ERR_ARG, "internal error: send and receive lists differ");
+            if (ps.n_dst == fvgpu::kMaxPeers) return set_error(FV_ERR_UNSUPPORTED, "a part reaches more than 16 parts");
+            const int sl = ps.n_dst++;
+            for (int64_t i = 0; i < n; ++i) {
+                slot.push_back(sl);
+                from.push_back(pp.send_idx[pp.send_off[r] + i]);
+                to.push_back(pr->recv_idx[pr->recv_off[p] + i]);
+            }
+            const int lr = g->local(r);
+            if (lr >= 0) {
+                for (int role = 0; role < 4; ++role) ps.buf[role][sl] = (uint32_t*)role_buffer(g->parts[lr], role);
+                ps.flag[sl] = g->flags + (size_t)lr * P + p;
+            } else {
+                for (int role = 0; role < 4; ++role) {
+                    void* q = nullptr;
+                    int rc = open(all[r].h[role], &q);
+                    if (rc) return rc;
+                    ps.buf[role][sl] = (uint32_t*)q;
+                }
+                void* fq = nullptr;
+                int rc = open(all[r].h[4], &fq);
+                if (rc) return rc;
+                const int r_lo = g->rank_of(r) * (P / g->n_ranks);
+                ps.flag[sl] = (unsigned long long*)fq + (size_t)(r - r_lo) * P + p;
+            }
+        }
+        ps.n = (int64_t)from.size();
+        auto up = [&](int32_t** d, const std::vector<int32_t>& v) -> int {
+            GK(g->alloc(d, v.size()));
+            if (!v.empty()) GK(cudaMemcpy(*d, v.data(), v.size() * 4, cudaMemcpyHostToDevice));
+            return FV_OK;
+        };
+        int rc;
+        if ((rc = up(&ps.slot, slot)) || (rc = up(&ps.from, from)) || (rc = up(&ps.to, to))) return rc;
+        GK(g->alloc(&ps.ctr, 1));
+        GK(cudaMemset(ps.ctr, 0, sizeof(unsigned long long)));
+        // what part p waits for: the parts that send to it
+        std::vector<int32_t> src;
+        for (int s2 = 0; s2 < P; ++s2)
+            if (s2 != p && pp.recv_off[s2 + 1] > pp.recv_off[s2]) src.push_back(s2);
+        int32_t* d_src = nullptr;
+        if ((rc = up(&d_src, src))) return rc;
+        g->wp.flags[j] = g->flags + (size_t)j * P;
+        g->wp.src[j] = d_src;
+        g->wp.n_src[j] = (int)src.size();
+    }
+    g->wp.err = g->err;
+    g->wp.ctrl = g->parts[0]->ctrl;
+    g->wp.limit = wait_limit;
+    return FV_OK;
+}
+
+// P2P: push local part j's outputs of stage k to the parts that read them (on st)
+int p2p_push(fv_group* g, int j, const void* out, int role, int stages, int k, cudaStream_t st) {
+    const fv_group::Push& ps = g->push[j];
+    if (ps.n == 0) return FV_OK;
+    fvgpu::PushParams pa{};
+    pa.src = (const uint32_t*)out;
+    for (int d = 0; d < ps.n_dst; ++d) { pa.dst[d] = ps.buf[role][d]; pa.flag[d] = ps.flag[d]; }
+    pa.n_dst = ps.n_dst;
+    pa.slot = ps.slot; pa.from = ps.from; pa.to = ps.to; pa.n = ps.n;
+    pa.words = (int)(g->V * g->parts[j]->ssz / 4);
+    pa.ctr = ps.ctr;
+    pa.ctrl = g->parts[j]->ctrl;
+    pa.stages = stages; pa.stage = k;
+    const int blocks = (int)std::min<int64_t>(std::max<int64_t>(fvgpu::blocks_of(ps.n * pa.words), 1), 148);
+    fvgpu::k_p2p_push<<<blocks, fvgpu::kBlock, 0, st>>>(pa);
+    GK(cudaGetLastError());
+    return FV_OK;
+}
+// P2P: every local part waits for the epoch of stage k's input (on st)
+int p2p_wait(fv_group* g, int stages, int k, cudaStream_t st) {
+    fvgpu::WaitParams w = g->wp;
+    w.stages = stages; w.stage = k;
+    fvgpu::k_p2p_wait<<<(int)g->parts.size(), 32, 0, st>>>(w);
+    GK(cudaGetLastError());
+    return FV_OK;
 }
 
 // RK1 leaves the state in qbase[1] after an odd number of steps
@@ -592,6 +874,13 @@ int fv_group_create(const fv_mesh* fm, const fv_physics* ph, int32_t precision, 
         const int T = s->fused ? s->FPm.T : 1;
         g->band_tiles.push_back((int)std::min<int64_t>((g->plans[j].n_band + T - 1) / T, s->n_tiles));
     }
+    if (o->transport == FV_EXCHANGE_P2P && (g->n_pack > 0 || g->n_unpack > 0)) {
+        g->p2p = true;
+        int rc2 = setup_p2p(g.get(), fm->m, o->wait_polls > 0 ? o->wait_polls : (1ll << 24));
+        if (rc2) return rc2;
+    } else if (o->transport != FV_EXCHANGE_COPY && o->transport != FV_EXCHANGE_P2P) {
+        return set_error(FV_ERR_ARG, "unknown transport");
+    }
     if (g->overlap) {
         int lo_pri = 0, hi_pri = 0;
         GK(cudaDeviceGetStreamPriorityRange(&lo_pri, &hi_pri));
@@ -655,6 +944,15 @@ int fv_group_run(fv_group* g, const fv_run_options* o, fv_run_info* info) {
     cudaStream_t st = g->stream;
     std::vector<double> alpha(o->alpha, o->alpha + o->n_alpha);
     const RunLimits L{o->max_step, o->max_time, o->tolerance, o->print_interval};
+    if (g->p2p && o->restart) {
+        // epochs count from step 0 again: flags, failures and push counts
+        // restart at zero (before this process's first dt all-gather, which
+        // no process passes before every process has reset)
+        GK(cudaMemsetAsync(g->flags, 0, sizeof(unsigned long long) * g->parts.size() * g->n_parts, st));
+        GK(cudaMemsetAsync(g->err, 0, sizeof(int) * g->parts.size(), st));
+        for (auto& ps : g->push)
+            if (ps.ctr) GK(cudaMemsetAsync(ps.ctr, 0, sizeof(unsigned long long), st));
+    }
     for (fv_solver* s : g->parts) {
         launch_set_limits(s->limits, L, st);
         if (o->restart) {
@@ -699,6 +997,17 @@ int fv_group_run(fv_group* g, const fv_run_options* o, fv_run_info* info) {
             break;
         }
         if ((rc = wait_chunk(g))) break;
+        if (g->p2p) {
+            std::vector<int> errs(g->parts.size());
+            if (cudaMemcpy(errs.data(), g->err, errs.size() * sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) {
+                rc = set_error(FV_ERR_CUDA, "fv_group_run: halo wait status");
+                break;
+            }
+            if (std::find(errs.begin(), errs.end(), 1) != errs.end()) {
+                rc = set_error(FV_ERR_COMM, "fv_group_run: a halo wait gave up before its senders' epoch arrived");
+                break;
+            }
+        }
         float ms = 0.f;
         cudaEventElapsedTime(&ms, e0, e1);
         total_ms += ms;
@@ -752,6 +1061,7 @@ int fv_group_info(fv_group* g, int64_t* out) {
     int64_t band = 0;
     for (int b : g->band_tiles) band += b;
     out[6] = g->overlap ? band : -1;
+    out[7] = g->p2p ? FV_EXCHANGE_P2P : FV_EXCHANGE_COPY;
     return FV_OK;
 }
 

@@ -129,7 +129,11 @@ struct StepCursor {
     const void* in = nullptr;
     void* out = nullptr;
 };
-int step_open(fv_solver* s, const std::vector<double>& alpha, int b, bool first, StepCursor& c, EventLog* log);
+// with_dt = false: step_open leaves the dt kernel to a later step_dt (a
+// decomposition waits for its halo in between).
+int step_open(fv_solver* s, const std::vector<double>& alpha, int b, bool first, StepCursor& c, EventLog* log,
+              bool with_dt = true);
+int step_dt(fv_solver* s, StepCursor& c, EventLog* log);
 // r: only tiles [r->t0, r->t0 + r->n) of the fused stage kernel (one CTA
 // per tile) on r->stream (nullptr: the solver's stream), with programmatic
 // dependent launch when r->pdl; the stage's output becomes the next stage's

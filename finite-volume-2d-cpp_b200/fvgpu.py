@@ -452,7 +452,8 @@ class Group:
     def __init__(self, mesh: Mesh, ph: _phys.Physics, precision: str = "fp64_exact", n_parts: int = 2,
                  rank: int = 0, n_ranks: int = 1, nccl_id_bytes: Optional[bytes] = None, device: int = 0,
                  nccl_local: bool = False, tile_cells: int = 0, schedule: str = "tile",
-                 serial_exchange: bool = False, timeout_ms: float = 0.0):
+                 serial_exchange: bool = False, timeout_ms: float = 0.0, transport: str = "copy",
+                 wait_polls: int = 0):
         self.mesh = mesh
         self.V = ph.V
         self._ps = physics_struct(ph, mesh.group_names)
@@ -461,6 +462,7 @@ class Group:
                           nccl_id=C.cast(self._id, C.c_void_p) if self._id is not None else None,
                           nccl_local=int(nccl_local), tile_cells=int(tile_cells), stage_kernels=0,
                           schedule=Solver.SCHEDULES[schedule], serial_exchange=int(serial_exchange),
+                          transport={"copy": 0, "p2p": 1}[transport], wait_polls=int(wait_polls),
                           timeout_ms=float(timeout_ms))
         h = C.c_void_p()
         _check(lib().fv_group_create(mesh._h, C.byref(self._ps), C.c_int32(PREC[precision]), C.c_int32(device),
@@ -493,10 +495,11 @@ class Group:
         return dict(step=info.step, time=info.time, R=np.array(info.R[: self.V]), R0=np.array(info.R0[: self.V]))
 
     def info(self):
-        out = np.zeros(7, np.int64)
+        out = np.zeros(8, np.int64)
         _check(lib().fv_group_info(self._h, _p(out, _i64p)))
         return dict(local_parts=int(out[0]), owned_cells=int(out[1]), halo_cells=int(out[2]),
-                    sent_cells=int(out[3]), tiles=int(out[4]), nccl=bool(out[5]), band_tiles=int(out[6]))
+                    sent_cells=int(out[3]), tiles=int(out[4]), nccl=bool(out[5]), band_tiles=int(out[6]),
+                    transport={0: "copy", 1: "p2p"}[int(out[7])])
 
     def last_run_stats(self):
         ms = C.c_double(); n = C.c_int64()
@@ -518,7 +521,8 @@ class Group:
 class _GroupOptions(C.Structure):
     _fields_ = [("n_parts", C.c_int32), ("rank", C.c_int32), ("n_ranks", C.c_int32), ("nccl_id", C.c_void_p),
                 ("nccl_local", C.c_int32), ("tile_cells", C.c_int32), ("stage_kernels", C.c_int32),
-                ("schedule", C.c_int32), ("serial_exchange", C.c_int32), ("timeout_ms", C.c_double)]
+                ("schedule", C.c_int32), ("serial_exchange", C.c_int32), ("transport", C.c_int32),
+                ("wait_polls", C.c_int64), ("timeout_ms", C.c_double)]
 
 
 def solver_info(s: Solver):

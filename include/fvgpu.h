@@ -283,6 +283,7 @@ int fv_solver_destroy(fv_solver* s);
  * Roe kinds); not the diffusive kinds or residual smoothing
  * (FV_ERR_UNSUPPORTED), not batches of cases. */
 typedef struct fv_group fv_group;
+enum { FV_EXCHANGE_COPY = 0, FV_EXCHANGE_P2P = 1 };
 typedef struct {
     int32_t n_parts;        /* parts of the decomposition, >= 1, a multiple of n_ranks */
     int32_t rank, n_ranks;  /* this process and the number of processes; process r holds
@@ -297,6 +298,14 @@ typedef struct {
                                   their tiles and then the halo exchange run on a second,
                                   high-priority stream while the remaining tiles compute.
                                   1: the exchange follows all tiles of the stage. */
+    int32_t transport;         /* halo states between parts: FV_EXCHANGE_COPY (0) NCCL
+                                  send/recv between processes (packed, then unpacked) and
+                                  device reads within one; FV_EXCHANGE_P2P (1) a push kernel
+                                  stores them straight into the reading part's stage buffer
+                                  (peer memory through CUDA IPC between processes), then
+                                  releases an epoch flag there, and the reader waits for it
+                                  (a bounded poll) before the stage that reads them */
+    int64_t wait_polls;        /* P2P: polls of one halo wait before it gives up (0 = 2^24) */
     double timeout_ms;         /* with NCCL: the longest wait for one chunk of steps (0 = 300 s).
                                   A chunk that makes no progress within it, or an NCCL error,
                                   aborts the communicator and fv_group_run returns FV_ERR_COMM
@@ -315,9 +324,10 @@ int fv_group_set_state(fv_group* g, const double* q);
 int fv_group_get_state(fv_group* g, double* q);
 /* fv_run for the decomposition (collective): same options and results. */
 int fv_group_run(fv_group* g, const fv_run_options* opt, fv_run_info* info);
-/* out[7]: local parts, owned real cells, halo cells received per stage,
+/* out[8]: local parts, owned real cells, halo cells received per stage,
  * cells sent per stage, tiles, 1 if an NCCL communicator exists, band tiles
- * (computed before the exchange; -1 when the exchange follows all tiles) */
+ * (computed before the exchange; -1 when the exchange follows all tiles),
+ * the transport in use (FV_EXCHANGE_*) */
 int fv_group_info(fv_group* g, int64_t* out);
 int fv_group_last_run_stats(fv_group* g, double* device_ms, int64_t* kernel_launches);
 /* Host-only: the plan of part `part` of n_parts.  sizes[11]: local real cells,

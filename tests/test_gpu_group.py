@@ -88,6 +88,43 @@ def test_group_exchange_through_nccl(prec, serial):
         assert q.tobytes() == q1.tobytes()
 
 
+@pytest.mark.parametrize("case", ["forward_step", "naca_local_dt", "sod_first_order"])
+@pytest.mark.parametrize("prec", ["fp64_exact", "fp32"])
+def test_group_p2p_transport(case, prec):
+    """The P2P transport: each part's push kernel stores the states other
+    parts read straight into their stage buffers and releases an epoch flag
+    in each; every part waits (a bounded poll) for its senders' epochs before
+    the dt kernel and each stage.  Overlapped and serial, with and without a
+    communicator (dt records and residual sums through NCCL): the same bits
+    as the single solver, and no wait gives up (fv_group_run would report
+    it)."""
+    import fvgpu
+    mk_em, mk_ph, ic, alpha, steps = _cases()[case]
+    em, ph = mk_em(), mk_ph()
+    mesh = fvgpu.Mesh.from_elements(em)
+    geo = mesh.geometry()
+    q0 = np.ascontiguousarray(ic(type("G", (), {"n_total": mesh.n_total, "ccx": geo["ccx"]})()), np.float64).ravel()
+    r1, q1 = _single(mesh, ph, prec, q0, alpha, steps)
+    for n_parts, serial, nccl in ((2, False, False), (3, True, False), (4, False, True)):
+        grp = fvgpu.Group(mesh, ph, prec, n_parts=n_parts, transport="p2p", serial_exchange=serial,
+                          nccl_local=nccl, wait_polls=200000)
+        inf = grp.info()
+        assert inf["transport"] == "p2p" and inf["nccl"] == nccl
+        grp.set_state(q0)
+        r = grp.run(steps, alpha=alpha)
+        r2 = grp.run(steps + 3, alpha=alpha, restart=False)
+        q = grp.get_state()
+        grp.close()
+        assert r["step"] == steps and r2["step"] == steps + 3
+        s = fvgpu.Solver(mesh, ph, prec)
+        s.set_state(q0)
+        s.run(steps + 3, alpha=alpha)
+        q3 = s.get_state()
+        s.close()
+        assert q.tobytes() == q3.tobytes(), (n_parts, serial, nccl)
+    del r1, q1
+
+
 def test_group_continues_across_runs_and_schedules():
     """run(4) then run(11, restart=False) equals run(11); tile sizes and the
     work-list schedule change nothing."""
