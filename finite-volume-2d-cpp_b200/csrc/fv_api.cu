@@ -858,6 +858,9 @@ int step_stage(fv_solver* s, const std::vector<double>& alpha, int k, StepCursor
         tile::launch_stage(s->precision, TP, so, st, pdl); ++n; mark(KK_STAGE);
     } else if (s->fused) {
         so.work = c.worklist ? s->work + k : nullptr;
+        so.remote = c.worklist ? nullptr : c.remote;
+        so.stage = k;
+        so.stages = ns;
         tile::launch_fused(s->precision, c.FPl, so, st, pdl, s->n_tiles, s->work_grid); ++n; mark(KK_FUSED);
     } else {
         tile::launch_stage(s->precision, TP, so, st, pdl); ++n; mark(KK_STAGE);

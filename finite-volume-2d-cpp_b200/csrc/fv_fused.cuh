@@ -134,7 +134,7 @@ __device__ __forceinline__ void cent(const uint4* C, int r, S& x, S& y) {
 }
 
 // One tile t.  Returns false when the step is inactive (nothing written).
-template <class M, int FLUX>
+template <class M, int FLUX, bool REMOTE = false>
 __device__ __forceinline__ bool fused_tile(const FusedParams& FP, const TileIO& io, const int t) {
     using S = typename M::S;
     using FT = typename std::conditional<M::exact, double, S>::type;  // flux storage
@@ -215,6 +215,35 @@ __device__ __forceinline__ bool fused_tile(const FusedParams& FP, const TileIO& 
     for (int r = l; r < nown; r += blockDim.x) PL::stage(Q, L.ls, r, (const S*)io.q_stage + 4 * (size_t)(c0 + r));
     cpa_commit();
     cpa_wait_prior();  // the constant group: edges, halo indices
+    if constexpr (REMOTE) {
+        // a band tile reads halo cells: wait for the senders' epoch of this
+        // stage's input (bounded; a tile that gives up is skipped)
+        __shared__ int s_gave_up;
+        const RemoteIO& R = *io.remote;
+        if (threadIdx.x == 0) {
+            s_gave_up = 0;
+            if (!inactive && t < R.n_band_tiles) {
+                const unsigned long long need = io.ctrl->step * (unsigned long long)io.stages + io.stage;
+                for (int i = 0; i < R.n_src && !s_gave_up; ++i) {
+                    const unsigned long long* f = R.my_flags + R.src[i];
+                    long long polls = 0;
+                    while (ld_acquire_sys_u64(f) < need) {
+                        if (++polls > R.limit) {
+                            atomicExch(R.err, 1);
+                            s_gave_up = 1;
+                            break;
+                        }
+                        __nanosleep(256);
+                    }
+                }
+            }
+        }
+        __syncthreads();
+        if (s_gave_up) {
+            cpa_wait();  // this tile's copies in flight land before it leaves
+            return false;
+        }
+    }
     __syncthreads();
     for (int h = l; h < n1 + n2; h += blockDim.x) {
         const int g = shalo[h];
@@ -481,6 +510,19 @@ __device__ __forceinline__ bool fused_tile(const FusedParams& FP, const TileIO& 
             st<S, V>((S*)io.s_out, c, qs);
             if (io.write_f64) st<double, V>(io.q_out, c, qnew);
         }
+        if constexpr (REMOTE) {
+            // this cell's new state into every part that reads it
+            const RemoteIO& R = *io.remote;
+            if (c < R.n_band) {
+                S qs[V];
+#pragma unroll
+                for (int k = 0; k < V; ++k) qs[k] = (S)qnew[k];
+                for (int i = R.cell_off[c]; i < R.cell_off[c + 1]; ++i) {
+                    const int2 d = R.cell_dst[i];
+                    st<S, V>((S*)R.dst[d.x], d.y, qs);
+                }
+            }
+        }
         if (has_ghost) {
             S gxs[V], gys[V];
             PL::get(GX, L.lg, l, gxs);
@@ -520,6 +562,15 @@ __device__ __forceinline__ bool fused_tile(const FusedParams& FP, const TileIO& 
                         st<double, V>(io.q_out, g, bd);
                     }
                 }
+                if constexpr (REMOTE) {
+                    const RemoteIO& R = *io.remote;
+                    const int go = g - N;
+                    if (go < R.n_own_ghost)
+                        for (int i = R.ghost_off[go]; i < R.ghost_off[go + 1]; ++i) {
+                            const int2 d = R.ghost_dst[i];
+                            st<S, V>((S*)R.dst[d.x], d.y, b);
+                        }
+                }
             }
         }
         if (io.partials != nullptr) {
@@ -548,14 +599,32 @@ __device__ __forceinline__ bool fused_tile(const FusedParams& FP, const TileIO& 
             }
         }
     }
+    if constexpr (REMOTE) {
+        // every band tile counts itself once its stores are visible; the
+        // last one releases this stage's epoch to the readers
+        const RemoteIO& R = *io.remote;
+        if (t < R.n_band_tiles) {
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                __threadfence_system();
+                const unsigned long long epoch = io.ctrl->step * (unsigned long long)io.stages + io.stage + 1;
+                const unsigned long long done = atomicAdd(R.ctr, 1ull) + 1ull;
+                if (done == epoch * (unsigned long long)R.n_band_tiles) {
+                    __threadfence_system();
+                    for (int d = 0; d < R.n_dst; ++d) st_release_sys_u64(R.flag[d], epoch);
+                }
+            }
+        }
+    }
     return true;
 }
 
-// One CTA per tile.
-template <class M, int FLUX>
+// One CTA per tile.  REMOTE: a decomposition part exchanging its halo
+// inside the launch (io.remote).
+template <class M, int FLUX, bool REMOTE = false>
 __global__ void __launch_bounds__(kTileMax) k_tile_fused(FusedParams FP, TileIO io) {
     pdl_trigger();
-    fused_tile<M, FLUX>(FP, io, io.t0 + (int)blockIdx.x);
+    fused_tile<M, FLUX, REMOTE>(FP, io, io.t0 + (int)blockIdx.x);
 }
 
 // Work-list schedule: as many CTAs as fit on the device at once, each taking
@@ -588,6 +657,7 @@ struct FusedLaunch {
         cudaError_t e = cudaSuccess;
         const size_t bytes = smem(FP);
         for (const void* fn : {(const void*)k_tile_fused<M, 1>, (const void*)k_tile_fused<M, 2>,
+                               (const void*)k_tile_fused<M, 1, true>, (const void*)k_tile_fused<M, 2, true>,
                                (const void*)k_tile_fused_work<M, 1>, (const void*)k_tile_fused_work<M, 2>}) {
             // only ever raised: a solver created earlier may launch with more
             cudaFuncAttributes fa{};
@@ -624,6 +694,9 @@ struct FusedLaunch {
         if (io.work) {
             if (FP.P.flux == 1) cudaLaunchKernelEx(&cfg, k_tile_fused_work<M, 1>, FP, io, n_tiles);
             else cudaLaunchKernelEx(&cfg, k_tile_fused_work<M, 2>, FP, io, n_tiles);
+        } else if (io.remote) {
+            if (FP.P.flux == 1) cudaLaunchKernelEx(&cfg, k_tile_fused<M, 1, true>, FP, io);
+            else cudaLaunchKernelEx(&cfg, k_tile_fused<M, 2, true>, FP, io);
         } else {
             if (FP.P.flux == 1) cudaLaunchKernelEx(&cfg, k_tile_fused<M, 1>, FP, io);
             else cudaLaunchKernelEx(&cfg, k_tile_fused<M, 2>, FP, io);

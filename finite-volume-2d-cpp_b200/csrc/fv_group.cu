@@ -161,7 +161,6 @@ int blocks_of(int64_t n) { return (int)((n + kBlock - 1) / kBlock); }
 // s's outputs of stage k of step n are complete in this part's buffers once
 // it reads n * stages + k + 1.  Epochs come from the step counter in device
 // memory, so captured graphs replay them.
-constexpr int kMaxPeers = 16;  // parts a local part sends to
 __device__ __forceinline__ unsigned long long ld_acquire_sys(const unsigned long long* p) {
     unsigned long long v;
     asm volatile("ld.acquire.sys.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
@@ -281,6 +280,10 @@ struct fv_group {
     // buffers by role (tmp[0], tmp[1], sbase[0], sbase[1]) and flag word per
     // slot, and the count of its completed push CTAs
     bool p2p = false;
+    // fused parts: the exchange inside each stage launch (RemoteIO per local
+    // part and output role, device memory), no push or wait launches per stage
+    bool fused_p2p = false;
+    fvgpu::RemoteIO* rio = nullptr;       // [local parts][4]
     struct Push {
         int32_t *slot = nullptr, *from = nullptr, *to = nullptr;
         int64_t n = 0;
@@ -404,6 +407,15 @@ int64_t group_step(fv_group* g, const std::vector<double>& alpha, int b, bool fi
     }
     GK(cudaGetLastError());
     for (int k = 0; k < S; ++k) {
+        if (g->fused_p2p) {
+            // one launch per part: its band tiles wait for the senders,
+            // compute, store into the readers' buffers and release the epoch
+            for (int j = 0; j < nl; ++j) {
+                cur[j].remote = g->rio + (size_t)j * 4 + role_of(k);
+                n += step_stage(g->parts[j], alpha, k, cur[j], nullptr);
+            }
+            continue;
+        }
         if (g->p2p && k > 0) {
             int rc = p2p_wait(g, S, k, st);
             if (rc) return rc;
@@ -644,6 +656,68 @@ int setup_p2p(fv_group* g, const HostMesh& gm, long long wait_limit) {
     g->wp.err = g->err;
     g->wp.ctrl = g->parts[0]->ctrl;
     g->wp.limit = wait_limit;
+    // fused parts with one CTA per tile: the stage launches exchange the
+    // halo themselves (destinations by sending cell and by sending ghost)
+    g->fused_p2p = true;
+    for (fv_solver* s : g->parts)
+        if (!s->fused || s->sched == FV_SCHED_WORKLIST) g->fused_p2p = false;
+    if (!g->fused_p2p) return FV_OK;
+    GK(g->alloc(&g->rio, (size_t)nl * 4));
+    for (int j = 0; j < nl; ++j) {
+        const PartPlan& pp = g->plans[j];
+        const fv_group::Push& ps = g->push[j];
+        std::vector<int32_t> slot((size_t)ps.n), from((size_t)ps.n), to((size_t)ps.n);
+        if (ps.n) {
+            GK(cudaMemcpy(slot.data(), ps.slot, ps.n * 4, cudaMemcpyDeviceToHost));
+            GK(cudaMemcpy(from.data(), ps.from, ps.n * 4, cudaMemcpyDeviceToHost));
+            GK(cudaMemcpy(to.data(), ps.to, ps.n * 4, cudaMemcpyDeviceToHost));
+        }
+        const int64_t nr = g->parts[j]->n_real;
+        std::vector<int32_t> coff(pp.n_band + 1, 0), goff(pp.n_own_ghost + 1, 0);
+        for (int64_t i = 0; i < ps.n; ++i) {
+            if (from[i] < nr) {
+                if (from[i] >= pp.n_band) return set_error(FV_ERR_ARG, "internal error: a sent cell outside the band");
+                ++coff[from[i] + 1];
+            } else {
+                if (from[i] - nr >= pp.n_own_ghost) return set_error(FV_ERR_ARG, "internal error: a sent ghost not owned");
+                ++goff[from[i] - nr + 1];
+            }
+        }
+        for (size_t i = 1; i < coff.size(); ++i) coff[i] += coff[i - 1];
+        for (size_t i = 1; i < goff.size(); ++i) goff[i] += goff[i - 1];
+        std::vector<int2> cdst((size_t)coff.back()), gdst((size_t)goff.back());
+        std::vector<int32_t> cfill(coff.begin(), coff.end() - 1), gfill(goff.begin(), goff.end() - 1);
+        for (int64_t i = 0; i < ps.n; ++i) {
+            if (from[i] < nr) cdst[(size_t)cfill[from[i]]++] = make_int2(slot[i], to[i]);
+            else gdst[(size_t)gfill[from[i] - nr]++] = make_int2(slot[i], to[i]);
+        }
+        int32_t *d_coff = nullptr, *d_goff = nullptr;
+        int2 *d_cdst = nullptr, *d_gdst = nullptr;
+        GK(g->alloc(&d_coff, coff.size()));
+        GK(g->alloc(&d_goff, goff.size()));
+        GK(g->alloc(&d_cdst, cdst.size()));
+        GK(g->alloc(&d_gdst, gdst.size()));
+        GK(cudaMemcpy(d_coff, coff.data(), coff.size() * 4, cudaMemcpyHostToDevice));
+        GK(cudaMemcpy(d_goff, goff.data(), goff.size() * 4, cudaMemcpyHostToDevice));
+        if (!cdst.empty()) GK(cudaMemcpy(d_cdst, cdst.data(), cdst.size() * sizeof(int2), cudaMemcpyHostToDevice));
+        if (!gdst.empty()) GK(cudaMemcpy(d_gdst, gdst.data(), gdst.size() * sizeof(int2), cudaMemcpyHostToDevice));
+        for (int role = 0; role < 4; ++role) {
+            fvgpu::RemoteIO R{};
+            R.n_dst = ps.n_dst;
+            for (int d = 0; d < ps.n_dst; ++d) { R.dst[d] = ps.buf[role][d]; R.flag[d] = ps.flag[d]; }
+            R.cell_off = d_coff; R.cell_dst = d_cdst; R.ghost_off = d_goff; R.ghost_dst = d_gdst;
+            R.n_band = (int)pp.n_band;
+            R.n_band_tiles = g->band_tiles[j];
+            R.n_own_ghost = (int)pp.n_own_ghost;
+            R.ctr = ps.ctr;
+            R.my_flags = g->wp.flags[j];
+            R.src = g->wp.src[j];
+            R.n_src = g->wp.n_src[j];
+            R.err = g->err + j;
+            R.limit = wait_limit;
+            GK(cudaMemcpy(g->rio + (size_t)j * 4 + role, &R, sizeof(R), cudaMemcpyHostToDevice));
+        }
+    }
     return FV_OK;
 }
 
@@ -878,6 +952,8 @@ int fv_group_create(const fv_mesh* fm, const fv_physics* ph, int32_t precision, 
         g->p2p = true;
         int rc2 = setup_p2p(g.get(), fm->m, o->wait_polls > 0 ? o->wait_polls : (1ll << 24));
         if (rc2) return rc2;
+        // the in-launch exchange overlaps the interior tiles by itself
+        if (g->fused_p2p) g->overlap = false;
     } else if (o->transport != FV_EXCHANGE_COPY && o->transport != FV_EXCHANGE_P2P) {
         return set_error(FV_ERR_ARG, "unknown transport");
     }
@@ -1060,7 +1136,7 @@ int fv_group_info(fv_group* g, int64_t* out) {
     out[5] = g->comm != nullptr ? 1 : 0;
     int64_t band = 0;
     for (int b : g->band_tiles) band += b;
-    out[6] = g->overlap ? band : -1;
+    out[6] = (g->overlap || g->fused_p2p) ? band : -1;
     out[7] = g->p2p ? FV_EXCHANGE_P2P : FV_EXCHANGE_COPY;
     return FV_OK;
 }

@@ -128,6 +128,8 @@ struct StepCursor {
     int b = 0;
     const void* in = nullptr;
     void* out = nullptr;
+    // the next fused stage launch exchanges its halo inside (device memory), or nullptr
+    const RemoteIO* remote = nullptr;
 };
 // with_dt = false: step_open leaves the dt kernel to a later step_dt (a
 // decomposition waits for its halo in between).

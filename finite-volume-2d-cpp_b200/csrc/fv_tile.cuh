@@ -75,8 +75,47 @@ struct TileIO {
     int* work;                 // fused stage kernel, work-list schedule: this launch's tile counter
     int* work_reset;           // dt kernel: tile counters zeroed after the dependency wait, or nullptr
     int t0;                    // fused stage kernel, one CTA per tile: the first tile of this launch
+    const struct RemoteIO* remote;  // fused stage kernel of a decomposition's part: the halo
+                                    // exchange done inside the launch (device memory), or nullptr
+    int stage, stages;         // with remote: this launch's RK stage, and the step's stages
 };
 constexpr int kWorkSlots = 8;  // tile counters of the work-list schedule (one per RK stage)
+
+// A decomposition part's halo exchange inside its fused stage launches (the
+// P2P transport).  Tiles [0, n_band_tiles) hold every owned cell other parts
+// read (local cells [0, n_band)).  Those tiles, and only those, read halo
+// cells: after the dependency wait their thread 0 polls the flag word of
+// every sending part until it holds the epoch of the stage's input
+// (step * stages + stage), giving up after `limit` polls (err, and the tile
+// is skipped).  After the update each such tile stores its cells' and
+// ghosts' new states into the reading parts' buffers of this stage's
+// output, and the last of them to finish releases step * stages + stage + 1
+// into each reader's flag word for this part.
+constexpr int kMaxPeers = 16;
+struct RemoteIO {
+    int n_dst;
+    void* dst[kMaxPeers];                     // each reader's buffer of this stage's output
+    unsigned long long* flag[kMaxPeers];      // this part's flag word in each reader
+    const int32_t* cell_off;                  // [n_band + 1] destinations of owned cell c
+    const int2* cell_dst;                     // (reader slot, the cell's index there)
+    const int32_t* ghost_off;                 // [n_own_ghost + 1] destinations of owned ghost g - n_real
+    const int2* ghost_dst;
+    int n_band, n_band_tiles, n_own_ghost;
+    unsigned long long* ctr;                  // band tiles completed (monotonic)
+    const unsigned long long* my_flags;       // [n_parts] flag words the senders write here
+    const int32_t* src;                       // the parts that send to this one
+    int n_src;
+    int* err;
+    long long limit;
+};
+__device__ __forceinline__ unsigned long long ld_acquire_sys_u64(const unsigned long long* p) {
+    unsigned long long v;
+    asm volatile("ld.acquire.sys.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release_sys_u64(unsigned long long* p, unsigned long long v) {
+    asm volatile("st.release.sys.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
 
 __device__ __forceinline__ unsigned long long tkey(double x) {
     if (x != x) return ~0ull;
