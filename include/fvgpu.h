@@ -300,11 +300,12 @@ typedef struct {
                                   1: the exchange follows all tiles of the stage. */
     int32_t transport;         /* halo states between parts: FV_EXCHANGE_COPY (0) NCCL
                                   send/recv between processes (packed, then unpacked) and
-                                  device reads within one; FV_EXCHANGE_P2P (1) a push kernel
-                                  stores them straight into the reading part's stage buffer
-                                  (peer memory through CUDA IPC between processes), then
-                                  releases an epoch flag there, and the reader waits for it
-                                  (a bounded poll) before the stage that reads them */
+                                  device reads within one; FV_EXCHANGE_P2P (1) stored straight
+                                  into the reading part's stage buffer (peer memory through
+                                  CUDA IPC between processes) by the fused stage launch that
+                                  computes them (a push kernel after first-order stages), which
+                                  then releases an epoch flag there; the reader waits for it (a
+                                  bounded poll) before reading them */
     int64_t wait_polls;        /* P2P: polls of one halo wait before it gives up (0 = 2^24) */
     double timeout_ms;         /* with NCCL: the longest wait for one chunk of steps (0 = 300 s).
                                   A chunk that makes no progress within it, or an NCCL error,

@@ -1,6 +1,7 @@
 """The P2P halo protocol of fv_group_run (finite-volume-2d-cpp_b200/csrc/
-fv_group.cu: group_step, k_p2p_push, k_p2p_wait), checked as a model under
-random interleavings of the processes.
+fv_group.cu: group_step, k_p2p_push, k_p2p_wait; and the same schedule
+inside the fused stage launch, fv_fused.cuh fused_tile<..., REMOTE>), checked
+as a model under random interleavings of the processes.
 
 Each simulated process owns one part and runs the step schedule of
 group_step with the P2P transport:

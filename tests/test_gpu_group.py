@@ -91,13 +91,14 @@ def test_group_exchange_through_nccl(prec, serial):
 @pytest.mark.parametrize("case", ["forward_step", "naca_local_dt", "sod_first_order"])
 @pytest.mark.parametrize("prec", ["fp64_exact", "fp32"])
 def test_group_p2p_transport(case, prec):
-    """The P2P transport: each part's push kernel stores the states other
-    parts read straight into their stage buffers and releases an epoch flag
-    in each; every part waits (a bounded poll) for its senders' epochs before
-    the dt kernel and each stage.  Overlapped and serial, with and without a
-    communicator (dt records and residual sums through NCCL): the same bits
-    as the single solver, and no wait gives up (fv_group_run would report
-    it)."""
+    """The P2P transport: the states other parts read are stored straight
+    into their stage buffers, and an epoch flag is released in each, by the
+    fused stage launch itself (second order: its band tiles wait for the
+    senders, compute, store and count) or by a push kernel (first order);
+    a bounded wait precedes the dt kernel (and, first order, each stage).
+    With and without a communicator (dt records and residual sums through
+    NCCL), across a continued run: the same bits as the single solver, and no
+    wait gives up (fv_group_run would report it)."""
     import fvgpu
     mk_em, mk_ph, ic, alpha, steps = _cases()[case]
     em, ph = mk_em(), mk_ph()
