@@ -473,9 +473,11 @@ int fv_solver_create_ex(const fv_mesh* fm, const fv_physics* ph, int32_t precisi
                 if (sk == FV_STAGE_HYBRID && sched == FV_SCHED_WORKLIST)
                     return fail(FV_ERR_ARG, "the work-list schedule needs the dt kernel of the fused layout");
                 s->sched = sched;
-                // automatic choice: the split first stage (its gradient kernel
-                // computes dt) saves the separate dt kernel of the fused layout
-                s->split_first = sk == FV_STAGE_HYBRID || (sk == FV_STAGE_AUTO && sched != FV_SCHED_WORKLIST);
+                // automatic choice: in FP32 the split first stage (its gradient
+                // kernel computes dt) saves more than it costs; in FP64 the
+                // fused first stage and the separate dt kernel are faster
+                s->split_first = sk == FV_STAGE_HYBRID ||
+                                 (sk == FV_STAGE_AUTO && sched != FV_SCHED_WORKLIST && precision == FV_PREC_FP32);
             }
         }
     }

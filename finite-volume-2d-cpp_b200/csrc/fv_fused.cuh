@@ -134,7 +134,9 @@ __device__ __forceinline__ void cent(const uint4* C, int r, S& x, S& y) {
 }
 
 // One tile t.  Returns false when the step is inactive (nothing written).
-template <class M, int FLUX, bool REMOTE = false>
+// PART: a decomposition part's tile, whose owned cells come from the tile
+// info (a part owns fewer real cells than its local mesh holds).
+template <class M, int FLUX, bool REMOTE = false, bool PART = false>
 __device__ __forceinline__ bool fused_tile(const FusedParams& FP, const TileIO& io, const int t) {
     using S = typename M::S;
     using FT = typename std::conditional<M::exact, double, S>::type;  // flux storage
@@ -147,7 +149,7 @@ __device__ __forceinline__ bool fused_tile(const FusedParams& FP, const TileIO& 
     const int4 ia = FP.info[2 * t], ib = FP.info[2 * t + 1];
     const int edge_off = ia.x, n_edges = ia.y, n_flux = ia.z, halo_off = ia.w;
     const int n1 = ib.x, n2 = ib.y, face_off = ib.z;
-    const int c0 = t * T, nown = min(T, P.n_own - c0);
+    const int c0 = t * T, nown = PART ? ib.w : min(T, N - c0);
     const FusedSmem L = fused_smem<M>(FP.max_slots, FP.max_grad, FP.max_edges, FP.max_flux, FP.T);
     uint4* Q = reinterpret_cast<uint4*>(smem_raw + L.q);
     uint4* C = reinterpret_cast<uint4*>(smem_raw + L.c);
@@ -619,12 +621,26 @@ __device__ __forceinline__ bool fused_tile(const FusedParams& FP, const TileIO& 
     return true;
 }
 
-// One CTA per tile.  REMOTE: a decomposition part exchanging its halo
-// inside the launch (io.remote).
-template <class M, int FLUX, bool REMOTE = false>
+// One CTA per tile, tiles [0, grid).
+template <class M, int FLUX>
 __global__ void __launch_bounds__(kTileMax) k_tile_fused(FusedParams FP, TileIO io) {
     pdl_trigger();
-    fused_tile<M, FLUX, REMOTE>(FP, io, io.t0 + (int)blockIdx.x);
+    fused_tile<M, FLUX, false, false>(FP, io, (int)blockIdx.x);
+}
+
+// A decomposition part's launches, one CTA per tile.  MODE 1: tiles
+// [io.t0, io.t0 + grid) (the band and interior launches); MODE 2: the halo
+// exchange inside the launch (io.remote).  Kept apart from k_tile_fused,
+// whose register allocation and code the tile offset and a register cap
+// make slower; here the cap holds FP32 to 64 registers (8 blocks of
+// 128-cell tiles per SM) and FP64 to 128 (4 blocks), which these modes
+// otherwise exceed.
+template <class M>
+constexpr int fused_part_min_blocks() { return sizeof(typename M::S) == 4 ? 4 : 2; }
+template <class M, int FLUX, int MODE>
+__global__ void __launch_bounds__(kTileMax, fused_part_min_blocks<M>()) k_tile_fused_part(FusedParams FP, TileIO io) {
+    pdl_trigger();
+    fused_tile<M, FLUX, MODE == 2, true>(FP, io, (MODE == 1 ? io.t0 : 0) + (int)blockIdx.x);
 }
 
 // Work-list schedule: as many CTAs as fit on the device at once, each taking
@@ -641,7 +657,7 @@ __global__ void __launch_bounds__(kTileMax) k_tile_fused_work(FusedParams FP, Ti
         __syncthreads();
         const int t = s_t;
         if (t >= n_tiles) return;
-        if (!fused_tile<M, FLUX>(FP, io, t)) return;
+        if (!fused_tile<M, FLUX, false, true>(FP, io, t)) return;
         __syncthreads();  // every thread is done with this tile's shared memory (and s_t)
     }
 }
@@ -657,7 +673,8 @@ struct FusedLaunch {
         cudaError_t e = cudaSuccess;
         const size_t bytes = smem(FP);
         for (const void* fn : {(const void*)k_tile_fused<M, 1>, (const void*)k_tile_fused<M, 2>,
-                               (const void*)k_tile_fused<M, 1, true>, (const void*)k_tile_fused<M, 2, true>,
+                               (const void*)k_tile_fused_part<M, 1, 1>, (const void*)k_tile_fused_part<M, 2, 1>,
+                               (const void*)k_tile_fused_part<M, 1, 2>, (const void*)k_tile_fused_part<M, 2, 2>,
                                (const void*)k_tile_fused_work<M, 1>, (const void*)k_tile_fused_work<M, 2>}) {
             // only ever raised: a solver created earlier may launch with more
             cudaFuncAttributes fa{};
@@ -695,8 +712,11 @@ struct FusedLaunch {
             if (FP.P.flux == 1) cudaLaunchKernelEx(&cfg, k_tile_fused_work<M, 1>, FP, io, n_tiles);
             else cudaLaunchKernelEx(&cfg, k_tile_fused_work<M, 2>, FP, io, n_tiles);
         } else if (io.remote) {
-            if (FP.P.flux == 1) cudaLaunchKernelEx(&cfg, k_tile_fused<M, 1, true>, FP, io);
-            else cudaLaunchKernelEx(&cfg, k_tile_fused<M, 2, true>, FP, io);
+            if (FP.P.flux == 1) cudaLaunchKernelEx(&cfg, k_tile_fused_part<M, 1, 2>, FP, io);
+            else cudaLaunchKernelEx(&cfg, k_tile_fused_part<M, 2, 2>, FP, io);
+        } else if (io.t0 != 0 || FP.P.n_own != FP.P.n_real) {
+            if (FP.P.flux == 1) cudaLaunchKernelEx(&cfg, k_tile_fused_part<M, 1, 1>, FP, io);
+            else cudaLaunchKernelEx(&cfg, k_tile_fused_part<M, 2, 1>, FP, io);
         } else {
             if (FP.P.flux == 1) cudaLaunchKernelEx(&cfg, k_tile_fused<M, 1>, FP, io);
             else cudaLaunchKernelEx(&cfg, k_tile_fused<M, 2>, FP, io);

@@ -505,7 +505,7 @@ void build_tiles2(const HostMesh& m, const FaceArrays& fa, int T, Tile2Arrays& t
         }
         int32_t* inf = &ta.info[(size_t)8 * t];
         inf[0] = edge_off; inf[1] = n_edges; inf[2] = n_flux; inf[3] = halo_off;
-        inf[4] = n1; inf[5] = n2; inf[6] = face_off; inf[7] = 0;
+        inf[4] = n1; inf[5] = n2; inf[6] = face_off; inf[7] = (int32_t)(c1 - c0);
         ta.max_slots = std::max(ta.max_slots, T + n1 + n2);
         ta.max_grad = std::max(ta.max_grad, T + n1);
         ta.max_edges = std::max(ta.max_edges, (n_edges + 3) / 4 * 4);

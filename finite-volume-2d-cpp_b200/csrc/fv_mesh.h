@@ -96,7 +96,7 @@ void build_tiles(const HostMesh& m, const FaceArrays& fa, int tile_cells, TileAr
 struct Tile2Arrays {
     int tile_cells = 0, n_tiles = 0;
     int max_slots = 0, max_grad = 0, max_edges = 0, max_flux = 0;  // max_edges: a multiple of 4
-    std::vector<int32_t> info;        // [n_tiles][8]: edge_off, n_edges, n_flux, halo_off, n1, n2, face_off, 0
+    std::vector<int32_t> info;        // [n_tiles][8]: edge_off, n_edges, n_flux, halo_off, n1, n2, face_off, owned cells
     std::vector<int32_t> halo;        // device cell index of each ring-1, then ring-2 slot
     std::vector<uint32_t> edge_ij;    // local i | local j << 16, reference orientation; each
                                       // tile's run padded to a multiple of 4 entries

@@ -224,9 +224,9 @@ typedef struct {
     int32_t tile_cells;  /* cells per tile = threads per CTA: 64, 128 or 256 (0 = 128) */
     /* Stage kernels of the second-order Euler kinds (Roe fluxes, no
      * diffusive terms, no residual smoothing):
-     * FV_STAGE_AUTO (0): FV_STAGE_HYBRID where the physics allow the fused
-     *   kernel (FV_STAGE_FUSED with the work-list schedule), otherwise
-     *   FV_STAGE_SPLIT.
+     * FV_STAGE_AUTO (0): where the physics allow the fused kernel,
+     *   FV_STAGE_HYBRID in FP32 and FV_STAGE_FUSED in FP64 and FP64_EXACT (and
+     *   with the work-list schedule); otherwise FV_STAGE_SPLIT.
      * FV_STAGE_SPLIT (1): a gradient + limiter kernel and a flux + update
      *   kernel per stage (the first stage's gradient kernel also computes dt).
      * FV_STAGE_FUSED (2): one fused kernel per RK stage (gradients, limiter,

@@ -367,10 +367,12 @@ def test_fused_stage_kernel_is_chosen_where_the_physics_allow():
     for name in sorted(CASES):
         case = CASES[name]
         ph = case["phys"]()
-        s = fvgpu.Solver(fvgpu.Mesh.from_elements(case["mesh"]()), ph, "fp64")
         fusable = ph.V == 4 and ph.order2 and ph.flux in ("roe_fs", "roe_st") and not ph.diffusive
-        assert s.stage_kernels == ("hybrid" if fusable else "split"), name
-        s.close()
+        mesh = fvgpu.Mesh.from_elements(case["mesh"]())
+        for prec, layout in (("fp64", "fused"), ("fp32", "hybrid")):
+            s = fvgpu.Solver(mesh, ph, prec)
+            assert s.stage_kernels == (layout if fusable else "split"), (name, prec)
+            s.close()
     case = CASES["heat"]
     with pytest.raises(fvgpu.FvError) as e:
         fvgpu.Solver(fvgpu.Mesh.from_elements(case["mesh"]()), case["phys"](), "fp64", stage_kernels="fused")
