@@ -631,14 +631,12 @@ __global__ void __launch_bounds__(kTileMax) k_tile_fused(FusedParams FP, TileIO 
 // A decomposition part's launches, one CTA per tile.  MODE 1: tiles
 // [io.t0, io.t0 + grid) (the band and interior launches); MODE 2: the halo
 // exchange inside the launch (io.remote).  Kept apart from k_tile_fused,
-// whose register allocation and code the tile offset and a register cap
-// make slower; here the cap holds FP32 to 64 registers (8 blocks of
-// 128-cell tiles per SM) and FP64 to 128 (4 blocks), which these modes
-// otherwise exceed.
-template <class M>
-constexpr int fused_part_min_blocks() { return sizeof(typename M::S) == 4 ? 4 : 2; }
+// whose register allocation the tile offset and the owned count from the
+// tile info upset (FP32: 80 registers instead of 64, 5.7 % slower); a
+// register cap on these launches restores 64 registers but runs slower
+// still, so they keep the compiler's choice.
 template <class M, int FLUX, int MODE>
-__global__ void __launch_bounds__(kTileMax, fused_part_min_blocks<M>()) k_tile_fused_part(FusedParams FP, TileIO io) {
+__global__ void __launch_bounds__(kTileMax) k_tile_fused_part(FusedParams FP, TileIO io) {
     pdl_trigger();
     fused_tile<M, FLUX, MODE == 2, true>(FP, io, (MODE == 1 ? io.t0 : 0) + (int)blockIdx.x);
 }
