@@ -836,9 +836,9 @@ int step_stage(fv_solver* s, const std::vector<double>& alpha, int k, StepCursor
     so.write_f64 = last ? 1 : 0;
     if (r) {
         if (!s->fused || c.worklist || c.split_first) return -1;
-        so.t0 = r->t0;
+        const PartIO pio{r->t0, nullptr, k, ns};
         if (r->n > 0) {
-            tile::launch_fused(s->precision, c.FPl, so, r->stream ? r->stream : st, r->pdl, r->n, r->n);
+            tile::launch_fused(s->precision, c.FPl, so, r->stream ? r->stream : st, r->pdl, r->n, r->n, &pio);
             ++n; mark(KK_FUSED);
         }
         c.out = out_s;
@@ -860,10 +860,9 @@ int step_stage(fv_solver* s, const std::vector<double>& alpha, int k, StepCursor
         tile::launch_stage(s->precision, TP, so, st, pdl); ++n; mark(KK_STAGE);
     } else if (s->fused) {
         so.work = c.worklist ? s->work + k : nullptr;
-        so.remote = c.worklist ? nullptr : c.remote;
-        so.stage = k;
-        so.stages = ns;
-        tile::launch_fused(s->precision, c.FPl, so, st, pdl, s->n_tiles, s->work_grid); ++n; mark(KK_FUSED);
+        const PartIO pio{0, c.worklist ? nullptr : c.remote, k, ns};
+        tile::launch_fused(s->precision, c.FPl, so, st, pdl, s->n_tiles, s->work_grid, c.part ? &pio : nullptr);
+        ++n; mark(KK_FUSED);
     } else {
         tile::launch_stage(s->precision, TP, so, st, pdl); ++n; mark(KK_STAGE);
     }

@@ -137,7 +137,7 @@ __device__ __forceinline__ void cent(const uint4* C, int r, S& x, S& y) {
 // PART: a decomposition part's tile, whose owned cells come from the tile
 // info (a part owns fewer real cells than its local mesh holds).
 template <class M, int FLUX, bool REMOTE = false, bool PART = false>
-__device__ __forceinline__ bool fused_tile(const FusedParams& FP, const TileIO& io, const int t) {
+__device__ __forceinline__ bool fused_tile(const FusedParams& FP, const TileIO& io, const int t, const PartIO& pio) {
     using S = typename M::S;
     using FT = typename std::conditional<M::exact, double, S>::type;  // flux storage
     using PL = Planes<S>;
@@ -221,11 +221,11 @@ __device__ __forceinline__ bool fused_tile(const FusedParams& FP, const TileIO& 
         // a band tile reads halo cells: wait for the senders' epoch of this
         // stage's input (bounded; a tile that gives up is skipped)
         __shared__ int s_gave_up;
-        const RemoteIO& R = *io.remote;
+        const RemoteIO& R = *pio.remote;
         if (threadIdx.x == 0) {
             s_gave_up = 0;
             if (!inactive && t < R.n_band_tiles) {
-                const unsigned long long need = io.ctrl->step * (unsigned long long)io.stages + io.stage;
+                const unsigned long long need = io.ctrl->step * (unsigned long long)pio.stages + pio.stage;
                 for (int i = 0; i < R.n_src && !s_gave_up; ++i) {
                     const unsigned long long* f = R.my_flags + R.src[i];
                     long long polls = 0;
@@ -514,7 +514,7 @@ __device__ __forceinline__ bool fused_tile(const FusedParams& FP, const TileIO& 
         }
         if constexpr (REMOTE) {
             // this cell's new state into every part that reads it
-            const RemoteIO& R = *io.remote;
+            const RemoteIO& R = *pio.remote;
             if (c < R.n_band) {
                 S qs[V];
 #pragma unroll
@@ -565,7 +565,7 @@ __device__ __forceinline__ bool fused_tile(const FusedParams& FP, const TileIO& 
                     }
                 }
                 if constexpr (REMOTE) {
-                    const RemoteIO& R = *io.remote;
+                    const RemoteIO& R = *pio.remote;
                     const int go = g - N;
                     if (go < R.n_own_ghost)
                         for (int i = R.ghost_off[go]; i < R.ghost_off[go + 1]; ++i) {
@@ -604,12 +604,12 @@ __device__ __forceinline__ bool fused_tile(const FusedParams& FP, const TileIO& 
     if constexpr (REMOTE) {
         // every band tile counts itself once its stores are visible; the
         // last one releases this stage's epoch to the readers
-        const RemoteIO& R = *io.remote;
+        const RemoteIO& R = *pio.remote;
         if (t < R.n_band_tiles) {
             __syncthreads();
             if (threadIdx.x == 0) {
                 __threadfence_system();
-                const unsigned long long epoch = io.ctrl->step * (unsigned long long)io.stages + io.stage + 1;
+                const unsigned long long epoch = io.ctrl->step * (unsigned long long)pio.stages + pio.stage + 1;
                 const unsigned long long done = atomicAdd(R.ctr, 1ull) + 1ull;
                 if (done == epoch * (unsigned long long)R.n_band_tiles) {
                     __threadfence_system();
@@ -625,7 +625,7 @@ __device__ __forceinline__ bool fused_tile(const FusedParams& FP, const TileIO& 
 template <class M, int FLUX>
 __global__ void __launch_bounds__(kTileMax) k_tile_fused(FusedParams FP, TileIO io) {
     pdl_trigger();
-    fused_tile<M, FLUX, false, false>(FP, io, (int)blockIdx.x);
+    fused_tile<M, FLUX, false, false>(FP, io, (int)blockIdx.x, PartIO{});
 }
 
 // A decomposition part's launches, one CTA per tile.  MODE 1: tiles
@@ -636,9 +636,9 @@ __global__ void __launch_bounds__(kTileMax) k_tile_fused(FusedParams FP, TileIO 
 // register cap on these launches restores 64 registers but runs slower
 // still, so they keep the compiler's choice.
 template <class M, int FLUX, int MODE>
-__global__ void __launch_bounds__(kTileMax) k_tile_fused_part(FusedParams FP, TileIO io) {
+__global__ void __launch_bounds__(kTileMax) k_tile_fused_part(FusedParams FP, TileIO io, PartIO pio) {
     pdl_trigger();
-    fused_tile<M, FLUX, MODE == 2, true>(FP, io, (MODE == 1 ? io.t0 : 0) + (int)blockIdx.x);
+    fused_tile<M, FLUX, MODE == 2, true>(FP, io, (MODE == 1 ? pio.t0 : 0) + (int)blockIdx.x, pio);
 }
 
 // Work-list schedule: as many CTAs as fit on the device at once, each taking
@@ -655,7 +655,7 @@ __global__ void __launch_bounds__(kTileMax) k_tile_fused_work(FusedParams FP, Ti
         __syncthreads();
         const int t = s_t;
         if (t >= n_tiles) return;
-        if (!fused_tile<M, FLUX, false, true>(FP, io, t)) return;
+        if (!fused_tile<M, FLUX, false, true>(FP, io, t, PartIO{})) return;
         __syncthreads();  // every thread is done with this tile's shared memory (and s_t)
     }
 }
@@ -694,7 +694,9 @@ struct FusedLaunch {
         return std::max(1, std::min(n_tiles, sms * std::max(nb, 1)));
     }
     // io.work != nullptr: the work-list schedule on `grid` CTAs
-    static void stage(const FusedParams& FP, const TileIO& io, cudaStream_t st, bool pdl, int n_tiles, int grid) {
+    // part: a decomposition part's launch (its tile offset, in-launch exchange)
+    static void stage(const FusedParams& FP, const TileIO& io, cudaStream_t st, bool pdl, int n_tiles, int grid,
+                      const PartIO* part = nullptr) {
         const size_t sm = smem(FP);
         cudaLaunchConfig_t cfg = {};
         cfg.gridDim = dim3((unsigned)(io.work ? grid : n_tiles));
@@ -709,12 +711,12 @@ struct FusedLaunch {
         if (io.work) {
             if (FP.P.flux == 1) cudaLaunchKernelEx(&cfg, k_tile_fused_work<M, 1>, FP, io, n_tiles);
             else cudaLaunchKernelEx(&cfg, k_tile_fused_work<M, 2>, FP, io, n_tiles);
-        } else if (io.remote) {
-            if (FP.P.flux == 1) cudaLaunchKernelEx(&cfg, k_tile_fused_part<M, 1, 2>, FP, io);
-            else cudaLaunchKernelEx(&cfg, k_tile_fused_part<M, 2, 2>, FP, io);
-        } else if (io.t0 != 0 || FP.P.n_own != FP.P.n_real) {
-            if (FP.P.flux == 1) cudaLaunchKernelEx(&cfg, k_tile_fused_part<M, 1, 1>, FP, io);
-            else cudaLaunchKernelEx(&cfg, k_tile_fused_part<M, 2, 1>, FP, io);
+        } else if (part && part->remote) {
+            if (FP.P.flux == 1) cudaLaunchKernelEx(&cfg, k_tile_fused_part<M, 1, 2>, FP, io, *part);
+            else cudaLaunchKernelEx(&cfg, k_tile_fused_part<M, 2, 2>, FP, io, *part);
+        } else if (part) {
+            if (FP.P.flux == 1) cudaLaunchKernelEx(&cfg, k_tile_fused_part<M, 1, 1>, FP, io, *part);
+            else cudaLaunchKernelEx(&cfg, k_tile_fused_part<M, 2, 1>, FP, io, *part);
         } else {
             if (FP.P.flux == 1) cudaLaunchKernelEx(&cfg, k_tile_fused<M, 1>, FP, io);
             else cudaLaunchKernelEx(&cfg, k_tile_fused<M, 2>, FP, io);
@@ -727,7 +729,7 @@ cudaError_t prepare_fused(int precision, const FusedParams& FP);
 size_t smem_fused(int precision, const FusedParams& FP);
 int work_grid_fused(int precision, const FusedParams& FP, int n_tiles);
 void launch_fused(int precision, const FusedParams& FP, const TileIO& io, cudaStream_t st, bool pdl, int n_tiles,
-                  int grid);
+                  int grid, const PartIO* part = nullptr);
 }  // namespace tile
 
 }  // namespace fvgpu

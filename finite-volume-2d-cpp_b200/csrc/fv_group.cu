@@ -387,7 +387,10 @@ int64_t group_step(fv_group* g, const std::vector<double>& alpha, int b, bool fi
     // the buffer role of stage k's output (tmp[0], tmp[1], sbase[0], sbase[1])
     auto role_of = [&](int k) { return S == 1 ? 2 + (1 - b) : (k == S - 1 ? 2 + b : k % 2); };
     int64_t n = 0;
-    for (int j = 0; j < nl; ++j) n += step_open(g->parts[j], alpha, b, first, cur[j], nullptr, !g->p2p);
+    for (int j = 0; j < nl; ++j) {
+        n += step_open(g->parts[j], alpha, b, first, cur[j], nullptr, !g->p2p);
+        cur[j].part = true;
+    }
     if (g->p2p) {
         // the previous step's last stage must have reached the halo before
         // the dt kernel reads it

@@ -2,6 +2,7 @@
 
 #include <dlfcn.h>
 
+#include <cstdlib>
 #include <mutex>
 #include <type_traits>
 
@@ -13,7 +14,13 @@ const NcclApi* nccl_api(std::string* err) {
     static bool ok = false;
     static std::string why;
     std::call_once(once, [] {
-        void* h = dlopen("libnccl.so.2", RTLD_NOW | RTLD_GLOBAL);
+        // FVGPU_NCCL_LIB names the NCCL library to use: a process that also
+        // loads PyTorch must hold PyTorch's own copy, since a second library
+        // of the same soname loaded first would stand in for it
+        const char* path = std::getenv("FVGPU_NCCL_LIB");
+        void* h = nullptr;
+        if (path && *path) h = dlopen(path, RTLD_NOW | RTLD_GLOBAL);
+        if (!h) h = dlopen("libnccl.so.2", RTLD_NOW | RTLD_GLOBAL);
         if (!h) {
             const char* e = dlerror();
             why = std::string("cannot load libnccl.so.2: ") + (e ? e : "unknown error");

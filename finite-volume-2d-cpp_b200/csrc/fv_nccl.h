@@ -1,7 +1,7 @@
 // NCCL entry points of a domain decomposition's exchanges, resolved at run
-// time from libnccl.so.2 (the copy a host process has already loaded, e.g.
-// PyTorch's, else the system's), so that the library itself loads and runs
-// single-part solves without NCCL.
+// time (the library named by the FVGPU_NCCL_LIB environment variable, else
+// libnccl.so.2: the copy the process has already loaded, else the system's),
+// so that the library itself loads and runs single-part solves without NCCL.
 #pragma once
 #include <nccl.h>
 

@@ -128,7 +128,10 @@ struct StepCursor {
     int b = 0;
     const void* in = nullptr;
     void* out = nullptr;
-    // the next fused stage launch exchanges its halo inside (device memory), or nullptr
+    // a decomposition part: its fused launches use the part kernel (owned
+    // count from the tile info); remote: the next one exchanges its halo
+    // inside (device memory), or nullptr
+    bool part = false;
     const RemoteIO* remote = nullptr;
 };
 // with_dt = false: step_open leaves the dt kernel to a later step_dt (a

@@ -74,10 +74,6 @@ struct TileIO {
     double* qt;                // [n_total][V] time derivatives of the smoothing phases (FP64)
     int* work;                 // fused stage kernel, work-list schedule: this launch's tile counter
     int* work_reset;           // dt kernel: tile counters zeroed after the dependency wait, or nullptr
-    int t0;                    // fused stage kernel, one CTA per tile: the first tile of this launch
-    const struct RemoteIO* remote;  // fused stage kernel of a decomposition's part: the halo
-                                    // exchange done inside the launch (device memory), or nullptr
-    int stage, stages;         // with remote: this launch's RK stage, and the step's stages
 };
 constexpr int kWorkSlots = 8;  // tile counters of the work-list schedule (one per RK stage)
 
@@ -107,6 +103,14 @@ struct RemoteIO {
     int n_src;
     int* err;
     long long limit;
+};
+// A decomposition part's fused stage launch, passed beside TileIO (whose
+// layout the single-solver kernel keeps: a larger TileIO made the FP64
+// fused kernel 1.1 % slower).
+struct PartIO {
+    int t0;                    // the launch's first tile
+    const RemoteIO* remote;    // the halo exchange inside the launch (device memory), or nullptr
+    int stage, stages;         // with remote: this launch's RK stage, and the step's stages
 };
 __device__ __forceinline__ unsigned long long ld_acquire_sys_u64(const unsigned long long* p) {
     unsigned long long v;

@@ -18,8 +18,9 @@ void launch_stage_exact(const TileParams& TP, const TileIO& io, cudaStream_t st,
 cudaError_t prepare_fused_exact(const FusedParams& FP) { return FusedLaunch<MExact>::prepare(FP); }
 size_t smem_fused_exact(const FusedParams& FP) { return FusedLaunch<MExact>::smem(FP); }
 int work_grid_fused_exact(const FusedParams& FP, int n_tiles) { return FusedLaunch<MExact>::work_grid(FP, n_tiles); }
-void launch_fused_exact(const FusedParams& FP, const TileIO& io, cudaStream_t st, bool pdl, int n_tiles, int grid) {
-    FusedLaunch<MExact>::stage(FP, io, st, pdl, n_tiles, grid);
+void launch_fused_exact(const FusedParams& FP, const TileIO& io, cudaStream_t st, bool pdl, int n_tiles, int grid,
+                        const PartIO* part) {
+    FusedLaunch<MExact>::stage(FP, io, st, pdl, n_tiles, grid, part);
 }
 }  // namespace tile
 }  // namespace fvgpu

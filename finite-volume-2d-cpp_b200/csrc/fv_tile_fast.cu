@@ -12,7 +12,8 @@ void launch_stage_exact(const TileParams& TP, const TileIO& io, cudaStream_t st,
 cudaError_t prepare_fused_exact(const FusedParams& FP);
 size_t smem_fused_exact(const FusedParams& FP);
 int work_grid_fused_exact(const FusedParams& FP, int n_tiles);
-void launch_fused_exact(const FusedParams& FP, const TileIO& io, cudaStream_t st, bool pdl, int n_tiles, int grid);
+void launch_fused_exact(const FusedParams& FP, const TileIO& io, cudaStream_t st, bool pdl, int n_tiles, int grid,
+                        const PartIO* part);
 
 cudaError_t prepare(int precision, const TileParams& TP) {
     if (precision == 0) return prepare_exact(TP);
@@ -50,10 +51,10 @@ int work_grid_fused(int precision, const FusedParams& FP, int n_tiles) {
     return FusedLaunch<MF32>::work_grid(FP, n_tiles);
 }
 void launch_fused(int precision, const FusedParams& FP, const TileIO& io, cudaStream_t st, bool pdl, int n_tiles,
-                  int grid) {
-    if (precision == 0) launch_fused_exact(FP, io, st, pdl, n_tiles, grid);
-    else if (precision == 1) FusedLaunch<MF64>::stage(FP, io, st, pdl, n_tiles, grid);
-    else FusedLaunch<MF32>::stage(FP, io, st, pdl, n_tiles, grid);
+                  int grid, const PartIO* part) {
+    if (precision == 0) launch_fused_exact(FP, io, st, pdl, n_tiles, grid, part);
+    else if (precision == 1) FusedLaunch<MF64>::stage(FP, io, st, pdl, n_tiles, grid, part);
+    else FusedLaunch<MF32>::stage(FP, io, st, pdl, n_tiles, grid, part);
 }
 }  // namespace tile
 }  // namespace fvgpu

@@ -60,10 +60,30 @@ class _RunInfo(C.Structure):
 _lib = None
 
 
+def _torch_nccl():
+    """PyTorch's bundled NCCL library (found without importing torch), or None."""
+    try:
+        import importlib.util
+        spec = importlib.util.find_spec("nvidia.nccl")
+    except (ImportError, ValueError):
+        return None
+    for base in (spec.submodule_search_locations or []) if spec else []:
+        path = os.path.join(base, "lib", "libnccl.so.2")
+        if os.path.exists(path):
+            return path
+    return None
+
+
 def lib():
     """Load libfvgpu.so (raises if it is not built: there is no fallback)."""
     global _lib
     if _lib is None:
+        # decompositions load NCCL on first use: make it PyTorch's copy, so a
+        # later `import torch` in this process finds the NCCL it was built for
+        if "FVGPU_NCCL_LIB" not in os.environ:
+            path = _torch_nccl()
+            if path:
+                os.environ["FVGPU_NCCL_LIB"] = path
         if not os.path.exists(LIB_PATH):
             raise FvError(-100, f"{LIB_PATH} is not built; run `make -C {HERE}` (or __graft_entry__.build())")
         L = C.CDLL(LIB_PATH)

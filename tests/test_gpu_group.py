@@ -205,3 +205,24 @@ def test_group_full_size_forward_step():
         print(f"{prec}: halo cells per stage {inf['halo_cells']} of {mesh.n_real}")
         assert r["time"] == r1["time"]
         assert q.tobytes() == q1.tobytes()
+
+
+def test_group_with_nccl_leaves_torch_importable():
+    """A decomposition that loads NCCL before PyTorch does loads PyTorch's own
+    copy (fvgpu.py sets FVGPU_NCCL_LIB), so `import torch` afterwards in the
+    same process finds the NCCL it was built for."""
+    import os
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    code = (f"import sys; sys.path[:0] = [{os.path.join(root, 'finite-volume-2d-cpp_b200')!r}]\n"
+            "import fvgpu, meshgen, physics as P\n"
+            "mesh = fvgpu.Mesh.from_elements(meshgen.forward_step(n=20))\n"
+            "g = fvgpu.Group(mesh, P.forward_step(order2=True), 'fp64', n_parts=2, nccl_local=True)\n"
+            "g.run(2)\n"
+            "g.close()\n"
+            "import torch\n"
+            "print('torch', torch.__version__)\n")
+    env = {k: v for k, v in os.environ.items() if k != "FVGPU_NCCL_LIB"}
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=300, env=env)
+    assert r.returncode == 0 and "torch" in r.stdout, r.stdout + r.stderr
