@@ -629,8 +629,8 @@ __global__ void __launch_bounds__(kTileMax) k_tile_fused(FusedParams FP, TileIO 
 }
 
 // A decomposition part's launches, one CTA per tile.  MODE 1: tiles
-// [io.t0, io.t0 + grid) (the band and interior launches); MODE 2: the halo
-// exchange inside the launch (io.remote).  Kept apart from k_tile_fused,
+// [pio.t0, pio.t0 + grid) (the band and interior launches); MODE 2: the halo
+// exchange inside the launch (pio.remote).  Kept apart from k_tile_fused,
 // whose register allocation the tile offset and the owned count from the
 // tile info upset (FP32: 80 registers instead of 64, 5.7 % slower); a
 // register cap on these launches restores 64 registers but runs slower

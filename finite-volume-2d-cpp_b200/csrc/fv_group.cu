@@ -247,7 +247,6 @@ struct fv_group {
     int n_parts = 1, rank = 0, n_ranks = 1, lo = 0, hi = 1;
     bool nccl_local = false;
     int owner0 = 0;
-    int64_t g_real = 0, g_total = 0;
     cudaStream_t stream = nullptr;
     // overlap: each stage computes the band tiles (every state another part
     // reads) and then the exchange on cstream (high priority) while the
@@ -830,7 +829,6 @@ int fv_group_create(const fv_mesh* fm, const fv_physics* ph, int32_t precision, 
     g->lo = o->rank * (P / R); g->hi = g->lo + P / R;
     g->nccl_local = o->nccl_local != 0;
     if (o->timeout_ms > 0) g->timeout_ms = o->timeout_ms;
-    g->g_real = fm->m.n_real; g->g_total = fm->m.n_total;
     GK(cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking));
     // the communicator first: every later failure of one process then ends
     // in the others' bounded waits, not in an unbounded initialisation
