@@ -665,7 +665,10 @@ def measure_decomposed(args, mesh, geo, ph, alpha, ic, prec, parts_per_gpu, loca
         out = {"value": mesh.n_real * len(alpha) * steps / (ms_max / 1e3), "unit": UNIT, "ms_per_step": ms_max / steps,
                "steps": steps, "n_parts": n_parts, "precision": prec, "gpu_launches": int(launches),
                "clocks": clk.summary(), "rank_parts": gi, "halo_bytes_per_stage": gi["halo_cells"] * cell_bytes,
-               "exchange": ("after all tiles" if args.serial_exchange else
+               "exchange": ("inside each stage launch: band tiles wait for their senders, store into the "
+                            "readers' buffers and release an epoch, beside the interior tiles"
+                            if gi["transport"] == "p2p" and ph.order2 else
+                            "after all tiles" if args.serial_exchange else
                             "band tiles + exchange on a second stream beside the interior tiles"),
                "transport": gi["transport"],
                "parallelism": (f"{n_parts} parts over {world} processes (NCCL)" if world > 1
