@@ -30,7 +30,18 @@ def _cases():
                          lambda g: P.ic_forward_step(g.n_total), P.RK5_ALPHA),
         "naca_local_dt": (lambda: meshgen.naca_ogrid(48, 12), P.naca, lambda g: P.ic_naca(g.n_total), P.RK5_ALPHA),
         "sod_first_order": (lambda: meshgen.sod_strip(40, 4), P.sod, lambda g: P.ic_sod(g.ccx), P.RK1_ALPHA),
+        "mixed_elements": (_mixed_strip, _mixed_physics, lambda g: P.ic_sod(g.ccx), P.RK5_ALPHA),
     }
+
+
+def _mixed_strip():
+    from test_mixed_elements import mixed_strip
+    return mixed_strip(32, 8)
+
+
+def _mixed_physics():
+    return P.Physics(V=4, flux="roe_fs", order2=True, limiter="venkat", K=5.0, dt_kind="cfl_sum", cfl=0.5,
+                     global_dt=True, bcs={"wall": ("wall", None), "ends": ("copy", None)})
 
 
 def _local_geom(g, pl):
@@ -56,7 +67,7 @@ def _local_geom(g, pl):
                     bound_edges=be.astype(np.uint32), bound_group=g.bound_group[rb].astype(np.int32))
 
 
-@pytest.mark.parametrize("case", ["forward_step", "naca_local_dt", "sod_first_order"])
+@pytest.mark.parametrize("case", ["forward_step", "naca_local_dt", "sod_first_order", "mixed_elements"])
 @pytest.mark.parametrize("n_parts", [2, 3, 5])
 def test_part_plans_cover_the_mesh(case, n_parts, oracle):
     import fvgpu
@@ -205,7 +216,8 @@ def _decomposed_run(rank, world, case, n_parts, steps, out):
 
 
 @pytest.mark.parametrize("case,n_parts,steps", [("forward_step", 2, 8), ("forward_step", 4, 6),
-                                                ("naca_local_dt", 4, 6), ("sod_first_order", 2, 10)])
+                                                ("naca_local_dt", 4, 6), ("sod_first_order", 2, 10),
+                                                ("mixed_elements", 4, 8)])
 def test_decomposed_oracle_run_on_two_gloo_ranks(case, n_parts, steps, oracle):
     import torch.multiprocessing as mp
 
